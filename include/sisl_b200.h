@@ -1,0 +1,219 @@
+/*
+ * sisl_b200.h -- C ABI of the B200 (sm_100a) SISL timestep.
+ *
+ * Drop-in boundary for the semi-implicit semi-Lagrangian core of the Suetes
+ * regional 3-D model (reference: suetes/regional3d/steppers.py,
+ * suetes/regional3d/euler.py, suetes/regional3d/operators.py).  The
+ * reference is pure Python/JAX and has no FFI of its own; each entry point
+ * below names the reference call it replaces (file:line in the reference
+ * project).  A jax.ffi / ctypes binding maps those Python calls onto these
+ * functions; no torch or C++ type crosses this boundary.
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer on the current CUDA device,
+ *    of the core's precision (SISL_F32 or SISL_F64) unless stated.
+ *  - Field layout: a field of stagger s has the extents of the reference
+ *    array, (ex, ey, ez) = (nx + [s==U], ny + [s==V], nz + [s==W]), stored
+ *    x-fastest: element (i, j, k) at offset i + ex * (j + ey * k).  This is
+ *    the Fortran order of the reference's (ex, ey, ez) array (numpy
+ *    np.asfortranarray / a torch tensor permuted to (ez, ey, ex) contiguous).
+ *    2-D horizontal arrays use i + ex * j.
+ *  - Thermodynamic state is passed in perturbation form: pi_p = pi - pi_bg,
+ *    th_p = th_v - theta_bg.
+ *  - Streams are cudaStream_t passed as void*; NULL is the legacy stream.
+ *  - Outputs are caller-allocated; scratch comes from a caller-provided
+ *    workspace of sisl_workspace_bytes() bytes (256-byte aligned).
+ *  - Return value: SISL_OK, a negative error code, or SISL_NOT_CONVERGED
+ *    (the GMRES iteration limit was hit; outputs are still written, as in
+ *    the reference, which discards GMRES's status at steppers.py:466).
+ *  - A core is not re-entrant: calls that share a core must be serialised
+ *    (they share its pinned host scratch).
+ */
+#ifndef SISL_B200_H
+#define SISL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { SISL_F32 = 0, SISL_F64 = 1 };
+enum { SISL_LOC_M = 0, SISL_LOC_U = 1, SISL_LOC_V = 2, SISL_LOC_W = 3 };
+enum { SISL_GMRES_BATCHED = 0, SISL_GMRES_INCREMENTAL = 1 };
+enum {
+  SISL_WS_STEP = 0, SISL_WS_GMRES = 1, SISL_WS_DEPARTURE = 2, SISL_WS_EXPLICIT = 3, SISL_WS_OPERATOR = 4,
+  SISL_WS_FFSL = 5
+};
+enum {
+  SISL_RELAX_U = 1, SISL_RELAX_V = 2, SISL_RELAX_W = 4, SISL_RELAX_TH = 8, SISL_RELAX_PI = 16
+};
+/* kernel classes for sisl_timing_select */
+enum {
+  SISL_K_NONE = 0, SISL_K_MATVEC = 1, SISL_K_PRECOND = 2, SISL_K_DOTS = 3, SISL_K_UPDATE = 4,
+  SISL_K_SL = 5, SISL_K_EXPLICIT = 6, SISL_K_OTHER = 7
+};
+
+#define SISL_OK 0
+#define SISL_NOT_CONVERGED 1
+#define SISL_ERR_ARG (-1)
+#define SISL_ERR_CUDA (-2)
+#define SISL_ERR_WORKSPACE (-3)
+#define SISL_ERR_NONFINITE (-4)
+
+/* Grid extents and spacing: RegionalGrid3D(nx, ny, nz, dx, dy, dz, ...)
+ * (geometry.py:141) plus CGridOperator3D's periodic axes (operators.py:16). */
+typedef struct SislGrid {
+  int32_t nx, ny, nz;
+  int32_t periodic_x, periodic_y;
+  int32_t dtype;
+  double dx, dy, dz;
+} SislGrid;
+
+/* Physical constants and SISL/GMRES settings: build_dynamical_core kwargs
+ * (steppers.py:37-53), the constants dict and SISLStepper3D's arguments. */
+typedef struct SislParams {
+  double dt, alpha;
+  double g, cp, Rd, cvd, p0;
+  double pi_scale;         /* 1000 (steppers.py:396) */
+  double nu_div, nu_h;     /* Euler3D.nu_div, Euler3D.nu_h (euler.py:62-67) */
+  double solver_tol, solver_atol;
+  int32_t solver_maxiter;  /* restart cycles */
+  int32_t solver_restart;  /* Krylov dimension, <= 128 */
+  int32_t solve_method;    /* SISL_GMRES_* */
+  int32_t use_limiter;
+  int32_t departure_iterations; /* 2 (steppers.py:318) */
+  int32_t pad;
+} SislParams;
+
+/* float64 background and metrics (device pointers, device layout):
+ * Euler3D.theta_bg / pi_bg / tau_damp (euler.py:76-121) and
+ * RegionalGrid3D.Z_m, dz_m_full, dz_w_full, z_xi_w, z_eta_w, m_factors,
+ * f_u, f_v, dm_dx_m, dm_dy_m (geometry.py:190-261).  Read only during
+ * sisl_core_create. */
+typedef struct SislBackground {
+  const double *theta_bg, *pi_bg, *Z_m, *dz_m_full, *dz_w_full, *z_xi_w, *z_eta_w, *tau_damp;
+  const double *m_m, *m_u, *m_v, *f_u, *f_v, *dm_dx_m, *dm_dy_m;
+} SislBackground;
+
+typedef struct SislCore SislCore;
+
+typedef struct SislSolveInfo {
+  int32_t cycles;          /* restart cycles run */
+  int32_t arnoldi_steps;   /* matvec + preconditioner applications inside cycles */
+  int32_t converged;       /* 1 when ||M(b - A x)|| <= atol */
+  int32_t pad;
+  double residual_norm;    /* final preconditioned residual norm */
+  double atol;             /* max(tol * ||b||, solver_atol) */
+  double b_norm;
+} SislSolveInfo;
+
+/* Prognostic state + SISL history (the state pytree of steppers.py:69-80,
+ * 1003-1071) in perturbation form. */
+typedef struct SislState {
+  void *u, *v, *w, *eta_dot, *pi_p, *th_p, *rho;
+  void *u_prev, *v_prev, *w_prev, *eta_dot_prev, *tend_th_prev;
+  double is_first_step;
+} SislState;
+
+/* Lateral relaxation applied as bc_fn (steppers.py:1042):
+ * f <- (1 - mask) f + mask * exterior on horizontal masks (precision of the
+ * core), e.g. the x relaxation of schaer_mountain_3d/run.py:104-126. */
+typedef struct SislRelaxation {
+  int32_t fields;          /* SISL_RELAX_* bitmask */
+  int32_t pad;
+  const void *mask_m, *mask_u, *mask_v;
+  double ext[5];           /* exterior u, v, w, th_p, pi_p */
+  const void* ext_field[5];/* optional 3-D exterior fields, override ext[] */
+} SislRelaxation;
+
+typedef struct SislStepInfo {
+  SislSolveInfo solve[2];
+  int64_t kernel_launches;
+} SislStepInfo;
+
+int sisl_version(void);
+const char* sisl_status_string(int status);
+size_t sisl_field_elems(const SislGrid* grid, int loc);
+
+/* Build the derived coefficient set of Euler3D.precompute_bg (euler.py:127-160)
+ * and VerticalPreconditioner.precompute_banded (steppers.py:153-185) once. */
+int sisl_core_create(const SislGrid* grid, const SislParams* params, const SislBackground* bg, void* stream,
+                     SislCore** out);
+int sisl_core_destroy(SislCore* core);
+/* Replace the GMRES settings of SemiImplicitSolver3D(solver_tol,
+ * solver_maxiter, solver_restart) (steppers.py:384-399) on an existing core. */
+int sisl_core_set_solver(SislCore* core, double tol, double atol, int maxiter, int restart, int method);
+size_t sisl_workspace_bytes(const SislCore* core, int what);
+
+/* Euler3D.linear_operator(state_prime, bg, dt, alpha) (euler.py:374-439).
+ * in/out: u, v, w, pi_p, eta_dot (physical). */
+int sisl_linear_operator(SislCore* core, const void* const in[5], void* const out[5], void* ws, size_t ws_bytes,
+                         void* stream);
+/* SemiImplicitSolver3D.solve.A_fn (steppers.py:439-461): the matvec on the
+ * scaled solver vector (u, v, w, pi * pi_scale, eta_dot * dz_w_full). */
+int sisl_helmholtz_matvec(SislCore* core, const void* const in[5], void* const out[5], void* stream);
+/* VerticalPreconditioner.__call__ (steppers.py:187-253) on the scaled vector.
+ * out must not alias in (except u, v). */
+int sisl_precond_apply(SislCore* core, const void* const in[5], void* const out[5], void* stream);
+/* SemiImplicitSolver3D.solve(rhs_prime, bg, x0) (steppers.py:401-496):
+ * physical rhs (u, v, w, pi_p, eta_dot) and x0 (NULL: x0 = rhs as in the
+ * reference); x may alias x0. */
+int sisl_gmres_solve(SislCore* core, const void* const rhs[5], const void* const x0[5], void* const x[5],
+                     void* ws, size_t ws_bytes, void* stream, SislSolveInfo* info);
+/* SemiLagrangianAdvector3D.compute_departure_indices(state, loc, iterations)
+ * (steppers.py:318-360); coords[3] have the extents of stagger loc. */
+int sisl_departure(SislCore* core, int loc, const void* u, const void* v, const void* eta_dot, int iterations,
+                   void* const coords[3], void* ws, size_t ws_bytes, void* stream);
+/* tensor_product_interp_3d(field, coords, use_limiter) (operators.py:146-209)
+ * for any field shape and any coordinate-array shape (both x-fastest). */
+int sisl_tricubic(int dtype, const int32_t src_shape[3], const void* field, const int32_t dst_shape[3],
+                  const void* const coords[3], void* out, int use_limiter, void* stream);
+/* map_coordinates(field, coords, order=1, mode='nearest'), the trilinear
+ * gather of SemiLagrangianAdvector3D.advect_linear (steppers.py:362-367). */
+int sisl_trilinear(int dtype, const int32_t src_shape[3], const void* field, const int32_t dst_shape[3],
+                   const void* const coords[3], void* out, void* stream);
+/* FluxFormAdvector.advect_1d(scalar_1d, cfl_inter_1d, periodic)
+ * (steppers.py:552-594) on nlines independent lines: scalar is (nlines, n)
+ * and cfl (nlines, n + 1), line-major; float64 workspace of
+ * sisl_ffsl_lines_workspace_bytes(n, nlines) bytes. */
+size_t sisl_ffsl_lines_workspace_bytes(int n, int nlines);
+int sisl_ffsl_lines(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic, void* out,
+                    void* ws, size_t ws_bytes, void* stream);
+/* Euler3D.get_tendencies(state_prime, bg, is_explicit) (euler.py:208-372):
+ * is_explicit = 0 gives the linear tendencies of the implicit operator.
+ * Same arguments as sisl_explicit_tendencies. */
+int sisl_tendencies(SislCore* core, int is_explicit, const void* const state_prime[6], void* const tend[6],
+                    void* const phys_diff[4], void* ws, size_t ws_bytes, void* stream);
+/* Euler3D.get_tendencies(state_prime, bg, is_explicit=True) (euler.py:208-372)
+ * and nonlinear_pi_tendency (euler.py:162-186).
+ * state_prime: u, v, w, pi_p, eta_dot, th_p.
+ * tend: u, v, w, pi (linear part), th_v, nonlinear pi; phys_diff: u, v, w, th_v. */
+int sisl_explicit_tendencies(SislCore* core, const void* const state_prime[6], void* const tend[6],
+                             void* const phys_diff[4], void* ws, size_t ws_bytes, void* stream);
+/* FluxFormAdvector.advect_3d_split(field, state, bg) (steppers.py:596-647):
+ * mass-conserving split transport of a mass-point density by u, v, eta_dot. */
+int sisl_ffsl_advect(SislCore* core, const void* field, const void* u, const void* v, const void* eta_dot, void* out,
+                     void* ws, size_t ws_bytes, void* stream);
+/* Equation of state rho = p0 / (Rd th_v) pi^(cvd/Rd) (steppers.py:1055-1056)
+ * from perturbation th_p, pi_p. */
+int sisl_eos(SislCore* core, const void* th_p, const void* pi_p, void* rho, void* stream);
+/* SISLStepper3D.step(state, t, forcing, bc_fn) (steppers.py:720-1073) with
+ * bc_fn = identity (relax NULL) or a lateral relaxation.  in and out must not
+ * overlap, except that out->*_prev may equal the matching in field. */
+int sisl_step(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
+              size_t ws_bytes, void* stream, SislStepInfo* info);
+
+/* Instrumentation: number of kernels this library launched, and CUDA-event
+ * timing of one kernel class (events recorded around each launch on the
+ * launching stream; read after the stream is synchronised). */
+int64_t sisl_kernel_launches(void);
+int sisl_timing_select(SislCore* core, int kernel_class);
+int sisl_timing_read(SislCore* core, double* total_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SISL_B200_H */

@@ -1,0 +1,966 @@
+// C ABI and host runtime of the SISL timestep: the core object (precomputed
+// coefficients), workspace carving, the GMRES driver loop and the step
+// orchestration of SISLStepper3D.step (steppers.py:720-1073).
+#include "../../include/sisl_b200.h"
+
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "sisl_core.cuh"
+#include "sisl_explicit.cuh"
+#include "sisl_gmres.cuh"
+
+using namespace sisl;
+
+static std::atomic<int64_t> g_launches{0};
+
+struct SislCore {
+  SislGrid grid;
+  SislParams prm;
+  Dims d;
+  Scalars s;
+  void* coef_mem = nullptr;
+  void* coef_ptr[C_COUNT];
+  GHostView* hv = nullptr;  // pinned
+  int timing_class = SISL_K_NONE;
+  std::vector<cudaEvent_t> ev0, ev1;
+  size_t ev_used = 0;
+};
+
+namespace {
+
+size_t esize(int dtype) { return dtype == SISL_F64 ? 8 : 4; }
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+size_t pad64(size_t x) { return (x + 63) & ~(size_t)63; }
+
+// Scoped launch bookkeeping: counts kernels and, for the selected class,
+// brackets the launch with CUDA events on the launching stream.
+struct KScope {
+  SislCore* c;
+  cudaStream_t st;
+  bool timed;
+  KScope(SislCore* core, int cls, cudaStream_t s, int nkernels = 1) : c(core), st(s), timed(false) {
+    g_launches += nkernels;
+    if (c && c->timing_class == cls && cls != SISL_K_NONE) {
+      if (c->ev_used == c->ev0.size()) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        c->ev0.push_back(a);
+        c->ev1.push_back(b);
+      }
+      cudaEventRecord(c->ev0[c->ev_used], st);
+      timed = true;
+    }
+  }
+  ~KScope() {
+    if (timed) {
+      cudaEventRecord(c->ev1[c->ev_used], st);
+      c->ev_used++;
+    }
+  }
+};
+
+struct Carver {
+  char* base;
+  size_t off = 0;
+  void* take(size_t bytes) {
+    off = align256(off);
+    void* p = base ? base + off : nullptr;
+    off += bytes;
+    return p;
+  }
+};
+
+int check_cuda() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? SISL_OK : SISL_ERR_CUDA;
+}
+
+template <typename T>
+Coef<T> coef_of(const SislCore* c) {
+  T* a[C_COUNT];
+  for (int q = 0; q < C_COUNT; ++q) a[q] = (T*)c->coef_ptr[q];
+  return make_coef<T>(a, c->s);
+}
+
+int loc_of_field(int q) {  // solver vector field -> stagger
+  static const int L[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_W};
+  return L[q];
+}
+
+// ---------------------------------------------------------------------------
+// small utility kernels
+// ---------------------------------------------------------------------------
+// dst = src with pi scaled by pi_mul and eta_dot by dz_w (mode 1), 1/dz_w
+// (mode 2) or unchanged (mode 0); also a plain per-field scale.
+template <typename T>
+__global__ void scale5_kernel(Dims d, CVec5<T> src, Vec5<T> dst, T pi_mul, int eta_mode, const T* __restrict__ dzw,
+                              const T* __restrict__ idzw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i > d.nx || j > d.ny || k > d.nz) return;
+  if (j < d.ny && k < d.nz) { const int p = iu(d, i, j, k); dst.f[0][p] = src.f[0][p]; }
+  if (i < d.nx && k < d.nz) { const int p = iv(d, i, j, k); dst.f[1][p] = src.f[1][p]; }
+  if (i < d.nx && j < d.ny) {
+    const int p = iw(d, i, j, k);
+    dst.f[2][p] = src.f[2][p];
+    T e = src.f[4][p];
+    if (eta_mode == 1) e *= dzw[p];
+    else if (eta_mode == 2) e *= idzw[p];
+    dst.f[4][p] = e;
+  }
+  if (i < d.nx && j < d.ny && k < d.nz) { const int p = im(d, i, j, k); dst.f[3][p] = src.f[3][p] * pi_mul; }
+}
+
+// zero the padding gaps of nvec contiguous solver vectors
+template <typename T>
+__global__ void zero_gaps_kernel(T* base, size_t npad, int nvec, size_t o0, size_t o1, size_t o2, size_t o3,
+                                 size_t o4, size_t s0, size_t s1, size_t s2, size_t s3, size_t s4) {
+  const size_t off[5] = {o0, o1, o2, o3, o4};
+  const size_t sz[5] = {s0, s1, s2, s3, s4};
+  const int v = blockIdx.x;
+  if (v >= nvec) return;
+  T* vb = base + (size_t)v * npad;
+  for (int q = 0; q < 5; ++q) {
+    const size_t end = (q < 4) ? off[q + 1] : npad;
+    for (size_t e = off[q] + sz[q] + threadIdx.x; e < end; e += blockDim.x) vb[e] = T(0);
+  }
+}
+
+// lateral overrides after advection (steppers.py:858-869) and the zero
+// lid/ground rows of R_eta_dot (steppers.py:893)
+template <typename T>
+__global__ void sl_fixup_kernel(Dims d, T* rhs_u, T* rhs_v, const T* __restrict__ u0, const T* __restrict__ v0,
+                                T* reta) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;  // generic 2-D index
+  const int k = blockIdx.y;
+  // u faces 0 and nx for every (j, k)
+  if (a < d.ny && k < d.nz) {
+    const int p0 = iu(d, 0, a, k), pn = iu(d, d.nx, a, k);
+    if (d.px) rhs_u[pn] = rhs_u[p0];
+    else { rhs_u[p0] = u0[p0]; rhs_u[pn] = u0[pn]; }
+  }
+  if (a < d.nx && k < d.nz) {
+    const int p0 = iv(d, a, 0, k), pn = iv(d, a, d.ny, k);
+    if (d.py) rhs_v[pn] = rhs_v[p0];
+    else { rhs_v[p0] = v0[p0]; rhs_v[pn] = v0[pn]; }
+  }
+  if (k == 0) {
+    for (int jj = 0; jj < d.ny; ++jj) {
+      if (a < d.nx) {
+        reta[iw(d, a, jj, 0)] = T(0);
+        reta[iw(d, a, jj, d.nz)] = T(0);
+      }
+    }
+  }
+}
+
+dim3 box(int ex, int ey, int ez, dim3 blk) {
+  return dim3((ex + blk.x - 1) / blk.x, (ey + blk.y - 1) / blk.y, (ez + blk.z - 1) / blk.z);
+}
+
+// ---------------------------------------------------------------------------
+// GMRES workspace
+// ---------------------------------------------------------------------------
+template <typename T>
+struct GWork {
+  GState* gs;
+  GHostView* dview;  // device copy of the per-cycle summary
+  double* partial;
+  T* vec;  // (R + 4) contiguous vectors
+  size_t npad;
+  size_t off[5], sz[5];
+  int R;
+  T* V(int i) const { return vec + (size_t)(3 + i) * npad; }
+  T* xg() const { return vec; }
+  T* bg() const { return vec + npad; }
+  T* z() const { return vec + 2 * npad; }
+  Vec5<T> view(T* b) const {
+    Vec5<T> v;
+    for (int q = 0; q < 5; ++q) v.f[q] = b + off[q];
+    return v;
+  }
+  CVec5<T> cview(const T* b) const {
+    CVec5<T> v;
+    for (int q = 0; q < 5; ++q) v.f[q] = b + off[q];
+    return v;
+  }
+};
+
+template <typename T>
+GWork<T> carve_gmres(Carver& cv, const Dims& d, int R) {
+  GWork<T> g;
+  g.R = R;
+  size_t o = 0;
+  for (int q = 0; q < 5; ++q) {
+    g.off[q] = o;
+    g.sz[q] = field_size(d, loc_of_field(q));
+    o += pad64(g.sz[q]);
+  }
+  g.npad = o;
+  g.gs = (GState*)cv.take(sizeof(GState));
+  g.dview = (GHostView*)cv.take(sizeof(GHostView));
+  g.partial = (double*)cv.take(sizeof(double) * GM_MAXBLOCKS * (GM_MAXR + 2));
+  g.vec = (T*)cv.take(sizeof(T) * g.npad * (size_t)(R + 4));
+  return g;
+}
+
+template <typename T>
+CVec5<T> cvec(const void* const p[5]) {
+  CVec5<T> v;
+  for (int q = 0; q < 5; ++q) v.f[q] = (const T*)p[q];
+  return v;
+}
+template <typename T>
+Vec5<T> vec(void* const p[5]) {
+  Vec5<T> v;
+  for (int q = 0; q < 5; ++q) v.f[q] = (T*)p[q];
+  return v;
+}
+
+template <typename T>
+void scale5(SislCore* c, const Coef<T>& cf, CVec5<T> src, Vec5<T> dst, T pi_mul, int eta_mode, cudaStream_t st) {
+  KScope k(c, SISL_K_OTHER, st);
+  dim3 blk(32, 4, 2);
+  scale5_kernel<T><<<box(c->d.nx + 1, c->d.ny + 1, c->d.nz + 1, blk), blk, 0, st>>>(c->d, src, dst, pi_mul,
+                                                                                   eta_mode, cf.dzw, cf.idzw);
+}
+
+template <typename T>
+CVec5<T> as_const(Vec5<T> v) {
+  CVec5<T> r;
+  for (int q = 0; q < 5; ++q) r.f[q] = v.f[q];
+  return r;
+}
+
+// Restarted GMRES on the packed vectors g.bg (rhs) and g.xg (initial guess).
+template <typename T>
+int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, SislSolveInfo* info) {
+  const Dims& d = c->d;
+  const int R = g.R;
+  const size_t n = g.npad;
+  const int method = c->prm.solve_method;
+  const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+  GState* gs = g.gs;
+  CVec5<T> none{};
+  {
+    KScope k(c, SISL_K_OTHER, st);
+    gm_setup(gs, eps, c->prm.solver_tol, c->prm.solver_atol, R, method, st);
+  }
+  {
+    KScope k(c, SISL_K_DOTS, st);
+    gm_dots<T>(g.V(0), n, 0, g.bg(), n, g.partial, gs, 1 /*BNORM*/, 0, st);
+  }
+  if (method == SISL_GMRES_INCREMENTAL) {
+    {
+      KScope k(c, SISL_K_PRECOND, st);
+      launch_precond<T>(d, cf, g.cview(g.bg()), g.view(g.V(1)), nullptr, st);
+    }
+    KScope k(c, SISL_K_DOTS, st);
+    gm_dots<T>(g.V(0), n, 0, g.V(1), n, g.partial, gs, 2 /*MBNORM*/, 0, st);
+  }
+  {
+    KScope k(c, SISL_K_OTHER, st);
+    gm_init_tol(gs, st);
+  }
+  // residual of the initial guess
+  auto residual_and_read = [&](GHostView* out) -> int {
+    {
+      KScope k(c, SISL_K_MATVEC, st);
+      launch_matvec<T>(d, cf, g.cview(g.xg()), nullptr, g.cview(g.bg()), g.view(g.z()), nullptr, st);
+    }
+    {
+      KScope k(c, SISL_K_PRECOND, st);
+      launch_precond<T>(d, cf, g.cview(g.z()), g.view(g.V(0)), nullptr, st);
+    }
+    {
+      KScope k(c, SISL_K_DOTS, st);
+      gm_dots<T>(g.V(0), n, 0, g.V(0), n, g.partial, gs, 3 /*RNORM*/, 0, st);
+    }
+    GHostView* dv = g.dview;
+    {
+      KScope k(c, SISL_K_OTHER, st);
+      gm_snapshot(gs, dv, st);
+    }
+    if (cudaMemcpyAsync(out, dv, sizeof(GHostView), cudaMemcpyDeviceToHost, st) != cudaSuccess) return SISL_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return SISL_ERR_CUDA;
+    return SISL_OK;
+  };
+  GHostView* hv = c->hv;
+  int rc = residual_and_read(hv);
+  if (rc) return rc;
+  int cycles = 0, steps = 0;
+  while (cycles < c->prm.solver_maxiter && hv->rnorm > hv->atol) {
+    {
+      KScope k(c, SISL_K_OTHER, st);
+      gm_begin_cycle(gs, st);
+    }
+    for (int j = 0; j < R; ++j) {
+      {
+        KScope k(c, SISL_K_MATVEC, st);
+        launch_matvec<T>(d, cf, g.cview(g.V(j)), &gs->s[j], none, g.view(g.z()), &gs->active, st);
+      }
+      {
+        KScope k(c, SISL_K_PRECOND, st);
+        launch_precond<T>(d, cf, g.cview(g.z()), g.view(g.V(j + 1)), &gs->active, st);
+      }
+      {
+        KScope k(c, SISL_K_DOTS, st);
+        gm_dots<T>(g.V(0), n, j + 1, g.V(j + 1), n, g.partial, gs, 0 /*PROJ*/, 1, st);
+      }
+      {
+        KScope k(c, SISL_K_UPDATE, st);
+        gm_update<T>(g.V(0), n, j + 1, g.V(j + 1), n, -1.0, g.partial, gs, 1 /*ARNOLDI*/, 1, 0, st);
+      }
+    }
+    {
+      KScope k(c, SISL_K_OTHER, st);
+      gm_small_solve(gs, R, st);
+    }
+    {
+      KScope k(c, SISL_K_UPDATE, st);
+      gm_update<T>(g.V(0), n, R, g.xg(), n, 1.0, g.partial, gs, 0 /*NONE*/, 0, 1, st);
+    }
+    rc = residual_and_read(hv);
+    if (rc) return rc;
+    steps += hv->kdone;
+    cycles++;
+  }
+  if (info) {
+    info->cycles = cycles;
+    info->arnoldi_steps = steps;
+    info->residual_norm = hv->rnorm;
+    info->atol = hv->atol;
+    info->b_norm = hv->bnorm;
+    info->converged = (hv->rnorm <= hv->atol) ? 1 : 0;
+  }
+  if (!std::isfinite(hv->rnorm)) return SISL_ERR_NONFINITE;
+  return (hv->rnorm <= hv->atol) ? SISL_OK : SISL_NOT_CONVERGED;
+}
+
+// SemiImplicitSolver3D.solve: scale, GMRES, unscale (steppers.py:401-496).
+template <typename T>
+int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, const CVec5<T>* x0, Vec5<T> x,
+                   cudaStream_t st, SislSolveInfo* info) {
+  const Dims& d = c->d;
+  {
+    KScope k(c, SISL_K_OTHER, st);
+    zero_gaps_kernel<T><<<g.R + 4, 256, 0, st>>>(g.vec, g.npad, g.R + 4, g.off[0], g.off[1], g.off[2], g.off[3],
+                                                g.off[4], g.sz[0], g.sz[1], g.sz[2], g.sz[3], g.sz[4]);
+  }
+  const T ps = (T)c->s.ps;
+  scale5<T>(c, cf, rhs, g.view(g.bg()), ps, 0, st);       // rhs_scaled: pi * pi_scale
+  if (x0) scale5<T>(c, cf, *x0, g.view(g.xg()), ps, 1, st);  // x0 scaled: pi * ps, eta * dz_w
+  else scale5<T>(c, cf, rhs, g.view(g.xg()), ps, 0, st);     // x0 = rhs_scaled
+  int rc = gmres_run<T>(c, cf, g, st, info);
+  if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+  scale5<T>(c, cf, g.cview(g.xg()), x, (T)(1.0 / c->s.ps), 2, st);  // pi / ps, eta / dz_w
+  (void)d;
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// step workspace
+// ---------------------------------------------------------------------------
+template <typename T>
+struct SWork {
+  GWork<T> g;
+  T* vel[12];
+  T *u_in, *v_in, *w_in, *pi_in, *th_in, *tth, *res;
+  T *ru, *rv, *rw, *rp, *tha, *reta;
+  T *hyp[4], *htmp[4];
+  T *ku, *kv, *kw, *kp;
+  T *su, *sv;
+  T* div;
+};
+
+template <typename T>
+SWork<T> carve_step(Carver& cv, const Dims& d, int R) {
+  SWork<T> w;
+  w.g = carve_gmres<T>(cv, d, R);
+  auto F = [&](int loc) { return (T*)cv.take(sizeof(T) * field_size(d, loc)); };
+  const int vl[4] = {LOC_M, LOC_U, LOC_V, LOC_W};
+  for (int l = 0; l < 4; ++l)
+    for (int q = 0; q < 3; ++q) w.vel[3 * l + q] = F(vl[l]);
+  w.u_in = F(LOC_U); w.v_in = F(LOC_V); w.w_in = F(LOC_W); w.pi_in = F(LOC_M); w.th_in = F(LOC_M);
+  w.tth = F(LOC_M); w.res = F(LOC_W);
+  w.ru = F(LOC_U); w.rv = F(LOC_V); w.rw = F(LOC_W); w.rp = F(LOC_M); w.tha = F(LOC_M); w.reta = F(LOC_W);
+  for (int q = 0; q < 4; ++q) { w.hyp[q] = F(LOC_M); w.htmp[q] = F(LOC_M); }
+  w.ku = F(LOC_U); w.kv = F(LOC_V); w.kw = F(LOC_W); w.kp = F(LOC_M);
+  w.su = F(LOC_U); w.sv = F(LOC_V);
+  w.div = F(LOC_M);
+  return w;
+}
+
+template <typename T>
+int step_impl(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
+              size_t ws_bytes, cudaStream_t st, SislStepInfo* info) {
+  const Dims& d = c->d;
+  const Coef<T> cf = coef_of<T>(c);
+  Carver cv{(char*)ws};
+  SWork<T> w = carve_step<T>(cv, d, c->prm.solver_restart);
+  if (cv.off > ws_bytes) return SISL_ERR_WORKSPACE;
+  const int64_t l0 = g_launches.load();
+  const T* u = (const T*)in->u;
+  const T* v = (const T*)in->v;
+  const T* wv = (const T*)in->w;
+  const T* eta = (const T*)in->eta_dot;
+  const T* pp = (const T*)in->pi_p;
+  const T* th = (const T*)in->th_p;
+  const double a = c->s.alpha, dt = c->s.dt;
+  // 1. trajectory index velocities (steppers.py:748-762, 276-316)
+  {
+    PtrTable<T> vt{};
+    for (int q = 0; q < 12; ++q) vt.p[q] = w.vel[q];
+    const int extrap = (in->is_first_step == 1.0) ? 0 : 1;
+    KScope k(c, SISL_K_SL, st);
+    launch_traj_velocity<T>(d, cf, u, v, eta, (const T*)in->u_prev, (const T*)in->v_prev,
+                            (const T*)in->eta_dot_prev, extrap, vt, st);
+  }
+  // 2. explicit tendencies with hyperdiffusion (euler.py:208-372)
+  ExplicitIn<T> ein{u, v, wv, eta, pp, th, {nullptr, nullptr, nullptr, nullptr}};
+  if (c->s.nu_h > 0.0) {
+    PtrTable<T> t4{}, o4{};
+    for (int q = 0; q < 4; ++q) { t4.p[q] = w.htmp[q]; o4.p[q] = w.hyp[q]; }
+    KScope k(c, SISL_K_EXPLICIT, st, 3);
+    launch_hyper<T>(d, cf, u, v, wv, th, t4, o4, st);
+    for (int q = 0; q < 4; ++q) ein.hyper[q] = w.hyp[q];
+  }
+  {
+    ExplicitOut<T> eo{};
+    eo.f[0] = w.u_in; eo.f[1] = w.v_in; eo.f[2] = w.w_in; eo.f[3] = w.pi_in; eo.f[4] = w.th_in;
+    eo.f[5] = w.tth; eo.f[6] = w.res;
+    KScope k(c, SISL_K_EXPLICIT, st);
+    launch_explicit<T>(d, cf, ein, eo, 0, st);
+  }
+  // 3. semi-Lagrangian advection at the departure points (steppers.py:852-876)
+  const int iters = c->prm.departure_iterations;
+  const int lim = c->prm.use_limiter;
+  {
+    const T* f[2] = {w.res, w.w_in};
+    T* o[2] = {w.reta, w.rw};
+    const T sc[2] = {(T)(-(1.0 - a)), T(1)};
+    KScope k(c, SISL_K_SL, st);
+    launch_sl_advect<T>(d, LOC_W, dt, w.vel + 9, iters, 2, f, o, sc, lim, st);
+  }
+  {
+    const T* f[1] = {w.u_in};
+    T* o[1] = {w.ru};
+    const T sc[1] = {T(1)};
+    KScope k(c, SISL_K_SL, st);
+    launch_sl_advect<T>(d, LOC_U, dt, w.vel + 3, iters, 1, f, o, sc, lim, st);
+  }
+  {
+    const T* f[1] = {w.v_in};
+    T* o[1] = {w.rv};
+    const T sc[1] = {T(1)};
+    KScope k(c, SISL_K_SL, st);
+    launch_sl_advect<T>(d, LOC_V, dt, w.vel + 6, iters, 1, f, o, sc, lim, st);
+  }
+  {
+    const T* f[2] = {w.pi_in, w.th_in};
+    T* o[2] = {w.rp, w.tha};
+    const T sc[2] = {T(1), T(1)};
+    KScope k(c, SISL_K_SL, st);
+    launch_sl_advect<T>(d, LOC_M, dt, w.vel + 0, iters, 2, f, o, sc, lim, st);
+  }
+  {
+    KScope k(c, SISL_K_OTHER, st);
+    const int na = (d.nx > d.ny ? d.nx : d.ny) + 1;
+    sl_fixup_kernel<T><<<dim3((na + 127) / 128, d.nz), 128, 0, st>>>(d, w.ru, w.rv, u, v, w.reta);
+  }
+  // 4. predictor-corrector with two implicit solves (steppers.py:911-998)
+  T* ow = (T*)out->w;
+  T* op = (T*)out->pi_p;
+  T* oe = (T*)out->eta_dot;
+  T* oth = (T*)out->th_p;
+  int status = SISL_OK;
+  for (int it = 0; it < 2; ++it) {
+    const T* w_next = (it == 0) ? wv : ow;
+    {
+      KScope k(c, SISL_K_EXPLICIT, st);
+      launch_corrector_theta<T>(d, cf, w.tha, w.tth, wv, w_next, oth, st);
+    }
+    CorrectorIn<T> ci;
+    ci.rhs_u = w.ru; ci.rhs_v = w.rv; ci.rhs_w = w.rw; ci.rhs_pi = w.rp;
+    ci.th_next = oth;
+    ci.pg = (it == 0) ? pp : op;
+    ci.gu = (it == 0) ? u : w.su;
+    ci.gv = (it == 0) ? v : w.sv;
+    ci.geta = (it == 0) ? eta : oe;
+    ci.ug = (it == 0) ? w.ru : w.su;
+    ci.vg = (it == 0) ? w.rv : w.sv;
+    Vec5<T> rk;
+    rk.f[0] = w.ku; rk.f[1] = w.kv; rk.f[2] = w.kw; rk.f[3] = w.kp; rk.f[4] = w.reta;
+    {
+      KScope k(c, SISL_K_EXPLICIT, st);
+      launch_corrector_rhs<T>(d, cf, ci, rk, st);
+    }
+    CVec5<T> x0;
+    if (it == 0) { x0.f[0] = u; x0.f[1] = v; x0.f[2] = wv; x0.f[3] = pp; x0.f[4] = eta; }
+    else { x0.f[0] = w.su; x0.f[1] = w.sv; x0.f[2] = ow; x0.f[3] = op; x0.f[4] = oe; }
+    Vec5<T> xs;
+    xs.f[0] = w.su; xs.f[1] = w.sv; xs.f[2] = ow; xs.f[3] = op; xs.f[4] = oe;
+    SislSolveInfo si{};
+    int rc = solve_physical<T>(c, cf, w.g, as_const(rk), &x0, xs, st, &si);
+    if (info) info->solve[it] = si;
+    if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+    if (rc != SISL_OK && status == SISL_OK) status = rc;
+  }
+  // 5. divergence damping, bc_fn relaxation, EOS (steppers.py:1022-1056)
+  FinalizeArgs<T> fa{};
+  fa.u_in = w.su; fa.v_in = w.sv;
+  fa.u_out = (T*)out->u; fa.v_out = (T*)out->v;
+  fa.w_io = ow; fa.th_io = oth; fa.pi_io = op;
+  fa.rho_out = (T*)out->rho;
+  fa.div = nullptr;
+  if (c->s.nu_div != 0.0) {
+    KScope k(c, SISL_K_OTHER, st);
+    launch_hdiv<T>(d, cf, w.su, w.sv, w.div, st);
+    fa.div = w.div;
+  }
+  fa.relax.on = 0;
+  if (relax) {
+    fa.relax.on = relax->fields;
+    fa.relax.mask_m = (const T*)relax->mask_m;
+    fa.relax.mask_u = (const T*)relax->mask_u;
+    fa.relax.mask_v = (const T*)relax->mask_v;
+    for (int q = 0; q < 5; ++q) { fa.relax.ext[q] = (T)relax->ext[q]; fa.relax.ext_field[q] = (const T*)relax->ext_field[q]; }
+  }
+  {
+    KScope k(c, SISL_K_OTHER, st);
+    launch_finalize<T>(d, cf, fa, st);
+  }
+  // 6. history (steppers.py:1061-1071)
+  auto cp = [&](void* dst, const void* src, int loc) {
+    if (dst && src && dst != src)
+      cudaMemcpyAsync(dst, src, sizeof(T) * field_size(d, loc), cudaMemcpyDeviceToDevice, st);
+  };
+  cp(out->u_prev, in->u, LOC_U);
+  cp(out->v_prev, in->v, LOC_V);
+  cp(out->w_prev, in->w, LOC_W);
+  cp(out->eta_dot_prev, in->eta_dot, LOC_W);
+  cp(out->tend_th_prev, w.tth, LOC_M);
+  if (info) info->kernel_launches = g_launches.load() - l0;
+  int e = check_cuda();
+  return e ? e : status;
+}
+
+bool valid_grid(const SislGrid* g) {
+  return g && g->nx >= 2 && g->ny >= 2 && g->nz >= 2 && (g->dtype == SISL_F32 || g->dtype == SISL_F64) &&
+         g->dx > 0 && g->dy > 0 && g->dz > 0 && (int64_t)(g->nx + 1) * (g->ny + 1) * (g->nz + 1) < (1LL << 31);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int sisl_version(void) { return 1; }
+
+const char* sisl_status_string(int s) {
+  switch (s) {
+    case SISL_OK: return "ok";
+    case SISL_NOT_CONVERGED: return "GMRES did not reach its tolerance within maxiter restart cycles";
+    case SISL_ERR_ARG: return "invalid argument";
+    case SISL_ERR_CUDA: return "CUDA error";
+    case SISL_ERR_WORKSPACE: return "workspace too small";
+    case SISL_ERR_NONFINITE: return "non-finite residual";
+    default: return "unknown status";
+  }
+}
+
+size_t sisl_field_elems(const SislGrid* g, int loc) {
+  if (!g || loc < 0 || loc > 3) return 0;
+  Dims d{g->nx, g->ny, g->nz, g->periodic_x, g->periodic_y, g->dx, g->dy, g->dz};
+  return field_size(d, loc);
+}
+
+int sisl_core_create(const SislGrid* grid, const SislParams* prm, const SislBackground* bg, void* stream,
+                     SislCore** out) {
+  if (!out || !valid_grid(grid) || !prm || !bg) return SISL_ERR_ARG;
+  if (prm->solver_restart < 1 || prm->solver_restart > GM_MAXR || prm->solver_maxiter < 0) return SISL_ERR_ARG;
+  if (prm->solve_method != SISL_GMRES_BATCHED && prm->solve_method != SISL_GMRES_INCREMENTAL) return SISL_ERR_ARG;
+  const double* req[] = {bg->theta_bg, bg->pi_bg, bg->Z_m, bg->dz_m_full, bg->dz_w_full, bg->z_xi_w,
+                         bg->z_eta_w, bg->tau_damp, bg->m_m, bg->m_u, bg->m_v, bg->f_u, bg->f_v,
+                         bg->dm_dx_m, bg->dm_dy_m};
+  for (const double* p : req)
+    if (!p) return SISL_ERR_ARG;
+  SislCore* c = new (std::nothrow) SislCore();
+  if (!c) return SISL_ERR_ARG;
+  c->grid = *grid;
+  c->prm = *prm;
+  c->d = Dims{grid->nx, grid->ny, grid->nz, grid->periodic_x ? 1 : 0, grid->periodic_y ? 1 : 0,
+              grid->dx, grid->dy, grid->dz};
+  c->s = Scalars{prm->dt, prm->alpha, prm->g, prm->cp, prm->Rd, prm->cvd, prm->p0, prm->pi_scale, prm->nu_div,
+                 prm->nu_h};
+  const size_t es = esize(grid->dtype);
+  size_t total = 0, offs[C_COUNT];
+  for (int q = 0; q < C_COUNT; ++q) {
+    offs[q] = total;
+    total += align256(es * coef_elems(c->d, q));
+  }
+  if (cudaMalloc(&c->coef_mem, total) != cudaSuccess) { delete c; return SISL_ERR_CUDA; }
+  if (cudaMallocHost((void**)&c->hv, sizeof(GHostView)) != cudaSuccess) {
+    cudaFree(c->coef_mem);
+    delete c;
+    return SISL_ERR_CUDA;
+  }
+  for (int q = 0; q < C_COUNT; ++q) c->coef_ptr[q] = (char*)c->coef_mem + offs[q];
+  Base64 b{bg->theta_bg, bg->pi_bg, bg->Z_m, bg->dz_m_full, bg->dz_w_full, bg->z_xi_w, bg->z_eta_w, bg->tau_damp,
+           bg->m_m, bg->m_u, bg->m_v, bg->f_u, bg->f_v, bg->dm_dx_m, bg->dm_dy_m};
+  cudaStream_t st = (cudaStream_t)stream;
+  g_launches += 2;
+  if (grid->dtype == SISL_F64) {
+    PtrTable<double> t;
+    for (int q = 0; q < C_COUNT; ++q) t.p[q] = (double*)c->coef_ptr[q];
+    launch_prepare<double>(c->d, c->s, b, t, st);
+  } else {
+    PtrTable<float> t;
+    for (int q = 0; q < C_COUNT; ++q) t.p[q] = (float*)c->coef_ptr[q];
+    launch_prepare<float>(c->d, c->s, b, t, st);
+  }
+  if (check_cuda() != SISL_OK || cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaFree(c->coef_mem);
+    cudaFreeHost(c->hv);
+    delete c;
+    return SISL_ERR_CUDA;
+  }
+  *out = c;
+  return SISL_OK;
+}
+
+int sisl_core_destroy(SislCore* c) {
+  if (!c) return SISL_ERR_ARG;
+  for (size_t q = 0; q < c->ev0.size(); ++q) { cudaEventDestroy(c->ev0[q]); cudaEventDestroy(c->ev1[q]); }
+  cudaFree(c->coef_mem);
+  cudaFreeHost(c->hv);
+  delete c;
+  return SISL_OK;
+}
+
+size_t sisl_workspace_bytes(const SislCore* c, int what) {
+  if (!c) return 0;
+  Carver cv{nullptr};
+  const bool f64 = c->grid.dtype == SISL_F64;
+  const size_t es = esize(c->grid.dtype);
+  switch (what) {
+    case SISL_WS_STEP:
+      if (f64) carve_step<double>(cv, c->d, c->prm.solver_restart);
+      else carve_step<float>(cv, c->d, c->prm.solver_restart);
+      break;
+    case SISL_WS_GMRES:
+      if (f64) carve_gmres<double>(cv, c->d, c->prm.solver_restart);
+      else carve_gmres<float>(cv, c->d, c->prm.solver_restart);
+      break;
+    case SISL_WS_DEPARTURE:
+      for (int l = 0; l < 4; ++l)
+        for (int q = 0; q < 3; ++q) cv.take(es * field_size(c->d, l));
+      break;
+    case SISL_WS_EXPLICIT:
+      for (int q = 0; q < 8; ++q) cv.take(es * field_size(c->d, LOC_M));
+      break;
+    case SISL_WS_OPERATOR:
+      for (int q = 0; q < 5; ++q) cv.take(es * field_size(c->d, loc_of_field(q)));
+      break;
+    case SISL_WS_FFSL:
+      cv.take(es * field_size(c->d, LOC_M));
+      cv.take(es * field_size(c->d, LOC_M));
+      cv.take(sizeof(double) * ffsl_scratch_doubles(c->d));
+      break;
+    default: return 0;
+  }
+  return align256(cv.off);
+}
+
+int sisl_linear_operator(SislCore* c, const void* const in[5], void* const out[5], void* ws, size_t ws_bytes,
+                         void* stream) {
+  if (!c || !in || !out) return SISL_ERR_ARG;
+  if (ws_bytes < sisl_workspace_bytes(c, SISL_WS_OPERATOR) || !ws) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv{(char*)ws};
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    const Coef<T> cf = coef_of<T>(c);
+    Vec5<T> tmp;
+    for (int q = 0; q < 5; ++q) tmp.f[q] = (T*)cv.take(sizeof(T) * field_size(c->d, loc_of_field(q)));
+    scale5<T>(c, cf, cvec<T>(in), tmp, (T)c->s.ps, 1, st);
+    {
+      KScope k(c, SISL_K_MATVEC, st);
+      launch_matvec<T>(c->d, cf, as_const(tmp), nullptr, CVec5<T>{}, vec<T>(out), nullptr, st);
+    }
+    // pi row back to physical units; the eta row of A_fn is already physical
+    Vec5<T> o = vec<T>(out);
+    scale5<T>(c, cf, as_const(o), o, (T)(1.0 / c->s.ps), 0, st);
+  };
+  if (c->grid.dtype == SISL_F64) run(double{});
+  else run(float{});
+  return check_cuda();
+}
+
+int sisl_helmholtz_matvec(SislCore* c, const void* const in[5], void* const out[5], void* stream) {
+  if (!c || !in || !out) return SISL_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(c, SISL_K_MATVEC, st);
+  if (c->grid.dtype == SISL_F64)
+    launch_matvec<double>(c->d, coef_of<double>(c), cvec<double>(in), nullptr, CVec5<double>{}, vec<double>(out),
+                          nullptr, st);
+  else
+    launch_matvec<float>(c->d, coef_of<float>(c), cvec<float>(in), nullptr, CVec5<float>{}, vec<float>(out),
+                         nullptr, st);
+  return check_cuda();
+}
+
+int sisl_precond_apply(SislCore* c, const void* const in[5], void* const out[5], void* stream) {
+  if (!c || !in || !out) return SISL_ERR_ARG;
+  for (int q = 2; q < 5; ++q)
+    if (in[q] == out[q]) return SISL_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(c, SISL_K_PRECOND, st);
+  if (c->grid.dtype == SISL_F64)
+    launch_precond<double>(c->d, coef_of<double>(c), cvec<double>(in), vec<double>(out), nullptr, st);
+  else
+    launch_precond<float>(c->d, coef_of<float>(c), cvec<float>(in), vec<float>(out), nullptr, st);
+  return check_cuda();
+}
+
+int sisl_gmres_solve(SislCore* c, const void* const rhs[5], const void* const x0[5], void* const x[5], void* ws,
+                     size_t ws_bytes, void* stream, SislSolveInfo* info) {
+  if (!c || !rhs || !x) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_GMRES)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv{(char*)ws};
+  int rc;
+  if (c->grid.dtype == SISL_F64) {
+    GWork<double> g = carve_gmres<double>(cv, c->d, c->prm.solver_restart);
+    CVec5<double> x0v;
+    if (x0) x0v = cvec<double>(x0);
+    rc = solve_physical<double>(c, coef_of<double>(c), g, cvec<double>(rhs), x0 ? &x0v : nullptr, vec<double>(x),
+                                st, info);
+  } else {
+    GWork<float> g = carve_gmres<float>(cv, c->d, c->prm.solver_restart);
+    CVec5<float> x0v;
+    if (x0) x0v = cvec<float>(x0);
+    rc = solve_physical<float>(c, coef_of<float>(c), g, cvec<float>(rhs), x0 ? &x0v : nullptr, vec<float>(x), st,
+                               info);
+  }
+  int e = check_cuda();
+  return e ? e : rc;
+}
+
+int sisl_departure(SislCore* c, int loc, const void* u, const void* v, const void* eta, int iterations,
+                   void* const coords[3], void* ws, size_t ws_bytes, void* stream) {
+  if (!c || loc < 0 || loc > 3 || !u || !v || !eta || !coords || iterations < 0) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_DEPARTURE)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv{(char*)ws};
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    const Coef<T> cf = coef_of<T>(c);
+    PtrTable<T> vt{};
+    for (int l = 0; l < 4; ++l)
+      for (int q = 0; q < 3; ++q) vt.p[3 * l + q] = (T*)cv.take(sizeof(T) * field_size(c->d, l));
+    {
+      KScope k(c, SISL_K_SL, st);
+      launch_traj_velocity<T>(c->d, cf, (const T*)u, (const T*)v, (const T*)eta, nullptr, nullptr, nullptr, 0, vt,
+                              st);
+    }
+    T* co[3] = {(T*)coords[0], (T*)coords[1], (T*)coords[2]};
+    KScope k(c, SISL_K_SL, st);
+    launch_departure<T>(c->d, loc, c->s.dt, (const T* const*)(vt.p + 3 * loc), iterations, co, st);
+  };
+  if (c->grid.dtype == SISL_F64) run(double{});
+  else run(float{});
+  return check_cuda();
+}
+
+int sisl_tricubic(int dtype, const int32_t src[3], const void* field, const int32_t dst[3],
+                  const void* const coords[3], void* out, int use_limiter, void* stream) {
+  if (!src || !dst || !field || !coords || !out) return SISL_ERR_ARG;
+  for (int q = 0; q < 3; ++q)
+    if (src[q] < 1 || dst[q] < 0) return SISL_ERR_ARG;
+  if ((int64_t)dst[0] * dst[1] * dst[2] == 0) return SISL_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(nullptr, SISL_K_SL, st);
+  if (dtype == SISL_F64) {
+    const double* co[3] = {(const double*)coords[0], (const double*)coords[1], (const double*)coords[2]};
+    launch_tricubic_ext<double>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const double*)field, co,
+                                (double*)out, use_limiter, 1.0, st);
+  } else if (dtype == SISL_F32) {
+    const float* co[3] = {(const float*)coords[0], (const float*)coords[1], (const float*)coords[2]};
+    launch_tricubic_ext<float>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const float*)field, co,
+                               (float*)out, use_limiter, 1.0f, st);
+  } else {
+    return SISL_ERR_ARG;
+  }
+  return check_cuda();
+}
+
+int sisl_trilinear(int dtype, const int32_t src[3], const void* field, const int32_t dst[3],
+                   const void* const coords[3], void* out, void* stream) {
+  if (!src || !dst || !field || !coords || !out) return SISL_ERR_ARG;
+  for (int q = 0; q < 3; ++q)
+    if (src[q] < 1 || dst[q] < 0) return SISL_ERR_ARG;
+  if ((int64_t)dst[0] * dst[1] * dst[2] == 0) return SISL_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(nullptr, SISL_K_SL, st);
+  if (dtype == SISL_F64) {
+    const double* co[3] = {(const double*)coords[0], (const double*)coords[1], (const double*)coords[2]};
+    launch_trilinear_ext<double>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const double*)field, co,
+                                 (double*)out, st);
+  } else if (dtype == SISL_F32) {
+    const float* co[3] = {(const float*)coords[0], (const float*)coords[1], (const float*)coords[2]};
+    launch_trilinear_ext<float>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const float*)field, co,
+                                (float*)out, st);
+  } else {
+    return SISL_ERR_ARG;
+  }
+  return check_cuda();
+}
+
+size_t sisl_ffsl_lines_workspace_bytes(int n, int nlines) {
+  if (n < 1 || nlines < 1) return 0;
+  return align256(sizeof(double) * (size_t)(n + 1) * nlines);
+}
+
+int sisl_ffsl_lines(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic, void* out,
+                    void* ws, size_t ws_bytes, void* stream) {
+  if (n < 1 || nlines < 1 || !scalar || !cfl || !out) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_ffsl_lines_workspace_bytes(n, nlines)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(nullptr, SISL_K_OTHER, st);
+  if (dtype == SISL_F64)
+    launch_ffsl_lines<double>(n, nlines, (const double*)scalar, (const double*)cfl, (double*)out, (double*)ws,
+                              periodic ? 1 : 0, st);
+  else if (dtype == SISL_F32)
+    launch_ffsl_lines<float>(n, nlines, (const float*)scalar, (const float*)cfl, (float*)out, (double*)ws,
+                             periodic ? 1 : 0, st);
+  else
+    return SISL_ERR_ARG;
+  return check_cuda();
+}
+
+int sisl_explicit_tendencies(SislCore* c, const void* const sp[6], void* const tend[6], void* const pd[4], void* ws,
+                             size_t ws_bytes, void* stream) {
+  return sisl_tendencies(c, 1, sp, tend, pd, ws, ws_bytes, stream);
+}
+
+int sisl_tendencies(SislCore* c, int is_explicit, const void* const sp[6], void* const tend[6],
+                    void* const pd[4], void* ws, size_t ws_bytes, void* stream) {
+  if (!c || !sp || !tend) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_EXPLICIT)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv{(char*)ws};
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    const Coef<T> cf = coef_of<T>(c);
+    ExplicitIn<T> ein{(const T*)sp[0], (const T*)sp[1], (const T*)sp[2], (const T*)sp[4], (const T*)sp[3],
+                      (const T*)sp[5], {nullptr, nullptr, nullptr, nullptr}};
+    if (is_explicit && (c->s.nu_h > 0.0 || c->s.nu_div > 0.0)) {
+      PtrTable<T> t4{}, o4{};
+      for (int q = 0; q < 4; ++q) o4.p[q] = (T*)cv.take(sizeof(T) * field_size(c->d, LOC_M));
+      for (int q = 0; q < 4; ++q) t4.p[q] = (T*)cv.take(sizeof(T) * field_size(c->d, LOC_M));
+      KScope k(c, SISL_K_EXPLICIT, st, 3);
+      launch_hyper<T>(c->d, cf, ein.u, ein.v, ein.w, ein.th, t4, o4, st);
+      for (int q = 0; q < 4; ++q) ein.hyper[q] = o4.p[q];
+    }
+    ExplicitOut<T> eo{};
+    for (int q = 0; q < 6; ++q) eo.f[q] = (T*)tend[q];
+    for (int q = 0; q < 4; ++q) eo.pd[q] = pd ? (T*)pd[q] : nullptr;
+    KScope k(c, SISL_K_EXPLICIT, st);
+    launch_explicit<T>(c->d, cf, ein, eo, is_explicit ? 1 : 2, st);
+  };
+  if (c->grid.dtype == SISL_F64) run(double{});
+  else run(float{});
+  return check_cuda();
+}
+
+int sisl_step(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
+              size_t ws_bytes, void* stream, SislStepInfo* info) {
+  if (!c || !in || !out) return SISL_ERR_ARG;
+  const void* need_in[] = {in->u, in->v, in->w, in->eta_dot, in->pi_p, in->th_p};
+  for (const void* p : need_in)
+    if (!p) return SISL_ERR_ARG;
+  if (in->is_first_step != 1.0 && (!in->u_prev || !in->v_prev || !in->eta_dot_prev)) return SISL_ERR_ARG;
+  const void* need_out[] = {out->u, out->v, out->w, out->eta_dot, out->pi_p, out->th_p};
+  for (const void* p : need_out)
+    if (!p) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_STEP)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (c->grid.dtype == SISL_F64) return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info);
+  return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info);
+}
+
+int sisl_core_set_solver(SislCore* c, double tol, double atol, int maxiter, int restart, int method) {
+  if (!c || restart < 1 || restart > GM_MAXR || maxiter < 0) return SISL_ERR_ARG;
+  if (method != SISL_GMRES_BATCHED && method != SISL_GMRES_INCREMENTAL) return SISL_ERR_ARG;
+  c->prm.solver_tol = tol;
+  c->prm.solver_atol = atol;
+  c->prm.solver_maxiter = maxiter;
+  c->prm.solver_restart = restart;
+  c->prm.solve_method = method;
+  return SISL_OK;
+}
+
+int sisl_ffsl_advect(SislCore* c, const void* field, const void* u, const void* v, const void* eta, void* out,
+                     void* ws, size_t ws_bytes, void* stream) {
+  if (!c || !field || !u || !v || !eta || !out) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_FFSL)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv{(char*)ws};
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    T* t0 = (T*)cv.take(sizeof(T) * field_size(c->d, LOC_M));
+    T* t1 = (T*)cv.take(sizeof(T) * field_size(c->d, LOC_M));
+    double* M = (double*)cv.take(sizeof(double) * ffsl_scratch_doubles(c->d));
+    KScope k(c, SISL_K_OTHER, st, 4);
+    launch_ffsl<T>(c->d, coef_of<T>(c), (const T*)field, (const T*)u, (const T*)v, (const T*)eta, (T*)out, t0, t1,
+                   M, st);
+  };
+  if (c->grid.dtype == SISL_F64) run(double{});
+  else run(float{});
+  return check_cuda();
+}
+
+int sisl_eos(SislCore* c, const void* th_p, const void* pi_p, void* rho, void* stream) {
+  if (!c || !th_p || !pi_p || !rho) return SISL_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(c, SISL_K_OTHER, st);
+  if (c->grid.dtype == SISL_F64)
+    launch_eos<double>(c->d, coef_of<double>(c), (const double*)th_p, (const double*)pi_p, (double*)rho, st);
+  else
+    launch_eos<float>(c->d, coef_of<float>(c), (const float*)th_p, (const float*)pi_p, (float*)rho, st);
+  return check_cuda();
+}
+
+int64_t sisl_kernel_launches(void) { return g_launches.load(); }
+
+int sisl_timing_select(SislCore* c, int cls) {
+  if (!c) return SISL_ERR_ARG;
+  c->timing_class = cls;
+  c->ev_used = 0;
+  return SISL_OK;
+}
+
+int sisl_timing_read(SislCore* c, double* total_ms, int64_t* launches) {
+  if (!c) return SISL_ERR_ARG;
+  double tot = 0.0;
+  for (size_t q = 0; q < c->ev_used; ++q) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(c->ev1[q]) != cudaSuccess) return SISL_ERR_CUDA;
+    if (cudaEventElapsedTime(&ms, c->ev0[q], c->ev1[q]) != cudaSuccess) return SISL_ERR_CUDA;
+    tot += ms;
+  }
+  if (total_ms) *total_ms = tot;
+  if (launches) *launches = (int64_t)c->ev_used;
+  return SISL_OK;
+}
+
+}  // extern "C"

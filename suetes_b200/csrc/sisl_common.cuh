@@ -1,0 +1,84 @@
+// Shared device-side definitions for the SISL kernels (sm_100a).
+//
+// Field layout on the device: a 3-D field of stagger s has the extents of the
+// reference array, (ex, ey, ez) = (nx + [s==u], ny + [s==v], nz + [s==w]),
+// stored x-fastest: element (i, j, k) lives at i + ex * (j + ey * k).  This is
+// the Fortran order of the reference's C-ordered (ex, ey, ez) arrays, so one
+// thread per (i, j) column reads a coalesced row per level, and mass and
+// w points share the same horizontal plane layout.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sisl {
+
+enum Loc { LOC_M = 0, LOC_U = 1, LOC_V = 2, LOC_W = 3 };
+
+struct Dims {
+  int nx, ny, nz;
+  int px, py;          // periodic flags for x and y
+  double dx, dy, dz;
+};
+
+__host__ __device__ inline int ext_x(const Dims& d, int loc) { return d.nx + (loc == LOC_U); }
+__host__ __device__ inline int ext_y(const Dims& d, int loc) { return d.ny + (loc == LOC_V); }
+__host__ __device__ inline int ext_z(const Dims& d, int loc) { return d.nz + (loc == LOC_W); }
+__host__ __device__ inline size_t field_size(const Dims& d, int loc) {
+  return (size_t)ext_x(d, loc) * ext_y(d, loc) * ext_z(d, loc);
+}
+
+// 3-D offsets per stagger.
+__device__ __forceinline__ int im(const Dims& d, int i, int j, int k) { return i + d.nx * (j + d.ny * k); }
+__device__ __forceinline__ int iu(const Dims& d, int i, int j, int k) { return i + (d.nx + 1) * (j + d.ny * k); }
+__device__ __forceinline__ int iv(const Dims& d, int i, int j, int k) { return i + d.nx * (j + (d.ny + 1) * k); }
+__device__ __forceinline__ int iw(const Dims& d, int i, int j, int k) { return i + d.nx * (j + d.ny * k); }
+// 2-D (horizontal) offsets per stagger.
+__device__ __forceinline__ int h_m(const Dims& d, int i, int j) { return i + d.nx * j; }
+__device__ __forceinline__ int h_u(const Dims& d, int i, int j) { return i + (d.nx + 1) * j; }
+__device__ __forceinline__ int h_v(const Dims& d, int i, int j) { return i + d.nx * j; }
+
+// Mass-to-face neighbour pair along a horizontal axis (operators.py:37-132).
+// Interior face f (0 < f < n) averages/differences cells f-1 and f.  The two
+// boundary faces of an open axis reuse the nearest interior face's pair (the
+// edge padding of operators.py:45-61); on a periodic axis both boundary faces
+// pair the last and first cells (operators.py:85-95, 123-131).
+__device__ __forceinline__ void face_pair(int f, int n, int periodic, int& l, int& r) {
+  if (f > 0 && f < n) { l = f - 1; r = f; return; }
+  if (periodic) { l = n - 1; r = 0; return; }
+  if (f == 0) { l = 0; r = 1; } else { l = n - 2; r = n - 1; }
+}
+// Mass-to-w pair along z (never periodic).
+__device__ __forceinline__ void level_pair(int k, int nz, int& l, int& r) {
+  if (k > 0 && k < nz) { l = k - 1; r = k; return; }
+  if (k == 0) { l = 0; r = 1; } else { l = nz - 2; r = nz - 1; }
+}
+
+template <typename T>
+__device__ __forceinline__ T ld(const T* __restrict__ p, int i) { return __ldg(p + i); }
+
+// Block-wide double-precision sum of NV values per thread; thread 0 of the
+// block ends up with the totals in out[].
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* smem /* blockDim/32 * NV */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double s = v[q];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) smem[warp * NV + q] = s;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = (lane < nw) ? smem[lane * NV + q] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      v[q] = s;
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace sisl

@@ -1,0 +1,507 @@
+// Explicit part of the SISL step: old-time tendencies with hyperdiffusion,
+// the departure-side right-hand sides, the predictor-corrector right-hand
+// sides, divergence damping, lateral relaxation and the equation of state.
+//
+// * Euler3D.get_tendencies(is_explicit=True)   euler.py:208-372
+// * Euler3D.nonlinear_pi_tendency               euler.py:162-186
+// * Euler3D.metric_curvature_tendencies         euler.py:188-206
+// * HyperFilter (horizontal part, nu_v = 0)     diffusion.py:93-173
+// * RHS assembly                                steppers.py:801-842
+// * predictor-corrector right-hand sides        steppers.py:911-983
+// * divergence damping, EOS                     steppers.py:1022-1031, 1055-1056
+//
+// Thermodynamic fields are carried in perturbation form: pi' = pi - pi_bg and
+// th' = th_v - theta_bg, so float32 never subtracts two O(1) numbers.
+#include "sisl_explicit.cuh"
+
+namespace sisl {
+namespace {
+
+dim3 box_grid(int ex, int ey, int ez, dim3 blk) {
+  return dim3((ex + blk.x - 1) / blk.x, (ey + blk.y - 1) / blk.y, (ez + blk.z - 1) / blk.z);
+}
+
+// pressure-gradient pieces of a mass field q (physical pi' or a guess)
+template <typename T>
+struct Grad {
+  const Dims& d;
+  const Coef<T>& c;
+  const T* __restrict__ q;
+  __device__ __forceinline__ T Q(int i, int j, int k) const { return ld(q, im(d, i, j, k)); }
+  __device__ __forceinline__ T gzw(int i, int j, int k) const {  // d q/dz at w level k (euler.py:252)
+    int kl, kr;
+    level_pair(k, d.nz, kl, kr);
+    return (Q(i, j, kr) - Q(i, j, kl)) * ld(c.idzw, iw(d, i, j, k));
+  }
+  __device__ __forceinline__ T gzm(int i, int j, int k) const { return T(0.5) * (gzw(i, j, k) + gzw(i, j, k + 1)); }
+  // Cartesian x-gradient at u face i: m_u dq/dxi - z_xi_u avg(dq/dz)  (euler.py:250-261)
+  __device__ __forceinline__ T gx(int i, int j, int k) const {
+    int l, r;
+    face_pair(i, d.nx, d.px, l, r);
+    const T g = (Q(r, j, k) - Q(l, j, k)) * (T)(1.0 / d.dx) * ld(c.mu, h_u(d, i, j));
+    return g - ld(c.zxu, iu(d, i, j, k)) * T(0.5) * (gzm(l, j, k) + gzm(r, j, k));
+  }
+  __device__ __forceinline__ T gy(int i, int j, int k) const {
+    int l, r;
+    face_pair(j, d.ny, d.py, l, r);
+    const T g = (Q(i, r, k) - Q(i, l, k)) * (T)(1.0 / d.dy) * ld(c.mv, h_v(d, i, j));
+    return g - ld(c.zev, iv(d, i, j, k)) * T(0.5) * (gzm(i, l, k) + gzm(i, r, k));
+  }
+};
+
+// horizontal winds at mass points and the map-curvature factor (euler.py:188-206)
+template <typename T>
+struct Winds {
+  const Dims& d;
+  const Coef<T>& c;
+  const T* __restrict__ u;
+  const T* __restrict__ v;
+  __device__ __forceinline__ T um(int i, int j, int k) const {
+    return T(0.5) * (ld(u, iu(d, i, j, k)) + ld(u, iu(d, i + 1, j, k)));
+  }
+  __device__ __forceinline__ T vm(int i, int j, int k) const {
+    return T(0.5) * (ld(v, iv(d, i, j, k)) + ld(v, iv(d, i, j + 1, k)));
+  }
+  __device__ __forceinline__ T metric_m(int i, int j, int k) const {
+    return vm(i, j, k) * ld(c.dmdx, h_m(d, i, j)) - um(i, j, k) * ld(c.dmdy, h_m(d, i, j));
+  }
+  // w-level averages of u, v (avg_u->m then avg_m->w, edge padded)
+  __device__ __forceinline__ T uw(int i, int j, int k) const {
+    int kl, kr;
+    level_pair(k, d.nz, kl, kr);
+    return T(0.5) * (um(i, j, kl) + um(i, j, kr));
+  }
+  __device__ __forceinline__ T vw(int i, int j, int k) const {
+    int kl, kr;
+    level_pair(k, d.nz, kl, kr);
+    return T(0.5) * (vm(i, j, kl) + vm(i, j, kr));
+  }
+};
+
+// averages of a mass field to the faces
+template <typename T>
+__device__ __forceinline__ T avg_mu(const Dims& d, const T* __restrict__ f, int i, int j, int k) {
+  int l, r;
+  face_pair(i, d.nx, d.px, l, r);
+  return T(0.5) * (ld(f, im(d, l, j, k)) + ld(f, im(d, r, j, k)));
+}
+template <typename T>
+__device__ __forceinline__ T avg_mv(const Dims& d, const T* __restrict__ f, int i, int j, int k) {
+  int l, r;
+  face_pair(j, d.ny, d.py, l, r);
+  return T(0.5) * (ld(f, im(d, i, l, k)) + ld(f, im(d, i, r, k)));
+}
+template <typename T>
+__device__ __forceinline__ T avg_mw(const Dims& d, const T* __restrict__ f, int i, int j, int k) {
+  int kl, kr;
+  level_pair(k, d.nz, kl, kr);
+  return T(0.5) * (ld(f, im(d, i, j, kl)) + ld(f, im(d, i, j, kr)));
+}
+
+// -C_pi/dz_m (m^2 (dFx/dx + dFy/dy) + dFz) for fluxes
+//   Fx = ux rdu thx, Fy = vy rdv thy, Fz = eta dz_w rho_w thz (zero on lid/ground)
+// where the face thetas come from `thsel` (euler.py:298-318, 172-186).
+template <typename T, typename ThU, typename ThV, typename ThW>
+__device__ __forceinline__ T divergence(const Dims& d, const Coef<T>& c, const T* __restrict__ u,
+                                        const T* __restrict__ v, const T* __restrict__ eta, int i, int j, int k,
+                                        ThU thu, ThV thv, ThW thw) {
+  const int u0 = iu(d, i, j, k), u1 = iu(d, i + 1, j, k);
+  const int v0 = iv(d, i, j, k), v1 = iv(d, i, j + 1, k);
+  const T fx0 = ld(u, u0) * ld(c.rdu, u0) * thu(i, j, k);
+  const T fx1 = ld(u, u1) * ld(c.rdu, u1) * thu(i + 1, j, k);
+  const T fy0 = ld(v, v0) * ld(c.rdv, v0) * thv(i, j, k);
+  const T fy1 = ld(v, v1) * ld(c.rdv, v1) * thv(i, j + 1, k);
+  const int w0 = iw(d, i, j, k), w1 = iw(d, i, j, k + 1);
+  const T fz0 = (k == 0) ? T(0) : ld(eta, w0) * ld(c.dzw, w0) * ld(c.rhow, w0) * thw(i, j, k);
+  const T fz1 = (k + 1 == d.nz) ? T(0) : ld(eta, w1) * ld(c.dzw, w1) * ld(c.rhow, w1) * thw(i, j, k + 1);
+  const T m = ld(c.mm, h_m(d, i, j));
+  const T divh = m * m * ((fx1 - fx0) * (T)(1.0 / d.dx) + (fy1 - fy0) * (T)(1.0 / d.dy));
+  return -ld(c.cpidz, im(d, i, j, k)) * (divh + (fz1 - fz0));
+}
+
+// ---------------------------------------------------------------------------
+// hyperdiffusion: mass-point copies of u, v, w, th' (diffusion.py:141-151)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void hyper_src_kernel(Dims d, const T* __restrict__ u, const T* __restrict__ v,
+                                 const T* __restrict__ w, const T* __restrict__ th, PtrTable<T> out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= d.nx || j >= d.ny || k >= d.nz) return;
+  const int p = im(d, i, j, k);
+  out.p[0][p] = T(0.5) * (ld(u, iu(d, i, j, k)) + ld(u, iu(d, i + 1, j, k)));
+  out.p[1][p] = T(0.5) * (ld(v, iv(d, i, j, k)) + ld(v, iv(d, i, j + 1, k)));
+  out.p[2][p] = T(0.5) * (ld(w, iw(d, i, j, k)) + ld(w, iw(d, i, j, k + 1)));
+  out.p[3][p] = ld(th, p);
+}
+
+// Cartesian horizontal Laplacian of a mass field (diffusion.py:93-129).
+template <typename T>
+struct HLap {
+  const Dims& d;
+  const Coef<T>& c;
+  const T* __restrict__ f;
+  __device__ __forceinline__ T F(int i, int j, int k) const { return ld(f, im(d, i, j, k)); }
+  __device__ __forceinline__ T dzw(int i, int j, int k) const {
+    int kl, kr;
+    level_pair(k, d.nz, kl, kr);
+    return (F(i, j, kr) - F(i, j, kl)) * ld(c.idzw, iw(d, i, j, k));
+  }
+  __device__ __forceinline__ T dzm(int i, int j, int k) const { return T(0.5) * (dzw(i, j, k) + dzw(i, j, k + 1)); }
+  __device__ __forceinline__ T Gx(int fi, int j, int k) const {  // at u face fi
+    int l, r;
+    face_pair(fi, d.nx, d.px, l, r);
+    const T dxi = (F(r, j, k) - F(l, j, k)) * (T)(1.0 / d.dx) * ld(c.mu, h_u(d, fi, j));
+    return dxi - ld(c.zxu, iu(d, fi, j, k)) * T(0.5) * (dzm(l, j, k) + dzm(r, j, k));
+  }
+  __device__ __forceinline__ T Gy(int i, int fj, int k) const {  // at v face fj
+    int l, r;
+    face_pair(fj, d.ny, d.py, l, r);
+    const T deta = (F(i, r, k) - F(i, l, k)) * (T)(1.0 / d.dy) * ld(c.mv, h_v(d, i, fj));
+    return deta - ld(c.zev, iv(d, i, fj, k)) * T(0.5) * (dzm(i, l, k) + dzm(i, r, k));
+  }
+  __device__ T lap(int i, int j, int k) const {
+    const int nz = d.nz;
+    // Gx at faces i, i+1 and Gy at faces j, j+1 on the levels k-1, k, k+1 (clamped)
+    const int kl = max(k - 1, 0), kh = min(k + 1, nz - 1);
+    const int lv[3] = {kl, k, kh};
+    T gxm[3], gym[3], gx0 = T(0), gx1 = T(0), gy0 = T(0), gy1 = T(0);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const T a0 = Gx(i, j, lv[q]), a1 = Gx(i + 1, j, lv[q]);
+      const T b0 = Gy(i, j, lv[q]), b1 = Gy(i, j + 1, lv[q]);
+      gxm[q] = T(0.5) * (a0 + a1);
+      gym[q] = T(0.5) * (b0 + b1);
+      if (q == 1) { gx0 = a0; gx1 = a1; gy0 = b0; gy1 = b1; }
+    }
+    // d/dz at w levels k and k+1 of the mass-point Gx_m, Gy_m (edge padded)
+    auto lvl = [&](int kk) { return kk == kl ? 0 : (kk == k ? 1 : 2); };
+    int al, ar, bl, br;
+    level_pair(k, nz, al, ar);
+    level_pair(k + 1, nz, bl, br);
+    const T iz0 = ld(c.idzw, iw(d, i, j, k)), iz1 = ld(c.idzw, iw(d, i, j, k + 1));
+    const T ex0 = (gxm[lvl(ar)] - gxm[lvl(al)]) * iz0, ex1 = (gxm[lvl(br)] - gxm[lvl(bl)]) * iz1;
+    const T ey0 = (gym[lvl(ar)] - gym[lvl(al)]) * iz0, ey1 = (gym[lvl(br)] - gym[lvl(bl)]) * iz1;
+    const T m = ld(c.mm, h_m(d, i, j));
+    const int p = im(d, i, j, k);
+    const T divx = m * (gx1 - gx0) * (T)(1.0 / d.dx) - ld(c.zxm, p) * T(0.5) * (ex0 + ex1);
+    const T divy = m * (gy1 - gy0) * (T)(1.0 / d.dy) - ld(c.zem, p) * T(0.5) * (ey0 + ey1);
+    return divx + divy;
+  }
+};
+
+template <typename T>
+__global__ void hyper_lap_kernel(Dims d, Coef<T> c, PtrTable<T> src, PtrTable<T> dst, T scale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kz = blockIdx.z * blockDim.z + threadIdx.z;
+  const int f = kz / d.nz, k = kz % d.nz;
+  if (i >= d.nx || j >= d.ny || f >= 4) return;
+  HLap<T> L{d, c, src.p[f]};
+  dst.p[f][im(d, i, j, k)] = scale * L.lap(i, j, k);
+}
+
+// ---------------------------------------------------------------------------
+// explicit tendencies.  mode 0: step inputs (u_in, v_in, w_in, pi_in, th_in,
+// tend_th, residual_n); mode 1: raw tendencies for the operator API.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) explicit_kernel(Dims d, Coef<T> c, ExplicitIn<T> in, ExplicitOut<T> out,
+                                                       int mode) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i > nx || j > ny || k > nz) return;
+  const T dt = (T)c.s.dt, a = (T)c.s.alpha, cp = (T)c.s.cp, g = (T)c.s.g;
+  const T oma = T(1) - a;
+  Grad<T> G{d, c, in.pi};
+  Winds<T> W{d, c, in.u, in.v};
+  const T* __restrict__ th = in.th;
+  const bool hyp = in.hyper[0] != nullptr && mode != 2;
+  const T lin = (mode == 2) ? T(0) : T(1);  // mode 2: linear tendencies (euler.py:240-247, 281-282)
+
+  if (j < ny && k < nz) {  // u faces
+    int l, r;
+    face_pair(i, nx, d.px, l, r);
+    const int p = iu(d, i, j, k);
+    const T thp = lin * T(0.5) * (ld(th, im(d, l, j, k)) + ld(th, im(d, r, j, k)));
+    const T vat = T(0.5) * (W.vm(l, j, k) + W.vm(r, j, k));
+    const T met = lin * T(0.5) * (W.metric_m(l, j, k) + W.metric_m(r, j, k)) * vat;
+    const T pd = hyp ? T(0.5) * (ld(in.hyper[0], im(d, l, j, k)) + ld(in.hyper[0], im(d, r, j, k))) : T(0);
+    const T tend = -cp * (ld(c.thu, p) + thp) * G.gx(i, j, k) + ld(c.fu, h_u(d, i, j)) * vat + met + pd;
+    if (mode == 0) {
+      out.f[0][p] = ld(in.u, p) + dt * (oma * tend + a * pd);
+    } else {
+      out.f[0][p] = tend;
+      if (out.pd[0]) out.pd[0][p] = pd;
+    }
+  }
+  if (i < nx && k < nz) {  // v faces
+    int l, r;
+    face_pair(j, ny, d.py, l, r);
+    const int p = iv(d, i, j, k);
+    const T thp = lin * T(0.5) * (ld(th, im(d, i, l, k)) + ld(th, im(d, i, r, k)));
+    const T uat = T(0.5) * (W.um(i, l, k) + W.um(i, r, k));
+    const T met = -lin * T(0.5) * (W.metric_m(i, l, k) + W.metric_m(i, r, k)) * uat;
+    const T pd = hyp ? T(0.5) * (ld(in.hyper[1], im(d, i, l, k)) + ld(in.hyper[1], im(d, i, r, k))) : T(0);
+    const T tend = -cp * (ld(c.thv, p) + thp) * G.gy(i, j, k) - ld(c.fv, h_v(d, i, j)) * uat + met + pd;
+    if (mode == 0) {
+      out.f[1][p] = ld(in.v, p) + dt * (oma * tend + a * pd);
+    } else {
+      out.f[1][p] = tend;
+      if (out.pd[1]) out.pd[1][p] = pd;
+    }
+  }
+  if (i < nx && j < ny) {  // w levels
+    int kl, kr;
+    level_pair(k, nz, kl, kr);
+    const int p = iw(d, i, j, k);
+    const T thp = lin * T(0.5) * (ld(th, im(d, i, j, kl)) + ld(th, im(d, i, j, kr)));
+    const T thw = ld(c.thw, p);
+    const T pd = hyp ? T(0.5) * (ld(in.hyper[2], im(d, i, j, kl)) + ld(in.hyper[2], im(d, i, j, kr))) : T(0);
+    const T tend = -cp * (thw + thp) * G.gzw(i, j, k) + g * (thp / thw) + pd;
+    if (mode == 0) {
+      out.f[2][p] = ld(in.w, p) + dt * (oma * tend + a * pd);
+      // residual_n = dz_w eta + u_w z_xi_w + v_w z_eta_w - w  (steppers.py:837-842)
+      out.f[6][p] = ld(c.dzw, p) * ld(in.eta, p) + W.uw(i, j, k) * ld(c.zxw, p) + W.vw(i, j, k) * ld(c.zew, p) -
+                    ld(in.w, p);
+    } else {
+      out.f[2][p] = tend;
+      if (out.pd[2]) out.pd[2][p] = pd;
+    }
+  }
+  if (i < nx && j < ny && k < nz) {  // mass points
+    const int p = im(d, i, j, k);
+    auto thu_lin = [&](int a_, int b_, int c_) { return ld(c.thu, iu(d, a_, b_, c_)); };
+    auto thv_lin = [&](int a_, int b_, int c_) { return ld(c.thv, iv(d, a_, b_, c_)); };
+    auto thw_lin = [&](int a_, int b_, int c_) { return ld(c.thw, iw(d, a_, b_, c_)); };
+    auto thu_nl = [&](int a_, int b_, int c_) { return avg_mu(d, th, a_, b_, c_); };
+    auto thv_nl = [&](int a_, int b_, int c_) { return avg_mv(d, th, a_, b_, c_); };
+    auto thw_nl = [&](int a_, int b_, int c_) { return avg_mw(d, th, a_, b_, c_); };
+    const T tpi = divergence(d, c, in.u, in.v, in.eta, i, j, k, thu_lin, thv_lin, thw_lin);
+    const T nlpi = (mode == 2) ? T(0) : divergence(d, c, in.u, in.v, in.eta, i, j, k, thu_nl, thv_nl, thw_nl);
+    const T wm = T(0.5) * (ld(in.w, iw(d, i, j, k)) + ld(in.w, iw(d, i, j, k + 1)));
+    const T pd = hyp ? ld(in.hyper[3], p) : T(0);
+    const T tth = -wm * ld(c.dthm, p) + pd;
+    if (mode == 0) {
+      out.f[3][p] = ld(in.pi, p) + oma * dt * (tpi + nlpi);
+      out.f[4][p] = ld(th, p) + oma * dt * tth;
+      out.f[5][p] = tth;
+    } else {
+      out.f[3][p] = tpi;
+      out.f[4][p] = tth;
+      out.f[5][p] = nlpi;
+      if (out.pd[3]) out.pd[3][p] = pd;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// predictor-corrector (steppers.py:911-983)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void corrector_theta_kernel(Dims d, Coef<T> c, const T* __restrict__ th_adv, const T* __restrict__ tth,
+                                       const T* __restrict__ w_now, const T* __restrict__ w_next, T* th_next) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= d.nx || j >= d.ny || k >= d.nz) return;
+  const int p = im(d, i, j, k);
+  const T wm = T(0.5) * (ld(w_now, iw(d, i, j, k)) + ld(w_now, iw(d, i, j, k + 1)));
+  const T wmn = T(0.5) * (ld(w_next, iw(d, i, j, k)) + ld(w_next, iw(d, i, j, k + 1)));
+  const T adt = (T)(c.s.alpha * c.s.dt);
+  th_next[p] = ld(th_adv, p) + adt * (ld(tth, p) + (wm - wmn) * ld(c.dthm, p));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) corrector_rhs_kernel(Dims d, Coef<T> c, CorrectorIn<T> in, Vec5<T> out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i > nx || j > ny || k > nz) return;
+  const T adt = (T)(c.s.alpha * c.s.dt);
+  const T cad = (T)(c.s.cp * c.s.alpha * c.s.dt);
+  const T g = (T)c.s.g;
+  Grad<T> G{d, c, in.pg};
+  Winds<T> WG{d, c, in.ug, in.vg};
+  const T* __restrict__ th = in.th_next;
+  if (j < ny && k < nz) {
+    int l, r;
+    face_pair(i, nx, d.px, l, r);
+    const int p = iu(d, i, j, k);
+    const T thp = T(0.5) * (ld(th, im(d, l, j, k)) + ld(th, im(d, r, j, k)));
+    const T vat = T(0.5) * (WG.vm(l, j, k) + WG.vm(r, j, k));
+    const T met = T(0.5) * (WG.metric_m(l, j, k) + WG.metric_m(r, j, k)) * vat;
+    out.f[0][p] = ld(in.rhs_u, p) - cad * thp * G.gx(i, j, k) + adt * met;
+  }
+  if (i < nx && k < nz) {
+    int l, r;
+    face_pair(j, ny, d.py, l, r);
+    const int p = iv(d, i, j, k);
+    const T thp = T(0.5) * (ld(th, im(d, i, l, k)) + ld(th, im(d, i, r, k)));
+    const T uat = T(0.5) * (WG.um(i, l, k) + WG.um(i, r, k));
+    const T met = -T(0.5) * (WG.metric_m(i, l, k) + WG.metric_m(i, r, k)) * uat;
+    out.f[1][p] = ld(in.rhs_v, p) - cad * thp * G.gy(i, j, k) + adt * met;
+  }
+  if (i < nx && j < ny) {
+    const int p = iw(d, i, j, k);
+    T val;
+    if (k == 0) {  // kinematic bottom boundary from the latest solver guess (steppers.py:974-983)
+      val = ld(c.mm, h_m(d, i, j)) * (WG.uw(i, j, 0) * ld(c.zxw, p) + WG.vw(i, j, 0) * ld(c.zew, p));
+    } else if (k == nz) {
+      val = T(0);
+    } else {
+      const T thp = T(0.5) * (ld(th, im(d, i, j, k - 1)) + ld(th, im(d, i, j, k)));
+      val = ld(in.rhs_w, p) + adt * (g * (thp / ld(c.thw, p))) - cad * thp * G.gzw(i, j, k);
+    }
+    out.f[2][p] = val;
+  }
+  if (i < nx && j < ny && k < nz) {
+    const int p = im(d, i, j, k);
+    auto thu_nl = [&](int a_, int b_, int c_) { return avg_mu(d, th, a_, b_, c_); };
+    auto thv_nl = [&](int a_, int b_, int c_) { return avg_mv(d, th, a_, b_, c_); };
+    auto thw_nl = [&](int a_, int b_, int c_) { return avg_mw(d, th, a_, b_, c_); };
+    const T nl = divergence(d, c, in.gu, in.gv, in.geta, i, j, k, thu_nl, thv_nl, thw_nl);
+    out.f[3][p] = ld(in.rhs_pi, p) + adt * nl;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// finalisation: divergence damping (steppers.py:1022-1031), relaxation
+// blend (the bc_fn of the mountain-wave runs, schaer_mountain_3d/run.py:104-126),
+// EOS (steppers.py:1055-1056)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void hdiv_kernel(Dims d, Coef<T> c, const T* __restrict__ u, const T* __restrict__ v, T* div) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= d.nx || j >= d.ny || k >= d.nz) return;
+  const T m = ld(c.mm, h_m(d, i, j));
+  const T dux = (ld(u, iu(d, i + 1, j, k)) - ld(u, iu(d, i, j, k))) * (T)(1.0 / d.dx) * m;
+  const T dvy = (ld(v, iv(d, i, j + 1, k)) - ld(v, iv(d, i, j, k))) * (T)(1.0 / d.dy) * m;
+  div[im(d, i, j, k)] = dux + dvy;
+}
+
+template <typename T>
+__device__ __forceinline__ T blend(T val, const T* mask, int h, T ext) {
+  if (!mask) return val;
+  const T m = ld(mask, h);
+  return (T(1) - m) * val + m * ext;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) finalize_kernel(Dims d, Coef<T> c, FinalizeArgs<T> fa) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i > nx || j > ny || k > nz) return;
+  const T nud = (T)(c.s.nu_div * c.s.dt);
+  const Relax<T>& R = fa.relax;
+  if (j < ny && k < nz) {
+    const int p = iu(d, i, j, k);
+    T val = ld(fa.u_in, p);
+    if (fa.div) {
+      int l, r;
+      face_pair(i, nx, d.px, l, r);
+      val += nud * (ld(fa.div, im(d, r, j, k)) - ld(fa.div, im(d, l, j, k))) * (T)(1.0 / d.dx) *
+             ld(c.mu, h_u(d, i, j));
+    }
+    if (R.on & RELAX_U) val = blend(val, R.mask_u, h_u(d, i, j), R.ext_field[0] ? ld(R.ext_field[0], p) : R.ext[0]);
+    fa.u_out[p] = val;
+  }
+  if (i < nx && k < nz) {
+    const int p = iv(d, i, j, k);
+    T val = ld(fa.v_in, p);
+    if (fa.div) {
+      int l, r;
+      face_pair(j, ny, d.py, l, r);
+      val += nud * (ld(fa.div, im(d, i, r, k)) - ld(fa.div, im(d, i, l, k))) * (T)(1.0 / d.dy) *
+             ld(c.mv, h_v(d, i, j));
+    }
+    if (R.on & RELAX_V) val = blend(val, R.mask_v, h_v(d, i, j), R.ext_field[1] ? ld(R.ext_field[1], p) : R.ext[1]);
+    fa.v_out[p] = val;
+  }
+  if (i < nx && j < ny) {
+    const int p = iw(d, i, j, k);
+    if (R.on & RELAX_W)
+      fa.w_io[p] = blend(fa.w_io[p], R.mask_m, h_m(d, i, j), R.ext_field[2] ? ld(R.ext_field[2], p) : R.ext[2]);
+  }
+  if (i < nx && j < ny && k < nz) {
+    const int p = im(d, i, j, k);
+    T th = fa.th_io[p], pi = fa.pi_io[p];
+    if (R.on & RELAX_TH) th = blend(th, R.mask_m, h_m(d, i, j), R.ext_field[3] ? ld(R.ext_field[3], p) : R.ext[3]);
+    if (R.on & RELAX_PI) pi = blend(pi, R.mask_m, h_m(d, i, j), R.ext_field[4] ? ld(R.ext_field[4], p) : R.ext[4]);
+    fa.th_io[p] = th;
+    fa.pi_io[p] = pi;
+    if (fa.rho_out) {
+      const T thf = th + ld(c.thb, p), pif = pi + ld(c.pib, p);
+      fa.rho_out[p] = (T)c.s.p0 / ((T)c.s.Rd * thf) * pow(pif, (T)(c.s.cvd / c.s.Rd));
+    }
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_hyper(const Dims& d, const Coef<T>& c, const T* u, const T* v, const T* w, const T* th,
+                  PtrTable<T> tmp4, PtrTable<T> out4, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  hyper_src_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, u, v, w, th, out4);
+  dim3 g2 = box_grid(d.nx, d.ny, 4 * d.nz, blk);
+  hyper_lap_kernel<T><<<g2, blk, 0, st>>>(d, c, out4, tmp4, T(1));
+  hyper_lap_kernel<T><<<g2, blk, 0, st>>>(d, c, tmp4, out4, (T)(-c.s.nu_h));
+}
+
+template <typename T>
+void launch_explicit(const Dims& d, const Coef<T>& c, const ExplicitIn<T>& in, const ExplicitOut<T>& out, int mode,
+                     cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  explicit_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, in, out, mode);
+}
+
+template <typename T>
+void launch_corrector_theta(const Dims& d, const Coef<T>& c, const T* th_adv, const T* tth, const T* w_now,
+                            const T* w_next, T* th_next, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  corrector_theta_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, c, th_adv, tth, w_now, w_next,
+                                                                            th_next);
+}
+
+template <typename T>
+void launch_corrector_rhs(const Dims& d, const Coef<T>& c, const CorrectorIn<T>& in, Vec5<T> out, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  corrector_rhs_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, in, out);
+}
+
+template <typename T>
+void launch_hdiv(const Dims& d, const Coef<T>& c, const T* u, const T* v, T* div, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  hdiv_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, c, u, v, div);
+}
+
+template <typename T>
+void launch_finalize(const Dims& d, const Coef<T>& c, const FinalizeArgs<T>& fa, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  finalize_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, fa);
+}
+
+#define SISL_INST_EX(T)                                                                                        \
+  template void launch_hyper<T>(const Dims&, const Coef<T>&, const T*, const T*, const T*, const T*,           \
+                                PtrTable<T>, PtrTable<T>, cudaStream_t);                                       \
+  template void launch_explicit<T>(const Dims&, const Coef<T>&, const ExplicitIn<T>&, const ExplicitOut<T>&,   \
+                                   int, cudaStream_t);                                                         \
+  template void launch_corrector_theta<T>(const Dims&, const Coef<T>&, const T*, const T*, const T*, const T*, \
+                                          T*, cudaStream_t);                                                   \
+  template void launch_corrector_rhs<T>(const Dims&, const Coef<T>&, const CorrectorIn<T>&, Vec5<T>,         \
+                                        cudaStream_t);                                                         \
+  template void launch_hdiv<T>(const Dims&, const Coef<T>&, const T*, const T*, T*, cudaStream_t);             \
+  template void launch_finalize<T>(const Dims&, const Coef<T>&, const FinalizeArgs<T>&, cudaStream_t);
+SISL_INST_EX(float)
+SISL_INST_EX(double)
+
+}  // namespace sisl

@@ -1,0 +1,197 @@
+// Flux-form semi-Lagrangian mass transport and the equation of state.
+//
+// FluxFormAdvector.advect_3d_split (steppers.py:596-647) with advect_1d
+// (steppers.py:552-594): cell masses rho dx dy / m^2 dz_m, one sweep per
+// axis (x, y, z) remapping the cumulative mass to the departure interfaces
+// with linear interpolation.  One thread per grid line; the cumulative mass
+// of each line is accumulated in float64 in a line-interleaved scratch array
+// (position-major, line-fastest, so neighbouring threads touch neighbouring
+// words).  Periodic axes use the three-copy extension of steppers.py:569-582
+// evaluated in closed form: M_ext(p) = floor(p / N) S + M(p mod N).
+#include "sisl_core.cuh"
+
+namespace sisl {
+namespace {
+
+template <typename T>
+__device__ __forceinline__ T cell_volume(const Dims& d, const Coef<T>& c, int i, int j, int k) {
+  const T m = ld(c.mm, h_m(d, i, j));
+  return (T)(d.dx * d.dy) / (m * m) * ld(c.dzm, im(d, i, j, k));
+}
+
+template <typename T>
+__global__ void ffsl_mass_kernel(Dims d, Coef<T> c, const T* __restrict__ rho, T* mass) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= d.nx || j >= d.ny || k >= d.nz) return;
+  const int p = im(d, i, j, k);
+  mass[p] = ld(rho, p) * cell_volume(d, c, i, j, k);
+}
+
+template <typename T>
+__global__ void ffsl_sweep_kernel(Dims d, Coef<T> c, int axis, const T* __restrict__ in, const T* __restrict__ vel,
+                                  T* out, double* __restrict__ M, int periodic, double dt, int to_density) {
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  int N, nlines, a, b;
+  if (axis == 0) { N = d.nx; nlines = d.ny * d.nz; a = line % d.ny; b = line / d.ny; }
+  else if (axis == 1) { N = d.ny; nlines = d.nx * d.nz; a = line % d.nx; b = line / d.nx; }
+  else { N = d.nz; nlines = d.nx * d.ny; a = line % d.nx; b = line / d.nx; }
+  if (line >= nlines) return;
+  auto cell = [&](int q) -> int {
+    if (axis == 0) return im(d, q, a, b);
+    if (axis == 1) return im(d, a, q, b);
+    return im(d, a, b, q);
+  };
+  auto cfl = [&](int q) -> double {  // interface Courant number (steppers.py:614-616)
+    if (axis == 0) return (double)ld(vel, iu(d, q, a, b)) * (double)ld(c.mu, h_u(d, q, a)) * dt / d.dx;
+    if (axis == 1) return (double)ld(vel, iv(d, a, q, b)) * (double)ld(c.mv, h_v(d, a, q)) * dt / d.dy;
+    return (double)ld(vel, iw(d, a, b, q)) * dt;
+  };
+  // cumulative mass M[0..N]
+  double s = 0.0;
+  M[line] = 0.0;
+  for (int q = 0; q < N; ++q) {
+    s += (double)ld(in, cell(q));
+    M[(size_t)(q + 1) * nlines + line] = s;
+  }
+  const double S = s;
+  auto Mext = [&](long long p) -> double {  // periodic three-copy cumulative mass
+    const long long blk = p / N, r = p % N;
+    return (double)blk * S + M[(size_t)r * nlines + line];
+  };
+  auto Mdep = [&](int q) -> double {
+    const double c0 = cfl(q);
+    if (periodic) {
+      const double dep = (double)(q + N) - c0;
+      const double lo = floor(dep);
+      const double w = dep - lo;
+      const long long L = 3LL * N + 1;
+      long long i0 = (long long)lo, i1 = i0 + 1;
+      i0 = i0 < 0 ? 0 : (i0 > L - 1 ? L - 1 : i0);
+      i1 = i1 < 0 ? 0 : (i1 > L - 1 ? L - 1 : i1);
+      return (1.0 - w) * Mext(i0) + w * Mext(i1);
+    }
+    double dep = (double)q - c0;
+    dep = fmin(fmax(dep, 0.0), (double)N);
+    const double lo = floor(dep);
+    const double w = dep - lo;
+    int i0 = (int)lo, i1 = i0 + 1;
+    i0 = min(max(i0, 0), N);
+    i1 = min(max(i1, 0), N);
+    return (1.0 - w) * M[(size_t)i0 * nlines + line] + w * M[(size_t)i1 * nlines + line];
+  };
+  double prev = Mdep(0);
+  for (int q = 0; q < N; ++q) {
+    const double nxt = Mdep(q + 1);
+    const int p = cell(q);
+    double val = nxt - prev;
+    if (to_density) {
+      int i, j, k;
+      if (axis == 0) { i = q; j = a; k = b; } else if (axis == 1) { i = a; j = q; k = b; } else { i = a; j = b; k = q; }
+      val /= (double)cell_volume(d, c, i, j, k);
+    }
+    out[p] = (T)val;
+    prev = nxt;
+  }
+}
+
+// advect_1d (steppers.py:552-594) on nlines independent lines: scalar is
+// (nlines, N) and cfl (nlines, N + 1), both line-major.
+template <typename T>
+__global__ void ffsl_line_kernel(int N, int nlines, const T* __restrict__ sc, const T* __restrict__ cf, T* out,
+                                 double* __restrict__ M, int periodic) {
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= nlines) return;
+  const T* s_ = sc + (size_t)line * N;
+  const T* c_ = cf + (size_t)line * (N + 1);
+  double s = 0.0;
+  M[line] = 0.0;
+  for (int q = 0; q < N; ++q) {
+    s += (double)s_[q];
+    M[(size_t)(q + 1) * nlines + line] = s;
+  }
+  const double S = s;
+  auto Mat = [&](long long p) -> double {
+    if (!periodic) return M[(size_t)p * nlines + line];
+    return (double)(p / N) * S + M[(size_t)(p % N) * nlines + line];
+  };
+  const long long L = periodic ? 3LL * N + 1 : (long long)N + 1;
+  auto Mdep = [&](int q) -> double {
+    double dep = periodic ? (double)(q + N) - (double)c_[q] : fmin(fmax((double)q - (double)c_[q], 0.0), (double)N);
+    const double lo = floor(dep), w = dep - lo;
+    long long i0 = (long long)lo, i1 = i0 + 1;
+    i0 = i0 < 0 ? 0 : (i0 > L - 1 ? L - 1 : i0);
+    i1 = i1 < 0 ? 0 : (i1 > L - 1 ? L - 1 : i1);
+    return (1.0 - w) * Mat(i0) + w * Mat(i1);
+  };
+  double prev = Mdep(0);
+  for (int q = 0; q < N; ++q) {
+    const double nxt = Mdep(q + 1);
+    out[(size_t)line * N + q] = (T)(nxt - prev);
+    prev = nxt;
+  }
+}
+
+template <typename T>
+__global__ void eos_kernel(Dims d, Coef<T> c, const T* __restrict__ th, const T* __restrict__ pi, T* rho) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= d.nx || j >= d.ny || k >= d.nz) return;
+  const int p = im(d, i, j, k);
+  const T thf = ld(th, p) + ld(c.thb, p), pif = ld(pi, p) + ld(c.pib, p);
+  rho[p] = (T)c.s.p0 / ((T)c.s.Rd * thf) * pow(pif, (T)(c.s.cvd / c.s.Rd));  // steppers.py:1056
+}
+
+dim3 box3(const Dims& d, dim3 blk) {
+  return dim3((d.nx + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, (d.nz + blk.z - 1) / blk.z);
+}
+
+}  // namespace
+
+size_t ffsl_scratch_doubles(const Dims& d) {
+  size_t x = (size_t)(d.nx + 1) * d.ny * d.nz, y = (size_t)(d.ny + 1) * d.nx * d.nz, z = (size_t)(d.nz + 1) * d.nx * d.ny;
+  size_t m = x > y ? x : y;
+  return m > z ? m : z;
+}
+
+// out = FFSL(field); tmp0/tmp1 are mass-point scratch fields, M the
+// float64 line scratch of ffsl_scratch_doubles() entries.
+template <typename T>
+int launch_ffsl(const Dims& d, const Coef<T>& c, const T* field, const T* u, const T* v, const T* eta, T* out, T* tmp0,
+                T* tmp1, double* M, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  ffsl_mass_kernel<T><<<box3(d, blk), blk, 0, st>>>(d, c, field, tmp0);
+  const int tb = 128;
+  const double dt = c.s.dt;
+  ffsl_sweep_kernel<T><<<(d.ny * d.nz + tb - 1) / tb, tb, 0, st>>>(d, c, 0, tmp0, u, tmp1, M, d.px, dt, 0);
+  ffsl_sweep_kernel<T><<<(d.nx * d.nz + tb - 1) / tb, tb, 0, st>>>(d, c, 1, tmp1, v, tmp0, M, d.py, dt, 0);
+  ffsl_sweep_kernel<T><<<(d.nx * d.ny + tb - 1) / tb, tb, 0, st>>>(d, c, 2, tmp0, eta, out, M, 0, dt, 1);
+  return 4;  // kernels launched
+}
+
+template <typename T>
+void launch_ffsl_lines(int N, int nlines, const T* scalar, const T* cfl, T* out, double* M, int periodic,
+                       cudaStream_t st) {
+  ffsl_line_kernel<T><<<(nlines + 127) / 128, 128, 0, st>>>(N, nlines, scalar, cfl, out, M, periodic);
+}
+
+template <typename T>
+void launch_eos(const Dims& d, const Coef<T>& c, const T* th, const T* pi, T* rho, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  eos_kernel<T><<<box3(d, blk), blk, 0, st>>>(d, c, th, pi, rho);
+}
+
+template int launch_ffsl<float>(const Dims&, const Coef<float>&, const float*, const float*, const float*,
+                                const float*, float*, float*, float*, double*, cudaStream_t);
+template int launch_ffsl<double>(const Dims&, const Coef<double>&, const double*, const double*, const double*,
+                                 const double*, double*, double*, double*, double*, cudaStream_t);
+template void launch_ffsl_lines<float>(int, int, const float*, const float*, float*, double*, int, cudaStream_t);
+template void launch_ffsl_lines<double>(int, int, const double*, const double*, double*, double*, int,
+                                        cudaStream_t);
+template void launch_eos<float>(const Dims&, const Coef<float>&, const float*, const float*, float*, cudaStream_t);
+template void launch_eos<double>(const Dims&, const Coef<double>&, const double*, const double*, double*,
+                                 cudaStream_t);
+
+}  // namespace sisl

@@ -1,0 +1,423 @@
+// Flat vector kernels and float64 bookkeeping of the device-resident GMRES.
+//
+// Restates jax.scipy.sparse.linalg.gmres (jax/jaxlib >= 0.10.0; called at
+// steppers.py:466 and :476): left preconditioning (Krylov space of M A), one
+// classical Gram-Schmidt projection per Arnoldi step over the basis, breakdown
+// when ||v|| <= eps ||M A v_k||, and either the 'batched' cycle (normal
+// equations + Cholesky for the Hessenberg least-squares problem) or the
+// 'incremental' cycle (Givens rotations, early exit on the rotated residual).
+//
+// A basis vector V_i is stored unnormalised next to its inverse norm s_i, so
+// normalisation never costs a pass over memory: the matvec scales its input
+// on load, projections use h_i = s_i <V_i, w>, updates use h_i s_i V_i.
+// Every reduction accumulates in float64; the last block of a reduction
+// kernel (ticket counter) finishes the sum and runs the scalar logic.
+#include "sisl_gmres.cuh"
+
+#include <math.h>
+
+namespace sisl {
+namespace {
+
+constexpr int GT = 256;  // threads per block of the flat kernels
+
+template <typename T> struct V16;
+template <> struct V16<float> { using type = float4; static constexpr int n = 4; };
+template <> struct V16<double> { using type = double2; static constexpr int n = 2; };
+
+template <typename T>
+__device__ __forceinline__ void load16(const T* p, T* r) {
+  using VT = typename V16<T>::type;
+  VT v = __ldg(reinterpret_cast<const VT*>(p));
+  const T* q = reinterpret_cast<const T*>(&v);
+#pragma unroll
+  for (int e = 0; e < V16<T>::n; ++e) r[e] = q[e];
+}
+template <typename T>
+__device__ __forceinline__ void store16(T* p, const T* r) {
+  using VT = typename V16<T>::type;
+  VT v;
+  T* q = reinterpret_cast<T*>(&v);
+#pragma unroll
+  for (int e = 0; e < V16<T>::n; ++e) q[e] = r[e];
+  *reinterpret_cast<VT*>(p) = v;
+}
+
+// Per-thread chunk: CH 16-byte loads (E = CH * 16/sizeof(T) elements).
+constexpr int CH = 4;
+
+__device__ __forceinline__ double warp_sum(double s) {
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// Last-block ticket.  Returns true in exactly one block, after every other
+// block's partial results are visible.
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+  __shared__ bool am_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = atomicAdd(counter, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (am_last) __threadfence();
+  return am_last;
+}
+
+enum DotMode { DM_PROJ = 0, DM_BNORM = 1, DM_MBNORM = 2, DM_RNORM = 3 };
+
+// result_i = <V_i, w> for i < m and <w, w>; finished according to `mode`.
+template <typename T>
+__global__ void __launch_bounds__(GT) dots_kernel(const T* __restrict__ Vb, size_t stride, int m,
+                                                  const T* __restrict__ w, size_t n, double* partial,
+                                                  GState* gs, int mode, int gated) {
+  if (gated && gs->active == 0) return;
+  extern __shared__ double acc[];  // m + 1
+  for (int q = threadIdx.x; q <= m; q += blockDim.x) acc[q] = 0.0;
+  __syncthreads();
+  constexpr int VN = V16<T>::n;
+  constexpr int E = CH * VN;
+  const size_t tile = (size_t)GT * E;
+  const int lane = threadIdx.x & 31;
+  for (size_t base = (size_t)blockIdx.x * tile; base < n; base += (size_t)gridDim.x * tile) {
+    T wr[E];
+    bool ok[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      const size_t off = base + ((size_t)c * GT + threadIdx.x) * VN;
+      ok[c] = off < n;
+      if (ok[c]) load16(w + off, wr + c * VN);
+      else
+#pragma unroll
+        for (int e = 0; e < VN; ++e) wr[c * VN + e] = T(0);
+    }
+    double sq = 0.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) sq += (double)wr[e] * (double)wr[e];
+    sq = warp_sum(sq);
+    if (lane == 0) atomicAdd(&acc[m], sq);
+    for (int i = 0; i < m; ++i) {
+      const T* __restrict__ Vi = Vb + (size_t)i * stride;
+      T vr[E];
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        const size_t off = base + ((size_t)c * GT + threadIdx.x) * VN;
+        if (ok[c]) load16(Vi + off, vr + c * VN);
+        else
+#pragma unroll
+          for (int e = 0; e < VN; ++e) vr[c * VN + e] = T(0);
+      }
+      double p = 0.0;
+#pragma unroll
+      for (int e = 0; e < E; ++e) p += (double)vr[e] * (double)wr[e];
+      p = warp_sum(p);
+      if (lane == 0) atomicAdd(&acc[i], p);
+    }
+  }
+  __syncthreads();
+  double* mine = partial + (size_t)blockIdx.x * (GM_MAXR + 2);
+  for (int q = threadIdx.x; q <= m; q += blockDim.x) mine[q] = acc[q];
+  if (!last_block(&gs->counter)) return;
+  // finish: sum the partials of all blocks
+  for (int q = threadIdx.x; q <= m; q += blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s += partial[(size_t)b * (GM_MAXR + 2) + q];
+    acc[q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    gs->counter = 0;
+    const double nrm = sqrt(acc[m]);
+    if (mode == DM_PROJ) {
+      for (int i = 0; i < m; ++i) gs->h[i] = gs->s[i] * acc[i];
+      gs->hn0 = nrm;
+    } else if (mode == DM_BNORM) {
+      gs->bnorm = nrm;
+    } else if (mode == DM_MBNORM) {
+      gs->mbnorm = nrm;
+    } else {  // DM_RNORM: _safe_normalize of the preconditioned residual
+      const bool use = nrm > gs->eps;
+      gs->s[0] = use ? 1.0 / nrm : 0.0;
+      gs->rnorm = use ? nrm : 0.0;
+    }
+  }
+}
+
+enum UpdMode { UM_NONE = 0, UM_ARNOLDI = 1 };
+
+// w <- w + sign * sum_{i<m'} coef_i V_i with coef from gs->coef (UM_NONE,
+// m' = min(m, kdone) when limit_kdone) or coef_i = h_i s_i (UM_ARNOLDI),
+// then optionally finish the Arnoldi step j = m - 1.
+template <typename T>
+__global__ void __launch_bounds__(GT) update_kernel(const T* __restrict__ Vb, size_t stride, int m,
+                                                    T* __restrict__ w, size_t n, double sign, double* partial,
+                                                    GState* gs, int mode, int gated, int limit_kdone) {
+  if (gated && gs->active == 0) return;
+  __shared__ double cf[GM_MAXR + 2];
+  __shared__ double red[GT / 32];
+  int mm = m;
+  if (limit_kdone) mm = min(m, gs->kdone);
+  for (int q = threadIdx.x; q < mm; q += blockDim.x)
+    cf[q] = sign * (mode == UM_ARNOLDI ? gs->h[q] * gs->s[q] : gs->coef[q]);
+  __syncthreads();
+  constexpr int VN = V16<T>::n;
+  constexpr int E = CH * VN;
+  const size_t tile = (size_t)GT * E;
+  double sq = 0.0;
+  for (size_t base = (size_t)blockIdx.x * tile; base < n; base += (size_t)gridDim.x * tile) {
+    T wr[E];
+    bool ok[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      const size_t off = base + ((size_t)c * GT + threadIdx.x) * VN;
+      ok[c] = off < n;
+      if (ok[c]) load16(w + off, wr + c * VN);
+    }
+    for (int i = 0; i < mm; ++i) {
+      const T* __restrict__ Vi = Vb + (size_t)i * stride;
+      const T ci = (T)cf[i];
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        if (!ok[c]) continue;
+        const size_t off = base + ((size_t)c * GT + threadIdx.x) * VN;
+        T vr[VN];
+        load16(Vi + off, vr);
+#pragma unroll
+        for (int e = 0; e < VN; ++e) wr[c * VN + e] += ci * vr[e];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      if (!ok[c]) continue;
+      const size_t off = base + ((size_t)c * GT + threadIdx.x) * VN;
+      store16(w + off, wr + c * VN);
+#pragma unroll
+      for (int e = 0; e < VN; ++e) sq += (double)wr[c * VN + e] * (double)wr[c * VN + e];
+    }
+  }
+  if (mode != UM_ARNOLDI) return;
+  sq = warp_sum(sq);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int q = 0; q < GT / 32; ++q) s += red[q];
+    partial[blockIdx.x] = s;
+  }
+  if (!last_block(&gs->counter)) return;
+  if (threadIdx.x != 0) return;
+  double tot = 0.0;
+  for (int b = 0; b < (int)gridDim.x; ++b) tot += partial[b];
+  gs->counter = 0;
+  // ---- finish Arnoldi step j (jax _kth_arnoldi_iteration) ----
+  const int j = m - 1;
+  const int R = gs->restart;
+  double vn1 = sqrt(tot);
+  const double thresh = gs->eps * gs->hn0;
+  if (vn1 > thresh) {
+    gs->s[j + 1] = 1.0 / vn1;
+  } else {
+    gs->s[j + 1] = 0.0;
+    vn1 = 0.0;
+  }
+  double row[GM_MAXR + 1];
+  for (int q = 0; q <= R; ++q) row[q] = 0.0;
+  for (int q = 0; q <= j; ++q) row[q] = gs->h[q];
+  row[j + 1] = vn1;
+  gs->kdone = j + 1;
+  if (gs->method == 0) {  // batched: H[j, :] = h
+    for (int q = 0; q <= R; ++q) gs->H[j][q] = row[q];
+    if (vn1 == 0.0) { gs->breakdown = 1; gs->active = 0; }
+  } else {  // incremental: rotate into R, update beta
+    for (int i = 0; i < j; ++i) {
+      const double c = gs->givens[i][0], s = gs->givens[i][1];
+      const double x1 = row[i], y1 = row[i + 1];
+      row[i] = c * x1 - s * y1;
+      row[i + 1] = s * x1 + c * y1;
+    }
+    // _givens_rotation(a, b)
+    const double a = row[j], b = row[j + 1];
+    double cs, sn;
+    if (b == 0.0) {
+      cs = 1.0; sn = 0.0;
+    } else if (fabs(a) < fabs(b)) {
+      const double t = -a / b, r = 1.0 / sqrt(1.0 + t * t);
+      cs = r * t; sn = r;
+    } else {
+      const double t = -b / a, r = 1.0 / sqrt(1.0 + t * t);
+      cs = r; sn = r * t;
+    }
+    gs->givens[j][0] = cs;
+    gs->givens[j][1] = sn;
+    row[j] = cs * a - sn * b;
+    row[j + 1] = sn * a + cs * b;
+    for (int q = 0; q <= R; ++q) gs->H[j][q] = row[q];
+    const double b0 = gs->beta[j], b1 = gs->beta[j + 1];
+    gs->beta[j] = cs * b0 - sn * b1;
+    gs->beta[j + 1] = sn * b0 + cs * b1;
+    gs->err = fabs(gs->beta[j + 1]);
+    if (!(gs->err > gs->ptol)) gs->active = 0;
+  }
+}
+
+__global__ void setup_kernel(GState* gs, double eps, double tol, double atol_in, int restart, int method) {
+  gs->eps = eps;
+  gs->tol = tol;
+  gs->atol_in = atol_in;
+  gs->restart = restart;
+  gs->method = method;
+  gs->counter = 0;
+  gs->active = 1;
+  gs->kdone = 0;
+  gs->breakdown = 0;
+  for (int q = 0; q < GM_MAXR + 2; ++q) gs->s[q] = 0.0;
+}
+
+__global__ void init_tol_kernel(GState* gs) {
+  // atol = max(tol ||b||, atol); ptol = ||M b|| min(1, atol / ||b||)
+  gs->atol = fmax(gs->tol * gs->bnorm, gs->atol_in);
+  gs->ptol = gs->mbnorm * fmin(1.0, gs->atol / gs->bnorm);
+}
+
+__global__ void begin_cycle_kernel(GState* gs) {
+  const int R = gs->restart;
+  for (int q = threadIdx.x; q < R * (GM_MAXR + 1); q += blockDim.x) {
+    const int r = q / (GM_MAXR + 1), c = q % (GM_MAXR + 1);
+    gs->H[r][c] = (r == c) ? 1.0 : 0.0;  // eye(restart, restart + 1)
+  }
+  for (int q = threadIdx.x; q <= R; q += blockDim.x) gs->beta[q] = 0.0;
+  for (int q = threadIdx.x; q < R; q += blockDim.x) { gs->givens[q][0] = 0.0; gs->givens[q][1] = 0.0; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    gs->beta[0] = gs->rnorm;
+    gs->err = gs->rnorm;
+    gs->active = 1;
+    gs->kdone = 0;
+    gs->breakdown = 0;
+  }
+}
+
+// y from the cycle's small problem; coef_i = y_i s_i.
+__global__ void small_solve_kernel(GState* gs) {
+  extern __shared__ double a2[];  // R * R
+  const int R = gs->restart;
+  __shared__ double b2[GM_MAXR];
+  __shared__ double y[GM_MAXR];
+  if (gs->method == 0) {
+    // _lstsq(H.T, beta): normal equations (H H^T) y = H beta, Cholesky solve
+    for (int q = threadIdx.x; q < R * R; q += blockDim.x) {
+      const int p = q / R, r = q % R;
+      double s = 0.0;
+      for (int c = 0; c <= R; ++c) s += gs->H[p][c] * gs->H[r][c];
+      a2[q] = s;
+    }
+    for (int p = threadIdx.x; p < R; p += blockDim.x) {
+      double s = 0.0;
+      for (int c = 0; c <= R; ++c) s += gs->H[p][c] * gs->beta[c];
+      b2[p] = s;
+    }
+    __syncthreads();
+    // right-looking Cholesky, lower factor stored in a2
+    for (int k = 0; k < R; ++k) {
+      if (threadIdx.x == 0) a2[k * R + k] = sqrt(a2[k * R + k]);
+      __syncthreads();
+      const double dkk = a2[k * R + k];
+      for (int i = k + 1 + threadIdx.x; i < R; i += blockDim.x) a2[i * R + k] /= dkk;
+      __syncthreads();
+      for (int q = threadIdx.x; q < (R - k - 1) * (R - k - 1); q += blockDim.x) {
+        const int i = k + 1 + q / (R - k - 1), jj = k + 1 + q % (R - k - 1);
+        if (jj <= i) a2[i * R + jj] -= a2[i * R + k] * a2[jj * R + k];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < R; ++i) {  // L z = b2
+        double s = b2[i];
+        for (int k = 0; k < i; ++k) s -= a2[i * R + k] * y[k];
+        y[i] = s / a2[i * R + i];
+      }
+      for (int i = R - 1; i >= 0; --i) {  // L^T y = z
+        double s = y[i];
+        for (int k = i + 1; k < R; ++k) s -= a2[k * R + i] * y[k];
+        y[i] = s / a2[i * R + i];
+      }
+      for (int i = 0; i < R; ++i) gs->coef[i] = y[i] * gs->s[i];
+    }
+  } else {
+    if (threadIdx.x == 0) {
+      // back substitution with the rotated rows: sum_j R[j][i] y_j = beta_i
+      const int kd = gs->kdone;
+      for (int i = kd - 1; i >= 0; --i) {
+        double s = gs->beta[i];
+        for (int jj = i + 1; jj < kd; ++jj) s -= gs->H[jj][i] * y[jj];
+        y[i] = s / gs->H[i][i];
+      }
+      for (int i = 0; i < R; ++i) gs->coef[i] = (i < kd) ? y[i] * gs->s[i] : 0.0;
+    }
+  }
+}
+
+__global__ void snapshot_kernel(const GState* gs, GHostView* v) {
+  v->rnorm = gs->rnorm;
+  v->atol = gs->atol;
+  v->bnorm = gs->bnorm;
+  v->kdone = gs->kdone;
+}
+
+int flat_grid(size_t n, int elems_per_block) {
+  size_t b = (n + elems_per_block - 1) / elems_per_block;
+  if (b > (size_t)GM_MAXBLOCKS) b = GM_MAXBLOCKS;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host wrappers
+// ---------------------------------------------------------------------------
+template <typename T>
+void gm_dots(const T* Vb, size_t stride, int m, const T* w, size_t n, double* partial, GState* gs, int mode,
+             int gated, cudaStream_t st) {
+  constexpr int E = CH * V16<T>::n;
+  const int g = flat_grid(n, GT * E);
+  dots_kernel<T><<<g, GT, (m + 1) * sizeof(double), st>>>(Vb, stride, m, w, n, partial, gs, mode, gated);
+}
+
+template <typename T>
+void gm_update(const T* Vb, size_t stride, int m, T* w, size_t n, double sign, double* partial, GState* gs,
+               int mode, int gated, int limit_kdone, cudaStream_t st) {
+  constexpr int E = CH * V16<T>::n;
+  const int g = flat_grid(n, GT * E);
+  update_kernel<T><<<g, GT, 0, st>>>(Vb, stride, m, w, n, sign, partial, gs, mode, gated, limit_kdone);
+}
+
+void gm_setup(GState* gs, double eps, double tol, double atol_in, int restart, int method, cudaStream_t st) {
+  setup_kernel<<<1, 1, 0, st>>>(gs, eps, tol, atol_in, restart, method);
+}
+void gm_init_tol(GState* gs, cudaStream_t st) { init_tol_kernel<<<1, 1, 0, st>>>(gs); }
+void gm_begin_cycle(GState* gs, cudaStream_t st) { begin_cycle_kernel<<<1, 256, 0, st>>>(gs); }
+void gm_small_solve(GState* gs, int restart, cudaStream_t st) {
+  const size_t smem = (size_t)restart * restart * sizeof(double);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(small_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         GM_MAXR * GM_MAXR * (int)sizeof(double));
+    attr_set = true;
+  }
+  small_solve_kernel<<<1, 256, smem, st>>>(gs);
+}
+void gm_snapshot(const GState* gs, GHostView* v, cudaStream_t st) { snapshot_kernel<<<1, 1, 0, st>>>(gs, v); }
+
+template void gm_dots<float>(const float*, size_t, int, const float*, size_t, double*, GState*, int, int,
+                             cudaStream_t);
+template void gm_dots<double>(const double*, size_t, int, const double*, size_t, double*, GState*, int, int,
+                              cudaStream_t);
+template void gm_update<float>(const float*, size_t, int, float*, size_t, double, double*, GState*, int, int,
+                               int, cudaStream_t);
+template void gm_update<double>(const double*, size_t, int, double*, size_t, double, double*, GState*, int,
+                                int, int, cudaStream_t);
+
+}  // namespace sisl

@@ -1,0 +1,185 @@
+"""``Euler3D`` with the B200 kernels behind its numerical methods.
+
+Mirrors ``suetes/regional3d/euler.py:13-439``.  The background state
+(``theta_bg``, ``pi_bg``, ``tau_damp``; euler.py:56-121) is built once in
+float64 on the grid's device.  ``precompute_bg`` returns the reference's
+dictionary (for user scripts); the kernels themselves read the coefficient
+set that ``sisl_core_create`` derives once per (precision, dt, alpha).
+"""
+
+import ctypes
+import math
+
+import torch
+
+from . import _lib
+from ._lib import check, ptrs
+from .core import F64, Core, empty_field, fortran
+from .operators import CGridOperator3D
+
+
+def jnp_interp(x, xp, fp):
+    """``jnp.interp`` with clamped ends (euler.py:82), float64 set-up."""
+    n = xp.shape[0]
+    i = torch.clamp(torch.searchsorted(xp, x.reshape(-1).contiguous(), right=True), 1, n - 1).reshape(x.shape)
+    dxx = xp[i] - xp[i - 1]
+    tiny = torch.finfo(F64).eps * 2.0 ** -52
+    dx0 = dxx.abs() <= tiny
+    f = torch.where(dx0, fp[i - 1], fp[i - 1] + ((x - xp[i - 1]) / torch.where(dx0, torch.ones_like(dxx), dxx))
+                    * (fp[i] - fp[i - 1]))
+    f = torch.where(x < xp[0], fp[0], f)
+    return torch.where(x > xp[-1], fp[-1], f)
+
+
+class Euler3D:
+    """Dry non-hydrostatic Euler core: background state plus operators."""
+
+    def __init__(self, grid, operators, constants, dt, initial_era5_state=None, N_bv=0.01,
+                 damp_height=20000.0, max_damp=0.5, nu_div_factor=0.8, nu_h_factor=0.1,
+                 physics_suite=None, interior_mask=None):
+        if physics_suite is not None:
+            raise NotImplementedError("physics suites are not part of the B200 SISL path")
+        self.grid, self.op, self.c, self.dt = grid, operators, dict(constants), float(dt)
+        self.nu_div = nu_div_factor * grid.dx ** 2 / (4.0 * dt)   # euler.py:62-67
+        self.nu_h = nu_h_factor * grid.dx ** 4 / (64.0 * dt)
+        self.physics_suite, self.interior_mask = None, interior_mask
+        g, cp = self.c["g"], self.c["cp"]
+        dev = grid.device
+        Z_m = grid.Z_m
+        if initial_era5_state is not None:  # euler.py:76-85
+            z_1d = Z_m.mean(dim=(0, 1))
+            th = torch.as_tensor(initial_era5_state["th_v"]).to(device=dev, dtype=F64)
+            pi = torch.as_tensor(initial_era5_state["pi"]).to(device=dev, dtype=F64)
+            self.theta_bg = jnp_interp(Z_m, z_1d, th.mean(dim=(0, 1)))
+            pi_top = pi[:, :, -1].mean()
+        else:  # euler.py:86-96
+            self.theta_0 = 300.0
+            self.theta_bg = (self.theta_0 * torch.exp((N_bv ** 2 / g) * Z_m) if N_bv > 0.0
+                             else self.theta_0 * torch.ones_like(Z_m))
+            z_max = Z_m.max()
+            if N_bv > 0.0:
+                pi_top = 1.0 + (g ** 2 / (cp * self.theta_0 * N_bv ** 2)) * (torch.exp(-N_bv ** 2 * z_max / g) - 1.0)
+            else:
+                pi_top = 1.0 - (g / (cp * self.theta_0)) * z_max
+        dz = Z_m[:, :, 1:] - Z_m[:, :, :-1]  # euler.py:100-112
+        thw = 0.5 * (self.theta_bg[:, :, 1:] + self.theta_bg[:, :, :-1])
+        dpi = -(g * dz) / (cp * thw)
+        rev = torch.flip(torch.cumsum(torch.flip(dpi, dims=[-1]), dim=-1), dims=[-1])
+        top = torch.full((grid.nx, grid.ny, 1), float(pi_top), dtype=F64, device=dev)
+        self.pi_bg = torch.cat([top - rev, top], dim=2)
+        zw = grid.Z_w  # euler.py:114-121
+        self.tau_damp = torch.where(
+            zw > damp_height,
+            max_damp * 0.5 * (1.0 + torch.tanh(math.pi * (zw - damp_height) / (grid.Lz - damp_height) - math.pi / 2)),
+            torch.zeros_like(zw))
+        self._cores = {}
+
+    # ------------------------------------------------------------------
+    def core(self, dtype, dt=None, alpha=0.55, bg=None, solver=None, use_limiter=False):
+        """The CUDA core for a precision, time step, off-centring and background."""
+        dt = self.dt if dt is None else float(dt)
+        theta, pi = (self.theta_bg, self.pi_bg) if bg is None else (bg["th_v"], bg["pi_bg"])
+        key = (dtype, dt, float(alpha), id(theta), id(pi), bool(use_limiter))
+        core = self._cores.get(key)
+        if core is None:
+            core = Core(self.grid, self.c, theta, pi, self.tau_damp, dtype, dt, alpha, self.nu_div, self.nu_h,
+                        periodic_axes=self.op.periodic_axes, solver=solver, use_limiter=use_limiter)
+            self._cores[key] = (core, theta, pi)  # keep the background alive while cached
+            return core
+        return core[0]
+
+    def bg_state_ref(self):
+        """Background dict built inside ``step`` (steppers.py:769-774)."""
+        c = self.c
+        rho = c["p0"] / (c["Rd"] * self.theta_bg) * self.pi_bg ** (c["cvd"] / c["Rd"])
+        return {"rho": rho, "pi": self.pi_bg, "th_v": self.theta_bg}
+
+    def precompute_bg(self, bg_state):
+        """``precompute_bg`` (euler.py:127-160): face-mapped background (float64)."""
+        op, g = self.op, self.grid
+        th, rho, pi = (torch.as_tensor(bg_state[k]).to(device=g.device, dtype=F64) for k in ("th_v", "rho", "pi"))
+        if bg_state.get("th_v") is self.theta_bg and bg_state.get("pi") is self.pi_bg:
+            th, pi = self.theta_bg, self.pi_bg
+        return {
+            "th_v_u": op.avg(th, 0, "m", "u"), "th_v_v": op.avg(th, 1, "m", "v"), "th_v_w": op.avg(th, 2, "m", "w"),
+            "rho_u": op.avg(rho, 0, "m", "u"), "rho_v": op.avg(rho, 1, "m", "v"), "rho_w": op.avg(rho, 2, "m", "w"),
+            "dz_m_full": g.dz_m_full, "dz_w_full": g.dz_w_full,
+            "dz_u": op.avg(g.dz_m_full, 0, "m", "u"), "dz_v": op.avg(g.dz_m_full, 1, "m", "v"),
+            "C_pi": (self.c["Rd"] / self.c["cvd"]) * (pi / (rho * th)), "pi_bg": pi, "th_v": th,
+        }
+
+    def _bg_arg(self, bg):
+        if bg is None or (bg.get("th_v") is self.theta_bg and bg.get("pi_bg") is self.pi_bg):
+            return None
+        if torch.equal(bg["th_v"], self.theta_bg) and torch.equal(bg["pi_bg"], self.pi_bg):
+            return None
+        return bg
+
+    @staticmethod
+    def _dtype_of(d):
+        for v in d.values():
+            if torch.is_tensor(v) and v.is_floating_point():
+                return v.dtype
+        return F64
+
+    # ------------------------------------------------------------------
+    def linear_operator(self, state_prime, bg, dt, alpha=0.55):
+        """Helmholtz operator ``x - alpha dt T_lin(x)`` (euler.py:374-439)."""
+        dtype = self._dtype_of(state_prime)
+        core = self.core(dtype, dt, alpha, bg=self._bg_arg(bg))
+        locs = (("u", "u"), ("v", "v"), ("w", "w"), ("pi", "m"), ("eta_dot", "w"))
+        ins = [core.field(state_prime[k], l) for k, l in locs]
+        outs = [core.new(l) for _, l in locs]
+        ws, n = core.workspace(_lib.WS_OPERATOR)
+        check(core.lib.sisl_linear_operator(core.handle, ptrs(ins, 5), ptrs(outs, 5), ws.data_ptr(), n, core.stream),
+              "sisl_linear_operator")
+        return {k: o for (k, _), o in zip(locs, outs)}
+
+    def _tendencies(self, state_prime, th_prime, bg, is_explicit):
+        dtype = self._dtype_of(state_prime)
+        core = self.core(dtype, self.dt, 0.55, bg=self._bg_arg(bg))
+        ins = [core.field(state_prime["u"], "u"), core.field(state_prime["v"], "v"),
+               core.field(state_prime["w"], "w"), core.field(state_prime["pi"], "m"),
+               core.field(state_prime["eta_dot"], "w"), core.field(th_prime, "m")]
+        outs = [core.new("u"), core.new("v"), core.new("w"), core.new("m"), core.new("m"), core.new("m")]
+        pd = [core.new("u"), core.new("v"), core.new("w"), core.new("m")]
+        for t in pd:
+            t.zero_()
+        pd_arr = ptrs(pd, 4)
+        ws, n = core.workspace(_lib.WS_EXPLICIT)
+        check(core.lib.sisl_tendencies(core.handle, int(is_explicit), ptrs(ins, 6), ptrs(outs, 6),
+                                       ctypes.cast(pd_arr, ctypes.c_void_p), ws.data_ptr(), n, core.stream),
+              "sisl_tendencies")
+        return outs, pd
+
+    def get_tendencies(self, state_prime, bg, is_explicit=False, ml_params=None):
+        """Tendencies of euler.py:208-372.  The theta perturbation is taken
+        from ``state_prime['th_v'] - bg['th_v']`` (or ``th_v_prime_m``); its
+        face averages are formed by the kernel."""
+        g = self.grid
+        if is_explicit:
+            if "th_v" in state_prime:
+                thp = fortran(state_prime["th_v"], dtype=F64) - fortran(bg["th_v"], dtype=F64)
+            elif "th_v_prime_m" in state_prime:
+                thp = state_prime["th_v_prime_m"]
+            else:
+                thp = torch.zeros(g.shape, dtype=F64, device=g.device)
+        else:
+            thp = torch.zeros(g.shape, dtype=F64, device=g.device)
+        thp = thp.to(self._dtype_of(state_prime))
+        (tu, tv, tw, tpi, tth, _), pd = self._tendencies(state_prime, thp, bg, is_explicit)
+        out = {"u": tu, "v": tv, "w": tw, "pi": tpi, "th_v": tth}
+        if is_explicit:
+            use = self.nu_h > 0.0 or self.nu_div > 0.0
+            out.update({"phys_diff_u": pd[0] if use else 0.0, "phys_diff_v": pd[1] if use else 0.0,
+                        "phys_diff_w": pd[2] if use else 0.0, "phys_diff_th_v": pd[3] if use else 0.0})
+        return out
+
+    def nonlinear_pi_tendency(self, state_prime, th_v_prime, bg):
+        """theta'-flux part of Exner continuity (euler.py:162-186)."""
+        sp = dict(state_prime)
+        sp.setdefault("w", torch.zeros(self.grid.shape_of("w"), dtype=self._dtype_of(state_prime),
+                                       device=self.grid.device))
+        sp.setdefault("pi", torch.zeros(self.grid.shape, dtype=self._dtype_of(state_prime), device=self.grid.device))
+        (_, _, _, _, _, nl), _ = self._tendencies(sp, th_v_prime, bg, True)
+        return nl

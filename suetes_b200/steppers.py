@@ -1,0 +1,373 @@
+"""SISL stepper and solvers on the B200 kernels.
+
+Mirrors ``suetes/regional3d/steppers.py``: ``build_dynamical_core``
+(:12-88, SISL branch), ``VerticalPreconditioner`` (:125-253),
+``SemiLagrangianAdvector3D`` (:256-374), ``SemiImplicitSolver3D``
+(:377-527), ``FluxFormAdvector`` (:530-647) and ``SISLStepper3D``
+(:650-1073).  Every numerical method calls the C ABI of
+``libsisl_b200.so``; a whole step is one ``sisl_step`` call.
+
+Precision follows the state: float32 tensors run the float32 kernels (with
+float64 GMRES reductions and Hessenberg algebra), float64 tensors the
+float64 kernels.  The thermodynamic fields are carried in perturbation form
+(``pi - pi_bg``, ``th_v - theta_bg``) between steps.
+"""
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import check, ptrs
+from .boundaries import LateralRelaxation
+from .core import F32, F64, empty_field, fortran, zeros_field
+from .euler import Euler3D
+
+SOLVE_METHODS = {"batched": _lib.SISL_GMRES_BATCHED, "incremental": _lib.SISL_GMRES_INCREMENTAL}
+LOC5 = (("u", "u"), ("v", "v"), ("w", "w"), ("pi", "m"), ("eta_dot", "w"))
+
+
+def build_dynamical_core(core_type, grid, operators, constants, initial_state, physics_suite=None,
+                         interior_mask=None, **kwargs):
+    """SISL branch of the factory (steppers.py:12-88)."""
+    if core_type.lower() != "sisl":
+        raise ValueError(f"Unknown core_type: '{core_type}'. The B200 path implements 'sisl'.")
+    params = {"dt": 120.0, "damp_height": 9000.0, "max_damp": 3.0, "nu_div_factor": 0.1, "nu_h_factor": 0.1,
+              "N_bv": 0.01, "alpha": 0.55, "use_limiter": False, "use_checkpointing": False,
+              "solver_tol": 1e-12, "solver_maxiter": 100, "solver_restart": 100, "background_state": None,
+              "solve_method": "batched"}
+    params.update(kwargs)
+    ref = params["background_state"] if params["background_state"] is not None else initial_state
+    physics = Euler3D(grid, operators, constants, dt=params["dt"], initial_era5_state=ref,
+                      damp_height=params["damp_height"], max_damp=params["max_damp"],
+                      nu_div_factor=params["nu_div_factor"], nu_h_factor=params["nu_h_factor"],
+                      N_bv=params["N_bv"], physics_suite=physics_suite, interior_mask=interior_mask)
+    if "u_prev" not in initial_state:  # steppers.py:69-80
+        initial_state["u_prev"] = initial_state["u"]
+        initial_state["v_prev"] = initial_state["v"]
+        initial_state["w_prev"] = initial_state["w"]
+        initial_state["eta_dot_prev"] = initial_state.get("eta_dot", torch.zeros_like(initial_state["w"]))
+        initial_state["tend_th_v_prev"] = torch.zeros_like(initial_state["th_v"])
+        initial_state["is_first_step"] = 1.0
+    stepper = SISLStepper3D(physics, params["dt"], alpha=params["alpha"], use_limiter=params["use_limiter"],
+                            use_checkpointing=params["use_checkpointing"], solver_tol=params["solver_tol"],
+                            solver_maxiter=params["solver_maxiter"], solver_restart=params["solver_restart"],
+                            solve_method=params["solve_method"])
+    return stepper, params["dt"]
+
+
+def _dtype_of(d):
+    for v in d.values():
+        if torch.is_tensor(v) and v.is_floating_point():
+            return v.dtype
+    return F64
+
+
+class VerticalPreconditioner:
+    """Column Helmholtz preconditioner M^-1 (steppers.py:125-253)."""
+
+    def __init__(self, physics, dt, alpha=0.55, pi_scale=1000.0):
+        if pi_scale != 1000.0:
+            raise ValueError("the CUDA preconditioner uses pi_scale = 1000")
+        self.physics, self.dt, self.alpha, self.pi_scale = physics, dt, alpha, pi_scale
+        self.bg = None
+
+    def precompute_banded(self, bg):
+        """The banded factorisation is prepared by the core (sisl_core_create)."""
+        self.bg = bg
+
+    def __call__(self, rhs_scaled):
+        core = self.physics.core(_dtype_of(rhs_scaled), self.dt, self.alpha, bg=self.physics._bg_arg(self.bg))
+        ins = [core.field(rhs_scaled[k], l) for k, l in LOC5]
+        outs = [core.new(l) for _, l in LOC5]
+        check(core.lib.sisl_precond_apply(core.handle, ptrs(ins, 5), ptrs(outs, 5), core.stream),
+              "sisl_precond_apply")
+        return {k: o for (k, _), o in zip(LOC5, outs)}
+
+
+class SemiLagrangianAdvector3D:
+    """Trajectories and SL interpolation (steppers.py:256-374)."""
+
+    def __init__(self, grid, physics, dt):
+        self.grid, self.physics, self.dt, self.op = grid, physics, dt, physics.op
+
+    def compute_departure_indices(self, state, loc="m", iterations=2):
+        """Midpoint departure points in index space (steppers.py:318-360);
+        returns a (3, ex, ey, ez) tensor."""
+        dtype = _dtype_of({k: state[k] for k in ("u", "v", "eta_dot")})
+        core = self.physics.core(dtype, self.dt, 0.55)
+        u, v, e = core.field(state["u"], "u"), core.field(state["v"], "v"), core.field(state["eta_dot"], "w")
+        co = [core.new(loc) for _ in range(3)]
+        ws, n = core.workspace(_lib.WS_DEPARTURE)
+        check(core.lib.sisl_departure(core.handle, _lib.LOC[loc], u.data_ptr(), v.data_ptr(), e.data_ptr(),
+                                      int(iterations), ptrs(co, 3), ws.data_ptr(), n, core.stream),
+              "sisl_departure")
+        return torch.stack(co, dim=0)
+
+    def advect_linear(self, field, coords):
+        from .operators import map_coordinates_linear
+        return map_coordinates_linear(field, coords)
+
+    def advect_cubic(self, field, coords, use_limiter=False):
+        from .operators import tensor_product_interp_3d
+        return tensor_product_interp_3d(field, coords, use_limiter=use_limiter)
+
+
+class SemiImplicitSolver3D:
+    """Preconditioned GMRES Helmholtz solve (steppers.py:377-527)."""
+
+    def __init__(self, physics, dt, alpha=0.55, solver_tol=1e-4, solver_maxiter=20, solver_restart=20,
+                 solve_method="batched"):
+        self.physics, self.dt, self.alpha = physics, dt, alpha
+        self.pi_scale = 1000.0
+        self.solver_tol, self.solver_maxiter, self.solver_restart = solver_tol, solver_maxiter, solver_restart
+        self.solve_method = solve_method
+        self.last_info = None
+
+    def _core(self, dtype, bg=None):
+        core = self.physics.core(dtype, self.dt, self.alpha, bg=self.physics._bg_arg(bg))
+        core.set_solver(self.solver_tol, self.solver_maxiter, self.solver_restart, SOLVE_METHODS[self.solve_method])
+        return core
+
+    def solve(self, rhs_prime, bg_precomputed, x0=None):
+        """Solve A x = b (steppers.py:401-496); x0 None means x0 = rhs."""
+        core = self._core(_dtype_of(rhs_prime), bg_precomputed)
+        b = [core.field(rhs_prime[k], l) for k, l in LOC5]
+        x = [core.new(l) for _, l in LOC5]
+        x0p, x0t = None, None
+        if x0 is not None:
+            x0t = [core.field(x0[k], l) for k, l in LOC5]  # keep alive across the call
+            x0p = ctypes.cast(ptrs(x0t, 5), ctypes.c_void_p)
+        ws, n = core.workspace(_lib.WS_GMRES)
+        info = _lib.SislSolveInfo()
+        check(core.lib.sisl_gmres_solve(core.handle, ptrs(b, 5), x0p, ptrs(x, 5), ws.data_ptr(), n, core.stream,
+                                        ctypes.byref(info)), "sisl_gmres_solve")
+        self.last_info = info.as_dict()
+        return {k: t for (k, _), t in zip(LOC5, x)}
+
+    def relative_residual(self, solution, rhs_prime, bg_precomputed):
+        """``||A x - b|| / ||b||`` in the scaled norm (steppers.py:498-527)."""
+        applied = self.physics.linear_operator(solution, bg_precomputed, self.dt, alpha=self.alpha)
+        num = torch.zeros((), dtype=F64, device=self.physics.grid.device)
+        den = torch.zeros_like(num)
+        for k, _ in LOC5:
+            s = self.pi_scale if k == "pi" else 1.0
+            a = applied[k].double() * s
+            r = fortran(rhs_prime[k]).double() * s
+            num = num + torch.sum((a - r) ** 2)
+            den = den + torch.sum(r ** 2)
+        return torch.sqrt(num / torch.clamp(den, min=torch.finfo(F64).tiny))
+
+
+class FluxFormAdvector:
+    """Split flux-form SL mass transport (steppers.py:530-647)."""
+
+    def __init__(self, grid, dt, periodic_axes=(), physics=None):
+        self.grid, self.dt, self.periodic_axes, self.physics = grid, dt, frozenset(periodic_axes), physics
+
+    def advect_1d(self, scalar_1d, cfl_inter_1d, periodic=False):
+        """advect_1d (steppers.py:552-594) for one line or a batch (..., N)."""
+        s = torch.as_tensor(scalar_1d)
+        c = torch.as_tensor(cfl_inter_1d).to(device=s.device, dtype=s.dtype)
+        N = s.shape[-1]
+        sb = s.reshape(-1, N).contiguous()
+        cb = c.reshape(-1, N + 1).contiguous()
+        out = torch.empty_like(sb)
+        lib = _lib.load()
+        n = int(lib.sisl_ffsl_lines_workspace_bytes(N, sb.shape[0]))
+        ws = torch.empty(max(n, 256), dtype=torch.uint8, device=s.device)
+        from .core import DTYPE_CODE, stream_ptr
+        check(lib.sisl_ffsl_lines(DTYPE_CODE[s.dtype], N, sb.shape[0], sb.data_ptr(), cb.data_ptr(),
+                                  int(bool(periodic)), out.data_ptr(), ws.data_ptr(), n, stream_ptr(s.device)),
+              "sisl_ffsl_lines")
+        return out.reshape(s.shape)
+
+    def advect_3d_split(self, field, state, bg_precomputed):
+        if self.physics is None:
+            raise RuntimeError("FluxFormAdvector needs the Euler3D physics for its metric coefficients")
+        core = self.physics.core(field.dtype, self.dt, 0.55)
+        f = core.field(field, "m")
+        u, v, e = core.field(state["u"], "u"), core.field(state["v"], "v"), core.field(state["eta_dot"], "w")
+        out = core.new("m")
+        ws, n = core.workspace(5)
+        check(core.lib.sisl_ffsl_advect(core.handle, f.data_ptr(), u.data_ptr(), v.data_ptr(), e.data_ptr(),
+                                        out.data_ptr(), ws.data_ptr(), n, core.stream), "sisl_ffsl_advect")
+        return out
+
+
+class DeviceState:
+    """Prognostic state + history on the device, perturbation form."""
+
+    FIELDS = (("u", "u"), ("v", "v"), ("w", "w"), ("eta_dot", "w"), ("pi_p", "m"), ("th_p", "m"), ("rho", "m"),
+              ("u_prev", "u"), ("v_prev", "v"), ("w_prev", "w"), ("eta_dot_prev", "w"), ("tend_th_prev", "m"))
+
+    def __init__(self, core, tensors=None, is_first_step=1.0):
+        self.core = core
+        self.t = {}
+        for k, loc in self.FIELDS:
+            self.t[k] = tensors[k] if tensors is not None and k in tensors else empty_field(
+                core.shape(loc), core.dtype, core.device)
+        self.is_first_step = float(is_first_step)
+
+    def c_struct(self):
+        s = _lib.SislState()
+        for k, _ in self.FIELDS:
+            setattr(s, k, self.t[k].data_ptr())
+        s.is_first_step = self.is_first_step
+        return s
+
+
+class SISLStepper3D:
+    """One SISL timestep (steppers.py:650-1073) as one ``sisl_step`` call."""
+
+    def __init__(self, physics, dt, alpha=0.55, use_limiter=False, use_checkpointing=False, solver_tol=1e-4,
+                 solver_maxiter=20, solver_restart=20, solve_method="batched"):
+        self.physics, self.dt, self.alpha = physics, dt, alpha
+        self.use_limiter = use_limiter
+        self.use_checkpointing = use_checkpointing
+        self.advector = SemiLagrangianAdvector3D(physics.grid, physics, dt)
+        self.ffsl_advector = FluxFormAdvector(physics.grid, dt, periodic_axes=physics.op.periodic_axes,
+                                              physics=physics)
+        self.implicit_solver = SemiImplicitSolver3D(physics, dt, alpha=alpha, solver_tol=solver_tol,
+                                                    solver_maxiter=solver_maxiter, solver_restart=solver_restart,
+                                                    solve_method=solve_method)
+        self.tracer_keys = []
+        self.last_info = None
+
+    # ------------------------------------------------------------------
+    def core(self, dtype):
+        s = self.implicit_solver
+        c = self.physics.core(dtype, self.dt, self.alpha, use_limiter=self.use_limiter)
+        c.set_solver(s.solver_tol, s.solver_maxiter, s.solver_restart, SOLVE_METHODS[s.solve_method])
+        return c
+
+    def to_device_state(self, state, dtype=None):
+        """Reference state dict (full pi, th_v) -> DeviceState (perturbations)."""
+        cached = state.get("_sisl_state")
+        if cached is not None and state.get("pi") is cached[1] and state.get("th_v") is cached[2]:
+            return cached[0]
+        dtype = dtype or _dtype_of({k: state[k] for k in ("u", "v", "w")})
+        core = self.core(dtype)
+        ph = self.physics
+        f = core.field
+        t = {"u": f(state["u"], "u"), "v": f(state["v"], "v"), "w": f(state["w"], "w")}
+        eta = state.get("eta_dot")
+        t["eta_dot"] = f(eta, "w") if eta is not None else zeros_field(core.shape("w"), dtype, core.device)
+        t["pi_p"] = fortran(torch.as_tensor(state["pi"]).to(core.device, F64) - ph.pi_bg, dtype=dtype)
+        t["th_p"] = fortran(torch.as_tensor(state["th_v"]).to(core.device, F64) - ph.theta_bg, dtype=dtype)
+        t["rho"] = f(state["rho"], "m") if "rho" in state else empty_field(core.shape("m"), dtype, core.device)
+        first = float(state.get("is_first_step", 1.0))
+        if "u_prev" in state:
+            t["u_prev"], t["v_prev"] = f(state["u_prev"], "u"), f(state["v_prev"], "v")
+            t["w_prev"], t["eta_dot_prev"] = f(state["w_prev"], "w"), f(state["eta_dot_prev"], "w")
+            t["tend_th_prev"] = f(state["tend_th_v_prev"], "m")
+        else:
+            first = 1.0
+            t["u_prev"], t["v_prev"], t["w_prev"], t["eta_dot_prev"] = t["u"], t["v"], t["w"], t["eta_dot"]
+            t["tend_th_prev"] = zeros_field(core.shape("m"), dtype, core.device)
+        return DeviceState(core, t, first)
+
+    def from_device_state(self, ds):
+        ph = self.physics
+        t = ds.t
+        dt_ = ds.core.dtype
+        out = {"u": t["u"], "v": t["v"], "w": t["w"], "eta_dot": t["eta_dot"], "rho": t["rho"],
+               "pi": fortran(t["pi_p"].double() + ph.pi_bg, dtype=dt_),
+               "th_v": fortran(t["th_p"].double() + ph.theta_bg, dtype=dt_),
+               "u_prev": t["u_prev"], "v_prev": t["v_prev"], "w_prev": t["w_prev"],
+               "eta_dot_prev": t["eta_dot_prev"], "tend_th_v_prev": t["tend_th_prev"],
+               "is_first_step": ds.is_first_step}
+        out["_sisl_state"] = (ds, out["pi"], out["th_v"])
+        return out
+
+    def step_device(self, ds_in, ds_out, relax=None):
+        """Advance ds_in by one step into ds_out (no aliasing between them,
+        except ds_out history fields that equal ds_in prognostic fields)."""
+        core = ds_in.core
+        sin, sout = ds_in.c_struct(), ds_out.c_struct()
+        rl = relax.c_struct(core) if relax is not None else None
+        ws, n = core.workspace(_lib.WS_STEP)
+        info = _lib.SislStepInfo()
+        rc = check(core.lib.sisl_step(core.handle, ctypes.byref(sin), ctypes.byref(sout),
+                                      ctypes.byref(rl) if rl is not None else None, ws.data_ptr(), n, core.stream,
+                                      ctypes.byref(info)), "sisl_step")
+        ds_out.is_first_step = 0.0
+        self.last_info = {"status": rc, "solves": [info.solve[0].as_dict(), info.solve[1].as_dict()],
+                          "kernel_launches": int(info.kernel_launches)}
+        return self.last_info
+
+    def _relax_of(self, bc_fn):
+        if bc_fn is None or isinstance(bc_fn, LateralRelaxation):
+            return bc_fn, None
+        return None, bc_fn
+
+    def step(self, state, t, forcing, bc_fn, ml_params=None):
+        """SISLStepper3D.step (steppers.py:720-1073)."""
+        ds = self.to_device_state(state)
+        out = DeviceState(ds.core)
+        # history of the new state aliases the old prognostic fields (steppers.py:1061-1064)
+        for k in ("u", "v", "w", "eta_dot"):
+            out.t[k + "_prev"] = ds.t[k]
+        relax, generic = self._relax_of(bc_fn)
+        self.step_device(ds, out, relax)
+        res = self.from_device_state(out)
+        if generic is not None:
+            res = self._apply_generic_bc(res, generic, forcing, out)
+        return res
+
+    def _apply_generic_bc(self, res, bc_fn, forcing, ds):
+        """A user bc_fn runs on the assembled state; the EOS of
+        steppers.py:1055-1056 is then recomputed if it changed anything."""
+        before = {k: res[k] for k in ("u", "v", "w", "pi", "th_v", "eta_dot")}
+        res2 = bc_fn(res, forcing)
+        if all(res2.get(k) is before[k] for k in before):
+            return res2
+        core = ds.core
+        ph = self.physics
+        f = core.field
+        ds.t["u"], ds.t["v"], ds.t["w"] = f(res2["u"], "u"), f(res2["v"], "v"), f(res2["w"], "w")
+        ds.t["eta_dot"] = f(res2["eta_dot"], "w")
+        ds.t["pi_p"] = fortran(torch.as_tensor(res2["pi"]).to(core.device, F64) - ph.pi_bg, dtype=core.dtype)
+        ds.t["th_p"] = fortran(torch.as_tensor(res2["th_v"]).to(core.device, F64) - ph.theta_bg, dtype=core.dtype)
+        check(core.lib.sisl_eos(core.handle, ds.t["th_p"].data_ptr(), ds.t["pi_p"].data_ptr(),
+                                ds.t["rho"].data_ptr(), core.stream), "sisl_eos")
+        out = self.from_device_state(ds)
+        for k, v in res2.items():
+            if k not in out:
+                out[k] = v
+        return out
+
+    def integrate(self, state, t_start, num_steps, forcing, bc_fn):
+        """lax.scan over ``step`` (steppers.py:692-714), device resident."""
+        relax, generic = self._relax_of(bc_fn)
+        if generic is not None:
+            for n in range(num_steps):
+                state = self.step(state, t_start + n * self.dt, forcing, bc_fn)
+            return state
+        cur = self.to_device_state(state)
+        ring = StateRing(cur.core)
+        for _ in range(num_steps):
+            nxt = ring.next_output(cur)
+            self.step_device(cur, nxt, relax)
+            cur = nxt
+        return self.from_device_state(cur)
+
+
+class StateRing:
+    """Three rotating output buffer sets for repeated steps.
+
+    The output of a step may not overlap its input, and the input's history
+    fields alias the previous state's prognostic buffers, so the output of
+    step n can reuse the buffers of step n - 3."""
+
+    def __init__(self, core):
+        self.core = core
+        self.sets = [DeviceState(core) for _ in range(3)]
+        self.n = 0
+
+    def next_output(self, cur):
+        out = self.sets[self.n % 3]
+        self.n += 1
+        for k in ("u", "v", "w", "eta_dot"):
+            out.t[k + "_prev"] = cur.t[k]
+        return out

@@ -1,0 +1,67 @@
+"""The C ABI library loads here (no GPU needed), exports every function
+declared in include/sisl_b200.h, and the ctypes structs match the C layout."""
+
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "sisl_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sisl_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from suetes_b200 import _lib
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(_lib.PROTOTYPES), set(names) ^ set(_lib.PROTOTYPES)
+
+
+def test_status_strings_and_version():
+    from suetes_b200 import _lib
+    lib = _lib.load()
+    assert lib.sisl_version() >= 1
+    assert _lib.status_string(0) == "ok"
+    assert "argument" in _lib.status_string(-1)
+
+
+def test_struct_layout_matches_header(tmp_path):
+    import ctypes
+    from suetes_b200 import _lib
+    src = tmp_path / "sz.c"
+    src.write_text('#include "sisl_b200.h"\n#include <stdio.h>\n#include <stddef.h>\n'
+                   'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(SislGrid), sizeof(SislParams),'
+                   ' sizeof(SislBackground), sizeof(SislSolveInfo), sizeof(SislState), sizeof(SislRelaxation),'
+                   ' sizeof(SislStepInfo), offsetof(SislParams, solver_maxiter)); return 0;}\n')
+    exe = tmp_path / "sz"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = [int(x) for x in subprocess.check_output([str(exe)]).split()]
+    want = [ctypes.sizeof(c) for c in (_lib.SislGrid, _lib.SislParams, _lib.SislBackground, _lib.SislSolveInfo,
+                                       _lib.SislState, _lib.SislRelaxation, _lib.SislStepInfo)]
+    want.append(_lib.SislParams.solver_maxiter.offset)
+    assert got == want
+
+
+def test_argument_validation_without_gpu():
+    """Invalid descriptors are rejected before any CUDA call."""
+    import ctypes
+    from suetes_b200 import _lib
+    lib = _lib.load()
+    g = _lib.SislGrid(1, 4, 4, 0, 0, _lib.SISL_F32, 1.0, 1.0, 1.0)  # nx < 2
+    p = _lib.SislParams()
+    p.solver_restart = 10
+    b = _lib.SislBackground()
+    h = ctypes.c_void_p()
+    assert lib.sisl_core_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(b), None, ctypes.byref(h)) == -1
+    assert lib.sisl_step(None, None, None, None, None, 0, None, None) == -1
+    assert lib.sisl_field_elems(ctypes.byref(_lib.SislGrid(4, 5, 6, 0, 0, 0, 1.0, 1.0, 1.0)), 1) == 5 * 5 * 6
