@@ -1,0 +1,393 @@
+#!/usr/bin/env python3
+"""SISL cell-steps/s on the B200.
+
+Workload: the 3-D mountain-wave configuration (256 x 256 x 80, dx = dy = 500 m,
+stretched SLEVE levels to 20 km, cos^2 ridge of 250 m, U = 10 m/s,
+N = 0.01 1/s, dt = 8 s, GMRES restart 30 / maxiter 30, x relaxation zone),
+synthetic analytic initial state.  One "step" is one SISLStepper3D.step.
+
+Default run (one JSON line on rank 0):
+  value   float32 kernels, state resident in HBM, cell-steps/s (whole job)
+  e2e     the same through the public API SISLStepper3D.step() with the
+          state in pinned host memory, host<->device copies of every state
+          field inside the timed region
+  fp64    the same kernels in float64 and the float32-vs-float64 field error
+  roofline  the dominant GMRES kernel class, timed with CUDA events on its
+          launching stream inside the timed region
+  cpu_baseline  the float64 CPU oracle on a bounded window of the workload
+
+``--impl reference`` times the CPU restatement of the reference SISL core
+(float64, all host threads) on the same workload (rank 0 only).
+"""
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import torch  # noqa: E402
+
+FALLBACK_HBM_GBS = 6650.0
+CELLS_NOTE = "cell-steps/s = nx*ny*nz*steps/time (benchmarks/performance/cpu_gpu_short_scaling/run.py:166)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--ny", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=80)
+    ap.add_argument("--tol32", type=float, default=1e-6, help="GMRES tolerance of the float32 path")
+    ap.add_argument("--tol64", type=float, default=1e-8, help="GMRES tolerance of the float64 path")
+    ap.add_argument("--method", default="batched", choices=["batched", "incremental"])
+    ap.add_argument("--roofline-class", default="update",
+                    choices=["matvec", "precond", "dots", "update"])
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-window", type=int, default=32, help="nx = ny of the CPU-baseline window")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle on a window of the workload (baseline / reference arm)
+# ---------------------------------------------------------------------------
+def oracle_mountain_wave(nx, ny, nz, tol):
+    from oracle.euler import Euler3D
+    from oracle.grid import RegionalGrid3D, StretchedSleveSimple
+    from oracle.ops import CGridOperator3D
+    from oracle.steppers import build_dynamical_core
+
+    C = {"g": 9.81, "cp": 1004.0, "Rd": 287.0, "cvd": 717.0, "p0": 100000.0}
+    ridge = lambda x, y: 250.0 * torch.exp(-(x / 5000.0) ** 2) * torch.cos(math.pi * x / 4000.0) ** 2 + 0.0 * y
+    g = RegionalGrid3D(nx, ny, nz, 500.0, 500.0, 20000.0 / nz, 45.0, 0.0, h_func=ridge,
+                       transform=StretchedSleveSimple(2.5, 4000.0, 1.35))
+    op = CGridOperator3D(g)
+    bgp = Euler3D(g, op, C, dt=8.0, N_bv=0.01)
+    rho = C["p0"] / (C["Rd"] * bgp.theta_bg) * bgp.pi_bg ** (C["cvd"] / C["Rd"])
+    z = lambda *s: torch.zeros(*s, dtype=torch.float64)
+    st = {"u": z(nx + 1, ny, nz) + 10.0, "v": z(nx, ny + 1, nz), "w": z(nx, ny, nz + 1), "eta_dot": z(nx, ny, nz + 1),
+          "pi": bgp.pi_bg.clone(), "rho": rho, "th_v": bgp.theta_bg.clone()}
+    stepper, _ = build_dynamical_core("sisl", g, op, C, st, dt=8.0, alpha=0.5, nu_div_factor=0.0, nu_h_factor=0.0,
+                                      damp_height=12000.0, max_damp=0.5, N_bv=0.01, solver_tol=tol,
+                                      solver_maxiter=30, solver_restart=30)
+    n = round(4000.0 / g.dx)
+    i = torch.arange(nx, dtype=torch.float64)
+    d = torch.minimum(i, nx - 1 - i)
+    mask = torch.where(d < n, torch.cos(0.5 * math.pi * d / n) ** 2, torch.zeros_like(d))[:, None, None]
+    ph = stepper.physics
+
+    def bc(s, forcing):  # schaer_mountain_3d/run.py:111-126
+        out = dict(s)
+        for k in ("u", "v", "th_v", "pi", "rho"):
+            m = torch.cat([mask, mask[-1:]], dim=0) if k == "u" else mask
+            ext = {"u": torch.full_like(s["u"], 10.0), "v": torch.zeros_like(s["v"]), "th_v": ph.theta_bg,
+                   "pi": ph.pi_bg, "rho": ph.bg_state_ref()["rho"]}[k]
+            out[k] = (1.0 - m) * s[k] + m * ext
+        return out
+
+    return stepper, st, bc
+
+
+def cpu_leg(steps, warmup, window, nz, tol):
+    """Time the CPU oracle: each step is one full SISL step of a window x
+    window x nz sample of the mountain-wave workload."""
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    stepper, st, bc = oracle_mountain_wave(window, window, nz, tol)
+    for n in range(warmup):
+        st = stepper.step(st, n * 8.0, None, bc)
+    times = []
+    for n in range(steps):
+        t0 = time.perf_counter()
+        st = stepper.step(st, n * 8.0, None, bc)
+        times.append(time.perf_counter() - t0)
+    cells = window * window * nz
+    sample = (f"{steps} SISL step(s) (after {warmup} warm-up) of a {window}x{window}x{nz} window of the "
+              f"mountain-wave workload (same spacing, terrain, dt, GMRES restart 30 / tol {tol:g}), float64, "
+              f"oracle restatement of the reference JAX core (JAX not installed)")
+    return cells * steps / sum(times), threads, sample, sum(times) / steps
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    value, threads, sample, sec = cpu_leg(args.steps, args.warmup, args.cpu_window, args.nz, args.tol64)
+    line = {"metric": "SISL cell-steps/s fwd (mountain wave 256x256x80)", "value": value, "unit": "cell-steps/s",
+            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"mountain wave {args.nx}x{args.ny}x{args.nz}, dt 8 s, restart 30",
+                       "sample_window": f"{args.cpu_window}x{args.cpu_window}x{args.nz}"},
+            "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def timed_device_steps(stepper, ds0, relax, steps, warmup, world, timing_class=None):
+    from suetes_b200 import StateRing
+    core = ds0.core
+    ring = StateRing(core)
+    cur = ds0
+    infos = []
+    for _ in range(warmup):
+        nxt = ring.next_output(cur)
+        stepper.step_device(cur, nxt, relax)
+        cur = nxt
+    if timing_class is not None:
+        core.timing_select(timing_class)
+    from suetes_b200.core import kernel_launches
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(steps):
+        nxt = ring.next_output(cur)
+        infos.append(stepper.step_device(cur, nxt, relax))
+        cur = nxt
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches = kernel_launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    kt = core.timing_read() if timing_class is not None else None
+    if timing_class is not None:
+        core.timing_select(0)
+    return ms, infos, launches, kt, cur
+
+
+def run_ours(args):
+    world, rank, local = dist_setup()
+    import suetes_b200 as sb
+    from suetes_b200 import _lib
+    from suetes_b200.workloads import mountain_wave
+
+    nx, ny, nz = args.nx, args.ny, args.nz
+    cells = nx * ny * nz
+    K, W = args.steps, max(args.warmup, 3)
+    cls = {"matvec": _lib.K_MATVEC, "precond": _lib.K_PRECOND, "dots": _lib.K_DOTS, "update": _lib.K_UPDATE}[
+        args.roofline_class]
+
+    # ---- float32 device-resident leg ----
+    st32, s32, bc = mountain_wave(nx, ny, nz, dtype=torch.float32, device=f"cuda:{local}", solver_tol=args.tol32,
+                                  solve_method=args.method)
+    ds = st32.to_device_state(s32)
+    with ClockSampler(local) as clk:
+        ms, infos, launches, kt, cur32 = timed_device_steps(st32, ds, bc, K, W, world, cls)
+    ms = dist_max(ms, world)
+    value = world * cells * K / (ms / 1e3)
+    solves = [s for i in infos for s in i["solves"]]
+    gm = {"solves": len(solves), "cycles_per_solve": sum(s["cycles"] for s in solves) / max(len(solves), 1),
+          "arnoldi_per_solve": sum(s["arnoldi_steps"] for s in solves) / max(len(solves), 1),
+          "converged_frac": sum(1 for s in solves if s["converged"]) / max(len(solves), 1),
+          "tol": args.tol32, "restart": 30, "maxiter": 30, "method": args.method}
+    peak, peak_kind = measured_peaks()
+    k_ms, k_n, k_bytes = kt
+    achieved = (k_bytes / k_n) / (k_ms / k_n / 1e3) / 1e9 if k_n else None
+    roofline = {"kernel": f"gmres_{args.roofline_class}", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "peak_kind": peak_kind, "launches_timed": k_n, "avg_launch_us": k_ms / max(k_n, 1) * 1e3,
+                "alg_bytes_per_launch": k_bytes / max(k_n, 1), "share_of_step": k_ms / ms}
+
+    line = {"metric": "SISL cell-steps/s fwd (mountain wave 256x256x80)", "value": value, "unit": "cell-steps/s",
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"mountain wave {nx}x{ny}x{nz}, dx 500 m, dt 8 s, SLEVE 20 km lid, "
+                                   f"GMRES restart 30 maxiter 30", "nx": nx, "ny": ny, "nz": nz,
+                       "parallelism": f"replicas x{world}", "l2": "working set > 126 MB L2 (no flush)",
+                       "gmres_tol_f32": args.tol32, "gmres_tol_f64": args.tol64},
+            "gmres": gm, "gpu_launches": launches, "clocks": clk.summary(), "roofline": roofline}
+
+    # ---- float64 leg and float32-vs-float64 error ----
+    if not args.no_fp64:
+        st64, s64, bc64 = mountain_wave(nx, ny, nz, dtype=torch.float64, device=f"cuda:{local}",
+                                        solver_tol=args.tol64, solve_method=args.method)
+        ds64 = st64.to_device_state(s64)
+        ms64, infos64, _, _, cur64 = timed_device_steps(st64, ds64, bc64, K, W, world)
+        ms64 = dist_max(ms64, world)
+        err = {}
+        for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p"):
+            a, b = cur32.t[k].double(), cur64.t[k]
+            den = float(torch.linalg.vector_norm(b))
+            err[k] = {"rel_l2": float(torch.linalg.vector_norm(a - b)) / max(den, 1e-300),
+                      "linf_rel": float((a - b).abs().max()) / max(float(b.abs().max()), 1e-300)}
+        solves64 = [s for i in infos64 for s in i["solves"]]
+        line["fp64"] = {"value": world * cells * K / (ms64 / 1e3), "ms_per_step": ms64 / K,
+                        "arnoldi_per_solve": sum(s["arnoldi_steps"] for s in solves64) / max(len(solves64), 1),
+                        "tol": args.tol64}
+        line["err_f32_vs_f64"] = {"after_steps": K + W, "fields": err}
+        del st64, ds64, cur64
+
+    # ---- end to end through the public API with host state ----
+    if not args.no_e2e:
+        host = {k: (v.detach().to("cpu").pin_memory() if torch.is_tensor(v) else v) for k, v in s32.items()}
+        keys = [k for k, v in host.items() if torch.is_tensor(v)]
+        h2d = sum(host[k].numel() * host[k].element_size() for k in keys)
+        out_host = None
+        e2e_steps = max(3, min(K, 10))
+        st = host
+        for n in range(2):  # warm-up of the host path
+            dev = {k: (v.to(f"cuda:{local}", non_blocking=True) if torch.is_tensor(v) else v) for k, v in st.items()}
+            res = st32.step(dev, 0.0, None, bc)
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        d2h = 0
+        for n in range(e2e_steps):
+            dev = {k: (v.to(f"cuda:{local}", non_blocking=True) if torch.is_tensor(v) else v) for k, v in st.items()}
+            res = st32.step(dev, n * 8.0, None, bc)
+            nxt = {}
+            d2h = 0
+            for k in keys:
+                t = res[k]
+                h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+                h.copy_(t, non_blocking=True)
+                nxt[k] = h
+                d2h += t.numel() * t.element_size()
+            nxt["is_first_step"] = 0.0
+            st = nxt
+        t1.record()
+        torch.cuda.synchronize()
+        e2e_ms = dist_max(t0.elapsed_time(t1), world)
+        line["e2e"] = {"value": world * cells * e2e_steps / (e2e_ms / 1e3), "unit": "cell-steps/s",
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                       "api": "SISLStepper3D.step(state in pinned host memory)"}
+
+    # ---- CPU baseline (rank 0, one GPU) ----
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, threads, sample, _ = cpu_leg(2, 1, args.cpu_window, nz, args.tol64)
+        line["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

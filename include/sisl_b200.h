@@ -205,12 +205,14 @@ int sisl_eos(SislCore* core, const void* th_p, const void* pi_p, void* rho, void
 int sisl_step(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
               size_t ws_bytes, void* stream, SislStepInfo* info);
 
-/* Instrumentation: number of kernels this library launched, and CUDA-event
- * timing of one kernel class (events recorded around each launch on the
- * launching stream; read after the stream is synchronised). */
+/* Instrumentation (no reference counterpart): number of kernels this library
+ * launched, and CUDA-event timing of one kernel class inside GMRES (events
+ * recorded around each launch on the launching stream; read after the
+ * stream is synchronised) with the algorithmic bytes those launches move
+ * (each distinct array touched once). */
 int64_t sisl_kernel_launches(void);
 int sisl_timing_select(SislCore* core, int kernel_class);
-int sisl_timing_read(SislCore* core, double* total_ms, int64_t* launches);
+int sisl_timing_read(SislCore* core, double* total_ms, int64_t* launches, double* alg_bytes);
 
 #ifdef __cplusplus
 }

@@ -101,7 +101,7 @@ PROTOTYPES = {
                                  ctypes.POINTER(SislStepInfo)]),
     "sisl_kernel_launches": (ctypes.c_int64, []),
     "sisl_timing_select": (ctypes.c_int, [vp, ctypes.c_int]),
-    "sisl_timing_read": (ctypes.c_int, [vp, c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "sisl_timing_read": (ctypes.c_int, [vp, c_double_p, ctypes.POINTER(ctypes.c_int64), c_double_p]),
 }
 
 _LIB = None

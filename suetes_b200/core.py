@@ -142,10 +142,13 @@ class Core:
         check(self.lib.sisl_timing_select(self.handle, int(kernel_class)), "sisl_timing_select")
 
     def timing_read(self):
+        """(total milliseconds, launches, algorithmic bytes) of the timed class."""
         ms = ctypes.c_double(0.0)
         n = ctypes.c_int64(0)
-        check(self.lib.sisl_timing_read(self.handle, ctypes.byref(ms), ctypes.byref(n)), "sisl_timing_read")
-        return ms.value, n.value
+        b = ctypes.c_double(0.0)
+        check(self.lib.sisl_timing_read(self.handle, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(b)),
+              "sisl_timing_read")
+        return ms.value, n.value, b.value
 
 
 LOCS5 = ("u", "v", "w", "m", "w")

@@ -28,6 +28,7 @@ struct SislCore {
   int timing_class = SISL_K_NONE;
   std::vector<cudaEvent_t> ev0, ev1;
   size_t ev_used = 0;
+  double timed_bytes = 0.0;  // algorithmic bytes of the timed launches
 };
 
 namespace {
@@ -42,9 +43,11 @@ struct KScope {
   SislCore* c;
   cudaStream_t st;
   bool timed;
-  KScope(SislCore* core, int cls, cudaStream_t s, int nkernels = 1) : c(core), st(s), timed(false) {
+  KScope(SislCore* core, int cls, cudaStream_t s, int nkernels = 1, double bytes = 0.0)
+      : c(core), st(s), timed(false) {
     g_launches += nkernels;
     if (c && c->timing_class == cls && cls != SISL_K_NONE) {
+      c->timed_bytes += bytes;
       if (c->ev_used == c->ev0.size()) {
         cudaEvent_t a, b;
         cudaEventCreate(&a);
@@ -238,6 +241,22 @@ CVec5<T> as_const(Vec5<T> v) {
   return r;
 }
 
+// Algorithmic bytes per launch (each distinct array touched once).
+double matvec_bytes(const Dims& d, size_t es) {
+  const double fu = field_size(d, LOC_U), fv = field_size(d, LOC_V), fw = field_size(d, LOC_W),
+               fm = field_size(d, LOC_M);
+  const double vec = fu + fv + 2 * fw + fm;
+  // 5 inputs + 5 outputs + coefficients thu zxu rdu | thv zev rdv | thw rhow idzw damp zxw zew | cpidz
+  return es * (2 * vec + 3 * fu + 3 * fv + 6 * fw + fm);
+}
+double precond_bytes(const Dims& d, size_t es) {
+  const double fu = field_size(d, LOC_U), fv = field_size(d, LOC_V), fw = field_size(d, LOC_W),
+               fm = field_size(d, LOC_M);
+  const double vec = fu + fv + 2 * fw + fm;
+  // 5 inputs + 5 outputs + lpi tlow tcp tinv | damp rhow thw idzw zxw zew
+  return es * (2 * vec + 4 * fm + 6 * fw);
+}
+
 // Restarted GMRES on the packed vectors g.bg (rhs) and g.xg (initial guess).
 template <typename T>
 int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, SislSolveInfo* info) {
@@ -248,6 +267,8 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
   const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
   GState* gs = g.gs;
   CVec5<T> none{};
+  const double es = sizeof(T), vb = es * (double)n;
+  const double mvb = matvec_bytes(d, sizeof(T)), pcb = precond_bytes(d, sizeof(T));
   {
     KScope k(c, SISL_K_OTHER, st);
     gm_setup(gs, eps, c->prm.solver_tol, c->prm.solver_atol, R, method, st);
@@ -302,19 +323,19 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
     }
     for (int j = 0; j < R; ++j) {
       {
-        KScope k(c, SISL_K_MATVEC, st);
+        KScope k(c, SISL_K_MATVEC, st, 1, mvb);
         launch_matvec<T>(d, cf, g.cview(g.V(j)), &gs->s[j], none, g.view(g.z()), &gs->active, st);
       }
       {
-        KScope k(c, SISL_K_PRECOND, st);
+        KScope k(c, SISL_K_PRECOND, st, 1, pcb);
         launch_precond<T>(d, cf, g.cview(g.z()), g.view(g.V(j + 1)), &gs->active, st);
       }
       {
-        KScope k(c, SISL_K_DOTS, st);
+        KScope k(c, SISL_K_DOTS, st, 1, vb * (j + 2));  // reads V_0..V_j and w
         gm_dots<T>(g.V(0), n, j + 1, g.V(j + 1), n, g.partial, gs, 0 /*PROJ*/, 1, st);
       }
       {
-        KScope k(c, SISL_K_UPDATE, st);
+        KScope k(c, SISL_K_UPDATE, st, 1, vb * (j + 3));  // reads V_0..V_j, reads and writes w
         gm_update<T>(g.V(0), n, j + 1, g.V(j + 1), n, -1.0, g.partial, gs, 1 /*ARNOLDI*/, 1, 0, st);
       }
     }
@@ -946,10 +967,11 @@ int sisl_timing_select(SislCore* c, int cls) {
   if (!c) return SISL_ERR_ARG;
   c->timing_class = cls;
   c->ev_used = 0;
+  c->timed_bytes = 0.0;
   return SISL_OK;
 }
 
-int sisl_timing_read(SislCore* c, double* total_ms, int64_t* launches) {
+int sisl_timing_read(SislCore* c, double* total_ms, int64_t* launches, double* alg_bytes) {
   if (!c) return SISL_ERR_ARG;
   double tot = 0.0;
   for (size_t q = 0; q < c->ev_used; ++q) {
@@ -960,6 +982,7 @@ int sisl_timing_read(SislCore* c, double* total_ms, int64_t* launches) {
   }
   if (total_ms) *total_ms = tot;
   if (launches) *launches = (int64_t)c->ev_used;
+  if (alg_bytes) *alg_bytes = c->timed_bytes;
   return SISL_OK;
 }
 

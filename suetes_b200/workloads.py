@@ -1,0 +1,74 @@
+"""Synthetic workloads of the SISL benchmarks, built on the CUDA package.
+
+* ``mountain_wave``: 3-D mountain-wave flow (the 256x256x80 configuration):
+  dx = dy = 500 m, 80 levels over a 20 km lid with the stretched SLEVE
+  coordinate (kappa 2.5, s = 4 km, n = 1.35; transforms.py:54-86), the ridge
+  h(x) = 250 exp(-(x/5 km)^2) cos^2(pi x / 4 km) uniform in y
+  (schaer_mountain_3d/run.py:83-85), U = 10 m/s, N = 0.01 1/s, dt = 8 s,
+  alpha 0.5, sponge from 12 km, x relaxation over 4 km
+  (schaer_mountain_3d/run.py:103-136).  No dataset is involved: the case
+  is analytic.
+* ``rising_bubble``: 3-D dry warm bubble (64x64x48, 50 m, dt = 1 s,
+  cos^2 bubble of 2 K, r = 1 km, 1.5 km above ground;
+  cpu_gpu_short_scaling/run.py:38-55 in 3-D).
+"""
+
+import math
+
+import torch
+
+from .boundaries import x_relaxation
+from .core import F32, F64
+from .euler import Euler3D
+from .geometry import RegionalGrid3D, StretchedSleveSimple
+from .operators import CGridOperator3D
+from .steppers import build_dynamical_core
+
+CONSTANTS = {"g": 9.81, "cp": 1004.0, "Rd": 287.0, "cvd": 717.0, "p0": 100000.0}
+
+
+def ridge(x, y):
+    return 250.0 * torch.exp(-(x / 5000.0) ** 2) * torch.cos(math.pi * x / 4000.0) ** 2 + 0.0 * y
+
+
+def mountain_wave(nx=256, ny=256, nz=80, dtype=F32, device="cuda", solver_tol=1e-8, solver_maxiter=30,
+                  solver_restart=30, solve_method="batched", dt=8.0):
+    grid = RegionalGrid3D(nx, ny, nz, 500.0, 500.0, 20000.0 / nz, 45.0, 0.0, h_func=ridge,
+                          transform=StretchedSleveSimple(2.5, 4000.0, 1.35), device=device)
+    op = CGridOperator3D(grid)
+    bgp = Euler3D(grid, op, CONSTANTS, dt=dt, N_bv=0.01)
+    c = CONSTANTS
+    rho = c["p0"] / (c["Rd"] * bgp.theta_bg) * bgp.pi_bg ** (c["cvd"] / c["Rd"])
+    z = lambda *s: torch.zeros(*s, dtype=F64, device=grid.device)
+    state = {"u": z(nx + 1, ny, nz) + 10.0, "v": z(nx, ny + 1, nz), "w": z(nx, ny, nz + 1),
+             "eta_dot": z(nx, ny, nz + 1), "pi": bgp.pi_bg.clone(), "rho": rho, "th_v": bgp.theta_bg.clone()}
+    stepper, _ = build_dynamical_core("sisl", grid, op, c, state, dt=dt, alpha=0.5, nu_div_factor=0.0,
+                                      nu_h_factor=0.0, damp_height=12000.0, max_damp=0.5, N_bv=0.01,
+                                      solver_tol=solver_tol, solver_maxiter=solver_maxiter,
+                                      solver_restart=solver_restart, solve_method=solve_method)
+    for k in ("u", "v", "w", "eta_dot", "u_prev", "v_prev", "w_prev", "eta_dot_prev", "tend_th_v_prev", "rho"):
+        state[k] = state[k].to(dtype)
+    bc = x_relaxation(grid, 4000.0, 10.0)
+    return stepper, state, bc
+
+
+def rising_bubble(nx=64, ny=64, nz=48, dx=50.0, amp=2.0, radius=1000.0, center=(0.0, 0.0, 1500.0), dtype=F64,
+                  device="cuda", solver_tol=1e-10, solver_maxiter=100, solver_restart=100, solve_method="batched",
+                  dt=1.0):
+    grid = RegionalGrid3D(nx, ny, nz, dx, dx, dx, 0.0, 0.0, device=device)
+    op = CGridOperator3D(grid)
+    bgp = Euler3D(grid, op, CONSTANTS, dt=dt, N_bv=0.0)
+    c = CONSTANTS
+    X, Y, Zc = torch.meshgrid(grid.x_m, grid.y_m, grid.z_m, indexing="ij")
+    r = torch.sqrt((X - center[0]) ** 2 + (Y - center[1]) ** 2 + (Zc - center[2]) ** 2)
+    th = bgp.theta_bg + torch.where(r < radius, amp * torch.cos(0.5 * math.pi * r / radius) ** 2, torch.zeros_like(r))
+    rho = c["p0"] / (c["Rd"] * th) * bgp.pi_bg ** (c["cvd"] / c["Rd"])
+    z = lambda *s: torch.zeros(*s, dtype=F64, device=grid.device)
+    state = {"u": z(nx + 1, ny, nz), "v": z(nx, ny + 1, nz), "w": z(nx, ny, nz + 1), "eta_dot": z(nx, ny, nz + 1),
+             "pi": bgp.pi_bg.clone(), "th_v": th, "rho": rho}
+    stepper, _ = build_dynamical_core("sisl", grid, op, c, state, dt=dt, N_bv=0.0, nu_div_factor=0.0,
+                                      nu_h_factor=0.0, solver_tol=solver_tol, solver_maxiter=solver_maxiter,
+                                      solver_restart=solver_restart, solve_method=solve_method)
+    for k in ("u", "v", "w", "eta_dot", "u_prev", "v_prev", "w_prev", "eta_dot_prev", "tend_th_v_prev", "rho"):
+        state[k] = state[k].to(dtype)
+    return stepper, state, None
