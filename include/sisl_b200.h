@@ -61,6 +61,7 @@ enum {
 #define SISL_ERR_CUDA (-2)
 #define SISL_ERR_WORKSPACE (-3)
 #define SISL_ERR_NONFINITE (-4)
+#define SISL_ERR_SCRATCH_LIMIT (-5)
 
 /* Grid extents and spacing: RegionalGrid3D(nx, ny, nz, dx, dy, dz, ...)
  * (geometry.py:141) plus CGridOperator3D's periodic axes (operators.py:16). */
@@ -181,6 +182,21 @@ int sisl_trilinear(int dtype, const int32_t src_shape[3], const void* field, con
 size_t sisl_ffsl_lines_workspace_bytes(int n, int nlines);
 int sisl_ffsl_lines(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic, void* out,
                     void* ws, size_t ws_bytes, void* stream);
+/* Allocation-free sisl_ffsl_lines; no counterpart in the reference.
+ * For callers that cannot call cudaMalloc while they run: a stream in
+ * global-mode graph capture, a host model that allots this library only
+ * buffers pre-sized from its own pool, an FFI handler registered without a
+ * workspace.  The float64 scratch is a fixed device array of
+ * SISL_FFSL_NOALLOC_MAX_DOUBLES doubles (8 MiB), held by every GPU that loads
+ * the library until exit; a call needs (n + 1) * nlines doubles of it and
+ * returns SISL_ERR_SCRATCH_LIMIT above that.  Nothing is allocated.  The
+ * first call on a device looks up the array's device address (with that
+ * device current), so make it before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+#define SISL_FFSL_NOALLOC_MAX_DOUBLES (1 << 20)
+int sisl_ffsl_lines_noalloc(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic,
+                            void* out, void* stream);
 /* Euler3D.get_tendencies(state_prime, bg, is_explicit) (euler.py:208-372):
  * is_explicit = 0 gives the linear tendencies of the implicit operator.
  * Same arguments as sisl_explicit_tendencies. */

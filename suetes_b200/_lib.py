@@ -18,6 +18,8 @@ WS_STEP, WS_GMRES, WS_DEPARTURE, WS_EXPLICIT, WS_OPERATOR = 0, 1, 2, 3, 4
 RELAX_U, RELAX_V, RELAX_W, RELAX_TH, RELAX_PI = 1, 2, 4, 8, 16
 K_NONE, K_MATVEC, K_PRECOND, K_DOTS, K_UPDATE, K_SL, K_EXPLICIT, K_OTHER = range(8)
 SISL_OK, SISL_NOT_CONVERGED = 0, 1
+SISL_ERR_SCRATCH_LIMIT = -5
+FFSL_NOALLOC_MAX_DOUBLES = 1 << 20
 
 c_double_p = ctypes.POINTER(ctypes.c_double)
 vp = ctypes.c_void_p
@@ -94,6 +96,8 @@ PROTOTYPES = {
     "sisl_ffsl_lines_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
     "sisl_ffsl_lines": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp,
                                        ctypes.c_size_t, vp]),
+    "sisl_ffsl_lines_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int,
+                                               vp, vp]),
     "sisl_ffsl_advect": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "sisl_eos": (ctypes.c_int, [vp, vp, vp, vp, vp]),
     "sisl_step": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),

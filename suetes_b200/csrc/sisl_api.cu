@@ -594,6 +594,7 @@ const char* sisl_status_string(int s) {
     case SISL_ERR_CUDA: return "CUDA error";
     case SISL_ERR_WORKSPACE: return "workspace too small";
     case SISL_ERR_NONFINITE: return "non-finite residual";
+    case SISL_ERR_SCRATCH_LIMIT: return "problem exceeds the fixed scratch of the allocation-free entry point";
     default: return "unknown status";
   }
 }

@@ -10,6 +10,10 @@
 // evaluated in closed form: M_ext(p) = floor(p / N) S + M(p mod N).
 #include "sisl_core.cuh"
 
+#include <mutex>
+
+#include "../../include/sisl_b200.h"
+
 namespace sisl {
 namespace {
 
@@ -195,3 +199,64 @@ template void launch_eos<double>(const Dims&, const Coef<double>&, const double*
                                  cudaStream_t);
 
 }  // namespace sisl
+
+// ---------------------------------------------------------------------------
+// Allocation-free line transport.
+//
+// Some callers cannot call cudaMalloc while they advance a model: a stream
+// in global-mode graph capture (an allocation there breaks the capture), a
+// host model that hands this library only buffers it pre-sized from its own
+// pool and forbids allocation inside its time loop, or an FFI handler that
+// was registered without a workspace.  sisl_ffsl_lines_noalloc serves them:
+// the float64 cumulative-mass scratch of the line kernel lives in the fixed
+// device array below (SISL_FFSL_NOALLOC_MAX_DOUBLES doubles = 8 MiB, held on
+// every GPU that loads this library until the process exits).  In host code
+// the array's name is only a host-side stand-in, never a device address: the
+// address is fetched with cudaGetSymbolAddress once per device (the first
+// call on a device does it, with that device current) and cached.
+// ---------------------------------------------------------------------------
+namespace sisl {
+
+static __device__ __align__(256) double g_ffsl_line_scratch[SISL_FFSL_NOALLOC_MAX_DOUBLES];
+
+namespace {
+std::mutex g_scratch_mutex;
+constexpr int kMaxDevices = 64;
+double* g_scratch_device_address[kMaxDevices] = {nullptr};
+
+int line_scratch_address(double** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SISL_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (g_scratch_device_address[dev] == nullptr) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_ffsl_line_scratch) != cudaSuccess) return SISL_ERR_CUDA;
+    g_scratch_device_address[dev] = static_cast<double*>(p);
+  }
+  *out = g_scratch_device_address[dev];
+  return SISL_OK;
+}
+}  // namespace
+
+}  // namespace sisl
+
+extern "C" int sisl_ffsl_lines_noalloc(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic,
+                                       void* out, void* stream) {
+  using namespace sisl;
+  if (n < 1 || nlines < 1 || !scalar || !cfl || !out) return SISL_ERR_ARG;
+  if (dtype != SISL_F32 && dtype != SISL_F64) return SISL_ERR_ARG;
+  if ((size_t)(n + 1) * (size_t)nlines > (size_t)SISL_FFSL_NOALLOC_MAX_DOUBLES) return SISL_ERR_SCRATCH_LIMIT;
+  double* M = nullptr;
+  int rc = line_scratch_address(&M);
+  if (rc != SISL_OK) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Every scratch word a line reads is written by that line first, so the
+  // previous call's contents never need clearing.
+  if (dtype == SISL_F64)
+    launch_ffsl_lines<double>(n, nlines, (const double*)scalar, (const double*)cfl, (double*)out, M,
+                              periodic ? 1 : 0, st);
+  else
+    launch_ffsl_lines<float>(n, nlines, (const float*)scalar, (const float*)cfl, (float*)out, M, periodic ? 1 : 0,
+                             st);
+  return cudaGetLastError() == cudaSuccess ? SISL_OK : SISL_ERR_CUDA;
+}
