@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-window", type=int, default=32, help="nx = ny of the CPU-baseline window")
+    ap.add_argument("--classes", action="store_true",
+                    help="also time every GMRES kernel class separately (diagnostic)")
     return ap.parse_args()
 
 
@@ -330,6 +332,17 @@ def run_ours(args):
                         "tol": args.tol64}
         line["err_f32_vs_f64"] = {"after_steps": K + W, "fields": err}
         del st64, ds64, cur64
+
+    # ---- per-class GMRES kernel timing (diagnostic; advances the float32 state) ----
+    if args.classes:
+        per = {}
+        for name, kc in (("matvec", _lib.K_MATVEC), ("precond", _lib.K_PRECOND), ("dots", _lib.K_DOTS),
+                         ("update", _lib.K_UPDATE)):
+            msc, _, _, (cms, cn, cb), cur32 = timed_device_steps(st32, cur32, bc, 3, 0, world, kc)
+            per[name] = {"achieved_GBs": (cb / cms / 1e6) if cms else None, "launches": cn,
+                         "avg_launch_us": cms / max(cn, 1) * 1e3, "share_of_step": cms / msc,
+                         "frac_of_measured": (cb / cms / 1e6) / peak if cms else None}
+        line["roofline"]["classes"] = per
 
     # ---- end to end through the public API with host state ----
     if not args.no_e2e:

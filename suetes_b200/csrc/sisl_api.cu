@@ -193,6 +193,12 @@ struct GWork {
     for (int q = 0; q < 5; ++q) v.f[q] = b + off[q];
     return v;
   }
+  // u, v from vector a; w, pi, eta_dot from vector b
+  Vec5<T> split(T* a, T* b) const {
+    Vec5<T> v;
+    for (int q = 0; q < 5; ++q) v.f[q] = (q < 2 ? a : b) + off[q];
+    return v;
+  }
 };
 
 template <typename T>
@@ -253,8 +259,8 @@ double precond_bytes(const Dims& d, size_t es) {
   const double fu = field_size(d, LOC_U), fv = field_size(d, LOC_V), fw = field_size(d, LOC_W),
                fm = field_size(d, LOC_M);
   const double vec = fu + fv + 2 * fw + fm;
-  // 5 inputs + 5 outputs + lpi tlow tcp tinv | damp rhow thw idzw zxw zew
-  return es * (2 * vec + 4 * fm + 6 * fw);
+  // 5 inputs + 3 outputs (u, v alias the matvec output) + lpi tlow tcp tinv | damp rhow thw idzw zxw zew
+  return es * (vec + 2 * fw + fm + 4 * fm + 6 * fw);
 }
 
 // Restarted GMRES on the packed vectors g.bg (rhs) and g.xg (initial guess).
@@ -291,13 +297,14 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
   }
   // residual of the initial guess
   auto residual_and_read = [&](GHostView* out) -> int {
+    const Vec5<T> az = g.split(g.V(0), g.z());
     {
       KScope k(c, SISL_K_MATVEC, st);
-      launch_matvec<T>(d, cf, g.cview(g.xg()), nullptr, g.cview(g.bg()), g.view(g.z()), nullptr, st);
+      launch_matvec<T>(d, cf, g.cview(g.xg()), nullptr, g.cview(g.bg()), az, nullptr, st);
     }
     {
       KScope k(c, SISL_K_PRECOND, st);
-      launch_precond<T>(d, cf, g.cview(g.z()), g.view(g.V(0)), nullptr, st);
+      launch_precond<T>(d, cf, as_const(az), g.view(g.V(0)), nullptr, st);
     }
     {
       KScope k(c, SISL_K_DOTS, st);
@@ -322,13 +329,16 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
       gm_begin_cycle(gs, st);
     }
     for (int j = 0; j < R; ++j) {
+      // A writes its u, v rows straight into the next basis vector: the
+      // preconditioner passes u, v through unchanged (steppers.py:247-249)
+      const Vec5<T> az = g.split(g.V(j + 1), g.z());
       {
         KScope k(c, SISL_K_MATVEC, st, 1, mvb);
-        launch_matvec<T>(d, cf, g.cview(g.V(j)), &gs->s[j], none, g.view(g.z()), &gs->active, st);
+        launch_matvec<T>(d, cf, g.cview(g.V(j)), &gs->s[j], none, az, &gs->active, st);
       }
       {
         KScope k(c, SISL_K_PRECOND, st, 1, pcb);
-        launch_precond<T>(d, cf, g.cview(g.z()), g.view(g.V(j + 1)), &gs->active, st);
+        launch_precond<T>(d, cf, as_const(az), g.view(g.V(j + 1)), &gs->active, st);
       }
       {
         KScope k(c, SISL_K_DOTS, st, 1, vb * (j + 2));  // reads V_0..V_j and w

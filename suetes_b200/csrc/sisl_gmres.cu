@@ -69,26 +69,25 @@ __device__ __forceinline__ bool last_block(unsigned int* counter) {
 enum DotMode { DM_PROJ = 0, DM_BNORM = 1, DM_MBNORM = 2, DM_RNORM = 3 };
 
 // result_i = <V_i, w> for i < m and <w, w>; finished according to `mode`.
+// Each thread accumulates its products in its own shared-memory slots
+// acc[q * blockDim + tid] (float64), so consecutive basis vectors stream
+// without a reduction in between; the block reduces once at the end.
 template <typename T>
-__global__ void __launch_bounds__(GT) dots_kernel(const T* __restrict__ Vb, size_t stride, int m,
-                                                  const T* __restrict__ w, size_t n, double* partial,
-                                                  GState* gs, int mode, int gated) {
+__global__ void dots_kernel(const T* __restrict__ Vb, size_t stride, int m, const T* __restrict__ w, size_t n,
+                            double* partial, GState* gs, int mode, int gated) {
   if (gated && gs->active == 0) return;
-  extern __shared__ double acc[];  // m + 1
-  for (int q = threadIdx.x; q <= m; q += blockDim.x) acc[q] = 0.0;
-  __syncthreads();
+  extern __shared__ double acc[];  // (m + 1) * blockDim.x
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int q = 0; q <= m; ++q) acc[q * nt + tid] = 0.0;
   constexpr int VN = V16<T>::n;
   constexpr int E = CH * VN;
-  const size_t tile = (size_t)GT * E;
-  const int lane = threadIdx.x & 31;
+  const size_t tile = (size_t)nt * E;
   for (size_t base = (size_t)blockIdx.x * tile; base < n; base += (size_t)gridDim.x * tile) {
     T wr[E];
-    bool ok[CH];
 #pragma unroll
     for (int c = 0; c < CH; ++c) {
-      const size_t off = base + ((size_t)c * GT + threadIdx.x) * VN;
-      ok[c] = off < n;
-      if (ok[c]) load16(w + off, wr + c * VN);
+      const size_t off = base + ((size_t)c * nt + tid) * VN;
+      if (off < n) load16(w + off, wr + c * VN);
       else
 #pragma unroll
         for (int e = 0; e < VN; ++e) wr[c * VN + e] = T(0);
@@ -96,15 +95,40 @@ __global__ void __launch_bounds__(GT) dots_kernel(const T* __restrict__ Vb, size
     double sq = 0.0;
 #pragma unroll
     for (int e = 0; e < E; ++e) sq += (double)wr[e] * (double)wr[e];
-    sq = warp_sum(sq);
-    if (lane == 0) atomicAdd(&acc[m], sq);
-    for (int i = 0; i < m; ++i) {
+    acc[m * nt + tid] += sq;
+    // two basis vectors per iteration: both chunks are in flight together
+    int i = 0;
+    for (; i + 1 < m; i += 2) {
+      const T* __restrict__ Va = Vb + (size_t)i * stride;
+      const T* __restrict__ Vc = Va + stride;
+      T va[E], vc[E];
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        const size_t off = base + ((size_t)c * nt + tid) * VN;
+        if (off < n) {
+          load16(Va + off, va + c * VN);
+          load16(Vc + off, vc + c * VN);
+        } else {
+#pragma unroll
+          for (int e = 0; e < VN; ++e) { va[c * VN + e] = T(0); vc[c * VN + e] = T(0); }
+        }
+      }
+      double pa = 0.0, pc = 0.0;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        pa += (double)va[e] * (double)wr[e];
+        pc += (double)vc[e] * (double)wr[e];
+      }
+      acc[i * nt + tid] += pa;
+      acc[(i + 1) * nt + tid] += pc;
+    }
+    if (i < m) {
       const T* __restrict__ Vi = Vb + (size_t)i * stride;
       T vr[E];
 #pragma unroll
       for (int c = 0; c < CH; ++c) {
-        const size_t off = base + ((size_t)c * GT + threadIdx.x) * VN;
-        if (ok[c]) load16(Vi + off, vr + c * VN);
+        const size_t off = base + ((size_t)c * nt + tid) * VN;
+        if (off < n) load16(Vi + off, vr + c * VN);
         else
 #pragma unroll
           for (int e = 0; e < VN; ++e) vr[c * VN + e] = T(0);
@@ -112,22 +136,27 @@ __global__ void __launch_bounds__(GT) dots_kernel(const T* __restrict__ Vb, size
       double p = 0.0;
 #pragma unroll
       for (int e = 0; e < E; ++e) p += (double)vr[e] * (double)wr[e];
-      p = warp_sum(p);
-      if (lane == 0) atomicAdd(&acc[i], p);
+      acc[i * nt + tid] += p;
     }
   }
   __syncthreads();
-  double* mine = partial + (size_t)blockIdx.x * (GM_MAXR + 2);
-  for (int q = threadIdx.x; q <= m; q += blockDim.x) mine[q] = acc[q];
+  // block reduction: warp wp reduces the slots of q = wp, wp + nwarps, ...
+  const int lane = tid & 31, wp = tid >> 5, nw = nt >> 5;
+  for (int q = wp; q <= m; q += nw) {
+    double s_ = 0.0;
+    for (int t = lane; t < nt; t += 32) s_ += acc[q * nt + t];
+    s_ = warp_sum(s_);
+    if (lane == 0) partial[(size_t)blockIdx.x * (GM_MAXR + 2) + q] = s_;
+  }
   if (!last_block(&gs->counter)) return;
   // finish: sum the partials of all blocks
-  for (int q = threadIdx.x; q <= m; q += blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) s += partial[(size_t)b * (GM_MAXR + 2) + q];
-    acc[q] = s;
+  for (int q = tid; q <= m; q += nt) {
+    double s_ = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s_ += partial[(size_t)b * (GM_MAXR + 2) + q];
+    acc[q] = s_;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     gs->counter = 0;
     const double nrm = sqrt(acc[m]);
     if (mode == DM_PROJ) {
@@ -378,12 +407,24 @@ int flat_grid(size_t n, int elems_per_block) {
 // ---------------------------------------------------------------------------
 // host wrappers
 // ---------------------------------------------------------------------------
+// shared memory of the dots kernel: (m + 1) slots per thread, at most 96 KB
+constexpr size_t DOTS_SMEM_MAX = 96 * 1024;
+
 template <typename T>
 void gm_dots(const T* Vb, size_t stride, int m, const T* w, size_t n, double* partial, GState* gs, int mode,
              int gated, cudaStream_t st) {
+  static bool attr_set = false;  // per instantiation
+  if (!attr_set) {
+    cudaFuncSetAttribute(dots_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DOTS_SMEM_MAX);
+    attr_set = true;
+  }
+  int nt = (int)(DOTS_SMEM_MAX / ((size_t)(m + 1) * sizeof(double)));
+  nt = nt >= 256 ? 256 : (nt / 32) * 32;
+  if (nt < 32) nt = 32;
   constexpr int E = CH * V16<T>::n;
-  const int g = flat_grid(n, GT * E);
-  dots_kernel<T><<<g, GT, (m + 1) * sizeof(double), st>>>(Vb, stride, m, w, n, partial, gs, mode, gated);
+  const int g = flat_grid(n, nt * E);
+  dots_kernel<T><<<g, nt, (size_t)(m + 1) * nt * sizeof(double), st>>>(Vb, stride, m, w, n, partial, gs, mode,
+                                                                        gated);
 }
 
 template <typename T>
