@@ -259,8 +259,8 @@ double precond_bytes(const Dims& d, size_t es) {
   const double fu = field_size(d, LOC_U), fv = field_size(d, LOC_V), fw = field_size(d, LOC_W),
                fm = field_size(d, LOC_M);
   const double vec = fu + fv + 2 * fw + fm;
-  // 5 inputs + 3 outputs (u, v alias the matvec output) + lpi tlow tcp tinv | damp rhow thw idzw zxw zew
-  return es * (vec + 2 * fw + fm + 4 * fm + 6 * fw);
+  // 5 inputs + 3 outputs (u, v alias the matvec output) + lpi | damp rhow thw idzw zxw zew
+  return es * (vec + 2 * fw + fm + fm + 6 * fw);
 }
 
 // Restarted GMRES on the packed vectors g.bg (rhs) and g.xg (initial guess).
@@ -649,7 +649,7 @@ int sisl_core_create(const SislGrid* grid, const SislParams* prm, const SislBack
   Base64 b{bg->theta_bg, bg->pi_bg, bg->Z_m, bg->dz_m_full, bg->dz_w_full, bg->z_xi_w, bg->z_eta_w, bg->tau_damp,
            bg->m_m, bg->m_u, bg->m_v, bg->f_u, bg->f_v, bg->dm_dx_m, bg->dm_dy_m};
   cudaStream_t st = (cudaStream_t)stream;
-  g_launches += 2;
+  g_launches += 1;
   if (grid->dtype == SISL_F64) {
     PtrTable<double> t;
     for (int q = 0; q < C_COUNT; ++q) t.p[q] = (double*)c->coef_ptr[q];

@@ -30,9 +30,6 @@ struct Coef {
   const T *cpidz;  // C_pi / dz_m_full  (C_pi = Rd/cvd * pi/(rho theta), euler.py:157)
   const T *dthm;   // avg_w->m( d theta_bg/dz )  (euler.py:321-322)
   const T *lpi;    // alpha dt C_pi / dz_m  (steppers.py:180)
-  const T *tlow;   // Thomas: lower diagonal (steppers.py:183)
-  const T *tcp;    // Thomas: modified upper diagonal c'
-  const T *tinv;   // Thomas: inverse pivots
   const T *zxm, *zem;  // avg_u->m z_xi_u, avg_v->m z_eta_v (diffusion.py:117,125)
   const T *dzm;        // dz_m_full (geometry.py:242)
   // u faces
@@ -47,7 +44,7 @@ struct Coef {
 };
 
 enum CoefId {
-  C_THB, C_PIB, C_CPIDZ, C_DTHM, C_LPI, C_TLOW, C_TCP, C_TINV, C_ZXM, C_ZEM, C_DZM,
+  C_THB, C_PIB, C_CPIDZ, C_DTHM, C_LPI, C_ZXM, C_ZEM, C_DZM,
   C_THU, C_ZXU, C_RDU, C_THV, C_ZEV, C_RDV,
   C_THW, C_RHOW, C_IDZW, C_DZW, C_DAMP, C_ZXW, C_ZEW,
   C_MM, C_MU, C_MV, C_FU, C_FV, C_DMDX, C_DMDY,

@@ -36,6 +36,9 @@ __device__ __forceinline__ T gz_mass(const T* __restrict__ p, const T* __restric
   return T(0.5) * (g0 + g1);
 }
 
+// Branch-free load phase: every index is clamped into its array, all values
+// are loaded unconditionally (one memory round trip per thread), the five
+// rows are formed with selects, and only the stores are predicated.
 template <typename T>
 __global__ void __launch_bounds__(256) matvec_kernel(Dims d, Coef<T> c, CVec5<T> x, const double* xscale,
                                                      CVec5<T> b, Vec5<T> out, const int* active) {
@@ -49,111 +52,155 @@ __global__ void __launch_bounds__(256) matvec_kernel(Dims d, Coef<T> c, CVec5<T>
   const T adt = (T)(c.s.alpha * c.s.dt), cp = (T)c.s.cp, a = (T)c.s.alpha, ps = (T)c.s.ps;
   const T sp = xs / ps;
   const T idx = (T)(1.0 / d.dx), idy = (T)(1.0 / d.dy);
-  const int pm = nx * ny;
+  const int pm = nx * ny, pu = (nx + 1) * ny, pv = nx * (ny + 1);
   const T* __restrict__ xu = x.f[0];
   const T* __restrict__ xv = x.f[1];
   const T* __restrict__ xw = x.f[2];
   const T* __restrict__ xp = x.f[3];
   const T* __restrict__ xW = x.f[4];
+  // clamped coordinates: mass columns ic < nx, jc < ny; mass levels km < nz
+  const int ic = min(i, nx - 1), jc = min(j, ny - 1), km = min(k, nz - 1);
+  const int il = (ic == 0) ? nx - 1 : ic - 1;   // left column of face i (wraps when periodic)
+  const int jl = (jc == 0) ? ny - 1 : jc - 1;
+  const int hO = ic + nx * jc, hX = il + nx * jc, hY = ic + nx * jl;
+  const int iuc = min(i, nx);  // u face index (valid for u arrays)
+  const int jvc = min(j, ny);
+  // ---- loads (unconditional, in bounds) ----
+  const T gmO = gz_mass(xp, c.idzw, hO, km, nz, pm, sp);
+  const T gmX = gz_mass(xp, c.idzw, hX, km, nz, pm, sp);
+  const T gmY = gz_mass(xp, c.idzw, hY, km, nz, pm, sp);
+  const T PO = ld(xp, hO + km * pm) * sp, PX = ld(xp, hX + km * pm) * sp, PY = ld(xp, hY + km * pm) * sp;
+  const int pU = iuc + (nx + 1) * (jc + ny * km);        // u face (i, jc, km)
+  const int pV = ic + nx * (jvc + (ny + 1) * km);        // v face (ic, j, km)
+  const int uO = ic + (nx + 1) * (jc + ny * km);         // u face (ic, jc, km): own cell west face
+  const int uY = ic + (nx + 1) * (jl + ny * km);
+  const int vO = ic + nx * (jc + (ny + 1) * km);         // v face (ic, jc, km): own cell south face
+  const int vX = il + nx * (jc + (ny + 1) * km);
+  const T xu_f = ld(xu, pU), xv_f = ld(xv, pV);
+  const T thu = ld(c.thu, pU), zxu = ld(c.zxu, pU), thv = ld(c.thv, pV), zev = ld(c.zev, pV);
+  const T mu_f = ld(c.mu, iuc + (nx + 1) * jc), fu_f = ld(c.fu, iuc + (nx + 1) * jc);
+  const T mv_f = ld(c.mv, ic + nx * jvc), fv_f = ld(c.fv, ic + nx * jvc);
+  const T vX0 = ld(xv, vX), vX1 = ld(xv, vX + nx), vO0 = ld(xv, vO), vO1 = ld(xv, vO + nx);
+  const T uY0 = ld(xu, uY), uY1 = ld(xu, uY + 1), uO0 = ld(xu, uO), uO1 = ld(xu, uO + 1);
+  // w level k (clamped into the interior rows for the stencil loads)
+  const int kw = min(max(k, 1), nz - 1);
+  const int pw = hO + k * pm, pwi = hO + kw * pm;
+  const T xw_k = ld(xw, pw), xW_k = ld(xW, pw), idzw_k = ld(c.idzw, pw);
+  const T damp = ld(c.damp, pwi), thw = ld(c.thw, pwi), zxw = ld(c.zxw, pwi), zew = ld(c.zew, pwi);
+  const T Pw1 = ld(xp, hO + kw * pm) * sp, Pw0 = ld(xp, hO + (kw - 1) * pm) * sp;
+  const int uw1 = ic + (nx + 1) * (jc + ny * kw), uw0 = uw1 - pu;
+  const int vw1 = ic + nx * (jc + (ny + 1) * kw), vw0 = vw1 - pv;
+  const T uwa = ld(xu, uw0), uwb = ld(xu, uw0 + 1), uwc = ld(xu, uw1), uwd = ld(xu, uw1 + 1);
+  const T vwa = ld(xv, vw0), vwb = ld(xv, vw0 + nx), vwc = ld(xv, vw1), vwd = ld(xv, vw1 + nx);
+  const T mw = ld(c.mm, hO);
+  // pi row at mass level km
+  const int pmk = hO + km * pm;
+  const T rdu0 = ld(c.rdu, uO), rdu1 = ld(c.rdu, uO + 1), thu0 = ld(c.thu, uO), thu1 = ld(c.thu, uO + 1);
+  const T rdv0 = ld(c.rdv, vO), rdv1 = ld(c.rdv, vO + nx), thv0 = ld(c.thv, vO), thv1 = ld(c.thv, vO + nx);
+  const int pz0 = hO + km * pm, pz1 = hO + min(km + 1, nz - 1) * pm;
+  const T W0 = ld(xW, pz0), rw0 = ld(c.rhow, pz0), tw0 = ld(c.thw, pz0);
+  const T W1 = ld(xW, pz1), rw1 = ld(c.rhow, pz1), tw1 = ld(c.thw, pz1);
+  const T cpidz = ld(c.cpidz, pmk), xp_k = ld(xp, pmk);
+  // ---- rows ----
+  // u face (i, j, k): locked on an open boundary (euler.py:414-415)
+  const bool u_lock = !d.px && (i == 0 || i == nx);
+  const T vat = T(0.25) * (vX0 + vX1 + vO0 + vO1) * xs;
+  const T tend_u = -cp * thu * ((PO - PX) * idx * mu_f - zxu * T(0.5) * (gmX + gmO)) + fu_f * vat;
+  const T Lu = u_lock ? xu_f * xs : xu_f * xs - adt * tend_u;
+  const bool v_lock = !d.py && (j == 0 || j == ny);
+  const T uat = T(0.25) * (uY0 + uY1 + uO0 + uO1) * xs;
+  const T tend_v = -cp * thv * ((PO - PY) * idy * mv_f - zev * T(0.5) * (gmY + gmO)) - fv_f * uat;
+  const T Lv = v_lock ? xv_f * xs : xv_f * xs - adt * tend_v;
+  // w and eta_dot rows at w level k; identity rows on the ground and lid (euler.py:426-437)
+  const bool wb = (k == 0 || k == nz);
+  const T gzw = (Pw1 - Pw0) * idzw_k;
+  const T Lw = wb ? xw_k * xs : damp * xw_k * xs + adt * cp * thw * gzw;
+  const T uw = T(0.25) * (uwa + uwb + uwc + uwd) * xs, vw = T(0.25) * (vwa + vwb + vwc + vwd) * xs;
+  const T Le = wb ? xW_k * xs * idzw_k : a * (xW_k * xs + mw * (uw * zxw + vw * zew) - xw_k * xs);
+  // pi row (euler.py:298-318 through linear_operator)
+  const T fx0 = uO0 * rdu0 * thu0, fx1 = uO1 * rdu1 * thu1;
+  const T fy0 = vO0 * rdv0 * thv0, fy1 = vO1 * rdv1 * thv1;
+  const T fz0 = (km == 0) ? T(0) : W0 * rw0 * tw0;
+  const T fz1 = (km + 1 == nz) ? T(0) : W1 * rw1 * tw1;
+  const T divh = mw * mw * ((fx1 - fx0) * idx + (fy1 - fy0) * idy);
+  const T Lp = xp_k * xs + adt * ps * cpidz * (xs * (divh + (fz1 - fz0)));
+  // ---- stores ----
+  const bool do_u = (k < nz) && (j < ny) && !(d.px && i == nx);
+  const bool do_v = (k < nz) && (i < nx) && !(d.py && j == ny);
   const bool own = (i < nx && j < ny);
-  const int il = (i == 0) ? nx - 1 : i - 1;
-  const int jl = (j == 0) ? ny - 1 : j - 1;
-  const int hO = i + nx * j;  // own column (valid when own)
-  T gmO = T(0);
-  if (own && k < nz) gmO = gz_mass(xp, c.idzw, hO, k, nz, pm, sp);
-
-  if (k < nz) {
-    // ---- u face (i, j, k) ----
-    if (j < ny && !(d.px && i == nx)) {
-      const int p = iu(d, i, j, k);
-      T L;
-      if (!d.px && (i == 0 || i == nx)) {
-        L = ld(xu, p) * xs;  // locked open boundary (euler.py:414-415)
-      } else {
-        const int hX = il + nx * j;
-        const T gmX = gz_mass(xp, c.idzw, hX, k, nz, pm, sp);
-        const T gpx = (ld(xp, hO + k * pm) - ld(xp, hX + k * pm)) * sp * idx * ld(c.mu, h_u(d, i, j));
-        const int vr = iv(d, i, j, k), vl = iv(d, il, j, k);
-        const T vat = T(0.25) * (ld(xv, vl) + ld(xv, vl + nx) + ld(xv, vr) + ld(xv, vr + nx)) * xs;
-        const T tend = -cp * ld(c.thu, p) * (gpx - ld(c.zxu, p) * T(0.5) * (gmX + gmO)) + ld(c.fu, h_u(d, i, j)) * vat;
-        L = ld(xu, p) * xs - adt * tend;
-      }
-      out.f[0][p] = b.f[0] ? ld(b.f[0], p) - L : L;
-      if (d.px && i == 0) {
-        const int pn = iu(d, nx, j, k);
-        out.f[0][pn] = b.f[0] ? ld(b.f[0], pn) - L : L;
-      }
-    }
-    // ---- v face (i, j, k) ----
-    if (i < nx && !(d.py && j == ny)) {
-      const int p = iv(d, i, j, k);
-      T L;
-      if (!d.py && (j == 0 || j == ny)) {
-        L = ld(xv, p) * xs;
-      } else {
-        const int hY = i + nx * jl;
-        const T gmY = gz_mass(xp, c.idzw, hY, k, nz, pm, sp);
-        const T gpy = (ld(xp, hO + k * pm) - ld(xp, hY + k * pm)) * sp * idy * ld(c.mv, h_v(d, i, j));
-        const int ur = iu(d, i, j, k), ul = iu(d, i, jl, k);
-        const T uat = T(0.25) * (ld(xu, ul) + ld(xu, ul + 1) + ld(xu, ur) + ld(xu, ur + 1)) * xs;
-        const T tend = -cp * ld(c.thv, p) * (gpy - ld(c.zev, p) * T(0.5) * (gmY + gmO)) - ld(c.fv, h_v(d, i, j)) * uat;
-        L = ld(xv, p) * xs - adt * tend;
-      }
-      out.f[1][p] = b.f[1] ? ld(b.f[1], p) - L : L;
-      if (d.py && j == 0) {
-        const int pn = iv(d, i, ny, k);
-        out.f[1][pn] = b.f[1] ? ld(b.f[1], pn) - L : L;
-      }
+  if (do_u) {
+    const int p = iu(d, i, j, k);
+    out.f[0][p] = b.f[0] ? ld(b.f[0], p) - Lu : Lu;
+    if (d.px && i == 0) {  // duplicate periodic face (euler.py:412)
+      const int pn = iu(d, nx, j, k);
+      out.f[0][pn] = b.f[0] ? ld(b.f[0], pn) - Lu : Lu;
     }
   }
-  if (!own) return;
-  // ---- w level k: w and eta_dot rows ----
-  const int pw = hO + k * pm;
-  T Lw, Le;
-  if (k == 0 || k == nz) {
-    Lw = ld(xw, pw) * xs;                      // euler.py:426-427
-    Le = ld(xW, pw) * xs * ld(c.idzw, pw);     // eta_dot = W / dz_w (euler.py:436-437)
-  } else {
-    const T gzw = (ld(xp, hO + k * pm) - ld(xp, hO + (k - 1) * pm)) * sp * ld(c.idzw, pw);
-    Lw = ld(c.damp, pw) * ld(xw, pw) * xs + adt * cp * ld(c.thw, pw) * gzw;
-    const int u1 = iu(d, i, j, k), u0 = u1 - (nx + 1) * ny;
-    const int v1 = iv(d, i, j, k), v0 = v1 - nx * (ny + 1);
-    const T uw = T(0.25) * (ld(xu, u0) + ld(xu, u0 + 1) + ld(xu, u1) + ld(xu, u1 + 1)) * xs;
-    const T vw = T(0.25) * (ld(xv, v0) + ld(xv, v0 + nx) + ld(xv, v1) + ld(xv, v1 + nx)) * xs;
-    Le = a * (ld(xW, pw) * xs + ld(c.mm, hO) * (uw * ld(c.zxw, pw) + vw * ld(c.zew, pw)) - ld(xw, pw) * xs);
+  if (do_v) {
+    const int p = iv(d, i, j, k);
+    out.f[1][p] = b.f[1] ? ld(b.f[1], p) - Lv : Lv;
+    if (d.py && j == 0) {
+      const int pn = iv(d, i, ny, k);
+      out.f[1][pn] = b.f[1] ? ld(b.f[1], pn) - Lv : Lv;
+    }
   }
-  if (b.f[2]) { Lw = ld(b.f[2], pw) - Lw; Le = ld(b.f[4], pw) - Le; }
-  out.f[2][pw] = Lw;
-  out.f[4][pw] = Le;
-  if (k == nz) return;
-  // ---- mass point: pi row ----
-  const int u0 = iu(d, i, j, k), v0 = iv(d, i, j, k);
-  const T fx0 = ld(xu, u0) * ld(c.rdu, u0) * ld(c.thu, u0);
-  const T fx1 = ld(xu, u0 + 1) * ld(c.rdu, u0 + 1) * ld(c.thu, u0 + 1);
-  const T fy0 = ld(xv, v0) * ld(c.rdv, v0) * ld(c.thv, v0);
-  const T fy1 = ld(xv, v0 + nx) * ld(c.rdv, v0 + nx) * ld(c.thv, v0 + nx);
-  const T fz0 = (k == 0) ? T(0) : ld(xW, pw) * ld(c.rhow, pw) * ld(c.thw, pw);
-  const int pw1 = pw + pm;
-  const T fz1 = (k + 1 == nz) ? T(0) : ld(xW, pw1) * ld(c.rhow, pw1) * ld(c.thw, pw1);
-  const T m = ld(c.mm, hO);
-  const T divh = m * m * ((fx1 - fx0) * idx + (fy1 - fy0) * idy);
-  const T tend = -ld(c.cpidz, pw) * (xs * (divh + (fz1 - fz0)));
-  const T L = ld(xp, pw) * xs - adt * ps * tend;
-  out.f[3][pw] = b.f[3] ? ld(b.f[3], pw) - L : L;
+  if (own) {
+    out.f[2][pw] = b.f[2] ? ld(b.f[2], pw) - Lw : Lw;
+    out.f[4][pw] = b.f[4] ? ld(b.f[4], pw) - Le : Le;
+    if (k < nz) out.f[3][pw] = b.f[3] ? ld(b.f[3], pw) - Lp : Lp;
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Column-tile preconditioner: a block owns 32 consecutive columns (same j).
-//   A: all threads compute w_tilde and the eta partial at the interior w
-//      levels and the Helmholtz RHS at the mass levels, and stage the Thomas
-//      coefficients, into shared memory (coalesced, fully parallel loads);
-//   B: warp 0 runs the forward/backward recurrences of its 32 columns from
-//      shared memory;
-//   C: all threads write w, eta_dot and pi from the solution.
-// Shared memory per block: (6 nz + 2) * 32 values of T.
+//   A: every thread takes (level k, column): it forms w_tilde at the w levels
+//      k and k+1 (steppers.py:215-219) and with them the Helmholtz RHS at mass
+//      level k (steppers.py:223), L_pi (steppers.py:180) and the acoustic
+//      coupling P = K_w rho_w th_w at w level k (steppers.py:171-177); the
+//      eta_dot/alpha - kin term is parked in the eta_dot output;
+//   B: warp 0 factors and solves its 32 tridiagonal systems
+//      (lower = -L_pi P_k, upper = -L_pi P_k+1, main = 1 - lower - upper;
+//      steppers.py:183-185, 227) by the Thomas algorithm in shared memory;
+//   C: every thread writes w, eta_dot and pi (steppers.py:231-251).
+// The banded system is strictly diagonally dominant, so no pivoting.
+// Shared memory per block: (3 nz + 1) * 32 values of T.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+
 constexpr int PT = 256;  // threads per block
 constexpr int PC = 32;   // columns per block
+
+template <typename T>
+struct PrecondW {  // w-level quantities of one column at one level
+  T wt, ep, P;
+};
+
+template <typename T>
+__device__ __forceinline__ PrecondW<T> precond_wlevel(const Dims& d, const Coef<T>& c, const T* __restrict__ ru,
+                                                     const T* __restrict__ rv, const T* __restrict__ rw,
+                                                     const T* __restrict__ rW, int i, int j, int k, T inva,
+                                                     T adtcp) {
+  // w_tilde and P vanish on the ground and the lid: the loads use a clamped
+  // interior level and the results are masked (no branch around the loads)
+  const int nx = d.nx, ny = d.ny;
+  const int kc = min(max(k, 1), d.nz - 1);
+  const T on = (k > 0 && k < d.nz) ? T(1) : T(0);
+  const int p = i + nx * j + kc * nx * ny;
+  const int u1 = iu(d, i, j, kc), u0 = u1 - (nx + 1) * ny;
+  const int v1 = iv(d, i, j, kc), v0 = v1 - nx * (ny + 1);
+  const T uw = T(0.25) * (ld(ru, u0) + ld(ru, u0 + 1) + ld(ru, u1) + ld(ru, u1 + 1));
+  const T vw = T(0.25) * (ld(rv, v0) + ld(rv, v0 + nx) + ld(rv, v1) + ld(rv, v1 + nx));
+  const T kin = ld(c.mm, i + nx * j) * (uw * ld(c.zxw, p) + vw * ld(c.zew, p));
+  const T thw = ld(c.thw, p);
+  const T rt = ld(c.rhow, p) * thw;
+  const T damp = ld(c.damp, p);
+  PrecondW<T> o;
+  o.ep = on * (ld(rW, p) * inva - kin);
+  o.wt = on * rt * (ld(rw, p) / damp + o.ep);
+  o.P = on * adtcp * thw * ld(c.idzw, p) / damp * rt;  // K_w rho_w th_w
+  return o;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
@@ -162,12 +209,9 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  T* s_x = sm;                        // [nz][PC]  rhs -> d' -> x
-  T* s_low = s_x + nz * PC;           // [nz][PC]
-  T* s_inv = s_low + nz * PC;         // [nz][PC]
-  T* s_cp = s_inv + nz * PC;          // [nz][PC]
-  T* s_wt = s_cp + nz * PC;           // [nz+1][PC]  w_tilde at w levels
-  T* s_ep = s_wt + (nz + 1) * PC;     // [nz+1][PC]  eta_dot / alpha - kin
+  T* s_x = sm;                 // [nz][PC]    rhs -> d' -> x
+  T* s_L = s_x + nz * PC;      // [nz][PC]    L_pi -> c'
+  T* s_P = s_L + nz * PC;      // [nz+1][PC]  P at w levels
   const int i0 = blockIdx.x * PC;
   const int j = blockIdx.y;
   const int tid = threadIdx.x;
@@ -176,11 +220,14 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
   const T* __restrict__ rw = r.f[2];
   const T* __restrict__ rp = r.f[3];
   const T* __restrict__ rW = r.f[4];
-  const T a = (T)c.s.alpha;
-  const T inva = T(1) / a;
+  T* __restrict__ ow = out.f[2];
+  T* __restrict__ op = out.f[3];
+  T* __restrict__ oW = out.f[4];
+  const T inva = T(1) / (T)c.s.alpha;
   const T ips = (T)(1.0 / c.s.ps);
   const T ps = (T)c.s.ps;
   const T adtcp = (T)(c.s.alpha * c.s.dt * c.s.cp);
+  const int pm = nx * ny;
 
   // u and v pass straight through (steppers.py:247-249) unless aliased
   if (out.f[0] != ru) {
@@ -200,74 +247,66 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
     }
   }
 
-  // ---- A1: interior w levels ----
-#pragma unroll 4
+  // ---- A ----
+#pragma unroll 2
   for (int q = tid; q < (nz + 1) * PC; q += PT) {
-    const int k = q / PC, l = q % PC, i = i0 + l;
-    T wt = T(0), ep = T(0);
-    if (i < nx && k > 0 && k < nz) {
-      const int p = iw(d, i, j, k);
-      const T um0 = T(0.5) * (ld(ru, iu(d, i, j, k - 1)) + ld(ru, iu(d, i + 1, j, k - 1)));
-      const T um1 = T(0.5) * (ld(ru, iu(d, i, j, k)) + ld(ru, iu(d, i + 1, j, k)));
-      const T vm0 = T(0.5) * (ld(rv, iv(d, i, j, k - 1)) + ld(rv, iv(d, i, j + 1, k - 1)));
-      const T vm1 = T(0.5) * (ld(rv, iv(d, i, j, k)) + ld(rv, iv(d, i, j + 1, k)));
-      const T kin = ld(c.mm, h_m(d, i, j)) * (T(0.5) * (um0 + um1) * ld(c.zxw, p) + T(0.5) * (vm0 + vm1) * ld(c.zew, p));
-      ep = ld(rW, p) * inva - kin;
-      wt = ld(c.rhow, p) * ld(c.thw, p) * (ld(rw, p) / ld(c.damp, p) + ep);
-    }
-    s_wt[q] = wt;
-    s_ep[q] = ep;
-  }
-  __syncthreads();
-  // ---- A2: Helmholtz RHS at mass levels and the Thomas coefficients ----
-#pragma unroll 4
-  for (int q = tid; q < nz * PC; q += PT) {
-    const int k = q / PC, l = q % PC, i = i0 + l;
-    if (i < nx) {
-      const int p = im(d, i, j, k);
-      s_x[q] = ld(rp, p) * ips - ld(c.lpi, p) * (s_wt[q + PC] - s_wt[q]);
-      s_low[q] = ld(c.tlow, p);
-      s_inv[q] = ld(c.tinv, p);
-      s_cp[q] = ld(c.tcp, p);
+    const int k = q / PC, l = q % PC, i = min(i0 + l, nx - 1);
+    const int km = min(k, nz - 1);
+    const PrecondW<T> lo = precond_wlevel(d, c, ru, rv, rw, rW, i, j, k, inva, adtcp);
+    const PrecondW<T> hi = precond_wlevel(d, c, ru, rv, rw, rW, i, j, k + 1, inva, adtcp);
+    const int p = i + nx * j + km * pm;
+    const T Lpi = ld(c.lpi, p);
+    const T rhs = ld(rp, p) * ips - Lpi * (hi.wt - lo.wt);
+    const bool col = (i0 + l < nx);
+    s_P[q] = col ? lo.P : T(0);
+    if (k < nz) {
+      s_x[q] = rhs;
+      s_L[q] = Lpi;
+      if (col && k > 0) oW[p] = lo.ep;  // eta_dot / alpha - kin, completed in C
     }
   }
   __syncthreads();
-  // ---- B: recurrences, one lane per column ----
+  // ---- B: factor and solve, one lane per column ----
   if (tid < PC) {
     const int l = tid;
-    T dprev = s_x[l] * s_inv[l];
-    s_x[l] = dprev;
-#pragma unroll 8
-    for (int k = 1; k < nz; ++k) {
+    T cprev = T(0), dprev = T(0), Plo = s_P[l];
+#pragma unroll 4
+    for (int k = 0; k < nz; ++k) {
       const int q = k * PC + l;
-      dprev = (s_x[q] - s_low[q] * dprev) * s_inv[q];
+      const T L = s_L[q], Phi = s_P[q + PC];
+      const T lower = -L * Plo, upper = -L * Phi;
+      const T inv = rcp_rn((T(1) - lower - upper) - lower * cprev);
+      cprev = upper * inv;
+      dprev = (s_x[q] - lower * dprev) * inv;
+      s_L[q] = cprev;
       s_x[q] = dprev;
+      Plo = Phi;
     }
     T xh = dprev;
 #pragma unroll 8
     for (int k = nz - 2; k >= 0; --k) {
       const int q = k * PC + l;
-      xh = s_x[q] - s_cp[q] * xh;
+      xh = s_x[q] - s_L[q] * xh;
       s_x[q] = xh;
     }
   }
   __syncthreads();
   // ---- C: back substitution for w, eta_dot and the scaled pi ----
-#pragma unroll 4
+#pragma unroll 2
   for (int q = tid; q < (nz + 1) * PC; q += PT) {
     const int k = q / PC, l = q % PC, i = i0 + l;
     if (i >= nx) continue;
-    const int p = iw(d, i, j, k);
+    const int p = i + nx * j + k * pm;
     if (k == 0 || k == nz) {  // boundary rows (steppers.py:237-238, 244-245)
-      out.f[2][p] = ld(rw, p);
-      out.f[4][p] = ld(rW, p) * ld(c.dzw, p);
+      ow[p] = ld(rw, p);
+      oW[p] = ld(rW, p) * ld(c.dzw, p);
     } else {
       const T grad = (s_x[q] - s_x[q - PC]) * ld(c.idzw, p);
       const T wv = (ld(rw, p) - adtcp * ld(c.thw, p) * grad) / ld(c.damp, p);
-      out.f[2][p] = wv;
-      out.f[4][p] = s_ep[q] + wv;
+      ow[p] = wv;
+      oW[p] = oW[p] + wv;
     }
-    if (k < nz) out.f[3][im(d, i, j, k)] = s_x[q] * ps;
+    if (k < nz) op[p] = s_x[q] * ps;
   }
 }
 
@@ -284,7 +323,7 @@ void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xs
 template <typename T>
 void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                     cudaStream_t st) {
-  const size_t smem = (size_t)(6 * d.nz + 2) * PC * sizeof(T);
+  const size_t smem = (size_t)(3 * d.nz + 1) * PC * sizeof(T);
   static size_t attr_bytes = 0;  // per instantiation
   if (smem > 48 * 1024 && smem > attr_bytes) {
     cudaFuncSetAttribute(precond_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

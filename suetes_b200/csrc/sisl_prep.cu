@@ -3,9 +3,8 @@
 // the working precision.  Follows euler.py:127-160 (precompute_bg),
 // euler.py:254-255 / 320-322 (z_xi_u, z_eta_v, d theta_bg / dz),
 // diffusion.py:117,125 (z_xi_m, z_eta_m) and steppers.py:153-185
-// (precompute_banded), plus the Thomas factorisation of the banded system
-// (jax.lax.linalg.tridiagonal_solve at steppers.py:227 solves the same
-// strictly diagonally dominant systems).
+// (precompute_banded: L_pi; the banded factorisation itself is formed on the
+// fly by the preconditioner from the face coefficients).
 #include "sisl_core.cuh"
 
 #include <math.h>
@@ -14,8 +13,7 @@ namespace sisl {
 
 int coef_loc(int id) {
   switch (id) {
-    case C_THB: case C_PIB: case C_CPIDZ: case C_DTHM: case C_LPI: case C_TLOW: case C_TCP:
-    case C_TINV: case C_ZXM: case C_ZEM: case C_DZM:
+    case C_THB: case C_PIB: case C_CPIDZ: case C_DTHM: case C_LPI: case C_ZXM: case C_ZEM: case C_DZM:
       return LOC_M;
     case C_THU: case C_ZXU: case C_RDU: return LOC_U;
     case C_THV: case C_ZEV: case C_RDV: return LOC_V;
@@ -39,7 +37,7 @@ template <typename T>
 Coef<T> make_coef(T* const* a, const Scalars& s) {
   Coef<T> c;
   c.thb = a[C_THB]; c.pib = a[C_PIB]; c.cpidz = a[C_CPIDZ]; c.dthm = a[C_DTHM]; c.lpi = a[C_LPI];
-  c.tlow = a[C_TLOW]; c.tcp = a[C_TCP]; c.tinv = a[C_TINV]; c.zxm = a[C_ZXM]; c.zem = a[C_ZEM]; c.dzm = a[C_DZM];
+  c.zxm = a[C_ZXM]; c.zem = a[C_ZEM]; c.dzm = a[C_DZM];
   c.thu = a[C_THU]; c.zxu = a[C_ZXU]; c.rdu = a[C_RDU];
   c.thv = a[C_THV]; c.zev = a[C_ZEV]; c.rdv = a[C_RDV];
   c.thw = a[C_THW]; c.rhow = a[C_RHOW]; c.idzw = a[C_IDZW]; c.dzw = a[C_DZW]; c.damp = a[C_DAMP];
@@ -164,46 +162,6 @@ __global__ void prep_points(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
   }
 }
 
-// Thomas factorisation of the column systems (steppers.py:170-185), one
-// thread per column, in float64.
-template <typename T>
-__global__ void prep_thomas(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= d.nx || j >= d.ny) return;
-  const int nz = d.nz;
-  auto Pw = [&](int k) -> double {  // P at w level k, zero on the lid and the ground
-    if (k <= 0 || k >= nz) return 0.0;
-    int kl, kr;
-    level_pair(k, nz, kl, kr);
-    const int pl = im(d, i, j, kl), pr = im(d, i, j, kr), p = iw(d, i, j, k);
-    const double th = 0.5 * (b.theta_bg[pl] + b.theta_bg[pr]);
-    const double rho = 0.5 * (rho_of(s, b.theta_bg[pl], b.pi_bg[pl]) + rho_of(s, b.theta_bg[pr], b.pi_bg[pr]));
-    const double Kw = (s.alpha * s.dt * s.cp * th) / (b.dz_w[p] * (1.0 + s.dt * b.tau[p]));
-    return Kw * rho * th;
-  };
-  double cprev = 0.0;
-  double Plo = Pw(0);
-  for (int k = 0; k < nz; ++k) {
-    const int p = im(d, i, j, k);
-    const double th = b.theta_bg[p], pi = b.pi_bg[p];
-    const double rho = rho_of(s, th, pi);
-    const double cpi = (s.Rd / s.cvd) * (pi / (rho * th));
-    const double Lpi = s.alpha * s.dt * cpi / b.dz_m[p];
-    const double Phi = Pw(k + 1);
-    const double lower = -Lpi * Plo;
-    const double upper = -Lpi * Phi;
-    const double mainv = 1.0 - lower - upper;
-    const double inv = 1.0 / (mainv - (k > 0 ? lower * cprev : 0.0));
-    const double cp = upper * inv;
-    out.p[C_TLOW][p] = (T)lower;
-    out.p[C_TCP][p] = (T)cp;
-    out.p[C_TINV][p] = (T)inv;
-    cprev = cp;
-    Plo = Phi;
-  }
-}
-
 }  // namespace
 
 template <typename T>
@@ -211,9 +169,6 @@ void launch_prepare(const Dims& d, const Scalars& s, const Base64& b, PtrTable<T
   dim3 blk(32, 4, 2);
   dim3 grd((d.nx + 1 + blk.x - 1) / blk.x, (d.ny + 1 + blk.y - 1) / blk.y, (d.nz + 1 + blk.z - 1) / blk.z);
   prep_points<T><<<grd, blk, 0, st>>>(d, s, b, out);
-  dim3 blk2(32, 4);
-  dim3 grd2((d.nx + 31) / 32, (d.ny + 3) / 4);
-  prep_thomas<T><<<grd2, blk2, 0, st>>>(d, s, b, out);
 }
 
 template Coef<float> make_coef<float>(float* const*, const Scalars&);
