@@ -54,6 +54,9 @@ enum {
   SISL_K_NONE = 0, SISL_K_MATVEC = 1, SISL_K_PRECOND = 2, SISL_K_DOTS = 3, SISL_K_UPDATE = 4,
   SISL_K_SL = 5, SISL_K_EXPLICIT = 6, SISL_K_OTHER = 7
 };
+enum {
+  SISL_STAGGER_AVG = 0, SISL_STAGGER_DIFF = 1
+};
 
 #define SISL_OK 0
 #define SISL_NOT_CONVERGED 1
@@ -163,6 +166,19 @@ int sisl_precond_apply(SislCore* core, const void* const in[5], void* const out[
  * reference); x may alias x0. */
 int sisl_gmres_solve(SislCore* core, const void* const rhs[5], const void* const x0[5], void* const x[5],
                      void* ws, size_t ws_bytes, void* stream, SislSolveInfo* info);
+/* Exact transpose of A_fn (steppers.py:439-461), the matvec_T that
+ * jax.lax.custom_linear_solve hands to bwd_solve (steppers.py:473-481).
+ * ws: sisl_workspace_bytes(core, SISL_WS_OPERATOR) bytes; out must not alias in. */
+int sisl_helmholtz_matvec_t(SislCore* core, const void* const in[5], void* const out[5], void* ws,
+                            size_t ws_bytes, void* stream);
+/* jax.linear_transpose(M_fn) of the column preconditioner (steppers.py:474-476).
+ * out must not alias in. */
+int sisl_precond_apply_t(SislCore* core, const void* const in[5], void* const out[5], void* stream);
+/* bwd_solve of SemiImplicitSolver3D.solve (steppers.py:473-485): the cotangent
+ * of the physical rhs from the cotangent of the physical solution, by GMRES on
+ * A^T with preconditioner M^T from a zero guess and the forward tol/restart. */
+int sisl_gmres_solve_transpose(SislCore* core, const void* const xbar[5], void* const bbar[5], void* ws,
+                               size_t ws_bytes, void* stream, SislSolveInfo* info);
 /* SemiLagrangianAdvector3D.compute_departure_indices(state, loc, iterations)
  * (steppers.py:318-360); coords[3] have the extents of stagger loc. */
 int sisl_departure(SislCore* core, int loc, const void* u, const void* v, const void* eta_dot, int iterations,
@@ -171,6 +187,23 @@ int sisl_departure(SislCore* core, int loc, const void* u, const void* v, const 
  * for any field shape and any coordinate-array shape (both x-fastest). */
 int sisl_tricubic(int dtype, const int32_t src_shape[3], const void* field, const int32_t dst_shape[3],
                   const void* const coords[3], void* out, int use_limiter, void* stream);
+/* VJP of tensor_product_interp_3d with respect to the field (operators.py:146-209;
+ * the departure coordinates are stop-gradiented, steppers.py:764-767):
+ * grad += scale * J^T cot, accumulated with atomics; field is read only with
+ * the limiter, whose clip and min/max chains route the cotangent as lax.min
+ * and lax.max do (ties split in half). */
+int sisl_tricubic_vjp(int dtype, const int32_t src_shape[3], const void* field, const int32_t dst_shape[3],
+                      const void* const coords[3], const void* cot, void* grad, int use_limiter, double scale,
+                      void* stream);
+/* CGridOperator3D.avg / .diff (operators.py:37-132) along one axis of an
+ * x-fastest field of shape in_shape: to_face = 1 maps centres to faces
+ * (n -> n+1, edge-padded or periodic), 0 faces to centres (n+1 -> n);
+ * mult: optional 2-D (x-fastest) multiplier at the output stagger (the map
+ * factor of diff).  transpose = 1 applies the transpose (src: output-shaped
+ * cotangent, dst: input-shaped), with stop_grad dropping the padded copies
+ * as jax.lax.stop_gradient does (operators.py:45-61). */
+int sisl_stagger(int dtype, int op, const int32_t in_shape[3], int axis, int to_face, int periodic, int stop_grad,
+                 int transpose, double inv_delta, const void* mult, const void* src, void* dst, void* stream);
 /* map_coordinates(field, coords, order=1, mode='nearest'), the trilinear
  * gather of SemiLagrangianAdvector3D.advect_linear (steppers.py:362-367). */
 int sisl_trilinear(int dtype, const int32_t src_shape[3], const void* field, const int32_t dst_shape[3],
@@ -220,6 +253,13 @@ int sisl_eos(SislCore* core, const void* th_p, const void* pi_p, void* rho, void
  * overlap, except that out->*_prev may equal the matching in field. */
 int sisl_step(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
               size_t ws_bytes, void* stream, SislStepInfo* info);
+/* sisl_step that also copies the physical solution (u, v, w, pi_p, eta_dot)
+ * of each of its two implicit solves into solves[0..4] and solves[5..9]
+ * (NULL entries skipped): the residuals a checkpointed VJP recomputation
+ * reuses instead of solving again (jax.checkpoint of the step,
+ * steppers.py:792-850). */
+int sisl_step_taped(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax,
+                    void* const solves[10], void* ws, size_t ws_bytes, void* stream, SislStepInfo* info);
 
 /* Instrumentation (no reference counterpart): number of kernels this library
  * launched, and CUDA-event timing of one kernel class inside GMRES (events

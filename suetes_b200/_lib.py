@@ -18,6 +18,7 @@ WS_STEP, WS_GMRES, WS_DEPARTURE, WS_EXPLICIT, WS_OPERATOR = 0, 1, 2, 3, 4
 RELAX_U, RELAX_V, RELAX_W, RELAX_TH, RELAX_PI = 1, 2, 4, 8, 16
 K_NONE, K_MATVEC, K_PRECOND, K_DOTS, K_UPDATE, K_SL, K_EXPLICIT, K_OTHER = range(8)
 SISL_OK, SISL_NOT_CONVERGED = 0, 1
+SISL_STAGGER_AVG, SISL_STAGGER_DIFF = 0, 1
 SISL_ERR_SCRATCH_LIMIT = -5
 FFSL_NOALLOC_MAX_DOUBLES = 1 << 20
 
@@ -86,10 +87,18 @@ PROTOTYPES = {
     "sisl_precond_apply": (ctypes.c_int, [vp, vp * 5, vp * 5, vp]),
     "sisl_gmres_solve": (ctypes.c_int, [vp, vp * 5, vp, vp * 5, vp, ctypes.c_size_t, vp,
                                         ctypes.POINTER(SislSolveInfo)]),
+    "sisl_helmholtz_matvec_t": (ctypes.c_int, [vp, vp * 5, vp * 5, vp, ctypes.c_size_t, vp]),
+    "sisl_precond_apply_t": (ctypes.c_int, [vp, vp * 5, vp * 5, vp]),
+    "sisl_gmres_solve_transpose": (ctypes.c_int, [vp, vp * 5, vp * 5, vp, ctypes.c_size_t, vp,
+                                                  ctypes.POINTER(SislSolveInfo)]),
     "sisl_departure": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp * 3, vp, ctypes.c_size_t,
                                       vp]),
     "sisl_tricubic": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32 * 3, vp, ctypes.c_int32 * 3, vp * 3, vp,
                                      ctypes.c_int, vp]),
+    "sisl_tricubic_vjp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32 * 3, vp, ctypes.c_int32 * 3, vp * 3, vp, vp,
+                                         ctypes.c_int, ctypes.c_double, vp]),
+    "sisl_stagger": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int32 * 3, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, vp, vp, vp, vp]),
     "sisl_explicit_tendencies": (ctypes.c_int, [vp, vp * 6, vp * 6, vp, vp, ctypes.c_size_t, vp]),
     "sisl_tendencies": (ctypes.c_int, [vp, ctypes.c_int, vp * 6, vp * 6, vp, vp, ctypes.c_size_t, vp]),
     "sisl_trilinear": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32 * 3, vp, ctypes.c_int32 * 3, vp * 3, vp, vp]),
@@ -103,6 +112,9 @@ PROTOTYPES = {
     "sisl_step": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
                                  ctypes.POINTER(SislRelaxation), vp, ctypes.c_size_t, vp,
                                  ctypes.POINTER(SislStepInfo)]),
+    "sisl_step_taped": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
+                                       ctypes.POINTER(SislRelaxation), vp * 10, vp, ctypes.c_size_t, vp,
+                                       ctypes.POINTER(SislStepInfo)]),
     "sisl_kernel_launches": (ctypes.c_int64, []),
     "sisl_timing_select": (ctypes.c_int, [vp, ctypes.c_int]),
     "sisl_timing_read": (ctypes.c_int, [vp, c_double_p, ctypes.POINTER(ctypes.c_int64), c_double_p]),

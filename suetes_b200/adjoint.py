@@ -1,0 +1,397 @@
+"""Differentiable SISL step and the checkpointed trajectory VJP.
+
+The reference differentiates ``SISLStepper3D.step`` (steppers.py:720-1073)
+with JAX autodiff: departure points are stop-gradiented (steppers.py:764-767),
+the implicit solve is a ``custom_linear_solve`` whose transpose is GMRES on
+A^T with M^T (steppers.py:463-485), the tricubic VJP scatters the 64 weights,
+and the explicit stencils honour the edge-padding ``stop_gradient`` of
+``CGridOperator3D`` (operators.py:45-61).  ``DifferentiableStep`` restates
+the step as a composition of differentiable CUDA primitives:
+
+* ``CGridOperator3D.diff/avg``: staggered stencil kernels and their
+  transposes (``sisl_stagger``);
+* ``tensor_product_interp_3d``: tricubic kernel, VJP by ``sisl_tricubic_vjp``;
+* the implicit solve: GMRES (``sisl_gmres_solve``), VJP by the transposed
+  solve (``sisl_gmres_solve_transpose``), or -- when recomputing a step whose
+  solves were recorded by ``sisl_step_taped`` -- the recorded solution;
+
+with pointwise products and sums between them.  ``trajectory_vjp`` runs the
+fused forward step (``sisl_step_taped``), keeps each step's input state and
+solve outputs (every step, or every ``checkpoint_every`` steps with the
+segment recomputed, the chunked ``jax.checkpoint`` of driver.py:102-116), and
+sweeps backwards one step at a time through ``DifferentiableStep``.
+"""
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import check, ptrs
+from .core import F64, empty_field, fortran
+from .operators import tensor_product_interp_3d
+
+KEYS5 = ("u", "v", "w", "pi", "eta_dot")
+LOCS5 = ("u", "v", "w", "m", "w")
+# perturbation-form state: the fields of DeviceState (pi_p = pi - pi_bg, th_p = th_v - theta_bg)
+STATE_KEYS = ("u", "v", "w", "eta_dot", "pi_p", "th_p", "rho", "u_prev", "v_prev", "w_prev", "eta_dot_prev",
+              "tend_th_prev")
+
+
+class _RecordedSolve(torch.autograd.Function):
+    """The implicit solve of a recomputed step: forward returns the solution
+    recorded by the fused step, backward is the transposed GMRES solve."""
+
+    @staticmethod
+    def forward(ctx, solver, core, recorded, *b):
+        ctx.solver, ctx.core = solver, core
+        return tuple(r.clone() for r in recorded)
+
+    @staticmethod
+    def backward(ctx, *g):
+        core = ctx.core
+        gs = [empty_field(core.shape(l), core.dtype, core.device).zero_() if t is None else core.field(t, l)
+              for t, l in zip(g, LOCS5)]
+        return (None, None, None) + tuple(ctx.solver._solve_transpose_core(core, gs))
+
+
+class DifferentiableStep:
+    """``SISLStepper3D.step`` (steppers.py:720-1073) as differentiable CUDA primitives."""
+
+    def __init__(self, stepper, dtype):
+        self.stepper = stepper
+        ph = stepper.physics
+        self.ph, self.op, self.c = ph, ph.op, ph.c
+        g = ph.grid
+        self.grid, self.dtype = g, dtype
+        self.a, self.dt = float(stepper.alpha), float(stepper.dt)
+        op = self.op
+        F = lambda t: fortran(t, dtype=dtype, device=g.device)
+        self.bg64 = ph.precompute_bg(ph.bg_state_ref())
+        self.bg = {k: F(v) for k, v in self.bg64.items()}
+        self.theta_bg, self.pi_bg = F(ph.theta_bg), F(ph.pi_bg)
+        self.m = {loc: F(g.m_factors[loc])[..., None] for loc in ("m", "u", "v", "w")}
+        self.f_u, self.f_v = F(g.f_u)[..., None], F(g.f_v)[..., None]
+        self.dmdx, self.dmdy = F(g.dm_dx_m)[..., None], F(g.dm_dy_m)[..., None]
+        self.z_xi_w, self.z_eta_w = F(g.z_xi_w), F(g.z_eta_w)
+        self.dz = float(g.dz)
+        with torch.no_grad():
+            b = self.bg64
+            z_xi_u = op.diff(g.Z_m, 0, "m", "u")
+            z_eta_v = op.diff(g.Z_m, 1, "m", "v")
+            self.z_xi_u, self.z_eta_v = F(z_xi_u), F(z_eta_v)
+            self.z_xi_m = F(op.avg(z_xi_u, 0, "u", "m"))
+            self.z_eta_m = F(op.avg(z_eta_v, 1, "v", "m"))
+            self.dzr_w = F(g.dz / b["dz_w_full"])
+            dth_w = op.diff(b["th_v"], 2, "m", "w") * (g.dz / b["dz_w_full"])
+            self.dth_m = F(op.avg(dth_w, 2, "w", "m"))
+            nz = g.nz
+            inner = torch.ones(g.shape_of("w"), dtype=F64, device=g.device)
+            inner[:, :, 0] = 0.0
+            inner[:, :, nz] = 0.0
+            self.w_inner = F(inner)
+            edge = torch.zeros(g.shape_of("u"), dtype=torch.bool, device=g.device)
+            edge[0], edge[-1] = True, True
+            self.u_edge = fortran(edge)
+            edge = torch.zeros(g.shape_of("v"), dtype=torch.bool, device=g.device)
+            edge[:, 0], edge[:, -1] = True, True
+            self.v_edge = fortran(edge)
+            ground = torch.zeros(g.shape_of("w"), dtype=torch.bool, device=g.device)
+            ground[:, :, 0] = True
+            self.w_ground = fortran(ground)
+
+    # ---- diffusion.py:93-173 (HyperFilter with nu_v = 0) ----
+    def _lap_h(self, f):
+        op = self.op
+        dfz_m = op.avg(op.diff(f, 2, "m", "w") * self.dzr_w, 2, "w", "m")
+        gx = op.diff(f, 0, "m", "u") - self.z_xi_u * op.avg(dfz_m, 0, "m", "u")
+        gy = op.diff(f, 1, "m", "v") - self.z_eta_v * op.avg(dfz_m, 1, "m", "v")
+        gxm = op.avg(gx, 0, "u", "m")
+        div_x = op.diff(gx, 0, "u", "m") - self.z_xi_m * op.avg(op.diff(gxm, 2, "m", "w") * self.dzr_w, 2, "w", "m")
+        gym = op.avg(gy, 1, "v", "m")
+        div_y = op.diff(gy, 1, "v", "m") - self.z_eta_m * op.avg(op.diff(gym, 2, "m", "w") * self.dzr_w, 2, "w",
+                                                                 "m")
+        return div_x + div_y
+
+    def _hyper(self, sp, thp):
+        op, nu = self.op, self.ph.nu_h
+        src = {"u": op.avg(sp["u"], 0, "u", "m"), "v": op.avg(sp["v"], 1, "v", "m"),
+               "w": op.avg(sp["w"], 2, "w", "m"), "th_v": thp}
+        out = {}
+        for k, f in src.items():
+            t = -nu * self._lap_h(self._lap_h(f))
+            if k == "u":
+                out[k] = op.avg(t, 0, "m", "u")
+            elif k == "v":
+                out[k] = op.avg(t, 1, "m", "v")
+            elif k == "w":
+                out[k] = op.avg(t, 2, "m", "w")
+            else:
+                out[k] = t
+        return out
+
+    # ---- euler.py:188-206 ----
+    def metric_curvature(self, u, v):
+        op = self.op
+        u_m, v_m = op.avg(u, 0, "u", "m"), op.avg(v, 1, "v", "m")
+        metric_m = v_m * self.dmdx - u_m * self.dmdy
+        v_at_u = op.avg(v_m, 0, "m", "u")
+        u_at_v = op.avg(u_m, 1, "m", "v")
+        return op.avg(metric_m, 0, "m", "u") * v_at_u, -op.avg(metric_m, 1, "m", "v") * u_at_v
+
+    # ---- euler.py:162-186 ----
+    def nonlinear_pi(self, sp, thp):
+        op, bg = self.op, self.bg
+        fx = sp["u"] * bg["rho_u"] * op.avg(thp, 0, "m", "u") * bg["dz_u"] / self.m["u"]
+        fy = sp["v"] * bg["rho_v"] * op.avg(thp, 1, "m", "v") * bg["dz_v"] / self.m["v"]
+        fz = sp["eta_dot"] * bg["dz_w_full"] * bg["rho_w"] * op.avg(thp, 2, "m", "w") * self.w_inner
+        div_h = (op.diff(fx, 0, "u", "m") + op.diff(fy, 1, "v", "m")) / bg["dz_m_full"]
+        div_z = op.diff(fz, 2, "w", "m") * self.dz / bg["dz_m_full"]
+        return -bg["C_pi"] * (self.m["m"] * div_h + div_z)
+
+    # ---- euler.py:208-372, is_explicit=True ----
+    def tendencies(self, sp, thp):
+        op, bg, c = self.op, self.bg, self.c
+        u, v, w, pi_p, eta = sp["u"], sp["v"], sp["w"], sp["pi"], sp["eta_dot"]
+        thp_u, thp_v, thp_w = op.avg(thp, 0, "m", "u"), op.avg(thp, 1, "m", "v"), op.avg(thp, 2, "m", "w")
+        gpz_w = op.diff(pi_p, 2, "m", "w") * self.dzr_w
+        gpz_m = op.avg(gpz_w, 2, "w", "m")
+        gx = op.diff(pi_p, 0, "m", "u") - self.z_xi_u * op.avg(gpz_m, 0, "m", "u")
+        gy = op.diff(pi_p, 1, "m", "v") - self.z_eta_v * op.avg(gpz_m, 1, "m", "v")
+        tend_u = -c["cp"] * (bg["th_v_u"] + thp_u) * gx
+        tend_v = -c["cp"] * (bg["th_v_v"] + thp_v) * gy
+        tend_w = -c["cp"] * (bg["th_v_w"] + thp_w) * gpz_w + c["g"] * (thp_w / bg["th_v_w"])
+        u_m, v_m = op.avg(u, 0, "u", "m"), op.avg(v, 1, "v", "m")
+        tend_u = tend_u + self.f_u * op.avg(v_m, 0, "m", "u")
+        tend_v = tend_v - self.f_v * op.avg(u_m, 1, "m", "v")
+        mu, mv = self.metric_curvature(u, v)
+        tend_u, tend_v = tend_u + mu, tend_v + mv
+        fx = (u * bg["rho_u"] * bg["th_v_u"] * bg["dz_u"]) / self.m["u"]
+        fy = (v * bg["rho_v"] * bg["th_v_v"] * bg["dz_v"]) / self.m["v"]
+        fz = eta * bg["dz_w_full"] * bg["rho_w"] * bg["th_v_w"] * self.w_inner
+        div_h = (op.diff(fx, 0, "u", "m") + op.diff(fy, 1, "v", "m")) / bg["dz_m_full"]
+        div_z = (op.diff(fz, 2, "w", "m") * self.dz) / bg["dz_m_full"]
+        tend_pi = -bg["C_pi"] * (self.m["m"] * div_h + div_z)
+        tend_th = -op.avg(w, 2, "w", "m") * self.dth_m
+        out = {"u": tend_u, "v": tend_v, "w": tend_w, "pi": tend_pi, "th_v": tend_th,
+               "phys_diff_u": 0.0, "phys_diff_v": 0.0, "phys_diff_w": 0.0, "phys_diff_th_v": 0.0}
+        if self.ph.nu_h > 0.0 or self.ph.nu_div > 0.0:
+            h = self._hyper(sp, thp)
+            for k in ("u", "v", "w", "th_v"):
+                out[k] = out[k] + h[k]
+                out["phys_diff_" + k] = h[k]
+        return out
+
+    # ---- steppers.py:720-1073 ----
+    def departure(self, state):
+        """Departure indices of the four staggers (no cotangent, steppers.py:748-767)."""
+        adv = self.stepper.advector
+        it = int(getattr(self.stepper, "departure_iterations", 2))
+        with torch.no_grad():
+            first = float(state.get("is_first_step", 1.0)) == 1.0
+            tr = {}
+            for k in ("u", "v", "eta_dot"):
+                x = state[k].detach()
+                if "u_prev" in state and not first:
+                    x = 1.5 * x - 0.5 * state[k + "_prev"].detach()
+                tr[k] = x
+            return {loc: adv.compute_departure_indices(tr, loc=loc, iterations=it) for loc in ("u", "v", "w", "m")}
+
+    def __call__(self, state, relax=None, recorded=None, coords=None):
+        """One step on a perturbation-form state (keys of ``STATE_KEYS`` plus
+        ``is_first_step``); returns the next state in the same form.
+
+        ``recorded``: the two five-field solutions of the fused step for this
+        state (replaces the forward GMRES solves); ``relax``: a
+        ``LateralRelaxation`` bc_fn."""
+        op, bg, c, ph = self.op, self.bg, self.c, self.ph
+        a, dt = self.a, self.dt
+        lim = self.stepper.use_limiter
+        cs = coords if coords is not None else self.departure(state)
+        thp_n = state["th_p"]
+        sp_n = {"u": state["u"], "v": state["v"], "w": state["w"], "pi": state["pi_p"], "eta_dot": state["eta_dot"]}
+        tn = self.tendencies(sp_n, thp_n)
+        u_in = state["u"] + dt * ((1.0 - a) * tn["u"] + a * tn["phys_diff_u"])
+        v_in = state["v"] + dt * ((1.0 - a) * tn["v"] + a * tn["phys_diff_v"])
+        w_in = state["w"] + dt * ((1.0 - a) * tn["w"] + a * tn["phys_diff_w"])
+        pi_in = sp_n["pi"] + (1.0 - a) * dt * (tn["pi"] + self.nonlinear_pi(sp_n, thp_n))
+        th_in = thp_n + (1.0 - a) * dt * tn["th_v"]
+        u_w = op.avg(op.avg(state["u"], 0, "u", "m"), 2, "m", "w")
+        v_w = op.avg(op.avg(state["v"], 1, "v", "m"), 2, "m", "w")
+        res_n = bg["dz_w_full"] * state["eta_dot"] + u_w * self.z_xi_w + v_w * self.z_eta_w - state["w"]
+        ac = lambda f, loc: tensor_product_interp_3d(f, cs[loc], use_limiter=lim)
+        R_eta = -(1.0 - a) * ac(res_n, "w")
+        rhs_u = ac(u_in, "u")
+        rhs_v = ac(v_in, "v")
+        if 0 in op.periodic_axes:
+            rhs_u = torch.cat([rhs_u[:-1], rhs_u[:1]], dim=0)
+        else:
+            rhs_u = torch.where(self.u_edge, state["u"], rhs_u)
+        if 1 in op.periodic_axes:
+            rhs_v = torch.cat([rhs_v[:, :-1], rhs_v[:, :1]], dim=1)
+        else:
+            rhs_v = torch.where(self.v_edge, state["v"], rhs_v)
+        rhs_w = ac(w_in, "w")
+        rhs_pi = ac(pi_in, "m")
+        th_adv = ac(th_in, "m")
+        R_eta_adv = R_eta * self.w_inner
+        w_m = op.avg(state["w"], 2, "w", "m")
+        w_m_next = w_m
+        guess = sp_n
+        u_g, v_g = rhs_u, rhs_v
+        cad = c["cp"] * a * dt
+        solver = self.stepper.implicit_solver
+        core = solver._core(self.dtype, self.bg64)
+        for it in range(2):  # steppers.py:911-998
+            t_th = tn["th_v"] + (w_m - w_m_next) * self.dth_m
+            thp_next = th_adv + a * dt * t_th
+            tpu, tpv, tpw = op.avg(thp_next, 0, "m", "u"), op.avg(thp_next, 1, "m", "v"), op.avg(thp_next, 2, "m", "w")
+            buoy = a * dt * (c["g"] * (tpw / bg["th_v_w"]))
+            pg = guess["pi"]
+            gz_w = op.diff(pg, 2, "m", "w") * self.dzr_w
+            gz_m = op.avg(gz_w, 2, "w", "m")
+            nl_u = -cad * tpu * (op.diff(pg, 0, "m", "u") - self.z_xi_u * op.avg(gz_m, 0, "m", "u"))
+            nl_v = -cad * tpv * (op.diff(pg, 1, "m", "v") - self.z_eta_v * op.avg(gz_m, 1, "m", "v"))
+            nl_w = -cad * tpw * gz_w
+            nl_div = self.nonlinear_pi(guess, thp_next)
+            mu, mv = self.metric_curvature(u_g, v_g)
+            rhs_u_k = rhs_u + nl_u + a * dt * mu
+            rhs_v_k = rhs_v + nl_v + a * dt * mv
+            rhs_pi_k = rhs_pi + a * dt * nl_div
+            ugw = op.avg(op.avg(u_g, 0, "u", "m"), 2, "m", "w")
+            vgw = op.avg(op.avg(v_g, 1, "v", "m"), 2, "m", "w")
+            kb = self.m["w"] * (ugw * self.z_xi_w + vgw * self.z_eta_w)
+            rhs_w_k = torch.where(self.w_ground, kb, (rhs_w + buoy + nl_w) * self.w_inner)
+            b = [core.field(t, l) for t, l in zip((rhs_u_k, rhs_v_k, rhs_w_k, rhs_pi_k, R_eta_adv), LOCS5)]
+            if recorded is not None:
+                x = _RecordedSolve.apply(solver, core, recorded[it], *b)
+            elif torch.is_grad_enabled() and any(t.requires_grad for t in b):
+                from .steppers import _LinearSolve
+                x = _LinearSolve.apply(solver, core, guess, *b)
+            else:
+                x = solver._solve_core(core, b, guess)
+            nxt = dict(zip(KEYS5, x))
+            guess = nxt
+            w_m_next = op.avg(nxt["w"], 2, "w", "m")
+            u_g, v_g = nxt["u"], nxt["v"]
+        u, v = nxt["u"], nxt["v"]
+        if ph.nu_div != 0.0:  # steppers.py:1022-1031
+            div_h = op.diff(u, 0, "u", "m") + op.diff(v, 1, "v", "m")
+            u = u + ph.nu_div * dt * op.diff(div_h, 0, "m", "u")
+            v = v + ph.nu_div * dt * op.diff(div_h, 1, "m", "v")
+        w, pi_p, th_p = nxt["w"], nxt["pi"], thp_next
+        if relax is not None:  # bc_fn blend, then the EOS (steppers.py:1055-1056)
+            u, v, w, th_p, pi_p = self._relax(relax, u, v, w, th_p, pi_p)
+        rho = c["p0"] / (c["Rd"] * (th_p + self.theta_bg)) * (pi_p + self.pi_bg) ** (c["cvd"] / c["Rd"])
+        return {"u": u, "v": v, "w": w, "eta_dot": nxt["eta_dot"], "pi_p": pi_p, "th_p": th_p, "rho": rho,
+                "u_prev": state["u"], "v_prev": state["v"], "w_prev": state["w"],
+                "eta_dot_prev": state["eta_dot"], "tend_th_prev": tn["th_v"], "is_first_step": 0.0}
+
+    def _relax(self, relax, u, v, w, th_p, pi_p):
+        F = lambda t: fortran(torch.as_tensor(t), dtype=self.dtype, device=self.grid.device)
+        masks = {"u": F(relax.mask_u)[..., None], "v": F(relax.mask_v)[..., None], "m": F(relax.mask_m)[..., None]}
+        vals = {"u": (u, "u"), "v": (v, "v"), "w": (w, "m"), "th_v": (th_p, "m"), "pi": (pi_p, "m")}
+        out = {}
+        for k, (val, mloc) in vals.items():
+            if k in relax.fields:
+                ext = relax.exterior.get(k, 0.0)
+                ext = F(ext) if torch.is_tensor(ext) else float(ext)
+                m = masks[mloc]
+                val = (1.0 - m) * val + m * ext
+            out[k] = val
+        return out["u"], out["v"], out["w"], out["th_v"], out["pi"]
+
+
+# ---------------------------------------------------------------------------
+# trajectory VJP with step checkpointing
+# ---------------------------------------------------------------------------
+def _taped_step(stepper, ds, relax, record=True):
+    """One fused step (``sisl_step_taped``): (next DeviceState, recorded solves or None)."""
+    from .steppers import DeviceState
+    core = ds.core
+    out = DeviceState(core)
+    rec = [[core.new(l) for l in LOCS5] for _ in range(2)] if record else None
+    tape = ptrs(rec[0] + rec[1], 10) if record else (ctypes.c_void_p * 10)()
+    sin, sout = ds.c_struct(), out.c_struct()
+    rl = relax.c_struct(core) if relax is not None else None
+    ws, n = core.workspace(_lib.WS_STEP)
+    info = _lib.SislStepInfo()
+    check(core.lib.sisl_step_taped(core.handle, ctypes.byref(sin), ctypes.byref(sout),
+                                   ctypes.byref(rl) if rl is not None else None, tape,
+                                   ws.data_ptr(), n, core.stream, ctypes.byref(info)), "sisl_step_taped")
+    out.is_first_step = 0.0
+    stepper.last_info = {"solves": [info.solve[0].as_dict(), info.solve[1].as_dict()]}
+    return out, rec
+
+
+def _as_dict(ds):
+    d = dict(ds.t)
+    d["is_first_step"] = ds.is_first_step
+    return d
+
+
+def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint_every=1, wrt=("th_p",)):
+    """Value and gradient of ``J = sum_n objective(n, state_n)`` over
+    ``num_steps`` SISL steps from ``state0`` (a reference state dict or a
+    ``DeviceState``).
+
+    ``objective(n, state)`` gets the perturbation-form state after step ``n``
+    (1-based; keys of ``STATE_KEYS``) and returns a scalar tensor or None.
+    Returns ``(J, grads)``, ``grads[k]`` the cotangent of the initial
+    ``state[k]`` for ``k`` in ``wrt`` (``th_p`` is the initial theta'; the
+    cotangent of th_v is the same).  The forward pass runs the fused step
+    and keeps every ``checkpoint_every``-th state; the backward pass
+    recomputes a segment with the fused step (recording its solves) and
+    differentiates it one step at a time through ``DifferentiableStep``
+    (jax.checkpoint of steppers.py:792-850, driver.py:91-132)."""
+    relax, generic = stepper._relax_of(bc_fn)
+    if generic is not None:
+        raise NotImplementedError("trajectory_vjp supports LateralRelaxation boundary conditions")
+    from .steppers import DeviceState
+    ds0 = state0 if isinstance(state0, DeviceState) else stepper.to_device_state(state0)
+    dstep = DifferentiableStep(stepper, ds0.core.dtype)
+    K = max(1, int(checkpoint_every))
+    checkpoints = {0: ds0}
+    cur = ds0
+    J = torch.zeros((), dtype=F64, device=ds0.core.device)
+    with torch.no_grad():
+        for n in range(num_steps):
+            cur, _ = _taped_step(stepper, cur, relax, record=False)
+            val = objective(n + 1, _as_dict(cur))
+            if val is not None:
+                J = J + val.double()
+            if (n + 1) % K == 0 and n + 1 < num_steps:
+                checkpoints[n + 1] = cur
+    keys = [k for k in STATE_KEYS]
+    cot = {}
+    for seg0 in range(((num_steps - 1) // K) * K, -1, -K):
+        seg1 = min(seg0 + K, num_steps)
+        states, recs = [checkpoints[seg0]], []
+        with torch.no_grad():
+            for n in range(seg0, seg1):
+                nxt, rec = _taped_step(stepper, states[-1], relax)
+                states.append(nxt)
+                recs.append(rec)
+        for n in range(seg1 - 1, seg0 - 1, -1):
+            after = {k: v.detach().requires_grad_(True) for k, v in states[n + 1 - seg0].t.items()}
+            g_after = dict(cot)
+            with torch.enable_grad():
+                val = objective(n + 1, dict(after, is_first_step=0.0))
+                if val is not None and val.requires_grad:
+                    gs = torch.autograd.grad(val, [after[k] for k in keys], allow_unused=True)
+                    for k, g in zip(keys, gs):
+                        if g is not None:
+                            g_after[k] = g_after[k] + g if k in g_after else g
+            before_ds = states[n - seg0]
+            before = {k: v.detach().requires_grad_(True) for k, v in before_ds.t.items()}
+            with torch.enable_grad():
+                out = dstep(dict(before, is_first_step=before_ds.is_first_step), relax=relax,
+                            recorded=recs[n - seg0])
+                outs, grads = [], []
+                for k, g in g_after.items():
+                    if k in out and torch.is_tensor(out[k]) and out[k].requires_grad:
+                        outs.append(out[k])
+                        grads.append(g)
+                gs = torch.autograd.grad(outs, [before[k] for k in keys], grads, allow_unused=True) if outs else []
+            cot = {k: g for k, g in zip(keys, gs) if g is not None}
+    return J, {k: cot.get(k) for k in wrt}

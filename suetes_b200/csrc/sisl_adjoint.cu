@@ -1,0 +1,556 @@
+// Transposed Helmholtz matvec A^T and transposed preconditioner M^T on the
+// scaled solver vector, in gather form (no atomics, deterministic).
+//
+// The reference differentiates SemiImplicitSolver3D.solve through
+// jax.lax.custom_linear_solve (steppers.py:483-485): the cotangent solve is
+// gmres(A^T, g, M=M^T) (steppers.py:473-481) where A^T is the exact transpose
+// of A_fn traced without the edge-padding stop_gradient (steppers.py:463) and
+// M^T = jax.linear_transpose(M_fn).  Both transposes are written out here from
+// the forward rows of sisl_linear.cu:
+//
+//  u face (interior or periodic face 0; the periodic face n row copies face 0)
+//    L_u = u - adt [ -cp thu ((P_r - P_l) m_u/dx - zxu (gzm_l + gzm_r)/2)
+//                   + f_u (v_l,j + v_l,j+1 + v_r,j + v_r,j+1)/4 ]
+//  v face analogous with -f_v * (u ...)/4
+//  w level (interior)   L_w = damp w + adt cp thw gzw
+//  eta row (interior)   L_e = a (W + m (uw zxw + vw zew) - w)
+//  boundary rows        L_u = u, L_v = v, L_w = w, L_e = W / dz_w
+//  pi row               L_p = p + adt ps cpidz (m^2 (dFx/dx + dFy/dy) + dFz)
+//  with P = p / ps, gzw(k) = (P(kr) - P(kl)) / dz_w(k) on the padded level
+//  pair, gzm(k) = (gzw(k) + gzw(k+1)) / 2, Fx = u rdu thu, Fz = W rhow thw.
+#include "sisl_core.cuh"
+
+namespace sisl {
+namespace {
+
+dim3 box_grid(int ex, int ey, int ez, dim3 blk) {
+  return dim3((ex + blk.x - 1) / blk.x, (ey + blk.y - 1) / blk.y, (ez + blk.z - 1) / blk.z);
+}
+
+// Is u face f computed (not locked, not the periodic duplicate)?
+__device__ __forceinline__ bool face_live(int f, int n, int periodic) {
+  return periodic ? (f < n) : (f > 0 && f < n);
+}
+
+// cotangent of the u row at face f as seen by its computation (the periodic
+// face n row is a copy of face 0)
+template <typename T>
+__device__ __forceinline__ T ybar_u(const Dims& d, const T* __restrict__ yu, T ys, int f, int j, int k) {
+  T y = ld(yu, iu(d, f, j, k)) * ys;
+  if (d.px && f == 0) y += ld(yu, iu(d, d.nx, j, k)) * ys;
+  return y;
+}
+template <typename T>
+__device__ __forceinline__ T ybar_v(const Dims& d, const T* __restrict__ yv, T ys, int i, int f, int k) {
+  T y = ld(yv, iv(d, i, f, k)) * ys;
+  if (d.py && f == 0) y += ld(yv, iv(d, i, d.ny, k)) * ys;
+  return y;
+}
+
+// Stage 1: gbar_zm(i, j, k) = sum over the live faces whose gradient reads
+// column (i, j) at mass level k of -adt cp th zx / 2 * ybar.
+template <typename T>
+__global__ void at_gzm_kernel(Dims d, Coef<T> c, const T* __restrict__ yu, const T* __restrict__ yv, const double* yscale,
+                              T* __restrict__ gzm, const int* active) {
+  if (active && *active == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny;
+  if (i >= nx || j >= ny || k >= d.nz) return;
+  const T ys = yscale ? (T)(*yscale) : T(1);
+  const T coef = -(T)(c.s.alpha * c.s.dt * c.s.cp) * T(0.5);
+  T g = T(0);
+  // u faces: column i is the right column of face i and the left column of face i+1
+  // (periodic: the left column of face 0 is nx-1)
+  if (face_live(i, nx, d.px)) {
+    const int p = iu(d, i, j, k);
+    g += coef * ld(c.thu, p) * ld(c.zxu, p) * ybar_u(d, yu, ys, i, j, k);
+  }
+  {
+    const int f = (i + 1 < nx) ? i + 1 : (d.px ? 0 : -1);
+    if (f >= 0 && face_live(f, nx, d.px)) {
+      const int p = iu(d, f, j, k);
+      g += coef * ld(c.thu, p) * ld(c.zxu, p) * ybar_u(d, yu, ys, f, j, k);
+    }
+  }
+  if (face_live(j, ny, d.py)) {
+    const int p = iv(d, i, j, k);
+    g += coef * ld(c.thv, p) * ld(c.zev, p) * ybar_v(d, yv, ys, i, j, k);
+  }
+  {
+    const int f = (j + 1 < ny) ? j + 1 : (d.py ? 0 : -1);
+    if (f >= 0 && face_live(f, ny, d.py)) {
+      const int p = iv(d, i, f, k);
+      g += coef * ld(c.thv, p) * ld(c.zev, p) * ybar_v(d, yv, ys, i, f, k);
+    }
+  }
+  gzm[im(d, i, j, k)] = g;
+}
+
+// Stage 2: every input cotangent at a union-box point.
+template <typename T>
+__global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T> y, const double* yscale,
+                                                      const T* __restrict__ gzm, CVec5<T> b, Vec5<T> out,
+                                                      const int* active) {
+  if (active && *active == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i > nx || j > ny || k > nz) return;
+  const T ys = yscale ? (T)(*yscale) : T(1);
+  const T adt = (T)(c.s.alpha * c.s.dt), cp = (T)c.s.cp, a = (T)c.s.alpha, ps = (T)c.s.ps;
+  const T idx = (T)(1.0 / d.dx), idy = (T)(1.0 / d.dy);
+  const T* __restrict__ yu = y.f[0];
+  const T* __restrict__ yv = y.f[1];
+  const T* __restrict__ yw = y.f[2];
+  const T* __restrict__ yp = y.f[3];
+  const T* __restrict__ ye = y.f[4];
+  // q(cell) = adt ps cpidz ybar_p: the weight of the flux divergence of a cell
+  auto qcell = [&](int ci, int cj, int ck) {
+    const int p = im(d, ci, cj, ck);
+    return adt * ps * ld(c.cpidz, p) * ld(yp, p) * ys;
+  };
+  // ---------------- xbar_u at face (i, j, k) ----------------
+  if (j < ny && k < nz) {
+    const int p = iu(d, i, j, k);
+    T g = T(0);
+    // diagonal: every u row reads its own face; on a periodic axis the row n is a
+    // copy of row 0, so face 0 also collects the row-n cotangent and face n none
+    if (d.px) {
+      if (i < nx) g += ybar_u(d, yu, ys, i, j, k);
+    } else {
+      g += ld(yu, p) * ys;
+    }
+    // Coriolis: v face (ii, jj) averages u faces ii, ii+1 (read directly, the
+    // periodic duplicate included) on rows jj and jj-1 (wrapped when periodic)
+    const T w4 = adt * T(0.25);
+    for (int ii = i - 1; ii <= i; ++ii) {
+      if (ii < 0 || ii >= nx) continue;
+      for (int dj = 0; dj <= 1; ++dj) {
+        int jj = j + dj;
+        if (d.py && jj == ny) jj = 0;
+        if (!face_live(jj, ny, d.py)) continue;
+        g += w4 * ld(c.fv, h_v(d, ii, jj)) * ybar_v(d, yv, ys, ii, jj, k);
+      }
+    }
+    // kinematic term of the eta rows of cells i' in {i-1, i} at w levels k, k+1
+    for (int di = -1; di <= 0; ++di) {
+      const int ii = i + di;
+      if (ii < 0 || ii >= nx) continue;
+      for (int kk = k; kk <= k + 1; ++kk) {
+        if (kk <= 0 || kk >= nz) continue;
+        const int pw = iw(d, ii, j, kk);
+        g += a * T(0.25) * ld(c.mm, h_m(d, ii, j)) * ld(c.zxw, pw) * ld(ye, pw) * ys;
+      }
+    }
+    // flux of the pi rows: face i is the east face of cell i-1 and the west face of cell i
+    {
+      const T m_f = ld(c.rdu, p) * ld(c.thu, p) * idx;
+      T acc = T(0);
+      if (i - 1 >= 0) { const T m = ld(c.mm, h_m(d, i - 1, j)); acc += m * m * qcell(i - 1, j, k); }
+      if (i < nx) { const T m = ld(c.mm, h_m(d, i, j)); acc -= m * m * qcell(i, j, k); }
+      g += m_f * acc;
+    }
+    T r = g;
+    if (b.f[0]) r = ld(b.f[0], p) - r;
+    out.f[0][p] = r;
+  }
+  // ---------------- xbar_v at face (i, j, k) ----------------
+  if (i < nx && k < nz) {
+    const int p = iv(d, i, j, k);
+    T g = T(0);
+    if (d.py) {
+      if (j < ny) g += ybar_v(d, yv, ys, i, j, k);
+    } else {
+      g += ld(yv, p) * ys;
+    }
+    // Coriolis: u face (ii, jj) averages v faces jj, jj+1 (read directly) on
+    // columns ii and ii-1 (wrapped when periodic)
+    const T w4 = -adt * T(0.25);
+    for (int jj = j - 1; jj <= j; ++jj) {
+      if (jj < 0 || jj >= ny) continue;
+      for (int di = 0; di <= 1; ++di) {
+        int ii = i + di;
+        if (d.px && ii == nx) ii = 0;
+        if (!face_live(ii, nx, d.px)) continue;
+        g += w4 * ld(c.fu, h_u(d, ii, jj)) * ybar_u(d, yu, ys, ii, jj, k);
+      }
+    }
+    for (int dj = -1; dj <= 0; ++dj) {
+      const int jj = j + dj;
+      if (jj < 0 || jj >= ny) continue;
+      for (int kk = k; kk <= k + 1; ++kk) {
+        if (kk <= 0 || kk >= nz) continue;
+        const int pw = iw(d, i, jj, kk);
+        g += a * T(0.25) * ld(c.mm, h_m(d, i, jj)) * ld(c.zew, pw) * ld(ye, pw) * ys;
+      }
+    }
+    {
+      const T m_f = ld(c.rdv, p) * ld(c.thv, p) * idy;
+      T acc = T(0);
+      if (j - 1 >= 0) { const T m = ld(c.mm, h_m(d, i, j - 1)); acc += m * m * qcell(i, j - 1, k); }
+      if (j < ny) { const T m = ld(c.mm, h_m(d, i, j)); acc -= m * m * qcell(i, j, k); }
+      g += m_f * acc;
+    }
+    T r = g;
+    if (b.f[1]) r = ld(b.f[1], p) - r;
+    out.f[1][p] = r;
+  }
+  if (i >= nx || j >= ny) return;
+  // ---------------- xbar_w and xbar_W at w level k ----------------
+  {
+    const int p = iw(d, i, j, k);
+    const bool inner = (k > 0 && k < nz);
+    const T ye_k = ld(ye, p) * ys, yw_k = ld(yw, p) * ys;
+    T gw = inner ? ld(c.damp, p) * yw_k - a * ye_k : yw_k;
+    T gW = inner ? a * ye_k : ld(c.idzw, p) * ye_k;
+    if (inner) gW += ld(c.rhow, p) * ld(c.thw, p) * (qcell(i, j, k - 1) - qcell(i, j, k));
+    if (b.f[2]) { gw = ld(b.f[2], p) - gw; gW = ld(b.f[4], p) - gW; }
+    out.f[2][p] = gw;
+    out.f[4][p] = gW;
+  }
+  if (k >= nz) return;
+  // ---------------- xbar_p at mass point (i, j, k) ----------------
+  {
+    const int p = im(d, i, j, k);
+    T gP = T(0);  // cotangent of P = p / ps
+    // horizontal gradients: column (i, j) is the right column of face i and the
+    // left column of face i+1 (periodic: of face 0 when i = nx-1)
+    if (face_live(i, nx, d.px)) {
+      const int pu = iu(d, i, j, k);
+      gP += adt * cp * ld(c.thu, pu) * ld(c.mu, h_u(d, i, j)) * idx * ybar_u(d, yu, ys, i, j, k);
+    }
+    {
+      const int f = (i + 1 < nx) ? i + 1 : (d.px ? 0 : -1);
+      if (f >= 0 && face_live(f, nx, d.px)) {
+        const int pu = iu(d, f, j, k);
+        gP -= adt * cp * ld(c.thu, pu) * ld(c.mu, h_u(d, f, j)) * idx * ybar_u(d, yu, ys, f, j, k);
+      }
+    }
+    if (face_live(j, ny, d.py)) {
+      const int pv = iv(d, i, j, k);
+      gP += adt * cp * ld(c.thv, pv) * ld(c.mv, h_v(d, i, j)) * idy * ybar_v(d, yv, ys, i, j, k);
+    }
+    {
+      const int f = (j + 1 < ny) ? j + 1 : (d.py ? 0 : -1);
+      if (f >= 0 && face_live(f, ny, d.py)) {
+        const int pv = iv(d, i, f, k);
+        gP -= adt * cp * ld(c.thv, pv) * ld(c.mv, h_v(d, i, f)) * idy * ybar_v(d, yv, ys, i, f, k);
+      }
+    }
+    // vertical gradient: gbar_zw(kk) idzw(kk) with the padded level pairs
+    auto gzwbar = [&](int kk) -> T {  // times idzw
+      const int pw = iw(d, i, j, kk);
+      T g = T(0);
+      if (kk - 1 >= 0) g += T(0.5) * ld(gzm, im(d, i, j, kk - 1));
+      if (kk < nz) g += T(0.5) * ld(gzm, im(d, i, j, kk));
+      if (kk > 0 && kk < nz) g += adt * cp * ld(c.thw, pw) * ld(yw, pw) * ys;
+      return g * ld(c.idzw, pw);
+    };
+    if (k >= 1) gP += gzwbar(k);
+    if (k + 1 <= nz - 1) gP -= gzwbar(k + 1);
+    if (k == 1) gP += gzwbar(0);
+    if (k == 0) gP -= gzwbar(0);
+    if (k == nz - 1) gP += gzwbar(nz);
+    if (k == nz - 2) gP -= gzwbar(nz);
+    T r = ld(yp, p) * ys + gP / ps;
+    if (b.f[3]) r = ld(b.f[3], p) - r;
+    out.f[3][p] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// M^T, column part: one thread per column.  With ybar the output cotangent
+// (ybar_pi = y_pi * ps on the unscaled pressure):
+//   G(K)   = -adt cp thw (yw + yW) idzw / damp at interior w levels, else 0
+//   pibar  = ybar_pi + G(k) - G(k+1)
+//   z      = T^-T pibar   (T: the Helmholtz tridiagonal of the forward)
+//   out_pi = z / ps,   divbar = -L_pi z
+//   wtbar(K) = divbar(K-1) - divbar(K),  epbar = yW + rho_w thw wtbar
+//   out_W  = epbar / alpha,  out_w = (yw + epbar) / damp  (interior levels)
+//   out_W  = yW dz_w,        out_w = yw                   (ground and lid)
+// The elimination factors c' and d' are parked in out_w and out_pi.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) pt_column_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
+                                                        const int* active) {
+  if (active && *active == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i >= nx || j >= ny) return;
+  const int pm = nx * ny, h = i + nx * j;
+  const T ps = (T)c.s.ps, ips = (T)(1.0 / c.s.ps), a = (T)c.s.alpha;
+  const T adtcp = (T)(c.s.alpha * c.s.dt * c.s.cp);
+  const T* __restrict__ yw = y.f[2];
+  const T* __restrict__ yp = y.f[3];
+  const T* __restrict__ yW = y.f[4];
+  T* __restrict__ ow = out.f[2];
+  T* __restrict__ op = out.f[3];
+  T* __restrict__ oW = out.f[4];
+  // w-level coupling P(K) = adt cp thw idzw / damp * rho_w thw (0 on ground and lid)
+  auto Pw = [&](int K) -> T {
+    if (K <= 0 || K >= nz) return T(0);
+    const int p = h + K * pm;
+    const T thw = ld(c.thw, p);
+    return adtcp * thw * ld(c.idzw, p) / ld(c.damp, p) * ld(c.rhow, p) * thw;
+  };
+  auto Gw = [&](int K) -> T {
+    if (K <= 0 || K >= nz) return T(0);
+    const int p = h + K * pm;
+    return -adtcp * ld(c.thw, p) * (ld(yw, p) + ld(yW, p)) * ld(c.idzw, p) / ld(c.damp, p);
+  };
+  // forward elimination of T^T: sub(k) = -L(k-1) P(k), sup(k) = -L(k+1) P(k+1),
+  // main(k) = 1 + L(k) (P(k) + P(k+1))
+  T cprev = T(0), dprev = T(0), Lprev = T(0);
+  T Pk = T(0), Gk = T(0);
+  for (int k = 0; k < nz; ++k) {
+    const int p = h + k * pm;
+    const T L = ld(c.lpi, p);
+    const T Pk1 = Pw(k + 1), Gk1 = Gw(k + 1);
+    const T Lnext = (k + 1 < nz) ? ld(c.lpi, p + pm) : T(0);
+    const T sub = -Lprev * Pk, sup = -Lnext * Pk1, mn = T(1) + L * (Pk + Pk1);
+    const T pib = ld(yp, p) * ps + Gk - Gk1;
+    const T inv = T(1) / (mn - sub * cprev);
+    cprev = sup * inv;
+    dprev = (pib - sub * dprev) * inv;
+    ow[p] = cprev;
+    op[p] = dprev;
+    Lprev = L;
+    Pk = Pk1;
+    Gk = Gk1;
+  }
+  // back substitution, finishing w level K = k + 1 on the way down
+  T znext = T(0), dvnext = T(0);
+  for (int k = nz - 1; k >= 0; --k) {
+    const int p = h + k * pm;
+    const T z = (k == nz - 1) ? op[p] : op[p] - ow[p] * znext;
+    op[p] = z * ips;
+    const T dv = -ld(c.lpi, p) * z;
+    if (k + 1 < nz) {
+      const int pw = p + pm;
+      const T wtb = dv - dvnext;
+      const T ep = ld(yW, pw) + ld(c.rhow, pw) * ld(c.thw, pw) * wtb;
+      oW[pw] = ep / a;
+      ow[pw] = (ld(yw, pw) + ep) / ld(c.damp, pw);
+    }
+    znext = z;
+    dvnext = dv;
+  }
+  ow[h] = ld(yw, h);
+  oW[h] = ld(yW, h) * ld(c.dzw, h);
+  const int pt = h + nz * pm;
+  ow[pt] = ld(yw, pt);
+  oW[pt] = ld(yW, pt) * ld(c.dzw, pt);
+}
+
+// M^T, horizontal part: out_u = y_u + sum of the kinematic cotangent
+// kinbar = -alpha out_W over the interior w levels of the adjacent cells.
+template <typename T>
+__global__ void __launch_bounds__(256) pt_uv_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out, const int* active) {
+  if (active && *active == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i > nx || j > ny || k >= nz) return;
+  const T qa = -(T)c.s.alpha * T(0.25);
+  const T* __restrict__ oW = out.f[4];
+  if (j < ny) {
+    const int p = iu(d, i, j, k);
+    T g = ld(y.f[0], p);
+    for (int ii = i - 1; ii <= i; ++ii) {
+      if (ii < 0 || ii >= nx) continue;
+      const T m = ld(c.mm, h_m(d, ii, j));
+      for (int K = k; K <= k + 1; ++K) {
+        if (K <= 0 || K >= nz) continue;
+        const int pw = iw(d, ii, j, K);
+        g += qa * m * ld(c.zxw, pw) * oW[pw];
+      }
+    }
+    out.f[0][p] = g;
+  }
+  if (i < nx) {
+    const int p = iv(d, i, j, k);
+    T g = ld(y.f[1], p);
+    for (int jj = j - 1; jj <= j; ++jj) {
+      if (jj < 0 || jj >= ny) continue;
+      const T m = ld(c.mm, h_m(d, i, jj));
+      for (int K = k; K <= k + 1; ++K) {
+        if (K <= 0 || K >= nz) continue;
+        const int pw = iw(d, i, jj, K);
+        g += qa * m * ld(c.zew, pw) * oW[pw];
+      }
+    }
+    out.f[1][p] = g;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tricubic VJP (cotangent of the field; the departure points carry none,
+// steppers.py:764-767): every destination point scatters its cotangent with
+// the 64 Catmull-Rom weights of tensor_product_interp_3d
+// (operators.py:146-209).  With the limiter, jnp.clip(f, lo, hi) and the
+// min/max chains over the 8 cell corners in the reference order route the
+// cotangent as lax.min/lax.max do: all of it to the strictly smaller
+// (larger) operand, half to each on a tie.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void cr_w(T t, T (&w)[4]) {
+  w[0] = t * (T(-0.5) + t * (T(1) - T(0.5) * t));
+  w[1] = T(1) + t * t * (T(-2.5) + T(1.5) * t);
+  w[2] = t * (T(0.5) + t * (T(2) - T(1.5) * t));
+  w[3] = t * t * (T(-0.5) + T(0.5) * t);
+}
+
+__device__ __forceinline__ void atomic_acc(float* a, float v) { atomicAdd(a, v); }
+__device__ __forceinline__ void atomic_acc(double* a, double v) { atomicAdd(a, v); }
+
+// share of the cotangent of op(a, b) that goes to a: 1, 0 or 1/2 on a tie
+template <typename T>
+__device__ __forceinline__ T share_min(T a, T b) { return a < b ? T(1) : (a > b ? T(0) : T(0.5)); }
+template <typename T>
+__device__ __forceinline__ T share_max(T a, T b) { return a > b ? T(1) : (a < b ? T(0) : T(0.5)); }
+
+template <typename T>
+__global__ void __launch_bounds__(256) tricubic_vjp_kernel(int sx, int sy, int sz, int dx, int dy, int dz,
+                                                           const T* __restrict__ f, const T* __restrict__ cx,
+                                                           const T* __restrict__ cy, const T* __restrict__ cz,
+                                                           const T* __restrict__ cot, T* grad, int limiter,
+                                                           T scale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= dx || j >= dy || k >= dz) return;
+  const int p = i + dx * (j + dy * k);
+  const T g = scale * ld(cot, p);
+  if (g == T(0)) return;
+  const T x = fmin(fmax(ld(cx, p), T(0)), (T)(sx - 1));
+  const T y = fmin(fmax(ld(cy, p), T(0)), (T)(sy - 1));
+  const T z = fmin(fmax(ld(cz, p), T(0)), (T)(sz - 1));
+  const int x0 = (int)floor(x), y0 = (int)floor(y), z0 = (int)floor(z);
+  T wx[4], wy[4], wz[4];
+  cr_w(x - (T)x0, wx);
+  cr_w(y - (T)y0, wy);
+  cr_w(z - (T)z0, wz);
+  const int ix[4] = {max(x0 - 1, 0), x0, min(x0 + 1, sx - 1), min(x0 + 2, sx - 1)};
+  const int iy[4] = {max(y0 - 1, 0), y0, min(y0 + 1, sy - 1), min(y0 + 2, sy - 1)};
+  const int iz[4] = {max(z0 - 1, 0), z0, min(z0 + 1, sz - 1), min(z0 + 2, sz - 1)};
+  const int plane = sx * sy;
+  T gf = g;
+  if (limiter) {
+    T fi = T(0);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      T syv = T(0);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int row = ix[a] + sx * iy[b];
+        T szv = T(0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) szv += wz[q] * ld(f, row + plane * iz[q]);
+        syv += wy[b] * szv;
+      }
+      fi += wx[a] * syv;
+    }
+    const int x1 = min(x0 + 1, sx - 1), y1 = min(y0 + 1, sy - 1), z1 = min(z0 + 1, sz - 1);
+    // corners in the reference order (operators.py:200-201)
+    const int cidx[8] = {x0 + sx * (y0 + sy * z0), x1 + sx * (y0 + sy * z0), x0 + sx * (y1 + sy * z0),
+                         x1 + sx * (y1 + sy * z0), x0 + sx * (y0 + sy * z1), x1 + sx * (y0 + sy * z1),
+                         x0 + sx * (y1 + sy * z1), x1 + sx * (y1 + sy * z1)};
+    T nb[8], mn[8], mx[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) nb[s] = ld(f, cidx[s]);
+    mn[0] = mx[0] = nb[0];
+#pragma unroll
+    for (int s = 1; s < 8; ++s) {
+      mn[s] = fmin(mn[s - 1], nb[s]);
+      mx[s] = fmax(mx[s - 1], nb[s]);
+    }
+    // jnp.clip(f, lo, hi) = minimum(hi, maximum(lo, f))
+    const T lo = mn[7], hi = mx[7];
+    const T v1 = fmax(lo, fi);
+    const T a1 = share_max(fi, lo);  // to f
+    const T a2 = share_min(v1, hi);  // to maximum(lo, f)
+    gf = g * a2 * a1;
+    T glo = g * a2 * (T(1) - a1), ghi = g * (T(1) - a2);
+    T gn[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) gn[s] = T(0);
+#pragma unroll
+    for (int s = 7; s >= 1; --s) {
+      const T wl = share_min(mn[s - 1], nb[s]);
+      gn[s] += glo * (T(1) - wl);
+      glo *= wl;
+      const T wh = share_max(mx[s - 1], nb[s]);
+      gn[s] += ghi * (T(1) - wh);
+      ghi *= wh;
+    }
+    gn[0] += glo + ghi;
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+      if (gn[s] != T(0)) atomic_acc(grad + cidx[s], gn[s]);
+    if (gf == T(0)) return;
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const T ga = gf * wx[a];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int row = ix[a] + sx * iy[b];
+      const T gb = ga * wy[b];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) atomic_acc(grad + row + plane * iz[q], gb * wz[q]);
+    }
+  }
+}
+
+}  // namespace
+
+// grad += scale * (d tricubic / d field)^T cot
+template <typename T>
+void launch_tricubic_vjp(int sx, int sy, int sz, int dx, int dy, int dz, const T* field, const T* const* coords3,
+                         const T* cot, T* grad, int use_limiter, T scale, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  tricubic_vjp_kernel<T><<<box_grid(dx, dy, dz, blk), blk, 0, st>>>(sx, sy, sz, dx, dy, dz, field, coords3[0],
+                                                                    coords3[1], coords3[2], cot, grad,
+                                                                    use_limiter, scale);
+}
+template void launch_tricubic_vjp<float>(int, int, int, int, int, int, const float*, const float* const*,
+                                         const float*, float*, int, float, cudaStream_t);
+template void launch_tricubic_vjp<double>(int, int, int, int, int, int, const double*, const double* const*,
+                                          const double*, double*, int, double, cudaStream_t);
+
+// out = M^T y (out must not alias y).
+template <typename T>
+void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
+                      cudaStream_t st) {
+  pt_column_kernel<T><<<dim3((d.nx + 127) / 128, d.ny), 128, 0, st>>>(d, c, y, out, active);
+  dim3 blk(32, 4, 2);
+  pt_uv_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz, blk), blk, 0, st>>>(d, c, y, out, active);
+}
+
+template void launch_precond_t<float>(const Dims&, const Coef<float>&, CVec5<float>, Vec5<float>, const int*,
+                                      cudaStream_t);
+template void launch_precond_t<double>(const Dims&, const Coef<double>&, CVec5<double>, Vec5<double>, const int*,
+                                       cudaStream_t);
+
+// out = A^T (y * yscale), or out = b - A^T(...) when b is given; gzm_tmp is a
+// mass-point scratch field.
+template <typename T>
+void launch_matvec_t(const Dims& d, const Coef<T>& c, CVec5<T> y, const double* yscale, CVec5<T> b, Vec5<T> out,
+                     T* gzm_tmp, const int* active, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  at_gzm_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, c, y.f[0], y.f[1], yscale, gzm_tmp, active);
+  at_main_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, y, yscale, gzm_tmp, b, out,
+                                                                              active);
+}
+
+template void launch_matvec_t<float>(const Dims&, const Coef<float>&, CVec5<float>, const double*, CVec5<float>,
+                                     Vec5<float>, float*, const int*, cudaStream_t);
+template void launch_matvec_t<double>(const Dims&, const Coef<double>&, CVec5<double>, const double*, CVec5<double>,
+                                      Vec5<double>, double*, const int*, cudaStream_t);
+
+}  // namespace sisl

@@ -176,6 +176,7 @@ struct GWork {
   GHostView* dview;  // device copy of the per-cycle summary
   double* partial;
   T* vec;  // (R + 4) contiguous vectors
+  T* tmp;  // mass-point scratch of the transposed matvec
   size_t npad;
   size_t off[5], sz[5];
   int R;
@@ -216,6 +217,7 @@ GWork<T> carve_gmres(Carver& cv, const Dims& d, int R) {
   g.dview = (GHostView*)cv.take(sizeof(GHostView));
   g.partial = (double*)cv.take(sizeof(double) * GM_MAXBLOCKS * (GM_MAXR + 2));
   g.vec = (T*)cv.take(sizeof(T) * g.npad * (size_t)(R + 4));
+  g.tmp = (T*)cv.take(sizeof(T) * field_size(d, LOC_M));
   return g;
 }
 
@@ -264,8 +266,11 @@ double precond_bytes(const Dims& d, size_t es) {
 }
 
 // Restarted GMRES on the packed vectors g.bg (rhs) and g.xg (initial guess).
+// transpose = 1 runs the same iteration on A^T with the preconditioner M^T
+// (the bwd_solve of steppers.py:473-481).
 template <typename T>
-int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, SislSolveInfo* info) {
+int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, SislSolveInfo* info,
+              int transpose = 0) {
   const Dims& d = c->d;
   const int R = g.R;
   const size_t n = g.npad;
@@ -283,10 +288,26 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
     KScope k(c, SISL_K_DOTS, st);
     gm_dots<T>(g.V(0), n, 0, g.bg(), n, g.partial, gs, 1 /*BNORM*/, 0, st);
   }
+  // z-space operators: forward A writes its u, v rows straight into the
+  // target vector (the preconditioner passes u, v through unchanged,
+  // steppers.py:247-249); the transposes go through z in full
+  auto apply_A = [&](const T* x, const double* xs, CVec5<T> b, T* target, const int* act) {
+    if (transpose) launch_matvec_t<T>(d, cf, g.cview(x), xs, b, g.view(g.z()), g.tmp, act, st);
+    else launch_matvec<T>(d, cf, g.cview(x), xs, b, g.split(target, g.z()), act, st);
+  };
+  auto apply_M = [&](const T* src_full, T* target, const int* act) {
+    if (transpose) launch_precond_t<T>(d, cf, g.cview(src_full), g.view(target), act, st);
+    else launch_precond<T>(d, cf, g.cview(src_full), g.view(target), act, st);
+  };
+  auto apply_M_after_A = [&](T* target, const int* act) {
+    if (transpose) launch_precond_t<T>(d, cf, g.cview(g.z()), g.view(target), act, st);
+    else launch_precond<T>(d, cf, as_const(g.split(target, g.z())), g.view(target), act, st);
+  };
+  const int na = transpose ? 2 : 1, nm = transpose ? 2 : 1;
   if (method == SISL_GMRES_INCREMENTAL) {
     {
-      KScope k(c, SISL_K_PRECOND, st);
-      launch_precond<T>(d, cf, g.cview(g.bg()), g.view(g.V(1)), nullptr, st);
+      KScope k(c, SISL_K_PRECOND, st, nm);
+      apply_M(g.bg(), g.V(1), nullptr);
     }
     KScope k(c, SISL_K_DOTS, st);
     gm_dots<T>(g.V(0), n, 0, g.V(1), n, g.partial, gs, 2 /*MBNORM*/, 0, st);
@@ -297,14 +318,13 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
   }
   // residual of the initial guess
   auto residual_and_read = [&](GHostView* out) -> int {
-    const Vec5<T> az = g.split(g.V(0), g.z());
     {
-      KScope k(c, SISL_K_MATVEC, st);
-      launch_matvec<T>(d, cf, g.cview(g.xg()), nullptr, g.cview(g.bg()), az, nullptr, st);
+      KScope k(c, SISL_K_MATVEC, st, na);
+      apply_A(g.xg(), nullptr, g.cview(g.bg()), g.V(0), nullptr);
     }
     {
-      KScope k(c, SISL_K_PRECOND, st);
-      launch_precond<T>(d, cf, as_const(az), g.view(g.V(0)), nullptr, st);
+      KScope k(c, SISL_K_PRECOND, st, nm);
+      apply_M_after_A(g.V(0), nullptr);
     }
     {
       KScope k(c, SISL_K_DOTS, st);
@@ -329,16 +349,13 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
       gm_begin_cycle(gs, st);
     }
     for (int j = 0; j < R; ++j) {
-      // A writes its u, v rows straight into the next basis vector: the
-      // preconditioner passes u, v through unchanged (steppers.py:247-249)
-      const Vec5<T> az = g.split(g.V(j + 1), g.z());
       {
-        KScope k(c, SISL_K_MATVEC, st, 1, mvb);
-        launch_matvec<T>(d, cf, g.cview(g.V(j)), &gs->s[j], none, az, &gs->active, st);
+        KScope k(c, SISL_K_MATVEC, st, na, mvb);
+        apply_A(g.V(j), &gs->s[j], none, g.V(j + 1), &gs->active);
       }
       {
-        KScope k(c, SISL_K_PRECOND, st, 1, pcb);
-        launch_precond<T>(d, cf, as_const(az), g.view(g.V(j + 1)), &gs->active, st);
+        KScope k(c, SISL_K_PRECOND, st, nm, pcb);
+        apply_M_after_A(g.V(j + 1), &gs->active);
       }
       {
         KScope k(c, SISL_K_DOTS, st, 1, vb * (j + 2));  // reads V_0..V_j and w
@@ -395,6 +412,28 @@ int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, co
   return rc;
 }
 
+// Cotangent of the physical right-hand side from the cotangent of the
+// physical solution (custom_linear_solve transpose, steppers.py:473-485):
+// unscale (x = S_out x_s), GMRES on A^T from a zero guess, rescale (b_s = S_in b).
+template <typename T>
+int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> xbar, Vec5<T> bbar,
+                             cudaStream_t st, SislSolveInfo* info) {
+  const Dims& d = c->d;
+  {
+    KScope k(c, SISL_K_OTHER, st);
+    zero_gaps_kernel<T><<<g.R + 4, 256, 0, st>>>(g.vec, g.npad, g.R + 4, g.off[0], g.off[1], g.off[2], g.off[3],
+                                                g.off[4], g.sz[0], g.sz[1], g.sz[2], g.sz[3], g.sz[4]);
+  }
+  const T ps = (T)c->s.ps;
+  scale5<T>(c, cf, xbar, g.view(g.bg()), (T)(1.0 / c->s.ps), 2, st);  // pi / ps, eta / dz_w
+  if (cudaMemsetAsync(g.xg(), 0, sizeof(T) * g.npad, st) != cudaSuccess) return SISL_ERR_CUDA;
+  int rc = gmres_run<T>(c, cf, g, st, info, 1);
+  if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+  scale5<T>(c, cf, g.cview(g.xg()), bbar, ps, 0, st);  // pi * ps
+  (void)d;
+  return rc;
+}
+
 // ---------------------------------------------------------------------------
 // step workspace
 // ---------------------------------------------------------------------------
@@ -430,7 +469,7 @@ SWork<T> carve_step(Carver& cv, const Dims& d, int R) {
 
 template <typename T>
 int step_impl(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
-              size_t ws_bytes, cudaStream_t st, SislStepInfo* info) {
+              size_t ws_bytes, cudaStream_t st, SislStepInfo* info, void* const* tape = nullptr) {
   const Dims& d = c->d;
   const Coef<T> cf = coef_of<T>(c);
   Carver cv{(char*)ws};
@@ -541,6 +580,14 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
     int rc = solve_physical<T>(c, cf, w.g, as_const(rk), &x0, xs, st, &si);
     if (info) info->solve[it] = si;
     if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+    if (tape) {  // the physical solution of this solve, for the recomputation of the VJP
+      static const int L5[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_W};
+      for (int q = 0; q < 5; ++q)
+        if (tape[5 * it + q] &&
+            cudaMemcpyAsync(tape[5 * it + q], xs.f[q], sizeof(T) * field_size(d, L5[q]), cudaMemcpyDeviceToDevice,
+                            st) != cudaSuccess)
+          return SISL_ERR_CUDA;
+    }
     if (rc != SISL_OK && status == SISL_OK) status = rc;
   }
   // 5. divergence damping, bc_fn relaxation, EOS (steppers.py:1022-1056)
@@ -787,6 +834,54 @@ int sisl_gmres_solve(SislCore* c, const void* const rhs[5], const void* const x0
   return e ? e : rc;
 }
 
+int sisl_helmholtz_matvec_t(SislCore* c, const void* const in[5], void* const out[5], void* ws, size_t ws_bytes,
+                            void* stream) {
+  if (!c || !in || !out) return SISL_ERR_ARG;
+  for (int q = 0; q < 5; ++q)
+    if (in[q] == out[q]) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_OPERATOR)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(c, SISL_K_MATVEC, st, 2);
+  if (c->grid.dtype == SISL_F64)
+    launch_matvec_t<double>(c->d, coef_of<double>(c), cvec<double>(in), nullptr, CVec5<double>{}, vec<double>(out),
+                            (double*)ws, nullptr, st);
+  else
+    launch_matvec_t<float>(c->d, coef_of<float>(c), cvec<float>(in), nullptr, CVec5<float>{}, vec<float>(out),
+                           (float*)ws, nullptr, st);
+  return check_cuda();
+}
+
+int sisl_precond_apply_t(SislCore* c, const void* const in[5], void* const out[5], void* stream) {
+  if (!c || !in || !out) return SISL_ERR_ARG;
+  for (int q = 0; q < 5; ++q)
+    if (in[q] == out[q]) return SISL_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(c, SISL_K_PRECOND, st, 2);
+  if (c->grid.dtype == SISL_F64)
+    launch_precond_t<double>(c->d, coef_of<double>(c), cvec<double>(in), vec<double>(out), nullptr, st);
+  else
+    launch_precond_t<float>(c->d, coef_of<float>(c), cvec<float>(in), vec<float>(out), nullptr, st);
+  return check_cuda();
+}
+
+int sisl_gmres_solve_transpose(SislCore* c, const void* const xbar[5], void* const bbar[5], void* ws,
+                               size_t ws_bytes, void* stream, SislSolveInfo* info) {
+  if (!c || !xbar || !bbar) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_GMRES)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv{(char*)ws};
+  int rc;
+  if (c->grid.dtype == SISL_F64) {
+    GWork<double> g = carve_gmres<double>(cv, c->d, c->prm.solver_restart);
+    rc = solve_transpose_physical<double>(c, coef_of<double>(c), g, cvec<double>(xbar), vec<double>(bbar), st, info);
+  } else {
+    GWork<float> g = carve_gmres<float>(cv, c->d, c->prm.solver_restart);
+    rc = solve_transpose_physical<float>(c, coef_of<float>(c), g, cvec<float>(xbar), vec<float>(bbar), st, info);
+  }
+  int e = check_cuda();
+  return e ? e : rc;
+}
+
 int sisl_departure(SislCore* c, int loc, const void* u, const void* v, const void* eta, int iterations,
                    void* const coords[3], void* ws, size_t ws_bytes, void* stream) {
   if (!c || loc < 0 || loc > 3 || !u || !v || !eta || !coords || iterations < 0) return SISL_ERR_ARG;
@@ -832,6 +927,52 @@ int sisl_tricubic(int dtype, const int32_t src[3], const void* field, const int3
   } else {
     return SISL_ERR_ARG;
   }
+  return check_cuda();
+}
+
+int sisl_tricubic_vjp(int dtype, const int32_t src[3], const void* field, const int32_t dst[3],
+                      const void* const coords[3], const void* cot, void* grad, int use_limiter, double scale,
+                      void* stream) {
+  if (!src || !dst || !coords || !cot || !grad || (use_limiter && !field)) return SISL_ERR_ARG;
+  for (int q = 0; q < 3; ++q)
+    if (src[q] < 1 || dst[q] < 0) return SISL_ERR_ARG;
+  if ((int64_t)dst[0] * dst[1] * dst[2] == 0) return SISL_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(nullptr, SISL_K_SL, st);
+  if (dtype == SISL_F64) {
+    const double* co[3] = {(const double*)coords[0], (const double*)coords[1], (const double*)coords[2]};
+    launch_tricubic_vjp<double>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const double*)field, co,
+                                (const double*)cot, (double*)grad, use_limiter, scale, st);
+  } else if (dtype == SISL_F32) {
+    const float* co[3] = {(const float*)coords[0], (const float*)coords[1], (const float*)coords[2]};
+    launch_tricubic_vjp<float>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const float*)field, co,
+                               (const float*)cot, (float*)grad, use_limiter, (float)scale, st);
+  } else {
+    return SISL_ERR_ARG;
+  }
+  return check_cuda();
+}
+
+int sisl_stagger(int dtype, int op, const int32_t in_shape[3], int axis, int to_face, int periodic, int stop_grad,
+                 int transpose, double inv_delta, const void* mult, const void* src, void* dst, void* stream) {
+  if (!in_shape || !src || !dst || axis < 0 || axis > 2 || (op != SISL_STAGGER_AVG && op != SISL_STAGGER_DIFF))
+    return SISL_ERR_ARG;
+  for (int q = 0; q < 3; ++q)
+    if (in_shape[q] < 1) return SISL_ERR_ARG;
+  if (in_shape[axis] < 2) return SISL_ERR_ARG;
+  if (periodic && (axis == 2 || !to_face)) periodic = 0;
+  const int sh[3] = {in_shape[0], in_shape[1], in_shape[2]};
+  const double c0 = op == SISL_STAGGER_AVG ? 0.5 : -inv_delta, c1 = op == SISL_STAGGER_AVG ? 0.5 : inv_delta;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(nullptr, SISL_K_EXPLICIT, st);
+  if (dtype == SISL_F64)
+    launch_stagger<double>(sh, axis, to_face ? 1 : 0, periodic ? 1 : 0, stop_grad ? 1 : 0, transpose ? 1 : 0, c0,
+                           c1, (const double*)mult, (const double*)src, (double*)dst, st);
+  else if (dtype == SISL_F32)
+    launch_stagger<float>(sh, axis, to_face ? 1 : 0, periodic ? 1 : 0, stop_grad ? 1 : 0, transpose ? 1 : 0,
+                          (float)c0, (float)c1, (const float*)mult, (const float*)src, (float*)dst, st);
+  else
+    return SISL_ERR_ARG;
   return check_cuda();
 }
 
@@ -916,6 +1057,11 @@ int sisl_tendencies(SislCore* c, int is_explicit, const void* const sp[6], void*
 
 int sisl_step(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
               size_t ws_bytes, void* stream, SislStepInfo* info) {
+  return sisl_step_taped(c, in, out, relax, nullptr, ws, ws_bytes, stream, info);
+}
+
+int sisl_step_taped(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax,
+                    void* const solves[10], void* ws, size_t ws_bytes, void* stream, SislStepInfo* info) {
   if (!c || !in || !out) return SISL_ERR_ARG;
   const void* need_in[] = {in->u, in->v, in->w, in->eta_dot, in->pi_p, in->th_p};
   for (const void* p : need_in)
@@ -926,8 +1072,8 @@ int sisl_step(SislCore* c, const SislState* in, const SislState* out, const Sisl
     if (!p) return SISL_ERR_ARG;
   if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_STEP)) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
-  if (c->grid.dtype == SISL_F64) return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info);
-  return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info);
+  if (c->grid.dtype == SISL_F64) return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info, solves);
+  return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info, solves);
 }
 
 int sisl_core_set_solver(SislCore* c, double tol, double atol, int maxiter, int restart, int method) {

@@ -84,6 +84,25 @@ template <typename T>
 void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                     cudaStream_t st);
 
+// transposes for the adjoint solve (sisl_adjoint.cu): out = A^T(y * ys), or
+// out = b - A^T(y * ys); gzm_tmp is a mass-point scratch field.  out = M^T y.
+template <typename T>
+void launch_matvec_t(const Dims& d, const Coef<T>& c, CVec5<T> y, const double* yscale, CVec5<T> b, Vec5<T> out,
+                     T* gzm_tmp, const int* active, cudaStream_t st);
+template <typename T>
+void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
+                      cudaStream_t st);
+
+// grad += scale * (d tricubic / d field)^T cot  (coordinates carry no cotangent)
+template <typename T>
+void launch_tricubic_vjp(int sx, int sy, int sz, int dx, int dy, int dz, const T* field, const T* const* coords3,
+                         const T* cot, T* grad, int use_limiter, T scale, cudaStream_t st);
+
+// staggered average / difference along one axis and its transpose (sisl_stagger.cu)
+template <typename T>
+void launch_stagger(const int in_shape[3], int axis, int to_face, int periodic, int stop_grad, int transpose, T c0,
+                    T c1, const T* mult, const T* src, T* dst, cudaStream_t st);
+
 // ---- semi-Lagrangian ----
 // vel.p[3*loc + 0..2] = index velocities (u m/dx, v m/dy, eta_dot) at stagger loc
 template <typename T>

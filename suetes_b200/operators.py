@@ -1,10 +1,13 @@
 """C-grid operators and the tricubic interpolator.
 
-``CGridOperator3D`` mirrors ``suetes/regional3d/operators.py:12-132``: its
-``diff``/``avg`` helpers are provided for user scripts (diagnostics, initial
-states) and run as plain tensor arithmetic; the step never calls them -- the
-CUDA kernels inline the same staggered stencils.  ``tensor_product_interp_3d``
-(operators.py:146-209) runs the sm_100a tricubic kernel.
+``CGridOperator3D`` mirrors ``suetes/regional3d/operators.py:12-132``: every
+``diff``/``avg`` runs the sm_100a staggered-stencil kernel and is
+differentiable, its backward being the transposed stencil, with the edge
+padding's ``stop_gradient`` honoured when ``use_stop_grad`` is set
+(operators.py:45-61).  ``tensor_product_interp_3d`` (operators.py:146-209)
+runs the tricubic kernel; its field cotangent is the scatter of the 64
+Catmull-Rom weights (the step stop-gradients the departure points,
+steppers.py:764-767).  CUDA tensors only: there is no CPU path.
 """
 
 import ctypes
@@ -14,6 +17,39 @@ import torch
 from . import _lib
 from ._lib import check
 from .core import DTYPE_CODE, empty_field, fortran, stream_ptr
+
+
+def _require_cuda(t, what):
+    if not torch.is_tensor(t) or t.device.type != "cuda":
+        raise RuntimeError(f"{what} runs on CUDA tensors only (no CPU path)")
+
+
+def _stagger_call(f, out, op, axis, to_face, periodic, stop_grad, transpose, inv_delta, mult, in_shape):
+    sh = (ctypes.c_int32 * 3)(*in_shape)
+    check(_lib.load().sisl_stagger(DTYPE_CODE[f.dtype], op, sh, axis, int(to_face), int(periodic), int(stop_grad),
+                                   int(transpose), float(inv_delta), mult.data_ptr() if mult is not None else None,
+                                   f.data_ptr(), out.data_ptr(), stream_ptr(f.device)), "sisl_stagger")
+
+
+class _Stagger(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, f, op, axis, to_face, periodic, stop_grad, inv_delta, mult):
+        f = fortran(f)
+        shape = list(f.shape)
+        oshape = list(shape)
+        oshape[axis] += 1 if to_face else -1
+        out = empty_field(tuple(oshape), f.dtype, f.device)
+        _stagger_call(f, out, op, axis, to_face, periodic, stop_grad, 0, inv_delta, mult, shape)
+        ctx.args = (op, axis, to_face, periodic, stop_grad, inv_delta, mult, shape)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        op, axis, to_face, periodic, stop_grad, inv_delta, mult, shape = ctx.args
+        g = fortran(g)
+        gin = empty_field(tuple(shape), g.dtype, g.device)
+        _stagger_call(g, gin, op, axis, to_face, periodic, stop_grad, 1, inv_delta, mult, shape)
+        return gin, None, None, None, None, None, None, None
 
 
 class CGridOperator3D:
@@ -26,32 +62,32 @@ class CGridOperator3D:
         self.periodic_axes = frozenset(periodic_axes)
         self.use_stop_grad = True
         self.m_factors = {loc: m[..., None] for loc, m in grid.m_factors.items()}
+        self._mult = {}
 
-    def _apply_padding(self, f, axis, from_loc, to_loc):
-        if from_loc == "m" and to_loc in ("u", "v", "w"):
-            n = f.shape[axis]
-            return torch.cat([f.narrow(axis, 0, 1), f, f.narrow(axis, n - 1, 1)], dim=axis)
-        return f
+    def _map_factor(self, loc, dtype):
+        key = (loc, dtype)
+        m = self._mult.get(key)
+        if m is None:
+            m = fortran(self.grid.m_factors[loc], dtype=dtype)
+            self._mult[key] = m
+        return m
+
+    def _apply(self, f, op, axis, from_loc, to_loc):
+        _require_cuda(f, "CGridOperator3D")
+        to_face = from_loc == "m" and to_loc in ("u", "v", "w")
+        periodic = axis in self.periodic_axes and from_loc == "m" and to_loc in ("u", "v")
+        mult = self._map_factor(to_loc, f.dtype) if (op == _lib.SISL_STAGGER_DIFF and axis in (0, 1)) else None
+        inv_delta = 1.0 / self.grid.delta[axis]
+        return _Stagger.apply(f, op, axis, to_face, periodic, self.use_stop_grad, inv_delta, mult)
 
     def diff(self, f, axis, from_loc, to_loc):
-        delta = self.grid.delta[axis]
-        d = torch.diff(f, dim=axis) / delta
-        if axis in self.periodic_axes and from_loc == "m" and to_loc in ("u", "v"):
-            b = ((f.select(axis, 0) - f.select(axis, f.shape[axis] - 1)) / delta).unsqueeze(axis)
-            d = torch.cat([b, d, b], dim=axis)
-        else:
-            d = self._apply_padding(d, axis, from_loc, to_loc)
-        if axis in (0, 1):
-            d = d * self.m_factors[to_loc].to(d.dtype)
-        return d
+        """``(f[i+1] - f[i]) / delta`` to the other stagger, edge-padded or
+        periodic, times the map factor on horizontal axes (operators.py:65-103)."""
+        return self._apply(f, _lib.SISL_STAGGER_DIFF, axis, from_loc, to_loc)
 
     def avg(self, f, axis, from_loc, to_loc):
-        n = f.shape[axis]
-        a = 0.5 * (f.narrow(axis, 0, n - 1) + f.narrow(axis, 1, n - 1))
-        if axis in self.periodic_axes and from_loc == "m" and to_loc in ("u", "v"):
-            b = (0.5 * (f.select(axis, 0) + f.select(axis, n - 1))).unsqueeze(axis)
-            return torch.cat([b, a, b], dim=axis)
-        return self._apply_padding(a, axis, from_loc, to_loc)
+        """Two-point average to the other stagger (operators.py:105-132)."""
+        return self._apply(f, _lib.SISL_STAGGER_AVG, axis, from_loc, to_loc)
 
 
 def _coords3(coords, dtype, device):
@@ -62,15 +98,58 @@ def _coords3(coords, dtype, device):
     return [fortran(c, dtype=dtype, device=device) for c in cs]
 
 
+class _Tricubic(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, field, use_limiter, scale, *cs):
+        out = _tricubic_fwd(field, cs, use_limiter)
+        if scale != 1.0:
+            out = out * scale
+        ctx.save_for_backward(field, *cs)
+        ctx.use_limiter, ctx.scale = use_limiter, scale
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        field, *cs = ctx.saved_tensors
+        grad = tricubic_vjp(field, cs, g, ctx.use_limiter, ctx.scale)
+        return (grad, None, None) + (None,) * len(cs)
+
+
+def tricubic_vjp(field, coords, cot, use_limiter=False, scale=1.0, out=None):
+    """Cotangent of ``field`` for ``scale * tensor_product_interp_3d(field,
+    coords)`` given the output cotangent (accumulated into ``out`` when given)."""
+    f = fortran(field)
+    cs = _coords3(coords, f.dtype, f.device)
+    g = fortran(cot, dtype=f.dtype)
+    if out is None:
+        out = empty_field(tuple(f.shape), f.dtype, f.device).zero_()
+    src = (ctypes.c_int32 * 3)(*f.shape)
+    dst = (ctypes.c_int32 * 3)(*cs[0].shape)
+    co = (ctypes.c_void_p * 3)(*[c.data_ptr() for c in cs])
+    check(_lib.load().sisl_tricubic_vjp(DTYPE_CODE[f.dtype], src, f.data_ptr(), dst, co, g.data_ptr(),
+                                        out.data_ptr(), int(bool(use_limiter)), float(scale),
+                                        stream_ptr(f.device)), "sisl_tricubic_vjp")
+    return out
+
+
 def tensor_product_interp_3d(field, coords, use_limiter=False):
     """Catmull-Rom tricubic at continuous indices (operators.py:146-209).
 
     ``field`` is a 3-D CUDA tensor; ``coords`` a (3, ...) tensor or a
-    sequence of three 3-D tensors of the output shape."""
-    if not torch.is_tensor(field) or field.device.type != "cuda":
-        raise RuntimeError("tensor_product_interp_3d runs on CUDA tensors only")
+    sequence of three 3-D tensors of the output shape.  Differentiable with
+    respect to ``field``; coordinates must not require gradients."""
+    _require_cuda(field, "tensor_product_interp_3d")
+    cs = _coords3(coords, field.dtype, field.device)
+    if any(c.requires_grad for c in cs):
+        raise NotImplementedError("tensor_product_interp_3d provides no coordinate cotangents "
+                                  "(departure points are stop-gradiented, steppers.py:764-767)")
+    if torch.is_grad_enabled() and field.requires_grad:
+        return _Tricubic.apply(field, bool(use_limiter), 1.0, *cs)
+    return _tricubic_fwd(field, cs, use_limiter)
+
+
+def _tricubic_fwd(field, cs, use_limiter):
     f = fortran(field)
-    cs = _coords3(coords, f.dtype, f.device)
     out = empty_field(tuple(cs[0].shape), f.dtype, f.device)
     src = (ctypes.c_int32 * 3)(*f.shape)
     dst = (ctypes.c_int32 * 3)(*cs[0].shape)

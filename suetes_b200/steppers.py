@@ -84,6 +84,15 @@ class VerticalPreconditioner:
               "sisl_precond_apply")
         return {k: o for (k, _), o in zip(LOC5, outs)}
 
+    def transpose(self, cot_scaled):
+        """``jax.linear_transpose(M_fn)`` applied to a cotangent (steppers.py:474-476)."""
+        core = self.physics.core(_dtype_of(cot_scaled), self.dt, self.alpha, bg=self.physics._bg_arg(self.bg))
+        ins = [core.field(cot_scaled[k], l) for k, l in LOC5]
+        outs = [core.new(l) for _, l in LOC5]
+        check(core.lib.sisl_precond_apply_t(core.handle, ptrs(ins, 5), ptrs(outs, 5), core.stream),
+              "sisl_precond_apply_t")
+        return {k: o for (k, _), o in zip(LOC5, outs)}
+
 
 class SemiLagrangianAdvector3D:
     """Trajectories and SL interpolation (steppers.py:256-374)."""
@@ -130,20 +139,62 @@ class SemiImplicitSolver3D:
         return core
 
     def solve(self, rhs_prime, bg_precomputed, x0=None):
-        """Solve A x = b (steppers.py:401-496); x0 None means x0 = rhs."""
+        """Solve A x = b (steppers.py:401-496); x0 None means x0 = rhs.
+
+        Differentiable like ``jax.lax.custom_linear_solve`` (steppers.py:483):
+        the cotangent of ``rhs_prime`` is the transpose solve of the
+        solution's cotangent; ``x0`` receives none."""
         core = self._core(_dtype_of(rhs_prime), bg_precomputed)
         b = [core.field(rhs_prime[k], l) for k, l in LOC5]
+        if torch.is_grad_enabled() and any(t.requires_grad for t in b):
+            x = _LinearSolve.apply(self, core, x0, *b)
+            return {k: t for (k, _), t in zip(LOC5, x)}
+        return {k: t for (k, _), t in zip(LOC5, self._solve_core(core, b, x0))}
+
+    def _solve_core(self, core, b, x0):
         x = [core.new(l) for _, l in LOC5]
         x0p, x0t = None, None
         if x0 is not None:
-            x0t = [core.field(x0[k], l) for k, l in LOC5]  # keep alive across the call
+            x0t = [core.field(x0[k], l).detach() for k, l in LOC5]  # keep alive across the call
             x0p = ctypes.cast(ptrs(x0t, 5), ctypes.c_void_p)
+        b = [t.detach() for t in b]
         ws, n = core.workspace(_lib.WS_GMRES)
         info = _lib.SislSolveInfo()
         check(core.lib.sisl_gmres_solve(core.handle, ptrs(b, 5), x0p, ptrs(x, 5), ws.data_ptr(), n, core.stream,
                                         ctypes.byref(info)), "sisl_gmres_solve")
         self.last_info = info.as_dict()
-        return {k: t for (k, _), t in zip(LOC5, x)}
+        return x
+
+    def solve_transpose(self, cot_solution, bg_precomputed, dtype=None):
+        """bwd_solve (steppers.py:473-481): the cotangent of the physical rhs
+        from the cotangent of the physical solution."""
+        core = self._core(dtype or _dtype_of(cot_solution), bg_precomputed)
+        g = [core.field(cot_solution[k], l) for k, l in LOC5]
+        return {k: t for (k, _), t in zip(LOC5, self._solve_transpose_core(core, g))}
+
+    def _solve_transpose_core(self, core, g):
+        out = [core.new(l) for _, l in LOC5]
+        g = [t.detach() for t in g]
+        ws, n = core.workspace(_lib.WS_GMRES)
+        info = _lib.SislSolveInfo()
+        check(core.lib.sisl_gmres_solve_transpose(core.handle, ptrs(g, 5), ptrs(out, 5), ws.data_ptr(), n,
+                                                  core.stream, ctypes.byref(info)), "sisl_gmres_solve_transpose")
+        self.last_transpose_info = info.as_dict()
+        return out
+
+    def matvec_scaled(self, x_scaled, bg_precomputed, transpose=False):
+        """A_fn (steppers.py:439-461), or its transpose, on the scaled vector."""
+        core = self._core(_dtype_of(x_scaled), bg_precomputed)
+        ins = [core.field(x_scaled[k], l) for k, l in LOC5]
+        outs = [core.new(l) for _, l in LOC5]
+        if transpose:
+            ws, n = core.workspace(_lib.WS_OPERATOR)
+            check(core.lib.sisl_helmholtz_matvec_t(core.handle, ptrs(ins, 5), ptrs(outs, 5), ws.data_ptr(), n,
+                                                   core.stream), "sisl_helmholtz_matvec_t")
+        else:
+            check(core.lib.sisl_helmholtz_matvec(core.handle, ptrs(ins, 5), ptrs(outs, 5), core.stream),
+                  "sisl_helmholtz_matvec")
+        return {k: o for (k, _), o in zip(LOC5, outs)}
 
     def relative_residual(self, solution, rhs_prime, bg_precomputed):
         """``||A x - b|| / ||b||`` in the scaled norm (steppers.py:498-527)."""
@@ -157,6 +208,23 @@ class SemiImplicitSolver3D:
             num = num + torch.sum((a - r) ** 2)
             den = den + torch.sum(r ** 2)
         return torch.sqrt(num / torch.clamp(den, min=torch.finfo(F64).tiny))
+
+
+class _LinearSolve(torch.autograd.Function):
+    """custom_linear_solve on the five physical rhs fields: forward GMRES on
+    A, backward GMRES on A^T with M^T (steppers.py:463-485)."""
+
+    @staticmethod
+    def forward(ctx, solver, core, x0, *b):
+        ctx.solver, ctx.core = solver, core
+        return tuple(solver._solve_core(core, list(b), x0))
+
+    @staticmethod
+    def backward(ctx, *g):
+        core = ctx.core
+        gs = [zeros_field(core.shape(l), core.dtype, core.device) if t is None else core.field(t, l)
+              for t, (_, l) in zip(g, LOC5)]
+        return (None, None, None) + tuple(ctx.solver._solve_transpose_core(core, gs))
 
 
 class FluxFormAdvector:
