@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--cpu-window", type=int, default=32, help="nx = ny of the CPU-baseline window")
     ap.add_argument("--classes", action="store_true",
                     help="also time every GMRES kernel class separately (diagnostic)")
+    ap.add_argument("--vjp-steps", type=int, default=4,
+                    help="trajectory length of the fwd+VJP leg (0 disables it)")
+    ap.add_argument("--vjp-checkpoint", type=int, default=1, help="checkpoint interval of the fwd+VJP leg")
     return ap.parse_args()
 
 
@@ -271,6 +274,57 @@ def timed_device_steps(stepper, ds0, relax, steps, warmup, world, timing_class=N
     return ms, infos, launches, kt, cur
 
 
+def vjp_leg(args, local, world, cells, warm_state32):
+    """Value and gradient of the box-energy objective over a trajectory of
+    ``--vjp-steps`` steps (forward with the fused step recording its solves,
+    backward through the transposed kernels), float32 and float64; the
+    gradient error is float32 against float64 from the same initial state."""
+    from suetes_b200.adjoint import trajectory_vjp
+    from suetes_b200.steppers import DeviceState
+    from suetes_b200.workloads import box_energy_objective, mountain_wave
+    from suetes_b200.core import kernel_launches
+    N, ck = args.vjp_steps, args.vjp_checkpoint
+    out = {"metric": "SISL cell-steps/s fwd+VJP", "unit": "cell-steps/s", "steps": N, "checkpoint_every": ck,
+           "objective": "mean over the last 10 states of the lee-box (x 5-25 km, z 1-6 km) average of "
+                        "1/2 rho (u'^2 + v^2 + w^2); gradient w.r.t. the initial theta'"}
+    res = {}
+    for dtype, tol in ((torch.float32, args.tol32), (torch.float64, args.tol64)):
+        if dtype == torch.float64 and args.no_fp64:
+            continue
+        st, s0, bc = mountain_wave(args.nx, args.ny, args.nz, dtype=dtype, device=f"cuda:{local}",
+                                   solver_tol=tol, solve_method=args.method)
+        core = st.core(dtype)
+        # start from the developed float32 flow (cast) so both precisions see the same state
+        t = {k: v.to(dtype).clone() for k, v in warm_state32.t.items()}
+        ds0 = DeviceState(core, t, 0.0)
+        obj = box_energy_objective(st, N)
+        trajectory_vjp(st, ds0, 1, obj, bc_fn=bc, checkpoint_every=ck)  # warm-up (allocations)
+        torch.cuda.synchronize()
+        barrier(world)
+        l0 = kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        J, g = trajectory_vjp(st, ds0, N, obj, bc_fn=bc, checkpoint_every=ck)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = dist_max(e0.elapsed_time(e1), world)
+        res[dtype] = (float(J), g["th_p"].double(), ms, kernel_launches() - l0,
+                      st.implicit_solver.__dict__.get("last_transpose_info"))
+        del st, core, ds0
+    J32, g32, ms32, l32, ti = res[torch.float32]
+    out.update({"value": world * cells * N / (ms32 / 1e3), "ms_per_step": ms32 / N, "J": J32,
+                "gpu_launches": l32, "dtype": "f32", "last_transpose_solve": ti})
+    if torch.float64 in res:
+        J64, g64, ms64, _, _ = res[torch.float64]
+        den = float(torch.linalg.vector_norm(g64))
+        out["fp64"] = {"value": world * cells * N / (ms64 / 1e3), "ms_per_step": ms64 / N, "J": J64}
+        out["err_f32_vs_f64"] = {"J_rel": abs(J32 - J64) / max(abs(J64), 1e-300),
+                                 "grad_rel_l2": float(torch.linalg.vector_norm(g32 - g64)) / max(den, 1e-300),
+                                 "grad_linf_rel": float((g32 - g64).abs().max()) / max(float(g64.abs().max()),
+                                                                                       1e-300)}
+    return out
+
+
 def run_ours(args):
     world, rank, local = dist_setup()
     import suetes_b200 as sb
@@ -343,6 +397,10 @@ def run_ours(args):
                          "avg_launch_us": cms / max(cn, 1) * 1e3, "share_of_step": cms / msc,
                          "frac_of_measured": (cb / cms / 1e6) / peak if cms else None}
         line["roofline"]["classes"] = per
+
+    # ---- fwd+VJP: gradient of the lee box energy w.r.t. the initial theta' ----
+    if args.vjp_steps > 0:
+        line["fwd_vjp"] = vjp_leg(args, local, world, cells, cur32)
 
     # ---- end to end through the public API with host state ----
     if not args.no_e2e:

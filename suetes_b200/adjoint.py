@@ -352,11 +352,16 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
     dstep = DifferentiableStep(stepper, ds0.core.dtype)
     K = max(1, int(checkpoint_every))
     checkpoints = {0: ds0}
+    keep_all = K == 1  # every state and solve kept: no recomputation of the forward
+    kept_states, kept_recs = [ds0], []
     cur = ds0
     J = torch.zeros((), dtype=F64, device=ds0.core.device)
     with torch.no_grad():
         for n in range(num_steps):
-            cur, _ = _taped_step(stepper, cur, relax, record=False)
+            cur, rec = _taped_step(stepper, cur, relax, record=keep_all)
+            if keep_all:
+                kept_states.append(cur)
+                kept_recs.append(rec)
             val = objective(n + 1, _as_dict(cur))
             if val is not None:
                 J = J + val.double()
@@ -366,12 +371,15 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
     cot = {}
     for seg0 in range(((num_steps - 1) // K) * K, -1, -K):
         seg1 = min(seg0 + K, num_steps)
-        states, recs = [checkpoints[seg0]], []
-        with torch.no_grad():
-            for n in range(seg0, seg1):
-                nxt, rec = _taped_step(stepper, states[-1], relax)
-                states.append(nxt)
-                recs.append(rec)
+        if keep_all:
+            states, recs = kept_states[seg0:seg1 + 1], kept_recs[seg0:seg1]
+        else:
+            states, recs = [checkpoints[seg0]], []
+            with torch.no_grad():
+                for n in range(seg0, seg1):
+                    nxt, rec = _taped_step(stepper, states[-1], relax)
+                    states.append(nxt)
+                    recs.append(rec)
         for n in range(seg1 - 1, seg0 - 1, -1):
             after = {k: v.detach().requires_grad_(True) for k, v in states[n + 1 - seg0].t.items()}
             g_after = dict(cot)

@@ -131,6 +131,7 @@ class SemiImplicitSolver3D:
         self.pi_scale = 1000.0
         self.solver_tol, self.solver_maxiter, self.solver_restart = solver_tol, solver_maxiter, solver_restart
         self.solve_method = solve_method
+        self.transpose_tol = None  # tolerance of the transposed (adjoint) solve; None: solver_tol as in bwd_solve
         self.last_info = None
 
     def _core(self, dtype, bg=None):
@@ -177,8 +178,16 @@ class SemiImplicitSolver3D:
         g = [t.detach() for t in g]
         ws, n = core.workspace(_lib.WS_GMRES)
         info = _lib.SislSolveInfo()
-        check(core.lib.sisl_gmres_solve_transpose(core.handle, ptrs(g, 5), ptrs(out, 5), ws.data_ptr(), n,
-                                                  core.stream, ctypes.byref(info)), "sisl_gmres_solve_transpose")
+        ttol = self.transpose_tol
+        if ttol is not None:
+            core.set_solver(ttol, self.solver_maxiter, self.solver_restart, SOLVE_METHODS[self.solve_method])
+        try:
+            check(core.lib.sisl_gmres_solve_transpose(core.handle, ptrs(g, 5), ptrs(out, 5), ws.data_ptr(), n,
+                                                      core.stream, ctypes.byref(info)), "sisl_gmres_solve_transpose")
+        finally:
+            if ttol is not None:
+                core.set_solver(self.solver_tol, self.solver_maxiter, self.solver_restart,
+                                SOLVE_METHODS[self.solve_method])
         self.last_transpose_info = info.as_dict()
         return out
 
@@ -370,7 +379,13 @@ class SISLStepper3D:
         return None, bc_fn
 
     def step(self, state, t, forcing, bc_fn, ml_params=None):
-        """SISLStepper3D.step (steppers.py:720-1073)."""
+        """SISLStepper3D.step (steppers.py:720-1073).
+
+        With autograd recording and a state field that requires grad, the
+        step runs as ``DifferentiableStep`` (differentiable CUDA primitives,
+        VJP through the transposed solve) instead of the fused kernel chain."""
+        if torch.is_grad_enabled() and any(torch.is_tensor(v) and v.requires_grad for v in state.values()):
+            return self._step_differentiable(state, bc_fn)
         ds = self.to_device_state(state)
         out = DeviceState(ds.core)
         # history of the new state aliases the old prognostic fields (steppers.py:1061-1064)
@@ -382,6 +397,36 @@ class SISLStepper3D:
         if generic is not None:
             res = self._apply_generic_bc(res, generic, forcing, out)
         return res
+
+    def _step_differentiable(self, state, bc_fn):
+        from .adjoint import DifferentiableStep
+        relax, generic = self._relax_of(bc_fn)
+        if generic is not None:
+            raise NotImplementedError("the differentiable step supports LateralRelaxation boundary conditions")
+        dtype = _dtype_of({k: state[k] for k in ("u", "v", "w")})
+        key = ("_dstep", dtype)
+        dstep = self.__dict__.get(key)
+        if dstep is None:
+            dstep = DifferentiableStep(self, dtype)
+            self.__dict__[key] = dstep
+        core = self.core(dtype)
+        f = lambda t, loc: core.field(t, loc)
+        ps = {"u": f(state["u"], "u"), "v": f(state["v"], "v"), "w": f(state["w"], "w"),
+              "eta_dot": f(state["eta_dot"], "w") if "eta_dot" in state else zeros_field(core.shape("w"), dtype,
+                                                                                           core.device),
+              "pi_p": state["pi"].to(dtype) - dstep.pi_bg, "th_p": state["th_v"].to(dtype) - dstep.theta_bg}
+        first = float(state.get("is_first_step", 1.0))
+        if "u_prev" in state:
+            for k, loc in (("u_prev", "u"), ("v_prev", "v"), ("w_prev", "w"), ("eta_dot_prev", "w")):
+                ps[k] = f(state[k], loc)
+        else:
+            first = 1.0
+        ps["is_first_step"] = first
+        out = dstep(ps, relax=relax)
+        return {"u": out["u"], "v": out["v"], "w": out["w"], "eta_dot": out["eta_dot"], "rho": out["rho"],
+                "pi": out["pi_p"] + dstep.pi_bg, "th_v": out["th_p"] + dstep.theta_bg,
+                "u_prev": state["u"], "v_prev": state["v"], "w_prev": state["w"],
+                "eta_dot_prev": ps["eta_dot"], "tend_th_v_prev": out["tend_th_prev"], "is_first_step": 0.0}
 
     def _apply_generic_bc(self, res, bc_fn, forcing, ds):
         """A user bc_fn runs on the assembled state; the EOS of

@@ -8,6 +8,11 @@
   alpha 0.5, sponge from 12 km, x relaxation over 4 km
   (schaer_mountain_3d/run.py:103-136).  No dataset is involved: the case
   is analytic.
+* ``box_energy_objective``: the adjoint objective of the mountain-wave
+  gradient runs -- the mean over the last steps of the box-averaged
+  1/2 rho (u'^2 + v^2 + w^2) in the lee (x in [5, 25] km, z in [1, 6] km,
+  all y), patterned on the box-energy objective of
+  experiments/schaer_optimal_perturbation/run.py:138-144.
 * ``rising_bubble``: 3-D dry warm bubble (64x64x48, 50 m, dt = 1 s,
   cos^2 bubble of 2 K, r = 1 km, 1.5 km above ground;
   cpu_gpu_short_scaling/run.py:38-55 in 3-D).
@@ -72,3 +77,36 @@ def rising_bubble(nx=64, ny=64, nz=48, dx=50.0, amp=2.0, radius=1000.0, center=(
     for k in ("u", "v", "w", "eta_dot", "u_prev", "v_prev", "w_prev", "eta_dot_prev", "tend_th_v_prev", "rho"):
         state[k] = state[k].to(dtype)
     return stepper, state, None
+
+
+def box_energy_objective(stepper, num_steps, last=10, u_ref=10.0, x_box=(5000.0, 25000.0), z_box=(1000.0, 6000.0)):
+    """``objective(n, state)`` for ``trajectory_vjp``: J = mean over the last
+    ``last`` of ``num_steps`` states of the box-averaged kinetic energy of
+    the perturbation wind, on mass points (perturbation-form state)."""
+    from .core import fortran
+    g = stepper.physics.grid
+    op = stepper.physics.op
+    X = g.x_m[:, None, None].expand(g.nx, g.ny, g.nz)
+    Z = g.Z_m
+    box = ((X >= x_box[0]) & (X <= x_box[1]) & (Z >= z_box[0]) & (Z <= z_box[1])).to(F64)
+    count = float(box.sum())
+    if count == 0.0:
+        raise ValueError("the objective box holds no mass points")
+    first = max(1, num_steps - last + 1)
+    nterms = num_steps - first + 1
+    cache = {}
+
+    def objective(n, st):
+        if n < first:
+            return None
+        dt_ = st["u"].dtype
+        w8 = cache.get(dt_)
+        if w8 is None:
+            w8 = fortran(box, dtype=dt_) / (count * nterms)
+            cache[dt_] = w8
+        um = op.avg(st["u"], 0, "u", "m") - u_ref
+        vm = op.avg(st["v"], 1, "v", "m")
+        wm = op.avg(st["w"], 2, "w", "m")
+        return (w8 * 0.5 * st["rho"] * (um * um + vm * vm + wm * wm)).sum()
+
+    return objective

@@ -335,3 +335,27 @@ def test_step_vjp_taylor_float64():
         rems.append(abs(float(Je) - float(J0) - e * slope))
     orders = [math.log10(rems[i] / rems[i + 1]) for i in range(len(rems) - 1)]
     assert min(orders) > 1.8, (rems, orders)
+
+
+def test_step_api_differentiable_matches_oracle():
+    """SISLStepper3D.step under autograd (the jax.grad use of the reference step)."""
+    from oracle.steppers import SISLStepper3D as OSt
+    from suetes_b200 import SISLStepper3D as PSt
+    kw = dict(dt=10.0, N_bv=0.01, nu_h_factor=0.05, nu_div_factor=0.1, lat=45.0)
+    o = build("oracle", 10, 9, 8, 500.0, 500.0, 500.0, h=mountain, **kw)
+    p = build("cuda", 10, 9, 8, 500.0, 500.0, 500.0, h=mountain, device="cuda", **kw)
+    skw = dict(alpha=0.55, solver_tol=1e-12, solver_maxiter=60, solver_restart=30)
+    os_, ps_ = OSt(o[2], 10.0, **skw), PSt(p[2], 10.0, **skw)
+    s0 = _bubble(o[2], o[0])
+    gen = torch.Generator().manual_seed(12)
+    wu = torch.randn(s0["u"].shape, generator=gen, dtype=torch.float64)
+    wt = torch.randn(s0["th_v"].shape, generator=gen, dtype=torch.float64)
+    th = s0["th_v"].clone().requires_grad_(True)
+    so = os_.step(dict(s0, th_v=th), 0.0, None, lambda s, f: s)
+    (gref,) = torch.autograd.grad((wu * so["u"]).sum() + (wt * so["th_v"]).sum(), th)
+    thc = s0["th_v"].cuda().requires_grad_(True)
+    sp = ps_.step(dict(to_cuda(s0), th_v=thc), 0.0, None, None)
+    for k in ("u", "w", "rho"):
+        assert rel_l2(sp[k], so[k]) < 1e-8, k
+    (g,) = torch.autograd.grad((wu.cuda() * sp["u"]).sum() + (wt.cuda() * sp["th_v"]).sum(), thc)
+    assert rel_l2(g, gref) < 1e-7, rel_l2(g, gref)
