@@ -149,6 +149,14 @@ int sisl_core_destroy(SislCore* core);
 /* Replace the GMRES settings of SemiImplicitSolver3D(solver_tol,
  * solver_maxiter, solver_restart) (steppers.py:384-399) on an existing core. */
 int sisl_core_set_solver(SislCore* core, double tol, double atol, int maxiter, int restart, int method);
+/* Settings of the transposed (adjoint) solve, the bwd_solve of
+ * steppers.py:473-481: tol <= 0 uses the forward solver_tol (the reference);
+ * normalize_rhs = 1 (the default) solves for the cotangent scaled to unit
+ * norm and rescales the result.  GMRES takes a preconditioned residual below
+ * machine epsilon as zero (_safe_normalize); unnormalised, a cotangent of
+ * small norm then stops after one cycle at a relative accuracy of
+ * eps / ||M b||.  normalize_rhs = 0 reproduces that behaviour. */
+int sisl_core_set_adjoint(SislCore* core, double tol, int normalize_rhs);
 size_t sisl_workspace_bytes(const SislCore* core, int what);
 
 /* Euler3D.linear_operator(state_prime, bg, dt, alpha) (euler.py:374-439).

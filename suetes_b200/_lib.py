@@ -81,6 +81,7 @@ PROTOTYPES = {
     "sisl_core_destroy": (ctypes.c_int, [vp]),
     "sisl_core_set_solver": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int]),
+    "sisl_core_set_adjoint": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
     "sisl_workspace_bytes": (ctypes.c_size_t, [vp, ctypes.c_int]),
     "sisl_linear_operator": (ctypes.c_int, [vp, vp * 5, vp * 5, vp, ctypes.c_size_t, vp]),
     "sisl_helmholtz_matvec": (ctypes.c_int, [vp, vp * 5, vp * 5, vp]),

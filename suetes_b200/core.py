@@ -113,6 +113,13 @@ class Core:
             self.params.solver_restart = key[3]
             self._solver_key = key
 
+    def set_adjoint(self, tol=None, normalize_rhs=True):
+        """Transposed-solve settings (``sisl_core_set_adjoint``)."""
+        key = (0.0 if tol is None else float(tol), int(bool(normalize_rhs)))
+        if key != getattr(self, "_adjoint_key", None):
+            check(self.lib.sisl_core_set_adjoint(self.handle, key[0], key[1]), "sisl_core_set_adjoint")
+            self._adjoint_key = key
+
     def workspace(self, kind):
         n = int(self.lib.sisl_workspace_bytes(self.handle, kind))
         buf = self._ws.get(kind)

@@ -29,6 +29,10 @@ struct SislCore {
   std::vector<cudaEvent_t> ev0, ev1;
   size_t ev_used = 0;
   double timed_bytes = 0.0;  // algorithmic bytes of the timed launches
+  // adjoint (transposed) solve: tolerance (<= 0: the forward solver_tol) and
+  // whether the cotangent is normalised before GMRES (see sisl_core_set_adjoint)
+  double adj_tol = -1.0;
+  int adj_normalize = 1;
 };
 
 namespace {
@@ -135,6 +139,19 @@ __global__ void zero_gaps_kernel(T* base, size_t npad, int nvec, size_t o0, size
   }
 }
 
+// norm of a packed vector kept for the transposed solve; v *= 1/norm (mode 0)
+// or v *= norm (mode 1), a zero norm leaving v unchanged
+__global__ void keep_norm_kernel(const GState* gs, double* scal) { *scal = gs->bnorm; }
+
+template <typename T>
+__global__ void scale_packed_kernel(T* v, size_t n, const double* scal, int mode) {
+  const double nrm = *scal;
+  if (!(nrm > 0.0)) return;
+  const T f = (T)(mode == 0 ? 1.0 / nrm : nrm);
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    v[e] *= f;
+}
+
 // lateral overrides after advection (steppers.py:858-869) and the zero
 // lid/ground rows of R_eta_dot (steppers.py:893)
 template <typename T>
@@ -177,6 +194,7 @@ struct GWork {
   double* partial;
   T* vec;  // (R + 4) contiguous vectors
   T* tmp;  // mass-point scratch of the transposed matvec
+  double* scal;  // norm of the normalised right-hand side (transposed solve)
   size_t npad;
   size_t off[5], sz[5];
   int R;
@@ -218,6 +236,7 @@ GWork<T> carve_gmres(Carver& cv, const Dims& d, int R) {
   g.partial = (double*)cv.take(sizeof(double) * GM_MAXBLOCKS * (GM_MAXR + 2));
   g.vec = (T*)cv.take(sizeof(T) * g.npad * (size_t)(R + 4));
   g.tmp = (T*)cv.take(sizeof(T) * field_size(d, LOC_M));
+  g.scal = (double*)cv.take(sizeof(double));
   return g;
 }
 
@@ -282,7 +301,8 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
   const double mvb = matvec_bytes(d, sizeof(T)), pcb = precond_bytes(d, sizeof(T));
   {
     KScope k(c, SISL_K_OTHER, st);
-    gm_setup(gs, eps, c->prm.solver_tol, c->prm.solver_atol, R, method, st);
+    const double tol = (transpose && c->adj_tol > 0.0) ? c->adj_tol : c->prm.solver_tol;
+    gm_setup(gs, eps, tol, c->prm.solver_atol, R, method, st);
   }
   {
     KScope k(c, SISL_K_DOTS, st);
@@ -427,8 +447,24 @@ int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<
   const T ps = (T)c->s.ps;
   scale5<T>(c, cf, xbar, g.view(g.bg()), (T)(1.0 / c->s.ps), 2, st);  // pi / ps, eta / dz_w
   if (cudaMemsetAsync(g.xg(), 0, sizeof(T) * g.npad, st) != cudaSuccess) return SISL_ERR_CUDA;
+  // GMRES treats a preconditioned residual below machine epsilon as zero
+  // (_safe_normalize's absolute threshold); cotangents are often far below
+  // unit norm, so the right-hand side is solved at unit norm and rescaled
+  const int norm_rhs = c->adj_normalize;
+  const int nb = 2 * 148;
+  if (norm_rhs) {
+    KScope k(c, SISL_K_OTHER, st, 4);
+    gm_setup(g.gs, 0.0, c->prm.solver_tol, c->prm.solver_atol, g.R, c->prm.solve_method, st);
+    gm_dots<T>(g.V(0), g.npad, 0, g.bg(), g.npad, g.partial, g.gs, 1 /*BNORM*/, 0, st);
+    keep_norm_kernel<<<1, 1, 0, st>>>(g.gs, g.scal);
+    scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.bg(), g.npad, g.scal, 0);
+  }
   int rc = gmres_run<T>(c, cf, g, st, info, 1);
   if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+  if (norm_rhs) {
+    KScope k(c, SISL_K_OTHER, st);
+    scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.xg(), g.npad, g.scal, 1);
+  }
   scale5<T>(c, cf, g.cview(g.xg()), bbar, ps, 0, st);  // pi * ps
   (void)d;
   return rc;
@@ -1074,6 +1110,13 @@ int sisl_step_taped(SislCore* c, const SislState* in, const SislState* out, cons
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64) return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info, solves);
   return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info, solves);
+}
+
+int sisl_core_set_adjoint(SislCore* c, double tol, int normalize_rhs) {
+  if (!c || !(tol < 1.0)) return SISL_ERR_ARG;
+  c->adj_tol = tol;
+  c->adj_normalize = normalize_rhs ? 1 : 0;
+  return SISL_OK;
 }
 
 int sisl_core_set_solver(SislCore* c, double tol, double atol, int maxiter, int restart, int method) {

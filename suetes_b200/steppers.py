@@ -131,7 +131,10 @@ class SemiImplicitSolver3D:
         self.pi_scale = 1000.0
         self.solver_tol, self.solver_maxiter, self.solver_restart = solver_tol, solver_maxiter, solver_restart
         self.solve_method = solve_method
-        self.transpose_tol = None  # tolerance of the transposed (adjoint) solve; None: solver_tol as in bwd_solve
+        # transposed (adjoint) solve: tolerance (None: solver_tol, as bwd_solve) and
+        # unit-norm scaling of the cotangent (False: the reference's absolute eps floor)
+        self.transpose_tol = None
+        self.adjoint_normalize = True
         self.last_info = None
 
     def _core(self, dtype, bg=None):
@@ -178,16 +181,9 @@ class SemiImplicitSolver3D:
         g = [t.detach() for t in g]
         ws, n = core.workspace(_lib.WS_GMRES)
         info = _lib.SislSolveInfo()
-        ttol = self.transpose_tol
-        if ttol is not None:
-            core.set_solver(ttol, self.solver_maxiter, self.solver_restart, SOLVE_METHODS[self.solve_method])
-        try:
-            check(core.lib.sisl_gmres_solve_transpose(core.handle, ptrs(g, 5), ptrs(out, 5), ws.data_ptr(), n,
-                                                      core.stream, ctypes.byref(info)), "sisl_gmres_solve_transpose")
-        finally:
-            if ttol is not None:
-                core.set_solver(self.solver_tol, self.solver_maxiter, self.solver_restart,
-                                SOLVE_METHODS[self.solve_method])
+        core.set_adjoint(self.transpose_tol, self.adjoint_normalize)
+        check(core.lib.sisl_gmres_solve_transpose(core.handle, ptrs(g, 5), ptrs(out, 5), ws.data_ptr(), n,
+                                                  core.stream, ctypes.byref(info)), "sisl_gmres_solve_transpose")
         self.last_transpose_info = info.as_dict()
         return out
 

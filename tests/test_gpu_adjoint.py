@@ -359,3 +359,21 @@ def test_step_api_differentiable_matches_oracle():
         assert rel_l2(sp[k], so[k]) < 1e-8, k
     (g,) = torch.autograd.grad((wu.cuda() * sp["u"]).sum() + (wt.cuda() * sp["th_v"]).sum(), thc)
     assert rel_l2(g, gref) < 1e-7, rel_l2(g, gref)
+
+
+def test_transpose_solve_scale_invariant_float32():
+    """A cotangent of tiny norm is solved as accurately as a unit one: the
+    transposed solve normalises its right-hand side (GMRES reads a
+    preconditioned residual below machine epsilon as zero)."""
+    from suetes_b200 import SemiImplicitSolver3D as PS
+    c, _, (pg, pop, pph) = _pair("mountain")
+    sh = shapes5(c["nx"], c["ny"], c["nz"])
+    cot = random_fields(sh, 19, {"u": 1.0, "v": 1.0, "w": 1.0, "pi": 100.0, "eta_dot": 100.0})
+    s64 = PS(pph, 40.0, alpha=0.55, solver_tol=1e-12, solver_maxiter=50, solver_restart=30)
+    ref = s64.solve_transpose(to_cuda(cot), _bg(pph))
+    s32 = PS(pph, 40.0, alpha=0.55, solver_tol=1e-6, solver_maxiter=50, solver_restart=30)
+    tiny = {k: v * 1e-9 for k, v in cot.items()}
+    out = s32.solve_transpose(to_cuda(tiny, torch.float32), _bg(pph))
+    assert s32.last_transpose_info["converged"]
+    for k in FIELDS5:
+        assert rel_l2(out[k].double() * 1e9, ref[k]) < 1e-4, (k, rel_l2(out[k].double() * 1e9, ref[k]))
