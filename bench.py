@@ -49,9 +49,12 @@ def parse():
     ap.add_argument("--nx", type=int, default=256)
     ap.add_argument("--ny", type=int, default=256)
     ap.add_argument("--nz", type=int, default=80)
-    ap.add_argument("--tol32", type=float, default=1e-6, help="GMRES tolerance of the float32 path")
+    ap.add_argument("--tol32", type=float, default=1e-7,
+                    help="GMRES tolerance of the float32 path (float64 iterative refinement makes it reachable)")
     ap.add_argument("--tol64", type=float, default=1e-8, help="GMRES tolerance of the float64 path")
-    ap.add_argument("--method", default="batched", choices=["batched", "incremental"])
+    ap.add_argument("--method", default="incremental", choices=["batched", "incremental"])
+    ap.add_argument("--no-refine", action="store_true",
+                    help="float32 GMRES without float64 iterative refinement")
     ap.add_argument("--roofline-class", default="update",
                     choices=["matvec", "precond", "dots", "update"])
     ap.add_argument("--no-fp64", action="store_true")
@@ -63,6 +66,10 @@ def parse():
     ap.add_argument("--vjp-steps", type=int, default=4,
                     help="trajectory length of the fwd+VJP leg (0 disables it)")
     ap.add_argument("--vjp-checkpoint", type=int, default=1, help="checkpoint interval of the fwd+VJP leg")
+    ap.add_argument("--adj-method", default="batched", choices=["batched", "incremental"],
+                    help="GMRES variant of the transposed solves")
+    ap.add_argument("--adj-tol32", type=float, default=1e-5,
+                    help="GMRES tolerance of the float32 transposed solves (the float64 ones use --tol64)")
     return ap.parse_args()
 
 
@@ -285,6 +292,8 @@ def vjp_leg(args, local, world, cells, warm_state32):
     from suetes_b200.core import kernel_launches
     N, ck = args.vjp_steps, args.vjp_checkpoint
     out = {"metric": "SISL cell-steps/s fwd+VJP", "unit": "cell-steps/s", "steps": N, "checkpoint_every": ck,
+           "adjoint_tol_f32": args.adj_tol32, "adjoint_tol_f64": args.tol64, "adjoint_rhs": "unit-norm",
+           "adjoint_method": args.adj_method,
            "objective": "mean over the last 10 states of the lee-box (x 5-25 km, z 1-6 km) average of "
                         "1/2 rho (u'^2 + v^2 + w^2); gradient w.r.t. the initial theta'"}
     res = {}
@@ -292,12 +301,14 @@ def vjp_leg(args, local, world, cells, warm_state32):
         if dtype == torch.float64 and args.no_fp64:
             continue
         st, s0, bc = mountain_wave(args.nx, args.ny, args.nz, dtype=dtype, device=f"cuda:{local}",
-                                   solver_tol=tol, solve_method=args.method)
+                                   solver_tol=tol, solve_method=args.method, refine=not args.no_refine)
         core = st.core(dtype)
         # start from the developed float32 flow (cast) so both precisions see the same state
         t = {k: v.to(dtype).clone() for k, v in warm_state32.t.items()}
         ds0 = DeviceState(core, t, 0.0)
         obj = box_energy_objective(st, N)
+        st.implicit_solver.transpose_tol = args.adj_tol32 if dtype == torch.float32 else None
+        st.implicit_solver.transpose_method = args.adj_method
         trajectory_vjp(st, ds0, 1, obj, bc_fn=bc, checkpoint_every=ck)  # warm-up (allocations)
         torch.cuda.synchronize()
         barrier(world)
@@ -339,7 +350,7 @@ def run_ours(args):
 
     # ---- float32 device-resident leg ----
     st32, s32, bc = mountain_wave(nx, ny, nz, dtype=torch.float32, device=f"cuda:{local}", solver_tol=args.tol32,
-                                  solve_method=args.method)
+                                  solve_method=args.method, refine=not args.no_refine)
     ds = st32.to_device_state(s32)
     with ClockSampler(local) as clk:
         ms, infos, launches, kt, cur32 = timed_device_steps(st32, ds, bc, K, W, world, cls)
@@ -349,7 +360,8 @@ def run_ours(args):
     gm = {"solves": len(solves), "cycles_per_solve": sum(s["cycles"] for s in solves) / max(len(solves), 1),
           "arnoldi_per_solve": sum(s["arnoldi_steps"] for s in solves) / max(len(solves), 1),
           "converged_frac": sum(1 for s in solves if s["converged"]) / max(len(solves), 1),
-          "tol": args.tol32, "restart": 30, "maxiter": 30, "method": args.method}
+          "tol": args.tol32, "restart": 30, "maxiter": 30, "method": args.method,
+          "refinement": "none" if args.no_refine else "float64 residual and solution per restart"}
     peak, peak_kind = measured_peaks()
     k_ms, k_n, k_bytes = kt
     achieved = (k_bytes / k_n) / (k_ms / k_n / 1e3) / 1e9 if k_n else None
@@ -385,6 +397,18 @@ def run_ours(args):
                         "arnoldi_per_solve": sum(s["arnoldi_steps"] for s in solves64) / max(len(solves64), 1),
                         "tol": args.tol64}
         line["err_f32_vs_f64"] = {"after_steps": K + W, "fields": err}
+        # one step from the same (float64) state: the per-step error of the float32 kernels
+        from suetes_b200.steppers import DeviceState
+        c32 = st32.core(torch.float32)
+        d32 = DeviceState(c32, {k: v.to(torch.float32).clone() for k, v in cur64.t.items()}, 0.0)
+        o32, o64 = DeviceState(c32), DeviceState(cur64.core)
+        st32.step_device(d32, o32, bc)
+        st64.step_device(cur64, o64, bc64)
+        one = {}
+        for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p"):
+            a, b = o32.t[k].double(), o64.t[k]
+            one[k] = float(torch.linalg.vector_norm(a - b)) / max(float(torch.linalg.vector_norm(b)), 1e-300)
+        line["err_f32_vs_f64"]["one_step_rel_l2"] = one
         del st64, ds64, cur64
 
     # ---- per-class GMRES kernel timing (diagnostic; advances the float32 state) ----

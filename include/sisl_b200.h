@@ -88,7 +88,9 @@ typedef struct SislParams {
   int32_t solve_method;    /* SISL_GMRES_* */
   int32_t use_limiter;
   int32_t departure_iterations; /* 2 (steppers.py:318) */
-  int32_t pad;
+  int32_t refine;          /* float32 cores: 1 = also build the float64 coefficients and run GMRES with
+                              float64 iterative refinement (sisl_core_set_refinement); no counterpart in
+                              the reference, whose GMRES runs wholly in the state precision */
 } SislParams;
 
 /* float64 background and metrics (device pointers, device layout):
@@ -150,13 +152,22 @@ int sisl_core_destroy(SislCore* core);
  * solver_maxiter, solver_restart) (steppers.py:384-399) on an existing core. */
 int sisl_core_set_solver(SislCore* core, double tol, double atol, int maxiter, int restart, int method);
 /* Settings of the transposed (adjoint) solve, the bwd_solve of
- * steppers.py:473-481: tol <= 0 uses the forward solver_tol (the reference);
+ * steppers.py:473-481: tol <= 0 uses the forward solver_tol and method < 0
+ * the forward SISL_GMRES_* variant (both as the reference does);
  * normalize_rhs = 1 (the default) solves for the cotangent scaled to unit
  * norm and rescales the result.  GMRES takes a preconditioned residual below
  * machine epsilon as zero (_safe_normalize); unnormalised, a cotangent of
  * small norm then stops after one cycle at a relative accuracy of
  * eps / ||M b||.  normalize_rhs = 0 reproduces that behaviour. */
-int sisl_core_set_adjoint(SislCore* core, double tol, int normalize_rhs);
+int sisl_core_set_adjoint(SislCore* core, double tol, int normalize_rhs, int method);
+/* Switch float64 iterative refinement of a float32 core's GMRES on or off
+ * (on needs a core created with SislParams.refine = 1).  The solution and
+ * right-hand side are held in float64 and every restart cycle starts from
+ * the residual b - A x of the float64 operator; the Krylov cycle itself
+ * (basis, matvec, preconditioner, Gram-Schmidt) stays in float32.  Without
+ * it the float32 residual floor (~1e-7 relative) stalls tolerances below
+ * about 1e-6.  No counterpart in the reference. */
+int sisl_core_set_refinement(SislCore* core, int on);
 size_t sisl_workspace_bytes(const SislCore* core, int what);
 
 /* Euler3D.linear_operator(state_prime, bg, dt, alpha) (euler.py:374-439).

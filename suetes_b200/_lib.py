@@ -39,7 +39,7 @@ class SislParams(ctypes.Structure):
                 ("nu_h", ctypes.c_double), ("solver_tol", ctypes.c_double), ("solver_atol", ctypes.c_double),
                 ("solver_maxiter", ctypes.c_int32), ("solver_restart", ctypes.c_int32),
                 ("solve_method", ctypes.c_int32), ("use_limiter", ctypes.c_int32),
-                ("departure_iterations", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("departure_iterations", ctypes.c_int32), ("refine", ctypes.c_int32)]
 
 
 class SislBackground(ctypes.Structure):
@@ -81,7 +81,8 @@ PROTOTYPES = {
     "sisl_core_destroy": (ctypes.c_int, [vp]),
     "sisl_core_set_solver": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int]),
-    "sisl_core_set_adjoint": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
+    "sisl_core_set_adjoint": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "sisl_core_set_refinement": (ctypes.c_int, [vp, ctypes.c_int]),
     "sisl_workspace_bytes": (ctypes.c_size_t, [vp, ctypes.c_int]),
     "sisl_linear_operator": (ctypes.c_int, [vp, vp * 5, vp * 5, vp, ctypes.c_size_t, vp]),
     "sisl_helmholtz_matvec": (ctypes.c_int, [vp, vp * 5, vp * 5, vp]),

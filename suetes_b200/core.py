@@ -80,6 +80,8 @@ class Core:
         p.solve_method = int(solver.get("method", _lib.SISL_GMRES_BATCHED))
         p.use_limiter = int(bool(use_limiter))
         p.departure_iterations = int(departure_iterations)
+        # float32 cores also carry the float64 operator of GMRES iterative refinement
+        p.refine = 1 if dtype == F32 else 0
         self.params = p
         f = lambda t: fortran(t, dtype=F64, device=self.device)
         keep = [f(theta_bg), f(pi_bg), f(grid.Z_m), f(grid.dz_m_full), f(grid.dz_w_full), f(grid.z_xi_w),
@@ -113,11 +115,20 @@ class Core:
             self.params.solver_restart = key[3]
             self._solver_key = key
 
-    def set_adjoint(self, tol=None, normalize_rhs=True):
-        """Transposed-solve settings (``sisl_core_set_adjoint``)."""
-        key = (0.0 if tol is None else float(tol), int(bool(normalize_rhs)))
+    def set_refinement(self, on):
+        """float64 iterative refinement of a float32 core's GMRES (``sisl_core_set_refinement``)."""
+        if self.dtype != F32:
+            return
+        on = int(bool(on))
+        if on != getattr(self, "_refine", None):
+            check(self.lib.sisl_core_set_refinement(self.handle, on), "sisl_core_set_refinement")
+            self._refine = on
+
+    def set_adjoint(self, tol=None, normalize_rhs=True, method=None):
+        """Transposed-solve settings (``sisl_core_set_adjoint``); None keeps the forward's."""
+        key = (0.0 if tol is None else float(tol), int(bool(normalize_rhs)), -1 if method is None else int(method))
         if key != getattr(self, "_adjoint_key", None):
-            check(self.lib.sisl_core_set_adjoint(self.handle, key[0], key[1]), "sisl_core_set_adjoint")
+            check(self.lib.sisl_core_set_adjoint(self.handle, key[0], key[1], key[2]), "sisl_core_set_adjoint")
             self._adjoint_key = key
 
     def workspace(self, kind):

@@ -262,8 +262,9 @@ __global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T
 }
 
 // ---------------------------------------------------------------------------
-// M^T, column part: one thread per column.  With ybar the output cotangent
-// (ybar_pi = y_pi * ps on the unscaled pressure):
+// M^T, column part, on tiles of 32 columns (same j) like the forward
+// preconditioner.  With ybar the output cotangent (ybar_pi = y_pi * ps on
+// the unscaled pressure):
 //   G(K)   = -adt cp thw (yw + yW) idzw / damp at interior w levels, else 0
 //   pibar  = ybar_pi + G(k) - G(k+1)
 //   z      = T^-T pibar   (T: the Helmholtz tridiagonal of the forward)
@@ -271,17 +272,33 @@ __global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T
 //   wtbar(K) = divbar(K-1) - divbar(K),  epbar = yW + rho_w thw wtbar
 //   out_W  = epbar / alpha,  out_w = (yw + epbar) / damp  (interior levels)
 //   out_W  = yW dz_w,        out_w = yw                   (ground and lid)
-// The elimination factors c' and d' are parked in out_w and out_pi.
+// A: every thread takes (level, column) pairs and forms pibar, L_pi and P;
+// B: warp 0 runs the transposed Thomas sweep of its 32 columns in shared
+//    memory (sub(k) = -L(k-1) P(k), sup(k) = -L(k+1) P(k+1),
+//    main(k) = 1 + L(k) (P(k) + P(k+1)));
+// C: every thread writes pi, w and eta_dot.
+// Shared memory per block: (3 nz + 1) * 32 values of T.
 // ---------------------------------------------------------------------------
+constexpr int TPT = 256;  // threads per block
+constexpr int TPC = 32;   // columns per block
+
 template <typename T>
-__global__ void __launch_bounds__(128) pt_column_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
+__device__ __forceinline__ T pt_rcp(T x) { return T(1) / x; }
+
+template <typename T>
+__global__ void __launch_bounds__(TPT) pt_column_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
                                                         const int* active) {
   if (active && *active == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  if (i >= nx || j >= ny) return;
-  const int pm = nx * ny, h = i + nx * j;
+  T* s_x = sm;                // [nz][TPC]    pibar -> d' -> z
+  T* s_L = s_x + nz * TPC;    // [nz][TPC]    L_pi
+  T* s_P = s_L + nz * TPC;    // [nz+1][TPC]  P at w levels, then c'
+  const int i0 = blockIdx.x * TPC;
+  const int j = blockIdx.y;
+  const int tid = threadIdx.x;
+  const int pm = nx * ny;
   const T ps = (T)c.s.ps, ips = (T)(1.0 / c.s.ps), a = (T)c.s.alpha;
   const T adtcp = (T)(c.s.alpha * c.s.dt * c.s.cp);
   const T* __restrict__ yw = y.f[2];
@@ -290,62 +307,73 @@ __global__ void __launch_bounds__(128) pt_column_kernel(Dims d, Coef<T> c, CVec5
   T* __restrict__ ow = out.f[2];
   T* __restrict__ op = out.f[3];
   T* __restrict__ oW = out.f[4];
-  // w-level coupling P(K) = adt cp thw idzw / damp * rho_w thw (0 on ground and lid)
-  auto Pw = [&](int K) -> T {
-    if (K <= 0 || K >= nz) return T(0);
-    const int p = h + K * pm;
-    const T thw = ld(c.thw, p);
-    return adtcp * thw * ld(c.idzw, p) / ld(c.damp, p) * ld(c.rhow, p) * thw;
-  };
-  auto Gw = [&](int K) -> T {
-    if (K <= 0 || K >= nz) return T(0);
-    const int p = h + K * pm;
-    return -adtcp * ld(c.thw, p) * (ld(yw, p) + ld(yW, p)) * ld(c.idzw, p) / ld(c.damp, p);
-  };
-  // forward elimination of T^T: sub(k) = -L(k-1) P(k), sup(k) = -L(k+1) P(k+1),
-  // main(k) = 1 + L(k) (P(k) + P(k+1))
-  T cprev = T(0), dprev = T(0), Lprev = T(0);
-  T Pk = T(0), Gk = T(0);
-  for (int k = 0; k < nz; ++k) {
-    const int p = h + k * pm;
-    const T L = ld(c.lpi, p);
-    const T Pk1 = Pw(k + 1), Gk1 = Gw(k + 1);
-    const T Lnext = (k + 1 < nz) ? ld(c.lpi, p + pm) : T(0);
-    const T sub = -Lprev * Pk, sup = -Lnext * Pk1, mn = T(1) + L * (Pk + Pk1);
-    const T pib = ld(yp, p) * ps + Gk - Gk1;
-    const T inv = T(1) / (mn - sub * cprev);
-    cprev = sup * inv;
-    dprev = (pib - sub * dprev) * inv;
-    ow[p] = cprev;
-    op[p] = dprev;
-    Lprev = L;
-    Pk = Pk1;
-    Gk = Gk1;
-  }
-  // back substitution, finishing w level K = k + 1 on the way down
-  T znext = T(0), dvnext = T(0);
-  for (int k = nz - 1; k >= 0; --k) {
-    const int p = h + k * pm;
-    const T z = (k == nz - 1) ? op[p] : op[p] - ow[p] * znext;
-    op[p] = z * ips;
-    const T dv = -ld(c.lpi, p) * z;
-    if (k + 1 < nz) {
-      const int pw = p + pm;
-      const T wtb = dv - dvnext;
-      const T ep = ld(yW, pw) + ld(c.rhow, pw) * ld(c.thw, pw) * wtb;
-      oW[pw] = ep / a;
-      ow[pw] = (ld(yw, pw) + ep) / ld(c.damp, pw);
+  // ---- A: pibar, L_pi, P (loads at a clamped interior level, masked) ----
+  for (int q = tid; q < (nz + 1) * TPC; q += TPT) {
+    const int k = q / TPC, l = q % TPC, i = min(i0 + l, nx - 1);
+    const int h = i + nx * j;
+    auto GP = [&](int K, T& G, T& P) {
+      const int kc = min(max(K, 1), nz - 1);
+      const T on = (K > 0 && K < nz) ? T(1) : T(0);
+      const int p = h + kc * pm;
+      const T thw = ld(c.thw, p), idzw = ld(c.idzw, p), idamp = T(1) / ld(c.damp, p);
+      G = -on * adtcp * thw * (ld(yw, p) + ld(yW, p)) * idzw * idamp;
+      P = on * adtcp * thw * idzw * idamp * ld(c.rhow, p) * thw;
+    };
+    T G0, P0, G1, P1;
+    GP(k, G0, P0);
+    s_P[q] = P0;
+    if (k < nz) {
+      GP(k + 1, G1, P1);
+      const int p = h + k * pm;
+      s_x[q] = ld(yp, p) * ps + G0 - G1;
+      s_L[q] = ld(c.lpi, p);
     }
-    znext = z;
-    dvnext = dv;
   }
-  ow[h] = ld(yw, h);
-  oW[h] = ld(yW, h) * ld(c.dzw, h);
-  const int pt = h + nz * pm;
-  ow[pt] = ld(yw, pt);
-  oW[pt] = ld(yW, pt) * ld(c.dzw, pt);
+  __syncthreads();
+  // ---- B: transposed Thomas, one lane per column ----
+  if (tid < TPC) {
+    const int l = tid;
+    T cprev = T(0), dprev = T(0), Lprev = T(0), Pk = s_P[l];
+    for (int k = 0; k < nz; ++k) {
+      const int q = k * TPC + l;
+      const T L = s_L[q], Pk1 = s_P[q + TPC];
+      const T Lnext = (k + 1 < nz) ? s_L[q + TPC] : T(0);
+      const T sub = -Lprev * Pk, sup = -Lnext * Pk1;
+      const T inv = pt_rcp((T(1) + L * (Pk + Pk1)) - sub * cprev);
+      cprev = sup * inv;
+      dprev = (s_x[q] - sub * dprev) * inv;
+      s_P[q] = cprev;  // P(k) is no longer needed
+      s_x[q] = dprev;
+      Lprev = L;
+      Pk = Pk1;
+    }
+    T zh = dprev;
+    for (int k = nz - 2; k >= 0; --k) {
+      const int q = k * TPC + l;
+      zh = s_x[q] - s_P[q] * zh;
+      s_x[q] = zh;
+    }
+  }
+  __syncthreads();
+  // ---- C: pi, w, eta_dot ----
+  for (int q = tid; q < (nz + 1) * TPC; q += TPT) {
+    const int k = q / TPC, l = q % TPC, i = i0 + l;
+    if (i >= nx) continue;
+    const int p = i + nx * j + k * pm;
+    if (k < nz) op[p] = s_x[q] * ips;
+    if (k == 0 || k == nz) {
+      ow[p] = ld(yw, p);
+      oW[p] = ld(yW, p) * ld(c.dzw, p);
+    } else {
+      const T dvl = -s_L[q - TPC] * s_x[q - TPC], dv = -s_L[q] * s_x[q];
+      const T ep = ld(yW, p) + ld(c.rhow, p) * ld(c.thw, p) * (dvl - dv);
+      oW[p] = ep / a;
+      ow[p] = (ld(yw, p) + ep) / ld(c.damp, p);
+    }
+  }
 }
 
+// ---------------------------------------------------------------------------
 // M^T, horizontal part: out_u = y_u + sum of the kinematic cotangent
 // kinbar = -alpha out_W over the interior w levels of the adjacent cells.
 template <typename T>
@@ -527,7 +555,13 @@ template void launch_tricubic_vjp<double>(int, int, int, int, int, int, const do
 template <typename T>
 void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                       cudaStream_t st) {
-  pt_column_kernel<T><<<dim3((d.nx + 127) / 128, d.ny), 128, 0, st>>>(d, c, y, out, active);
+  const size_t smem = (size_t)(3 * d.nz + 1) * TPC * sizeof(T);
+  static size_t attr_bytes = 0;  // per instantiation
+  if (smem > 48 * 1024 && smem > attr_bytes) {
+    cudaFuncSetAttribute(pt_column_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_bytes = smem;
+  }
+  pt_column_kernel<T><<<dim3((d.nx + TPC - 1) / TPC, d.ny), TPT, smem, st>>>(d, c, y, out, active);
   dim3 blk(32, 4, 2);
   pt_uv_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz, blk), blk, 0, st>>>(d, c, y, out, active);
 }

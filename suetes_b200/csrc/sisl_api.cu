@@ -33,6 +33,12 @@ struct SislCore {
   // whether the cotangent is normalised before GMRES (see sisl_core_set_adjoint)
   double adj_tol = -1.0;
   int adj_normalize = 1;
+  int adj_method = -1;  // GMRES variant of the transposed solve; < 0: the forward's
+  // float32 cores: float64 coefficient set for GMRES with float64 iterative
+  // refinement (outer residual and solution in float64), and its switch
+  void* coef64_mem = nullptr;
+  void* coef64_ptr[C_COUNT];
+  int refine_on = 0;
 };
 
 namespace {
@@ -94,6 +100,18 @@ Coef<T> coef_of(const SislCore* c) {
   return make_coef<T>(a, c->s);
 }
 
+Coef<double> coef64_of(const SislCore* c) {
+  double* a[C_COUNT];
+  for (int q = 0; q < C_COUNT; ++q) a[q] = (double*)c->coef64_ptr[q];
+  return make_coef<double>(a, c->s);
+}
+
+// iterative refinement applies to float32 cores holding the float64 coefficients
+template <typename T>
+bool refining(const SislCore* c) {
+  return sizeof(T) == 4 && c->refine_on && c->coef64_mem;
+}
+
 int loc_of_field(int q) {  // solver vector field -> stagger
   static const int L[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_W};
   return L[q];
@@ -137,6 +155,14 @@ __global__ void zero_gaps_kernel(T* base, size_t npad, int nvec, size_t o0, size
     const size_t end = (q < 4) ? off[q + 1] : npad;
     for (size_t e = off[q] + sz[q] + threadIdx.x; e < end; e += blockDim.x) vb[e] = T(0);
   }
+}
+
+// dst = (D) src over a packed vector; elements below `split` go to dst_lo,
+// the rest to dst_hi (the u, v | w, pi, eta_dot split of the solver vectors)
+template <typename S, typename D>
+__global__ void convert_packed_kernel(const S* __restrict__ src, D* dst_lo, D* dst_hi, size_t split, size_t n) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    (e < split ? dst_lo : dst_hi)[e] = (D)src[e];
 }
 
 // norm of a packed vector kept for the transposed solve; v *= 1/norm (mode 0)
@@ -195,6 +221,9 @@ struct GWork {
   T* vec;  // (R + 4) contiguous vectors
   T* tmp;  // mass-point scratch of the transposed matvec
   double* scal;  // norm of the normalised right-hand side (transposed solve)
+  // iterative refinement (float32 cores): solution, rhs and residual in float64
+  bool refine = false;
+  double *x64 = nullptr, *b64 = nullptr, *r64 = nullptr, *tmp64 = nullptr;
   size_t npad;
   size_t off[5], sz[5];
   int R;
@@ -221,7 +250,7 @@ struct GWork {
 };
 
 template <typename T>
-GWork<T> carve_gmres(Carver& cv, const Dims& d, int R) {
+GWork<T> carve_gmres(Carver& cv, const Dims& d, int R, bool refine) {
   GWork<T> g;
   g.R = R;
   size_t o = 0;
@@ -237,6 +266,13 @@ GWork<T> carve_gmres(Carver& cv, const Dims& d, int R) {
   g.vec = (T*)cv.take(sizeof(T) * g.npad * (size_t)(R + 4));
   g.tmp = (T*)cv.take(sizeof(T) * field_size(d, LOC_M));
   g.scal = (double*)cv.take(sizeof(double));
+  g.refine = refine;
+  if (refine) {
+    g.x64 = (double*)cv.take(sizeof(double) * g.npad);
+    g.b64 = (double*)cv.take(sizeof(double) * g.npad);
+    g.r64 = (double*)cv.take(sizeof(double) * g.npad);
+    g.tmp64 = (double*)cv.take(sizeof(double) * field_size(d, LOC_M));
+  }
   return g;
 }
 
@@ -293,12 +329,25 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
   const Dims& d = c->d;
   const int R = g.R;
   const size_t n = g.npad;
-  const int method = c->prm.solve_method;
+  const int method = (transpose && c->adj_method >= 0) ? c->adj_method : c->prm.solve_method;
   const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
   GState* gs = g.gs;
   CVec5<T> none{};
   const double es = sizeof(T), vb = es * (double)n;
   const double mvb = matvec_bytes(d, sizeof(T)), pcb = precond_bytes(d, sizeof(T));
+  // float64 iterative refinement: x and b held in float64, every restart's
+  // residual b - A x formed with the float64 operator, the Krylov cycle in T
+  const bool refine = g.refine;
+  const int nconv = 2 * 148;
+  Coef<double> cf64{};
+  if (refine) {
+    cf64 = coef64_of(c);
+    KScope k(c, SISL_K_OTHER, st, 2);
+    convert_packed_kernel<T, double><<<nconv, 256, 0, st>>>(g.bg(), g.b64, g.b64, n, n);
+    convert_packed_kernel<T, double><<<nconv, 256, 0, st>>>(g.xg(), g.x64, g.x64, n, n);
+    // the operator writes no padding gaps: they stay zero for the norms
+    if (cudaMemsetAsync(g.r64, 0, sizeof(double) * n, st) != cudaSuccess) return SISL_ERR_CUDA;
+  }
   {
     KScope k(c, SISL_K_OTHER, st);
     const double tol = (transpose && c->adj_tol > 0.0) ? c->adj_tol : c->prm.solver_tol;
@@ -338,7 +387,23 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
   }
   // residual of the initial guess
   auto residual_and_read = [&](GHostView* out) -> int {
-    {
+    if (refine) {
+      KScope k(c, SISL_K_MATVEC, st, na + 1);
+      CVec5<double> x5, b5;
+      Vec5<double> r5;
+      for (int q = 0; q < 5; ++q) {
+        x5.f[q] = g.x64 + g.off[q];
+        b5.f[q] = g.b64 + g.off[q];
+        r5.f[q] = g.r64 + g.off[q];
+      }
+      if (transpose) {
+        launch_matvec_t<double>(d, cf64, x5, nullptr, b5, r5, g.tmp64, nullptr, st);
+        convert_packed_kernel<double, T><<<nconv, 256, 0, st>>>(g.r64, g.z(), g.z(), n, n);
+      } else {
+        launch_matvec<double>(d, cf64, x5, nullptr, b5, r5, nullptr, st);
+        convert_packed_kernel<double, T><<<nconv, 256, 0, st>>>(g.r64, g.V(0), g.z(), g.off[2], n);
+      }
+    } else {
       KScope k(c, SISL_K_MATVEC, st, na);
       apply_A(g.xg(), nullptr, g.cview(g.bg()), g.V(0), nullptr);
     }
@@ -392,12 +457,17 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
     }
     {
       KScope k(c, SISL_K_UPDATE, st);
-      gm_update<T>(g.V(0), n, R, g.xg(), n, 1.0, g.partial, gs, 0 /*NONE*/, 0, 1, st);
+      if (refine) gm_update_x64<T>(g.V(0), n, R, g.x64, n, gs, st);
+      else gm_update<T>(g.V(0), n, R, g.xg(), n, 1.0, g.partial, gs, 0 /*NONE*/, 0, 1, st);
     }
     rc = residual_and_read(hv);
     if (rc) return rc;
     steps += hv->kdone;
     cycles++;
+  }
+  if (refine) {
+    KScope k(c, SISL_K_OTHER, st);
+    convert_packed_kernel<double, T><<<nconv, 256, 0, st>>>(g.x64, g.xg(), g.xg(), n, n);
   }
   if (info) {
     info->cycles = cycles;
@@ -486,9 +556,9 @@ struct SWork {
 };
 
 template <typename T>
-SWork<T> carve_step(Carver& cv, const Dims& d, int R) {
+SWork<T> carve_step(Carver& cv, const Dims& d, int R, bool refine) {
   SWork<T> w;
-  w.g = carve_gmres<T>(cv, d, R);
+  w.g = carve_gmres<T>(cv, d, R, refine);
   auto F = [&](int loc) { return (T*)cv.take(sizeof(T) * field_size(d, loc)); };
   const int vl[4] = {LOC_M, LOC_U, LOC_V, LOC_W};
   for (int l = 0; l < 4; ++l)
@@ -509,7 +579,7 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
   const Dims& d = c->d;
   const Coef<T> cf = coef_of<T>(c);
   Carver cv{(char*)ws};
-  SWork<T> w = carve_step<T>(cv, d, c->prm.solver_restart);
+  SWork<T> w = carve_step<T>(cv, d, c->prm.solver_restart, refining<T>(c));
   if (cv.off > ws_bytes) return SISL_ERR_WORKSPACE;
   const int64_t l0 = g_launches.load();
   const T* u = (const T*)in->u;
@@ -742,8 +812,26 @@ int sisl_core_create(const SislGrid* grid, const SislParams* prm, const SislBack
     for (int q = 0; q < C_COUNT; ++q) t.p[q] = (float*)c->coef_ptr[q];
     launch_prepare<float>(c->d, c->s, b, t, st);
   }
-  if (check_cuda() != SISL_OK || cudaStreamSynchronize(st) != cudaSuccess) {
+  if (grid->dtype == SISL_F32 && prm->refine) {  // float64 operator of the refinement
+    size_t t64 = 0, o64[C_COUNT];
+    for (int q = 0; q < C_COUNT; ++q) {
+      o64[q] = t64;
+      t64 += align256(sizeof(double) * coef_elems(c->d, q));
+    }
+    if (cudaMalloc(&c->coef64_mem, t64) == cudaSuccess) {
+      for (int q = 0; q < C_COUNT; ++q) c->coef64_ptr[q] = (char*)c->coef64_mem + o64[q];
+      PtrTable<double> t;
+      for (int q = 0; q < C_COUNT; ++q) t.p[q] = (double*)c->coef64_ptr[q];
+      g_launches += 1;
+      launch_prepare<double>(c->d, c->s, b, t, st);
+      c->refine_on = 1;
+    } else {
+      c->coef64_mem = nullptr;
+    }
+  }
+  if (check_cuda() != SISL_OK || cudaStreamSynchronize(st) != cudaSuccess || (prm->refine && grid->dtype == SISL_F32 && !c->coef64_mem)) {
     cudaFree(c->coef_mem);
+    if (c->coef64_mem) cudaFree(c->coef64_mem);
     cudaFreeHost(c->hv);
     delete c;
     return SISL_ERR_CUDA;
@@ -756,6 +844,7 @@ int sisl_core_destroy(SislCore* c) {
   if (!c) return SISL_ERR_ARG;
   for (size_t q = 0; q < c->ev0.size(); ++q) { cudaEventDestroy(c->ev0[q]); cudaEventDestroy(c->ev1[q]); }
   cudaFree(c->coef_mem);
+  if (c->coef64_mem) cudaFree(c->coef64_mem);
   cudaFreeHost(c->hv);
   delete c;
   return SISL_OK;
@@ -768,12 +857,12 @@ size_t sisl_workspace_bytes(const SislCore* c, int what) {
   const size_t es = esize(c->grid.dtype);
   switch (what) {
     case SISL_WS_STEP:
-      if (f64) carve_step<double>(cv, c->d, c->prm.solver_restart);
-      else carve_step<float>(cv, c->d, c->prm.solver_restart);
+      if (f64) carve_step<double>(cv, c->d, c->prm.solver_restart, false);
+      else carve_step<float>(cv, c->d, c->prm.solver_restart, refining<float>(c));
       break;
     case SISL_WS_GMRES:
-      if (f64) carve_gmres<double>(cv, c->d, c->prm.solver_restart);
-      else carve_gmres<float>(cv, c->d, c->prm.solver_restart);
+      if (f64) carve_gmres<double>(cv, c->d, c->prm.solver_restart, false);
+      else carve_gmres<float>(cv, c->d, c->prm.solver_restart, refining<float>(c));
       break;
     case SISL_WS_DEPARTURE:
       for (int l = 0; l < 4; ++l)
@@ -854,13 +943,13 @@ int sisl_gmres_solve(SislCore* c, const void* const rhs[5], const void* const x0
   Carver cv{(char*)ws};
   int rc;
   if (c->grid.dtype == SISL_F64) {
-    GWork<double> g = carve_gmres<double>(cv, c->d, c->prm.solver_restart);
+    GWork<double> g = carve_gmres<double>(cv, c->d, c->prm.solver_restart, false);
     CVec5<double> x0v;
     if (x0) x0v = cvec<double>(x0);
     rc = solve_physical<double>(c, coef_of<double>(c), g, cvec<double>(rhs), x0 ? &x0v : nullptr, vec<double>(x),
                                 st, info);
   } else {
-    GWork<float> g = carve_gmres<float>(cv, c->d, c->prm.solver_restart);
+    GWork<float> g = carve_gmres<float>(cv, c->d, c->prm.solver_restart, refining<float>(c));
     CVec5<float> x0v;
     if (x0) x0v = cvec<float>(x0);
     rc = solve_physical<float>(c, coef_of<float>(c), g, cvec<float>(rhs), x0 ? &x0v : nullptr, vec<float>(x), st,
@@ -908,10 +997,10 @@ int sisl_gmres_solve_transpose(SislCore* c, const void* const xbar[5], void* con
   Carver cv{(char*)ws};
   int rc;
   if (c->grid.dtype == SISL_F64) {
-    GWork<double> g = carve_gmres<double>(cv, c->d, c->prm.solver_restart);
+    GWork<double> g = carve_gmres<double>(cv, c->d, c->prm.solver_restart, false);
     rc = solve_transpose_physical<double>(c, coef_of<double>(c), g, cvec<double>(xbar), vec<double>(bbar), st, info);
   } else {
-    GWork<float> g = carve_gmres<float>(cv, c->d, c->prm.solver_restart);
+    GWork<float> g = carve_gmres<float>(cv, c->d, c->prm.solver_restart, refining<float>(c));
     rc = solve_transpose_physical<float>(c, coef_of<float>(c), g, cvec<float>(xbar), vec<float>(bbar), st, info);
   }
   int e = check_cuda();
@@ -1112,10 +1201,18 @@ int sisl_step_taped(SislCore* c, const SislState* in, const SislState* out, cons
   return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info, solves);
 }
 
-int sisl_core_set_adjoint(SislCore* c, double tol, int normalize_rhs) {
-  if (!c || !(tol < 1.0)) return SISL_ERR_ARG;
+int sisl_core_set_refinement(SislCore* c, int on) {
+  if (!c) return SISL_ERR_ARG;
+  if (on && !c->coef64_mem) return SISL_ERR_ARG;
+  c->refine_on = on ? 1 : 0;
+  return SISL_OK;
+}
+
+int sisl_core_set_adjoint(SislCore* c, double tol, int normalize_rhs, int method) {
+  if (!c || !(tol < 1.0) || method > SISL_GMRES_INCREMENTAL) return SISL_ERR_ARG;
   c->adj_tol = tol;
   c->adj_normalize = normalize_rhs ? 1 : 0;
+  c->adj_method = method < 0 ? -1 : method;
   return SISL_OK;
 }
 

@@ -144,6 +144,8 @@ void gm_dots(const T* Vb, size_t stride, int m, const T* w, size_t n, double* pa
 template <typename T>
 void gm_update(const T* Vb, size_t stride, int m, T* w, size_t n, double sign, double* partial, GState* gs,
                int mode, int gated, int limit_kdone, cudaStream_t st);
+template <typename T>
+void gm_update_x64(const T* Vb, size_t stride, int m, double* x, size_t n, const GState* gs, cudaStream_t st);
 void gm_setup(GState* gs, double eps, double tol, double atol_in, int restart, int method, cudaStream_t st);
 void gm_init_tol(GState* gs, cudaStream_t st);
 void gm_begin_cycle(GState* gs, cudaStream_t st);

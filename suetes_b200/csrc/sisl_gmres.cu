@@ -176,6 +176,22 @@ __global__ void dots_kernel(const T* __restrict__ Vb, size_t stride, int m, cons
 
 enum UpdMode { UM_NONE = 0, UM_ARNOLDI = 1 };
 
+// x64 += sum_{i < min(m, kdone)} coef_i V_i with a float64 solution (the
+// end-of-cycle update of GMRES with iterative refinement)
+template <typename T>
+__global__ void __launch_bounds__(256) update_x64_kernel(const T* __restrict__ Vb, size_t stride, int m,
+                                                         double* __restrict__ x, size_t n, const GState* gs) {
+  __shared__ double cf[GM_MAXR + 2];
+  const int mm = min(m, gs->kdone);
+  for (int q = threadIdx.x; q < mm; q += blockDim.x) cf[q] = gs->coef[q];
+  __syncthreads();
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    double acc = x[e];
+    for (int i = 0; i < mm; ++i) acc += cf[i] * (double)Vb[(size_t)i * stride + e];
+    x[e] = acc;
+  }
+}
+
 // w <- w + sign * sum_{i<m'} coef_i V_i with coef from gs->coef (UM_NONE,
 // m' = min(m, kdone) when limit_kdone) or coef_i = h_i s_i (UM_ARNOLDI),
 // then optionally finish the Arnoldi step j = m - 1.
@@ -435,6 +451,11 @@ void gm_update(const T* Vb, size_t stride, int m, T* w, size_t n, double sign, d
   update_kernel<T><<<g, GT, 0, st>>>(Vb, stride, m, w, n, sign, partial, gs, mode, gated, limit_kdone);
 }
 
+template <typename T>
+void gm_update_x64(const T* Vb, size_t stride, int m, double* x, size_t n, const GState* gs, cudaStream_t st) {
+  update_x64_kernel<T><<<flat_grid(n, 256 * 4), 256, 0, st>>>(Vb, stride, m, x, n, gs);
+}
+
 void gm_setup(GState* gs, double eps, double tol, double atol_in, int restart, int method, cudaStream_t st) {
   setup_kernel<<<1, 1, 0, st>>>(gs, eps, tol, atol_in, restart, method);
 }
@@ -460,5 +481,7 @@ template void gm_update<float>(const float*, size_t, int, float*, size_t, double
                                int, cudaStream_t);
 template void gm_update<double>(const double*, size_t, int, double*, size_t, double, double*, GState*, int,
                                 int, int, cudaStream_t);
+template void gm_update_x64<float>(const float*, size_t, int, double*, size_t, const GState*, cudaStream_t);
+template void gm_update_x64<double>(const double*, size_t, int, double*, size_t, const GState*, cudaStream_t);
 
 }  // namespace sisl

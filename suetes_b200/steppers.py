@@ -126,20 +126,24 @@ class SemiImplicitSolver3D:
     """Preconditioned GMRES Helmholtz solve (steppers.py:377-527)."""
 
     def __init__(self, physics, dt, alpha=0.55, solver_tol=1e-4, solver_maxiter=20, solver_restart=20,
-                 solve_method="batched"):
+                 solve_method="batched", refine=True):
         self.physics, self.dt, self.alpha = physics, dt, alpha
+        # float32 solves: float64 iterative refinement of the restarted GMRES
+        self.refine = bool(refine)
         self.pi_scale = 1000.0
         self.solver_tol, self.solver_maxiter, self.solver_restart = solver_tol, solver_maxiter, solver_restart
         self.solve_method = solve_method
         # transposed (adjoint) solve: tolerance (None: solver_tol, as bwd_solve) and
         # unit-norm scaling of the cotangent (False: the reference's absolute eps floor)
         self.transpose_tol = None
+        self.transpose_method = None  # "batched" / "incremental"; None: solve_method
         self.adjoint_normalize = True
         self.last_info = None
 
     def _core(self, dtype, bg=None):
         core = self.physics.core(dtype, self.dt, self.alpha, bg=self.physics._bg_arg(bg))
         core.set_solver(self.solver_tol, self.solver_maxiter, self.solver_restart, SOLVE_METHODS[self.solve_method])
+        core.set_refinement(self.refine)
         return core
 
     def solve(self, rhs_prime, bg_precomputed, x0=None):
@@ -181,7 +185,8 @@ class SemiImplicitSolver3D:
         g = [t.detach() for t in g]
         ws, n = core.workspace(_lib.WS_GMRES)
         info = _lib.SislSolveInfo()
-        core.set_adjoint(self.transpose_tol, self.adjoint_normalize)
+        core.set_adjoint(self.transpose_tol, self.adjoint_normalize,
+                         None if self.transpose_method is None else SOLVE_METHODS[self.transpose_method])
         check(core.lib.sisl_gmres_solve_transpose(core.handle, ptrs(g, 5), ptrs(out, 5), ws.data_ptr(), n,
                                                   core.stream, ctypes.byref(info)), "sisl_gmres_solve_transpose")
         self.last_transpose_info = info.as_dict()
@@ -312,6 +317,7 @@ class SISLStepper3D:
         s = self.implicit_solver
         c = self.physics.core(dtype, self.dt, self.alpha, use_limiter=self.use_limiter)
         c.set_solver(s.solver_tol, s.solver_maxiter, s.solver_restart, SOLVE_METHODS[s.solve_method])
+        c.set_refinement(s.refine)
         return c
 
     def to_device_state(self, state, dtype=None):

@@ -37,7 +37,7 @@ def ridge(x, y):
 
 
 def mountain_wave(nx=256, ny=256, nz=80, dtype=F32, device="cuda", solver_tol=1e-8, solver_maxiter=30,
-                  solver_restart=30, solve_method="batched", dt=8.0):
+                  solver_restart=30, solve_method="batched", dt=8.0, refine=True):
     grid = RegionalGrid3D(nx, ny, nz, 500.0, 500.0, 20000.0 / nz, 45.0, 0.0, h_func=ridge,
                           transform=StretchedSleveSimple(2.5, 4000.0, 1.35), device=device)
     op = CGridOperator3D(grid)
@@ -53,6 +53,7 @@ def mountain_wave(nx=256, ny=256, nz=80, dtype=F32, device="cuda", solver_tol=1e
                                       solver_restart=solver_restart, solve_method=solve_method)
     for k in ("u", "v", "w", "eta_dot", "u_prev", "v_prev", "w_prev", "eta_dot_prev", "tend_th_v_prev", "rho"):
         state[k] = state[k].to(dtype)
+    stepper.implicit_solver.refine = bool(refine)
     bc = x_relaxation(grid, 4000.0, 10.0)
     return stepper, state, bc
 

@@ -280,3 +280,33 @@ def test_ffsl_1d_periodic_shift():
     c = torch.ones(9, dtype=torch.float64, device="cuda")
     assert torch.allclose(adv.advect_1d(s, c, periodic=True), torch.roll(s, 1))
     assert torch.allclose(adv.advect_1d(s, -c, periodic=True), torch.roll(s, -1))
+
+
+def test_gmres_float32_refinement_reaches_float64_accuracy(mountain_pair):
+    """float32 GMRES with float64 iterative refinement converges to a
+    tolerance the float32 residual cannot resolve (manufactured solution as
+    tests/test_dynamical_core_3d.py:230-280) in as many cycles as float64."""
+    from suetes_b200 import SemiImplicitSolver3D
+    (og, oop, oph), (pg, pop, pph) = mountain_pair
+    gen = torch.Generator().manual_seed(42)
+    sh = shapes5(NX, NY, NZ)
+    known = {k: torch.rand(sh[k], generator=gen, dtype=torch.float64) * s
+             for k, s in (("u", 0.1), ("v", 0.1), ("w", 0.01), ("pi", 0.001), ("eta_dot", 0.001))}
+    for k in ("w", "eta_dot"):
+        known[k][:, :, 0] = 0.0
+        known[k][:, :, -1] = 0.0
+    bg = _bg(pph)
+    rhs = pph.linear_operator(to_cuda(known), bg, dt=100.0, alpha=0.55)
+    kw = dict(solver_tol=1e-9, solver_maxiter=40, solver_restart=100)
+    s64 = SemiImplicitSolver3D(pph, 100.0, **kw)
+    ref = s64.solve(rhs, bg)
+    r32 = {k: v.float() for k, v in rhs.items()}
+    s32 = SemiImplicitSolver3D(pph, 100.0, **kw)
+    out = s32.solve(r32, bg)
+    assert s32.last_info["converged"], s32.last_info
+    assert s32.last_info["cycles"] <= s64.last_info["cycles"] + 1
+    for k in ref:  # float32 rounding of the rhs, amplified by the conditioning
+        assert rel_l2(out[k], ref[k]) < 1e-4, (k, rel_l2(out[k], ref[k]))
+    plain = SemiImplicitSolver3D(pph, 100.0, refine=False, **kw)
+    plain.solve(r32, bg)
+    assert not plain.last_info["converged"]
