@@ -139,6 +139,9 @@ typedef struct SislStepInfo {
   int64_t kernel_launches;
 } SislStepInfo;
 
+/* The last CUDA failure recorded by this thread (call, error name and
+ * text), or "" (no reference counterpart: diagnostics of SISL_ERR_CUDA). */
+const char* sisl_last_error(void);
 int sisl_version(void);
 const char* sisl_status_string(int status);
 size_t sisl_field_elems(const SislGrid* grid, int loc);
@@ -279,6 +282,26 @@ int sisl_step(SislCore* core, const SislState* in, const SislState* out, const S
  * steppers.py:792-850). */
 int sisl_step_taped(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax,
                     void* const solves[10], void* ws, size_t ws_bytes, void* stream, SislStepInfo* info);
+
+/* CUDA graph of one step of n members (n >= 1; member m advances ins[m]
+ * into outs[m] on core m with workspace ws[m]), captured once for these
+ * buffers and replayed by sisl_step_graph_launch with no host
+ * synchronisation.  Members are parallel branches of the graph; each GMRES
+ * restart loop is a conditional WHILE node whose condition a kernel sets on
+ * the device (rnorm > atol and cycles < maxiter), so a replay runs exactly
+ * the cycles the host loop of sisl_step would.  The replay of lax.scan's
+ * jitted step (steppers.py:692-714) in one launch; the ensemble launch of
+ * the many-member configuration.  Cores must be distinct and have no timing
+ * class selected; relax may be NULL (or hold NULL entries). */
+typedef struct SislStepGraph SislStepGraph;
+int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                           const SislRelaxation* const* relax, void* const* ws, const size_t* ws_bytes,
+                           void* stream, SislStepGraph** out);
+int sisl_step_graph_launch(SislStepGraph* graph, void* stream);
+/* Solve statistics of the last replay for one member (synchronises stream);
+ * returns SISL_NOT_CONVERGED / SISL_ERR_NONFINITE like sisl_step. */
+int sisl_step_graph_info(SislStepGraph* graph, int member, SislStepInfo* info, void* stream);
+int sisl_step_graph_destroy(SislStepGraph* graph);
 
 /* Instrumentation (no reference counterpart): number of kernels this library
  * launched, and CUDA-event timing of one kernel class inside GMRES (events

@@ -12,12 +12,12 @@ from .boundaries import LateralRelaxation, x_relaxation
 from .euler import Euler3D
 from .geometry import (GalChenSigma, HybridSigma, RegionalGrid3D, SleveSimple, StretchedSleveSimple)
 from .operators import CGridOperator3D, map_coordinates_linear, tensor_product_interp_3d
-from .steppers import (DeviceState, FluxFormAdvector, SemiImplicitSolver3D, SemiLagrangianAdvector3D,
-                       SISLStepper3D, StateRing, VerticalPreconditioner, build_dynamical_core)
+from .steppers import (DeviceState, FluxFormAdvector, PingPong, SemiImplicitSolver3D, SemiLagrangianAdvector3D,
+                       SISLStepper3D, StateRing, StepGraph, VerticalPreconditioner, build_dynamical_core)
 
 __all__ = [
     "RegionalGrid3D", "GalChenSigma", "HybridSigma", "SleveSimple", "StretchedSleveSimple", "CGridOperator3D",
     "tensor_product_interp_3d", "map_coordinates_linear", "Euler3D", "VerticalPreconditioner",
     "SemiLagrangianAdvector3D", "SemiImplicitSolver3D", "FluxFormAdvector", "SISLStepper3D", "DeviceState",
-    "StateRing", "build_dynamical_core", "LateralRelaxation", "x_relaxation",
+    "StateRing", "StepGraph", "PingPong", "build_dynamical_core", "LateralRelaxation", "x_relaxation",
 ]

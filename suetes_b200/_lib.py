@@ -74,6 +74,7 @@ class SislStepInfo(ctypes.Structure):
 # name -> (restype, argtypes); the exported symbol set of sisl_b200.h
 PROTOTYPES = {
     "sisl_version": (ctypes.c_int, []),
+    "sisl_last_error": (ctypes.c_char_p, []),
     "sisl_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "sisl_field_elems": (ctypes.c_size_t, [ctypes.POINTER(SislGrid), ctypes.c_int]),
     "sisl_core_create": (ctypes.c_int, [ctypes.POINTER(SislGrid), ctypes.POINTER(SislParams),
@@ -117,6 +118,11 @@ PROTOTYPES = {
     "sisl_step_taped": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
                                        ctypes.POINTER(SislRelaxation), vp * 10, vp, ctypes.c_size_t, vp,
                                        ctypes.POINTER(SislStepInfo)]),
+    "sisl_step_graph_create": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
+                                              vp, vp, vp, vp, ctypes.POINTER(vp)]),
+    "sisl_step_graph_launch": (ctypes.c_int, [vp, vp]),
+    "sisl_step_graph_info": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SislStepInfo), vp]),
+    "sisl_step_graph_destroy": (ctypes.c_int, [vp]),
     "sisl_kernel_launches": (ctypes.c_int64, []),
     "sisl_timing_select": (ctypes.c_int, [vp, ctypes.c_int]),
     "sisl_timing_read": (ctypes.c_int, [vp, c_double_p, ctypes.POINTER(ctypes.c_int64), c_double_p]),
@@ -149,7 +155,13 @@ def status_string(rc):
 def check(rc, what):
     """Raise on a negative status; return the status otherwise."""
     if rc < 0:
-        raise RuntimeError(f"{what} failed: {status_string(rc)} (status {rc})")
+        detail = ""
+        if rc == -2:
+            try:
+                detail = load().sisl_last_error().decode()
+            except Exception:
+                detail = ""
+        raise RuntimeError(f"{what} failed: {status_string(rc)} (status {rc})" + (f": {detail}" if detail else ""))
     return rc
 
 

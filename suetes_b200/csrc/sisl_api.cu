@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -16,6 +17,15 @@
 using namespace sisl;
 
 static std::atomic<int64_t> g_launches{0};
+static thread_local char g_last_error[256] = "";
+
+// Record a failing CUDA call for sisl_last_error; true when e is an error.
+static bool cuda_failed(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return false;
+  snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+  return true;
+}
+static_assert(sizeof(GDevInfo) == sizeof(SislSolveInfo), "device solve statistics mirror SislSolveInfo");
 
 struct SislCore {
   SislGrid grid;
@@ -39,6 +49,7 @@ struct SislCore {
   void* coef64_mem = nullptr;
   void* coef64_ptr[C_COUNT];
   int refine_on = 0;
+  cudaStream_t cap_side = nullptr;  // side stream for conditional-node bodies while a graph is captured
 };
 
 namespace {
@@ -89,8 +100,7 @@ struct Carver {
 };
 
 int check_cuda() {
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? SISL_OK : SISL_ERR_CUDA;
+  return cuda_failed(cudaGetLastError(), "kernel launch") ? SISL_ERR_CUDA : SISL_OK;
 }
 
 template <typename T>
@@ -323,9 +333,17 @@ double precond_bytes(const Dims& d, size_t es) {
 // Restarted GMRES on the packed vectors g.bg (rhs) and g.xg (initial guess).
 // transpose = 1 runs the same iteration on A^T with the preconditioner M^T
 // (the bwd_solve of steppers.py:473-481).
+//
+// Host mode (dev_info == nullptr): one device-to-host read of the residual
+// summary per restart cycle decides whether another cycle runs.
+// Graph mode (dev_info != nullptr, st capturing): the restart loop becomes a
+// CUDA-graph conditional WHILE node whose body is one restart cycle; a gate
+// kernel after every residual sets the condition (rnorm > atol and cycles <
+// maxiter) on the device, and the final statistics land in *dev_info.  No
+// host synchronisation: the whole solve replays inside one graph launch.
 template <typename T>
 int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, SislSolveInfo* info,
-              int transpose = 0) {
+              int transpose = 0, GDevInfo* dev_info = nullptr) {
   const Dims& d = c->d;
   const int R = g.R;
   const size_t n = g.npad;
@@ -360,23 +378,23 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
   // z-space operators: forward A writes its u, v rows straight into the
   // target vector (the preconditioner passes u, v through unchanged,
   // steppers.py:247-249); the transposes go through z in full
-  auto apply_A = [&](const T* x, const double* xs, CVec5<T> b, T* target, const int* act) {
-    if (transpose) launch_matvec_t<T>(d, cf, g.cview(x), xs, b, g.view(g.z()), g.tmp, act, st);
-    else launch_matvec<T>(d, cf, g.cview(x), xs, b, g.split(target, g.z()), act, st);
+  auto apply_A = [&](const T* x, const double* xs, CVec5<T> b, T* target, const int* act, cudaStream_t s) {
+    if (transpose) launch_matvec_t<T>(d, cf, g.cview(x), xs, b, g.view(g.z()), g.tmp, act, s);
+    else launch_matvec<T>(d, cf, g.cview(x), xs, b, g.split(target, g.z()), act, s);
   };
-  auto apply_M = [&](const T* src_full, T* target, const int* act) {
-    if (transpose) launch_precond_t<T>(d, cf, g.cview(src_full), g.view(target), act, st);
-    else launch_precond<T>(d, cf, g.cview(src_full), g.view(target), act, st);
+  auto apply_M = [&](const T* src_full, T* target, const int* act, cudaStream_t s) {
+    if (transpose) launch_precond_t<T>(d, cf, g.cview(src_full), g.view(target), act, s);
+    else launch_precond<T>(d, cf, g.cview(src_full), g.view(target), act, s);
   };
-  auto apply_M_after_A = [&](T* target, const int* act) {
-    if (transpose) launch_precond_t<T>(d, cf, g.cview(g.z()), g.view(target), act, st);
-    else launch_precond<T>(d, cf, as_const(g.split(target, g.z())), g.view(target), act, st);
+  auto apply_M_after_A = [&](T* target, const int* act, cudaStream_t s) {
+    if (transpose) launch_precond_t<T>(d, cf, g.cview(g.z()), g.view(target), act, s);
+    else launch_precond<T>(d, cf, as_const(g.split(target, g.z())), g.view(target), act, s);
   };
   const int na = transpose ? 2 : 1, nm = transpose ? 2 : 1;
   if (method == SISL_GMRES_INCREMENTAL) {
     {
       KScope k(c, SISL_K_PRECOND, st, nm);
-      apply_M(g.bg(), g.V(1), nullptr);
+      apply_M(g.bg(), g.V(1), nullptr, st);
     }
     KScope k(c, SISL_K_DOTS, st);
     gm_dots<T>(g.V(0), n, 0, g.V(1), n, g.partial, gs, 2 /*MBNORM*/, 0, st);
@@ -385,10 +403,10 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
     KScope k(c, SISL_K_OTHER, st);
     gm_init_tol(gs, st);
   }
-  // residual of the initial guess
-  auto residual_and_read = [&](GHostView* out) -> int {
+  // preconditioned residual M (b - A x), normalised into V(0)
+  auto residual = [&](cudaStream_t s) {
     if (refine) {
-      KScope k(c, SISL_K_MATVEC, st, na + 1);
+      KScope k(c, SISL_K_MATVEC, s, na + 1);
       CVec5<double> x5, b5;
       Vec5<double> r5;
       for (int q = 0; q < 5; ++q) {
@@ -397,78 +415,143 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
         r5.f[q] = g.r64 + g.off[q];
       }
       if (transpose) {
-        launch_matvec_t<double>(d, cf64, x5, nullptr, b5, r5, g.tmp64, nullptr, st);
-        convert_packed_kernel<double, T><<<nconv, 256, 0, st>>>(g.r64, g.z(), g.z(), n, n);
+        launch_matvec_t<double>(d, cf64, x5, nullptr, b5, r5, g.tmp64, nullptr, s);
+        convert_packed_kernel<double, T><<<nconv, 256, 0, s>>>(g.r64, g.z(), g.z(), n, n);
       } else {
-        launch_matvec<double>(d, cf64, x5, nullptr, b5, r5, nullptr, st);
-        convert_packed_kernel<double, T><<<nconv, 256, 0, st>>>(g.r64, g.V(0), g.z(), g.off[2], n);
+        launch_matvec<double>(d, cf64, x5, nullptr, b5, r5, nullptr, s);
+        convert_packed_kernel<double, T><<<nconv, 256, 0, s>>>(g.r64, g.V(0), g.z(), g.off[2], n);
       }
     } else {
-      KScope k(c, SISL_K_MATVEC, st, na);
-      apply_A(g.xg(), nullptr, g.cview(g.bg()), g.V(0), nullptr);
+      KScope k(c, SISL_K_MATVEC, s, na);
+      apply_A(g.xg(), nullptr, g.cview(g.bg()), g.V(0), nullptr, s);
     }
     {
-      KScope k(c, SISL_K_PRECOND, st, nm);
-      apply_M_after_A(g.V(0), nullptr);
+      KScope k(c, SISL_K_PRECOND, s, nm);
+      apply_M_after_A(g.V(0), nullptr, s);
     }
     {
-      KScope k(c, SISL_K_DOTS, st);
-      gm_dots<T>(g.V(0), n, 0, g.V(0), n, g.partial, gs, 3 /*RNORM*/, 0, st);
+      KScope k(c, SISL_K_DOTS, s);
+      gm_dots<T>(g.V(0), n, 0, g.V(0), n, g.partial, gs, 3 /*RNORM*/, 0, s);
     }
+  };
+  // one restart cycle: R Arnoldi steps, the small least-squares solve, x update
+  auto cycle = [&](cudaStream_t s) {
+    {
+      KScope k(c, SISL_K_OTHER, s);
+      gm_begin_cycle(gs, s);
+    }
+    for (int j = 0; j < R; ++j) {
+      {
+        KScope k(c, SISL_K_MATVEC, s, na, mvb);
+        apply_A(g.V(j), &gs->s[j], none, g.V(j + 1), &gs->active, s);
+      }
+      {
+        KScope k(c, SISL_K_PRECOND, s, nm, pcb);
+        apply_M_after_A(g.V(j + 1), &gs->active, s);
+      }
+      {
+        KScope k(c, SISL_K_DOTS, s, 1, vb * (j + 2));  // reads V_0..V_j and w
+        gm_dots<T>(g.V(0), n, j + 1, g.V(j + 1), n, g.partial, gs, 0 /*PROJ*/, 1, s);
+      }
+      {
+        KScope k(c, SISL_K_UPDATE, s, 1, vb * (j + 3));  // reads V_0..V_j, reads and writes w
+        gm_update<T>(g.V(0), n, j + 1, g.V(j + 1), n, -1.0, g.partial, gs, 1 /*ARNOLDI*/, 1, 0, s);
+      }
+    }
+    {
+      KScope k(c, SISL_K_OTHER, s);
+      gm_small_solve(gs, R, s);
+    }
+    {
+      KScope k(c, SISL_K_UPDATE, s);
+      if (refine) gm_update_x64<T>(g.V(0), n, R, g.x64, n, gs, s);
+      else gm_update<T>(g.V(0), n, R, g.xg(), n, 1.0, g.partial, gs, 0 /*NONE*/, 0, 1, s);
+    }
+  };
+  auto finish_x = [&]() {
+    if (refine) {
+      KScope k(c, SISL_K_OTHER, st);
+      convert_packed_kernel<double, T><<<nconv, 256, 0, st>>>(g.x64, g.xg(), g.xg(), n, n);
+    }
+  };
+  const int maxiter = c->prm.solver_maxiter;
+
+  if (dev_info) {  // ---- graph mode ----
+    if (!c->cap_side) return SISL_ERR_ARG;
+    residual(st);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t gr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    if (cuda_failed(cudaStreamGetCaptureInfo(st, &cs, nullptr, &gr, &deps, &nd), "cudaStreamGetCaptureInfo") ||
+        cs != cudaStreamCaptureStatusActive)
+      return SISL_ERR_ARG;
+    cudaGraphConditionalHandle h;
+    if (cuda_failed(cudaGraphConditionalHandleCreate(&h, gr, 0, cudaGraphCondAssignDefault),
+                    "cudaGraphConditionalHandleCreate"))
+      return SISL_ERR_CUDA;
+    {
+      KScope k(c, SISL_K_OTHER, st);
+      gm_gate(gs, h, maxiter, 0, st);
+    }
+    if (cuda_failed(cudaStreamGetCaptureInfo(st, &cs, nullptr, &gr, &deps, &nd), "cudaStreamGetCaptureInfo"))
+      return SISL_ERR_CUDA;
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cuda_failed(cudaGraphAddNode(&node, gr, deps, nd, &np), "cudaGraphAddNode(conditional)")) return SISL_ERR_CUDA;
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    if (cuda_failed(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
+                    "cudaStreamUpdateCaptureDependencies"))
+      return SISL_ERR_CUDA;
+    cudaStream_t sb = c->cap_side;
+    if (cuda_failed(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+                    "cudaStreamBeginCaptureToGraph"))
+      return SISL_ERR_CUDA;
+    cycle(sb);
+    residual(sb);
+    {
+      KScope k(c, SISL_K_OTHER, sb);
+      gm_gate(gs, h, maxiter, 1, sb);
+    }
+    cudaGraph_t body_out = nullptr;
+    if (cuda_failed(cudaStreamEndCapture(sb, &body_out), "cudaStreamEndCapture(body)")) return SISL_ERR_CUDA;
+    {
+      KScope k(c, SISL_K_OTHER, st);
+      gm_info(gs, dev_info, st);
+    }
+    finish_x();
+    return check_cuda();
+  }
+
+  // ---- host mode ----
+  GHostView* hv = c->hv;
+  auto read = [&]() -> int {
     GHostView* dv = g.dview;
     {
       KScope k(c, SISL_K_OTHER, st);
       gm_snapshot(gs, dv, st);
     }
-    if (cudaMemcpyAsync(out, dv, sizeof(GHostView), cudaMemcpyDeviceToHost, st) != cudaSuccess) return SISL_ERR_CUDA;
+    if (cudaMemcpyAsync(hv, dv, sizeof(GHostView), cudaMemcpyDeviceToHost, st) != cudaSuccess) return SISL_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return SISL_ERR_CUDA;
     return SISL_OK;
   };
-  GHostView* hv = c->hv;
-  int rc = residual_and_read(hv);
+  residual(st);
+  int rc = read();
   if (rc) return rc;
   int cycles = 0, steps = 0;
-  while (cycles < c->prm.solver_maxiter && hv->rnorm > hv->atol) {
-    {
-      KScope k(c, SISL_K_OTHER, st);
-      gm_begin_cycle(gs, st);
-    }
-    for (int j = 0; j < R; ++j) {
-      {
-        KScope k(c, SISL_K_MATVEC, st, na, mvb);
-        apply_A(g.V(j), &gs->s[j], none, g.V(j + 1), &gs->active);
-      }
-      {
-        KScope k(c, SISL_K_PRECOND, st, nm, pcb);
-        apply_M_after_A(g.V(j + 1), &gs->active);
-      }
-      {
-        KScope k(c, SISL_K_DOTS, st, 1, vb * (j + 2));  // reads V_0..V_j and w
-        gm_dots<T>(g.V(0), n, j + 1, g.V(j + 1), n, g.partial, gs, 0 /*PROJ*/, 1, st);
-      }
-      {
-        KScope k(c, SISL_K_UPDATE, st, 1, vb * (j + 3));  // reads V_0..V_j, reads and writes w
-        gm_update<T>(g.V(0), n, j + 1, g.V(j + 1), n, -1.0, g.partial, gs, 1 /*ARNOLDI*/, 1, 0, st);
-      }
-    }
-    {
-      KScope k(c, SISL_K_OTHER, st);
-      gm_small_solve(gs, R, st);
-    }
-    {
-      KScope k(c, SISL_K_UPDATE, st);
-      if (refine) gm_update_x64<T>(g.V(0), n, R, g.x64, n, gs, st);
-      else gm_update<T>(g.V(0), n, R, g.xg(), n, 1.0, g.partial, gs, 0 /*NONE*/, 0, 1, st);
-    }
-    rc = residual_and_read(hv);
+  while (cycles < maxiter && hv->rnorm > hv->atol) {
+    cycle(st);
+    residual(st);
+    rc = read();
     if (rc) return rc;
     steps += hv->kdone;
     cycles++;
   }
-  if (refine) {
-    KScope k(c, SISL_K_OTHER, st);
-    convert_packed_kernel<double, T><<<nconv, 256, 0, st>>>(g.x64, g.xg(), g.xg(), n, n);
-  }
+  finish_x();
   if (info) {
     info->cycles = cycles;
     info->arnoldi_steps = steps;
@@ -484,7 +567,7 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
 // SemiImplicitSolver3D.solve: scale, GMRES, unscale (steppers.py:401-496).
 template <typename T>
 int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, const CVec5<T>* x0, Vec5<T> x,
-                   cudaStream_t st, SislSolveInfo* info) {
+                   cudaStream_t st, SislSolveInfo* info, GDevInfo* dev_info = nullptr) {
   const Dims& d = c->d;
   {
     KScope k(c, SISL_K_OTHER, st);
@@ -495,7 +578,7 @@ int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, co
   scale5<T>(c, cf, rhs, g.view(g.bg()), ps, 0, st);       // rhs_scaled: pi * pi_scale
   if (x0) scale5<T>(c, cf, *x0, g.view(g.xg()), ps, 1, st);  // x0 scaled: pi * ps, eta * dz_w
   else scale5<T>(c, cf, rhs, g.view(g.xg()), ps, 0, st);     // x0 = rhs_scaled
-  int rc = gmres_run<T>(c, cf, g, st, info);
+  int rc = gmres_run<T>(c, cf, g, st, info, 0, dev_info);
   if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
   scale5<T>(c, cf, g.cview(g.xg()), x, (T)(1.0 / c->s.ps), 2, st);  // pi / ps, eta / dz_w
   (void)d;
@@ -575,7 +658,8 @@ SWork<T> carve_step(Carver& cv, const Dims& d, int R, bool refine) {
 
 template <typename T>
 int step_impl(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
-              size_t ws_bytes, cudaStream_t st, SislStepInfo* info, void* const* tape = nullptr) {
+              size_t ws_bytes, cudaStream_t st, SislStepInfo* info, void* const* tape = nullptr,
+              GDevInfo* dev_info = nullptr) {
   const Dims& d = c->d;
   const Coef<T> cf = coef_of<T>(c);
   Carver cv{(char*)ws};
@@ -683,7 +767,7 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
     Vec5<T> xs;
     xs.f[0] = w.su; xs.f[1] = w.sv; xs.f[2] = ow; xs.f[3] = op; xs.f[4] = oe;
     SislSolveInfo si{};
-    int rc = solve_physical<T>(c, cf, w.g, as_const(rk), &x0, xs, st, &si);
+    int rc = solve_physical<T>(c, cf, w.g, as_const(rk), &x0, xs, st, &si, dev_info ? dev_info + it : nullptr);
     if (info) info->solve[it] = si;
     if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
     if (tape) {  // the physical solution of this solve, for the recomputation of the VJP
@@ -748,6 +832,8 @@ bool valid_grid(const SislGrid* g) {
 extern "C" {
 
 int sisl_version(void) { return 1; }
+
+const char* sisl_last_error(void) { return g_last_error; }
 
 const char* sisl_status_string(int s) {
   switch (s) {
@@ -1199,6 +1285,139 @@ int sisl_step_taped(SislCore* c, const SislState* in, const SislState* out, cons
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64) return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info, solves);
   return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info, solves);
+}
+
+}  // extern "C"
+
+struct SislStepGraph {
+  int n = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  GDevInfo* dinfo = nullptr;  // 2 per member, device
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;
+};
+
+namespace {
+void destroy_graph(SislStepGraph* g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->dinfo) cudaFree(g->dinfo);
+  for (cudaStream_t s : g->streams) cudaStreamDestroy(s);
+  for (cudaEvent_t e : g->events) cudaEventDestroy(e);
+  delete g;
+}
+}  // namespace
+
+extern "C" {
+
+int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                           const SislRelaxation* const* relax, void* const* ws, const size_t* ws_bytes, void* stream,
+                           SislStepGraph** out) {
+  if (!out || n < 1 || !cores || !ins || !outs || !ws || !ws_bytes) return SISL_ERR_ARG;
+  for (int m = 0; m < n; ++m) {
+    SislCore* c = cores[m];
+    if (!c || !ws[m] || ws_bytes[m] < sisl_workspace_bytes(c, SISL_WS_STEP)) return SISL_ERR_WORKSPACE;
+    const SislState& a = ins[m];
+    const SislState& b = outs[m];
+    const void* need[] = {a.u, a.v, a.w, a.eta_dot, a.pi_p, a.th_p, b.u, b.v, b.w, b.eta_dot, b.pi_p, b.th_p};
+    for (const void* p : need)
+      if (!p) return SISL_ERR_ARG;
+    if (a.is_first_step != 1.0 && (!a.u_prev || !a.v_prev || !a.eta_dot_prev)) return SISL_ERR_ARG;
+    for (int q = 0; q < m; ++q)
+      if (cores[q] == c) return SISL_ERR_ARG;  // a core's side stream serves one branch
+  }
+  SislStepGraph* g = new (std::nothrow) SislStepGraph();
+  if (!g) return SISL_ERR_ARG;
+  g_last_error[0] = 0;
+  g->n = n;
+  (void)stream;  // the graph is captured on a private stream (the caller's may be the legacy stream)
+  cudaStream_t st = nullptr;
+  auto fail = [&](int rc) {
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(st, &junk);
+      if (junk) cudaGraphDestroy(junk);
+    }
+    for (int m = 0; m < n; ++m) cores[m]->cap_side = nullptr;
+    cudaGetLastError();
+    destroy_graph(g);
+    return rc;
+  };
+  if (cuda_failed(cudaMalloc(&g->dinfo, sizeof(GDevInfo) * 2 * n), "cudaMalloc")) return fail(SISL_ERR_CUDA);
+  if (cuda_failed(cudaMemset(g->dinfo, 0, sizeof(GDevInfo) * 2 * n), "cudaMemset")) return fail(SISL_ERR_CUDA);
+  // member streams, side streams for the conditional bodies, fork and join events
+  for (int q = 0; q < 2 * n + 1; ++q) {
+    cudaStream_t s;
+    if (cuda_failed(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate")) return fail(SISL_ERR_CUDA);
+    g->streams.push_back(s);
+  }
+  st = g->streams[2 * n];
+  for (int q = 0; q < n + 1; ++q) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(SISL_ERR_CUDA);
+    g->events.push_back(e);
+  }
+  for (int m = 0; m < n; ++m)
+    if (cores[m]->timing_class != SISL_K_NONE) return fail(SISL_ERR_ARG);  // no timing events inside a graph
+  if (cuda_failed(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture"))
+    return fail(SISL_ERR_CUDA);
+  if (cuda_failed(cudaEventRecord(g->events[n], st), "cudaEventRecord(fork)")) return fail(SISL_ERR_CUDA);
+  for (int m = 0; m < n; ++m) {
+    SislCore* c = cores[m];
+    cudaStream_t ms = g->streams[m];
+    if (cuda_failed(cudaStreamWaitEvent(ms, g->events[n], 0), "cudaStreamWaitEvent(fork)")) return fail(SISL_ERR_CUDA);
+    c->cap_side = g->streams[n + m];
+    const SislRelaxation* rl = relax ? relax[m] : nullptr;
+    int rc = (c->grid.dtype == SISL_F64)
+                 ? step_impl<double>(c, &ins[m], &outs[m], rl, ws[m], ws_bytes[m], ms, nullptr, nullptr,
+                                     g->dinfo + 2 * m)
+                 : step_impl<float>(c, &ins[m], &outs[m], rl, ws[m], ws_bytes[m], ms, nullptr, nullptr,
+                                    g->dinfo + 2 * m);
+    c->cap_side = nullptr;
+    if (rc < 0) {
+      if (!g_last_error[0]) snprintf(g_last_error, sizeof(g_last_error), "step of member %d: status %d", m, rc);
+      return fail(rc);
+    }
+    if (cuda_failed(cudaEventRecord(g->events[m], ms), "cudaEventRecord(join)")) return fail(SISL_ERR_CUDA);
+    if (cuda_failed(cudaStreamWaitEvent(st, g->events[m], 0), "cudaStreamWaitEvent(join)")) return fail(SISL_ERR_CUDA);
+  }
+  if (cuda_failed(cudaStreamEndCapture(st, &g->graph), "cudaStreamEndCapture")) return fail(SISL_ERR_CUDA);
+  if (cuda_failed(cudaGraphInstantiate(&g->exec, g->graph, 0), "cudaGraphInstantiate")) return fail(SISL_ERR_CUDA);
+  *out = g;
+  return SISL_OK;
+}
+
+int sisl_step_graph_launch(SislStepGraph* g, void* stream) {
+  if (!g || !g->exec) return SISL_ERR_ARG;
+  g_launches += 1;
+  if (cuda_failed(cudaGraphLaunch(g->exec, (cudaStream_t)stream), "cudaGraphLaunch")) return SISL_ERR_CUDA;
+  return SISL_OK;
+}
+
+int sisl_step_graph_info(SislStepGraph* g, int member, SislStepInfo* info, void* stream) {
+  if (!g || !info || member < 0 || member >= g->n) return SISL_ERR_ARG;
+  GDevInfo h[2];
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(h, g->dinfo + 2 * member, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return SISL_ERR_CUDA;
+  int status = SISL_OK;
+  for (int q = 0; q < 2; ++q) {
+    std::memcpy(&info->solve[q], &h[q], sizeof(SislSolveInfo));
+    if (!std::isfinite(h[q].residual_norm)) status = SISL_ERR_NONFINITE;
+    else if (!h[q].converged && status == SISL_OK) status = SISL_NOT_CONVERGED;
+  }
+  info->kernel_launches = 0;
+  return status;
+}
+
+int sisl_step_graph_destroy(SislStepGraph* g) {
+  if (!g) return SISL_ERR_ARG;
+  destroy_graph(g);
+  return SISL_OK;
 }
 
 int sisl_core_set_refinement(SislCore* c, int on) {

@@ -148,6 +148,9 @@ template <typename T>
 void gm_update_x64(const T* Vb, size_t stride, int m, double* x, size_t n, const GState* gs, cudaStream_t st);
 void gm_setup(GState* gs, double eps, double tol, double atol_in, int restart, int method, cudaStream_t st);
 void gm_init_tol(GState* gs, cudaStream_t st);
+struct GDevInfo;
+void gm_gate(GState* gs, cudaGraphConditionalHandle h, int maxiter, int after_cycle, cudaStream_t st);
+void gm_info(const GState* gs, GDevInfo* o, cudaStream_t st);
 void gm_begin_cycle(GState* gs, cudaStream_t st);
 void gm_small_solve(GState* gs, int restart, cudaStream_t st);
 void gm_snapshot(const GState* gs, GHostView* v, cudaStream_t st);

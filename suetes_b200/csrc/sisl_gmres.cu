@@ -317,7 +317,30 @@ __global__ void setup_kernel(GState* gs, double eps, double tol, double atol_in,
   gs->active = 1;
   gs->kdone = 0;
   gs->breakdown = 0;
+  gs->cycles = 0;
+  gs->steps = 0;
   for (int q = 0; q < GM_MAXR + 2; ++q) gs->s[q] = 0.0;
+}
+
+// Graph mode: after a residual, count the finished cycle and set the WHILE
+// condition: another cycle while ||M r|| > atol and cycles < maxiter.
+__global__ void gate_kernel(GState* gs, cudaGraphConditionalHandle h, int maxiter, int after_cycle) {
+  if (after_cycle) {
+    gs->cycles += 1;
+    gs->steps += gs->kdone;
+  }
+  const bool more = (gs->rnorm > gs->atol) && (gs->cycles < maxiter);
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+__global__ void info_kernel(const GState* gs, GDevInfo* o) {
+  o->cycles = gs->cycles;
+  o->arnoldi_steps = gs->steps;
+  o->converged = (gs->rnorm <= gs->atol) ? 1 : 0;
+  o->pad = 0;
+  o->residual_norm = gs->rnorm;
+  o->atol = gs->atol;
+  o->b_norm = gs->bnorm;
 }
 
 __global__ void init_tol_kernel(GState* gs) {
@@ -460,6 +483,10 @@ void gm_setup(GState* gs, double eps, double tol, double atol_in, int restart, i
   setup_kernel<<<1, 1, 0, st>>>(gs, eps, tol, atol_in, restart, method);
 }
 void gm_init_tol(GState* gs, cudaStream_t st) { init_tol_kernel<<<1, 1, 0, st>>>(gs); }
+void gm_gate(GState* gs, cudaGraphConditionalHandle h, int maxiter, int after_cycle, cudaStream_t st) {
+  gate_kernel<<<1, 1, 0, st>>>(gs, h, maxiter, after_cycle);
+}
+void gm_info(const GState* gs, GDevInfo* o, cudaStream_t st) { info_kernel<<<1, 1, 0, st>>>(gs, o); }
 void gm_begin_cycle(GState* gs, cudaStream_t st) { begin_cycle_kernel<<<1, 256, 0, st>>>(gs); }
 void gm_small_solve(GState* gs, int restart, cudaStream_t st) {
   const size_t smem = (size_t)restart * restart * sizeof(double);

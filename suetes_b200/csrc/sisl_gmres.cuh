@@ -26,6 +26,14 @@ struct GState {
   int method;                       // 0 batched, 1 incremental
   int breakdown;
   unsigned int counter;             // last-block-done ticket
+  int cycles, steps;                // restart cycles and Arnoldi steps taken (graph mode)
+};
+
+// Per-solve statistics written on the device in graph mode; the same layout
+// as SislSolveInfo.
+struct GDevInfo {
+  int32_t cycles, arnoldi_steps, converged, pad;
+  double residual_norm, atol, b_norm;
 };
 
 // Host-visible summary copied back once per restart cycle.

@@ -486,3 +486,114 @@ class StateRing:
         for k in ("u", "v", "w", "eta_dot"):
             out.t[k + "_prev"] = cur.t[k]
         return out
+
+
+class StepGraph:
+    """One step of one or more members as a single CUDA graph (``sisl_step_graph_*``).
+
+    ``members``: sequence of ``(stepper, ds_in, ds_out, relax)``; member m
+    advances ``ds_in`` into ``ds_out`` (fixed buffers, distinct cores).  The
+    GMRES restart loops are conditional nodes decided on the device, so a
+    launch needs no host synchronisation; ``info(m)`` reads the solve
+    statistics of the last launch.  ``PingPong`` alternates two graphs for
+    repeated steps."""
+
+    def __init__(self, members):
+        self.lib = _lib.load()
+        n = len(members)
+        cores, ins, outs, relax, ws, nbytes = [], [], [], [], [], []
+        self._keep = []
+        for stepper, din, dout, rl in members:
+            core = din.core
+            if dout.core is not core:
+                raise ValueError("input and output states of a member must share a core")
+            if core in cores:
+                raise ValueError("every member needs its own core")
+            cores.append(core)
+            ins.append(din.c_struct())
+            outs.append(dout.c_struct())
+            relax.append(ctypes.pointer(rl.c_struct(core)) if rl is not None else None)
+            buf, nb = core.workspace(_lib.WS_STEP)
+            ws.append(buf)
+            nbytes.append(nb)
+            self._keep += [din, dout, rl, buf]
+        self.cores = cores
+        self.device = cores[0].device
+        carr = (ctypes.c_void_p * n)(*[c.handle.value for c in cores])
+        iarr = (_lib.SislState * n)(*ins)
+        oarr = (_lib.SislState * n)(*outs)
+        rarr = (ctypes.c_void_p * n)(*[ctypes.cast(r, ctypes.c_void_p).value if r is not None else None
+                                      for r in relax])
+        warr = (ctypes.c_void_p * n)(*[b.data_ptr() for b in ws])
+        barr = (ctypes.c_size_t * n)(*nbytes)
+        self._keep += [carr, iarr, oarr, rarr, warr, barr, relax]
+        h = ctypes.c_void_p()
+        from .core import stream_ptr
+        check(self.lib.sisl_step_graph_create(n, carr, iarr, oarr, rarr, warr, barr, stream_ptr(self.device),
+                                              ctypes.byref(h)), "sisl_step_graph_create")
+        self.handle, self.n = h, n
+        self.outs = [m[2] for m in members]
+
+    def launch(self):
+        from .core import stream_ptr
+        check(self.lib.sisl_step_graph_launch(self.handle, stream_ptr(self.device)), "sisl_step_graph_launch")
+        for ds in self.outs:
+            ds.is_first_step = 0.0
+
+    def info(self, member=0):
+        from .core import stream_ptr
+        inf = _lib.SislStepInfo()
+        rc = self.lib.sisl_step_graph_info(self.handle, int(member), ctypes.byref(inf), stream_ptr(self.device))
+        check(rc, "sisl_step_graph_info")
+        return {"status": rc, "solves": [inf.solve[0].as_dict(), inf.solve[1].as_dict()]}
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self.lib.sisl_step_graph_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+class PingPong:
+    """Repeated graph steps of a set of members: two DeviceStates per member
+    (A, B) and the graphs A -> B and B -> A; ``step()`` launches the next one.
+
+    The first-step flag (no trajectory extrapolation, steppers.py:748-762)
+    is fixed when a graph is captured, so a member still on its first step
+    takes that step eagerly here (``steps_done`` counts it)."""
+
+    def __init__(self, members):
+        """``members``: sequence of ``(stepper, ds0, relax)``; ds0 is copied."""
+        self.a, self.b, spec_ab, spec_ba = [], [], [], []
+        self.steps_done = 0
+        for stepper, ds0, rl in members:
+            core = ds0.core
+            A, B = DeviceState(core), DeviceState(core)
+            if ds0.is_first_step == 1.0:
+                stepper.step_device(ds0, A, rl)
+                self.steps_done = 1
+            else:
+                for k, v in ds0.t.items():
+                    A.t[k].copy_(v)
+            A.is_first_step = B.is_first_step = 0.0
+            self.a.append(A)
+            self.b.append(B)
+            spec_ab.append((stepper, A, B, rl))
+            spec_ba.append((stepper, B, A, rl))
+        if self.steps_done and any(ds0.is_first_step != 1.0 for _, ds0, _ in members):
+            raise ValueError("members must all be on their first step or all past it")
+        self.g = [StepGraph(spec_ab), StepGraph(spec_ba)]
+        self.k = 0
+
+    def step(self):
+        self.g[self.k % 2].launch()
+        self.k += 1
+
+    def current(self):
+        return self.b if self.k % 2 == 1 else self.a
+
+    def info(self, member=0):
+        return self.g[(self.k - 1) % 2].info(member)

@@ -1,0 +1,82 @@
+"""CUDA-graph steps (sisl_step_graph_*) against the eager sisl_step.
+
+A graph replays the same kernels in the same order, the GMRES restart loops
+as device-decided conditional nodes, so its states must equal the eager
+steps bit for bit, with the same solve statistics; members of different
+sizes in one graph must each equal their own eager run.
+"""
+
+import pytest
+import torch
+
+from suetes_b200.workloads import rising_bubble
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u", "v", "w", "eta_dot", "pi_p", "th_p", "rho", "u_prev", "tend_th_prev")
+
+
+def _eager(stepper, ds0, relax, nsteps):
+    from suetes_b200 import DeviceState
+    core = ds0.core
+    cur = DeviceState(core, {k: v.clone() for k, v in ds0.t.items()}, ds0.is_first_step)
+    infos = []
+    for _ in range(nsteps):
+        nxt = DeviceState(core)
+        infos.append(stepper.step_device(cur, nxt, relax))
+        cur = nxt
+    return cur, infos
+
+
+def _member(n, nz, dtype, amp=2.0, tol=None, maxiter=30):
+    st, s0, bc = rising_bubble(n, n, nz, dx=50.0, amp=amp, dtype=dtype,
+                               solver_tol=tol or (1e-10 if dtype == torch.float64 else 1e-7),
+                               solver_maxiter=maxiter, solver_restart=30)
+    return st, st.to_device_state(s0), bc
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_graph_steps_equal_eager(dtype):
+    from suetes_b200 import PingPong
+    st, ds0, bc = _member(24, 16, dtype)
+    ref, infos = _eager(st, ds0, bc, 4)
+    pp = PingPong([(st, ds0, bc)])
+    assert pp.steps_done == 1
+    for _ in range(3):
+        pp.step()
+    out = pp.current()[0]
+    for k in FIELDS:
+        assert torch.equal(out.t[k], ref.t[k]), k
+    gi = pp.info(0)["solves"]
+    for q in range(2):
+        assert gi[q]["cycles"] == infos[-1]["solves"][q]["cycles"]
+        assert gi[q]["arnoldi_steps"] == infos[-1]["solves"][q]["arnoldi_steps"]
+        assert gi[q]["converged"]
+
+
+def test_graph_ensemble_members_equal_their_eager_runs():
+    from suetes_b200 import PingPong
+    specs = [(16, 12, 1.5), (24, 16, 2.5), (20, 10, 2.0)]
+    members = [_member(n, nz, torch.float32, amp=a) for n, nz, a in specs]
+    refs = [_eager(st, ds0, bc, 3)[0] for st, ds0, bc in members]
+    pp = PingPong(members)
+    pp.step()
+    pp.step()
+    for m, ref in enumerate(refs):
+        out = pp.current()[m]
+        for k in FIELDS:
+            assert torch.equal(out.t[k], ref.t[k]), (m, k)
+
+
+def test_graph_reports_unconverged_solves():
+    from suetes_b200 import PingPong
+    st, ds0, bc = _member(16, 12, torch.float64, tol=1e-14, maxiter=1)
+    ref, infos = _eager(st, ds0, bc, 2)
+    assert infos[-1]["status"] == 1  # SISL_NOT_CONVERGED
+    pp = PingPong([(st, ds0, bc)])
+    pp.step()
+    gi = pp.info(0)
+    assert gi["status"] == 1
+    assert gi["solves"][0]["cycles"] == 1 and not gi["solves"][0]["converged"]
+    for k in FIELDS:
+        assert torch.equal(pp.current()[0].t[k], ref.t[k]), k
