@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--cpu-window", type=int, default=32, help="nx = ny of the CPU-baseline window")
     ap.add_argument("--classes", action="store_true",
                     help="also time every GMRES kernel class separately (diagnostic)")
+    ap.add_argument("--ens-members", type=int, default=32,
+                    help="members of the uneven-size bubble ensemble leg (0 disables it)")
+    ap.add_argument("--ens-steps", type=int, default=10, help="timed graph steps of the ensemble leg")
     ap.add_argument("--vjp-steps", type=int, default=4,
                     help="trajectory length of the fwd+VJP leg (0 disables it)")
     ap.add_argument("--vjp-checkpoint", type=int, default=1, help="checkpoint interval of the fwd+VJP leg")
@@ -281,6 +284,57 @@ def timed_device_steps(stepper, ds0, relax, steps, warmup, world, timing_class=N
     return ms, infos, launches, kt, cur
 
 
+def ensemble_leg(args, local, world):
+    """The uneven-size bubble ensemble advanced as one CUDA graph per step
+    (members as parallel branches, GMRES loops as device-decided conditional
+    nodes), against the same members stepped one after another eagerly."""
+    from suetes_b200 import PingPong
+    from suetes_b200.core import kernel_launches
+    from suetes_b200.workloads import bubble_ensemble
+    ens = bubble_ensemble(args.ens_members, seed=1, device=f"cuda:{local}", solver_tol=args.tol32,
+                          solve_method=args.method)
+    cells = sum(sp["nx"] * sp["ny"] * sp["nz"] for _, _, _, sp in ens)
+    dss = [(st, st.to_device_state(s0), bc) for st, s0, bc, _ in ens]
+    pp = PingPong(dss)
+    W, K = 3, args.ens_steps
+    for _ in range(W):
+        pp.step()
+    torch.cuda.synchronize()
+    barrier(world)
+    l0 = kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(K):
+        pp.step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = dist_max(e0.elapsed_time(e1), world)
+    launches = kernel_launches() - l0
+    infos = [pp.info(m) for m in range(len(ens))]
+    conv = sum(1 for i in infos for q in i["solves"] if q["converged"]) / (2 * len(infos))
+    # the same members stepped eagerly one after another (host-driven GMRES loops)
+    from suetes_b200 import DeviceState
+    cur = [a for a in pp.current()]
+    nxt = [DeviceState(a.core) for a in cur]
+    for (st, _, bc), a, b in zip(dss, cur, nxt):
+        st.step_device(a, b, bc)
+    torch.cuda.synchronize()
+    e0.record()
+    for (st, _, bc), a, b in zip(dss, cur, nxt):
+        st.step_device(a, b, bc)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_seq = e0.elapsed_time(e1)
+    sizes = sorted({(sp["nx"], sp["ny"], sp["nz"]) for _, _, _, sp in ens})
+    return {"metric": "SISL cell-steps/s, uneven-size bubble ensemble", "value": world * cells * K / (ms / 1e3),
+            "unit": "cell-steps/s", "members": len(ens), "cells_per_step": cells, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "launch": "one CUDA graph per ensemble step (graph launches timed)",
+            "graph_launches": launches, "converged_frac": conv,
+            "eager_sequential": {"value": cells / (ms_seq / 1e3), "ms_per_step": ms_seq},
+            "speedup_vs_eager_sequential": ms_seq / (ms / K), "distinct_shapes": len(sizes),
+            "dtype": "f32", "gmres_tol": args.tol32, "method": args.method}
+
+
 def vjp_leg(args, local, world, cells, warm_state32):
     """Value and gradient of the box-energy objective over a trajectory of
     ``--vjp-steps`` steps (forward with the fused step recording its solves,
@@ -425,6 +479,10 @@ def run_ours(args):
     # ---- fwd+VJP: gradient of the lee box energy w.r.t. the initial theta' ----
     if args.vjp_steps > 0:
         line["fwd_vjp"] = vjp_leg(args, local, world, cells, cur32)
+
+    # ---- uneven-size ensemble under one CUDA graph per step ----
+    if args.ens_members > 0:
+        line["ensemble"] = ensemble_leg(args, local, world)
 
     # ---- end to end through the public API with host state ----
     if not args.no_e2e:

@@ -13,6 +13,10 @@
   1/2 rho (u'^2 + v^2 + w^2) in the lee (x in [5, 25] km, z in [1, 6] km,
   all y), patterned on the box-energy objective of
   experiments/schaer_optimal_perturbation/run.py:138-144.
+* ``bubble_ensemble``: the many-member configuration -- 32 warm-bubble
+  members of uneven sizes (nx, ny in {64, 96, 128, 160}, nz in {40, 48, 64},
+  dx = 50 m), amplitudes U[1, 3] K and centres jittered by +-300 m per axis,
+  seeded with numpy's default_rng.
 * ``rising_bubble``: 3-D dry warm bubble (64x64x48, 50 m, dt = 1 s,
   cos^2 bubble of 2 K, r = 1 km, 1.5 km above ground;
   cpu_gpu_short_scaling/run.py:38-55 in 3-D).
@@ -111,3 +115,23 @@ def box_energy_objective(stepper, num_steps, last=10, u_ref=10.0, x_box=(5000.0,
         return (w8 * 0.5 * st["rho"] * (um * um + vm * vm + wm * wm)).sum()
 
     return objective
+
+
+def bubble_ensemble(n_members=32, seed=0, dtype=F32, device="cuda", solver_tol=1e-7, solver_maxiter=30,
+                    solver_restart=30, solve_method="incremental", dt=1.0):
+    """[(stepper, state, bc, spec)] for the uneven-size bubble ensemble."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_members):
+        nx = int(rng.choice([64, 96, 128, 160]))
+        ny = int(rng.choice([64, 96, 128, 160]))
+        nz = int(rng.choice([40, 48, 64]))
+        amp = float(rng.uniform(1.0, 3.0))
+        jit = rng.uniform(-300.0, 300.0, size=3)
+        center = (float(jit[0]), float(jit[1]), 1500.0 + float(jit[2]))
+        st, state, bc = rising_bubble(nx, ny, nz, dx=50.0, amp=amp, center=center, dtype=dtype, device=device,
+                                      solver_tol=solver_tol, solver_maxiter=solver_maxiter,
+                                      solver_restart=solver_restart, solve_method=solve_method, dt=dt)
+        out.append((st, state, bc, {"nx": nx, "ny": ny, "nz": nz, "amp": amp, "center": center}))
+    return out
