@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--cpu-window", type=int, default=32, help="nx = ny of the CPU-baseline window")
     ap.add_argument("--classes", action="store_true",
                     help="also time every GMRES kernel class separately (diagnostic)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--ens-members", type=int, default=32,
                     help="members of the uneven-size bubble ensemble leg (0 disables it)")
     ap.add_argument("--ens-steps", type=int, default=10, help="timed graph steps of the ensemble leg")
@@ -295,7 +296,7 @@ def ensemble_leg(args, local, world):
                           solve_method=args.method)
     cells = sum(sp["nx"] * sp["ny"] * sp["nz"] for _, _, _, sp in ens)
     dss = [(st, st.to_device_state(s0), bc) for st, s0, bc, _ in ens]
-    pp = PingPong(dss)
+    pp = PingPong(dss, autotune=not args.no_autotune)
     W, K = 3, args.ens_steps
     for _ in range(W):
         pp.step()
@@ -332,7 +333,18 @@ def ensemble_leg(args, local, world):
             "graph_launches": launches, "converged_frac": conv,
             "eager_sequential": {"value": cells / (ms_seq / 1e3), "ms_per_step": ms_seq},
             "speedup_vs_eager_sequential": ms_seq / (ms / K), "distinct_shapes": len(sizes),
-            "dtype": "f32", "gmres_tol": args.tol32, "method": args.method}
+            "dtype": "f32", "gmres_tol": args.tol32, "method": args.method,
+            "autotune": _tuning_summary(pp.tuning)}
+
+
+def _tuning_summary(tunings):
+    """Histogram of the autotuner's choices over the members."""
+    out = {}
+    for t in tunings:
+        for k in ("matvec_block", "precond_tile", "matvec_t_block", "precond_t_tile"):
+            out.setdefault(k, {})
+            out[k][str(t[k])] = out[k].get(str(t[k]), 0) + 1
+    return out
 
 
 def vjp_leg(args, local, world, cells, warm_state32):
@@ -406,6 +418,7 @@ def run_ours(args):
     st32, s32, bc = mountain_wave(nx, ny, nz, dtype=torch.float32, device=f"cuda:{local}", solver_tol=args.tol32,
                                   solve_method=args.method, refine=not args.no_refine)
     ds = st32.to_device_state(s32)
+    tuning = None if args.no_autotune else ds.core.autotune()
     with ClockSampler(local) as clk:
         ms, infos, launches, kt, cur32 = timed_device_steps(st32, ds, bc, K, W, world, cls)
     ms = dist_max(ms, world)
@@ -431,7 +444,8 @@ def run_ours(args):
                                    f"GMRES restart 30 maxiter 30", "nx": nx, "ny": ny, "nz": nz,
                        "parallelism": f"replicas x{world}", "l2": "working set > 126 MB L2 (no flush)",
                        "gmres_tol_f32": args.tol32, "gmres_tol_f64": args.tol64},
-            "gmres": gm, "gpu_launches": launches, "clocks": clk.summary(), "roofline": roofline}
+            "gmres": gm, "gpu_launches": launches, "clocks": clk.summary(), "roofline": roofline,
+            "autotune": tuning}
 
     # ---- float64 leg and float32-vs-float64 error ----
     if not args.no_fp64:

@@ -293,6 +293,22 @@ int sisl_step_taped(SislCore* core, const SislState* in, const SislState* out, c
  * jitted step (steppers.py:692-714) in one launch; the ensemble launch of
  * the many-member configuration.  Cores must be distinct and have no timing
  * class selected; relax may be NULL (or hold NULL entries). */
+/* Launch shapes of the Helmholtz kernels: stencil block variants (0-3:
+ * 32x4x2, 32x8x1, 32x2x4, 64x4x1 threads) of the matvec and of its
+ * transpose, and column-tile variants (0-2: 256 threads / 32 columns,
+ * 128 / 16, 256 / 64) of the preconditioner and of its transpose. */
+typedef struct SislTuning {
+  int32_t matvec_block, precond_tile, matvec_t_block, precond_t_tile;
+  float us[4];  /* microseconds per launch of the chosen shapes (sisl_autotune only) */
+} SislTuning;
+/* Project autotuner (no reference counterpart): time every candidate shape
+ * on this core's grid with CUDA events and keep the fastest in the core;
+ * results are bitwise the same for every shape.  ws: sisl_workspace_bytes(
+ * core, SISL_WS_GMRES) bytes; synchronises stream; not during a capture. */
+int sisl_autotune(SislCore* core, void* ws, size_t ws_bytes, void* stream, SislTuning* out);
+int sisl_autotune_query(const SislCore* core, SislTuning* out);
+/* Apply stored launch shapes (e.g. a cached sisl_autotune result). */
+int sisl_core_set_tuning(SislCore* core, const SislTuning* tuning);
 typedef struct SislStepGraph SislStepGraph;
 int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
                            const SislRelaxation* const* relax, void* const* ws, const size_t* ws_bytes,

@@ -57,6 +57,17 @@ class SislSolveInfo(ctypes.Structure):
                 "residual_norm": self.residual_norm, "atol": self.atol, "b_norm": self.b_norm}
 
 
+class SislTuning(ctypes.Structure):
+    _fields_ = [("matvec_block", ctypes.c_int32), ("precond_tile", ctypes.c_int32),
+                ("matvec_t_block", ctypes.c_int32), ("precond_t_tile", ctypes.c_int32),
+                ("us", ctypes.c_float * 4)]
+
+    def as_dict(self):
+        return {"matvec_block": self.matvec_block, "precond_tile": self.precond_tile,
+                "matvec_t_block": self.matvec_t_block, "precond_t_tile": self.precond_t_tile,
+                "us": [round(float(x), 2) for x in self.us]}
+
+
 class SislState(ctypes.Structure):
     _fields_ = [(n, vp) for n in ("u", "v", "w", "eta_dot", "pi_p", "th_p", "rho", "u_prev", "v_prev",
                                   "w_prev", "eta_dot_prev", "tend_th_prev")] + [("is_first_step", ctypes.c_double)]
@@ -123,6 +134,9 @@ PROTOTYPES = {
     "sisl_step_graph_launch": (ctypes.c_int, [vp, vp]),
     "sisl_step_graph_info": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SislStepInfo), vp]),
     "sisl_step_graph_destroy": (ctypes.c_int, [vp]),
+    "sisl_autotune": (ctypes.c_int, [vp, vp, ctypes.c_size_t, vp, ctypes.POINTER(SislTuning)]),
+    "sisl_autotune_query": (ctypes.c_int, [vp, ctypes.POINTER(SislTuning)]),
+    "sisl_core_set_tuning": (ctypes.c_int, [vp, ctypes.POINTER(SislTuning)]),
     "sisl_kernel_launches": (ctypes.c_int64, []),
     "sisl_timing_select": (ctypes.c_int, [vp, ctypes.c_int]),
     "sisl_timing_read": (ctypes.c_int, [vp, c_double_p, ctypes.POINTER(ctypes.c_int64), c_double_p]),

@@ -115,6 +115,22 @@ class Core:
             self.params.solver_restart = key[3]
             self._solver_key = key
 
+    def autotune(self):
+        """Choose the Helmholtz kernels' launch shapes by timing (``sisl_autotune``)."""
+        ws, n = self.workspace(_lib.WS_GMRES)
+        t = _lib.SislTuning()
+        check(self.lib.sisl_autotune(self.handle, ws.data_ptr(), n, self.stream, ctypes.byref(t)), "sisl_autotune")
+        return t.as_dict()
+
+    def set_tuning(self, matvec_block=0, precond_tile=0, matvec_t_block=0, precond_t_tile=0, **_):
+        t = _lib.SislTuning(matvec_block, precond_tile, matvec_t_block, precond_t_tile)
+        check(self.lib.sisl_core_set_tuning(self.handle, ctypes.byref(t)), "sisl_core_set_tuning")
+
+    def tuning(self):
+        t = _lib.SislTuning()
+        check(self.lib.sisl_autotune_query(self.handle, ctypes.byref(t)), "sisl_autotune_query")
+        return t.as_dict()
+
     def set_refinement(self, on):
         """float64 iterative refinement of a float32 core's GMRES (``sisl_core_set_refinement``)."""
         if self.dtype != F32:

@@ -279,13 +279,11 @@ __global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T
 // C: every thread writes pi, w and eta_dot.
 // Shared memory per block: (3 nz + 1) * 32 values of T.
 // ---------------------------------------------------------------------------
-constexpr int TPT = 256;  // threads per block
-constexpr int TPC = 32;   // columns per block
 
 template <typename T>
 __device__ __forceinline__ T pt_rcp(T x) { return T(1) / x; }
 
-template <typename T>
+template <typename T, int TPT, int TPC>
 __global__ void __launch_bounds__(TPT) pt_column_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
                                                         const int* active) {
   if (active && *active == 0) return;
@@ -552,17 +550,27 @@ template void launch_tricubic_vjp<double>(int, int, int, int, int, int, const do
                                           const double*, double*, int, double, cudaStream_t);
 
 // out = M^T y (out must not alias y).
-template <typename T>
-void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
+template <typename T, int TPT, int TPC>
+void launch_pt_column(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                       cudaStream_t st) {
   const size_t smem = (size_t)(3 * d.nz + 1) * TPC * sizeof(T);
   static size_t attr_bytes = 0;  // per instantiation
   if (smem > 48 * 1024 && smem > attr_bytes) {
-    cudaFuncSetAttribute(pt_column_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(pt_column_kernel<T, TPT, TPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr_bytes = smem;
   }
-  pt_column_kernel<T><<<dim3((d.nx + TPC - 1) / TPC, d.ny), TPT, smem, st>>>(d, c, y, out, active);
-  dim3 blk(32, 4, 2);
+  pt_column_kernel<T, TPT, TPC><<<dim3((d.nx + TPC - 1) / TPC, d.ny), TPT, smem, st>>>(d, c, y, out, active);
+}
+
+template <typename T>
+void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
+                      cudaStream_t st) {
+  switch (d.tune_pct) {
+    case 1: launch_pt_column<T, 128, 16>(d, c, y, out, active, st); break;
+    case 2: launch_pt_column<T, 256, 64>(d, c, y, out, active, st); break;
+    default: launch_pt_column<T, 256, 32>(d, c, y, out, active, st); break;
+  }
+  const dim3 blk = stencil_block(d.tune_mvt);
   pt_uv_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz, blk), blk, 0, st>>>(d, c, y, out, active);
 }
 
@@ -576,7 +584,7 @@ template void launch_precond_t<double>(const Dims&, const Coef<double>&, CVec5<d
 template <typename T>
 void launch_matvec_t(const Dims& d, const Coef<T>& c, CVec5<T> y, const double* yscale, CVec5<T> b, Vec5<T> out,
                      T* gzm_tmp, const int* active, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
+  const dim3 blk = stencil_block(d.tune_mvt);
   at_gzm_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, c, y.f[0], y.f[1], yscale, gzm_tmp, active);
   at_main_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, y, yscale, gzm_tmp, b, out,
                                                                               active);

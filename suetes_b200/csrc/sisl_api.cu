@@ -1420,6 +1420,106 @@ int sisl_step_graph_destroy(SislStepGraph* g) {
   return SISL_OK;
 }
 
+int sisl_core_set_tuning(SislCore* c, const SislTuning* t) {
+  if (!c || !t) return SISL_ERR_ARG;
+  if (t->matvec_block < 0 || t->matvec_block >= N_STENCIL_BLOCKS || t->matvec_t_block < 0 ||
+      t->matvec_t_block >= N_STENCIL_BLOCKS || t->precond_tile < 0 || t->precond_tile >= N_COLUMN_TILES ||
+      t->precond_t_tile < 0 || t->precond_t_tile >= N_COLUMN_TILES)
+    return SISL_ERR_ARG;
+  c->d.tune_mv = t->matvec_block;
+  c->d.tune_pc = t->precond_tile;
+  c->d.tune_mvt = t->matvec_t_block;
+  c->d.tune_pct = t->precond_t_tile;
+  return SISL_OK;
+}
+
+int sisl_autotune_query(const SislCore* c, SislTuning* out) {
+  if (!c || !out) return SISL_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->matvec_block = c->d.tune_mv;
+  out->precond_tile = c->d.tune_pc;
+  out->matvec_t_block = c->d.tune_mvt;
+  out->precond_t_tile = c->d.tune_pct;
+  return SISL_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// Time every candidate launch shape of the four tunable Helmholtz kernels on
+// this core's grid (CUDA events, warm launches) and keep the fastest.
+template <typename T>
+int autotune_impl(SislCore* c, void* ws, cudaStream_t st, SislTuning* out) {
+  Carver cv{(char*)ws};
+  GWork<T> g = carve_gmres<T>(cv, c->d, c->prm.solver_restart, false);
+  const Coef<T> cf = coef_of<T>(c);
+  for (int q = 0; q < 3; ++q)
+    if (cuda_failed(cudaMemsetAsync(g.V(q), 0, sizeof(T) * g.npad, st), "cudaMemsetAsync")) return SISL_ERR_CUDA;
+  if (cuda_failed(cudaMemsetAsync(g.z(), 0, sizeof(T) * g.npad, st), "cudaMemsetAsync")) return SISL_ERR_CUDA;
+  cudaEvent_t e0, e1;
+  if (cuda_failed(cudaEventCreate(&e0), "cudaEventCreate") || cuda_failed(cudaEventCreate(&e1), "cudaEventCreate"))
+    return SISL_ERR_CUDA;
+  const int reps = 8;
+  int rc = SISL_OK;
+  auto time_it = [&](auto&& launch) -> float {
+    launch();
+    launch();
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(e1, st);
+    float ms = 0.f;
+    if (cuda_failed(cudaEventSynchronize(e1), "cudaEventSynchronize") ||
+        cuda_failed(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime") || check_cuda() != SISL_OK) {
+      rc = SISL_ERR_CUDA;
+      return 1e30f;
+    }
+    return ms * 1000.f / reps;
+  };
+  CVec5<T> none{};
+  Dims& d = c->d;
+  auto pick = [&](int* field, int ncand, auto&& launch, float* us_out) {
+    int best = 0;
+    float tbest = 1e30f;
+    for (int v = 0; v < ncand && rc == SISL_OK; ++v) {
+      *field = v;
+      const float t = time_it(launch);
+      if (t < tbest) { tbest = t; best = v; }
+    }
+    *field = best;
+    *us_out = tbest;
+  };
+  pick(&d.tune_mv, N_STENCIL_BLOCKS,
+       [&] { launch_matvec<T>(d, cf, g.cview(g.V(0)), nullptr, none, g.split(g.V(1), g.z()), nullptr, st); },
+       &out->us[0]);
+  pick(&d.tune_pc, N_COLUMN_TILES,
+       [&] { launch_precond<T>(d, cf, as_const(g.split(g.V(1), g.z())), g.view(g.V(2)), nullptr, st); },
+       &out->us[1]);
+  pick(&d.tune_mvt, N_STENCIL_BLOCKS,
+       [&] { launch_matvec_t<T>(d, cf, g.cview(g.V(0)), nullptr, none, g.view(g.z()), g.tmp, nullptr, st); },
+       &out->us[2]);
+  pick(&d.tune_pct, N_COLUMN_TILES,
+       [&] { launch_precond_t<T>(d, cf, g.cview(g.z()), g.view(g.V(2)), nullptr, st); }, &out->us[3]);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  out->matvec_block = d.tune_mv;
+  out->precond_tile = d.tune_pc;
+  out->matvec_t_block = d.tune_mvt;
+  out->precond_t_tile = d.tune_pct;
+  return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int sisl_autotune(SislCore* c, void* ws, size_t ws_bytes, void* stream, SislTuning* out) {
+  if (!c || !out) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_GMRES)) return SISL_ERR_WORKSPACE;
+  if (c->timing_class != SISL_K_NONE) return SISL_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  cudaStream_t st = (cudaStream_t)stream;
+  return c->grid.dtype == SISL_F64 ? autotune_impl<double>(c, ws, st, out) : autotune_impl<float>(c, ws, st, out);
+}
+
 int sisl_core_set_refinement(SislCore* c, int on) {
   if (!c) return SISL_ERR_ARG;
   if (on && !c->coef64_mem) return SISL_ERR_ARG;

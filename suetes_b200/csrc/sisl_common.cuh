@@ -19,7 +19,23 @@ struct Dims {
   int nx, ny, nz;
   int px, py;          // periodic flags for x and y
   double dx, dy, dz;
+  // launch shapes chosen by the autotuner (sisl_autotune): Helmholtz matvec
+  // and its transpose (block shape), column preconditioner and its transpose
+  // (tile); 0 = the default
+  int tune_mv = 0, tune_pc = 0, tune_mvt = 0, tune_pct = 0;
 };
+
+// block shapes of the 3-D stencil kernels (256 threads each)
+__host__ inline dim3 stencil_block(int variant) {
+  switch (variant) {
+    case 1: return dim3(32, 8, 1);
+    case 2: return dim3(32, 2, 4);
+    case 3: return dim3(64, 4, 1);
+    default: return dim3(32, 4, 2);
+  }
+}
+constexpr int N_STENCIL_BLOCKS = 4;
+constexpr int N_COLUMN_TILES = 3;  // (threads, columns) = (256, 32), (128, 16), (256, 64)
 
 __host__ __device__ inline int ext_x(const Dims& d, int loc) { return d.nx + (loc == LOC_U); }
 __host__ __device__ inline int ext_y(const Dims& d, int loc) { return d.ny + (loc == LOC_V); }

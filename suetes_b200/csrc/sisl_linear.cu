@@ -168,8 +168,6 @@ __global__ void __launch_bounds__(256) matvec_kernel(Dims d, Coef<T> c, CVec5<T>
 __device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
 
-constexpr int PT = 256;  // threads per block
-constexpr int PC = 32;   // columns per block
 
 template <typename T>
 struct PrecondW {  // w-level quantities of one column at one level
@@ -202,7 +200,7 @@ __device__ __forceinline__ PrecondW<T> precond_wlevel(const Dims& d, const Coef<
   return o;
 }
 
-template <typename T>
+template <typename T, int PT, int PC>
 __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
                                                           const int* active) {
   if (active && *active == 0) return;
@@ -315,22 +313,32 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
 template <typename T>
 void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xscale, CVec5<T> b,
                    Vec5<T> out, const int* active, cudaStream_t st) {
-  dim3 blk(32, 4, 2);
-  dim3 grd((d.nx + 1 + 31) / 32, (d.ny + 1 + 3) / 4, (d.nz + 1 + 1) / 2);
+  const dim3 blk = stencil_block(d.tune_mv);
+  dim3 grd((d.nx + 1 + blk.x - 1) / blk.x, (d.ny + 1 + blk.y - 1) / blk.y, (d.nz + 1 + blk.z - 1) / blk.z);
   matvec_kernel<T><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+}
+
+template <typename T, int PT, int PC>
+void launch_precond_tile(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
+                         cudaStream_t st) {
+  const size_t smem = (size_t)(3 * d.nz + 1) * PC * sizeof(T);
+  static size_t attr_bytes = 0;  // per instantiation
+  if (smem > 48 * 1024 && smem > attr_bytes) {
+    cudaFuncSetAttribute(precond_tile_kernel<T, PT, PC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_bytes = smem;
+  }
+  dim3 grd((d.nx + PC - 1) / PC, d.ny);
+  precond_tile_kernel<T, PT, PC><<<grd, PT, smem, st>>>(d, c, r, out, active);
 }
 
 template <typename T>
 void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                     cudaStream_t st) {
-  const size_t smem = (size_t)(3 * d.nz + 1) * PC * sizeof(T);
-  static size_t attr_bytes = 0;  // per instantiation
-  if (smem > 48 * 1024 && smem > attr_bytes) {
-    cudaFuncSetAttribute(precond_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_bytes = smem;
+  switch (d.tune_pc) {
+    case 1: launch_precond_tile<T, 128, 16>(d, c, r, out, active, st); break;
+    case 2: launch_precond_tile<T, 256, 64>(d, c, r, out, active, st); break;
+    default: launch_precond_tile<T, 256, 32>(d, c, r, out, active, st); break;
   }
-  dim3 grd((d.nx + PC - 1) / PC, d.ny);
-  precond_tile_kernel<T><<<grd, PT, smem, st>>>(d, c, r, out, active);
 }
 
 template void launch_matvec<float>(const Dims&, const Coef<float>&, CVec5<float>, const double*, CVec5<float>,

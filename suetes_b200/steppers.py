@@ -565,12 +565,17 @@ class PingPong:
     is fixed when a graph is captured, so a member still on its first step
     takes that step eagerly here (``steps_done`` counts it)."""
 
-    def __init__(self, members):
-        """``members``: sequence of ``(stepper, ds0, relax)``; ds0 is copied."""
+    def __init__(self, members, autotune=False):
+        """``members``: sequence of ``(stepper, ds0, relax)``; ds0 is copied.
+        ``autotune``: choose each member core's launch shapes (``Core.autotune``)
+        before the graphs are captured."""
         self.a, self.b, spec_ab, spec_ba = [], [], [], []
         self.steps_done = 0
+        self.tuning = []
         for stepper, ds0, rl in members:
             core = ds0.core
+            if autotune:
+                self.tuning.append(core.autotune())
             A, B = DeviceState(core), DeviceState(core)
             if ds0.is_first_step == 1.0:
                 stepper.step_device(ds0, A, rl)

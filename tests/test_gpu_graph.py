@@ -80,3 +80,36 @@ def test_graph_reports_unconverged_solves():
     assert gi["solves"][0]["cycles"] == 1 and not gi["solves"][0]["converged"]
     for k in FIELDS:
         assert torch.equal(pp.current()[0].t[k], ref.t[k]), k
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_every_launch_shape_gives_identical_results(dtype):
+    """The autotuner's candidates (stencil blocks, column tiles) change only
+    the launch shape: forward and transposed operators are bitwise equal."""
+    from suetes_b200 import SemiImplicitSolver3D, VerticalPreconditioner
+    st, ds0, bc = _member(37, 13, dtype)
+    ph = st.physics
+    bg = ph.precompute_bg(ph.bg_state_ref())
+    sol = SemiImplicitSolver3D(ph, st.dt, alpha=st.alpha)
+    core = sol._core(dtype, bg)
+    pm = VerticalPreconditioner(ph, st.dt, alpha=st.alpha)
+    pm.precompute_banded(bg)
+    g = ph.grid
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    x = {k: torch.randn(g.shape_of(l), generator=gen, device="cuda", dtype=dtype)
+         for k, l in (("u", "u"), ("v", "v"), ("w", "w"), ("pi", "m"), ("eta_dot", "w"))}
+    ops = lambda: [sol.matvec_scaled(x, bg), sol.matvec_scaled(x, bg, transpose=True), pm(x), pm.transpose(x)]
+    core.set_tuning()
+    ref = ops()
+    for knob, n in (("matvec_block", 4), ("matvec_t_block", 4), ("precond_tile", 3), ("precond_t_tile", 3)):
+        for v in range(1, n):
+            core.set_tuning(**{knob: v})
+            out = ops()
+            for a, b in zip(out, ref):
+                for k in a:
+                    assert torch.equal(a[k], b[k]), (knob, v, k)
+    choice = core.autotune()
+    assert 0 <= choice["matvec_block"] < 4 and 0 <= choice["precond_tile"] < 3
+    assert all(t > 0 for t in choice["us"])
+    assert core.tuning()["matvec_block"] == choice["matvec_block"]
+    core.set_tuning()
