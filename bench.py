@@ -206,31 +206,18 @@ def cpu_leg(steps, warmup, window, nz, tol):
 
 # ---------------------------------------------------------------------------
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(local)
-    return world, rank, local
+    from suetes_b200 import replicas
+    return replicas.init(timeout_s=300)
 
 
 def dist_max(x, world):
-    if world == 1:
-        return x
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from suetes_b200 import replicas
+    return replicas.max_over_ranks(x, world)
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from suetes_b200 import replicas
+    replicas.barrier(world)
 
 
 def run_reference(args):
@@ -292,7 +279,8 @@ def ensemble_leg(args, local, world):
     from suetes_b200 import PingPong
     from suetes_b200.core import kernel_launches
     from suetes_b200.workloads import bubble_ensemble
-    ens = bubble_ensemble(args.ens_members, seed=1, device=f"cuda:{local}", solver_tol=args.tol32,
+    rank = int(os.environ.get("RANK", "0"))
+    ens = bubble_ensemble(args.ens_members, seed=1 + rank, device=f"cuda:{local}", solver_tol=args.tol32,
                           solve_method=args.method)
     cells = sum(sp["nx"] * sp["ny"] * sp["nz"] for _, _, _, sp in ens)
     dss = [(st, st.to_device_state(s0), bc) for st, s0, bc, _ in ens]
@@ -543,9 +531,8 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     barrier(world)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from suetes_b200 import replicas
+    replicas.finalize(world)
 
 
 def main():
