@@ -565,7 +565,9 @@ void launch_pt_column(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, 
 template <typename T>
 void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                       cudaStream_t st) {
-  switch (d.tune_pct) {
+  int v = d.tune_pct;
+  if (v == 2 && (size_t)(3 * d.nz + 1) * 64 * sizeof(T) > 200 * 1024) v = 0;  // 64-column tile too large
+  switch (v) {
     case 1: launch_pt_column<T, 128, 16>(d, c, y, out, active, st); break;
     case 2: launch_pt_column<T, 256, 64>(d, c, y, out, active, st); break;
     default: launch_pt_column<T, 256, 32>(d, c, y, out, active, st); break;

@@ -39,8 +39,11 @@ __device__ __forceinline__ T gz_mass(const T* __restrict__ p, const T* __restric
 // Branch-free load phase: every index is clamped into its array, all values
 // are loaded unconditionally (one memory round trip per thread), the five
 // rows are formed with selects, and only the stores are predicated.
+// float: 6 resident blocks of 256 (<= 40 registers, no spills) for more
+// loads in flight; double keeps 4 (more would spill)
 template <typename T>
-__global__ void __launch_bounds__(256) matvec_kernel(Dims d, Coef<T> c, CVec5<T> x, const double* xscale,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) matvec_kernel(Dims d, Coef<T> c, CVec5<T> x,
+                                                                            const double* xscale,
                                                      CVec5<T> b, Vec5<T> out, const int* active) {
   if (active && *active == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -153,17 +156,18 @@ __global__ void __launch_bounds__(256) matvec_kernel(Dims d, Coef<T> c, CVec5<T>
 
 // ---------------------------------------------------------------------------
 // Column-tile preconditioner: a block owns 32 consecutive columns (same j).
-//   A: every thread takes (level k, column): it forms w_tilde at the w levels
-//      k and k+1 (steppers.py:215-219) and with them the Helmholtz RHS at mass
-//      level k (steppers.py:223), L_pi (steppers.py:180) and the acoustic
-//      coupling P = K_w rho_w th_w at w level k (steppers.py:171-177); the
-//      eta_dot/alpha - kin term is parked in the eta_dot output;
+//   A1: every thread takes (w level k, column) pairs and forms w_tilde
+//       (steppers.py:215-219), the acoustic coupling P = K_w rho_w th_w
+//       (steppers.py:171-177) and the eta_dot/alpha - kin term (parked in
+//       the eta_dot output), each once;
+//   A2: the Helmholtz RHS (steppers.py:223) and L_pi (steppers.py:180) at
+//       every mass level from the shared w_tilde;
 //   B: warp 0 factors and solves its 32 tridiagonal systems
 //      (lower = -L_pi P_k, upper = -L_pi P_k+1, main = 1 - lower - upper;
 //      steppers.py:183-185, 227) by the Thomas algorithm in shared memory;
 //   C: every thread writes w, eta_dot and pi (steppers.py:231-251).
 // The banded system is strictly diagonally dominant, so no pivoting.
-// Shared memory per block: (3 nz + 1) * 32 values of T.
+// Shared memory per block: (4 nz + 2) * columns values of T.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
@@ -210,6 +214,7 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
   T* s_x = sm;                 // [nz][PC]    rhs -> d' -> x
   T* s_L = s_x + nz * PC;      // [nz][PC]    L_pi -> c'
   T* s_P = s_L + nz * PC;      // [nz+1][PC]  P at w levels
+  T* s_W = s_P + (nz + 1) * PC;  // [nz+1][PC]  w_tilde at w levels
   const int i0 = blockIdx.x * PC;
   const int j = blockIdx.y;
   const int tid = threadIdx.x;
@@ -245,23 +250,24 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
     }
   }
 
-  // ---- A ----
+  // ---- A1: the w-level quantities once per (level, column) ----
 #pragma unroll 2
   for (int q = tid; q < (nz + 1) * PC; q += PT) {
     const int k = q / PC, l = q % PC, i = min(i0 + l, nx - 1);
-    const int km = min(k, nz - 1);
-    const PrecondW<T> lo = precond_wlevel(d, c, ru, rv, rw, rW, i, j, k, inva, adtcp);
-    const PrecondW<T> hi = precond_wlevel(d, c, ru, rv, rw, rW, i, j, k + 1, inva, adtcp);
-    const int p = i + nx * j + km * pm;
-    const T Lpi = ld(c.lpi, p);
-    const T rhs = ld(rp, p) * ips - Lpi * (hi.wt - lo.wt);
+    const PrecondW<T> w = precond_wlevel(d, c, ru, rv, rw, rW, i, j, k, inva, adtcp);
     const bool col = (i0 + l < nx);
-    s_P[q] = col ? lo.P : T(0);
-    if (k < nz) {
-      s_x[q] = rhs;
-      s_L[q] = Lpi;
-      if (col && k > 0) oW[p] = lo.ep;  // eta_dot / alpha - kin, completed in C
-    }
+    s_P[q] = col ? w.P : T(0);
+    s_W[q] = w.wt;
+    if (col && k > 0 && k < nz) oW[i + nx * j + k * pm] = w.ep;  // eta_dot / alpha - kin, completed in C
+  }
+  __syncthreads();
+  // ---- A2: Helmholtz right-hand side at mass levels (steppers.py:223) ----
+  for (int q = tid; q < nz * PC; q += PT) {
+    const int k = q / PC, l = q % PC, i = min(i0 + l, nx - 1);
+    const int p = i + nx * j + k * pm;
+    const T Lpi = ld(c.lpi, p);
+    s_x[q] = ld(rp, p) * ips - Lpi * (s_W[q + PC] - s_W[q]);
+    s_L[q] = Lpi;
   }
   __syncthreads();
   // ---- B: factor and solve, one lane per column ----
@@ -321,7 +327,7 @@ void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xs
 template <typename T, int PT, int PC>
 void launch_precond_tile(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                          cudaStream_t st) {
-  const size_t smem = (size_t)(3 * d.nz + 1) * PC * sizeof(T);
+  const size_t smem = (size_t)(4 * d.nz + 2) * PC * sizeof(T);
   static size_t attr_bytes = 0;  // per instantiation
   if (smem > 48 * 1024 && smem > attr_bytes) {
     cudaFuncSetAttribute(precond_tile_kernel<T, PT, PC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -334,7 +340,9 @@ void launch_precond_tile(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> ou
 template <typename T>
 void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                     cudaStream_t st) {
-  switch (d.tune_pc) {
+  int v = d.tune_pc;
+  if (v == 2 && (size_t)(4 * d.nz + 2) * 64 * sizeof(T) > 200 * 1024) v = 0;  // 64-column tile too large
+  switch (v) {
     case 1: launch_precond_tile<T, 128, 16>(d, c, r, out, active, st); break;
     case 2: launch_precond_tile<T, 256, 64>(d, c, r, out, active, st); break;
     default: launch_precond_tile<T, 256, 32>(d, c, r, out, active, st); break;
