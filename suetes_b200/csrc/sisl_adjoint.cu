@@ -272,16 +272,19 @@ __global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T
 //   wtbar(K) = divbar(K-1) - divbar(K),  epbar = yW + rho_w thw wtbar
 //   out_W  = epbar / alpha,  out_w = (yw + epbar) / damp  (interior levels)
 //   out_W  = yW dz_w,        out_w = yw                   (ground and lid)
-// A: every thread takes (level, column) pairs and forms pibar, L_pi and P;
-// B: warp 0 runs the transposed Thomas sweep of its 32 columns in shared
-//    memory (sub(k) = -L(k-1) P(k), sup(k) = -L(k+1) P(k+1),
-//    main(k) = 1 + L(k) (P(k) + P(k+1)));
-// C: every thread writes pi, w and eta_dot.
-// Shared memory per block: (3 nz + 1) * 32 values of T.
+// With the factorisation T = L U of prep_thomas, T^T z = pibar is
+// U^T w = pibar (upward) then L^T z = w (downward), the arithmetic of
+// pt_march_kernel term for term (every column variant is bitwise equal).
+// A: every thread takes (level, column) pairs and forms pibar and stages
+//    the factors; B: one thread per column runs both sweeps in shared
+//    memory; C: every thread writes pi, w and eta_dot.
+// Shared memory per block: 4 nz * columns values of T.
 // ---------------------------------------------------------------------------
 
-template <typename T>
-__device__ __forceinline__ T pt_rcp(T x) { return T(1) / x; }
+// rounded products that the compiler may not fuse into a following add, so
+// that the column variants of M^T round identically
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 
 template <typename T, int TPT, int TPC>
 __global__ void __launch_bounds__(TPT) pt_column_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
@@ -290,70 +293,58 @@ __global__ void __launch_bounds__(TPT) pt_column_kernel(Dims d, Coef<T> c, CVec5
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  T* s_x = sm;                // [nz][TPC]    pibar -> d' -> z
-  T* s_L = s_x + nz * TPC;    // [nz][TPC]    L_pi
-  T* s_P = s_L + nz * TPC;    // [nz+1][TPC]  P at w levels, then c'
+  T* s_x = sm;                // [nz][TPC]  pibar -> w -> z
+  T* s_cp = s_x + nz * TPC;   // [nz][TPC]  c'
+  T* s_lo = s_cp + nz * TPC;  // [nz][TPC]  lower
+  T* s_iv = s_lo + nz * TPC;  // [nz][TPC]  1 / pivot
   const int i0 = blockIdx.x * TPC;
   const int j = blockIdx.y;
   const int tid = threadIdx.x;
   const int pm = nx * ny;
-  const T ps = (T)c.s.ps, ips = (T)(1.0 / c.s.ps), a = (T)c.s.alpha;
-  const T adtcp = (T)(c.s.alpha * c.s.dt * c.s.cp);
+  const T ps = (T)c.s.ps, ips = (T)(1.0 / c.s.ps), inva = T(1) / (T)c.s.alpha;
   const T* __restrict__ yw = y.f[2];
   const T* __restrict__ yp = y.f[3];
   const T* __restrict__ yW = y.f[4];
   T* __restrict__ ow = out.f[2];
   T* __restrict__ op = out.f[3];
   T* __restrict__ oW = out.f[4];
-  // ---- A: pibar, L_pi, P (loads at a clamped interior level, masked) ----
-  for (int q = tid; q < (nz + 1) * TPC; q += TPT) {
+  // G(K) = -adt cp thw (yw + yW) idzw / damp at interior w levels
+  auto Gw = [&](int i, int K) -> T {
+    const int kc = min(max(K, 1), nz - 1);
+    const int pw = i + nx * j + kc * pm;
+    const T g = -ld(c.pbw, pw) * (ld(yw, pw) + ld(yW, pw));
+    return (K > 0 && K < nz) ? g : T(0);
+  };
+  // ---- A: pibar and the factorisation ----
+  for (int q = tid; q < nz * TPC; q += TPT) {
     const int k = q / TPC, l = q % TPC, i = min(i0 + l, nx - 1);
-    const int h = i + nx * j;
-    auto GP = [&](int K, T& G, T& P) {
-      const int kc = min(max(K, 1), nz - 1);
-      const T on = (K > 0 && K < nz) ? T(1) : T(0);
-      const int p = h + kc * pm;
-      const T thw = ld(c.thw, p), idzw = ld(c.idzw, p), idamp = T(1) / ld(c.damp, p);
-      G = -on * adtcp * thw * (ld(yw, p) + ld(yW, p)) * idzw * idamp;
-      P = on * adtcp * thw * idzw * idamp * ld(c.rhow, p) * thw;
-    };
-    T G0, P0, G1, P1;
-    GP(k, G0, P0);
-    s_P[q] = P0;
-    if (k < nz) {
-      GP(k + 1, G1, P1);
-      const int p = h + k * pm;
-      s_x[q] = ld(yp, p) * ps + G0 - G1;
-      s_L[q] = ld(c.lpi, p);
-    }
+    const int p = i + nx * j + k * pm;
+    s_x[q] = ld(yp, p) * ps + Gw(i, k) - Gw(i, k + 1);
+    s_cp[q] = ld(c.tcp, p);
+    s_lo[q] = ld(c.tlo, p);
+    s_iv[q] = ld(c.tinv, p);
   }
   __syncthreads();
-  // ---- B: transposed Thomas, one lane per column ----
+  // ---- B: U^T w = pibar upward, L^T z = w downward, one thread per column ----
   if (tid < TPC) {
     const int l = tid;
-    T cprev = T(0), dprev = T(0), Lprev = T(0), Pk = s_P[l];
+    T wprev = T(0), cprev = T(0);
     for (int k = 0; k < nz; ++k) {
       const int q = k * TPC + l;
-      const T L = s_L[q], Pk1 = s_P[q + TPC];
-      const T Lnext = (k + 1 < nz) ? s_L[q + TPC] : T(0);
-      const T sub = -Lprev * Pk, sup = -Lnext * Pk1;
-      const T inv = pt_rcp((T(1) + L * (Pk + Pk1)) - sub * cprev);
-      cprev = sup * inv;
-      dprev = (s_x[q] - sub * dprev) * inv;
-      s_P[q] = cprev;  // P(k) is no longer needed
-      s_x[q] = dprev;
-      Lprev = L;
-      Pk = Pk1;
+      wprev = s_x[q] - cprev * wprev;
+      s_x[q] = wprev;
+      cprev = s_cp[q];
     }
-    T zh = dprev;
-    for (int k = nz - 2; k >= 0; --k) {
+    T zh = T(0), loh = T(0);
+    for (int k = nz - 1; k >= 0; --k) {
       const int q = k * TPC + l;
-      zh = s_x[q] - s_P[q] * zh;
+      zh = (s_x[q] - loh * zh) * s_iv[q];
       s_x[q] = zh;
+      loh = s_lo[q];
     }
   }
   __syncthreads();
-  // ---- C: pi, w, eta_dot ----
+  // ---- C: pi, w and eta_dot cotangents ----
   for (int q = tid; q < (nz + 1) * TPC; q += TPT) {
     const int k = q / TPC, l = q % TPC, i = i0 + l;
     if (i >= nx) continue;
@@ -363,10 +354,10 @@ __global__ void __launch_bounds__(TPT) pt_column_kernel(Dims d, Coef<T> c, CVec5
       ow[p] = ld(yw, p);
       oW[p] = ld(yW, p) * ld(c.dzw, p);
     } else {
-      const T dvl = -s_L[q - TPC] * s_x[q - TPC], dv = -s_L[q] * s_x[q];
-      const T ep = ld(yW, p) + ld(c.rhow, p) * ld(c.thw, p) * (dvl - dv);
-      oW[p] = ep / a;
-      ow[p] = (ld(yw, p) + ep) / ld(c.damp, p);
+      const T dvl = mul_rn(-ld(c.lpi, p - pm), s_x[q - TPC]), dv = mul_rn(-ld(c.lpi, p), s_x[q]);
+      const T ep = ld(yW, p) + ld(c.rtw, p) * (dvl - dv);
+      oW[p] = ep * inva;
+      ow[p] = (ld(yw, p) + ep) * ld(c.idamp, p);
     }
   }
 }
@@ -550,10 +541,86 @@ template void launch_tricubic_vjp<double>(int, int, int, int, int, int, const do
                                           const double*, double*, int, double, cudaStream_t);
 
 // out = M^T y (out must not alias y).
+// M^T as a column march (one thread per column, NT columns per block) with
+// the factorisation T = L U of prep_thomas: T^T z = pibar is U^T w = pibar
+// upward (w(k) = pibar(k) - c'(k-1) w(k-1), w kept in shared memory), then
+// L^T z = w downward (z(k) = (w(k) - lower(k+1) z(k+1)) / pivot(k)), where
+// the w and eta_dot cotangents of the w level between z(k) and z(k+1) are
+// formed.  Shared memory per block: nz * NT values of T.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) pt_march_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
+                                                      const int* active) {
+  if (active && *active == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_w = reinterpret_cast<T*>(smem_raw);  // [nz][NT]
+  const int t = threadIdx.x;
+  const int i = blockIdx.x * NT + t, j = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i >= nx) return;
+  const int pm = nx * ny, h = i + nx * j;
+  const T ps = (T)c.s.ps, ips = (T)(1.0 / c.s.ps), inva = T(1) / (T)c.s.alpha;
+  const T* __restrict__ yw = y.f[2];
+  const T* __restrict__ yp = y.f[3];
+  const T* __restrict__ yW = y.f[4];
+  T* __restrict__ ow = out.f[2];
+  T* __restrict__ op = out.f[3];
+  T* __restrict__ oW = out.f[4];
+  T G_lo = T(0), wprev = T(0), cprev = T(0);
+#pragma unroll 4
+  for (int k = 0; k < nz; ++k) {
+    const int p = h + k * pm;
+    T G_hi = T(0);
+    if (k + 1 < nz) {
+      const int pw = p + pm;
+      G_hi = -ld(c.pbw, pw) * (ld(yw, pw) + ld(yW, pw));
+    }
+    const T pib = ld(yp, p) * ps + G_lo - G_hi;
+    const T wv = pib - cprev * wprev;
+    s_w[k * NT + t] = wv;
+    wprev = wv;
+    cprev = ld(c.tcp, p);
+    G_lo = G_hi;
+  }
+  T zh = T(0), loh = T(0), dvh = T(0);
+#pragma unroll 4
+  for (int k = nz - 1; k >= 0; --k) {
+    const int p = h + k * pm;
+    const T z = (s_w[k * NT + t] - loh * zh) * ld(c.tinv, p);
+    op[p] = z * ips;
+    const T dv = mul_rn(-ld(c.lpi, p), z);
+    if (k + 1 < nz) {
+      const int pw = p + pm;
+      const T ep = ld(yW, pw) + ld(c.rtw, pw) * (dv - dvh);
+      oW[pw] = ep * inva;
+      ow[pw] = (ld(yw, pw) + ep) * ld(c.idamp, pw);
+    }
+    zh = z;
+    loh = ld(c.tlo, p);
+    dvh = dv;
+  }
+  ow[h] = ld(yw, h);
+  oW[h] = ld(yW, h) * ld(c.dzw, h);
+  const int ptop = h + nz * pm;
+  ow[ptop] = ld(yw, ptop);
+  oW[ptop] = ld(yW, ptop) * ld(c.dzw, ptop);
+}
+
+template <typename T, int NT>
+void launch_pt_march(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
+                     cudaStream_t st) {
+  const size_t smem = (size_t)d.nz * NT * sizeof(T);
+  static size_t attr_bytes = 0;  // per instantiation
+  if (smem > 48 * 1024 && smem > attr_bytes) {
+    cudaFuncSetAttribute(pt_march_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_bytes = smem;
+  }
+  pt_march_kernel<T, NT><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, y, out, active);
+}
+
 template <typename T, int TPT, int TPC>
 void launch_pt_column(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                       cudaStream_t st) {
-  const size_t smem = (size_t)(3 * d.nz + 1) * TPC * sizeof(T);
+  const size_t smem = (size_t)(4 * d.nz) * TPC * sizeof(T);
   static size_t attr_bytes = 0;  // per instantiation
   if (smem > 48 * 1024 && smem > attr_bytes) {
     cudaFuncSetAttribute(pt_column_kernel<T, TPT, TPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -566,10 +633,11 @@ template <typename T>
 void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                       cudaStream_t st) {
   int v = d.tune_pct;
-  if (v == 2 && (size_t)(3 * d.nz + 1) * 64 * sizeof(T) > 200 * 1024) v = 0;  // 64-column tile too large
+  if (v == 2 && (size_t)(4 * d.nz) * 64 * sizeof(T) > 200 * 1024) v = 0;  // 64-column tile too large
   switch (v) {
     case 1: launch_pt_column<T, 128, 16>(d, c, y, out, active, st); break;
     case 2: launch_pt_column<T, 256, 64>(d, c, y, out, active, st); break;
+    case 3: launch_pt_march<T, 128>(d, c, y, out, active, st); break;
     default: launch_pt_column<T, 256, 32>(d, c, y, out, active, st); break;
   }
   const dim3 blk = stencil_block(d.tune_mvt);

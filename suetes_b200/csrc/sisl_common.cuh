@@ -35,7 +35,9 @@ __host__ inline dim3 stencil_block(int variant) {
   }
 }
 constexpr int N_STENCIL_BLOCKS = 4;
-constexpr int N_COLUMN_TILES = 3;  // (threads, columns) = (256, 32), (128, 16), (256, 64)
+// column variants: tiles of (threads, columns) = (256, 32), (128, 16), (256, 64),
+// and the one-thread-per-column march (128 columns per block)
+constexpr int N_COLUMN_TILES = 4;
 
 __host__ __device__ inline int ext_x(const Dims& d, int loc) { return d.nx + (loc == LOC_U); }
 __host__ __device__ inline int ext_y(const Dims& d, int loc) { return d.ny + (loc == LOC_V); }

@@ -40,6 +40,12 @@ struct Coef {
   const T *thw, *rhow, *idzw, *dzw, *damp, *zxw, *zew;  // damp = 1 + dt tau
   // horizontal 2-D
   const T *mm, *mu, *mv, *fu, *fv, *dmdx, *dmdy;
+  // column Helmholtz system of the preconditioner, factorised once
+  // (steppers.py:171-185): lower(k) = -L_pi(k) P(k), and the Thomas factors
+  // c'(k) and 1/pivot(k) of T = L U (mass levels); rho_w th_w, the w
+  // back-substitution factor adt cp th_w / (dz_w (1 + dt tau)) and
+  // 1/(1 + dt tau) (w levels)
+  const T *tlo, *tcp, *tinv, *rtw, *pbw, *idamp;
   Scalars s;
 };
 
@@ -48,6 +54,7 @@ enum CoefId {
   C_THU, C_ZXU, C_RDU, C_THV, C_ZEV, C_RDV,
   C_THW, C_RHOW, C_IDZW, C_DZW, C_DAMP, C_ZXW, C_ZEW,
   C_MM, C_MU, C_MV, C_FU, C_FV, C_DMDX, C_DMDY,
+  C_TLO, C_TCP, C_TINV, C_RTW, C_PBW, C_IDAMP,
   C_COUNT
 };
 int coef_loc(int id);      // LOC_* of a 3-D coefficient, or -1 for 2-D

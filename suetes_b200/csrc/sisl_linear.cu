@@ -162,45 +162,42 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) matvec_kernel(Dim
 //       the eta_dot output), each once;
 //   A2: the Helmholtz RHS (steppers.py:223) and L_pi (steppers.py:180) at
 //       every mass level from the shared w_tilde;
-//   B: warp 0 factors and solves its 32 tridiagonal systems
+//   B: one thread per column solves its tridiagonal system
 //      (lower = -L_pi P_k, upper = -L_pi P_k+1, main = 1 - lower - upper;
-//      steppers.py:183-185, 227) by the Thomas algorithm in shared memory;
+//      steppers.py:183-185, 227) with the Thomas factorisation prepared once
+//      per core (prep_thomas), in shared memory;
 //   C: every thread writes w, eta_dot and pi (steppers.py:231-251).
 // The banded system is strictly diagonally dominant, so no pivoting.
-// Shared memory per block: (4 nz + 2) * columns values of T.
+// Shared memory per block: (5 nz + 1) * columns values of T.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
-__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
-
 
 template <typename T>
 struct PrecondW {  // w-level quantities of one column at one level
-  T wt, ep, P;
+  T wt, ep;
 };
 
+// w_tilde and the eta_dot/alpha - kin term at w level k (zero on the ground
+// and the lid: the loads use a clamped interior level and the results are
+// masked).  The arithmetic is term for term the one of precond_march_kernel,
+// so every column variant gives bitwise the same result.
 template <typename T>
 __device__ __forceinline__ PrecondW<T> precond_wlevel(const Dims& d, const Coef<T>& c, const T* __restrict__ ru,
                                                      const T* __restrict__ rv, const T* __restrict__ rw,
-                                                     const T* __restrict__ rW, int i, int j, int k, T inva,
-                                                     T adtcp) {
-  // w_tilde and P vanish on the ground and the lid: the loads use a clamped
-  // interior level and the results are masked (no branch around the loads)
+                                                     const T* __restrict__ rW, int i, int j, int k, T inva) {
   const int nx = d.nx, ny = d.ny;
   const int kc = min(max(k, 1), d.nz - 1);
   const T on = (k > 0 && k < d.nz) ? T(1) : T(0);
   const int p = i + nx * j + kc * nx * ny;
   const int u1 = iu(d, i, j, kc), u0 = u1 - (nx + 1) * ny;
   const int v1 = iv(d, i, j, kc), v0 = v1 - nx * (ny + 1);
-  const T uw = T(0.25) * (ld(ru, u0) + ld(ru, u0 + 1) + ld(ru, u1) + ld(ru, u1 + 1));
-  const T vw = T(0.25) * (ld(rv, v0) + ld(rv, v0 + nx) + ld(rv, v1) + ld(rv, v1 + nx));
-  const T kin = ld(c.mm, i + nx * j) * (uw * ld(c.zxw, p) + vw * ld(c.zew, p));
-  const T thw = ld(c.thw, p);
-  const T rt = ld(c.rhow, p) * thw;
-  const T damp = ld(c.damp, p);
+  const T su_lo = ld(ru, u0) + ld(ru, u0 + 1), su_hi = ld(ru, u1) + ld(ru, u1 + 1);
+  const T sv_lo = ld(rv, v0) + ld(rv, v0 + nx), sv_hi = ld(rv, v1) + ld(rv, v1 + nx);
+  const T mq = T(0.25) * ld(c.mm, i + nx * j);
+  const T kin = mq * ((su_lo + su_hi) * ld(c.zxw, p) + (sv_lo + sv_hi) * ld(c.zew, p));
+  const T ep = ld(rW, p) * inva - kin;
   PrecondW<T> o;
-  o.ep = on * (ld(rW, p) * inva - kin);
-  o.wt = on * rt * (ld(rw, p) / damp + o.ep);
-  o.P = on * adtcp * thw * ld(c.idzw, p) / damp * rt;  // K_w rho_w th_w
+  o.ep = on * ep;
+  o.wt = on * (ld(c.rtw, p) * (ld(rw, p) * ld(c.idamp, p) + ep));
   return o;
 }
 
@@ -211,10 +208,11 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  T* s_x = sm;                 // [nz][PC]    rhs -> d' -> x
-  T* s_L = s_x + nz * PC;      // [nz][PC]    L_pi -> c'
-  T* s_P = s_L + nz * PC;      // [nz+1][PC]  P at w levels
-  T* s_W = s_P + (nz + 1) * PC;  // [nz+1][PC]  w_tilde at w levels
+  T* s_x = sm;                    // [nz][PC]    rhs -> d' -> x
+  T* s_W = s_x + nz * PC;         // [nz+1][PC]  w_tilde at w levels
+  T* s_lo = s_W + (nz + 1) * PC;  // [nz][PC]    lower
+  T* s_iv = s_lo + nz * PC;       // [nz][PC]    1 / pivot
+  T* s_cp = s_iv + nz * PC;       // [nz][PC]    c'
   const int i0 = blockIdx.x * PC;
   const int j = blockIdx.y;
   const int tid = threadIdx.x;
@@ -229,7 +227,6 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
   const T inva = T(1) / (T)c.s.alpha;
   const T ips = (T)(1.0 / c.s.ps);
   const T ps = (T)c.s.ps;
-  const T adtcp = (T)(c.s.alpha * c.s.dt * c.s.cp);
   const int pm = nx * ny;
 
   // u and v pass straight through (steppers.py:247-249) unless aliased
@@ -254,43 +251,34 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
 #pragma unroll 2
   for (int q = tid; q < (nz + 1) * PC; q += PT) {
     const int k = q / PC, l = q % PC, i = min(i0 + l, nx - 1);
-    const PrecondW<T> w = precond_wlevel(d, c, ru, rv, rw, rW, i, j, k, inva, adtcp);
-    const bool col = (i0 + l < nx);
-    s_P[q] = col ? w.P : T(0);
+    const PrecondW<T> w = precond_wlevel(d, c, ru, rv, rw, rW, i, j, k, inva);
     s_W[q] = w.wt;
-    if (col && k > 0 && k < nz) oW[i + nx * j + k * pm] = w.ep;  // eta_dot / alpha - kin, completed in C
+    if (i0 + l < nx && k > 0 && k < nz) oW[i + nx * j + k * pm] = w.ep;  // eta_dot / alpha - kin, completed in C
   }
   __syncthreads();
-  // ---- A2: Helmholtz right-hand side at mass levels (steppers.py:223) ----
+  // ---- A2: Helmholtz right-hand side (steppers.py:223) and the factorisation ----
   for (int q = tid; q < nz * PC; q += PT) {
     const int k = q / PC, l = q % PC, i = min(i0 + l, nx - 1);
     const int p = i + nx * j + k * pm;
-    const T Lpi = ld(c.lpi, p);
-    s_x[q] = ld(rp, p) * ips - Lpi * (s_W[q + PC] - s_W[q]);
-    s_L[q] = Lpi;
+    s_x[q] = ld(rp, p) * ips - ld(c.lpi, p) * (s_W[q + PC] - s_W[q]);
+    s_lo[q] = ld(c.tlo, p);
+    s_iv[q] = ld(c.tinv, p);
+    s_cp[q] = ld(c.tcp, p);
   }
   __syncthreads();
-  // ---- B: factor and solve, one lane per column ----
+  // ---- B: Thomas with the prepared factorisation, one thread per column ----
   if (tid < PC) {
     const int l = tid;
-    T cprev = T(0), dprev = T(0), Plo = s_P[l];
-#pragma unroll 4
+    T dprev = T(0);
     for (int k = 0; k < nz; ++k) {
       const int q = k * PC + l;
-      const T L = s_L[q], Phi = s_P[q + PC];
-      const T lower = -L * Plo, upper = -L * Phi;
-      const T inv = rcp_rn((T(1) - lower - upper) - lower * cprev);
-      cprev = upper * inv;
-      dprev = (s_x[q] - lower * dprev) * inv;
-      s_L[q] = cprev;
+      dprev = (s_x[q] - s_lo[q] * dprev) * s_iv[q];
       s_x[q] = dprev;
-      Plo = Phi;
     }
     T xh = dprev;
-#pragma unroll 8
     for (int k = nz - 2; k >= 0; --k) {
       const int q = k * PC + l;
-      xh = s_x[q] - s_L[q] * xh;
+      xh = s_x[q] - s_cp[q] * xh;
       s_x[q] = xh;
     }
   }
@@ -305,8 +293,7 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
       ow[p] = ld(rw, p);
       oW[p] = ld(rW, p) * ld(c.dzw, p);
     } else {
-      const T grad = (s_x[q] - s_x[q - PC]) * ld(c.idzw, p);
-      const T wv = (ld(rw, p) - adtcp * ld(c.thw, p) * grad) / ld(c.damp, p);
+      const T wv = ld(rw, p) * ld(c.idamp, p) - ld(c.pbw, p) * (s_x[q] - s_x[q - PC]);
       ow[p] = wv;
       oW[p] = oW[p] + wv;
     }
@@ -324,10 +311,105 @@ void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xs
   matvec_kernel<T><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
 }
 
+// ---------------------------------------------------------------------------
+// Column march: one thread per (i, j) column, NT consecutive columns per
+// block so every level's loads are coalesced across the warp.  Upward over
+// the mass levels it forms w_tilde and the eta_dot/alpha - kin term at the
+// w level above (parked in the eta_dot output), the Helmholtz RHS and the
+// forward elimination d'(k) = (rhs - lower d'(k-1)) / pivot with the
+// factorisation prepared once per core (prep_thomas); d' stays in shared
+// memory.  Downward it back-substitutes x(k) = d'(k) - c'(k) x(k+1) and
+// writes pi, w and eta_dot at the w level between x(k) and x(k+1).
+// Shared memory per block: nz * NT values of T.
+// ---------------------------------------------------------------------------
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) precond_march_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
+                                                           const int* active) {
+  if (active && *active == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_d = reinterpret_cast<T*>(smem_raw);  // [nz][NT]
+  const int t = threadIdx.x;
+  const int i = blockIdx.x * NT + t, j = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i >= nx) return;
+  const int pm = nx * ny, h = i + nx * j;
+  const int pu = (nx + 1) * ny, pv = nx * (ny + 1);
+  const T inva = T(1) / (T)c.s.alpha, ips = (T)(1.0 / c.s.ps), ps = (T)c.s.ps;
+  const T* __restrict__ ru = r.f[0];
+  const T* __restrict__ rv = r.f[1];
+  const T* __restrict__ rw = r.f[2];
+  const T* __restrict__ rp = r.f[3];
+  const T* __restrict__ rW = r.f[4];
+  T* __restrict__ ow = out.f[2];
+  T* __restrict__ op = out.f[3];
+  T* __restrict__ oW = out.f[4];
+  const T mq = T(0.25) * ld(c.mm, h);
+  const int ub = iu(d, i, j, 0), vb = iv(d, i, j, 0);
+  // u over faces i, i+1 and v over faces j, j+1 at mass level k
+  auto su = [&](int k) { const int q = ub + k * pu; return ld(ru, q) + ld(ru, q + 1); };
+  auto sv = [&](int k) { const int q = vb + k * pv; return ld(rv, q) + ld(rv, q + nx); };
+  T su_lo = su(0), sv_lo = sv(0);
+  T wt_lo = T(0), dprev = T(0);
+#pragma unroll 4
+  for (int k = 0; k < nz; ++k) {
+    const int p = h + k * pm;
+    T wt_hi = T(0);
+    if (k + 1 < nz) {  // interior w level k + 1 (steppers.py:211-219)
+      const int pw = p + pm;
+      const T su_hi = su(k + 1), sv_hi = sv(k + 1);
+      const T kin = mq * ((su_lo + su_hi) * ld(c.zxw, pw) + (sv_lo + sv_hi) * ld(c.zew, pw));
+      const T ep = ld(rW, pw) * inva - kin;
+      wt_hi = ld(c.rtw, pw) * (ld(rw, pw) * ld(c.idamp, pw) + ep);
+      oW[pw] = ep;
+      su_lo = su_hi;
+      sv_lo = sv_hi;
+    }
+    const T rhs = ld(rp, p) * ips - ld(c.lpi, p) * (wt_hi - wt_lo);  // steppers.py:223
+    dprev = (rhs - ld(c.tlo, p) * dprev) * ld(c.tinv, p);
+    s_d[k * NT + t] = dprev;
+    wt_lo = wt_hi;
+  }
+  T xh = dprev;
+  op[h + (nz - 1) * pm] = xh * ps;
+#pragma unroll 4
+  for (int k = nz - 2; k >= 0; --k) {  // steppers.py:227-245
+    const int p = h + k * pm;
+    const T x = s_d[k * NT + t] - ld(c.tcp, p) * xh;
+    op[p] = x * ps;
+    const int pw = p + pm;
+    const T wv = ld(rw, pw) * ld(c.idamp, pw) - ld(c.pbw, pw) * (xh - x);
+    ow[pw] = wv;
+    oW[pw] = oW[pw] + wv;
+    xh = x;
+  }
+  ow[h] = ld(rw, h);  // ground and lid rows (steppers.py:237-238, 244-245)
+  oW[h] = ld(rW, h) * ld(c.dzw, h);
+  const int ptop = h + nz * pm;
+  ow[ptop] = ld(rw, ptop);
+  oW[ptop] = ld(rW, ptop) * ld(c.dzw, ptop);
+}
+
+template <typename T, int NT>
+void launch_precond_march(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
+                          cudaStream_t st) {
+  const size_t smem = (size_t)d.nz * NT * sizeof(T);
+  static size_t attr_bytes = 0;  // per instantiation
+  if (smem > 48 * 1024 && smem > attr_bytes) {
+    cudaFuncSetAttribute(precond_march_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_bytes = smem;
+  }
+  // u and v pass straight through (steppers.py:247-249) unless aliased
+  if (out.f[0] != r.f[0])
+    cudaMemcpyAsync(out.f[0], r.f[0], sizeof(T) * field_size(d, LOC_U), cudaMemcpyDeviceToDevice, st);
+  if (out.f[1] != r.f[1])
+    cudaMemcpyAsync(out.f[1], r.f[1], sizeof(T) * field_size(d, LOC_V), cudaMemcpyDeviceToDevice, st);
+  precond_march_kernel<T, NT><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, r, out, active);
+}
+
 template <typename T, int PT, int PC>
 void launch_precond_tile(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                          cudaStream_t st) {
-  const size_t smem = (size_t)(4 * d.nz + 2) * PC * sizeof(T);
+  const size_t smem = (size_t)(5 * d.nz + 1) * PC * sizeof(T);
   static size_t attr_bytes = 0;  // per instantiation
   if (smem > 48 * 1024 && smem > attr_bytes) {
     cudaFuncSetAttribute(precond_tile_kernel<T, PT, PC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -341,10 +423,11 @@ template <typename T>
 void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                     cudaStream_t st) {
   int v = d.tune_pc;
-  if (v == 2 && (size_t)(4 * d.nz + 2) * 64 * sizeof(T) > 200 * 1024) v = 0;  // 64-column tile too large
+  if (v == 2 && (size_t)(5 * d.nz + 1) * 64 * sizeof(T) > 200 * 1024) v = 0;  // 64-column tile too large
   switch (v) {
     case 1: launch_precond_tile<T, 128, 16>(d, c, r, out, active, st); break;
     case 2: launch_precond_tile<T, 256, 64>(d, c, r, out, active, st); break;
+    case 3: launch_precond_march<T, 128>(d, c, r, out, active, st); break;
     default: launch_precond_tile<T, 256, 32>(d, c, r, out, active, st); break;
   }
 }

@@ -3,8 +3,8 @@
 // the working precision.  Follows euler.py:127-160 (precompute_bg),
 // euler.py:254-255 / 320-322 (z_xi_u, z_eta_v, d theta_bg / dz),
 // diffusion.py:117,125 (z_xi_m, z_eta_m) and steppers.py:153-185
-// (precompute_banded: L_pi; the banded factorisation itself is formed on the
-// fly by the preconditioner from the face coefficients).
+// (precompute_banded: L_pi and the Thomas factorisation of the column
+// Helmholtz system, once per core).
 #include "sisl_core.cuh"
 
 #include <math.h>
@@ -14,10 +14,12 @@ namespace sisl {
 int coef_loc(int id) {
   switch (id) {
     case C_THB: case C_PIB: case C_CPIDZ: case C_DTHM: case C_LPI: case C_ZXM: case C_ZEM: case C_DZM:
+    case C_TLO: case C_TCP: case C_TINV:
       return LOC_M;
     case C_THU: case C_ZXU: case C_RDU: return LOC_U;
     case C_THV: case C_ZEV: case C_RDV: return LOC_V;
     case C_THW: case C_RHOW: case C_IDZW: case C_DZW: case C_DAMP: case C_ZXW: case C_ZEW:
+    case C_RTW: case C_PBW: case C_IDAMP:
       return LOC_W;
     default: return -1;
   }
@@ -44,6 +46,8 @@ Coef<T> make_coef(T* const* a, const Scalars& s) {
   c.zxw = a[C_ZXW]; c.zew = a[C_ZEW];
   c.mm = a[C_MM]; c.mu = a[C_MU]; c.mv = a[C_MV]; c.fu = a[C_FU]; c.fv = a[C_FV];
   c.dmdx = a[C_DMDX]; c.dmdy = a[C_DMDY];
+  c.tlo = a[C_TLO]; c.tcp = a[C_TCP]; c.tinv = a[C_TINV];
+  c.rtw = a[C_RTW]; c.pbw = a[C_PBW]; c.idamp = a[C_IDAMP];
   c.s = s;
   return c;
 }
@@ -138,6 +142,9 @@ __global__ void prep_points(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
     out.p[C_IDZW][p] = (T)(1.0 / dzw);
     out.p[C_DZW][p] = (T)dzw;
     out.p[C_DAMP][p] = (T)(1.0 + s.dt * b.tau[p]);
+    out.p[C_IDAMP][p] = (T)(1.0 / (1.0 + s.dt * b.tau[p]));
+    out.p[C_RTW][p] = (T)(rho * th);
+    out.p[C_PBW][p] = (T)(s.alpha * s.dt * s.cp * th / dzw / (1.0 + s.dt * b.tau[p]));
     out.p[C_ZXW][p] = (T)b.z_xi_w[p];
     out.p[C_ZEW][p] = (T)b.z_eta_w[p];
   }
@@ -162,6 +169,43 @@ __global__ void prep_points(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
   }
 }
 
+// Column Helmholtz system of VerticalPreconditioner.precompute_banded
+// (steppers.py:153-185), one thread per column in float64:
+//   P(K) = adt cp th_w / (dz_w (1 + dt tau)) rho_w th_w (0 on ground and lid)
+//   L(k) = adt C_pi / dz_m,  lower = -L(k) P(k),  upper = -L(k) P(k+1),
+//   main = 1 - lower - upper;  Thomas: pivot(k) = main(k) - lower(k) c'(k-1),
+//   c'(k) = upper(k) / pivot(k).
+template <typename T>
+__global__ void prep_thomas(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i >= nx || j >= ny) return;
+  auto Pw = [&](int K) -> double {
+    if (K <= 0 || K >= nz) return 0.0;
+    const int pl = im(d, i, j, K - 1), pr = im(d, i, j, K);
+    const double th = 0.5 * (b.theta_bg[pl] + b.theta_bg[pr]);
+    const double rho = 0.5 * (rho_of(s, b.theta_bg[pl], b.pi_bg[pl]) + rho_of(s, b.theta_bg[pr], b.pi_bg[pr]));
+    const int pw = iw(d, i, j, K);
+    return s.alpha * s.dt * s.cp * th / (b.dz_w[pw] * (1.0 + s.dt * b.tau[pw])) * rho * th;
+  };
+  double cprev = 0.0, Pk = Pw(0);
+  for (int k = 0; k < nz; ++k) {
+    const int p = im(d, i, j, k);
+    const double th = b.theta_bg[p], pi = b.pi_bg[p];
+    const double cpi = (s.Rd / s.cvd) * (pi / (rho_of(s, th, pi) * th));
+    const double L = s.alpha * s.dt * cpi / b.dz_m[p];
+    const double Pk1 = Pw(k + 1);
+    const double lower = -L * Pk, upper = -L * Pk1;
+    const double piv = (1.0 - lower - upper) - lower * cprev;
+    cprev = upper / piv;
+    out.p[C_TLO][p] = (T)lower;
+    out.p[C_TCP][p] = (T)cprev;
+    out.p[C_TINV][p] = (T)(1.0 / piv);
+    Pk = Pk1;
+  }
+}
+
 }  // namespace
 
 template <typename T>
@@ -169,6 +213,7 @@ void launch_prepare(const Dims& d, const Scalars& s, const Base64& b, PtrTable<T
   dim3 blk(32, 4, 2);
   dim3 grd((d.nx + 1 + blk.x - 1) / blk.x, (d.ny + 1 + blk.y - 1) / blk.y, (d.nz + 1 + blk.z - 1) / blk.z);
   prep_points<T><<<grd, blk, 0, st>>>(d, s, b, out);
+  prep_thomas<T><<<dim3((d.nx + 127) / 128, d.ny), 128, 0, st>>>(d, s, b, out);
 }
 
 template Coef<float> make_coef<float>(float* const*, const Scalars&);
