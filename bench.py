@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--classes", action="store_true",
                     help="also time every GMRES kernel class separately (diagnostic)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--roofline-only", action="store_true",
+                    help="run only the roofline leg (batched GMRES, one kernel class timed): the profiling command")
     ap.add_argument("--ens-members", type=int, default=32,
                     help="members of the uneven-size bubble ensemble leg (0 disables it)")
     ap.add_argument("--ens-steps", type=int, default=10, help="timed graph steps of the ensemble leg")
@@ -272,6 +274,39 @@ def timed_device_steps(stepper, ds0, relax, steps, warmup, world, timing_class=N
     return ms, infos, launches, kt, cur
 
 
+# DRAM traffic per launch of the roofline kernel class from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum averaged over one restart
+# cycle of batched GMRES on this workload, float32), in bytes; the capture
+# and its command are summarised under profiles/.
+NCU_TRAFFIC = {("update", 256, 256, 80): 1.8199e9}
+
+
+def roofline_leg(args, local, world, cls, peak, peak_kind):
+    """The roofline of one GMRES kernel class, timed with CUDA events on its
+    launching stream inside two steps of the same workload with batched GMRES
+    (every launch of a cycle does its full work, so the algorithmic bytes the
+    library adds up are the bytes moved; incremental GMRES skips the rest of
+    a cycle once converged, which those counts cannot see)."""
+    from suetes_b200.workloads import mountain_wave
+    st, s0, bc = mountain_wave(args.nx, args.ny, args.nz, dtype=torch.float32, device=f"cuda:{local}",
+                               solver_tol=args.tol32, solve_method="batched", refine=not args.no_refine)
+    ds = st.to_device_state(s0)
+    if not args.no_autotune:
+        ds.core.autotune()
+    ms, _, _, kt, _ = timed_device_steps(st, ds, bc, 2, 1, world, cls)
+    k_ms, k_n, k_bytes = kt
+    k_ms = dist_max(k_ms, world)
+    achieved = (k_bytes / k_n) / (k_ms / k_n / 1e3) / 1e9 if k_n else None
+    traffic = NCU_TRAFFIC.get((args.roofline_class, args.nx, args.ny, args.nz))
+    out = {"kernel": f"gmres_{args.roofline_class}", "bound": "hbm", "achieved": achieved, "peak": peak,
+           "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+           "peak_kind": peak_kind, "launches_timed": k_n, "avg_launch_us": k_ms / max(k_n, 1) * 1e3,
+           "alg_bytes_per_launch": k_bytes / max(k_n, 1), "share_of_step": k_ms / ms,
+           "timed_in": "2 steps of the same workload with batched GMRES (CUDA events on the launching stream)"}
+    del st, ds
+    return out
+
+
 def ensemble_leg(args, local, world):
     """The uneven-size bubble ensemble advanced as one CUDA graph per step
     (members as parallel branches, GMRES loops as device-decided conditional
@@ -392,6 +427,15 @@ def vjp_leg(args, local, world, cells, warm_state32):
 
 def run_ours(args):
     world, rank, local = dist_setup()
+    if args.roofline_only:
+        from suetes_b200 import _lib
+        cls = {"matvec": _lib.K_MATVEC, "precond": _lib.K_PRECOND, "dots": _lib.K_DOTS, "update": _lib.K_UPDATE}[
+            args.roofline_class]
+        peak, peak_kind = measured_peaks()
+        r = roofline_leg(args, local, world, cls, peak, peak_kind)
+        if rank == 0:
+            print(json.dumps({"roofline": r, "nx": args.nx, "ny": args.ny, "nz": args.nz}), flush=True)
+        return
     import suetes_b200 as sb
     from suetes_b200 import _lib
     from suetes_b200.workloads import mountain_wave
@@ -408,7 +452,7 @@ def run_ours(args):
     ds = st32.to_device_state(s32)
     tuning = None if args.no_autotune else ds.core.autotune()
     with ClockSampler(local) as clk:
-        ms, infos, launches, kt, cur32 = timed_device_steps(st32, ds, bc, K, W, world, cls)
+        ms, infos, launches, _, cur32 = timed_device_steps(st32, ds, bc, K, W, world)
     ms = dist_max(ms, world)
     value = world * cells * K / (ms / 1e3)
     solves = [s for i in infos for s in i["solves"]]
@@ -418,12 +462,7 @@ def run_ours(args):
           "tol": args.tol32, "restart": 30, "maxiter": 30, "method": args.method,
           "refinement": "none" if args.no_refine else "float64 residual and solution per restart"}
     peak, peak_kind = measured_peaks()
-    k_ms, k_n, k_bytes = kt
-    achieved = (k_bytes / k_n) / (k_ms / k_n / 1e3) / 1e9 if k_n else None
-    roofline = {"kernel": f"gmres_{args.roofline_class}", "bound": "hbm", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
-                "peak_kind": peak_kind, "launches_timed": k_n, "avg_launch_us": k_ms / max(k_n, 1) * 1e3,
-                "alg_bytes_per_launch": k_bytes / max(k_n, 1), "share_of_step": k_ms / ms}
+    roofline = roofline_leg(args, local, world, cls, peak, peak_kind)
 
     line = {"metric": "SISL cell-steps/s fwd (mountain wave 256x256x80)", "value": value, "unit": "cell-steps/s",
             "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
