@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--cpu-window", type=int, default=32, help="nx = ny of the CPU-baseline window")
     ap.add_argument("--classes", action="store_true",
                     help="also time every GMRES kernel class separately (diagnostic)")
+    ap.add_argument("--no-micro", action="store_true", help="skip the 384x384x96 microbenchmark leg")
+    ap.add_argument("--micro-solves", type=int, default=10,
+                    help="GMRES solves of the 384x384x96 microbenchmark leg (0 disables the leg)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--roofline-only", action="store_true",
                     help="run only the roofline leg (batched GMRES, one kernel class timed): the profiling command")
@@ -307,6 +310,102 @@ def roofline_leg(args, local, world, cls, peak, peak_kind):
     return out
 
 
+def micro_leg(args, local, world, peak):
+    """Kernel microbenchmarks on the 384x384x96 grid (float32): tricubic
+    interpolation of a 32-mode cosine field at seeded smooth displacements
+    with Courant numbers in [0, 3] (and its VJP), departure points, and
+    standalone GMRES solves of N(0, 1) right-hand sides on the mountain-wave
+    physics over flat terrain.  Achieved GB/s count each distinct array once."""
+    import math as _m
+    from suetes_b200 import SemiImplicitSolver3D, SemiLagrangianAdvector3D
+    from suetes_b200.operators import tensor_product_interp_3d, tricubic_vjp
+    from suetes_b200.core import fortran
+    from suetes_b200.workloads import mountain_wave
+    dev = torch.device(f"cuda:{local}")
+    nx, ny, nz = 384, 384, 96
+    N = nx * ny * nz
+    gen = torch.Generator(device="cpu").manual_seed(3)
+    x = torch.arange(nx, device=dev, dtype=torch.float32)[:, None, None] / nx
+    y = torch.arange(ny, device=dev, dtype=torch.float32)[None, :, None] / ny
+    z = torch.arange(nz, device=dev, dtype=torch.float32)[None, None, :] / nz
+    f = torch.zeros(nx, ny, nz, device=dev, dtype=torch.float32)
+    ks = torch.randint(1, 25, (32, 3), generator=gen)
+    ph = torch.rand(32, generator=gen) * 2 * _m.pi
+    for m in range(32):
+        f += torch.cos(2 * _m.pi * (ks[m, 0] * x + ks[m, 1] * y + ks[m, 2] * z) + float(ph[m]))
+    f = fortran(f)
+    coords = []
+    for a, n in enumerate((nx, ny, nz)):
+        sm = torch.zeros(nx, ny, nz, device=dev, dtype=torch.float32)
+        for m in range(6):  # smooth field of modes 1-3
+            kk = torch.randint(1, 4, (3,), generator=gen)
+            sm += torch.cos(2 * _m.pi * (kk[0] * x + kk[1] * y + kk[2] * z) + float(torch.rand(1, generator=gen)) * 6.28)
+        rank = torch.empty(N, device=dev, dtype=torch.float32)
+        rank[torch.argsort(sm.reshape(-1))] = torch.arange(N, device=dev, dtype=torch.float32) / (N - 1)
+        disp = 3.0 * rank.reshape(nx, ny, nz)  # empirical CDF -> U[0, 1], Courant in [0, 3]
+        idx = (x * nx, y * ny, z * nz)[a].expand(nx, ny, nz)
+        coords.append(fortran(idx - disp))
+    out = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=10):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms = timed(lambda: tensor_product_interp_3d(f, coords))
+    out["tricubic"] = {"us": ms * 1e3, "achieved_GBs": 5 * N * 4 / (ms / 1e3) / 1e9,
+                       "frac_of_measured": 5 * N * 4 / (ms / 1e3) / 1e9 / peak,
+                       "bytes": "field + 3 coordinates + output (each once)"}
+    cot = torch.ones_like(f)
+    grad = torch.zeros_like(f)
+    ms = timed(lambda: tricubic_vjp(f, coords, cot, out=grad))
+    out["tricubic_vjp"] = {"us": ms * 1e3, "achieved_GBs": 6 * N * 4 / (ms / 1e3) / 1e9,
+                           "frac_of_measured": 6 * N * 4 / (ms / 1e3) / 1e9 / peak,
+                           "bytes": "cotangent + 3 coordinates + gradient read and written",
+                           "form": "64 float atomic adds per point"}
+    st, s0, bc = mountain_wave(nx, ny, nz, dtype=torch.float32, device=dev, solver_tol=args.tol32,
+                               solve_method=args.method, flat=True)
+    adv = SemiLagrangianAdvector3D(st.physics.grid, st.physics, st.dt)
+    vel = {"u": fortran(s0["u"]) + 0.0, "v": fortran(s0["v"]) + 0.0, "eta_dot": fortran(s0["eta_dot"]) + 0.0}
+    ms = timed(lambda: adv.compute_departure_indices(vel, loc="m"))
+    out["departure_m"] = {"us": ms * 1e3, "achieved_GBs": 6 * N * 4 / (ms / 1e3) / 1e9,
+                          "frac_of_measured": 6 * N * 4 / (ms / 1e3) / 1e9 / peak,
+                          "bytes": "u, v, eta_dot in, 3 coordinates out (velocity averaging included)"}
+    if args.micro_solves > 0:
+        sol = st.implicit_solver
+        bg = st.physics.precompute_bg(st.physics.bg_state_ref())
+        g = st.physics.grid
+        rhs = {}
+        for k, loc in (("u", "u"), ("v", "v"), ("w", "w"), ("pi", "m"), ("eta_dot", "w")):
+            t = torch.randn(g.shape_of(loc), generator=gen).to(dev, torch.float32)
+            if k in ("w", "eta_dot"):
+                t[:, :, 0] = 0.0
+                t[:, :, -1] = 0.0
+            rhs[k] = fortran(t)
+        sol.solve(rhs, bg)
+        torch.cuda.synchronize()
+        steps = []
+        e0.record()
+        for _ in range(args.micro_solves):
+            sol.solve(rhs, bg)
+            steps.append(sol.last_info["arnoldi_steps"])
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.micro_solves
+        out["gmres_solve"] = {"ms_per_solve": ms, "solves": args.micro_solves,
+                              "arnoldi_per_solve": sum(steps) / len(steps), "rhs": "N(0,1), w/eta_dot ends zero",
+                              "tol": args.tol32, "method": args.method, "restart": 30}
+    del st
+    return {"grid": [nx, ny, nz], "dtype": "f32", "kernels": out}
+
+
 def ensemble_leg(args, local, world):
     """The uneven-size bubble ensemble advanced as one CUDA graph per step
     (members as parallel branches, GMRES loops as device-decided conditional
@@ -520,6 +619,10 @@ def run_ours(args):
     # ---- fwd+VJP: gradient of the lee box energy w.r.t. the initial theta' ----
     if args.vjp_steps > 0:
         line["fwd_vjp"] = vjp_leg(args, local, world, cells, cur32)
+
+    # ---- 384x384x96 kernel microbenchmarks ----
+    if args.micro_solves >= 0 and not args.no_micro:
+        line["micro"] = micro_leg(args, local, world, peak)
 
     # ---- uneven-size ensemble under one CUDA graph per step ----
     if args.ens_members > 0:

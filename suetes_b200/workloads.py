@@ -41,8 +41,10 @@ def ridge(x, y):
 
 
 def mountain_wave(nx=256, ny=256, nz=80, dtype=F32, device="cuda", solver_tol=1e-8, solver_maxiter=30,
-                  solver_restart=30, solve_method="batched", dt=8.0, refine=True):
-    grid = RegionalGrid3D(nx, ny, nz, 500.0, 500.0, 20000.0 / nz, 45.0, 0.0, h_func=ridge,
+                  solver_restart=30, solve_method="batched", dt=8.0, refine=True, flat=False):
+    """``flat``: the same physics over flat terrain ("flat-then-SLEVE")."""
+    h = (lambda x, y: 0.0 * x + 0.0 * y) if flat else ridge
+    grid = RegionalGrid3D(nx, ny, nz, 500.0, 500.0, 20000.0 / nz, 45.0, 0.0, h_func=h,
                           transform=StretchedSleveSimple(2.5, 4000.0, 1.35), device=device)
     op = CGridOperator3D(grid)
     bgp = Euler3D(grid, op, CONSTANTS, dt=dt, N_bv=0.01)
