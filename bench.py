@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--classes", action="store_true",
                     help="also time every GMRES kernel class separately (diagnostic)")
     ap.add_argument("--no-micro", action="store_true", help="skip the 384x384x96 microbenchmark leg")
+    ap.add_argument("--c4", action="store_true",
+                    help="also run the 192x192x64 60-step checkpointed fwd+VJP leg with its float64 Taylor test")
     ap.add_argument("--micro-solves", type=int, default=10,
                     help="GMRES solves of the 384x384x96 microbenchmark leg (0 disables the leg)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
@@ -406,6 +408,69 @@ def micro_leg(args, local, world, peak):
     return {"grid": [nx, ny, nz], "dtype": "f32", "kernels": out}
 
 
+def c4_leg(args, local, world):
+    """The reduced mountain wave (192x192x64) over a 60-step float32
+    trajectory with a checkpoint every 10 steps: value and gradient of the
+    mean lee-box energy of the last 10 states w.r.t. the initial theta',
+    timed; the float64 gradient of the same trajectory; and the float64
+    Taylor remainders |J(x + e d) - J(x) - e <g, d>| for a smooth seeded d
+    (verification/adjoint_gradient_convergence.py:131-157)."""
+    import math as _m
+    from suetes_b200.adjoint import trajectory_vjp
+    from suetes_b200.workloads import box_energy_objective, mountain_wave
+    N, K = 60, 10
+    nx, ny, nz = 192, 192, 64
+    out = {"metric": "SISL cell-steps/s fwd+VJP (192x192x64, 60 steps, checkpoint every 10)",
+           "unit": "cell-steps/s", "steps": N, "checkpoint_every": K}
+    res = {}
+    for dtype, tol in ((torch.float32, args.tol32), (torch.float64, args.tol64)):
+        st, s0, bc = mountain_wave(nx, ny, nz, dtype=dtype, device=f"cuda:{local}", solver_tol=tol,
+                                   solve_method=args.method, refine=not args.no_refine)
+        st.implicit_solver.transpose_tol = args.adj_tol32 if dtype == torch.float32 else None
+        st.implicit_solver.transpose_method = args.adj_method
+        obj = box_energy_objective(st, N)
+        ds0 = st.to_device_state(s0)
+        trajectory_vjp(st, ds0, 2, box_energy_objective(st, 2), bc_fn=bc, checkpoint_every=K)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        J, g = trajectory_vjp(st, ds0, N, obj, bc_fn=bc, checkpoint_every=K)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = dist_max(e0.elapsed_time(e1), world)
+        res[dtype] = (float(J), g["th_p"].double(), ms, st, ds0, bc, obj)
+    J32, g32, ms32 = res[torch.float32][:3]
+    J64, g64, ms64, st64, ds64, bc64, obj64 = res[torch.float64]
+    cells = nx * ny * nz
+    out.update({"value": world * cells * N / (ms32 / 1e3), "ms_per_step": ms32 / N, "J": J32,
+                "fp64": {"value": world * cells * N / (ms64 / 1e3), "ms_per_step": ms64 / N, "J": J64},
+                "err_f32_vs_f64": {"J_rel": abs(J32 - J64) / abs(J64),
+                                   "grad_rel_l2": float((g32 - g64).norm() / g64.norm())}})
+    # float64 Taylor test along a smooth seeded direction
+    gen = torch.Generator(device="cpu").manual_seed(4)
+    g = st64.physics.grid
+    X = g.x_m[:, None, None] / (g.nx * g.dx)
+    Z = g.Z_m / 20000.0
+    kx, kz = torch.randint(1, 4, (2,), generator=gen)
+    d = torch.sin(2 * _m.pi * kx * X + 0.3) * torch.sin(_m.pi * kz * Z)
+    from suetes_b200.core import fortran
+    d = fortran(d.expand(g.nx, g.ny, g.nz).to(torch.float64))
+    slope = float((g64 * d).sum())
+    rems = []
+    from suetes_b200.steppers import DeviceState
+    for e in (1e-1, 1e-2, 1e-3):
+        t = {k: v.clone() for k, v in ds64.t.items()}
+        t["th_p"] += e * d
+        Je, _ = trajectory_vjp(st64, DeviceState(ds64.core, t, ds64.is_first_step), N, obj64, bc_fn=bc64,
+                               checkpoint_every=K, wrt=())
+        rems.append(abs(float(Je) - J64 - e * slope))
+    orders = [_m.log10(rems[q] / rems[q + 1]) if rems[q + 1] > 0 else None for q in range(len(rems) - 1)]
+    out["taylor_f64"] = {"eps": [1e-1, 1e-2, 1e-3], "remainders": rems, "orders": orders,
+                         "direction": "sin(2 pi kx x / Lx + 0.3) sin(pi kz z / 20 km), seeded"}
+    del res
+    return out
+
+
 def ensemble_leg(args, local, world):
     """The uneven-size bubble ensemble advanced as one CUDA graph per step
     (members as parallel branches, GMRES loops as device-decided conditional
@@ -619,6 +684,10 @@ def run_ours(args):
     # ---- fwd+VJP: gradient of the lee box energy w.r.t. the initial theta' ----
     if args.vjp_steps > 0:
         line["fwd_vjp"] = vjp_leg(args, local, world, cells, cur32)
+
+    # ---- 192x192x64 60-step checkpointed fwd+VJP with the Taylor test ----
+    if args.c4:
+        line["fwd_vjp_c4"] = c4_leg(args, local, world)
 
     # ---- 384x384x96 kernel microbenchmarks ----
     if args.micro_solves >= 0 and not args.no_micro:

@@ -198,9 +198,12 @@ int sisl_helmholtz_matvec_t(SislCore* core, const void* const in[5], void* const
 int sisl_precond_apply_t(SislCore* core, const void* const in[5], void* const out[5], void* stream);
 /* bwd_solve of SemiImplicitSolver3D.solve (steppers.py:473-485): the cotangent
  * of the physical rhs from the cotangent of the physical solution, by GMRES on
- * A^T with preconditioner M^T from a zero guess and the forward tol/restart. */
-int sisl_gmres_solve_transpose(SislCore* core, const void* const xbar[5], void* const bbar[5], void* ws,
-                               size_t ws_bytes, void* stream, SislSolveInfo* info);
+ * A^T with preconditioner M^T and the settings of sisl_core_set_adjoint.
+ * x0 NULL starts from zero as bwd_solve does; otherwise x0 (in the units of
+ * bbar) is the initial guess, e.g. the previous step's result in a backward
+ * sweep (same solution within the tolerance, fewer cycles). */
+int sisl_gmres_solve_transpose(SislCore* core, const void* const xbar[5], const void* const x0[5],
+                               void* const bbar[5], void* ws, size_t ws_bytes, void* stream, SislSolveInfo* info);
 /* SemiLagrangianAdvector3D.compute_departure_indices(state, loc, iterations)
  * (steppers.py:318-360); coords[3] have the extents of stagger loc. */
 int sisl_departure(SislCore* core, int loc, const void* u, const void* v, const void* eta_dot, int iterations,

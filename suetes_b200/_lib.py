@@ -103,7 +103,7 @@ PROTOTYPES = {
                                         ctypes.POINTER(SislSolveInfo)]),
     "sisl_helmholtz_matvec_t": (ctypes.c_int, [vp, vp * 5, vp * 5, vp, ctypes.c_size_t, vp]),
     "sisl_precond_apply_t": (ctypes.c_int, [vp, vp * 5, vp * 5, vp]),
-    "sisl_gmres_solve_transpose": (ctypes.c_int, [vp, vp * 5, vp * 5, vp, ctypes.c_size_t, vp,
+    "sisl_gmres_solve_transpose": (ctypes.c_int, [vp, vp * 5, vp, vp * 5, vp, ctypes.c_size_t, vp,
                                                   ctypes.POINTER(SislSolveInfo)]),
     "sisl_departure": (ctypes.c_int, [vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp * 3, vp, ctypes.c_size_t,
                                       vp]),

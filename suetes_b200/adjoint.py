@@ -40,11 +40,13 @@ STATE_KEYS = ("u", "v", "w", "eta_dot", "pi_p", "th_p", "rho", "u_prev", "v_prev
 
 class _RecordedSolve(torch.autograd.Function):
     """The implicit solve of a recomputed step: forward returns the solution
-    recorded by the fused step, backward is the transposed GMRES solve."""
+    recorded by the fused step, backward is the transposed GMRES solve,
+    warm-started from ``warm[slot]`` (the same solve of the step after, in a
+    backward sweep) when given, which it then replaces."""
 
     @staticmethod
-    def forward(ctx, solver, core, recorded, *b):
-        ctx.solver, ctx.core = solver, core
+    def forward(ctx, solver, core, recorded, warm, slot, *b):
+        ctx.solver, ctx.core, ctx.warm, ctx.slot = solver, core, warm, slot
         return tuple(r.clone() for r in recorded)
 
     @staticmethod
@@ -52,7 +54,11 @@ class _RecordedSolve(torch.autograd.Function):
         core = ctx.core
         gs = [empty_field(core.shape(l), core.dtype, core.device).zero_() if t is None else core.field(t, l)
               for t, l in zip(g, LOCS5)]
-        return (None, None, None) + tuple(ctx.solver._solve_transpose_core(core, gs))
+        x0 = ctx.warm.get(ctx.slot) if ctx.warm is not None else None
+        out = ctx.solver._solve_transpose_core(core, gs, x0)
+        if ctx.warm is not None:
+            ctx.warm[ctx.slot] = out
+        return (None, None, None, None, None) + tuple(out)
 
 
 class DifferentiableStep:
@@ -197,7 +203,7 @@ class DifferentiableStep:
                 tr[k] = x
             return {loc: adv.compute_departure_indices(tr, loc=loc, iterations=it) for loc in ("u", "v", "w", "m")}
 
-    def __call__(self, state, relax=None, recorded=None, coords=None):
+    def __call__(self, state, relax=None, recorded=None, coords=None, warm=None):
         """One step on a perturbation-form state (keys of ``STATE_KEYS`` plus
         ``is_first_step``); returns the next state in the same form.
 
@@ -264,7 +270,7 @@ class DifferentiableStep:
             rhs_w_k = torch.where(self.w_ground, kb, (rhs_w + buoy + nl_w) * self.w_inner)
             b = [core.field(t, l) for t, l in zip((rhs_u_k, rhs_v_k, rhs_w_k, rhs_pi_k, R_eta_adv), LOCS5)]
             if recorded is not None:
-                x = _RecordedSolve.apply(solver, core, recorded[it], *b)
+                x = _RecordedSolve.apply(solver, core, recorded[it], warm, it, *b)
             elif torch.is_grad_enabled() and any(t.requires_grad for t in b):
                 from .steppers import _LinearSolve
                 x = _LinearSolve.apply(solver, core, guess, *b)
@@ -330,7 +336,8 @@ def _as_dict(ds):
     return d
 
 
-def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint_every=1, wrt=("th_p",)):
+def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint_every=1, wrt=("th_p",),
+                   warm_start=False):
     """Value and gradient of ``J = sum_n objective(n, state_n)`` over
     ``num_steps`` SISL steps from ``state0`` (a reference state dict or a
     ``DeviceState``).
@@ -343,7 +350,10 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
     and keeps every ``checkpoint_every``-th state; the backward pass
     recomputes a segment with the fused step (recording its solves) and
     differentiates it one step at a time through ``DifferentiableStep``
-    (jax.checkpoint of steppers.py:792-850, driver.py:91-132)."""
+    (jax.checkpoint of steppers.py:792-850, driver.py:91-132).  With
+    ``warm_start`` each transposed solve starts from the same solve's result
+    of the step after (the reference's bwd_solve starts from zero; both
+    converge to the same cotangent within the solver tolerance)."""
     relax, generic = stepper._relax_of(bc_fn)
     if generic is not None:
         raise NotImplementedError("trajectory_vjp supports LateralRelaxation boundary conditions")
@@ -369,6 +379,7 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
                 checkpoints[n + 1] = cur
     keys = [k for k in STATE_KEYS]
     cot = {}
+    warm = {} if warm_start else None  # transposed-solve guesses carried along the backward sweep
     for seg0 in range(((num_steps - 1) // K) * K, -1, -K):
         seg1 = min(seg0 + K, num_steps)
         if keep_all:
@@ -394,7 +405,7 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
             before = {k: v.detach().requires_grad_(True) for k, v in before_ds.t.items()}
             with torch.enable_grad():
                 out = dstep(dict(before, is_first_step=before_ds.is_first_step), relax=relax,
-                            recorded=recs[n - seg0])
+                            recorded=recs[n - seg0], warm=warm)
                 outs, grads = [], []
                 for k, g in g_after.items():
                     if k in out and torch.is_tensor(out[k]) and out[k].requires_grad:

@@ -589,8 +589,8 @@ int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, co
 // physical solution (custom_linear_solve transpose, steppers.py:473-485):
 // unscale (x = S_out x_s), GMRES on A^T from a zero guess, rescale (b_s = S_in b).
 template <typename T>
-int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> xbar, Vec5<T> bbar,
-                             cudaStream_t st, SislSolveInfo* info) {
+int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> xbar, const CVec5<T>* x0,
+                             Vec5<T> bbar, cudaStream_t st, SislSolveInfo* info) {
   const Dims& d = c->d;
   {
     KScope k(c, SISL_K_OTHER, st);
@@ -599,7 +599,10 @@ int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<
   }
   const T ps = (T)c->s.ps;
   scale5<T>(c, cf, xbar, g.view(g.bg()), (T)(1.0 / c->s.ps), 2, st);  // pi / ps, eta / dz_w
-  if (cudaMemsetAsync(g.xg(), 0, sizeof(T) * g.npad, st) != cudaSuccess) return SISL_ERR_CUDA;
+  // initial guess: zero as in bwd_solve, or a caller's guess in the units of
+  // the result (a warm start: the same solution within the tolerance)
+  if (x0) scale5<T>(c, cf, *x0, g.view(g.xg()), (T)(1.0 / c->s.ps), 0, st);
+  else if (cudaMemsetAsync(g.xg(), 0, sizeof(T) * g.npad, st) != cudaSuccess) return SISL_ERR_CUDA;
   // GMRES treats a preconditioned residual below machine epsilon as zero
   // (_safe_normalize's absolute threshold); cotangents are often far below
   // unit norm, so the right-hand side is solved at unit norm and rescaled
@@ -611,6 +614,7 @@ int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<
     gm_dots<T>(g.V(0), g.npad, 0, g.bg(), g.npad, g.partial, g.gs, 1 /*BNORM*/, 0, st);
     keep_norm_kernel<<<1, 1, 0, st>>>(g.gs, g.scal);
     scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.bg(), g.npad, g.scal, 0);
+    if (x0) scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.xg(), g.npad, g.scal, 0);
   }
   int rc = gmres_run<T>(c, cf, g, st, info, 1);
   if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
@@ -1075,8 +1079,8 @@ int sisl_precond_apply_t(SislCore* c, const void* const in[5], void* const out[5
   return check_cuda();
 }
 
-int sisl_gmres_solve_transpose(SislCore* c, const void* const xbar[5], void* const bbar[5], void* ws,
-                               size_t ws_bytes, void* stream, SislSolveInfo* info) {
+int sisl_gmres_solve_transpose(SislCore* c, const void* const xbar[5], const void* const x0[5],
+                               void* const bbar[5], void* ws, size_t ws_bytes, void* stream, SislSolveInfo* info) {
   if (!c || !xbar || !bbar) return SISL_ERR_ARG;
   if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_GMRES)) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
@@ -1084,10 +1088,16 @@ int sisl_gmres_solve_transpose(SislCore* c, const void* const xbar[5], void* con
   int rc;
   if (c->grid.dtype == SISL_F64) {
     GWork<double> g = carve_gmres<double>(cv, c->d, c->prm.solver_restart, false);
-    rc = solve_transpose_physical<double>(c, coef_of<double>(c), g, cvec<double>(xbar), vec<double>(bbar), st, info);
+    CVec5<double> x0v;
+    if (x0) x0v = cvec<double>(x0);
+    rc = solve_transpose_physical<double>(c, coef_of<double>(c), g, cvec<double>(xbar), x0 ? &x0v : nullptr,
+                                          vec<double>(bbar), st, info);
   } else {
     GWork<float> g = carve_gmres<float>(cv, c->d, c->prm.solver_restart, refining<float>(c));
-    rc = solve_transpose_physical<float>(c, coef_of<float>(c), g, cvec<float>(xbar), vec<float>(bbar), st, info);
+    CVec5<float> x0v;
+    if (x0) x0v = cvec<float>(x0);
+    rc = solve_transpose_physical<float>(c, coef_of<float>(c), g, cvec<float>(xbar), x0 ? &x0v : nullptr,
+                                         vec<float>(bbar), st, info);
   }
   int e = check_cuda();
   return e ? e : rc;

@@ -137,6 +137,7 @@ class SemiImplicitSolver3D:
         # unit-norm scaling of the cotangent (False: the reference's absolute eps floor)
         self.transpose_tol = None
         self.transpose_method = None  # "batched" / "incremental"; None: solve_method
+        self.transpose_log = None  # a list collects every transposed solve's statistics
         self.adjoint_normalize = True
         self.last_info = None
 
@@ -173,23 +174,31 @@ class SemiImplicitSolver3D:
         self.last_info = info.as_dict()
         return x
 
-    def solve_transpose(self, cot_solution, bg_precomputed, dtype=None):
+    def solve_transpose(self, cot_solution, bg_precomputed, dtype=None, x0=None):
         """bwd_solve (steppers.py:473-481): the cotangent of the physical rhs
-        from the cotangent of the physical solution."""
+        from the cotangent of the physical solution; ``x0`` an optional
+        initial guess (zero as in the reference otherwise)."""
         core = self._core(dtype or _dtype_of(cot_solution), bg_precomputed)
         g = [core.field(cot_solution[k], l) for k, l in LOC5]
-        return {k: t for (k, _), t in zip(LOC5, self._solve_transpose_core(core, g))}
+        x0l = [x0[k] for k, _ in LOC5] if x0 is not None else None
+        return {k: t for (k, _), t in zip(LOC5, self._solve_transpose_core(core, g, x0l))}
 
-    def _solve_transpose_core(self, core, g):
+    def _solve_transpose_core(self, core, g, x0=None):
         out = [core.new(l) for _, l in LOC5]
         g = [t.detach() for t in g]
+        x0p = None
+        if x0 is not None:
+            x0 = [core.field(t, l).detach() for t, (_, l) in zip(x0, LOC5)]
+            x0p = ctypes.cast(ptrs(x0, 5), ctypes.c_void_p)
         ws, n = core.workspace(_lib.WS_GMRES)
         info = _lib.SislSolveInfo()
         core.set_adjoint(self.transpose_tol, self.adjoint_normalize,
                          None if self.transpose_method is None else SOLVE_METHODS[self.transpose_method])
-        check(core.lib.sisl_gmres_solve_transpose(core.handle, ptrs(g, 5), ptrs(out, 5), ws.data_ptr(), n,
+        check(core.lib.sisl_gmres_solve_transpose(core.handle, ptrs(g, 5), x0p, ptrs(out, 5), ws.data_ptr(), n,
                                                   core.stream, ctypes.byref(info)), "sisl_gmres_solve_transpose")
         self.last_transpose_info = info.as_dict()
+        if self.transpose_log is not None:
+            self.transpose_log.append(self.last_transpose_info)
         return out
 
     def matvec_scaled(self, x_scaled, bg_precomputed, transpose=False):

@@ -377,3 +377,21 @@ def test_transpose_solve_scale_invariant_float32():
     assert s32.last_transpose_info["converged"]
     for k in FIELDS5:
         assert rel_l2(out[k].double() * 1e9, ref[k]) < 1e-4, (k, rel_l2(out[k].double() * 1e9, ref[k]))
+
+
+def test_transpose_solve_warm_start_same_solution():
+    """A warm start (the backward sweep's previous result) converges to the
+    cotangent of the zero-started bwd_solve within the tolerance."""
+    from suetes_b200 import SemiImplicitSolver3D as PS
+    c, _, (pg, pop, pph) = _pair("mountain")
+    sh = shapes5(c["nx"], c["ny"], c["nz"])
+    cot = to_cuda(random_fields(sh, 29, {"u": 1.0, "v": 1.0, "w": 1.0, "pi": 100.0, "eta_dot": 100.0}))
+    sol = PS(pph, 40.0, alpha=0.55, solver_tol=1e-12, solver_maxiter=50, solver_restart=30)
+    cold = sol.solve_transpose(cot, _bg(pph))
+    cold_cycles = sol.last_transpose_info["cycles"]
+    guess = {k: v * 1.001 for k, v in cold.items()}
+    warm = sol.solve_transpose(cot, _bg(pph), x0=guess)
+    assert sol.last_transpose_info["converged"]
+    assert sol.last_transpose_info["cycles"] < cold_cycles
+    for k in FIELDS5:
+        assert rel_l2(warm[k], cold[k]) < 1e-9, (k, rel_l2(warm[k], cold[k]))
