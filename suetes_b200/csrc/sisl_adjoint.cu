@@ -19,7 +19,6 @@
 //  with P = p / ps, gzw(k) = (P(kr) - P(kl)) / dz_w(k) on the padded level
 //  pair, gzm(k) = (gzw(k) + gzw(k+1)) / 2, Fx = u rdu thu, Fz = W rhow thw.
 #include "sisl_core.cuh"
-#include "sisl_tile.cuh"
 
 namespace sisl {
 namespace {
@@ -432,130 +431,95 @@ __device__ __forceinline__ T share_min(T a, T b) { return a < b ? T(1) : (a > b 
 template <typename T>
 __device__ __forceinline__ T share_max(T a, T b) { return a > b ? T(1) : (a < b ? T(0) : T(0.5)); }
 
-// Scatter-add in two levels: a block's contributions land in a staged
-// shared-memory box of its stencils (shared-memory atomics), which is then
-// added to the field's cotangent with one global atomic per touched box
-// element; blocks whose box does not fit scatter straight to global memory.
 template <typename T>
 __global__ void __launch_bounds__(256) tricubic_vjp_kernel(int sx, int sy, int sz, int dx, int dy, int dz,
                                                            const T* __restrict__ f, const T* __restrict__ cx,
                                                            const T* __restrict__ cy, const T* __restrict__ cz,
                                                            const T* __restrict__ cot, T* grad, int limiter,
                                                            T scale) {
-  __shared__ T sacc[TileCap<T>::n];
-  __shared__ int sb[6];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
-  const bool inr = i < dx && j < dy && k < dz;
-  const int p = inr ? i + dx * (j + dy * k) : 0;
-  const T g = inr ? scale * ld(cot, p) : T(0);
-  const bool valid = inr && g != T(0);
-  T x = T(0), y = T(0), z = T(0);
-  if (valid) {
-    x = fmin(fmax(ld(cx, p), T(0)), (T)(sx - 1));
-    y = fmin(fmax(ld(cy, p), T(0)), (T)(sy - 1));
-    z = fmin(fmax(ld(cz, p), T(0)), (T)(sz - 1));
-  }
+  if (i >= dx || j >= dy || k >= dz) return;
+  const int p = i + dx * (j + dy * k);
+  const T g = scale * ld(cot, p);
+  if (g == T(0)) return;
+  const T x = fmin(fmax(ld(cx, p), T(0)), (T)(sx - 1));
+  const T y = fmin(fmax(ld(cy, p), T(0)), (T)(sy - 1));
+  const T z = fmin(fmax(ld(cz, p), T(0)), (T)(sz - 1));
   const int x0 = (int)floor(x), y0 = (int)floor(y), z0 = (int)floor(z);
-  const SlBox b = block_box(sb, valid, x0, y0, z0, sx, sy, sz);
-  const int vol = b.vol();
-  const bool tiled = vol > 0 && vol <= TileCap<T>::n;
-  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-  const int nt = blockDim.x * blockDim.y * blockDim.z;
-  if (tiled) {
-    for (int q = tid; q < vol; q += nt) sacc[q] = T(0);
-    __syncthreads();
-  }
+  T wx[4], wy[4], wz[4];
+  cr_w(x - (T)x0, wx);
+  cr_w(y - (T)y0, wy);
+  cr_w(z - (T)z0, wz);
+  const int ix[4] = {max(x0 - 1, 0), x0, min(x0 + 1, sx - 1), min(x0 + 2, sx - 1)};
+  const int iy[4] = {max(y0 - 1, 0), y0, min(y0 + 1, sy - 1), min(y0 + 2, sy - 1)};
+  const int iz[4] = {max(z0 - 1, 0), z0, min(z0 + 1, sz - 1), min(z0 + 2, sz - 1)};
   const int plane = sx * sy;
-  auto acc = [&](int a, int bb, int c, T v) {
-    if (tiled) atomicAdd(&sacc[(a - b.lx) + b.nx * ((bb - b.ly) + b.ny * (c - b.lz))], v);
-    else atomic_acc(grad + a + sx * bb + plane * c, v);
-  };
-  if (valid) {
-    T wx[4], wy[4], wz[4];
-    cr_w(x - (T)x0, wx);
-    cr_w(y - (T)y0, wy);
-    cr_w(z - (T)z0, wz);
-    const int ix[4] = {max(x0 - 1, 0), x0, min(x0 + 1, sx - 1), min(x0 + 2, sx - 1)};
-    const int iy[4] = {max(y0 - 1, 0), y0, min(y0 + 1, sy - 1), min(y0 + 2, sy - 1)};
-    const int iz[4] = {max(z0 - 1, 0), z0, min(z0 + 1, sz - 1), min(z0 + 2, sz - 1)};
-    T gf = g;
-    if (limiter) {
-      T fi = T(0);
+  T gf = g;
+  if (limiter) {
+    T fi = T(0);
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        T syv = T(0);
+    for (int a = 0; a < 4; ++a) {
+      T syv = T(0);
 #pragma unroll
-        for (int q2 = 0; q2 < 4; ++q2) {
-          const int row = ix[a] + sx * iy[q2];
-          T szv = T(0);
+      for (int b = 0; b < 4; ++b) {
+        const int row = ix[a] + sx * iy[b];
+        T szv = T(0);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) szv += wz[q] * ld(f, row + plane * iz[q]);
-          syv += wy[q2] * szv;
-        }
-        fi += wx[a] * syv;
+        for (int q = 0; q < 4; ++q) szv += wz[q] * ld(f, row + plane * iz[q]);
+        syv += wy[b] * szv;
       }
-      const int x1 = min(x0 + 1, sx - 1), y1 = min(y0 + 1, sy - 1), z1 = min(z0 + 1, sz - 1);
-      // corners in the reference order (operators.py:200-201)
-      const int cxs[8] = {x0, x1, x0, x1, x0, x1, x0, x1};
-      const int cys[8] = {y0, y0, y1, y1, y0, y0, y1, y1};
-      const int czs[8] = {z0, z0, z0, z0, z1, z1, z1, z1};
-      T nb[8], mn[8], mx[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) nb[q] = ld(f, cxs[q] + sx * cys[q] + plane * czs[q]);
-      mn[0] = mx[0] = nb[0];
-#pragma unroll
-      for (int q = 1; q < 8; ++q) {
-        mn[q] = fmin(mn[q - 1], nb[q]);
-        mx[q] = fmax(mx[q - 1], nb[q]);
-      }
-      // jnp.clip(f, lo, hi) = minimum(hi, maximum(lo, f))
-      const T lo = mn[7], hi = mx[7];
-      const T v1 = fmax(lo, fi);
-      const T a1 = share_max(fi, lo);  // to f
-      const T a2 = share_min(v1, hi);  // to maximum(lo, f)
-      gf = g * a2 * a1;
-      T glo = g * a2 * (T(1) - a1), ghi = g * (T(1) - a2);
-      T gn[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) gn[q] = T(0);
-#pragma unroll
-      for (int q = 7; q >= 1; --q) {
-        const T wl = share_min(mn[q - 1], nb[q]);
-        gn[q] += glo * (T(1) - wl);
-        glo *= wl;
-        const T wh = share_max(mx[q - 1], nb[q]);
-        gn[q] += ghi * (T(1) - wh);
-        ghi *= wh;
-      }
-      gn[0] += glo + ghi;
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        if (gn[q] != T(0)) acc(cxs[q], cys[q], czs[q], gn[q]);
+      fi += wx[a] * syv;
     }
-    if (gf != T(0)) {
+    const int x1 = min(x0 + 1, sx - 1), y1 = min(y0 + 1, sy - 1), z1 = min(z0 + 1, sz - 1);
+    // corners in the reference order (operators.py:200-201)
+    const int cidx[8] = {x0 + sx * (y0 + sy * z0), x1 + sx * (y0 + sy * z0), x0 + sx * (y1 + sy * z0),
+                         x1 + sx * (y1 + sy * z0), x0 + sx * (y0 + sy * z1), x1 + sx * (y0 + sy * z1),
+                         x0 + sx * (y1 + sy * z1), x1 + sx * (y1 + sy * z1)};
+    T nb[8], mn[8], mx[8];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const T ga = gf * wx[a];
+    for (int s = 0; s < 8; ++s) nb[s] = ld(f, cidx[s]);
+    mn[0] = mx[0] = nb[0];
 #pragma unroll
-        for (int q2 = 0; q2 < 4; ++q2) {
-          const T gb = ga * wy[q2];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) acc(ix[a], iy[q2], iz[q], gb * wz[q]);
-        }
-      }
+    for (int s = 1; s < 8; ++s) {
+      mn[s] = fmin(mn[s - 1], nb[s]);
+      mx[s] = fmax(mx[s - 1], nb[s]);
     }
+    // jnp.clip(f, lo, hi) = minimum(hi, maximum(lo, f))
+    const T lo = mn[7], hi = mx[7];
+    const T v1 = fmax(lo, fi);
+    const T a1 = share_max(fi, lo);  // to f
+    const T a2 = share_min(v1, hi);  // to maximum(lo, f)
+    gf = g * a2 * a1;
+    T glo = g * a2 * (T(1) - a1), ghi = g * (T(1) - a2);
+    T gn[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) gn[s] = T(0);
+#pragma unroll
+    for (int s = 7; s >= 1; --s) {
+      const T wl = share_min(mn[s - 1], nb[s]);
+      gn[s] += glo * (T(1) - wl);
+      glo *= wl;
+      const T wh = share_max(mx[s - 1], nb[s]);
+      gn[s] += ghi * (T(1) - wh);
+      ghi *= wh;
+    }
+    gn[0] += glo + ghi;
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+      if (gn[s] != T(0)) atomic_acc(grad + cidx[s], gn[s]);
+    if (gf == T(0)) return;
   }
-  if (tiled) {
-    __syncthreads();
-    for (int q = tid; q < vol; q += nt) {
-      const T v = sacc[q];
-      if (v != T(0)) {
-        const int a = q % b.nx, r = q / b.nx;
-        const int c = r / b.ny, bb = r - c * b.ny;
-        atomic_acc(grad + (b.lx + a) + sx * (b.ly + bb) + plane * (b.lz + c), v);
-      }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const T ga = gf * wx[a];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int row = ix[a] + sx * iy[b];
+      const T gb = ga * wy[b];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) atomic_acc(grad + row + plane * iz[q], gb * wz[q]);
     }
   }
 }

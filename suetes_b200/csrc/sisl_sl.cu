@@ -7,7 +7,6 @@
 //   map_coordinates(order=1, mode='nearest') (steppers.py:362-367);
 // * tricubic: tensor_product_interp_3d (operators.py:146-209).
 #include "sisl_core.cuh"
-#include "sisl_tile.cuh"
 
 namespace sisl {
 namespace {
@@ -135,11 +134,8 @@ __device__ __forceinline__ void cr_weights(T t, T (&w)[4]) {
   w[3] = t * t * (T(-0.5) + T(0.5) * t);
 }
 
-// Catmull-Rom tricubic with the reference's clamped stencil and optional
-// limiter; `fetch(ix, iy, iz)` reads the field (global memory or a staged
-// shared-memory box: the arithmetic, hence the result, is the same).
-template <typename T, typename Fetch>
-__device__ __forceinline__ T tricubic_gen(const Fetch& fetch, const Ext& e, T x, T y, T z, int limiter) {
+template <typename T>
+__device__ __forceinline__ T tricubic_at(const T* __restrict__ f, const Ext& e, T x, T y, T z, int limiter) {
   x = fmin(fmax(x, T(0)), (T)(e.ex - 1));
   y = fmin(fmax(y, T(0)), (T)(e.ey - 1));
   z = fmin(fmax(z, T(0)), (T)(e.ez - 1));
@@ -151,15 +147,17 @@ __device__ __forceinline__ T tricubic_gen(const Fetch& fetch, const Ext& e, T x,
   const int ix[4] = {max(x0 - 1, 0), x0, min(x0 + 1, e.ex - 1), min(x0 + 2, e.ex - 1)};
   const int iy[4] = {max(y0 - 1, 0), y0, min(y0 + 1, e.ey - 1), min(y0 + 2, e.ey - 1)};
   const int iz[4] = {max(z0 - 1, 0), z0, min(z0 + 1, e.ez - 1), min(z0 + 2, e.ez - 1)};
+  const int plane = e.ex * e.ey;
   T out = T(0);
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     T sy = T(0);
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
+      const int row = ix[a] + e.ex * iy[b];
       T sz = T(0);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) sz += wz[q] * fetch(ix[a], iy[b], iz[q]);
+      for (int q = 0; q < 4; ++q) sz += wz[q] * ld(f, row + plane * iz[q]);
       sy += wy[b] * sz;
     }
     out += wx[a] * sy;
@@ -167,32 +165,20 @@ __device__ __forceinline__ T tricubic_gen(const Fetch& fetch, const Ext& e, T x,
   if (limiter) {
     const int x1 = min(x0 + 1, e.ex - 1), y1 = min(y0 + 1, e.ey - 1), z1 = min(z0 + 1, e.ez - 1);
     const int xs[2] = {x0, x1}, ys[2] = {y0, y1}, zs[2] = {z0, z1};
-    T lo = fetch(x0, y0, z0), hi = lo;
+    T lo = ld(f, x0 + e.ex * (y0 + e.ey * z0)), hi = lo;
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
       for (int b = 0; b < 2; ++b)
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-          const T nb = fetch(xs[a], ys[b], zs[q]);
+          const T nb = ld(f, xs[a] + e.ex * (ys[b] + e.ey * zs[q]));
           lo = fmin(lo, nb);
           hi = fmax(hi, nb);
         }
     out = fmin(fmax(out, lo), hi);
   }
   return out;
-}
-
-template <typename T>
-struct GlobalFetch {
-  const T* __restrict__ f;
-  int ex, plane;
-  __device__ __forceinline__ T operator()(int a, int b, int c) const { return ld(f, a + ex * b + plane * c); }
-};
-
-template <typename T>
-__device__ __forceinline__ T tricubic_at(const T* __restrict__ f, const Ext& e, T x, T y, T z, int limiter) {
-  return tricubic_gen(GlobalFetch<T>{f, e.ex, e.ex * e.ey}, e, x, y, z, limiter);
 }
 
 template <typename T>
@@ -211,29 +197,16 @@ __global__ void departure_kernel(Dims d, int loc, T dt, const T* __restrict__ vx
   cz[p] = z;
 }
 
-// Tricubic at given coordinates through a staged halo tile (sisl_tile.cuh).
 template <typename T>
-__global__ void __launch_bounds__(256) tricubic_kernel(Ext src, Ext dst, const T* __restrict__ f,
-                                                       const T* __restrict__ cx, const T* __restrict__ cy,
-                                                       const T* __restrict__ cz, T* out, int limiter, T scale) {
-  __shared__ T sbox[TileCap<T>::n];
-  __shared__ int sb[6];
+__global__ void tricubic_kernel(Ext src, Ext dst, const T* __restrict__ f, const T* __restrict__ cx,
+                                const T* __restrict__ cy, const T* __restrict__ cz, T* out, int limiter,
+                                T scale) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
-  const bool valid = i < dst.ex && j < dst.ey && k < dst.ez;
-  const int p = valid ? i + dst.ex * (j + dst.ey * k) : 0;
-  T x = T(0), y = T(0), z = T(0);
-  if (valid) {
-    x = fmin(fmax(ld(cx, p), T(0)), (T)(src.ex - 1));
-    y = fmin(fmax(ld(cy, p), T(0)), (T)(src.ey - 1));
-    z = fmin(fmax(ld(cz, p), T(0)), (T)(src.ez - 1));
-  }
-  const SlBox b = block_box(sb, valid, (int)floor(x), (int)floor(y), (int)floor(z), src.ex, src.ey, src.ez);
-  const int vol = b.vol();
-  const bool tiled = vol > 0 && vol <= TileCap<T>::n;
-  if (tiled) stage_box(f, src.ex, src.ey, b, sbox);
-  if (valid) out[p] = scale * tricubic_gen(box_or_global(tiled, sbox, b, f, src.ex, src.ey), src, x, y, z, limiter);
+  if (i >= dst.ex || j >= dst.ey || k >= dst.ez) return;
+  const int p = i + dst.ex * (j + dst.ey * k);
+  out[p] = scale * tricubic_at(f, src, ld(cx, p), ld(cy, p), ld(cz, p), limiter);
 }
 
 template <typename T>
@@ -247,43 +220,21 @@ __global__ void trilinear_kernel(Ext src, Ext dst, const T* __restrict__ f, cons
   out[p] = trilinear(f, src, ld(cx, p), ld(cy, p), ld(cz, p));
 }
 
-// Departure point + tricubic of up to 2 fields sharing the stagger; the
-// fields are read through one staged halo tile each (sisl_tile.cuh).
+// Departure point + tricubic of up to 2 fields sharing the stagger.
 template <typename T>
-__global__ void __launch_bounds__(256) sl_advect_kernel(Dims d, int loc, T dt, const T* __restrict__ vx,
-                                                        const T* __restrict__ vy, const T* __restrict__ vz,
-                                                        int iters, int nf, const T* __restrict__ f0,
-                                                        const T* __restrict__ f1, T* o0, T* o1, T s0, T s1,
-                                                        int limiter) {
-  __shared__ T sbox[TileCap<T>::n];
-  __shared__ int sb[6];
+__global__ void sl_advect_kernel(Dims d, int loc, T dt, const T* __restrict__ vx, const T* __restrict__ vy,
+                                 const T* __restrict__ vz, int iters, int nf, const T* __restrict__ f0,
+                                 const T* __restrict__ f1, T* o0, T* o1, T s0, T s1, int limiter) {
   const Ext e = loc_ext(d, loc);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
-  const bool valid = i < e.ex && j < e.ey && k < e.ez;
-  const int p = valid ? i + e.ex * (j + e.ey * k) : 0;
-  T x = T(0), y = T(0), z = T(0);
-  if (valid) {
-    departure_at(e, i, j, k, dt, vx, vy, vz, iters, x, y, z);
-    x = fmin(fmax(x, T(0)), (T)(e.ex - 1));
-    y = fmin(fmax(y, T(0)), (T)(e.ey - 1));
-    z = fmin(fmax(z, T(0)), (T)(e.ez - 1));
-  }
-  const SlBox b = block_box(sb, valid, (int)floor(x), (int)floor(y), (int)floor(z), e.ex, e.ey, e.ez);
-  const int vol = b.vol();
-  const bool tiled = vol > 0 && vol <= TileCap<T>::n;
-#pragma unroll 1
-  for (int q = 0; q < nf; ++q) {
-    const T* __restrict__ f = q == 0 ? f0 : f1;
-    T* o = q == 0 ? o0 : o1;
-    const T sc = q == 0 ? s0 : s1;
-    if (tiled) {
-      if (q > 0) __syncthreads();  // the previous field's gathers are done
-      stage_box(f, e.ex, e.ey, b, sbox);
-    }
-    if (valid) o[p] = sc * tricubic_gen(box_or_global(tiled, sbox, b, f, e.ex, e.ey), e, x, y, z, limiter);
-  }
+  if (i >= e.ex || j >= e.ey || k >= e.ez) return;
+  T x, y, z;
+  departure_at(e, i, j, k, dt, vx, vy, vz, iters, x, y, z);
+  const int p = i + e.ex * (j + e.ey * k);
+  o0[p] = s0 * tricubic_at(f0, e, x, y, z, limiter);
+  if (nf > 1) o1[p] = s1 * tricubic_at(f1, e, x, y, z, limiter);
 }
 
 dim3 box_grid(int ex, int ey, int ez, dim3 blk) {
