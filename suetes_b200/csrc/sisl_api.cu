@@ -1432,7 +1432,7 @@ int sisl_step_graph_destroy(SislStepGraph* g) {
 
 int sisl_core_set_tuning(SislCore* c, const SislTuning* t) {
   if (!c || !t) return SISL_ERR_ARG;
-  if (t->matvec_block < 0 || t->matvec_block >= N_STENCIL_BLOCKS || t->matvec_t_block < 0 ||
+  if (t->matvec_block < 0 || t->matvec_block >= N_MATVEC_SHAPES || t->matvec_t_block < 0 ||
       t->matvec_t_block >= N_STENCIL_BLOCKS || t->precond_tile < 0 || t->precond_tile >= N_COLUMN_TILES ||
       t->precond_t_tile < 0 || t->precond_t_tile >= N_COLUMN_TILES)
     return SISL_ERR_ARG;
@@ -1498,7 +1498,7 @@ int autotune_impl(SislCore* c, void* ws, cudaStream_t st, SislTuning* out) {
     *field = best;
     *us_out = tbest;
   };
-  pick(&d.tune_mv, N_STENCIL_BLOCKS,
+  pick(&d.tune_mv, N_MATVEC_SHAPES,
        [&] { launch_matvec<T>(d, cf, g.cview(g.V(0)), nullptr, none, g.split(g.V(1), g.z()), nullptr, st); },
        &out->us[0]);
   pick(&d.tune_pc, N_COLUMN_TILES,

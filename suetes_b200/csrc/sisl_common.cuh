@@ -20,9 +20,9 @@ struct Dims {
   int px, py;          // periodic flags for x and y
   double dx, dy, dz;
   // launch shapes chosen by the autotuner (sisl_autotune): Helmholtz matvec
-  // and its transpose (block shape), column preconditioner and its transpose
-  // (tile); 0 = the default
-  int tune_mv = 0, tune_pc = 0, tune_mvt = 0, tune_pct = 0;
+  // (block shape; default 4: two levels per thread) and its transpose,
+  // column preconditioner and its transpose (tile)
+  int tune_mv = 4, tune_pc = 0, tune_mvt = 0, tune_pct = 0;
 };
 
 // block shapes of the 3-D stencil kernels (256 threads each)
@@ -35,6 +35,7 @@ __host__ inline dim3 stencil_block(int variant) {
   }
 }
 constexpr int N_STENCIL_BLOCKS = 4;
+constexpr int N_MATVEC_SHAPES = 5;  // the 4 blocks, and 32x8 columns of 2 levels per thread
 // column variants: tiles of (threads, columns) = (256, 32), (128, 16), (256, 64),
 // and the one-thread-per-column march (128 columns per block)
 constexpr int N_COLUMN_TILES = 4;

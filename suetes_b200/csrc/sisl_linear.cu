@@ -39,19 +39,11 @@ __device__ __forceinline__ T gz_mass(const T* __restrict__ p, const T* __restric
 // Branch-free load phase: every index is clamped into its array, all values
 // are loaded unconditionally (one memory round trip per thread), the five
 // rows are formed with selects, and only the stores are predicated.
-// float: 6 resident blocks of 256 (<= 40 registers, no spills) for more
-// loads in flight; double keeps 4 (more would spill)
+// All rows of one point of the union box (the matvec_kernel body).
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) matvec_kernel(Dims d, Coef<T> c, CVec5<T> x,
-                                                                            const double* xscale,
-                                                     CVec5<T> b, Vec5<T> out, const int* active) {
-  if (active && *active == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+__device__ __forceinline__ void matvec_point(const Dims& d, const Coef<T>& c, const CVec5<T>& x, const T xs,
+                                             const CVec5<T>& b, const Vec5<T>& out, int i, int j, int k) {
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  if (i > nx || j > ny || k > nz) return;
-  const T xs = xscale ? (T)(*xscale) : T(1);
   const T adt = (T)(c.s.alpha * c.s.dt), cp = (T)c.s.cp, a = (T)c.s.alpha, ps = (T)c.s.ps;
   const T sp = xs / ps;
   const T idx = (T)(1.0 / d.dx), idy = (T)(1.0 / d.dy);
@@ -152,6 +144,25 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 4) matvec_kernel(Dim
     out.f[4][pw] = b.f[4] ? ld(b.f[4], pw) - Le : Le;
     if (k < nz) out.f[3][pw] = b.f[3] ? ld(b.f[3], pw) - Lp : Lp;
   }
+}
+
+// One thread per point, or LV consecutive levels of a column per thread (the
+// loads the levels share -- pressure at k+-1, the w-level winds, 1/dz_w --
+// are then common subexpressions).  float: 6 resident blocks of 256 (<= 40
+// registers, no spills) for more loads in flight; double keeps 4.
+template <typename T, int LV>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 && LV == 1) ? 6 : 4) matvec_kernel(Dims d, Coef<T> c, CVec5<T> x,
+                                                                            const double* xscale,
+                                                     CVec5<T> b, Vec5<T> out, const int* active) {
+  if (active && *active == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k0 = (blockIdx.z * blockDim.z + threadIdx.z) * LV;
+  if (i > d.nx || j > d.ny) return;
+  const T xs = xscale ? (T)(*xscale) : T(1);
+#pragma unroll
+  for (int l = 0; l < LV; ++l)
+    if (k0 + l <= d.nz) matvec_point(d, c, x, xs, b, out, i, j, k0 + l);
 }
 
 // ---------------------------------------------------------------------------
@@ -306,9 +317,15 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
 template <typename T>
 void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xscale, CVec5<T> b,
                    Vec5<T> out, const int* active, cudaStream_t st) {
+  if (d.tune_mv == 4) {  // two levels per thread
+    const dim3 blk(32, 8, 1);
+    dim3 grd((d.nx + 1 + 31) / 32, (d.ny + 1 + 7) / 8, (d.nz + 2) / 2);
+    matvec_kernel<T, 2><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+    return;
+  }
   const dim3 blk = stencil_block(d.tune_mv);
   dim3 grd((d.nx + 1 + blk.x - 1) / blk.x, (d.ny + 1 + blk.y - 1) / blk.y, (d.nz + 1 + blk.z - 1) / blk.z);
-  matvec_kernel<T><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+  matvec_kernel<T, 1><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
 }
 
 // ---------------------------------------------------------------------------
