@@ -44,7 +44,7 @@ enum { SISL_LOC_M = 0, SISL_LOC_U = 1, SISL_LOC_V = 2, SISL_LOC_W = 3 };
 enum { SISL_GMRES_BATCHED = 0, SISL_GMRES_INCREMENTAL = 1 };
 enum {
   SISL_WS_STEP = 0, SISL_WS_GMRES = 1, SISL_WS_DEPARTURE = 2, SISL_WS_EXPLICIT = 3, SISL_WS_OPERATOR = 4,
-  SISL_WS_FFSL = 5
+  SISL_WS_FFSL = 5, SISL_WS_STEP_VJP = 6, SISL_WS_EXPLICIT_VJP = 7
 };
 enum {
   SISL_RELAX_U = 1, SISL_RELAX_V = 2, SISL_RELAX_W = 4, SISL_RELAX_TH = 8, SISL_RELAX_PI = 16
@@ -266,6 +266,14 @@ int sisl_tendencies(SislCore* core, int is_explicit, const void* const state_pri
  * tend: u, v, w, pi (linear part), th_v, nonlinear pi; phys_diff: u, v, w, th_v. */
 int sisl_explicit_tendencies(SislCore* core, const void* const state_prime[6], void* const tend[6],
                              void* const phys_diff[4], void* ws, size_t ws_bytes, void* stream);
+/* VJP of sisl_explicit_tendencies: state_prime_bar (u, v, w, pi_p, eta_dot,
+ * th_p; written) from the cotangents of tend (6) and phys_diff (4; the
+ * array or any entry NULL: zero), with the reference's stop_gradient on
+ * padded stagger copies (operators.py:37-63).
+ * ws: sisl_workspace_bytes(core, SISL_WS_EXPLICIT_VJP) bytes. */
+int sisl_explicit_tendencies_vjp(SislCore* core, const void* const state_prime[6], const void* const tend_bar[6],
+                                 const void* const phys_diff_bar[4], void* const state_prime_bar[6], void* ws,
+                                 size_t ws_bytes, void* stream);
 /* FluxFormAdvector.advect_3d_split(field, state, bg) (steppers.py:596-647):
  * mass-conserving split transport of a mass-point density by u, v, eta_dot. */
 int sisl_ffsl_advect(SislCore* core, const void* field, const void* u, const void* v, const void* eta_dot, void* out,
@@ -285,6 +293,22 @@ int sisl_step(SislCore* core, const SislState* in, const SislState* out, const S
  * steppers.py:792-850). */
 int sisl_step_taped(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax,
                     void* const solves[10], void* ws, size_t ws_bytes, void* stream, SislStepInfo* info);
+/* Cotangent of one step's input state from the cotangent of its output
+ * (the VJP of SISLStepper3D.step under jax.checkpoint, steppers.py:720-1073,
+ * 792-850, with the reference's stop_gradient on the departure points and
+ * on padded stagger copies).  in, relax: the step's input and bc_fn as given
+ * to sisl_step_taped; solves: that call's ten recorded solutions.
+ * out_bar: cotangents of the output fields, NULL members are zero (the
+ * history members u_prev .. tend_th_prev included).  in_bar: u, v, w,
+ * eta_dot, pi_p, th_p receive the cotangents of the input state; rho and
+ * the history members, where given, are zeroed (no cotangent).  The two
+ * transposed solves follow sisl_core_set_adjoint and report in
+ * info->solve[0..1].  in_bar must not overlap in, solves or out_bar.
+ * ws: sisl_workspace_bytes(core, SISL_WS_STEP_VJP) bytes.  Float32
+ * cotangents use atomic adds and are reproducible to rounding. */
+int sisl_step_vjp(SislCore* core, const SislState* in, void* const solves[10], const SislRelaxation* relax,
+                  const SislState* out_bar, const SislState* in_bar, void* ws, size_t ws_bytes, void* stream,
+                  SislStepInfo* info);
 
 /* CUDA graph of one step of n members (n >= 1; member m advances ins[m]
  * into outs[m] on core m with workspace ws[m]), captured once for these

@@ -15,6 +15,7 @@ SISL_F32, SISL_F64 = 0, 1
 LOC = {"m": 0, "u": 1, "v": 2, "w": 3}
 SISL_GMRES_BATCHED, SISL_GMRES_INCREMENTAL = 0, 1
 WS_STEP, WS_GMRES, WS_DEPARTURE, WS_EXPLICIT, WS_OPERATOR = 0, 1, 2, 3, 4
+WS_STEP_VJP, WS_EXPLICIT_VJP = 6, 7
 RELAX_U, RELAX_V, RELAX_W, RELAX_TH, RELAX_PI = 1, 2, 4, 8, 16
 K_NONE, K_MATVEC, K_PRECOND, K_DOTS, K_UPDATE, K_SL, K_EXPLICIT, K_OTHER = range(8)
 SISL_OK, SISL_NOT_CONVERGED = 0, 1
@@ -129,6 +130,10 @@ PROTOTYPES = {
     "sisl_step_taped": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
                                        ctypes.POINTER(SislRelaxation), vp * 10, vp, ctypes.c_size_t, vp,
                                        ctypes.POINTER(SislStepInfo)]),
+    "sisl_step_vjp": (ctypes.c_int, [vp, ctypes.POINTER(SislState), vp * 10, ctypes.POINTER(SislRelaxation),
+                                     ctypes.POINTER(SislState), ctypes.POINTER(SislState), vp, ctypes.c_size_t, vp,
+                                     ctypes.POINTER(SislStepInfo)]),
+    "sisl_explicit_tendencies_vjp": (ctypes.c_int, [vp, vp * 6, vp * 6, vp, vp * 6, vp, ctypes.c_size_t, vp]),
     "sisl_step_graph_create": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
                                               vp, vp, vp, vp, ctypes.POINTER(vp)]),
     "sisl_step_graph_launch": (ctypes.c_int, [vp, vp]),

@@ -330,6 +330,49 @@ def _taped_step(stepper, ds, relax, record=True):
     return out, rec
 
 
+def step_vjp(stepper, state, recorded, cotangents, relax=None):
+    """Cotangent of one step's input state (``sisl_step_vjp``): the reverse
+    sweep of the fused step in native kernels, the counterpart of
+    ``DifferentiableStep`` under autograd.
+
+    ``state``: the step's input ``DeviceState``; ``recorded``: its ten solve
+    outputs from ``sisl_step_taped``; ``cotangents``: output-field
+    cotangents by ``STATE_KEYS`` name (missing: zero); ``relax``: the
+    ``LateralRelaxation`` of the step.  Returns the cotangents of u, v, w,
+    eta_dot, pi_p and th_p.  The transposed solves follow the solver's
+    ``transpose_tol`` / ``transpose_method`` / ``adjoint_normalize``."""
+    core = state.core
+    solver = stepper.implicit_solver
+    from .steppers import SOLVE_METHODS
+    core.set_adjoint(solver.transpose_tol, solver.adjoint_normalize,
+                     None if solver.transpose_method is None else SOLVE_METHODS[solver.transpose_method])
+    from .steppers import DeviceState
+    locs = dict(DeviceState.FIELDS)
+    ob = _lib.SislState()
+    keep = []
+    for k, g in cotangents.items():
+        if g is None or k not in locs:
+            continue
+        g = core.field(g, locs[k])
+        keep.append(g)
+        setattr(ob, k, g.data_ptr())
+    out = {k: core.new(locs[k]) for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p")}
+    ib = _lib.SislState()
+    for k, t in out.items():
+        setattr(ib, k, t.data_ptr())
+    sin = state.c_struct()
+    rl = relax.c_struct(core) if relax is not None else None
+    ws, n = core.workspace(_lib.WS_STEP_VJP)
+    info = _lib.SislStepInfo()
+    check(core.lib.sisl_step_vjp(core.handle, ctypes.byref(sin), ptrs(recorded[0] + recorded[1], 10),
+                                 ctypes.byref(rl) if rl is not None else None, ctypes.byref(ob), ctypes.byref(ib),
+                                 ws.data_ptr(), n, core.stream, ctypes.byref(info)), "sisl_step_vjp")
+    solver.last_transpose_info = info.solve[1].as_dict()
+    if solver.transpose_log is not None:
+        solver.transpose_log.extend([info.solve[1].as_dict(), info.solve[0].as_dict()])
+    return out
+
+
 def _as_dict(ds):
     d = dict(ds.t)
     d["is_first_step"] = ds.is_first_step
@@ -337,7 +380,7 @@ def _as_dict(ds):
 
 
 def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint_every=1, wrt=("th_p",),
-                   warm_start=False):
+                   warm_start=False, native=True):
     """Value and gradient of ``J = sum_n objective(n, state_n)`` over
     ``num_steps`` SISL steps from ``state0`` (a reference state dict or a
     ``DeviceState``).
@@ -353,7 +396,10 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
     (jax.checkpoint of steppers.py:792-850, driver.py:91-132).  With
     ``warm_start`` each transposed solve starts from the same solve's result
     of the step after (the reference's bwd_solve starts from zero; both
-    converge to the same cotangent within the solver tolerance)."""
+    converge to the same cotangent within the solver tolerance).  With
+    ``native`` (and no warm start) each step's reverse sweep is one
+    ``sisl_step_vjp`` call; otherwise autograd through
+    ``DifferentiableStep``."""
     relax, generic = stepper._relax_of(bc_fn)
     if generic is not None:
         raise NotImplementedError("trajectory_vjp supports LateralRelaxation boundary conditions")
@@ -402,6 +448,9 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
                         if g is not None:
                             g_after[k] = g_after[k] + g if k in g_after else g
             before_ds = states[n - seg0]
+            if native and not warm_start:
+                cot = step_vjp(stepper, before_ds, recs[n - seg0], g_after, relax=relax) if g_after else {}
+                continue
             before = {k: v.detach().requires_grad_(True) for k, v in before_ds.t.items()}
             with torch.enable_grad():
                 out = dstep(dict(before, is_first_step=before_ds.is_first_step), relax=relax,

@@ -13,6 +13,7 @@
 #include "sisl_core.cuh"
 #include "sisl_explicit.cuh"
 #include "sisl_gmres.cuh"
+#include "sisl_step_vjp.cuh"
 
 using namespace sisl;
 
@@ -823,6 +824,240 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
   return e ? e : status;
 }
 
+// ---------------------------------------------------------------------------
+// step VJP: recompute the step's explicit part from the input state and the
+// recorded solutions, then run the reverse sweep
+// ---------------------------------------------------------------------------
+template <typename T>
+struct VWork {
+  T* coords[12];
+  T *th1, *th2;
+  T *x1b[5], *x2b[5], *bb[5];
+  T *rub, *rvb, *rwb, *rpb, *reb, *thab, *tthb, *th1b, *th2b;
+  T *uinb, *vinb, *winb, *pinb, *thinb, *resb;
+  T *hypb[4], *gx4[4], *gy4[4], *tmp4[4];
+  T* divb;
+  char* zero_begin;  // the cotangent arrays that start at zero: [zero_begin, zero_end)
+  char* zero_end;
+};
+
+template <typename T>
+VWork<T> carve_vjp(Carver& cv, const Dims& d) {
+  VWork<T> v;
+  auto F = [&](int loc) { return (T*)cv.take(sizeof(T) * field_size(d, loc)); };
+  static const int L5[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_W};
+  for (int l = 0; l < 4; ++l)
+    for (int q = 0; q < 3; ++q) v.coords[3 * l + q] = F(l);
+  v.th1 = F(LOC_M); v.th2 = F(LOC_M);
+  for (int q = 0; q < 5; ++q) v.bb[q] = F(L5[q]);
+  for (int q = 0; q < 5; ++q) v.x2b[q] = F(L5[q]);
+  for (int q = 0; q < 4; ++q) { v.gx4[q] = F(LOC_U); v.gy4[q] = F(LOC_V); v.tmp4[q] = F(LOC_M); }
+  v.divb = F(LOC_M);
+  v.th2b = F(LOC_M);
+  v.zero_begin = (char*)cv.take(0);
+  for (int q = 0; q < 5; ++q) v.x1b[q] = F(L5[q]);
+  v.rub = F(LOC_U); v.rvb = F(LOC_V); v.rwb = F(LOC_W); v.rpb = F(LOC_M); v.reb = F(LOC_W);
+  v.thab = F(LOC_M); v.th1b = F(LOC_M);
+  v.uinb = F(LOC_U); v.vinb = F(LOC_V); v.winb = F(LOC_W); v.pinb = F(LOC_M); v.thinb = F(LOC_M);
+  v.resb = F(LOC_W);
+  for (int q = 0; q < 4; ++q) v.hypb[q] = F(LOC_M);
+  v.zero_end = (char*)cv.take(0);
+  v.tthb = F(LOC_M);
+  return v;
+}
+
+template <typename T>
+int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const SislRelaxation* relax,
+                  const SislState* ob, const SislState* ib, void* ws, size_t ws_bytes, cudaStream_t st,
+                  SislStepInfo* info) {
+  const Dims& d = c->d;
+  const Coef<T> cf = coef_of<T>(c);
+  Carver cv{(char*)ws};
+  SWork<T> w = carve_step<T>(cv, d, c->prm.solver_restart, refining<T>(c));
+  VWork<T> v = carve_vjp<T>(cv, d);
+  if (cv.off > ws_bytes) return SISL_ERR_WORKSPACE;
+  const int64_t l0 = g_launches.load();
+  const T* u = (const T*)in->u;
+  const T* vv = (const T*)in->v;
+  const T* wv = (const T*)in->w;
+  const T* eta = (const T*)in->eta_dot;
+  const T* pp = (const T*)in->pi_p;
+  const T* th = (const T*)in->th_p;
+  const T* x1[5];
+  const T* x2[5];
+  for (int q = 0; q < 5; ++q) { x1[q] = (const T*)tape[q]; x2[q] = (const T*)tape[5 + q]; }
+  const double a = c->s.alpha, dt = c->s.dt;
+  auto bytes = [&](int loc) { return sizeof(T) * field_size(d, loc); };
+  // cotangents of the input state: the history passes straight through
+  // (u_prev' = u, ...), everything else accumulates on top
+  T* ub = (T*)ib->u;
+  T* vb = (T*)ib->v;
+  T* wb = (T*)ib->w;
+  T* eb = (T*)ib->eta_dot;
+  T* pb = (T*)ib->pi_p;
+  T* hb = (T*)ib->th_p;
+  auto init = [&](T* dst, const void* src, int loc) -> bool {
+    if (src) return cudaMemcpyAsync(dst, src, bytes(loc), cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+    return cudaMemsetAsync(dst, 0, bytes(loc), st) == cudaSuccess;
+  };
+  if (!init(ub, ob->u_prev, LOC_U) || !init(vb, ob->v_prev, LOC_V) || !init(wb, ob->w_prev, LOC_W) ||
+      !init(eb, ob->eta_dot_prev, LOC_W) || !init(pb, nullptr, LOC_M) || !init(hb, nullptr, LOC_M) ||
+      !init(v.tthb, ob->tend_th_prev, LOC_M))
+    return SISL_ERR_CUDA;
+  void* dead[6] = {ib->rho, ib->u_prev, ib->v_prev, ib->w_prev, ib->eta_dot_prev, ib->tend_th_prev};
+  const int dead_loc[6] = {LOC_M, LOC_U, LOC_V, LOC_W, LOC_W, LOC_M};
+  for (int q = 0; q < 6; ++q)  // no cotangent: the departure points are stop_gradient, rho is rebuilt by the EOS
+    if (dead[q] && cudaMemsetAsync(dead[q], 0, bytes(dead_loc[q]), st) != cudaSuccess) return SISL_ERR_CUDA;
+  if (cudaMemsetAsync(v.zero_begin, 0, (size_t)(v.zero_end - v.zero_begin), st) != cudaSuccess)
+    return SISL_ERR_CUDA;
+
+  // ---- recompute: trajectory velocities, departure points, explicit part,
+  // advection and the theta' predictors (bitwise the forward step's kernels)
+  {
+    PtrTable<T> vt{};
+    for (int q = 0; q < 12; ++q) vt.p[q] = w.vel[q];
+    const int extrap = (in->is_first_step == 1.0) ? 0 : 1;
+    KScope k(c, SISL_K_SL, st);
+    launch_traj_velocity<T>(d, cf, u, vv, eta, (const T*)in->u_prev, (const T*)in->v_prev,
+                            (const T*)in->eta_dot_prev, extrap, vt, st);
+  }
+  const int iters = c->prm.departure_iterations;
+  const int lim = c->prm.use_limiter;
+  {
+    KScope k(c, SISL_K_SL, st, 4);
+    for (int l = 0; l < 4; ++l) launch_departure<T>(d, l, dt, w.vel + 3 * l, iters, v.coords + 3 * l, st);
+  }
+  ExplicitIn<T> ein{u, vv, wv, eta, pp, th, {nullptr, nullptr, nullptr, nullptr}};
+  const bool hyp = c->s.nu_h > 0.0;
+  if (hyp) {
+    PtrTable<T> t4{}, o4{};
+    for (int q = 0; q < 4; ++q) { t4.p[q] = w.htmp[q]; o4.p[q] = w.hyp[q]; }
+    KScope k(c, SISL_K_EXPLICIT, st, 3);
+    launch_hyper<T>(d, cf, u, vv, wv, th, t4, o4, st);
+    for (int q = 0; q < 4; ++q) ein.hyper[q] = w.hyp[q];
+  }
+  {
+    ExplicitOut<T> eo{};
+    eo.f[0] = w.u_in; eo.f[1] = w.v_in; eo.f[2] = w.w_in; eo.f[3] = w.pi_in; eo.f[4] = w.th_in;
+    eo.f[5] = w.tth; eo.f[6] = w.res;
+    KScope k(c, SISL_K_EXPLICIT, st);
+    launch_explicit<T>(d, cf, ein, eo, 0, st);
+  }
+  {  // ru, rv (guess winds of the first corrector) and th_adv are read back
+    const T* fu[1] = {w.u_in};
+    T* ou[1] = {w.ru};
+    const T* fv[1] = {w.v_in};
+    T* ov[1] = {w.rv};
+    const T* fm[1] = {w.th_in};
+    T* om[1] = {w.tha};
+    const T one[1] = {T(1)};
+    KScope k(c, SISL_K_SL, st, 4);
+    launch_sl_advect<T>(d, LOC_U, dt, w.vel + 3, iters, 1, fu, ou, one, lim, st);
+    launch_sl_advect<T>(d, LOC_V, dt, w.vel + 6, iters, 1, fv, ov, one, lim, st);
+    launch_sl_advect<T>(d, LOC_M, dt, w.vel + 0, iters, 1, fm, om, one, lim, st);
+    const int na = (d.nx > d.ny ? d.nx : d.ny) + 1;
+    sl_fixup_kernel<T><<<dim3((na + 127) / 128, d.nz), 128, 0, st>>>(d, w.ru, w.rv, u, vv, w.reta);
+  }
+  {
+    KScope k(c, SISL_K_EXPLICIT, st, 2);
+    launch_corrector_theta<T>(d, cf, w.tha, w.tth, wv, wv, v.th1, st);
+    launch_corrector_theta<T>(d, cf, w.tha, w.tth, wv, x1[2], v.th2, st);
+  }
+
+  // ---- reverse sweep
+  {  // divergence damping, relaxation and EOS (steppers.py:1022-1056)
+    FinalizeBar<T> fb{};
+    fb.th2 = v.th2; fb.pi2 = x2[3];
+    fb.u = (const T*)ob->u; fb.v = (const T*)ob->v; fb.w = (const T*)ob->w; fb.eta = (const T*)ob->eta_dot;
+    fb.pi = (const T*)ob->pi_p; fb.th = (const T*)ob->th_p; fb.rho = (const T*)ob->rho;
+    fb.x2u = v.x2b[0]; fb.x2v = v.x2b[1]; fb.x2w = v.x2b[2]; fb.x2pi = v.x2b[3]; fb.x2eta = v.x2b[4];
+    fb.th2b = v.th2b;
+    fb.relax.on = 0;
+    if (relax) {
+      fb.relax.on = relax->fields;
+      fb.relax.mask_m = (const T*)relax->mask_m;
+      fb.relax.mask_u = (const T*)relax->mask_u;
+      fb.relax.mask_v = (const T*)relax->mask_v;
+      for (int q = 0; q < 5; ++q) {
+        fb.relax.ext[q] = (T)relax->ext[q];
+        fb.relax.ext_field[q] = (const T*)relax->ext_field[q];
+      }
+    }
+    KScope k(c, SISL_K_OTHER, st, c->s.nu_div != 0.0 ? 3 : 1);
+    launch_finalize_vjp<T>(d, cf, fb, v.divb, st);
+  }
+  int status = SISL_OK;
+  for (int it = 1; it >= 0; --it) {
+    // b_bar = A^-T x_bar (custom_linear_solve transpose, steppers.py:473-485)
+    CVec5<T> xb;
+    Vec5<T> bo;
+    for (int q = 0; q < 5; ++q) { xb.f[q] = it ? v.x2b[q] : v.x1b[q]; bo.f[q] = v.bb[q]; }
+    SislSolveInfo si{};
+    int rc = solve_transpose_physical<T>(c, cf, w.g, xb, nullptr, bo, st, &si);
+    if (info) info->solve[it] = si;
+    if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+    if (rc != SISL_OK && status == SISL_OK) status = rc;
+    CorrectorIn<T> ci;
+    ci.rhs_u = w.ru; ci.rhs_v = w.rv; ci.rhs_w = nullptr; ci.rhs_pi = nullptr;
+    ci.th_next = it ? v.th2 : v.th1;
+    ci.pg = it ? x1[3] : pp;
+    ci.gu = it ? x1[0] : u;
+    ci.gv = it ? x1[1] : vv;
+    ci.geta = it ? x1[4] : eta;
+    ci.ug = it ? x1[0] : w.ru;
+    ci.vg = it ? x1[1] : w.rv;
+    CorrectorBar<T> cb;
+    for (int q = 0; q < 5; ++q) cb.b[q] = v.bb[q];
+    cb.rhs_u = v.rub; cb.rhs_v = v.rvb; cb.rhs_w = v.rwb; cb.rhs_pi = v.rpb; cb.reta = v.reb;
+    cb.th = it ? v.th2b : v.th1b;
+    cb.pg = it ? v.x1b[3] : pb;
+    cb.gu = it ? v.x1b[0] : ub;
+    cb.gv = it ? v.x1b[1] : vb;
+    cb.geta = it ? v.x1b[4] : eb;
+    cb.ug = it ? v.x1b[0] : v.rub;
+    cb.vg = it ? v.x1b[1] : v.rvb;
+    KScope k(c, SISL_K_EXPLICIT, st, 2);
+    launch_corrector_vjp<T>(d, cf, ci, cb, st);
+    // theta' predictor; the first predictor's w terms cancel (w_next = w)
+    launch_corrector_theta_vjp<T>(d, cf, it ? v.th2b : v.th1b, v.thab, v.tthb, it ? wb : nullptr,
+                                  it ? v.x1b[2] : nullptr, st);
+  }
+  {  // lateral overrides, then the six departure-point interpolations
+    KScope k(c, SISL_K_SL, st, 7);
+    launch_fixup_vjp<T>(d, v.rub, v.rvb, ub, vb, v.reb, st);
+    const T* cu[3] = {v.coords[3], v.coords[4], v.coords[5]};
+    const T* cvv[3] = {v.coords[6], v.coords[7], v.coords[8]};
+    const T* cwv[3] = {v.coords[9], v.coords[10], v.coords[11]};
+    const T* cm[3] = {v.coords[0], v.coords[1], v.coords[2]};
+    const int ux = d.nx + 1, vy = d.ny + 1, wz = d.nz + 1;
+    launch_tricubic_vjp<T>(ux, d.ny, d.nz, ux, d.ny, d.nz, w.u_in, cu, v.rub, v.uinb, lim, T(1), st);
+    launch_tricubic_vjp<T>(d.nx, vy, d.nz, d.nx, vy, d.nz, w.v_in, cvv, v.rvb, v.vinb, lim, T(1), st);
+    launch_tricubic_vjp<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.w_in, cwv, v.rwb, v.winb, lim, T(1), st);
+    launch_tricubic_vjp<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.res, cwv, v.reb, v.resb, lim, (T)(-(1.0 - a)), st);
+    launch_tricubic_vjp<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.pi_in, cm, v.rpb, v.pinb, lim, T(1), st);
+    launch_tricubic_vjp<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.th_in, cm, v.thab, v.thinb, lim, T(1), st);
+  }
+  {  // explicit tendencies with hyperdiffusion (euler.py:208-372, diffusion.py:93-173)
+    ExplicitBar<T> bi{};
+    bi.f[0] = v.uinb; bi.f[1] = v.vinb; bi.f[2] = v.winb; bi.f[3] = v.pinb; bi.f[4] = v.thinb;
+    bi.f[5] = v.tthb; bi.f[6] = v.resb;
+    StateBar<T> so{ub, vb, wb, eb, pb, hb, {nullptr, nullptr, nullptr, nullptr}};
+    if (hyp)
+      for (int q = 0; q < 4; ++q) so.hyper[q] = v.hypb[q];
+    KScope k(c, SISL_K_EXPLICIT, st);
+    launch_explicit_vjp<T>(d, cf, ein, bi, so, 0, st);
+  }
+  if (hyp) {
+    PtrTable<T> h4{}, gx{}, gy{}, t4{};
+    for (int q = 0; q < 4; ++q) { h4.p[q] = v.hypb[q]; gx.p[q] = v.gx4[q]; gy.p[q] = v.gy4[q]; t4.p[q] = v.tmp4[q]; }
+    KScope k(c, SISL_K_EXPLICIT, st, 5);
+    launch_hyper_vjp<T>(d, cf, h4, gx, gy, t4, ub, vb, wb, hb, st);
+  }
+  if (info) info->kernel_launches = g_launches.load() - l0;
+  int e = check_cuda();
+  return e ? e : status;
+}
+
 bool valid_grid(const SislGrid* g) {
   return g && g->nx >= 2 && g->ny >= 2 && g->nz >= 2 && (g->dtype == SISL_F32 || g->dtype == SISL_F64) &&
          g->dx > 0 && g->dy > 0 && g->dz > 0 && (int64_t)(g->nx + 1) * (g->ny + 1) * (g->nz + 1) < (1LL << 31);
@@ -969,6 +1204,20 @@ size_t sisl_workspace_bytes(const SislCore* c, int what) {
       cv.take(es * field_size(c->d, LOC_M));
       cv.take(sizeof(double) * ffsl_scratch_doubles(c->d));
       break;
+    case SISL_WS_STEP_VJP:
+      if (f64) {
+        carve_step<double>(cv, c->d, c->prm.solver_restart, false);
+        carve_vjp<double>(cv, c->d);
+      } else {
+        carve_step<float>(cv, c->d, c->prm.solver_restart, refining<float>(c));
+        carve_vjp<float>(cv, c->d);
+      }
+      break;
+    case SISL_WS_EXPLICIT_VJP:
+      for (int q = 0; q < 8; ++q) cv.take(es * field_size(c->d, LOC_M));
+      for (int q = 0; q < 4; ++q) cv.take(es * field_size(c->d, LOC_U));
+      for (int q = 0; q < 4; ++q) cv.take(es * field_size(c->d, LOC_V));
+      break;
     default: return 0;
   }
   return align256(cv.off);
@@ -1112,9 +1361,8 @@ int sisl_departure(SislCore* c, int loc, const void* u, const void* v, const voi
   auto run = [&](auto tag) {
     using T = decltype(tag);
     const Coef<T> cf = coef_of<T>(c);
-    PtrTable<T> vt{};
-    for (int l = 0; l < 4; ++l)
-      for (int q = 0; q < 3; ++q) vt.p[3 * l + q] = (T*)cv.take(sizeof(T) * field_size(c->d, l));
+    PtrTable<T> vt{};  // only the requested stagger's index velocities
+    for (int q = 0; q < 3; ++q) vt.p[3 * loc + q] = (T*)cv.take(sizeof(T) * field_size(c->d, loc));
     {
       KScope k(c, SISL_K_SL, st);
       launch_traj_velocity<T>(c->d, cf, (const T*)u, (const T*)v, (const T*)eta, nullptr, nullptr, nullptr, 0, vt,
@@ -1295,6 +1543,79 @@ int sisl_step_taped(SislCore* c, const SislState* in, const SislState* out, cons
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64) return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info, solves);
   return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info, solves);
+}
+
+int sisl_step_vjp(SislCore* c, const SislState* in, void* const solves[10], const SislRelaxation* relax,
+                  const SislState* out_bar, const SislState* in_bar, void* ws, size_t ws_bytes, void* stream,
+                  SislStepInfo* info) {
+  if (!c || !in || !solves || !out_bar || !in_bar) return SISL_ERR_ARG;
+  const void* need_in[] = {in->u, in->v, in->w, in->eta_dot, in->pi_p, in->th_p};
+  for (const void* p : need_in)
+    if (!p) return SISL_ERR_ARG;
+  if (in->is_first_step != 1.0 && (!in->u_prev || !in->v_prev || !in->eta_dot_prev)) return SISL_ERR_ARG;
+  for (int q = 0; q < 10; ++q)
+    if (!solves[q]) return SISL_ERR_ARG;
+  const void* need_bar[] = {in_bar->u, in_bar->v, in_bar->w, in_bar->eta_dot, in_bar->pi_p, in_bar->th_p};
+  for (const void* p : need_bar)
+    if (!p) return SISL_ERR_ARG;
+  if (relax && (((relax->fields & (SISL_RELAX_W | SISL_RELAX_TH | SISL_RELAX_PI)) && !relax->mask_m) ||
+                ((relax->fields & SISL_RELAX_U) && !relax->mask_u) ||
+                ((relax->fields & SISL_RELAX_V) && !relax->mask_v)))
+    return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_STEP_VJP)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (c->grid.dtype == SISL_F64)
+    return step_vjp_impl<double>(c, in, solves, relax, out_bar, in_bar, ws, ws_bytes, st, info);
+  return step_vjp_impl<float>(c, in, solves, relax, out_bar, in_bar, ws, ws_bytes, st, info);
+}
+
+int sisl_explicit_tendencies_vjp(SislCore* c, const void* const sp[6], const void* const tend_bar[6],
+                                 const void* const pd_bar[4], void* const sp_bar[6], void* ws, size_t ws_bytes,
+                                 void* stream) {
+  if (!c || !sp || !tend_bar || !sp_bar) return SISL_ERR_ARG;
+  for (int q = 0; q < 6; ++q)
+    if (!sp[q] || !sp_bar[q]) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_EXPLICIT_VJP)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  static const int LOCS[6] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_W, LOC_M};
+  Carver cv{(char*)ws};
+  auto run = [&](auto tag) -> int {
+    using T = decltype(tag);
+    const Dims& d = c->d;
+    const Coef<T> cf = coef_of<T>(c);
+    for (int q = 0; q < 6; ++q)
+      if (cudaMemsetAsync(sp_bar[q], 0, sizeof(T) * field_size(d, LOCS[q]), st) != cudaSuccess) return SISL_ERR_CUDA;
+    PtrTable<T> h4{}, gx{}, gy{}, t4{};
+    for (int q = 0; q < 4; ++q) h4.p[q] = (T*)cv.take(sizeof(T) * field_size(d, LOC_M));
+    for (int q = 0; q < 4; ++q) t4.p[q] = (T*)cv.take(sizeof(T) * field_size(d, LOC_M));
+    for (int q = 0; q < 4; ++q) gx.p[q] = (T*)cv.take(sizeof(T) * field_size(d, LOC_U));
+    for (int q = 0; q < 4; ++q) gy.p[q] = (T*)cv.take(sizeof(T) * field_size(d, LOC_V));
+    const bool hyp = c->s.nu_h > 0.0;
+    if (hyp)
+      for (int q = 0; q < 4; ++q)
+        if (cudaMemsetAsync(h4.p[q], 0, sizeof(T) * field_size(d, LOC_M), st) != cudaSuccess) return SISL_ERR_CUDA;
+    ExplicitIn<T> ein{(const T*)sp[0], (const T*)sp[1], (const T*)sp[2], (const T*)sp[4], (const T*)sp[3],
+                      (const T*)sp[5], {nullptr, nullptr, nullptr, nullptr}};
+    ExplicitBar<T> bi{};
+    for (int q = 0; q < 6; ++q) bi.f[q] = (const T*)tend_bar[q];
+    for (int q = 0; q < 4; ++q) bi.pd[q] = pd_bar ? (const T*)pd_bar[q] : nullptr;
+    StateBar<T> so{(T*)sp_bar[0], (T*)sp_bar[1], (T*)sp_bar[2], (T*)sp_bar[4], (T*)sp_bar[3], (T*)sp_bar[5],
+                   {nullptr, nullptr, nullptr, nullptr}};
+    if (hyp)
+      for (int q = 0; q < 4; ++q) so.hyper[q] = h4.p[q];
+    {
+      KScope k(c, SISL_K_EXPLICIT, st);
+      launch_explicit_vjp<T>(d, cf, ein, bi, so, 1, st);
+    }
+    if (hyp) {
+      KScope k(c, SISL_K_EXPLICIT, st, 5);
+      launch_hyper_vjp<T>(d, cf, h4, gx, gy, t4, so.u, so.v, so.w, so.th, st);
+    }
+    return SISL_OK;
+  };
+  const int rc = (c->grid.dtype == SISL_F64) ? run(double{}) : run(float{});
+  if (rc) return rc;
+  return check_cuda();
 }
 
 }  // extern "C"

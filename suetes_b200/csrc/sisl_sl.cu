@@ -49,14 +49,15 @@ __global__ void traj_velocity_kernel(Dims d, Coef<T> c, const T* __restrict__ u,
   auto Vm = [&](int a, int b, int cc) { return T(0.5) * (V(a, b, cc) + V(a, b + 1, cc)); };
   auto Em = [&](int a, int b, int cc) { return T(0.5) * (E(a, b, cc) + E(a, b, cc + 1)); };
 
-  if (i < nx && j < ny && k < nz) {  // m
+  // a null first pointer skips a stagger
+  if (vel.p[0] && i < nx && j < ny && k < nz) {  // m
     const int p = im(d, i, j, k);
     const T m = ld(c.mm, h_m(d, i, j));
     vel.p[0][p] = Um(i, j, k) * m * idx;
     vel.p[1][p] = Vm(i, j, k) * m * idy;
     vel.p[2][p] = Em(i, j, k);
   }
-  if (j < ny && k < nz) {  // u
+  if (vel.p[3] && j < ny && k < nz) {  // u
     int l, r;
     face_pair(i, nx, d.px, l, r);
     const int p = iu(d, i, j, k);
@@ -65,7 +66,7 @@ __global__ void traj_velocity_kernel(Dims d, Coef<T> c, const T* __restrict__ u,
     vel.p[4][p] = T(0.5) * (Vm(l, j, k) + Vm(r, j, k)) * m * idy;
     vel.p[5][p] = T(0.5) * (Em(l, j, k) + Em(r, j, k));
   }
-  if (i < nx && k < nz) {  // v
+  if (vel.p[6] && i < nx && k < nz) {  // v
     int l, r;
     face_pair(j, ny, d.py, l, r);
     const int p = iv(d, i, j, k);
@@ -74,7 +75,7 @@ __global__ void traj_velocity_kernel(Dims d, Coef<T> c, const T* __restrict__ u,
     vel.p[7][p] = V(i, j, k) * m * idy;
     vel.p[8][p] = T(0.5) * (Em(i, l, k) + Em(i, r, k));
   }
-  if (i < nx && j < ny) {  // w
+  if (vel.p[9] && i < nx && j < ny) {  // w
     int kl, kr;
     level_pair(k, nz, kl, kr);
     const int p = iw(d, i, j, k);

@@ -152,6 +152,39 @@ class Euler3D:
               "sisl_tendencies")
         return outs, pd
 
+    def explicit_tendencies_vjp(self, state_prime, th_prime, bg, tend_bar, phys_diff_bar=None):
+        """VJP of the explicit tendencies (``sisl_explicit_tendencies_vjp``).
+
+        ``tend_bar``: cotangents of the tendencies by name (``u``, ``v``,
+        ``w``, ``pi`` (linear part), ``th_v``, ``nl_pi`` (nonlinear Exner
+        tendency)); ``phys_diff_bar``: of the hyperdiffusion parts (``u``,
+        ``v``, ``w``, ``th_v``); missing entries are zero.  Returns the
+        cotangents of ``u``, ``v``, ``w``, ``pi``, ``eta_dot`` and ``th_p``
+        (the theta perturbation)."""
+        dtype = self._dtype_of(state_prime)
+        core = self.core(dtype, self.dt, 0.55, bg=self._bg_arg(bg))
+        locs = (("u", "u"), ("v", "v"), ("w", "w"), ("pi", "m"), ("eta_dot", "w"))
+        ins = [core.field(state_prime[k], l) for k, l in locs] + [core.field(th_prime, "m")]
+        tl = (("u", "u"), ("v", "v"), ("w", "w"), ("pi", "m"), ("th_v", "m"), ("nl_pi", "m"))
+        keep = []
+
+        def arr(d, names, n):
+            a = (ctypes.c_void_p * n)()
+            for q, (k, l) in enumerate(names):
+                if d is not None and d.get(k) is not None:
+                    t = core.field(d[k], l)
+                    keep.append(t)
+                    a[q] = t.data_ptr()
+            return a
+        tb = arr(tend_bar, tl, 6)
+        pb = arr(phys_diff_bar, (("u", "u"), ("v", "v"), ("w", "w"), ("th_v", "m")), 4)
+        outs = [core.new(l) for _, l in locs] + [core.new("m")]
+        ws, n = core.workspace(_lib.WS_EXPLICIT_VJP)
+        check(core.lib.sisl_explicit_tendencies_vjp(core.handle, ptrs(ins, 6), tb, ctypes.cast(pb, ctypes.c_void_p),
+                                                    ptrs(outs, 6), ws.data_ptr(), n, core.stream),
+              "sisl_explicit_tendencies_vjp")
+        return dict(zip(("u", "v", "w", "pi", "eta_dot", "th_p"), outs))
+
     def get_tendencies(self, state_prime, bg, is_explicit=False, ml_params=None):
         """Tendencies of euler.py:208-372.  The theta perturbation is taken
         from ``state_prime['th_v'] - bg['th_v']`` (or ``th_v_prime_m``); its

@@ -265,9 +265,10 @@ def _relax_pair(og, pg, width=1000.0, u_ext=3.0):
     return make_bc, rl
 
 
+@pytest.mark.parametrize("native", [True, False])
 @pytest.mark.parametrize("relaxed", [False, True])
 @pytest.mark.parametrize("limiter", [False, True])
-def test_step_vjp_matches_oracle(limiter, relaxed):
+def test_step_vjp_matches_oracle(limiter, relaxed, native):
     from oracle.steppers import SISLStepper3D as OSt
     from suetes_b200 import SISLStepper3D as PSt
     from suetes_b200.adjoint import trajectory_vjp
@@ -300,7 +301,7 @@ def test_step_vjp_matches_oracle(limiter, relaxed):
 
     for ck in (1, 2):
         Jp, g = trajectory_vjp(ps_, to_cuda(s0), nsteps, objective, bc_fn=rl if relaxed else None,
-                               checkpoint_every=ck, wrt=("u", "v", "w", "eta_dot", "pi_p", "th_p"))
+                               checkpoint_every=ck, wrt=("u", "v", "w", "eta_dot", "pi_p", "th_p"), native=native)
         assert abs(float(Jp) - float(J.detach())) <= 1e-8 * abs(float(J.detach())), (float(Jp), float(J.detach()))
         for ko, kp in (("u", "u"), ("v", "v"), ("w", "w"), ("eta_dot", "eta_dot"), ("pi", "pi_p"),
                        ("th_v", "th_p")):
