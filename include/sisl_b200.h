@@ -44,7 +44,7 @@ enum { SISL_LOC_M = 0, SISL_LOC_U = 1, SISL_LOC_V = 2, SISL_LOC_W = 3 };
 enum { SISL_GMRES_BATCHED = 0, SISL_GMRES_INCREMENTAL = 1 };
 enum {
   SISL_WS_STEP = 0, SISL_WS_GMRES = 1, SISL_WS_DEPARTURE = 2, SISL_WS_EXPLICIT = 3, SISL_WS_OPERATOR = 4,
-  SISL_WS_FFSL = 5, SISL_WS_STEP_VJP = 6, SISL_WS_EXPLICIT_VJP = 7
+  SISL_WS_FFSL = 5, SISL_WS_STEP_VJP = 6, SISL_WS_EXPLICIT_VJP = 7, SISL_WS_FFSL_VJP = 8
 };
 enum {
   SISL_RELAX_U = 1, SISL_RELAX_V = 2, SISL_RELAX_W = 4, SISL_RELAX_TH = 8, SISL_RELAX_PI = 16
@@ -238,6 +238,13 @@ int sisl_trilinear(int dtype, const int32_t src_shape[3], const void* field, con
  * and cfl (nlines, n + 1), line-major; float64 workspace of
  * sisl_ffsl_lines_workspace_bytes(n, nlines) bytes. */
 size_t sisl_ffsl_lines_workspace_bytes(int n, int nlines);
+/* VJP of sisl_ffsl_lines: scalar_bar (n per line) and, where non-NULL,
+ * cfl_bar (n + 1 per line), written, from out_bar, in the layouts of
+ * sisl_ffsl_lines; float64 scratch of sisl_ffsl_lines_vjp_workspace_bytes. */
+size_t sisl_ffsl_lines_vjp_workspace_bytes(int n, int nlines);
+int sisl_ffsl_lines_vjp(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic,
+                        const void* out_bar, void* scalar_bar, void* cfl_bar, void* ws, size_t ws_bytes,
+                        void* stream);
 int sisl_ffsl_lines(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic, void* out,
                     void* ws, size_t ws_bytes, void* stream);
 /* Allocation-free sisl_ffsl_lines; no counterpart in the reference.
@@ -278,6 +285,14 @@ int sisl_explicit_tendencies_vjp(SislCore* core, const void* const state_prime[6
  * mass-conserving split transport of a mass-point density by u, v, eta_dot. */
 int sisl_ffsl_advect(SislCore* core, const void* field, const void* u, const void* v, const void* eta_dot, void* out,
                      void* ws, size_t ws_bytes, void* stream);
+/* VJP of sisl_ffsl_advect (XLA's reverse of steppers.py:552-647):
+ * field_bar and, where non-NULL, u_bar, v_bar, eta_dot_bar (written) from
+ * out_bar.  The clipped departure interfaces pass half the cotangent at an
+ * exact tie (jnp.clip is maximum then minimum) and none beyond it.
+ * ws: sisl_workspace_bytes(core, SISL_WS_FFSL_VJP) bytes. */
+int sisl_ffsl_advect_vjp(SislCore* core, const void* field, const void* u, const void* v, const void* eta_dot,
+                         const void* out_bar, void* field_bar, void* u_bar, void* v_bar, void* eta_dot_bar, void* ws,
+                         size_t ws_bytes, void* stream);
 /* Equation of state rho = p0 / (Rd th_v) pi^(cvd/Rd) (steppers.py:1055-1056)
  * from perturbation th_p, pi_p. */
 int sisl_eos(SislCore* core, const void* th_p, const void* pi_p, void* rho, void* stream);

@@ -256,7 +256,11 @@ class FluxFormAdvector:
         else:
             M = torch.nn.functional.pad(torch.cumsum(s, dim=-1), (1, 0))
             idx = torch.arange(N + 1, dtype=s.dtype)
-            dep = torch.clamp(idx - cfl, 0.0, float(N))
+            # jnp.clip is maximum then minimum: at an exact tie each passes half
+            # the cotangent (torch.clamp would pass all of it)
+            lo_b = torch.zeros((), dtype=s.dtype)
+            hi_b = torch.full((), float(N), dtype=s.dtype)
+            dep = torch.minimum(torch.maximum(idx - cfl, lo_b), hi_b)
         L = M.shape[-1]
         lo = torch.floor(dep)
         w = dep - lo

@@ -15,7 +15,7 @@ SISL_F32, SISL_F64 = 0, 1
 LOC = {"m": 0, "u": 1, "v": 2, "w": 3}
 SISL_GMRES_BATCHED, SISL_GMRES_INCREMENTAL = 0, 1
 WS_STEP, WS_GMRES, WS_DEPARTURE, WS_EXPLICIT, WS_OPERATOR = 0, 1, 2, 3, 4
-WS_STEP_VJP, WS_EXPLICIT_VJP = 6, 7
+WS_STEP_VJP, WS_EXPLICIT_VJP, WS_FFSL_VJP = 6, 7, 8
 RELAX_U, RELAX_V, RELAX_W, RELAX_TH, RELAX_PI = 1, 2, 4, 8, 16
 K_NONE, K_MATVEC, K_PRECOND, K_DOTS, K_UPDATE, K_SL, K_EXPLICIT, K_OTHER = range(8)
 SISL_OK, SISL_NOT_CONVERGED = 0, 1
@@ -123,6 +123,10 @@ PROTOTYPES = {
     "sisl_ffsl_lines_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int,
                                                vp, vp]),
     "sisl_ffsl_advect": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
+    "sisl_ffsl_advect_vjp": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
+    "sisl_ffsl_lines_vjp_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
+    "sisl_ffsl_lines_vjp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp,
+                                           vp, vp, ctypes.c_size_t, vp]),
     "sisl_eos": (ctypes.c_int, [vp, vp, vp, vp, vp]),
     "sisl_step": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
                                  ctypes.POINTER(SislRelaxation), vp, ctypes.c_size_t, vp,

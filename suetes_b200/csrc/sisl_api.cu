@@ -1213,6 +1213,11 @@ size_t sisl_workspace_bytes(const SislCore* c, int what) {
         carve_vjp<float>(cv, c->d);
       }
       break;
+    case SISL_WS_FFSL_VJP:
+      for (int q = 0; q < 5; ++q) cv.take(es * field_size(c->d, LOC_M));
+      cv.take(sizeof(double) * ffsl_scratch_doubles(c->d));
+      cv.take(sizeof(double) * ffsl_scratch_doubles(c->d));
+      break;
     case SISL_WS_EXPLICIT_VJP:
       for (int q = 0; q < 8; ++q) cv.take(es * field_size(c->d, LOC_M));
       for (int q = 0; q < 4; ++q) cv.take(es * field_size(c->d, LOC_U));
@@ -1484,6 +1489,31 @@ int sisl_ffsl_lines(int dtype, int n, int nlines, const void* scalar, const void
   else if (dtype == SISL_F32)
     launch_ffsl_lines<float>(n, nlines, (const float*)scalar, (const float*)cfl, (float*)out, (double*)ws,
                              periodic ? 1 : 0, st);
+  else
+    return SISL_ERR_ARG;
+  return check_cuda();
+}
+
+size_t sisl_ffsl_lines_vjp_workspace_bytes(int n, int nlines) {
+  if (n < 1 || nlines < 1) return 0;
+  return 2 * align256(sizeof(double) * (size_t)(n + 1) * nlines);
+}
+
+int sisl_ffsl_lines_vjp(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic,
+                        const void* out_bar, void* scalar_bar, void* cfl_bar, void* ws, size_t ws_bytes,
+                        void* stream) {
+  if (n < 1 || nlines < 1 || !scalar || !cfl || !out_bar || !scalar_bar) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_ffsl_lines_vjp_workspace_bytes(n, nlines)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  double* M = (double*)ws;
+  double* Mb = (double*)((char*)ws + align256(sizeof(double) * (size_t)(n + 1) * nlines));
+  KScope k(nullptr, SISL_K_OTHER, st);
+  if (dtype == SISL_F64)
+    launch_ffsl_lines_vjp<double>(n, nlines, (const double*)scalar, (const double*)cfl, (const double*)out_bar,
+                                  (double*)scalar_bar, (double*)cfl_bar, M, Mb, periodic ? 1 : 0, st);
+  else if (dtype == SISL_F32)
+    launch_ffsl_lines_vjp<float>(n, nlines, (const float*)scalar, (const float*)cfl, (const float*)out_bar,
+                                 (float*)scalar_bar, (float*)cfl_bar, M, Mb, periodic ? 1 : 0, st);
   else
     return SISL_ERR_ARG;
   return check_cuda();
@@ -1891,6 +1921,28 @@ int sisl_ffsl_advect(SislCore* c, const void* field, const void* u, const void* 
     KScope k(c, SISL_K_OTHER, st, 4);
     launch_ffsl<T>(c->d, coef_of<T>(c), (const T*)field, (const T*)u, (const T*)v, (const T*)eta, (T*)out, t0, t1,
                    M, st);
+  };
+  if (c->grid.dtype == SISL_F64) run(double{});
+  else run(float{});
+  return check_cuda();
+}
+
+int sisl_ffsl_advect_vjp(SislCore* c, const void* field, const void* u, const void* v, const void* eta,
+                         const void* out_bar, void* field_bar, void* u_bar, void* v_bar, void* eta_bar, void* ws,
+                         size_t ws_bytes, void* stream) {
+  if (!c || !field || !u || !v || !eta || !out_bar || !field_bar) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_FFSL_VJP)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv{(char*)ws};
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    T* tmp[5];
+    for (int q = 0; q < 5; ++q) tmp[q] = (T*)cv.take(sizeof(T) * field_size(c->d, LOC_M));
+    double* M = (double*)cv.take(sizeof(double) * ffsl_scratch_doubles(c->d));
+    double* Mb = (double*)cv.take(sizeof(double) * ffsl_scratch_doubles(c->d));
+    KScope k(c, SISL_K_OTHER, st, 6);
+    launch_ffsl_vjp<T>(c->d, coef_of<T>(c), (const T*)field, (const T*)u, (const T*)v, (const T*)eta,
+                       (const T*)out_bar, (T*)field_bar, (T*)u_bar, (T*)v_bar, (T*)eta_bar, tmp, M, Mb, st);
   };
   if (c->grid.dtype == SISL_F64) run(double{});
   else run(float{});

@@ -137,6 +137,13 @@ template <typename T>
 int launch_ffsl(const Dims& d, const Coef<T>& c, const T* field, const T* u, const T* v, const T* eta, T* out,
                 T* tmp0, T* tmp1, double* M, cudaStream_t st);
 template <typename T>
+int launch_ffsl_vjp(const Dims& d, const Coef<T>& c, const T* field, const T* u, const T* v, const T* eta,
+                    const T* out_bar, T* field_bar, T* u_bar, T* v_bar, T* eta_bar, T* const* tmp, double* M,
+                    double* Mb, cudaStream_t st);
+template <typename T>
+void launch_ffsl_lines_vjp(int N, int nlines, const T* scalar, const T* cfl, const T* out_bar, T* scalar_bar,
+                           T* cfl_bar, double* M, double* Mb, int periodic, cudaStream_t st);
+template <typename T>
 void launch_ffsl_lines(int N, int nlines, const T* scalar, const T* cfl, T* out, double* M, int periodic,
                        cudaStream_t st);
 template <typename T>

@@ -137,6 +137,145 @@ __global__ void ffsl_line_kernel(int N, int nlines, const T* __restrict__ sc, co
   }
 }
 
+// ---------------------------------------------------------------------------
+// Reverse of advect_1d on one line (the VJP XLA forms for steppers.py:552-594):
+//   Md(q) = map_coordinates(M, dep(q), order 1, nearest), out(q) = Md(q+1) - Md(q)
+//   dep(q) = clip(q - cfl(q), 0, N) (open) or q + N - cfl(q) (periodic, three
+//   copies); clip = maximum then minimum, so an exact tie passes half the
+//   cotangent; floor() carries none.
+// Md_bar(q) = out_bar(q-1) - out_bar(q); M_bar gets the interpolation weights;
+// cfl_bar(q) = -clip'(q) Md_bar(q) (M(i1) - M(i0)); scalar_bar(t) = sum of
+// M_bar(p) over p > t (plus the periodic total's cotangent).  M and M_bar are
+// float64 line scratch, position-major and line-fastest.
+// ---------------------------------------------------------------------------
+template <typename ScalarAt, typename CflAt, typename OutBarAt, typename ScalarBarSet, typename CflBarSet>
+__device__ __forceinline__ void advect_line_vjp(int N, int nlines, int line, int periodic, ScalarAt sc, CflAt cfl,
+                                                OutBarAt ob, ScalarBarSet set_sb, CflBarSet set_cb,
+                                                double* __restrict__ M, double* __restrict__ Mb) {
+  auto at = [&](const double* A, long long p) -> double { return A[(size_t)p * nlines + line]; };
+  double s = 0.0;
+  M[line] = 0.0;
+  Mb[line] = 0.0;
+  for (int q = 0; q < N; ++q) {
+    s += sc(q);
+    M[(size_t)(q + 1) * nlines + line] = s;
+    Mb[(size_t)(q + 1) * nlines + line] = 0.0;
+  }
+  const double S = s;
+  double Sb = 0.0;
+  const long long L = periodic ? 3LL * N + 1 : (long long)N + 1;
+  auto Mat = [&](long long p) -> double {
+    if (!periodic) return at(M, p);
+    return (double)(p / N) * S + at(M, p % N);
+  };
+  auto Mb_add = [&](long long p, double x) {
+    if (!periodic) {
+      Mb[(size_t)p * nlines + line] += x;
+      return;
+    }
+    Mb[(size_t)(p % N) * nlines + line] += x;
+    Sb += (double)(p / N) * x;
+  };
+  for (int q = 0; q <= N; ++q) {
+    const double mdb = (q >= 1 ? ob(q - 1) : 0.0) - (q <= N - 1 ? ob(q) : 0.0);
+    const double c0 = cfl(q);
+    double dep, cg = 1.0;
+    if (periodic) {
+      dep = (double)(q + N) - c0;
+    } else {
+      const double x = (double)q - c0;
+      if (x < 0.0) { dep = 0.0; cg = 0.0; }
+      else if (x == 0.0) { dep = 0.0; cg = 0.5; }
+      else if (x < (double)N) { dep = x; }
+      else if (x == (double)N) { dep = (double)N; cg = 0.5; }
+      else { dep = (double)N; cg = 0.0; }
+    }
+    const double lo = floor(dep), w = dep - lo;
+    long long i0 = (long long)lo, i1 = i0 + 1;
+    i0 = i0 < 0 ? 0 : (i0 > L - 1 ? L - 1 : i0);
+    i1 = i1 < 0 ? 0 : (i1 > L - 1 ? L - 1 : i1);
+    set_cb(q, -cg * mdb * (Mat(i1) - Mat(i0)));
+    if (mdb != 0.0) {
+      Mb_add(i0, (1.0 - w) * mdb);
+      Mb_add(i1, w * mdb);
+    }
+  }
+  double acc = periodic ? Sb : 0.0;
+  for (int q = N - 1; q >= 0; --q) {
+    if (q + 1 <= N - 1 || !periodic) acc += at(Mb, q + 1);
+    set_sb(q, acc);
+  }
+}
+
+// one reverse x, y or z sweep of advect_3d_split; ob_density: the forward
+// sweep divided by the cell volume (the z sweep); ib_density: its input was
+// the density times the cell volume (the x sweep)
+template <typename T>
+__global__ void ffsl_sweep_vjp_kernel(Dims d, Coef<T> c, int axis, const T* __restrict__ in,
+                                      const T* __restrict__ vel, const T* __restrict__ ob, T* ib, T* velb,
+                                      double* __restrict__ M, double* __restrict__ Mb, int periodic, double dt,
+                                      int ob_density, int ib_density) {
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  int N, nlines, a, b;
+  if (axis == 0) { N = d.nx; nlines = d.ny * d.nz; a = line % d.ny; b = line / d.ny; }
+  else if (axis == 1) { N = d.ny; nlines = d.nx * d.nz; a = line % d.nx; b = line / d.nx; }
+  else { N = d.nz; nlines = d.nx * d.ny; a = line % d.nx; b = line / d.nx; }
+  if (line >= nlines) return;
+  auto ijk = [&](int q, int& i, int& j, int& k) {
+    if (axis == 0) { i = q; j = a; k = b; } else if (axis == 1) { i = a; j = q; k = b; } else { i = a; j = b; k = q; }
+  };
+  auto cell = [&](int q) -> int {
+    int i, j, k;
+    ijk(q, i, j, k);
+    return im(d, i, j, k);
+  };
+  auto vol = [&](int q) -> double {
+    int i, j, k;
+    ijk(q, i, j, k);
+    return (double)cell_volume(d, c, i, j, k);
+  };
+  auto face = [&](int q) -> int {
+    if (axis == 0) return iu(d, q, a, b);
+    if (axis == 1) return iv(d, a, q, b);
+    return iw(d, a, b, q);
+  };
+  auto factor = [&](int q) -> double {  // d cfl / d velocity (steppers.py:614-616)
+    if (axis == 0) return (double)ld(c.mu, h_u(d, q, a)) * dt / d.dx;
+    if (axis == 1) return (double)ld(c.mv, h_v(d, a, q)) * dt / d.dy;
+    return dt;
+  };
+  advect_line_vjp(
+      N, nlines, line, periodic, [&](int q) { return (double)ld(in, cell(q)); },
+      [&](int q) { return (double)ld(vel, face(q)) * factor(q); },
+      [&](int q) {
+        const double x = (double)ld(ob, cell(q));
+        return ob_density ? x / vol(q) : x;
+      },
+      [&](int q, double x) { ib[cell(q)] = (T)(ib_density ? x * vol(q) : x); },
+      [&](int q, double x) {
+        if (velb) velb[face(q)] = (T)(x * factor(q));
+      },
+      M, Mb);
+}
+
+// advect_1d VJP on nlines independent lines (layouts of ffsl_line_kernel)
+template <typename T>
+__global__ void ffsl_line_vjp_kernel(int N, int nlines, const T* __restrict__ sc, const T* __restrict__ cf,
+                                     const T* __restrict__ ob, T* sb, T* cb, double* __restrict__ M,
+                                     double* __restrict__ Mb, int periodic) {
+  const int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= nlines) return;
+  const size_t s0 = (size_t)line * N, c0 = (size_t)line * (N + 1);
+  advect_line_vjp(
+      N, nlines, line, periodic, [&](int q) { return (double)sc[s0 + q]; },
+      [&](int q) { return (double)cf[c0 + q]; }, [&](int q) { return (double)ob[s0 + q]; },
+      [&](int q, double x) { sb[s0 + q] = (T)x; },
+      [&](int q, double x) {
+        if (cb) cb[c0 + q] = (T)x;
+      },
+      M, Mb);
+}
+
 template <typename T>
 __global__ void eos_kernel(Dims d, Coef<T> c, const T* __restrict__ th, const T* __restrict__ pi, T* rho) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -175,6 +314,38 @@ int launch_ffsl(const Dims& d, const Coef<T>& c, const T* field, const T* u, con
   return 4;  // kernels launched
 }
 
+// field_bar (and u_bar, v_bar, eta_bar where non-null) of out = FFSL(field)
+// from out_bar; tmp[0..4] mass-point scratch, M and Mb float64 line scratch
+// of ffsl_scratch_doubles() entries each.
+template <typename T>
+int launch_ffsl_vjp(const Dims& d, const Coef<T>& c, const T* field, const T* u, const T* v, const T* eta,
+                    const T* out_bar, T* field_bar, T* u_bar, T* v_bar, T* eta_bar, T* const* tmp, double* M,
+                    double* Mb, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  const int tb = 128;
+  const double dt = c.s.dt;
+  T *mass = tmp[0], *mx = tmp[1], *my = tmp[2], *b1 = tmp[3], *b2 = tmp[4];
+  // recompute the sweeps' inputs
+  ffsl_mass_kernel<T><<<box3(d, blk), blk, 0, st>>>(d, c, field, mass);
+  ffsl_sweep_kernel<T><<<(d.ny * d.nz + tb - 1) / tb, tb, 0, st>>>(d, c, 0, mass, u, mx, M, d.px, dt, 0);
+  ffsl_sweep_kernel<T><<<(d.nx * d.nz + tb - 1) / tb, tb, 0, st>>>(d, c, 1, mx, v, my, M, d.py, dt, 0);
+  // reverse z, y, x
+  ffsl_sweep_vjp_kernel<T><<<(d.nx * d.ny + tb - 1) / tb, tb, 0, st>>>(d, c, 2, my, eta, out_bar, b1, eta_bar, M,
+                                                                     Mb, 0, dt, 1, 0);
+  ffsl_sweep_vjp_kernel<T><<<(d.nx * d.nz + tb - 1) / tb, tb, 0, st>>>(d, c, 1, mx, v, b1, b2, v_bar, M, Mb, d.py,
+                                                                     dt, 0, 0);
+  ffsl_sweep_vjp_kernel<T><<<(d.ny * d.nz + tb - 1) / tb, tb, 0, st>>>(d, c, 0, mass, u, b2, field_bar, u_bar, M,
+                                                                     Mb, d.px, dt, 0, 1);
+  return 6;  // kernels launched
+}
+
+template <typename T>
+void launch_ffsl_lines_vjp(int N, int nlines, const T* scalar, const T* cfl, const T* out_bar, T* scalar_bar,
+                           T* cfl_bar, double* M, double* Mb, int periodic, cudaStream_t st) {
+  ffsl_line_vjp_kernel<T><<<(nlines + 127) / 128, 128, 0, st>>>(N, nlines, scalar, cfl, out_bar, scalar_bar, cfl_bar,
+                                                                M, Mb, periodic);
+}
+
 template <typename T>
 void launch_ffsl_lines(int N, int nlines, const T* scalar, const T* cfl, T* out, double* M, int periodic,
                        cudaStream_t st) {
@@ -191,6 +362,16 @@ template int launch_ffsl<float>(const Dims&, const Coef<float>&, const float*, c
                                 const float*, float*, float*, float*, double*, cudaStream_t);
 template int launch_ffsl<double>(const Dims&, const Coef<double>&, const double*, const double*, const double*,
                                  const double*, double*, double*, double*, double*, cudaStream_t);
+template int launch_ffsl_vjp<float>(const Dims&, const Coef<float>&, const float*, const float*, const float*,
+                                    const float*, const float*, float*, float*, float*, float*, float* const*,
+                                    double*, double*, cudaStream_t);
+template int launch_ffsl_vjp<double>(const Dims&, const Coef<double>&, const double*, const double*, const double*,
+                                     const double*, const double*, double*, double*, double*, double*,
+                                     double* const*, double*, double*, cudaStream_t);
+template void launch_ffsl_lines_vjp<float>(int, int, const float*, const float*, const float*, float*, float*,
+                                           double*, double*, int, cudaStream_t);
+template void launch_ffsl_lines_vjp<double>(int, int, const double*, const double*, const double*, double*, double*,
+                                            double*, double*, int, cudaStream_t);
 template void launch_ffsl_lines<float>(int, int, const float*, const float*, float*, double*, int, cudaStream_t);
 template void launch_ffsl_lines<double>(int, int, const double*, const double*, double*, double*, int,
                                         cudaStream_t);

@@ -269,6 +269,41 @@ class FluxFormAdvector:
               "sisl_ffsl_lines")
         return out.reshape(s.shape)
 
+    def advect_1d_vjp(self, scalar_1d, cfl_inter_1d, out_bar, periodic=False):
+        """VJP of ``advect_1d`` (``sisl_ffsl_lines_vjp``): the cotangents of
+        the scalar (..., N) and of the interface Courant numbers (..., N + 1)."""
+        s = torch.as_tensor(scalar_1d)
+        c = torch.as_tensor(cfl_inter_1d).to(device=s.device, dtype=s.dtype)
+        N = s.shape[-1]
+        sb = s.reshape(-1, N).contiguous()
+        cb = c.reshape(-1, N + 1).contiguous()
+        ob = torch.as_tensor(out_bar).to(device=s.device, dtype=s.dtype).reshape(-1, N).contiguous()
+        gs, gc = torch.empty_like(sb), torch.empty_like(cb)
+        lib = _lib.load()
+        n = int(lib.sisl_ffsl_lines_vjp_workspace_bytes(N, sb.shape[0]))
+        ws = torch.empty(max(n, 256), dtype=torch.uint8, device=s.device)
+        from .core import DTYPE_CODE, stream_ptr
+        check(lib.sisl_ffsl_lines_vjp(DTYPE_CODE[s.dtype], N, sb.shape[0], sb.data_ptr(), cb.data_ptr(),
+                                      int(bool(periodic)), ob.data_ptr(), gs.data_ptr(), gc.data_ptr(),
+                                      ws.data_ptr(), n, stream_ptr(s.device)), "sisl_ffsl_lines_vjp")
+        return gs.reshape(s.shape), gc.reshape(c.shape)
+
+    def advect_3d_split_vjp(self, field, state, bg_precomputed, out_bar):
+        """VJP of ``advect_3d_split`` (``sisl_ffsl_advect_vjp``): cotangents of
+        the field and of ``u``, ``v``, ``eta_dot``."""
+        if self.physics is None:
+            raise RuntimeError("FluxFormAdvector needs the Euler3D physics for its metric coefficients")
+        core = self.physics.core(field.dtype, self.dt, 0.55)
+        f = core.field(field, "m")
+        u, v, e = core.field(state["u"], "u"), core.field(state["v"], "v"), core.field(state["eta_dot"], "w")
+        ob = core.field(out_bar, "m")
+        gf, gu, gv, ge = core.new("m"), core.new("u"), core.new("v"), core.new("w")
+        ws, n = core.workspace(_lib.WS_FFSL_VJP)
+        check(core.lib.sisl_ffsl_advect_vjp(core.handle, f.data_ptr(), u.data_ptr(), v.data_ptr(), e.data_ptr(),
+                                            ob.data_ptr(), gf.data_ptr(), gu.data_ptr(), gv.data_ptr(), ge.data_ptr(),
+                                            ws.data_ptr(), n, core.stream), "sisl_ffsl_advect_vjp")
+        return {"field": gf, "u": gu, "v": gv, "eta_dot": ge}
+
     def advect_3d_split(self, field, state, bg_precomputed):
         if self.physics is None:
             raise RuntimeError("FluxFormAdvector needs the Euler3D physics for its metric coefficients")

@@ -284,3 +284,17 @@ def test_thomas_matches_scipy_banded():
     ab[2, :-1] = lo[1:].numpy()
     ref = solve_banded((1, 1), ab, b.numpy())
     assert np.max(np.abs(tridiagonal_solve(lo, main, up, b).numpy() - ref)) < 1e-13
+
+
+def test_ffsl_clip_tie_passes_half_the_cotangent():
+    """jnp.clip (steppers.py:589) is maximum then minimum, whose gradient
+    splits an exact tie: a wall interface at rest (departure point exactly
+    0) passes half the Courant-number cotangent."""
+    adv = FluxFormAdvector(RegionalGrid3D(4, 4, 4, 1.0, 1.0, 1.0, 0.0, 0.0), 1.0)
+    s = torch.tensor([[1.0, 2.0, 4.0]], dtype=F64)
+    c = torch.zeros(1, 4, dtype=F64, requires_grad=True)
+    out = adv._advect_last(s, c, False)
+    (g,) = torch.autograd.grad(out[0, 0], c)
+    # out[0] = Md(1) - Md(0); Md(0) at the tie dep = 0 has slope M(1) - M(0) = s[0]
+    assert float(g[0, 0]) == pytest.approx(0.5 * float(s[0, 0]))
+    assert float(g[0, 1]) == pytest.approx(-float(s[0, 1]))
