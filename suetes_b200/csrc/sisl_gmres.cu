@@ -441,6 +441,25 @@ int flat_grid(size_t n, int elems_per_block) {
   return (int)b;
 }
 
+// Grid of a grid-stride Krylov kernel: every block resident at once (one
+// wave, no tail of a partial second wave), at most GM_MAXBLOCKS.
+int resident_grid(const void* fn, int threads, size_t smem, size_t n, int elems_per_block) {
+  static int sms[16] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& ns = sms[dev & 15];
+  if (ns == 0 && cudaDeviceGetAttribute(&ns, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) ns = 148;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  size_t want = (n + elems_per_block - 1) / elems_per_block;
+  size_t cap = (size_t)per_sm * ns;
+  if (cap > (size_t)GM_MAXBLOCKS) cap = GM_MAXBLOCKS;
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  return (int)want;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -461,16 +480,16 @@ void gm_dots(const T* Vb, size_t stride, int m, const T* w, size_t n, double* pa
   nt = nt >= 256 ? 256 : (nt / 32) * 32;
   if (nt < 32) nt = 32;
   constexpr int E = CH * V16<T>::n;
-  const int g = flat_grid(n, nt * E);
-  dots_kernel<T><<<g, nt, (size_t)(m + 1) * nt * sizeof(double), st>>>(Vb, stride, m, w, n, partial, gs, mode,
-                                                                        gated);
+  const size_t smem = (size_t)(m + 1) * nt * sizeof(double);
+  const int g = resident_grid((const void*)dots_kernel<T>, nt, smem, n, nt * E);
+  dots_kernel<T><<<g, nt, smem, st>>>(Vb, stride, m, w, n, partial, gs, mode, gated);
 }
 
 template <typename T>
 void gm_update(const T* Vb, size_t stride, int m, T* w, size_t n, double sign, double* partial, GState* gs,
                int mode, int gated, int limit_kdone, cudaStream_t st) {
   constexpr int E = CH * V16<T>::n;
-  const int g = flat_grid(n, GT * E);
+  const int g = resident_grid((const void*)update_kernel<T>, GT, 0, n, GT * E);
   update_kernel<T><<<g, GT, 0, st>>>(Vb, stride, m, w, n, sign, partial, gs, mode, gated, limit_kdone);
 }
 
