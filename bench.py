@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--ens-members", type=int, default=32,
                     help="members of the uneven-size bubble ensemble leg (0 disables it)")
     ap.add_argument("--ens-steps", type=int, default=10, help="timed graph steps of the ensemble leg")
+    ap.add_argument("--ens-vjp-steps", type=int, default=2,
+                    help="trajectory length of the per-member fwd+VJP of the ensemble leg (0 disables it)")
     ap.add_argument("--vjp-steps", type=int, default=4,
                     help="trajectory length of the fwd+VJP leg (0 disables it)")
     ap.add_argument("--vjp-checkpoint", type=int, default=1, help="checkpoint interval of the fwd+VJP leg")
@@ -514,6 +516,7 @@ def ensemble_leg(args, local, world):
     torch.cuda.synchronize()
     ms_seq = e0.elapsed_time(e1)
     sizes = sorted({(sp["nx"], sp["ny"], sp["nz"]) for _, _, _, sp in ens})
+    vjp = ensemble_vjp(args, world, dss, pp, cells) if args.ens_vjp_steps > 0 else None
     return {"metric": "SISL cell-steps/s, uneven-size bubble ensemble", "value": world * cells * K / (ms / 1e3),
             "unit": "cell-steps/s", "members": len(ens), "cells_per_step": cells, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "launch": "one CUDA graph per ensemble step (graph launches timed)",
@@ -521,7 +524,45 @@ def ensemble_leg(args, local, world):
             "eager_sequential": {"value": cells / (ms_seq / 1e3), "ms_per_step": ms_seq},
             "speedup_vs_eager_sequential": ms_seq / (ms / K), "distinct_shapes": len(sizes),
             "dtype": "f32", "gmres_tol": args.tol32, "method": args.method,
-            "autotune": _tuning_summary(pp.tuning)}
+            "autotune": _tuning_summary(pp.tuning), "fwd_vjp_per_member": vjp}
+
+
+def ensemble_vjp(args, world, dss, pp, cells):
+    """Value and gradient of J_i = max w of member i after ``--ens-vjp-steps``
+    steps from its current state, w.r.t. its initial theta', one member
+    after another (trajectory_vjp: fused taped forward, native reverse sweep)."""
+    from suetes_b200.adjoint import trajectory_vjp
+    from suetes_b200.core import kernel_launches
+    N = args.ens_vjp_steps
+    starts = list(pp.current())
+
+    def objective(n, st):
+        return st["w"].max() if n == N else None
+
+    def run():
+        Js, gn = [], []
+        for (st, _, bc), ds in zip(dss, starts):
+            st.implicit_solver.transpose_tol = args.adj_tol32
+            st.implicit_solver.transpose_method = args.adj_method
+            J, g = trajectory_vjp(st, ds, N, objective, bc_fn=bc)
+            Js.append(float(J))
+            gn.append(float(torch.linalg.vector_norm(g["th_p"].double())))
+        return Js, gn
+    run()  # warm-up (allocations)
+    torch.cuda.synchronize()
+    barrier(world)
+    l0 = kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    Js, gn = run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = dist_max(e0.elapsed_time(e1), world)
+    return {"metric": "SISL cell-steps/s fwd+VJP, per member", "value": world * cells * N / (ms / 1e3),
+            "unit": "cell-steps/s", "steps": N, "ms_per_ensemble_step": ms / N, "gpu_launches": kernel_launches() - l0,
+            "objective": "J_i = max w of member i after the trajectory; gradient w.r.t. its initial theta'",
+            "J_max_w": [min(Js), max(Js)], "grad_norm": [min(gn), max(gn)], "adjoint_tol_f32": args.adj_tol32,
+            "adjoint_method": args.adj_method}
 
 
 def _tuning_summary(tunings):

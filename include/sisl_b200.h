@@ -336,8 +336,9 @@ int sisl_step_vjp(SislCore* core, const SislState* in, void* const solves[10], c
  * the many-member configuration.  Cores must be distinct and have no timing
  * class selected; relax may be NULL (or hold NULL entries). */
 /* Launch shapes of the Helmholtz kernels: stencil block variants (0-3:
- * 32x4x2, 32x8x1, 32x2x4, 64x4x1 threads; the matvec also 4: 32x8 columns
- * of two levels per thread) of the matvec and of its transpose, and column
+ * 32x4x2, 32x8x1, 32x2x4, 64x4x1 threads; the matvec also 4 and 5: 32x8
+ * columns of two or four levels per thread) of the matvec and of its
+ * transpose, and column
  * variants (0-2: tiles of 256 threads / 32 columns,
  * 128 / 16, 256 / 64; 3: one thread per column marching up and down the
  * precomputed factorisation, 128 columns per block) of the preconditioner

@@ -283,8 +283,6 @@ __global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T
 
 // rounded products that the compiler may not fuse into a following add, so
 // that the column variants of M^T round identically
-__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 
 template <typename T, int TPT, int TPC>
 __global__ void __launch_bounds__(TPT) pt_column_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,

@@ -35,7 +35,7 @@ __host__ inline dim3 stencil_block(int variant) {
   }
 }
 constexpr int N_STENCIL_BLOCKS = 4;
-constexpr int N_MATVEC_SHAPES = 5;  // the 4 blocks, and 32x8 columns of 2 levels per thread
+constexpr int N_MATVEC_SHAPES = 6;  // the 4 blocks, and 32x8 columns of 2 or 4 levels per thread
 // column variants: tiles of (threads, columns) = (256, 32), (128, 16), (256, 64),
 // and the one-thread-per-column march (128 columns per block)
 constexpr int N_COLUMN_TILES = 4;
@@ -75,6 +75,11 @@ __device__ __forceinline__ void level_pair(int k, int nz, int& l, int& r) {
 
 template <typename T>
 __device__ __forceinline__ T ld(const T* __restrict__ p, int i) { return __ldg(p + i); }
+
+// A product rounded on its own (never contracted into an FMA), for values
+// that several code paths share and must round identically.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 
 // Block-wide double-precision sum of NV values per thread; thread 0 of the
 // block ends up with the totals in out[].

@@ -30,9 +30,10 @@ template <typename T>
 __device__ __forceinline__ T gz_mass(const T* __restrict__ p, const T* __restrict__ iz, int base, int k, int nz,
                                      int plane, T sp) {
   const int kl = k > 0 ? k - 1 : 0, kh = k + 1 < nz ? k + 1 : nz - 1;
-  const T Pl = ld(p, base + kl * plane) * sp, P0 = ld(p, base + k * plane) * sp, Ph = ld(p, base + kh * plane) * sp;
-  const T g0 = (k == 0 ? Ph - P0 : P0 - Pl) * ld(iz, base + k * plane);
-  const T g1 = (k + 1 == nz ? P0 - Pl : Ph - P0) * ld(iz, base + (k + 1) * plane);
+  const T Pl = mul_rn(ld(p, base + kl * plane), sp), P0 = mul_rn(ld(p, base + k * plane), sp),
+          Ph = mul_rn(ld(p, base + kh * plane), sp);
+  const T g0 = mul_rn(k == 0 ? Ph - P0 : P0 - Pl, ld(iz, base + k * plane));
+  const T g1 = mul_rn(k + 1 == nz ? P0 - Pl : Ph - P0, ld(iz, base + (k + 1) * plane));
   return T(0.5) * (g0 + g1);
 }
 
@@ -64,7 +65,8 @@ __device__ __forceinline__ void matvec_point(const Dims& d, const Coef<T>& c, co
   const T gmO = gz_mass(xp, c.idzw, hO, km, nz, pm, sp);
   const T gmX = gz_mass(xp, c.idzw, hX, km, nz, pm, sp);
   const T gmY = gz_mass(xp, c.idzw, hY, km, nz, pm, sp);
-  const T PO = ld(xp, hO + km * pm) * sp, PX = ld(xp, hX + km * pm) * sp, PY = ld(xp, hY + km * pm) * sp;
+  const T PO = mul_rn(ld(xp, hO + km * pm), sp), PX = mul_rn(ld(xp, hX + km * pm), sp),
+          PY = mul_rn(ld(xp, hY + km * pm), sp);
   const int pU = iuc + (nx + 1) * (jc + ny * km);        // u face (i, jc, km)
   const int pV = ic + nx * (jvc + (ny + 1) * km);        // v face (ic, j, km)
   const int uO = ic + (nx + 1) * (jc + ny * km);         // u face (ic, jc, km): own cell west face
@@ -82,7 +84,7 @@ __device__ __forceinline__ void matvec_point(const Dims& d, const Coef<T>& c, co
   const int pw = hO + k * pm, pwi = hO + kw * pm;
   const T xw_k = ld(xw, pw), xW_k = ld(xW, pw), idzw_k = ld(c.idzw, pw);
   const T damp = ld(c.damp, pwi), thw = ld(c.thw, pwi), zxw = ld(c.zxw, pwi), zew = ld(c.zew, pwi);
-  const T Pw1 = ld(xp, hO + kw * pm) * sp, Pw0 = ld(xp, hO + (kw - 1) * pm) * sp;
+  const T Pw1 = mul_rn(ld(xp, hO + kw * pm), sp), Pw0 = mul_rn(ld(xp, hO + (kw - 1) * pm), sp);
   const int uw1 = ic + (nx + 1) * (jc + ny * kw), uw0 = uw1 - pu;
   const int vw1 = ic + nx * (jc + (ny + 1) * kw), vw0 = vw1 - pv;
   const T uwa = ld(xu, uw0), uwb = ld(xu, uw0 + 1), uwc = ld(xu, uw1), uwd = ld(xu, uw1 + 1);
@@ -108,15 +110,15 @@ __device__ __forceinline__ void matvec_point(const Dims& d, const Coef<T>& c, co
   const T Lv = v_lock ? xv_f * xs : xv_f * xs - adt * tend_v;
   // w and eta_dot rows at w level k; identity rows on the ground and lid (euler.py:426-437)
   const bool wb = (k == 0 || k == nz);
-  const T gzw = (Pw1 - Pw0) * idzw_k;
+  const T gzw = mul_rn(Pw1 - Pw0, idzw_k);
   const T Lw = wb ? xw_k * xs : damp * xw_k * xs + adt * cp * thw * gzw;
   const T uw = T(0.25) * (uwa + uwb + uwc + uwd) * xs, vw = T(0.25) * (vwa + vwb + vwc + vwd) * xs;
   const T Le = wb ? xW_k * xs * idzw_k : a * (xW_k * xs + mw * (uw * zxw + vw * zew) - xw_k * xs);
   // pi row (euler.py:298-318 through linear_operator)
   const T fx0 = uO0 * rdu0 * thu0, fx1 = uO1 * rdu1 * thu1;
   const T fy0 = vO0 * rdv0 * thv0, fy1 = vO1 * rdv1 * thv1;
-  const T fz0 = (km == 0) ? T(0) : W0 * rw0 * tw0;
-  const T fz1 = (km + 1 == nz) ? T(0) : W1 * rw1 * tw1;
+  const T fz0 = (km == 0) ? T(0) : mul_rn(mul_rn(W0, rw0), tw0);
+  const T fz1 = (km + 1 == nz) ? T(0) : mul_rn(mul_rn(W1, rw1), tw1);
   const T divh = mw * mw * ((fx1 - fx0) * idx + (fy1 - fy0) * idy);
   const T Lp = xp_k * xs + adt * ps * cpidz * (xs * (divh + (fz1 - fz0)));
   // ---- stores ----
@@ -148,10 +150,13 @@ __device__ __forceinline__ void matvec_point(const Dims& d, const Coef<T>& c, co
 
 // One thread per point, or LV consecutive levels of a column per thread (the
 // loads the levels share -- pressure at k+-1, the w-level winds, 1/dz_w --
-// are then common subexpressions).  float: 6 resident blocks of 256 (<= 40
-// registers, no spills) for more loads in flight; double keeps 4.
+// are then common subexpressions; the scaled pressures and the vertical
+// gradients and fluxes two levels share are rounded on their own, so every
+// shape gives bitwise the same rows).  float: 6 resident blocks of 256
+// (<= 40 registers, no spills) for one level per thread, 4 for several;
+// double 4 and 3.
 template <typename T, int LV>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 && LV == 1) ? 6 : 4) matvec_kernel(Dims d, Coef<T> c, CVec5<T> x,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LV == 1 ? 6 : 4) : (LV == 1 ? 4 : 3)) matvec_kernel(Dims d, Coef<T> c, CVec5<T> x,
                                                                             const double* xscale,
                                                      CVec5<T> b, Vec5<T> out, const int* active) {
   if (active && *active == 0) return;
@@ -317,10 +322,12 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
 template <typename T>
 void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xscale, CVec5<T> b,
                    Vec5<T> out, const int* active, cudaStream_t st) {
-  if (d.tune_mv == 4) {  // two levels per thread
+  if (d.tune_mv == 4 || d.tune_mv == 5) {  // two or four levels per thread
     const dim3 blk(32, 8, 1);
-    dim3 grd((d.nx + 1 + 31) / 32, (d.ny + 1 + 7) / 8, (d.nz + 2) / 2);
-    matvec_kernel<T, 2><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+    const int lv = d.tune_mv == 4 ? 2 : 4;
+    dim3 grd((d.nx + 1 + 31) / 32, (d.ny + 1 + 7) / 8, (d.nz + lv) / lv);
+    if (lv == 2) matvec_kernel<T, 2><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+    else matvec_kernel<T, 4><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
     return;
   }
   const dim3 blk = stencil_block(d.tune_mv);
