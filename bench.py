@@ -549,6 +549,10 @@ def ensemble_vjp(args, world, dss, pp, cells):
             gn.append(float(torch.linalg.vector_norm(g["th_p"].double())))
         return Js, gn
     run()  # warm-up (allocations)
+    logs = []
+    for st, _, _ in dss:
+        st.implicit_solver.transpose_log = []
+        logs.append(st.implicit_solver.transpose_log)
     torch.cuda.synchronize()
     barrier(world)
     l0 = kernel_launches()
@@ -558,7 +562,15 @@ def ensemble_vjp(args, world, dss, pp, cells):
     e1.record()
     torch.cuda.synchronize()
     ms = dist_max(e0.elapsed_time(e1), world)
+    ts = [t for lg in logs for t in lg]
+    for st, _, _ in dss:
+        st.implicit_solver.transpose_log = None
+    tstat = {"solves": len(ts), "cycles_mean": sum(t["cycles"] for t in ts) / max(len(ts), 1),
+             "cycles_max": max((t["cycles"] for t in ts), default=0),
+             "converged_frac": sum(1 for t in ts if t["converged"]) / max(len(ts), 1),
+             "note": "the cotangent of max w is a delta at one point: a broadband right-hand side"}
     return {"metric": "SISL cell-steps/s fwd+VJP, per member", "value": world * cells * N / (ms / 1e3),
+            "transposed_solves": tstat,
             "unit": "cell-steps/s", "steps": N, "ms_per_ensemble_step": ms / N, "gpu_launches": kernel_launches() - l0,
             "objective": "J_i = max w of member i after the trajectory; gradient w.r.t. its initial theta'",
             "J_max_w": [min(Js), max(Js)], "grad_norm": [min(gn), max(gn)], "adjoint_tol_f32": args.adj_tol32,
