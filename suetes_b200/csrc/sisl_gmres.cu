@@ -149,11 +149,13 @@ __global__ void dots_kernel(const T* __restrict__ Vb, size_t stride, int m, cons
     if (lane == 0) partial[(size_t)blockIdx.x * (GM_MAXR + 2) + q] = s_;
   }
   if (!last_block(&gs->counter)) return;
-  // finish: sum the partials of all blocks
-  for (int q = tid; q <= m; q += nt) {
+  // finish: sum the partials of all blocks, one warp per result (lanes
+  // stride over the blocks, so the loads are independent)
+  for (int q = wp; q <= m; q += nw) {
     double s_ = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) s_ += partial[(size_t)b * (GM_MAXR + 2) + q];
-    acc[q] = s_;
+    for (int b = lane; b < (int)gridDim.x; b += 32) s_ += partial[(size_t)b * (GM_MAXR + 2) + q];
+    s_ = warp_sum(s_);
+    if (lane == 0) acc[q] = s_;
   }
   __syncthreads();
   if (tid == 0) {
@@ -252,9 +254,11 @@ __global__ void __launch_bounds__(GT) update_kernel(const T* __restrict__ Vb, si
     partial[blockIdx.x] = s;
   }
   if (!last_block(&gs->counter)) return;
+  if (threadIdx.x >= 32) return;
+  double tot = 0.0;  // warp 0 sums the blocks' partials
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) tot += partial[b];
+  tot = warp_sum(tot);
   if (threadIdx.x != 0) return;
-  double tot = 0.0;
-  for (int b = 0; b < (int)gridDim.x; ++b) tot += partial[b];
   gs->counter = 0;
   // ---- finish Arnoldi step j (jax _kth_arnoldi_iteration) ----
   const int j = m - 1;
