@@ -153,8 +153,8 @@ __device__ __forceinline__ void matvec_point(const Dims& d, const Coef<T>& c, co
 // are then common subexpressions; the scaled pressures and the vertical
 // gradients and fluxes two levels share are rounded on their own, so every
 // shape gives bitwise the same rows).  float: 6 resident blocks of 256
-// (<= 40 registers, no spills) for one level per thread, 4 for several;
-// double 4 and 3.
+// (<= 40 registers, no spills) for one level per thread, 4 for several
+// (a 3-block budget for four levels measured slower); double 4 and 3.
 template <typename T, int LV>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LV == 1 ? 6 : 4) : (LV == 1 ? 4 : 3)) matvec_kernel(Dims d, Coef<T> c, CVec5<T> x,
                                                                             const double* xscale,
