@@ -529,49 +529,68 @@ def ensemble_leg(args, local, world):
 
 def ensemble_vjp(args, world, dss, pp, cells):
     """Value and gradient of J_i = max w of member i after ``--ens-vjp-steps``
-    steps from its current state, w.r.t. its initial theta', one member
-    after another (trajectory_vjp: fused taped forward, native reverse sweep)."""
-    from suetes_b200.adjoint import trajectory_vjp
+    steps from its current state, w.r.t. its initial theta' (trajectory_vjp:
+    fused taped forward, native reverse sweep): the members driven
+    concurrently, each on its own stream from its own host thread
+    (ensemble_trajectory_vjp), and, for comparison, one after another."""
+    from suetes_b200.adjoint import ensemble_trajectory_vjp, trajectory_vjp
     from suetes_b200.core import kernel_launches
     N = args.ens_vjp_steps
     starts = list(pp.current())
+    for st, _, _ in dss:
+        st.implicit_solver.transpose_tol = args.adj_tol32
+        st.implicit_solver.transpose_method = args.adj_method
 
-    def objective(n, st):
+    def objective(m, n, st):
         return st["w"].max() if n == N else None
 
-    def run():
-        Js, gn = [], []
-        for (st, _, bc), ds in zip(dss, starts):
-            st.implicit_solver.transpose_tol = args.adj_tol32
-            st.implicit_solver.transpose_method = args.adj_method
-            J, g = trajectory_vjp(st, ds, N, objective, bc_fn=bc)
-            Js.append(float(J))
-            gn.append(float(torch.linalg.vector_norm(g["th_p"].double())))
-        return Js, gn
-    run()  # warm-up (allocations)
+    members = [(st, ds, bc) for (st, _, bc), ds in zip(dss, starts)]
+
+    def concurrent():
+        return ensemble_trajectory_vjp(members, N, objective)
+
+    def sequential():
+        return [trajectory_vjp(st, ds, N, lambda n, x, m=m: objective(m, n, x), bc_fn=bc)
+                for m, (st, ds, bc) in enumerate(members)]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return res, dist_max(e0.elapsed_time(e1), world)
+
+    concurrent()  # warm-up (allocations, streams, threads)
     logs = []
     for st, _, _ in dss:
         st.implicit_solver.transpose_log = []
         logs.append(st.implicit_solver.transpose_log)
-    torch.cuda.synchronize()
-    barrier(world)
     l0 = kernel_launches()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    Js, gn = run()
-    e1.record()
-    torch.cuda.synchronize()
-    ms = dist_max(e0.elapsed_time(e1), world)
+    res_c, ms = timed(concurrent)
+    launches = kernel_launches() - l0
     ts = [t for lg in logs for t in lg]
     for st, _, _ in dss:
         st.implicit_solver.transpose_log = None
+    res_s, ms_seq = timed(sequential)
+    Js = [float(J) for J, _ in res_c]
+    gn = [float(torch.linalg.vector_norm(g["th_p"].double())) for _, g in res_c]
+    dJ = max(abs(float(a) - float(b)) / max(abs(float(b)), 1e-300) for (a, _), (b, _) in zip(res_c, res_s))
+    dg = max(float(torch.linalg.vector_norm(ga["th_p"].double() - gb["th_p"].double()))
+             / max(float(torch.linalg.vector_norm(gb["th_p"].double())), 1e-300)
+             for (_, ga), (_, gb) in zip(res_c, res_s))
     tstat = {"solves": len(ts), "cycles_mean": sum(t["cycles"] for t in ts) / max(len(ts), 1),
              "cycles_max": max((t["cycles"] for t in ts), default=0),
              "converged_frac": sum(1 for t in ts if t["converged"]) / max(len(ts), 1),
              "note": "the cotangent of max w is a delta at one point: a broadband right-hand side"}
     return {"metric": "SISL cell-steps/s fwd+VJP, per member", "value": world * cells * N / (ms / 1e3),
+            "unit": "cell-steps/s", "steps": N, "ms_per_ensemble_step": ms / N, "gpu_launches": launches,
+            "launch": "members concurrently, one CUDA stream and host thread each",
+            "sequential": {"value": world * cells * N / (ms_seq / 1e3), "ms_per_ensemble_step": ms_seq / N},
+            "concurrent_vs_sequential": {"J_max_rel": dJ, "grad_max_rel_l2": dg},
             "transposed_solves": tstat,
-            "unit": "cell-steps/s", "steps": N, "ms_per_ensemble_step": ms / N, "gpu_launches": kernel_launches() - l0,
             "objective": "J_i = max w of member i after the trajectory; gradient w.r.t. its initial theta'",
             "J_max_w": [min(Js), max(Js)], "grad_norm": [min(gn), max(gn)], "adjoint_tol_f32": args.adj_tol32,
             "adjoint_method": args.adj_method}

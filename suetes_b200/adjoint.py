@@ -463,3 +463,42 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
                 gs = torch.autograd.grad(outs, [before[k] for k in keys], grads, allow_unused=True) if outs else []
             cot = {k: g for k, g in zip(keys, gs) if g is not None}
     return J, {k: cot.get(k) for k in wrt}
+
+
+def ensemble_trajectory_vjp(members, num_steps, objective, checkpoint_every=1, wrt=("th_p",), max_workers=None):
+    """``trajectory_vjp`` of every member of an ensemble, the members driven
+    concurrently: each on its own CUDA stream from its own host thread.  The
+    library's calls release the interpreter lock and keep their state in the
+    member's core and workspace, so the members' kernels and the
+    host round trips of their GMRES restart loops overlap on the GPU.
+
+    ``members``: ``[(stepper, state0, bc_fn)]`` (distinct steppers);
+    ``objective(m, n, state)`` as for ``trajectory_vjp`` with the member index
+    first.  Returns ``[(J_m, grads_m)]`` in member order, ready on the
+    caller's current stream."""
+    import concurrent.futures
+
+    from .steppers import DeviceState
+    if not members:
+        return []
+    first = members[0][1]
+    dev = torch.device(first.core.device if isinstance(first, DeviceState) else first["u"].device)
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    base = torch.cuda.current_stream(dev)
+    streams = [torch.cuda.Stream(device=dev) for _ in members]
+
+    def run(m):
+        torch.cuda.set_device(dev)  # a new host thread starts on device 0
+        st, s0, bc = members[m]
+        s = streams[m]
+        s.wait_stream(base)
+        with torch.cuda.stream(s):
+            return trajectory_vjp(st, s0, num_steps, lambda n, x: objective(m, n, x), bc_fn=bc,
+                                  checkpoint_every=checkpoint_every, wrt=wrt)
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max_workers or len(members)) as ex:
+        out = list(ex.map(run, range(len(members))))
+    for s in streams:
+        base.wait_stream(s)
+    return out

@@ -607,11 +607,8 @@ template <typename T, int NT>
 void launch_pt_march(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                      cudaStream_t st) {
   const size_t smem = (size_t)d.nz * NT * sizeof(T);
-  static size_t attr_bytes = 0;  // per instantiation
-  if (smem > 48 * 1024 && smem > attr_bytes) {
-    cudaFuncSetAttribute(pt_march_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_bytes = smem;
-  }
+  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  ensure_smem_limit((const void*)pt_march_kernel<T, NT>, attr_bytes, smem);
   pt_march_kernel<T, NT><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, y, out, active);
 }
 
@@ -619,11 +616,8 @@ template <typename T, int TPT, int TPC>
 void launch_pt_column(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                       cudaStream_t st) {
   const size_t smem = (size_t)(4 * d.nz) * TPC * sizeof(T);
-  static size_t attr_bytes = 0;  // per instantiation
-  if (smem > 48 * 1024 && smem > attr_bytes) {
-    cudaFuncSetAttribute(pt_column_kernel<T, TPT, TPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_bytes = smem;
-  }
+  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  ensure_smem_limit((const void*)pt_column_kernel<T, TPT, TPC>, attr_bytes, smem);
   pt_column_kernel<T, TPT, TPC><<<dim3((d.nx + TPC - 1) / TPC, d.ny), TPT, smem, st>>>(d, c, y, out, active);
 }
 

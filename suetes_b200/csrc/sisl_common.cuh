@@ -11,7 +11,23 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
+
 namespace sisl {
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` (never
+// lowers it).  Host threads that drive different cores call the launchers
+// concurrently, so the check-and-set runs under one lock.
+inline void ensure_smem_limit(const void* fn, std::atomic<size_t>& current, size_t bytes) {
+  if (bytes <= 48 * 1024 || bytes <= current.load()) return;
+  static std::mutex m;
+  std::lock_guard<std::mutex> lock(m);
+  if (bytes > current.load()) {
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    current.store(bytes);
+  }
+}
 
 enum Loc { LOC_M = 0, LOC_U = 1, LOC_V = 2, LOC_W = 3 };
 

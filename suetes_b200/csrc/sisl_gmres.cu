@@ -448,11 +448,14 @@ int flat_grid(size_t n, int elems_per_block) {
 // Grid of a grid-stride Krylov kernel: every block resident at once (one
 // wave, no tail of a partial second wave), at most GM_MAXBLOCKS.
 int resident_grid(const void* fn, int threads, size_t smem, size_t n, int elems_per_block) {
-  static int sms[16] = {0};
+  static std::atomic<int> sms[16];  // SM count per device, found once
   int dev = 0;
   cudaGetDevice(&dev);
-  int& ns = sms[dev & 15];
-  if (ns == 0 && cudaDeviceGetAttribute(&ns, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) ns = 148;
+  int ns = sms[dev & 15].load();
+  if (ns == 0) {
+    if (cudaDeviceGetAttribute(&ns, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || ns < 1) ns = 148;
+    sms[dev & 15].store(ns);
+  }
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
@@ -475,11 +478,8 @@ constexpr size_t DOTS_SMEM_MAX = 96 * 1024;
 template <typename T>
 void gm_dots(const T* Vb, size_t stride, int m, const T* w, size_t n, double* partial, GState* gs, int mode,
              int gated, cudaStream_t st) {
-  static bool attr_set = false;  // per instantiation
-  if (!attr_set) {
-    cudaFuncSetAttribute(dots_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DOTS_SMEM_MAX);
-    attr_set = true;
-  }
+  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  ensure_smem_limit((const void*)dots_kernel<T>, attr_bytes, (size_t)DOTS_SMEM_MAX);
   int nt = (int)(DOTS_SMEM_MAX / ((size_t)(m + 1) * sizeof(double)));
   nt = nt >= 256 ? 256 : (nt / 32) * 32;
   if (nt < 32) nt = 32;
@@ -513,12 +513,8 @@ void gm_info(const GState* gs, GDevInfo* o, cudaStream_t st) { info_kernel<<<1, 
 void gm_begin_cycle(GState* gs, cudaStream_t st) { begin_cycle_kernel<<<1, 256, 0, st>>>(gs); }
 void gm_small_solve(GState* gs, int restart, cudaStream_t st) {
   const size_t smem = (size_t)restart * restart * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(small_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         GM_MAXR * GM_MAXR * (int)sizeof(double));
-    attr_set = true;
-  }
+  static std::atomic<size_t> attr_bytes{0};
+  ensure_smem_limit((const void*)small_solve_kernel, attr_bytes, (size_t)GM_MAXR * GM_MAXR * sizeof(double));
   small_solve_kernel<<<1, 256, smem, st>>>(gs);
 }
 void gm_snapshot(const GState* gs, GHostView* v, cudaStream_t st) { snapshot_kernel<<<1, 1, 0, st>>>(gs, v); }

@@ -417,11 +417,8 @@ template <typename T, int NT>
 void launch_precond_march(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                           cudaStream_t st) {
   const size_t smem = (size_t)d.nz * NT * sizeof(T);
-  static size_t attr_bytes = 0;  // per instantiation
-  if (smem > 48 * 1024 && smem > attr_bytes) {
-    cudaFuncSetAttribute(precond_march_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_bytes = smem;
-  }
+  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  ensure_smem_limit((const void*)precond_march_kernel<T, NT>, attr_bytes, smem);
   // u and v pass straight through (steppers.py:247-249) unless aliased
   if (out.f[0] != r.f[0])
     cudaMemcpyAsync(out.f[0], r.f[0], sizeof(T) * field_size(d, LOC_U), cudaMemcpyDeviceToDevice, st);
@@ -434,11 +431,8 @@ template <typename T, int PT, int PC>
 void launch_precond_tile(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                          cudaStream_t st) {
   const size_t smem = (size_t)(5 * d.nz + 1) * PC * sizeof(T);
-  static size_t attr_bytes = 0;  // per instantiation
-  if (smem > 48 * 1024 && smem > attr_bytes) {
-    cudaFuncSetAttribute(precond_tile_kernel<T, PT, PC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_bytes = smem;
-  }
+  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  ensure_smem_limit((const void*)precond_tile_kernel<T, PT, PC>, attr_bytes, smem);
   dim3 grd((d.nx + PC - 1) / PC, d.ny);
   precond_tile_kernel<T, PT, PC><<<grd, PT, smem, st>>>(d, c, r, out, active);
 }

@@ -144,3 +144,26 @@ def test_explicit_tendencies_vjp_matches_autograd(periodic):
     for kn, kr in (("u", "u"), ("v", "v"), ("w", "w"), ("pi", "pi_p"), ("eta_dot", "eta_dot"), ("th_p", "th_p")):
         err = rel_l2(g[kn], gs[kr])
         assert err < 1e-11, (kn, err)
+
+
+def test_ensemble_vjp_concurrent_matches_sequential():
+    """Members driven concurrently (own stream and host thread each) give the
+    gradients of the same members one after another.  Open boundaries only:
+    on a periodic axis the transposed system is inconsistent and its GMRES
+    runs to maxiter, so its result follows the atomic summation order of
+    the scatter kernels, concurrent or not."""
+    from suetes_b200.adjoint import ensemble_trajectory_vjp, trajectory_vjp
+    members = []
+    for periodic, nx in (((), 12), ((), 10), ((), 14)):
+        st, s0, p = _setup(periodic, nx=nx)
+        members.append((st, st.to_device_state(s0), None))
+
+    def objective(m, n, s):
+        return (s["w"] ** 2).sum() * (m + 1) if n == 2 else None
+
+    conc = ensemble_trajectory_vjp(members, 2, objective, wrt=("th_p", "u"))
+    for m, (st, ds, bc) in enumerate(members):
+        J, g = trajectory_vjp(st, ds, 2, lambda n, s: objective(m, n, s), bc_fn=bc, wrt=("th_p", "u"))
+        assert abs(float(conc[m][0]) - float(J)) <= 1e-12 * abs(float(J)), m
+        for k in ("th_p", "u"):
+            assert rel_l2(conc[m][1][k], g[k]) < 1e-10, (m, k)
