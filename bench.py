@@ -241,9 +241,21 @@ def run_reference(args):
             "config": {"workload": f"mountain wave {args.nx}x{args.ny}x{args.nz}, dt 8 s, restart 30",
                        "sample_window": f"{args.cpu_window}x{args.cpu_window}x{args.nz}"},
             "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "reference_runtime": jax_probe()},
             "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def jax_probe():
+    """Whether the reference's own JAX core could run on this host: the JAX
+    version (None when ``import jax`` fails) and the host's CPU count.  Without
+    JAX the CPU baseline is the float64 oracle restatement, not the reference."""
+    try:
+        import jax  # noqa: F401
+        ver = getattr(jax, "__version__", "unknown")
+    except Exception:
+        ver = None
+    return {"jax_version": ver, "cpu_count": os.cpu_count()}
 
 
 def timed_device_steps(stepper, ds0, relax, steps, warmup, world, timing_class=None):
@@ -810,7 +822,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         v, threads, sample, _ = cpu_leg(2, 1, args.cpu_window, nz, args.tol64)
         line["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
-                                "sample": sample}
+                                "sample": sample, "reference_runtime": jax_probe()}
     if rank == 0:
         print(json.dumps(line), flush=True)
     barrier(world)
