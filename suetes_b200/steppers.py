@@ -496,14 +496,26 @@ class SISLStepper3D:
                 out[k] = v
         return out
 
-    def integrate(self, state, t_start, num_steps, forcing, bc_fn):
-        """lax.scan over ``step`` (steppers.py:692-714), device resident."""
+    def integrate(self, state, t_start, num_steps, forcing, bc_fn, graph=True):
+        """lax.scan over ``step`` (steppers.py:692-714), device resident.
+
+        With ``graph`` (and at least 4 steps) the steps replay two captured
+        CUDA graphs (``PingPong``: every GMRES restart loop decided on the
+        device, no host synchronisation inside a step), bitwise the eager
+        steps; otherwise one ``sisl_step`` call per step."""
         relax, generic = self._relax_of(bc_fn)
         if generic is not None:
             for n in range(num_steps):
                 state = self.step(state, t_start + n * self.dt, forcing, bc_fn)
             return state
         cur = self.to_device_state(state)
+        if graph and num_steps >= 4:
+            pp = PingPong([(self, cur, relax)])
+            for _ in range(num_steps - pp.steps_done):
+                pp.step()
+            if pp.k:
+                self.last_info = pp.info(0)
+            return self.from_device_state(pp.current()[0])
         ring = StateRing(cur.core)
         for _ in range(num_steps):
             nxt = ring.next_output(cur)
