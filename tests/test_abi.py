@@ -65,3 +65,12 @@ def test_argument_validation_without_gpu():
     assert lib.sisl_core_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(b), None, ctypes.byref(h)) == -1
     assert lib.sisl_step(None, None, None, None, None, 0, None, None) == -1
     assert lib.sisl_field_elems(ctypes.byref(_lib.SislGrid(4, 5, 6, 0, 0, 0, 1.0, 1.0, 1.0)), 1) == 5 * 5 * 6
+    # the reverse-mode entry points reject missing arguments the same way
+    nul6, nul10 = (ctypes.c_void_p * 6)(), (ctypes.c_void_p * 10)()
+    assert lib.sisl_step_vjp(None, None, nul10, None, None, None, None, 0, None, None) == -1
+    assert lib.sisl_explicit_tendencies_vjp(None, nul6, nul6, None, nul6, None, 0, None) == -1
+    assert lib.sisl_ffsl_advect_vjp(None, None, None, None, None, None, None, None, None, None, None, 0,
+                                    None) == -1
+    assert lib.sisl_ffsl_lines_vjp(_lib.SISL_F32, 0, 4, None, None, 0, None, None, None, None, 0, None) == -1
+    assert lib.sisl_ffsl_lines_vjp_workspace_bytes(16, 8) >= 2 * 17 * 8 * 8
+    assert lib.sisl_ffsl_lines_vjp_workspace_bytes(0, 8) == 0
