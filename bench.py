@@ -783,40 +783,50 @@ def run_ours(args):
 
     # ---- end to end through the public API with host state ----
     if not args.no_e2e:
-        host = {k: (v.detach().to("cpu").pin_memory() if torch.is_tensor(v) else v) for k, v in s32.items()}
+        def pinned_like(t):  # page-locked host twin with the same (x-fastest) strides: one DMA per copy
+            return torch.empty_strided(tuple(t.shape), tuple(t.stride()), dtype=t.dtype, pin_memory=True)
+        host = {}
+        for k, v in s32.items():
+            if torch.is_tensor(v):
+                host[k] = pinned_like(v)
+                host[k].copy_(v)
+            else:
+                host[k] = v
         keys = [k for k, v in host.items() if torch.is_tensor(v)]
         h2d = sum(host[k].numel() * host[k].element_size() for k in keys)
-        out_host = None
         e2e_steps = max(3, min(K, 10))
-        st = host
-        for n in range(2):  # warm-up of the host path
+        outs = None  # two sets of pinned result buffers, alternated (allocated once, like a host model)
+
+        def e2e_step(st, n):
+            nonlocal outs
             dev = {k: (v.to(f"cuda:{local}", non_blocking=True) if torch.is_tensor(v) else v) for k, v in st.items()}
-            res = st32.step(dev, 0.0, None, bc)
+            res = st32.step(dev, n * 8.0, None, bc)
+            if outs is None:
+                outs = [{k: pinned_like(res[k]) for k in keys} for _ in range(2)]
+            nxt = outs[n % 2]
+            for k in keys:
+                nxt[k].copy_(res[k], non_blocking=True)
+            return dict(nxt, is_first_step=0.0)
+
+        st = host
+        for n in range(3):  # warm-up of exactly the timed path
+            st = e2e_step(st, n)
         torch.cuda.synchronize()
+        st = host
         barrier(world)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record()
-        d2h = 0
         for n in range(e2e_steps):
-            dev = {k: (v.to(f"cuda:{local}", non_blocking=True) if torch.is_tensor(v) else v) for k, v in st.items()}
-            res = st32.step(dev, n * 8.0, None, bc)
-            nxt = {}
-            d2h = 0
-            for k in keys:
-                t = res[k]
-                h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-                h.copy_(t, non_blocking=True)
-                nxt[k] = h
-                d2h += t.numel() * t.element_size()
-            nxt["is_first_step"] = 0.0
-            st = nxt
+            st = e2e_step(st, n)
         t1.record()
         torch.cuda.synchronize()
+        d2h = sum(st[k].numel() * st[k].element_size() for k in keys)
         e2e_ms = dist_max(t0.elapsed_time(t1), world)
         line["e2e"] = {"value": world * cells * e2e_steps / (e2e_ms / 1e3), "unit": "cell-steps/s",
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                       "api": "SISLStepper3D.step(state in pinned host memory)"}
+                       "api": "SISLStepper3D.step(state in pinned host memory, results copied back to "
+                              "two alternating pinned buffer sets)"}
 
     # ---- CPU baseline (rank 0, one GPU) ----
     if rank == 0 and world == 1 and not args.no_cpu:
