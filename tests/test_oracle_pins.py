@@ -298,3 +298,75 @@ def test_ffsl_clip_tie_passes_half_the_cotangent():
     # out[0] = Md(1) - Md(0); Md(0) at the tie dep = 0 has slope M(1) - M(0) = s[0]
     assert float(g[0, 0]) == pytest.approx(0.5 * float(s[0, 0]))
     assert float(g[0, 1]) == pytest.approx(-float(s[0, 1]))
+
+
+def _sine(x, y, z, lx, ly, lz):
+    return torch.sin(2 * math.pi * x / lx) * torch.cos(2 * math.pi * y / ly) * torch.sin(2 * math.pi * z / lz)
+
+
+def test_tricubic_convergence_order():
+    """verification/sisl_component_convergence.py:53-90: interpolating a sine
+    field at a fixed fractional offset converges at order 3-4."""
+    errs = []
+    for N in (16, 32, 64):
+        lx = 10000.0
+        dx = lx / N
+        g = RegionalGrid3D(N, N, N, dx, dx, dx, 0.0, 0.0)
+        X, Y, Z = torch.meshgrid(g.x_m, g.y_m, g.z_m, indexing="ij")
+        Xt, Yt, Zt = X + 0.37 * dx, Y + 0.23 * dx, Z + 0.45 * dx
+        co = torch.stack([(Xt + lx / 2) / dx - 0.5, (Yt + lx / 2) / dx - 0.5, Zt / dx - 0.5])
+        out = tensor_product_interp_3d(_sine(X, Y, Z, lx, lx, lx), co)
+        ex, m = _sine(Xt, Yt, Zt, lx, lx, lx), N // 4
+        errs.append(float(torch.sqrt(torch.mean((out - ex)[m:-m, m:-m, m:-m] ** 2))))
+    rates = [math.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert all(2.8 < r < 4.2 for r in rates), (errs, rates)
+
+
+def test_trajectory_convergence_order():
+    """verification/sisl_component_convergence.py:147-197: the midpoint
+    departure points of the strain flow u = a x against the exact
+    characteristic x exp(-a dt) converge at local order 3."""
+    r, L, Lz, a = 64, 2.0e6, 1.0e4, 1.0e-4
+    dx = L / r
+    g = RegionalGrid3D(r, r, r, dx, dx, Lz / r, 0.0, 0.0)
+    for k in g.m_factors:
+        g.m_factors[k] = torch.ones_like(g.m_factors[k])
+    ph = build_physics(g)
+    Xu, _, _ = torch.meshgrid(g.x_c, g.y_m, g.z_m, indexing="ij")
+    Xm, _, _ = torch.meshgrid(g.x_m, g.y_m, g.z_m, indexing="ij")
+    st = {"u": a * Xu, "v": z(r, r + 1, r), "w": z(r, r, r + 1), "eta_dot": z(r, r, r + 1)}
+    errs = []
+    for dt in (400.0, 200.0, 100.0, 50.0):
+        c = SemiLagrangianAdvector3D(g, ph, dt).compute_departure_indices(st, loc="m", iterations=8)
+        ex, m = (Xm * math.exp(-a * dt) + L / 2) / dx - 0.5, r // 4
+        errs.append(dx * float(torch.sqrt(torch.mean((c[0] - ex)[m:-m, m:-m, m:-m] ** 2))))
+    rates = [math.log2(errs[i] / errs[i + 1]) for i in range(3)]
+    assert all(2.8 < q < 3.2 for q in rates), (errs, rates)
+
+
+def build_physics(g):
+    from oracle.euler import Euler3D
+    return Euler3D(g, CGridOperator3D(g), C, dt=1.0)
+
+
+@pytest.mark.parametrize("r", [8, 16])
+def test_gmres_inversion_sweep(r):
+    """verification/sisl_component_convergence.py:203-260: the preconditioned
+    GMRES (tol 1e-12, the solver's default restart 20 / maxiter 20) inverts
+    the Helmholtz operator of a 60N grid to relative residual < 1e-9."""
+    from oracle.euler import Euler3D
+    L, Lz, dt = 2.0e6, 1.0e4, 60.0
+    g = RegionalGrid3D(r, r, r, L / r, L / r, Lz / r, 60.0, 30.0)
+    ph = Euler3D(g, CGridOperator3D(g), C, dt=dt, N_bv=0.01)
+    sol = SemiImplicitSolver3D(ph, dt, alpha=0.55, solver_tol=1e-12)
+    gen = torch.Generator().manual_seed(42)
+    U = lambda *s: torch.rand(*s, generator=gen, dtype=F64)
+    x = {"u": U(r + 1, r, r) * 5.0, "v": U(r, r + 1, r) * 5.0, "w": U(r, r, r + 1) * 0.1,
+         "pi": U(r, r, r) * 0.001, "eta_dot": U(r, r, r + 1) * 0.001}
+    for k in ("w", "eta_dot"):
+        x[k][:, :, 0] = 0.0
+        x[k][:, :, -1] = 0.0
+    bg = bgp(ph)
+    rhs = ph.linear_operator(x, bg, dt, alpha=0.55)
+    xn = sol.solve(rhs, bg)
+    assert float(sol.relative_residual(xn, rhs, bg)) < 1e-9
