@@ -359,6 +359,24 @@ typedef struct SislStepGraph SislStepGraph;
 int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
                            const SislRelaxation* const* relax, void* const* ws, const size_t* ws_bytes,
                            void* stream, SislStepGraph** out);
+/* sisl_step_graph_create whose members also record their two solve
+ * outputs, as sisl_step_taped: solves holds 10 pointers per member (member
+ * m at solves[10 m ..]), NULL entries skipped; solves may be NULL. */
+int sisl_step_graph_create_taped(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                                 const SislRelaxation* const* relax, void* const* solves, void* const* ws,
+                                 const size_t* ws_bytes, void* stream, SislStepGraph** out);
+/* The reverse sweep of a step (sisl_step_vjp) of n members as one CUDA graph:
+ * member m maps out_bars[m] to in_bars[m] with its input ins[m] and the ten
+ * recorded solutions solves[10 m ..]; the transposed GMRES loops are
+ * device-decided conditional nodes, so a launch needs no host
+ * synchronisation (the command-buffer form of the step's VJP).  ws[m]:
+ * sisl_workspace_bytes(cores[m], SISL_WS_STEP_VJP) bytes.  Statistics of
+ * the transposed solves: sisl_step_graph_info; release with
+ * sisl_step_graph_destroy. */
+int sisl_step_vjp_graph_create(int n, SislCore* const* cores, const SislState* ins, void* const* solves,
+                               const SislRelaxation* const* relax, const SislState* out_bars,
+                               const SislState* in_bars, void* const* ws, const size_t* ws_bytes, void* stream,
+                               SislStepGraph** out);
 int sisl_step_graph_launch(SislStepGraph* graph, void* stream);
 /* Solve statistics of the last replay for one member (synchronises stream);
  * returns SISL_NOT_CONVERGED / SISL_ERR_NONFINITE like sisl_step. */

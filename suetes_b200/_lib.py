@@ -140,6 +140,12 @@ PROTOTYPES = {
     "sisl_explicit_tendencies_vjp": (ctypes.c_int, [vp, vp * 6, vp * 6, vp, vp * 6, vp, ctypes.c_size_t, vp]),
     "sisl_step_graph_create": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
                                               vp, vp, vp, vp, ctypes.POINTER(vp)]),
+    "sisl_step_graph_create_taped": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState),
+                                                    ctypes.POINTER(SislState), vp, vp, vp, vp, vp,
+                                                    ctypes.POINTER(vp)]),
+    "sisl_step_vjp_graph_create": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState), vp, vp,
+                                                  ctypes.POINTER(SislState), ctypes.POINTER(SislState), vp, vp, vp,
+                                                  ctypes.POINTER(vp)]),
     "sisl_step_graph_launch": (ctypes.c_int, [vp, vp]),
     "sisl_step_graph_info": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SislStepInfo), vp]),
     "sisl_step_graph_destroy": (ctypes.c_int, [vp]),

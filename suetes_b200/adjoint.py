@@ -502,3 +502,161 @@ def ensemble_trajectory_vjp(members, num_steps, objective, checkpoint_every=1, w
     for s in streams:
         base.wait_stream(s)
     return out
+
+
+def _state_struct(fields, is_first_step=0.0):
+    """A SislState of the tensors in ``fields`` (STATE_KEYS names; missing: NULL)."""
+    s = _lib.SislState()
+    for k, t in fields.items():
+        if t is not None:
+            setattr(s, k, t.data_ptr())
+    s.is_first_step = float(is_first_step)
+    return s
+
+
+class StepVJPGraph:
+    """The reverse sweep of one step of one or more members as a single CUDA
+    graph (``sisl_step_vjp_graph_create``): member m maps the output
+    cotangents ``out_bar`` to the input cotangents ``in_bar`` (dicts of
+    fixed tensors by ``STATE_KEYS`` name) with its input ``DeviceState`` and
+    the ten solve outputs its taped step recorded; the transposed GMRES loops
+    are decided on the device.  ``members``: ``(stepper, ds_in, tape, relax,
+    out_bar, in_bar)``, distinct cores."""
+
+    def __init__(self, members):
+        from .core import stream_ptr
+        from .steppers import SOLVE_METHODS
+        self.lib = _lib.load()
+        n = len(members)
+        self._keep = []
+        cores, ins, obs, ibs, relax, ws, nbytes, tps = [], [], [], [], [], [], [], []
+        for stepper, din, tape, rl, ob, ib in members:
+            core = din.core
+            if core in cores:
+                raise ValueError("every member needs its own core")
+            sol = stepper.implicit_solver
+            core.set_adjoint(sol.transpose_tol, sol.adjoint_normalize,
+                             None if sol.transpose_method is None else SOLVE_METHODS[sol.transpose_method])
+            cores.append(core)
+            ins.append(din.c_struct())
+            obs.append(_state_struct(ob))
+            ibs.append(_state_struct(ib))
+            relax.append(ctypes.pointer(rl.c_struct(core)) if rl is not None else None)
+            buf, nb = core.workspace(_lib.WS_STEP_VJP)
+            ws.append(buf)
+            nbytes.append(nb)
+            tps += [t.data_ptr() for t in tape]
+            self._keep += [din, tape, rl, ob, ib, buf]
+        self.device = cores[0].device
+        carr = (ctypes.c_void_p * n)(*[c.handle.value for c in cores])
+        iarr = (_lib.SislState * n)(*ins)
+        oarr = (_lib.SislState * n)(*obs)
+        barr_ = (_lib.SislState * n)(*ibs)
+        tarr = (ctypes.c_void_p * (10 * n))(*tps)
+        rarr = (ctypes.c_void_p * n)(*[ctypes.cast(r, ctypes.c_void_p).value if r is not None else None
+                                      for r in relax])
+        warr = (ctypes.c_void_p * n)(*[b.data_ptr() for b in ws])
+        narr = (ctypes.c_size_t * n)(*nbytes)
+        self._keep += [carr, iarr, oarr, barr_, tarr, rarr, warr, narr, relax]
+        h = ctypes.c_void_p()
+        check(self.lib.sisl_step_vjp_graph_create(n, carr, iarr, tarr, rarr, oarr, barr_, warr, narr,
+                                                  stream_ptr(self.device), ctypes.byref(h)),
+              "sisl_step_vjp_graph_create")
+        self.handle, self.n = h, n
+
+    def launch(self):
+        from .core import stream_ptr
+        check(self.lib.sisl_step_graph_launch(self.handle, stream_ptr(self.device)), "sisl_step_graph_launch")
+
+    def info(self, member=0):
+        from .core import stream_ptr
+        inf = _lib.SislStepInfo()
+        rc = self.lib.sisl_step_graph_info(self.handle, int(member), ctypes.byref(inf), stream_ptr(self.device))
+        check(rc, "sisl_step_graph_info")
+        return {"status": rc, "solves": [inf.solve[1].as_dict(), inf.solve[0].as_dict()]}
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self.lib.sisl_step_graph_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+class EnsembleVJPGraph:
+    """Value and gradient of ``J_m = sum_n objective(m, n, state_m,n)`` over
+    ``num_steps`` steps for every member of an ensemble, replayed as CUDA
+    graphs: per step one graph advancing every member while recording its
+    solves, and one graph of every member's reverse sweep (2 ``num_steps``
+    graph launches per evaluation, no host synchronisation inside a step).
+    Every state, tape and cotangent buffer is allocated once; ``run`` copies
+    the starting states in.  The objective's own cotangents are added
+    between the reverse launches (stream-ordered).
+
+    ``members``: ``[(stepper, ds0, relax)]`` with distinct cores; ``ds0``
+    fixes the shapes and the first-step flag of every later start."""
+
+    def __init__(self, members, num_steps):
+        from .steppers import DeviceState, StepGraph
+        N = int(num_steps)
+        if N < 1:
+            raise ValueError("num_steps must be >= 1")
+        self.N, self.members = N, members
+        self.first = [float(ds0.is_first_step) for _, ds0, _ in members]
+        self.S, self.T, self.B = [], [], []
+        for stepper, ds0, rl in members:
+            core = ds0.core
+            S = [DeviceState(core, None, self.first[len(self.S)] if n == 0 else 0.0) for n in range(N + 1)]
+            for n in range(N + 1):
+                for k in S[n].t:
+                    S[n].t[k].zero_()
+            T = [[core.new(l) for l in LOCS5 + LOCS5] for _ in range(N)]
+            B = [{k: core.new(l).zero_() for k, l in DeviceState.FIELDS} for _ in range(N + 1)]
+            self.S.append(S)
+            self.T.append(T)
+            self.B.append(B)
+        M = len(members)
+        self.fwd = [StepGraph([(members[m][0], self.S[m][n], self.S[m][n + 1], members[m][2]) for m in range(M)],
+                              tapes=[self.T[m][n] for m in range(M)]) for n in range(N)]
+        self.rev = [StepVJPGraph([(members[m][0], self.S[m][n], self.T[m][n], members[m][2], self.B[m][n + 1],
+                                   self.B[m][n]) for m in range(M)]) for n in range(N)]
+
+    def run(self, starts, objective, wrt=("th_p",)):
+        """``starts``: a ``DeviceState`` per member (same shapes and first-step
+        flag as at construction); ``objective(m, n, state)`` as for
+        ``ensemble_trajectory_vjp``.  Returns ``[(J_m, grads_m)]``."""
+        M, N = len(self.members), self.N
+        for m, ds in enumerate(starts):
+            if float(ds.is_first_step) != self.first[m]:
+                raise ValueError("a start's first-step flag differs from the captured one")
+            for k, t in self.S[m][0].t.items():
+                t.copy_(ds.t[k])
+        for g in self.fwd:
+            g.launch()
+        keys = list(STATE_KEYS)
+        J = [torch.zeros((), dtype=F64, device=self.S[0][0].core.device) for _ in range(M)]
+        G = [[None] * (N + 1) for _ in range(M)]  # objective cotangents per member and state
+        for m in range(M):
+            for n in range(1, N + 1):
+                after = {k: v.detach().requires_grad_(True) for k, v in self.S[m][n].t.items()}
+                with torch.enable_grad():
+                    val = objective(m, n, dict(after, is_first_step=0.0))
+                    if val is None or not val.requires_grad:
+                        continue
+                    J[m] = J[m] + val.detach().double()
+                    gs = torch.autograd.grad(val, [after[k] for k in keys], allow_unused=True)
+                G[m][n] = {k: g for k, g in zip(keys, gs) if g is not None}
+        for m in range(M):
+            for t in self.B[m][N].values():
+                t.zero_()
+            for k, g in (G[m][N] or {}).items():
+                self.B[m][N][k].add_(g)
+        for n in range(N - 1, -1, -1):
+            if n + 1 < N:  # the reverse of step n + 1 wrote B[n + 1]; add the objective's own cotangent
+                for m in range(M):
+                    for k, g in (G[m][n + 1] or {}).items():
+                        self.B[m][n + 1][k].add_(g)
+            self.rev[n].launch()
+        return [(J[m], {k: self.B[m][0][k] for k in wrt}) for m in range(M)]

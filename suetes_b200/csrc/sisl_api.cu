@@ -591,7 +591,7 @@ int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, co
 // unscale (x = S_out x_s), GMRES on A^T from a zero guess, rescale (b_s = S_in b).
 template <typename T>
 int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> xbar, const CVec5<T>* x0,
-                             Vec5<T> bbar, cudaStream_t st, SislSolveInfo* info) {
+                             Vec5<T> bbar, cudaStream_t st, SislSolveInfo* info, GDevInfo* dev_info = nullptr) {
   const Dims& d = c->d;
   {
     KScope k(c, SISL_K_OTHER, st);
@@ -617,7 +617,7 @@ int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<
     scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.bg(), g.npad, g.scal, 0);
     if (x0) scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.xg(), g.npad, g.scal, 0);
   }
-  int rc = gmres_run<T>(c, cf, g, st, info, 1);
+  int rc = gmres_run<T>(c, cf, g, st, info, 1, dev_info);
   if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
   if (norm_rhs) {
     KScope k(c, SISL_K_OTHER, st);
@@ -869,7 +869,7 @@ VWork<T> carve_vjp(Carver& cv, const Dims& d) {
 template <typename T>
 int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const SislRelaxation* relax,
                   const SislState* ob, const SislState* ib, void* ws, size_t ws_bytes, cudaStream_t st,
-                  SislStepInfo* info) {
+                  SislStepInfo* info, GDevInfo* dev_info = nullptr) {
   const Dims& d = c->d;
   const Coef<T> cf = coef_of<T>(c);
   Carver cv{(char*)ws};
@@ -993,7 +993,7 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
     Vec5<T> bo;
     for (int q = 0; q < 5; ++q) { xb.f[q] = it ? v.x2b[q] : v.x1b[q]; bo.f[q] = v.bb[q]; }
     SislSolveInfo si{};
-    int rc = solve_transpose_physical<T>(c, cf, w.g, xb, nullptr, bo, st, &si);
+    int rc = solve_transpose_physical<T>(c, cf, w.g, xb, nullptr, bo, st, &si, dev_info ? dev_info + it : nullptr);
     if (info) info->solve[it] = si;
     if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
     if (rc != SISL_OK && status == SISL_OK) status = rc;
@@ -1669,35 +1669,22 @@ void destroy_graph(SislStepGraph* g) {
   for (cudaEvent_t e : g->events) cudaEventDestroy(e);
   delete g;
 }
-}  // namespace
 
-extern "C" {
-
-int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
-                           const SislRelaxation* const* relax, void* const* ws, const size_t* ws_bytes, void* stream,
-                           SislStepGraph** out) {
-  if (!out || n < 1 || !cores || !ins || !outs || !ws || !ws_bytes) return SISL_ERR_ARG;
-  for (int m = 0; m < n; ++m) {
-    SislCore* c = cores[m];
-    if (!c || !ws[m] || ws_bytes[m] < sisl_workspace_bytes(c, SISL_WS_STEP)) return SISL_ERR_WORKSPACE;
-    const SislState& a = ins[m];
-    const SislState& b = outs[m];
-    const void* need[] = {a.u, a.v, a.w, a.eta_dot, a.pi_p, a.th_p, b.u, b.v, b.w, b.eta_dot, b.pi_p, b.th_p};
-    for (const void* p : need)
-      if (!p) return SISL_ERR_ARG;
-    if (a.is_first_step != 1.0 && (!a.u_prev || !a.v_prev || !a.eta_dot_prev)) return SISL_ERR_ARG;
-    for (int q = 0; q < m; ++q)
-      if (cores[q] == c) return SISL_ERR_ARG;  // a core's side stream serves one branch
-  }
+// Captures one branch per member into a new SislStepGraph: a fork on a
+// private stream (the caller's may be the legacy stream, which cannot be
+// captured), member m's work on its own stream with its GMRES loop bodies
+// captured on a side stream, a join, then instantiation.  record(m, stream,
+// dev_info) issues member m's work; dev_info holds two solve summaries.
+template <typename F>
+int capture_members(int n, SislCore* const* cores, F&& record, SislStepGraph** out) {
   SislStepGraph* g = new (std::nothrow) SislStepGraph();
   if (!g) return SISL_ERR_ARG;
   g_last_error[0] = 0;
   g->n = n;
-  (void)stream;  // the graph is captured on a private stream (the caller's may be the legacy stream)
   cudaStream_t st = nullptr;
   auto fail = [&](int rc) {
     cudaStreamCaptureStatus cs;
-    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+    if (st && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
       cudaGraph_t junk = nullptr;
       cudaStreamEndCapture(st, &junk);
       if (junk) cudaGraphDestroy(junk);
@@ -1731,15 +1718,10 @@ int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, 
     cudaStream_t ms = g->streams[m];
     if (cuda_failed(cudaStreamWaitEvent(ms, g->events[n], 0), "cudaStreamWaitEvent(fork)")) return fail(SISL_ERR_CUDA);
     c->cap_side = g->streams[n + m];
-    const SislRelaxation* rl = relax ? relax[m] : nullptr;
-    int rc = (c->grid.dtype == SISL_F64)
-                 ? step_impl<double>(c, &ins[m], &outs[m], rl, ws[m], ws_bytes[m], ms, nullptr, nullptr,
-                                     g->dinfo + 2 * m)
-                 : step_impl<float>(c, &ins[m], &outs[m], rl, ws[m], ws_bytes[m], ms, nullptr, nullptr,
-                                    g->dinfo + 2 * m);
+    const int rc = record(m, ms, g->dinfo + 2 * m);
     c->cap_side = nullptr;
     if (rc < 0) {
-      if (!g_last_error[0]) snprintf(g_last_error, sizeof(g_last_error), "step of member %d: status %d", m, rc);
+      if (!g_last_error[0]) snprintf(g_last_error, sizeof(g_last_error), "member %d: status %d", m, rc);
       return fail(rc);
     }
     if (cuda_failed(cudaEventRecord(g->events[m], ms), "cudaEventRecord(join)")) return fail(SISL_ERR_CUDA);
@@ -1749,6 +1731,88 @@ int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, 
   if (cuda_failed(cudaGraphInstantiate(&g->exec, g->graph, 0), "cudaGraphInstantiate")) return fail(SISL_ERR_CUDA);
   *out = g;
   return SISL_OK;
+}
+
+// Argument checks shared by the graph builders: distinct cores (a core's
+// side stream serves one branch), workspaces of the given kind.
+int check_members(int n, SislCore* const* cores, void* const* ws, const size_t* ws_bytes, int ws_kind) {
+  for (int m = 0; m < n; ++m) {
+    SislCore* c = cores[m];
+    if (!c || !ws[m] || ws_bytes[m] < sisl_workspace_bytes(c, ws_kind)) return SISL_ERR_WORKSPACE;
+    for (int q = 0; q < m; ++q)
+      if (cores[q] == c) return SISL_ERR_ARG;
+  }
+  return SISL_OK;
+}
+
+bool step_args_ok(const SislState& a, const SislState& b) {
+  const void* need[] = {a.u, a.v, a.w, a.eta_dot, a.pi_p, a.th_p, b.u, b.v, b.w, b.eta_dot, b.pi_p, b.th_p};
+  for (const void* p : need)
+    if (!p) return false;
+  return a.is_first_step == 1.0 || (a.u_prev && a.v_prev && a.eta_dot_prev);
+}
+}  // namespace
+
+extern "C" {
+
+int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                           const SislRelaxation* const* relax, void* const* ws, const size_t* ws_bytes, void* stream,
+                           SislStepGraph** out) {
+  return sisl_step_graph_create_taped(n, cores, ins, outs, relax, nullptr, ws, ws_bytes, stream, out);
+}
+
+int sisl_step_graph_create_taped(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                                 const SislRelaxation* const* relax, void* const* solves, void* const* ws,
+                                 const size_t* ws_bytes, void* stream, SislStepGraph** out) {
+  if (!out || n < 1 || !cores || !ins || !outs || !ws || !ws_bytes) return SISL_ERR_ARG;
+  int rc = check_members(n, cores, ws, ws_bytes, SISL_WS_STEP);
+  if (rc) return rc;
+  for (int m = 0; m < n; ++m)
+    if (!step_args_ok(ins[m], outs[m])) return SISL_ERR_ARG;
+  (void)stream;  // captured on a private stream
+  return capture_members(
+      n, cores,
+      [&](int m, cudaStream_t ms, GDevInfo* di) {
+        SislCore* c = cores[m];
+        const SislRelaxation* rl = relax ? relax[m] : nullptr;
+        void* const* tape = solves ? solves + 10 * m : nullptr;
+        return (c->grid.dtype == SISL_F64)
+                   ? step_impl<double>(c, &ins[m], &outs[m], rl, ws[m], ws_bytes[m], ms, nullptr, tape, di)
+                   : step_impl<float>(c, &ins[m], &outs[m], rl, ws[m], ws_bytes[m], ms, nullptr, tape, di);
+      },
+      out);
+}
+
+int sisl_step_vjp_graph_create(int n, SislCore* const* cores, const SislState* ins, void* const* solves,
+                               const SislRelaxation* const* relax, const SislState* out_bars,
+                               const SislState* in_bars, void* const* ws, const size_t* ws_bytes, void* stream,
+                               SislStepGraph** out) {
+  if (!out || n < 1 || !cores || !ins || !solves || !out_bars || !in_bars || !ws || !ws_bytes) return SISL_ERR_ARG;
+  int rc = check_members(n, cores, ws, ws_bytes, SISL_WS_STEP_VJP);
+  if (rc) return rc;
+  for (int m = 0; m < n; ++m) {
+    const SislState& a = ins[m];
+    const SislState& ib = in_bars[m];
+    const void* need[] = {a.u, a.v, a.w, a.eta_dot, a.pi_p, a.th_p, ib.u, ib.v, ib.w, ib.eta_dot, ib.pi_p, ib.th_p};
+    for (const void* p : need)
+      if (!p) return SISL_ERR_ARG;
+    if (a.is_first_step != 1.0 && (!a.u_prev || !a.v_prev || !a.eta_dot_prev)) return SISL_ERR_ARG;
+    for (int q = 0; q < 10; ++q)
+      if (!solves[10 * m + q]) return SISL_ERR_ARG;
+  }
+  (void)stream;  // captured on a private stream
+  return capture_members(
+      n, cores,
+      [&](int m, cudaStream_t ms, GDevInfo* di) {
+        SislCore* c = cores[m];
+        const SislRelaxation* rl = relax ? relax[m] : nullptr;
+        return (c->grid.dtype == SISL_F64)
+                   ? step_vjp_impl<double>(c, &ins[m], solves + 10 * m, rl, &out_bars[m], &in_bars[m], ws[m],
+                                           ws_bytes[m], ms, nullptr, di)
+                   : step_vjp_impl<float>(c, &ins[m], solves + 10 * m, rl, &out_bars[m], &in_bars[m], ws[m],
+                                          ws_bytes[m], ms, nullptr, di);
+      },
+      out);
 }
 
 int sisl_step_graph_launch(SislStepGraph* g, void* stream) {

@@ -554,7 +554,9 @@ class StepGraph:
     statistics of the last launch.  ``PingPong`` alternates two graphs for
     repeated steps."""
 
-    def __init__(self, members):
+    def __init__(self, members, tapes=None):
+        """``tapes``: optional per-member lists of the ten solve-output
+        tensors to record (``sisl_step_graph_create_taped``)."""
         self.lib = _lib.load()
         n = len(members)
         cores, ins, outs, relax, ws, nbytes = [], [], [], [], [], []
@@ -585,8 +587,15 @@ class StepGraph:
         self._keep += [carr, iarr, oarr, rarr, warr, barr, relax]
         h = ctypes.c_void_p()
         from .core import stream_ptr
-        check(self.lib.sisl_step_graph_create(n, carr, iarr, oarr, rarr, warr, barr, stream_ptr(self.device),
-                                              ctypes.byref(h)), "sisl_step_graph_create")
+        if tapes is None:
+            check(self.lib.sisl_step_graph_create(n, carr, iarr, oarr, rarr, warr, barr, stream_ptr(self.device),
+                                                  ctypes.byref(h)), "sisl_step_graph_create")
+        else:
+            tarr = (ctypes.c_void_p * (10 * n))(*[t.data_ptr() for tp in tapes for t in tp])
+            self._keep += [tarr, tapes]
+            check(self.lib.sisl_step_graph_create_taped(n, carr, iarr, oarr, rarr, tarr, warr, barr,
+                                                        stream_ptr(self.device), ctypes.byref(h)),
+                  "sisl_step_graph_create_taped")
         self.handle, self.n = h, n
         self.outs = [m[2] for m in members]
 
