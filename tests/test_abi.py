@@ -74,3 +74,8 @@ def test_argument_validation_without_gpu():
     assert lib.sisl_ffsl_lines_vjp(_lib.SISL_F32, 0, 4, None, None, 0, None, None, None, None, 0, None) == -1
     assert lib.sisl_ffsl_lines_vjp_workspace_bytes(16, 8) >= 2 * 17 * 8 * 8
     assert lib.sisl_ffsl_lines_vjp_workspace_bytes(0, 8) == 0
+    out = ctypes.c_void_p()
+    assert lib.sisl_step_graph_create_taped(0, None, None, None, None, None, None, None, None,
+                                            ctypes.byref(out)) == -1
+    assert lib.sisl_step_vjp_graph_create(0, None, None, None, None, None, None, None, None, None,
+                                          ctypes.byref(out)) == -1
