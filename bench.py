@@ -79,7 +79,7 @@ def parse():
     ap.add_argument("--vjp-steps", type=int, default=4,
                     help="trajectory length of the fwd+VJP leg (0 disables it)")
     ap.add_argument("--vjp-checkpoint", type=int, default=1, help="checkpoint interval of the fwd+VJP leg")
-    ap.add_argument("--adj-method", default="batched", choices=["batched", "incremental"],
+    ap.add_argument("--adj-method", default="incremental", choices=["batched", "incremental"],
                     help="GMRES variant of the transposed solves")
     ap.add_argument("--adj-tol32", type=float, default=1e-5,
                     help="GMRES tolerance of the float32 transposed solves (the float64 ones use --tol64)")
