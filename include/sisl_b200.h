@@ -308,6 +308,17 @@ int sisl_step(SislCore* core, const SislState* in, const SislState* out, const S
  * steppers.py:792-850). */
 int sisl_step_taped(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax,
                     void* const solves[10], void* ws, size_t ws_bytes, void* stream, SislStepInfo* info);
+/* SISLStepper3D.step with a physics suite (steppers.py:720-1073 with
+ * Euler3D.get_tendencies' physics call, euler.py:347-366): phys_tend holds
+ * the suite's explicit tendencies of u (u faces), v (v faces), w (w levels)
+ * and th_v (mass points), NULL entries zero; they join the tendencies and
+ * their phys_diff share exactly as the reference adds them.  The suite's
+ * state updates, tracer transport and the caller's bc_fn follow on the
+ * caller's side (sisl_ffsl_advect for tracers); relax may be NULL.  solves
+ * as for sisl_step_taped (may be NULL). */
+int sisl_step_physics(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax,
+                      const void* const phys_tend[4], void* const solves[10], void* ws, size_t ws_bytes,
+                      void* stream, SislStepInfo* info);
 /* Cotangent of one step's input state from the cotangent of its output
  * (the VJP of SISLStepper3D.step under jax.checkpoint, steppers.py:720-1073,
  * 792-850, with the reference's stop_gradient on the departure points and

@@ -57,6 +57,25 @@ class LateralRelaxation:
     def __call__(self, state, forcing):
         raise RuntimeError("LateralRelaxation is applied inside the CUDA step")
 
+    def apply_state(self, state, physics):
+        """The same blend on a reference state dict (full ``th_v`` and
+        ``pi``): thermodynamic fields blend as perturbations from the
+        background, in float64, as the fused step blends them.  Used where
+        other work (a physics suite's state updates) sits between the step
+        and the boundary condition."""
+        out = dict(state)
+        masks = {"u": self.mask_u, "v": self.mask_v, "w": self.mask_m, "th_v": self.mask_m, "pi": self.mask_m}
+        bgs = {"th_v": physics.theta_bg, "pi": physics.pi_bg}
+        for k in self.fields:
+            f = torch.as_tensor(state[k])
+            m = torch.as_tensor(masks[k]).to(device=f.device, dtype=torch.float64)[..., None]
+            ext = self.exterior.get(k, 0.0)
+            ext = ext.to(device=f.device, dtype=torch.float64) if torch.is_tensor(ext) else float(ext)
+            bg = bgs[k].to(device=f.device) if k in bgs else 0.0
+            val = f.double() - bg
+            out[k] = ((1.0 - m) * val + m * ext + bg).to(f.dtype)
+        return out
+
 
 def x_relaxation(grid, width_m, exterior_u, fields=("u", "v", "th_v", "pi")):
     """The cos^2 x-relaxation zone of schaer_mountain_3d/run.py:104-126:

@@ -664,7 +664,7 @@ SWork<T> carve_step(Carver& cv, const Dims& d, int R, bool refine) {
 template <typename T>
 int step_impl(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
               size_t ws_bytes, cudaStream_t st, SislStepInfo* info, void* const* tape = nullptr,
-              GDevInfo* dev_info = nullptr) {
+              GDevInfo* dev_info = nullptr, const void* const* phys = nullptr) {
   const Dims& d = c->d;
   const Coef<T> cf = coef_of<T>(c);
   Carver cv{(char*)ws};
@@ -688,7 +688,9 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
                             (const T*)in->eta_dot_prev, extrap, vt, st);
   }
   // 2. explicit tendencies with hyperdiffusion (euler.py:208-372)
-  ExplicitIn<T> ein{u, v, wv, eta, pp, th, {nullptr, nullptr, nullptr, nullptr}};
+  ExplicitIn<T> ein{u, v, wv, eta, pp, th, {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
+  if (phys)
+    for (int q = 0; q < 4; ++q) ein.extra[q] = (const T*)phys[q];
   if (c->s.nu_h > 0.0) {
     PtrTable<T> t4{}, o4{};
     for (int q = 0; q < 4; ++q) { t4.p[q] = w.htmp[q]; o4.p[q] = w.hyp[q]; }
@@ -1573,6 +1575,24 @@ int sisl_step_taped(SislCore* c, const SislState* in, const SislState* out, cons
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64) return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info, solves);
   return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info, solves);
+}
+
+int sisl_step_physics(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax,
+                      const void* const phys_tend[4], void* const solves[10], void* ws, size_t ws_bytes,
+                      void* stream, SislStepInfo* info) {
+  if (!c || !in || !out || !phys_tend) return SISL_ERR_ARG;
+  const void* need_in[] = {in->u, in->v, in->w, in->eta_dot, in->pi_p, in->th_p};
+  for (const void* p : need_in)
+    if (!p) return SISL_ERR_ARG;
+  if (in->is_first_step != 1.0 && (!in->u_prev || !in->v_prev || !in->eta_dot_prev)) return SISL_ERR_ARG;
+  const void* need_out[] = {out->u, out->v, out->w, out->eta_dot, out->pi_p, out->th_p};
+  for (const void* p : need_out)
+    if (!p) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_STEP)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (c->grid.dtype == SISL_F64)
+    return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info, solves, nullptr, phys_tend);
+  return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info, solves, nullptr, phys_tend);
 }
 
 int sisl_step_vjp(SislCore* c, const SislState* in, void* const solves[10], const SislRelaxation* relax,

@@ -79,7 +79,8 @@ __global__ void __launch_bounds__(256) explicit_kernel(Dims d, Coef<T> c, Explic
     const T thp = lin * T(0.5) * (ld(th, im(d, l, j, k)) + ld(th, im(d, r, j, k)));
     const T vat = T(0.5) * (W.vm(l, j, k) + W.vm(r, j, k));
     const T met = lin * T(0.5) * (W.metric_m(l, j, k) + W.metric_m(r, j, k)) * vat;
-    const T pd = hyp ? T(0.5) * (ld(in.hyper[0], im(d, l, j, k)) + ld(in.hyper[0], im(d, r, j, k))) : T(0);
+    T pd = hyp ? T(0.5) * (ld(in.hyper[0], im(d, l, j, k)) + ld(in.hyper[0], im(d, r, j, k))) : T(0);
+    if (mode != 2 && in.extra[0]) pd += ld(in.extra[0], p);  // physics tendencies join phys_diff (euler.py:347-366)
     const T tend = -cp * (ld(c.thu, p) + thp) * G.gx(i, j, k) + ld(c.fu, h_u(d, i, j)) * vat + met + pd;
     if (mode == 0) {
       out.f[0][p] = ld(in.u, p) + dt * (oma * tend + a * pd);
@@ -95,7 +96,8 @@ __global__ void __launch_bounds__(256) explicit_kernel(Dims d, Coef<T> c, Explic
     const T thp = lin * T(0.5) * (ld(th, im(d, i, l, k)) + ld(th, im(d, i, r, k)));
     const T uat = T(0.5) * (W.um(i, l, k) + W.um(i, r, k));
     const T met = -lin * T(0.5) * (W.metric_m(i, l, k) + W.metric_m(i, r, k)) * uat;
-    const T pd = hyp ? T(0.5) * (ld(in.hyper[1], im(d, i, l, k)) + ld(in.hyper[1], im(d, i, r, k))) : T(0);
+    T pd = hyp ? T(0.5) * (ld(in.hyper[1], im(d, i, l, k)) + ld(in.hyper[1], im(d, i, r, k))) : T(0);
+    if (mode != 2 && in.extra[1]) pd += ld(in.extra[1], p);
     const T tend = -cp * (ld(c.thv, p) + thp) * G.gy(i, j, k) - ld(c.fv, h_v(d, i, j)) * uat + met + pd;
     if (mode == 0) {
       out.f[1][p] = ld(in.v, p) + dt * (oma * tend + a * pd);
@@ -110,7 +112,8 @@ __global__ void __launch_bounds__(256) explicit_kernel(Dims d, Coef<T> c, Explic
     const int p = iw(d, i, j, k);
     const T thp = lin * T(0.5) * (ld(th, im(d, i, j, kl)) + ld(th, im(d, i, j, kr)));
     const T thw = ld(c.thw, p);
-    const T pd = hyp ? T(0.5) * (ld(in.hyper[2], im(d, i, j, kl)) + ld(in.hyper[2], im(d, i, j, kr))) : T(0);
+    T pd = hyp ? T(0.5) * (ld(in.hyper[2], im(d, i, j, kl)) + ld(in.hyper[2], im(d, i, j, kr))) : T(0);
+    if (mode != 2 && in.extra[2]) pd += ld(in.extra[2], p);
     const T tend = -cp * (thw + thp) * G.gzw(i, j, k) + g * (thp / thw) + pd;
     if (mode == 0) {
       out.f[2][p] = ld(in.w, p) + dt * (oma * tend + a * pd);
@@ -133,7 +136,8 @@ __global__ void __launch_bounds__(256) explicit_kernel(Dims d, Coef<T> c, Explic
     const T tpi = divergence(d, c, in.u, in.v, in.eta, i, j, k, thu_lin, thv_lin, thw_lin);
     const T nlpi = (mode == 2) ? T(0) : divergence(d, c, in.u, in.v, in.eta, i, j, k, thu_nl, thv_nl, thw_nl);
     const T wm = T(0.5) * (ld(in.w, iw(d, i, j, k)) + ld(in.w, iw(d, i, j, k + 1)));
-    const T pd = hyp ? ld(in.hyper[3], p) : T(0);
+    T pd = hyp ? ld(in.hyper[3], p) : T(0);
+    if (mode != 2 && in.extra[3]) pd += ld(in.extra[3], p);
     const T tth = -wm * ld(c.dthm, p) + pd;
     if (mode == 0) {
       out.f[3][p] = ld(in.pi, p) + oma * dt * (tpi + nlpi);

@@ -9,6 +9,7 @@ template <typename T>
 struct ExplicitIn {
   const T *u, *v, *w, *eta, *pi, *th;  // pi' and th' (perturbations)
   const T* hyper[4];                   // hyperdiffusion tendencies of u, v, w, th' at mass points, or null
+  const T* extra[4];                   // physics-suite tendencies of u, v, w (own staggers), th (mass), or null
 };
 // mode 0: f = {u_in, v_in, w_in, pi_in, th_in, tend_th, residual_n}
 // mode 1: f = {tend_u, tend_v, tend_w, tend_pi, tend_th, nl_pi, -}, pd = phys_diff u, v, w, th

@@ -37,12 +37,10 @@ class Euler3D:
     def __init__(self, grid, operators, constants, dt, initial_era5_state=None, N_bv=0.01,
                  damp_height=20000.0, max_damp=0.5, nu_div_factor=0.8, nu_h_factor=0.1,
                  physics_suite=None, interior_mask=None):
-        if physics_suite is not None:
-            raise NotImplementedError("physics suites are not part of the B200 SISL path")
         self.grid, self.op, self.c, self.dt = grid, operators, dict(constants), float(dt)
         self.nu_div = nu_div_factor * grid.dx ** 2 / (4.0 * dt)   # euler.py:62-67
         self.nu_h = nu_h_factor * grid.dx ** 4 / (64.0 * dt)
-        self.physics_suite, self.interior_mask = None, interior_mask
+        self.physics_suite, self.interior_mask = physics_suite, interior_mask
         g, cp = self.c["g"], self.c["cp"]
         dev = grid.device
         Z_m = grid.Z_m
@@ -206,6 +204,13 @@ class Euler3D:
             use = self.nu_h > 0.0 or self.nu_div > 0.0
             out.update({"phys_diff_u": pd[0] if use else 0.0, "phys_diff_v": pd[1] if use else 0.0,
                         "phys_diff_w": pd[2] if use else 0.0, "phys_diff_th_v": pd[3] if use else 0.0})
+            if self.physics_suite is not None:  # euler.py:347-366
+                pt = self.physics_suite.get_explicit_tendencies(state_prime, bg, interior_mask=self.interior_mask,
+                                                                ml_params=ml_params)
+                for k in ("u", "v", "w", "th_v"):
+                    if k in pt:
+                        out[k] = out[k] + pt[k]
+                        out["phys_diff_" + k] = out["phys_diff_" + k] + pt[k]
         return out
 
     def nonlinear_pi_tendency(self, state_prime, th_v_prime, bg):

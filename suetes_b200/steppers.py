@@ -49,6 +49,9 @@ def build_dynamical_core(core_type, grid, operators, constants, initial_state, p
         initial_state["eta_dot_prev"] = initial_state.get("eta_dot", torch.zeros_like(initial_state["w"]))
         initial_state["tend_th_v_prev"] = torch.zeros_like(initial_state["th_v"])
         initial_state["is_first_step"] = 1.0
+        for key in (physics_suite.tracer_keys if physics_suite is not None else []):
+            if key in initial_state:
+                initial_state[f"tend_{key}_prev"] = torch.zeros_like(initial_state[key])
     stepper = SISLStepper3D(physics, params["dt"], alpha=params["alpha"], use_limiter=params["use_limiter"],
                             use_checkpointing=params["use_checkpointing"], solver_tol=params["solver_tol"],
                             solver_maxiter=params["solver_maxiter"], solver_restart=params["solver_restart"],
@@ -106,12 +109,16 @@ class SemiLagrangianAdvector3D:
         dtype = _dtype_of({k: state[k] for k in ("u", "v", "eta_dot")})
         core = self.physics.core(dtype, self.dt, 0.55)
         u, v, e = core.field(state["u"], "u"), core.field(state["v"], "v"), core.field(state["eta_dot"], "w")
-        co = [core.new(loc) for _ in range(3)]
+        ex, ey, ez = core.shape(loc)
+        # one (3, ex, ey, ez) tensor whose three slices are x-fastest fields: the
+        # kernel writes them in place (no stacking copy)
+        out = torch.empty((3, ez, ey, ex), dtype=core.dtype, device=core.device).permute(0, 3, 2, 1)
+        co = [out[q] for q in range(3)]
         ws, n = core.workspace(_lib.WS_DEPARTURE)
         check(core.lib.sisl_departure(core.handle, _lib.LOC[loc], u.data_ptr(), v.data_ptr(), e.data_ptr(),
                                       int(iterations), ptrs(co, 3), ws.data_ptr(), n, core.stream),
               "sisl_departure")
-        return torch.stack(co, dim=0)
+        return out
 
     def advect_linear(self, field, coords):
         from .operators import map_coordinates_linear
@@ -311,7 +318,7 @@ class FluxFormAdvector:
         f = core.field(field, "m")
         u, v, e = core.field(state["u"], "u"), core.field(state["v"], "v"), core.field(state["eta_dot"], "w")
         out = core.new("m")
-        ws, n = core.workspace(5)
+        ws, n = core.workspace(_lib.WS_FFSL)
         check(core.lib.sisl_ffsl_advect(core.handle, f.data_ptr(), u.data_ptr(), v.data_ptr(), e.data_ptr(),
                                         out.data_ptr(), ws.data_ptr(), n, core.stream), "sisl_ffsl_advect")
         return out
@@ -353,7 +360,8 @@ class SISLStepper3D:
         self.implicit_solver = SemiImplicitSolver3D(physics, dt, alpha=alpha, solver_tol=solver_tol,
                                                     solver_maxiter=solver_maxiter, solver_restart=solver_restart,
                                                     solve_method=solve_method)
-        self.tracer_keys = []
+        suite = physics.physics_suite
+        self.tracer_keys = list(suite.tracer_keys) if suite is not None else []
         self.last_info = None
 
     # ------------------------------------------------------------------
@@ -432,6 +440,8 @@ class SISLStepper3D:
         VJP through the transposed solve) instead of the fused kernel chain."""
         if torch.is_grad_enabled() and any(torch.is_tensor(v) and v.requires_grad for v in state.values()):
             return self._step_differentiable(state, bc_fn)
+        if self.physics.physics_suite is not None:
+            return self._step_physics(state, forcing, bc_fn, ml_params)
         ds = self.to_device_state(state)
         out = DeviceState(ds.core)
         # history of the new state aliases the old prognostic fields (steppers.py:1061-1064)
@@ -444,8 +454,97 @@ class SISLStepper3D:
             res = self._apply_generic_bc(res, generic, forcing, out)
         return res
 
+    def _ffsl_device(self, core, field, ds):
+        """Split flux-form transport of a mass-point field by the winds of
+        ``ds`` (steppers.py:863-873), device layout in and out."""
+        out = core.new("m")
+        ws, n = core.workspace(_lib.WS_FFSL)
+        check(core.lib.sisl_ffsl_advect(core.handle, field.data_ptr(), ds.t["u"].data_ptr(), ds.t["v"].data_ptr(),
+                                        ds.t["eta_dot"].data_ptr(), out.data_ptr(), ws.data_ptr(), n, core.stream),
+              "sisl_ffsl_advect")
+        return out
+
+    def _step_physics(self, state, forcing, bc_fn, ml_params):
+        """``step`` with a physics suite (steppers.py:720-1073).
+
+        The suite's explicit tendencies of the input state (the state_prime of
+        steppers.py:767-784; euler.py:347-366) join the fused CUDA step
+        through ``sisl_step_physics``.  Density and the registered tracers
+        are carried by flux-form transport with the input winds; the suite's
+        state updates, then ``bc_fn``, then the equation of state with the
+        tracers' mass kept follow in the reference's order
+        (steppers.py:1030-1068)."""
+        ph, op, suite = self.physics, self.physics.op, self.physics.physics_suite
+        if "rho" not in state:
+            raise ValueError("a step with a physics suite needs the density 'rho' in the state")
+        ds = self.to_device_state(state)
+        core = ds.core
+        thp = ds.t["th_p"]
+        sp_n = {"u": ds.t["u"], "v": ds.t["v"], "w": ds.t["w"], "th_v": core.field(state["th_v"], "m"),
+                "pi": ds.t["pi_p"], "eta_dot": ds.t["eta_dot"], "th_v_prime_u": op.avg(thp, 0, "m", "u"),
+                "th_v_prime_v": op.avg(thp, 1, "m", "v"), "th_v_prime_w": op.avg(thp, 2, "m", "w")}
+        for k in ("theta_surf", "target_th_v"):
+            if k in state:
+                sp_n[k] = state[k]
+        bg = ph.precompute_bg(ph.bg_state_ref())
+        pt = suite.get_explicit_tendencies(sp_n, bg, interior_mask=ph.interior_mask, ml_params=ml_params)
+        tend = [core.field(pt[k], loc) if k in pt else None
+                for k, loc in (("u", "u"), ("v", "v"), ("w", "w"), ("th_v", "m"))]
+        out = DeviceState(core)
+        for k in ("u", "v", "w", "eta_dot"):
+            out.t[k + "_prev"] = ds.t[k]
+        sin, sout = ds.c_struct(), out.c_struct()
+        ws, n = core.workspace(_lib.WS_STEP)
+        info = _lib.SislStepInfo()
+        arr = (ctypes.c_void_p * 4)(*[t.data_ptr() if t is not None else None for t in tend])
+        rc = check(core.lib.sisl_step_physics(core.handle, ctypes.byref(sin), ctypes.byref(sout), None, arr, None,
+                                              ws.data_ptr(), n, core.stream, ctypes.byref(info)),
+                   "sisl_step_physics")
+        self.last_info = {"status": rc, "solves": [info.solve[0].as_dict(), info.solve[1].as_dict()],
+                          "kernel_launches": int(info.kernel_launches)}
+        eps = ph.c.get("eps", 1e-15)
+        rho_next = self._ffsl_device(core, ds.t["rho"], ds)
+        sn = self.from_device_state(out)
+        sn.pop("_sisl_state")
+        for k in ("u_prev", "v_prev", "w_prev", "eta_dot_prev", "tend_th_v_prev", "is_first_step"):
+            sn.pop(k)
+        sn["rho"] = rho_next
+        first = float(state.get("is_first_step", 1.0)) == 1.0 or "u_prev" not in state
+        for key in self.tracer_keys:
+            if key in state:
+                q_in = core.field(state[key], "m")
+                prev = state.get(f"tend_{key}_prev")
+                if not first and prev is not None:  # AB2 of a zero tendency (steppers.py:800-812)
+                    q_in = q_in + ph.dt * (-0.5 * core.field(prev, "m"))
+                sn[key] = self._ffsl_device(core, ds.t["rho"] * q_in, ds) / (rho_next + eps)
+        sn = suite.apply_state_updates(sn)
+        relax, generic = self._relax_of(bc_fn)
+        if relax is not None:
+            sn = relax.apply_state(sn, ph)
+        elif generic is not None:
+            sn = generic(sn, forcing)
+        tmass = {k: sn["rho"] * sn[k] for k in self.tracer_keys if k in sn}
+        th_p = fortran(torch.as_tensor(sn["th_v"]).to(core.device, F64) - ph.theta_bg, dtype=core.dtype)
+        pi_p = fortran(torch.as_tensor(sn["pi"]).to(core.device, F64) - ph.pi_bg, dtype=core.dtype)
+        rho = core.new("m")
+        check(core.lib.sisl_eos(core.handle, th_p.data_ptr(), pi_p.data_ptr(), rho.data_ptr(), core.stream),
+              "sisl_eos")
+        sn["rho"] = rho
+        for k, rq in tmass.items():
+            sn[k] = rq / (rho + eps)
+        sn["u_prev"], sn["v_prev"], sn["w_prev"] = ds.t["u"], ds.t["v"], ds.t["w"]
+        sn["eta_dot_prev"] = ds.t["eta_dot"]
+        sn["tend_th_v_prev"] = out.t["tend_th_prev"]
+        for key in self.tracer_keys:
+            if key in sn:
+                sn[f"tend_{key}_prev"] = torch.zeros_like(sn[key])
+        sn["is_first_step"] = 0.0
+        return sn
+
     def _step_differentiable(self, state, bc_fn):
         from .adjoint import DifferentiableStep
+        if self.physics.physics_suite is not None:
+            raise NotImplementedError("the differentiable step has no physics-suite cotangents")
         relax, generic = self._relax_of(bc_fn)
         if generic is not None:
             raise NotImplementedError("the differentiable step supports LateralRelaxation boundary conditions")
@@ -504,7 +603,7 @@ class SISLStepper3D:
         device, no host synchronisation inside a step), bitwise the eager
         steps; otherwise one ``sisl_step`` call per step."""
         relax, generic = self._relax_of(bc_fn)
-        if generic is not None:
+        if generic is not None or self.physics.physics_suite is not None:
             for n in range(num_steps):
                 state = self.step(state, t_start + n * self.dt, forcing, bc_fn)
             return state

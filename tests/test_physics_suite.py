@@ -1,0 +1,69 @@
+"""Host logic of the physics-suite hooks (CPU): the suite's aggregation
+(suetes/physics/base.py:28-69) and the relaxation blend on a state dict."""
+
+import torch
+
+from suetes_b200 import LateralRelaxation, PhysicsSuite
+
+
+class _A:
+    def get_tendencies(self, state, bg):
+        return {"u": state["u"] * 2.0, "q": state["th_v"] * 0.5}
+
+
+class _ML:
+    is_ml_closure = True
+
+    def get_tendencies(self, state, bg, ml_params=None):
+        return {"u": ml_params["c"] + 0.0 * state["u"], "th_v": state["th_v"] - bg["th_v"]}
+
+
+class _Up:
+    def __init__(self, k, f):
+        self.k, self.f = k, f
+
+    def apply_update(self, state):
+        return {self.k: self.f(state)}
+
+
+def test_suite_aggregates_masks_and_orders_updates():
+    g = torch.Generator().manual_seed(0)
+    st = {k: torch.randn(*s, generator=g, dtype=torch.float64) for k, s in
+          (("u", (5, 4, 3)), ("v", (4, 5, 3)), ("w", (4, 4, 4)), ("th_v", (4, 4, 3)))}
+    bg = {"th_v": torch.full((4, 4, 3), 0.25, dtype=torch.float64)}
+    s = PhysicsSuite()
+    s.add_tendency_scheme(_A())
+    s.add_tendency_scheme(_ML())
+    s.register_tracer("q")
+    s.register_tracer("q")
+    assert s.tracer_keys == ["q"]
+    mask = {"u": torch.linspace(0, 1, 5, dtype=torch.float64)[:, None, None]}
+    t = s.get_explicit_tendencies(st, bg, interior_mask=mask, ml_params={"c": 3.0})
+    assert torch.equal(t["u"], (st["u"] * 2.0 + 3.0) * mask["u"])
+    assert torch.equal(t["th_v"], st["th_v"] - bg["th_v"])
+    assert torch.equal(t["q"], st["th_v"] * 0.5)
+    assert torch.equal(t["v"], torch.zeros_like(st["v"])) and torch.equal(t["w"], torch.zeros_like(st["w"]))
+    s.add_update_scheme(_Up("u", lambda x: x["u"] + 1.0))
+    s.add_update_scheme(_Up("u", lambda x: x["u"] * 2.0))  # sees its predecessor's result
+    out = s.apply_state_updates(st)
+    assert torch.equal(out["u"], (st["u"] + 1.0) * 2.0) and out["v"] is st["v"]
+
+
+def test_relaxation_blend_on_state_dict():
+    class Ph:
+        theta_bg = torch.full((4, 3, 2), 300.0, dtype=torch.float64)
+        pi_bg = torch.full((4, 3, 2), 0.9, dtype=torch.float64)
+    mm = torch.rand(4, 3, dtype=torch.float64)
+    mu = torch.rand(5, 3, dtype=torch.float64)
+    mv = torch.rand(4, 4, dtype=torch.float64)
+    r = LateralRelaxation(mm, mu, mv, exterior={"u": 7.0, "v": 0.0, "th_v": 1.5, "pi": 0.0})
+    st = {"u": torch.randn(5, 3, 2, dtype=torch.float64), "v": torch.randn(4, 4, 2, dtype=torch.float64),
+          "th_v": 300.0 + torch.randn(4, 3, 2, dtype=torch.float64), "pi": torch.full((4, 3, 2), 0.91),
+          "w": torch.randn(4, 3, 3, dtype=torch.float64)}
+    out = r.apply_state(st, Ph)
+    m = mu[..., None]
+    assert torch.allclose(out["u"], (1 - m) * st["u"] + m * 7.0, rtol=0, atol=1e-14)
+    m = mm[..., None]
+    assert torch.allclose(out["th_v"], (1 - m) * st["th_v"] + m * 301.5, rtol=0, atol=1e-12)
+    assert torch.allclose(out["pi"].double(), (1 - m) * 0.91 + m * 0.9, rtol=0, atol=1e-7)
+    assert out["pi"].dtype == st["pi"].dtype and out["w"] is st["w"]
