@@ -353,7 +353,10 @@ int sisl_step_vjp(SislCore* core, const SislState* in, void* const solves[10], c
  * variants (0-2: tiles of 256 threads / 32 columns,
  * 128 / 16, 256 / 64; 3: one thread per column marching up and down the
  * precomputed factorisation, 128 columns per block) of the preconditioner
- * and of its transpose. */
+ * and of its transpose; the preconditioner also 4: the 256 / 32 tile with
+ * its loads issued in batches of four items and the face sums of u and v
+ * staged in shared memory; the transpose also 4: the 256 / 32 tile with
+ * its loads issued in batches of four items. */
 typedef struct SislTuning {
   int32_t matvec_block, precond_tile, matvec_t_block, precond_t_tile;
   float us[4];  /* microseconds per launch of the chosen shapes (sisl_autotune only) */

@@ -360,6 +360,135 @@ __global__ void __launch_bounds__(TPT) pt_column_kernel(Dims d, Coef<T> c, CVec5
   }
 }
 
+// The same tile with its global loads batched: every thread issues PU
+// items' loads before it computes any of them (the forward tile's
+// batching).  Arithmetic is term for term that of pt_column_kernel, so the
+// results are bitwise those of every other column variant.
+template <typename T, int TPT, int TPC, int PU>
+__global__ void __launch_bounds__(TPT) pt_column_batched_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
+                                                                const int* active) {
+  if (active && *active == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  T* s_x = sm;                // [nz][TPC]  pibar -> w -> z
+  T* s_cp = s_x + nz * TPC;   // [nz][TPC]  c'
+  T* s_lo = s_cp + nz * TPC;  // [nz][TPC]  lower
+  T* s_iv = s_lo + nz * TPC;  // [nz][TPC]  1 / pivot
+  const int i0 = blockIdx.x * TPC;
+  const int j = blockIdx.y;
+  const int tid = threadIdx.x;
+  const int pm = nx * ny;
+  const int nm = nz * TPC, nw = (nz + 1) * TPC;
+  const T ps = (T)c.s.ps, ips = (T)(1.0 / c.s.ps), inva = T(1) / (T)c.s.alpha;
+  const T* __restrict__ yw = y.f[2];
+  const T* __restrict__ yp = y.f[3];
+  const T* __restrict__ yW = y.f[4];
+  T* __restrict__ ow = out.f[2];
+  T* __restrict__ op = out.f[3];
+  T* __restrict__ oW = out.f[4];
+  (void)ny;
+  // ---- A: pibar and the factorisation ----
+  for (int q0 = tid; q0 < nm; q0 += PU * TPT) {
+    T a_p[PU], a_b0[PU], a_w0[PU], a_W0[PU], a_b1[PU], a_w1[PU], a_W1[PU], a_cp[PU], a_lo[PU], a_iv[PU];
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * TPT;
+      if (q < nm) {
+        const int k = q / TPC, i = min(i0 + q % TPC, nx - 1);
+        const int p = i + nx * j + k * pm;
+        const int p0 = i + nx * j + min(max(k, 1), nz - 1) * pm;
+        const int p1 = i + nx * j + min(max(k + 1, 1), nz - 1) * pm;
+        a_p[u] = ld(yp, p);
+        a_b0[u] = ld(c.pbw, p0);
+        a_w0[u] = ld(yw, p0);
+        a_W0[u] = ld(yW, p0);
+        a_b1[u] = ld(c.pbw, p1);
+        a_w1[u] = ld(yw, p1);
+        a_W1[u] = ld(yW, p1);
+        a_cp[u] = ld(c.tcp, p);
+        a_lo[u] = ld(c.tlo, p);
+        a_iv[u] = ld(c.tinv, p);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * TPT;
+      if (q < nm) {
+        const int k = q / TPC;
+        const T g0 = -a_b0[u] * (a_w0[u] + a_W0[u]);
+        const T g1 = -a_b1[u] * (a_w1[u] + a_W1[u]);
+        const T G0 = (k > 0 && k < nz) ? g0 : T(0);
+        const T G1 = (k + 1 > 0 && k + 1 < nz) ? g1 : T(0);
+        s_x[q] = a_p[u] * ps + G0 - G1;
+        s_cp[q] = a_cp[u];
+        s_lo[q] = a_lo[u];
+        s_iv[q] = a_iv[u];
+      }
+    }
+  }
+  __syncthreads();
+  // ---- B: U^T w = pibar upward, L^T z = w downward, one thread per column ----
+  if (tid < TPC) {
+    const int l = tid;
+    T wprev = T(0), cprev = T(0);
+    for (int k = 0; k < nz; ++k) {
+      const int q = k * TPC + l;
+      wprev = s_x[q] - cprev * wprev;
+      s_x[q] = wprev;
+      cprev = s_cp[q];
+    }
+    T zh = T(0), loh = T(0);
+    for (int k = nz - 1; k >= 0; --k) {
+      const int q = k * TPC + l;
+      zh = (s_x[q] - loh * zh) * s_iv[q];
+      s_x[q] = zh;
+      loh = s_lo[q];
+    }
+  }
+  __syncthreads();
+  // ---- C: pi, w and eta_dot cotangents ----
+  for (int q0 = tid; q0 < nw; q0 += PU * TPT) {
+    T c_w[PU], c_W[PU], c_a[PU], c_b[PU], c_r[PU], c_d[PU];
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * TPT;
+      const int k = q / TPC, i = i0 + q % TPC;
+      if (q < nw && i < nx) {
+        const int p = i + nx * j + k * pm;
+        c_w[u] = ld(yw, p);
+        c_W[u] = ld(yW, p);
+        if (k == 0 || k == nz) {
+          c_d[u] = ld(c.dzw, p);
+        } else {
+          c_a[u] = ld(c.lpi, p - pm);
+          c_b[u] = ld(c.lpi, p);
+          c_r[u] = ld(c.rtw, p);
+          c_d[u] = ld(c.idamp, p);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * TPT;
+      const int k = q / TPC, i = i0 + q % TPC;
+      if (q < nw && i < nx) {
+        const int p = i + nx * j + k * pm;
+        if (k < nz) op[p] = s_x[q] * ips;
+        if (k == 0 || k == nz) {
+          ow[p] = c_w[u];
+          oW[p] = c_W[u] * c_d[u];
+        } else {
+          const T dvl = mul_rn(-c_a[u], s_x[q - TPC]), dv = mul_rn(-c_b[u], s_x[q]);
+          const T ep = c_W[u] + c_r[u] * (dvl - dv);
+          oW[p] = ep * inva;
+          ow[p] = (c_w[u] + ep) * c_d[u];
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // M^T, horizontal part: out_u = y_u + sum of the kinematic cotangent
 // kinbar = -alpha out_W over the interior w levels of the adjacent cells.
@@ -621,6 +750,16 @@ void launch_pt_column(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, 
   pt_column_kernel<T, TPT, TPC><<<dim3((d.nx + TPC - 1) / TPC, d.ny), TPT, smem, st>>>(d, c, y, out, active);
 }
 
+template <typename T, int TPT, int TPC, int PU>
+void launch_pt_column_batched(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
+                              cudaStream_t st) {
+  const size_t smem = (size_t)(4 * d.nz) * TPC * sizeof(T);
+  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  ensure_smem_limit((const void*)pt_column_batched_kernel<T, TPT, TPC, PU>, attr_bytes, smem);
+  pt_column_batched_kernel<T, TPT, TPC, PU>
+      <<<dim3((d.nx + TPC - 1) / TPC, d.ny), TPT, smem, st>>>(d, c, y, out, active);
+}
+
 template <typename T>
 void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                       cudaStream_t st) {
@@ -630,6 +769,7 @@ void launch_precond_t(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, 
     case 1: launch_pt_column<T, 128, 16>(d, c, y, out, active, st); break;
     case 2: launch_pt_column<T, 256, 64>(d, c, y, out, active, st); break;
     case 3: launch_pt_march<T, 128>(d, c, y, out, active, st); break;
+    case 4: launch_pt_column_batched<T, 256, 32, 4>(d, c, y, out, active, st); break;
     default: launch_pt_column<T, 256, 32>(d, c, y, out, active, st); break;
   }
   const dim3 blk = stencil_block(d.tune_mvt);

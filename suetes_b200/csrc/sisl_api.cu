@@ -1868,8 +1868,8 @@ int sisl_step_graph_destroy(SislStepGraph* g) {
 int sisl_core_set_tuning(SislCore* c, const SislTuning* t) {
   if (!c || !t) return SISL_ERR_ARG;
   if (t->matvec_block < 0 || t->matvec_block >= N_MATVEC_SHAPES || t->matvec_t_block < 0 ||
-      t->matvec_t_block >= N_STENCIL_BLOCKS || t->precond_tile < 0 || t->precond_tile >= N_COLUMN_TILES ||
-      t->precond_t_tile < 0 || t->precond_t_tile >= N_COLUMN_TILES)
+      t->matvec_t_block >= N_STENCIL_BLOCKS || t->precond_tile < 0 || t->precond_tile >= N_PRECOND_SHAPES ||
+      t->precond_t_tile < 0 || t->precond_t_tile >= N_PRECOND_T_SHAPES)
     return SISL_ERR_ARG;
   c->d.tune_mv = t->matvec_block;
   c->d.tune_pc = t->precond_tile;
@@ -1936,13 +1936,13 @@ int autotune_impl(SislCore* c, void* ws, cudaStream_t st, SislTuning* out) {
   pick(&d.tune_mv, N_MATVEC_SHAPES,
        [&] { launch_matvec<T>(d, cf, g.cview(g.V(0)), nullptr, none, g.split(g.V(1), g.z()), nullptr, st); },
        &out->us[0]);
-  pick(&d.tune_pc, N_COLUMN_TILES,
+  pick(&d.tune_pc, N_PRECOND_SHAPES,
        [&] { launch_precond<T>(d, cf, as_const(g.split(g.V(1), g.z())), g.view(g.V(2)), nullptr, st); },
        &out->us[1]);
   pick(&d.tune_mvt, N_STENCIL_BLOCKS,
        [&] { launch_matvec_t<T>(d, cf, g.cview(g.V(0)), nullptr, none, g.view(g.z()), g.tmp, nullptr, st); },
        &out->us[2]);
-  pick(&d.tune_pct, N_COLUMN_TILES,
+  pick(&d.tune_pct, N_PRECOND_T_SHAPES,
        [&] { launch_precond_t<T>(d, cf, g.cview(g.z()), g.view(g.V(2)), nullptr, st); }, &out->us[3]);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

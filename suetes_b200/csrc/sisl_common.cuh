@@ -55,6 +55,11 @@ constexpr int N_MATVEC_SHAPES = 6;  // the 4 blocks, and 32x8 columns of 2 or 4 
 // column variants: tiles of (threads, columns) = (256, 32), (128, 16), (256, 64),
 // and the one-thread-per-column march (128 columns per block)
 constexpr int N_COLUMN_TILES = 4;
+// forward preconditioner only: also the (256, 32) tile with
+// batched loads and staged face sums
+constexpr int N_PRECOND_SHAPES = 5;
+// its transpose: also the (256, 32) tile with batched loads
+constexpr int N_PRECOND_T_SHAPES = 5;
 
 __host__ __device__ inline int ext_x(const Dims& d, int loc) { return d.nx + (loc == LOC_U); }
 __host__ __device__ inline int ext_y(const Dims& d, int loc) { return d.ny + (loc == LOC_V); }

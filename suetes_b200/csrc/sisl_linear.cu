@@ -317,6 +317,207 @@ __global__ void __launch_bounds__(PT) precond_tile_kernel(Dims d, Coef<T> c, CVe
   }
 }
 
+// The same tile with its global loads batched: every thread issues PU
+// items' loads before it computes any of them, so each phase waits on one
+// or two rounds of memory latency instead of one per item.  The horizontal
+// wind sums over faces (i, i+1) and (j, j+1) are staged per mass level
+// first (A0, into the buffers the factorisation fills later), so the
+// w-level phase reads six arrays instead of fifteen values.  Arithmetic is
+// term for term that of precond_wlevel and precond_tile_kernel: results
+// are bitwise those of every other column variant.
+template <typename T, int PT, int PC, int PU>
+__global__ void __launch_bounds__(PT) precond_tile_batched_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
+                                                                  const int* active) {
+  if (active && *active == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  T* s_x = sm;                    // [nz][PC]    rhs -> d' -> x
+  T* s_W = s_x + nz * PC;         // [nz+1][PC]  w_tilde at w levels
+  T* s_lo = s_W + (nz + 1) * PC;  // [nz][PC]    u face sum (A0-A1), then lower
+  T* s_iv = s_lo + nz * PC;       // [nz][PC]    v face sum (A0-A1), then 1 / pivot
+  T* s_cp = s_iv + nz * PC;       // [nz][PC]    c'
+  const int i0 = blockIdx.x * PC;
+  const int j = blockIdx.y;
+  const int tid = threadIdx.x;
+  const T* __restrict__ ru = r.f[0];
+  const T* __restrict__ rv = r.f[1];
+  const T* __restrict__ rw = r.f[2];
+  const T* __restrict__ rp = r.f[3];
+  const T* __restrict__ rW = r.f[4];
+  T* __restrict__ ow = out.f[2];
+  T* __restrict__ op = out.f[3];
+  T* __restrict__ oW = out.f[4];
+  const T inva = T(1) / (T)c.s.alpha;
+  const T ips = (T)(1.0 / c.s.ps);
+  const T ps = (T)c.s.ps;
+  const int pm = nx * ny;
+  const int nm = nz * PC, nw = (nz + 1) * PC;
+
+  if (out.f[0] != ru) {
+    const int ncol = min(PC + (i0 + PC >= nx ? 1 : 0), nx + 1 - i0);
+    for (int q = tid; q < ncol * nz; q += PT) {
+      const int k = q / ncol, ii = i0 + q % ncol;
+      out.f[0][iu(d, ii, j, k)] = ld(ru, iu(d, ii, j, k));
+    }
+  }
+  if (out.f[1] != rv) {
+    const int ncol = min(PC, nx - i0);
+    const int nj = (j == ny - 1) ? 2 : 1;
+    for (int q = tid; q < ncol * nz * nj; q += PT) {
+      const int jj = j + q / (ncol * nz), rem = q % (ncol * nz);
+      const int k = rem / ncol, ii = i0 + rem % ncol;
+      out.f[1][iv(d, ii, jj, k)] = ld(rv, iv(d, ii, jj, k));
+    }
+  }
+
+  // ---- A0: face sums of u and v per mass level ----
+  for (int q0 = tid; q0 < nm; q0 += PU * PT) {
+    T a0[PU], a1[PU], b0[PU], b1[PU];
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * PT;
+      if (q < nm) {
+        const int k = q / PC, i = min(i0 + q % PC, nx - 1);
+        const int pu = iu(d, i, j, k), pv = iv(d, i, j, k);
+        a0[u] = ld(ru, pu);
+        a1[u] = ld(ru, pu + 1);
+        b0[u] = ld(rv, pv);
+        b1[u] = ld(rv, pv + nx);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * PT;
+      if (q < nm) {
+        s_lo[q] = a0[u] + a1[u];
+        s_iv[q] = b0[u] + b1[u];
+      }
+    }
+  }
+  __syncthreads();
+  // ---- A1: the w-level quantities (precond_wlevel) ----
+  for (int q0 = tid; q0 < nw; q0 += PU * PT) {
+    T zx[PU], ze[PU], wW[PU], rt[PU], ww[PU], id[PU], mq[PU];
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * PT;
+      if (q < nw) {
+        const int k = q / PC, i = min(i0 + q % PC, nx - 1);
+        const int kc = min(max(k, 1), nz - 1);
+        const int p = i + nx * j + kc * pm;
+        zx[u] = ld(c.zxw, p);
+        ze[u] = ld(c.zew, p);
+        wW[u] = ld(rW, p);
+        rt[u] = ld(c.rtw, p);
+        ww[u] = ld(rw, p);
+        id[u] = ld(c.idamp, p);
+        mq[u] = ld(c.mm, i + nx * j);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * PT;
+      if (q < nw) {
+        const int k = q / PC, l = q % PC, i = min(i0 + l, nx - 1);
+        const int kc = min(max(k, 1), nz - 1);
+        const T on = (k > 0 && k < nz) ? T(1) : T(0);
+        const int ql = (kc - 1) * PC + l, qh = kc * PC + l;
+        const T m4 = T(0.25) * mq[u];
+        const T kin = m4 * ((s_lo[ql] + s_lo[qh]) * zx[u] + (s_iv[ql] + s_iv[qh]) * ze[u]);
+        const T ep = wW[u] * inva - kin;
+        s_W[q] = on * (rt[u] * (ww[u] * id[u] + ep));
+        if (i0 + l < nx && k > 0 && k < nz) oW[i + nx * j + k * pm] = on * ep;
+      }
+    }
+  }
+  __syncthreads();
+  // ---- A2: Helmholtz right-hand side and the factorisation ----
+  for (int q0 = tid; q0 < nm; q0 += PU * PT) {
+    T pp[PU], lp[PU], tl[PU], ti[PU], tc[PU];
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * PT;
+      if (q < nm) {
+        const int k = q / PC, i = min(i0 + q % PC, nx - 1);
+        const int p = i + nx * j + k * pm;
+        pp[u] = ld(rp, p);
+        lp[u] = ld(c.lpi, p);
+        tl[u] = ld(c.tlo, p);
+        ti[u] = ld(c.tinv, p);
+        tc[u] = ld(c.tcp, p);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * PT;
+      if (q < nm) {
+        s_x[q] = pp[u] * ips - lp[u] * (s_W[q + PC] - s_W[q]);
+        s_lo[q] = tl[u];
+        s_iv[q] = ti[u];
+        s_cp[q] = tc[u];
+      }
+    }
+  }
+  __syncthreads();
+  // ---- B: Thomas with the prepared factorisation, one thread per column ----
+  if (tid < PC) {
+    const int l = tid;
+    T dprev = T(0);
+    for (int k = 0; k < nz; ++k) {
+      const int q = k * PC + l;
+      dprev = (s_x[q] - s_lo[q] * dprev) * s_iv[q];
+      s_x[q] = dprev;
+    }
+    T xh = dprev;
+    for (int k = nz - 2; k >= 0; --k) {
+      const int q = k * PC + l;
+      xh = s_x[q] - s_cp[q] * xh;
+      s_x[q] = xh;
+    }
+  }
+  __syncthreads();
+  // ---- C: back substitution for w, eta_dot and the scaled pi ----
+  T ww[PU], id[PU], pb[PU];
+  auto c_load = [&](int q0) {
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * PT;
+      const int k = q / PC, i = i0 + q % PC;
+      if (q < nw && i < nx) {
+        const int p = i + nx * j + k * pm;
+        ww[u] = ld(rw, p);
+        const bool edge = (k == 0 || k == nz);
+        id[u] = edge ? ld(rW, p) : ld(c.idamp, p);
+        pb[u] = edge ? ld(c.dzw, p) : ld(c.pbw, p);
+      }
+    }
+  };
+  auto c_store = [&](int q0) {
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+      const int q = q0 + u * PT;
+      const int k = q / PC, i = i0 + q % PC;
+      if (q < nw && i < nx) {
+        const int p = i + nx * j + k * pm;
+        if (k == 0 || k == nz) {
+          ow[p] = ww[u];
+          oW[p] = id[u] * pb[u];
+        } else {
+          const T wv = ww[u] * id[u] - pb[u] * (s_x[q] - s_x[q - PC]);
+          ow[p] = wv;
+          oW[p] = oW[p] + wv;
+        }
+        if (k < nz) op[p] = s_x[q] * ps;
+      }
+    }
+  };
+  for (int q0 = tid; q0 < nw; q0 += PU * PT) {
+    c_load(q0);
+    c_store(q0);
+  }
+}
+
 }  // namespace
 
 template <typename T>
@@ -437,6 +638,16 @@ void launch_precond_tile(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> ou
   precond_tile_kernel<T, PT, PC><<<grd, PT, smem, st>>>(d, c, r, out, active);
 }
 
+template <typename T, int PT, int PC, int PU>
+void launch_precond_tile_batched(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
+                                 cudaStream_t st) {
+  const size_t smem = (size_t)(5 * d.nz + 1) * PC * sizeof(T);
+  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  ensure_smem_limit((const void*)precond_tile_batched_kernel<T, PT, PC, PU>, attr_bytes, smem);
+  dim3 grd((d.nx + PC - 1) / PC, d.ny);
+  precond_tile_batched_kernel<T, PT, PC, PU><<<grd, PT, smem, st>>>(d, c, r, out, active);
+}
+
 template <typename T>
 void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                     cudaStream_t st) {
@@ -446,6 +657,7 @@ void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, co
     case 1: launch_precond_tile<T, 128, 16>(d, c, r, out, active, st); break;
     case 2: launch_precond_tile<T, 256, 64>(d, c, r, out, active, st); break;
     case 3: launch_precond_march<T, 128>(d, c, r, out, active, st); break;
+    case 4: launch_precond_tile_batched<T, 256, 32, 4>(d, c, r, out, active, st); break;
     default: launch_precond_tile<T, 256, 32>(d, c, r, out, active, st); break;
   }
 }
