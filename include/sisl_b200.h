@@ -44,7 +44,8 @@ enum { SISL_LOC_M = 0, SISL_LOC_U = 1, SISL_LOC_V = 2, SISL_LOC_W = 3 };
 enum { SISL_GMRES_BATCHED = 0, SISL_GMRES_INCREMENTAL = 1 };
 enum {
   SISL_WS_STEP = 0, SISL_WS_GMRES = 1, SISL_WS_DEPARTURE = 2, SISL_WS_EXPLICIT = 3, SISL_WS_OPERATOR = 4,
-  SISL_WS_FFSL = 5, SISL_WS_STEP_VJP = 6, SISL_WS_EXPLICIT_VJP = 7, SISL_WS_FFSL_VJP = 8
+  SISL_WS_FFSL = 5, SISL_WS_STEP_VJP = 6, SISL_WS_EXPLICIT_VJP = 7, SISL_WS_FFSL_VJP = 8,
+  SISL_WS_SPLIT = 9
 };
 enum {
   SISL_RELAX_U = 1, SISL_RELAX_V = 2, SISL_RELAX_W = 4, SISL_RELAX_TH = 8, SISL_RELAX_PI = 16
@@ -319,6 +320,25 @@ int sisl_step_taped(SislCore* core, const SislState* in, const SislState* out, c
 int sisl_step_physics(SislCore* core, const SislState* in, const SislState* out, const SislRelaxation* relax,
                       const void* const phys_tend[4], void* const solves[10], void* ws, size_t ws_bytes,
                       void* stream, SislStepInfo* info);
+/* Split-explicit core (SplitExplicitStepper3D, steppers.py:1076-1737).
+ * sisl_split_diagnose: eta_dot and the kinematic w boundaries of a state
+ * (_diagnose_eta_dot, steppers.py:1272-1310); w_out may alias w.
+ * sisl_split_step: the three RK3 stages with their acoustic sub-cycles
+ * (ns acoustic steps in the last stage, round(ns/3) and round(ns/2) in the
+ * first two; off-centring alpha) from a diagnosed state in (u, v, w,
+ * eta_dot, pi_p, th_p) to out (same fields; rho is copied through, the
+ * history fields are not used).  tau_damp: the Rayleigh damping rate at w
+ * levels (Euler3D.tau_damp), in the core's precision and layout.
+ * phys_tend: the physics suite's tendencies of u, v, w, th_v at the step
+ * start (NULL entries, or NULL, for none); eps_l: the flux noise gate of
+ * the upwind advection (constants 'eps_l', default 1e-12).  The suite's
+ * updates, tracer transport, bc_fn, the final diagnosis and the equation of
+ * state follow on the caller's side (steppers.py:1233-1270).  out must not
+ * alias in.  ws: sisl_workspace_bytes(core, SISL_WS_SPLIT) bytes. */
+int sisl_split_diagnose(SislCore* core, const void* u, const void* v, const void* w, void* eta_out, void* w_out,
+                        void* stream);
+int sisl_split_step(SislCore* core, const SislState* in, const SislState* out, int ns, double alpha, double eps_l,
+                    const void* tau_damp, const void* const phys_tend[4], void* ws, size_t ws_bytes, void* stream);
 /* Cotangent of one step's input state from the cotangent of its output
  * (the VJP of SISLStepper3D.step under jax.checkpoint, steppers.py:720-1073,
  * 792-850, with the reference's stop_gradient on the departure points and

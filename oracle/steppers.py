@@ -31,7 +31,18 @@ def unpack(x, like):
 
 def build_dynamical_core(core_type, grid, operators, constants, initial_state,
                          physics_suite=None, interior_mask=None, **kwargs):
-    """SISL branch of the factory (steppers.py:12-88)."""
+    """The factory (steppers.py:12-122): SISL and split-explicit branches."""
+    if core_type.lower() == "split-explicit":  # steppers.py:90-119
+        from .split_explicit import SplitExplicitStepper3D
+        params = {"dt": 40.0, "ns": 3, "damp_height": 12000.0, "max_damp": 3.0, "nu_div_factor": 0.03,
+                  "nu_h_factor": 0.03, "N_bv": 0.01, "alpha": 0.55, "background_state": None}
+        params.update(kwargs)
+        ref = params["background_state"] if params["background_state"] is not None else initial_state
+        physics = Euler3D(grid, operators, constants, dt=params["dt"], initial_era5_state=ref,
+                          damp_height=params["damp_height"], max_damp=params["max_damp"],
+                          nu_div_factor=params["nu_div_factor"], nu_h_factor=params["nu_h_factor"],
+                          N_bv=params["N_bv"], physics_suite=physics_suite, interior_mask=interior_mask)
+        return SplitExplicitStepper3D(physics, dt=params["dt"], ns=params["ns"], alpha=params["alpha"]), params["dt"]
     if core_type.lower() != "sisl":
         raise ValueError(f"Unknown core_type: '{core_type}'. Use 'sisl' or 'split-explicit'.")
     params = {"dt": 120.0, "damp_height": 9000.0, "max_damp": 3.0, "nu_div_factor": 0.1,

@@ -13,6 +13,7 @@ from .euler import Euler3D
 from .geometry import (GalChenSigma, HybridSigma, RegionalGrid3D, SleveSimple, StretchedSleveSimple)
 from .operators import CGridOperator3D, map_coordinates_linear, tensor_product_interp_3d
 from .physics import PhysicsSuite
+from .split_explicit import SplitExplicitStepper3D
 from .steppers import (DeviceState, FluxFormAdvector, PingPong, SemiImplicitSolver3D, SemiLagrangianAdvector3D,
                        SISLStepper3D, StateRing, StepGraph, VerticalPreconditioner, build_dynamical_core)
 
@@ -21,5 +22,5 @@ __all__ = [
     "tensor_product_interp_3d", "map_coordinates_linear", "Euler3D", "VerticalPreconditioner",
     "SemiLagrangianAdvector3D", "SemiImplicitSolver3D", "FluxFormAdvector", "SISLStepper3D", "DeviceState",
     "StateRing", "StepGraph", "PingPong", "build_dynamical_core", "LateralRelaxation", "x_relaxation",
-    "PhysicsSuite",
+    "PhysicsSuite", "SplitExplicitStepper3D",
 ]

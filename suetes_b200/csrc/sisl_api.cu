@@ -13,6 +13,7 @@
 #include "sisl_core.cuh"
 #include "sisl_explicit.cuh"
 #include "sisl_gmres.cuh"
+#include "sisl_split.cuh"
 #include "sisl_step_vjp.cuh"
 
 using namespace sisl;
@@ -1070,6 +1071,140 @@ bool valid_grid(const SislGrid* g) {
 // ===========================================================================
 // C ABI
 // ===========================================================================
+namespace {
+
+// Workspace of the split-explicit step: acoustic perturbations (two
+// u''/v'' buffers swapped by the corrector), midpoint winds, the old
+// pressure gradients, the slow forcings, the explicit kernel's outputs, the
+// advection terms, the hyperdiffusion of the step start and of the stage,
+// the Thomas sweep, and two stage states.
+template <typename T>
+struct SplitWork {
+  T *upp, *upp2, *vpp, *vpp2, *wpp, *ppp, *uh, *vh, *gx0, *gy0;
+  T* sf[5];
+  T* tend[6];
+  T* adv[4];
+  T *hyp_t[4], *hyp_s[4], *htmp[4];
+  T *cpr, *dpr;
+  T* st[2][6];  // stage states: u, v, w, eta, pi', th'
+};
+
+template <typename T>
+void carve_split(Carver& cv, const Dims& d, SplitWork<T>& w) {
+  auto f = [&](int loc) { return (T*)cv.take(sizeof(T) * field_size(d, loc)); };
+  w.upp = f(LOC_U); w.upp2 = f(LOC_U); w.vpp = f(LOC_V); w.vpp2 = f(LOC_V);
+  w.wpp = f(LOC_W); w.ppp = f(LOC_M); w.uh = f(LOC_U); w.vh = f(LOC_V); w.gx0 = f(LOC_U); w.gy0 = f(LOC_V);
+  const int sf_loc[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_M};
+  for (int q = 0; q < 5; ++q) w.sf[q] = f(sf_loc[q]);
+  const int t_loc[6] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_M, LOC_M};
+  for (int q = 0; q < 6; ++q) w.tend[q] = f(t_loc[q]);
+  for (int q = 0; q < 4; ++q) {
+    w.adv[q] = f(LOC_M);
+    w.hyp_t[q] = f(LOC_M);
+    w.hyp_s[q] = f(LOC_M);
+    w.htmp[q] = f(LOC_M);
+  }
+  w.cpr = f(LOC_M);
+  w.dpr = f(LOC_M);
+  const int s_loc[6] = {LOC_U, LOC_V, LOC_W, LOC_W, LOC_M, LOC_M};
+  for (int b = 0; b < 2; ++b)
+    for (int q = 0; q < 6; ++q) w.st[b][q] = f(s_loc[q]);
+}
+
+}  // namespace
+
+namespace {
+
+// steppers.py:1117-1231: hyperdiffusion and physics tendencies of the step
+// start, then three stages of slow tendencies and acoustic sub-steps
+template <typename T>
+void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int ns, double alpha, double eps_l,
+                     const T* tau, const void* const* phys, void* ws, cudaStream_t st) {
+  const Dims& d = c->d;
+  const Coef<T> cf = coef_of<T>(c);
+  Carver cv{(char*)ws};
+  SplitWork<T> w;
+  carve_split<T>(cv, d, w);
+  const T* s0[6] = {(const T*)in->u, (const T*)in->v, (const T*)in->w, (const T*)in->eta_dot, (const T*)in->pi_p,
+                    (const T*)in->th_p};
+  T* dst_out[6] = {(T*)out->u, (T*)out->v, (T*)out->w, (T*)out->eta_dot, (T*)out->pi_p, (T*)out->th_p};
+  // the HyperFilter of the step start (diff_tends); inside the stages the
+  // explicit tendencies run with nu_h hidden, so their own hyperdiffusion
+  // is on exactly when nu_div > 0 (euler.py:336), with the filter's nu_h
+  const bool hyp_t = c->s.nu_h > 0.0, hyp_s = c->s.nu_h > 0.0 && c->s.nu_div > 0.0;
+  auto table4 = [](T* const* a) {
+    PtrTable<T> t{};
+    for (int q = 0; q < 4; ++q) t.p[q] = a[q];
+    return t;
+  };
+  if (hyp_t) {
+    KScope k(c, SISL_K_EXPLICIT, st, 3);
+    launch_hyper<T>(d, cf, s0[0], s0[1], s0[2], s0[5], table4(w.htmp), table4(w.hyp_t), st);
+  }
+  const int nst[3] = {std::max(1, (int)std::nearbyint(ns / 3.0)), std::max(1, (int)std::nearbyint(ns / 2.0)), ns};
+  const double dts[3] = {(c->s.dt / 3.0) / nst[0], (c->s.dt / 2.0) / nst[1], c->s.dt / nst[2]};
+  const T* cur[6];
+  for (int q = 0; q < 6; ++q) cur[q] = s0[q];
+  for (int stage = 0; stage < 3; ++stage) {
+    T* const* dst = stage == 2 ? dst_out : w.st[stage];
+    // ---- slow tendencies (steppers.py:1362-1465) ----
+    const T* hyp[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (hyp_s) {
+      KScope k(c, SISL_K_EXPLICIT, st, 3 + (hyp_t ? 4 : 0));
+      launch_hyper<T>(d, cf, cur[0], cur[1], cur[2], cur[5], table4(w.htmp), table4(w.hyp_s), st);
+      if (hyp_t)
+        for (int q = 0; q < 4; ++q) launch_split_axpy<T>(field_size(d, LOC_M), w.hyp_t[q], w.hyp_s[q], st);
+      for (int q = 0; q < 4; ++q) hyp[q] = w.hyp_s[q];
+    } else if (hyp_t) {
+      for (int q = 0; q < 4; ++q) hyp[q] = w.hyp_t[q];
+    }
+    ExplicitIn<T> ein{cur[0], cur[1], cur[2], cur[3], cur[4], cur[5], {hyp[0], hyp[1], hyp[2], hyp[3]},
+                      {nullptr, nullptr, nullptr, nullptr}};
+    if (phys)
+      for (int q = 0; q < 4; ++q) ein.extra[q] = (const T*)phys[q];
+    ExplicitOut<T> eout{};
+    for (int q = 0; q < 6; ++q) eout.f[q] = w.tend[q];
+    {
+      KScope k(c, SISL_K_EXPLICIT, st, 3);
+      launch_explicit<T>(d, cf, ein, eout, 1, st);
+      launch_split_adv<T>(d, cf, cur[0], cur[1], cur[2], cur[3], cur[5], (T)eps_l, w.adv, st);
+      launch_split_slow<T>(d, (const T* const*)w.tend, (const T* const*)w.adv, w.sf, st);
+    }
+    // ---- acoustic sub-steps (steppers.py:1467-1633) ----
+    SplitArgs<T> a{};
+    a.u0 = s0[0]; a.v0 = s0[1]; a.w0 = s0[2]; a.p0 = s0[4]; a.th0 = s0[5];
+    a.uc = cur[0]; a.vc = cur[1]; a.wc = cur[2]; a.pc = cur[4]; a.ec = cur[3];
+    a.upp = w.upp; a.vpp = w.vpp; a.wpp = w.wpp; a.ppp = w.ppp;
+    a.uh = w.uh; a.vh = w.vh; a.gx0 = w.gx0; a.gy0 = w.gy0;
+    a.sfu = w.sf[0]; a.sfv = w.sf[1]; a.sfw = w.sf[2]; a.sfp = w.sf[3]; a.sfth = w.sf[4];
+    a.tau = tau; a.cpr = w.cpr; a.dpr = w.dpr;
+    a.dtau = (T)dts[stage]; a.alpha = (T)alpha; a.nu_div = (T)c->s.nu_div;
+    T* spare_u = w.upp2;
+    T* spare_v = w.vpp2;
+    {
+      KScope k(c, SISL_K_OTHER, st, 1 + 3 * nst[stage]);
+      launch_split_init<T>(d, a, st);
+      for (int n = 0; n < nst[stage]; ++n) {
+        launch_split_predict<T>(d, cf, a, st);
+        launch_split_column<T>(d, cf, a, st);
+        launch_split_correct<T>(d, cf, a, spare_u, spare_v, st);
+        std::swap(a.upp, spare_u);
+        std::swap(a.vpp, spare_v);
+      }
+    }
+    {
+      KScope k(c, SISL_K_OTHER, st, stage < 2 ? 2 : 1);
+      launch_split_end<T>(d, a, nst[stage], dst[0], dst[1], dst[2], dst[3], dst[4], dst[5], st);
+      if (stage < 2) launch_split_diag<T>(d, cf, dst[0], dst[1], dst[2], dst[3], dst[2], st);
+    }
+    for (int q = 0; q < 6; ++q) cur[q] = dst[q];
+  }
+  if (out->rho && in->rho && out->rho != in->rho)
+    cudaMemcpyAsync(out->rho, in->rho, sizeof(T) * field_size(d, LOC_M), cudaMemcpyDeviceToDevice, st);
+}
+
+}  // namespace
+
 extern "C" {
 
 int sisl_version(void) { return 1; }
@@ -1213,6 +1348,15 @@ size_t sisl_workspace_bytes(const SislCore* c, int what) {
       } else {
         carve_step<float>(cv, c->d, c->prm.solver_restart, refining<float>(c));
         carve_vjp<float>(cv, c->d);
+      }
+      break;
+    case SISL_WS_SPLIT:
+      if (f64) {
+        SplitWork<double> w;
+        carve_split<double>(cv, c->d, w);
+      } else {
+        SplitWork<float> w;
+        carve_split<float>(cv, c->d, w);
       }
       break;
     case SISL_WS_FFSL_VJP:
@@ -1989,6 +2133,42 @@ int sisl_core_set_solver(SislCore* c, double tol, double atol, int maxiter, int 
   c->prm.solver_restart = restart;
   c->prm.solve_method = method;
   return SISL_OK;
+}
+
+int sisl_split_diagnose(SislCore* c, const void* u, const void* v, const void* w, void* eta_out, void* w_out,
+                        void* stream) {
+  if (!c || !u || !v || !w || !eta_out || !w_out) return SISL_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    KScope k(c, SISL_K_OTHER, st, 1);
+    launch_split_diag<T>(c->d, coef_of<T>(c), (const T*)u, (const T*)v, (const T*)w, (T*)eta_out, (T*)w_out, st);
+  };
+  if (c->grid.dtype == SISL_F64) run(double{});
+  else run(float{});
+  return check_cuda();
+}
+
+int sisl_split_step(SislCore* c, const SislState* in, const SislState* out, int ns, double alpha, double eps_l,
+                    const void* tau_damp, const void* const phys_tend[4], void* ws, size_t ws_bytes, void* stream) {
+  if (!c || !in || !out || !tau_damp || ns < 1 || !(alpha >= 0.0 && alpha <= 1.0) || !(eps_l >= 0.0))
+    return SISL_ERR_ARG;
+  const void* need_in[] = {in->u, in->v, in->w, in->eta_dot, in->pi_p, in->th_p};
+  const void* need_out[] = {out->u, out->v, out->w, out->eta_dot, out->pi_p, out->th_p};
+  for (const void* p : need_in)
+    if (!p) return SISL_ERR_ARG;
+  for (const void* p : need_out) {
+    if (!p) return SISL_ERR_ARG;
+    for (const void* q : need_in)
+      if (p == q) return SISL_ERR_ARG;  // out must not alias in
+  }
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_SPLIT)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (c->grid.dtype == SISL_F64)
+    split_step_impl<double>(c, in, out, ns, alpha, eps_l, (const double*)tau_damp, phys_tend, ws, st);
+  else
+    split_step_impl<float>(c, in, out, ns, alpha, eps_l, (const float*)tau_damp, phys_tend, ws, st);
+  return check_cuda();
 }
 
 int sisl_ffsl_advect(SislCore* c, const void* field, const void* u, const void* v, const void* eta, void* out,

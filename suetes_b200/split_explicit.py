@@ -1,0 +1,139 @@
+"""``SplitExplicitStepper3D`` on the B200 kernels.
+
+Mirrors ``suetes/regional3d/steppers.py:1076-1737``: a WRF-style RK3 step
+whose three stages each evaluate the slow tendencies (explicit dynamics,
+3rd-order upwind flux advection, the physics and hyperdiffusion
+tendencies of the step start) and advance the fast acoustic modes with a
+forward-backward horizontal / vertically implicit sub-cycle.  The stages
+run in one ``sisl_split_step`` call; the physics suite, the tracer
+transport (``sisl_ffsl_advect``), ``bc_fn``, the final eta_dot diagnosis
+(``sisl_split_diagnose``) and the equation of state (``sisl_eos``) follow
+on the host side in the reference's order (steppers.py:1233-1270).
+"""
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import check
+from .boundaries import LateralRelaxation
+from .core import F64, fortran
+
+LOCS4 = (("u", "u"), ("v", "v"), ("w", "w"), ("th_v", "m"))
+
+
+class SplitExplicitStepper3D:
+    """Split-explicit RK3 core (steppers.py:1076-1114 for the constructor)."""
+
+    def __init__(self, physics, dt, ns, alpha=0.55):
+        from .steppers import FluxFormAdvector
+        self.physics, self.dt, self.ns, self.alpha = physics, dt, ns, alpha
+        self.ns_stage1 = max(1, round(ns / 3))
+        self.ns_stage2 = max(1, round(ns / 2))
+        self.ns_stage3 = ns
+        self.dtau_stage1 = (dt / 3.0) / float(self.ns_stage1)
+        self.dtau_stage2 = (dt / 2.0) / float(self.ns_stage2)
+        self.dtau_stage3 = dt / float(self.ns_stage3)
+        self.ffsl_advector = FluxFormAdvector(physics.grid, dt, periodic_axes=physics.op.periodic_axes,
+                                              physics=physics)
+        self._tau = {}
+
+    def core(self, dtype):
+        return self.physics.core(dtype, self.dt, self.alpha)
+
+    def _tau_damp(self, core):
+        key = (core.dtype, str(core.device))
+        if key not in self._tau:
+            self._tau[key] = core.field(self.physics.tau_damp, "w")
+        return self._tau[key]
+
+    def _diagnose(self, core, u, v, w):
+        """``_diagnose_eta_dot`` (steppers.py:1272-1310): (eta_dot, w)."""
+        eta, w_out = core.new("w"), core.new("w")
+        check(core.lib.sisl_split_diagnose(core.handle, u.data_ptr(), v.data_ptr(), w.data_ptr(), eta.data_ptr(),
+                                           w_out.data_ptr(), core.stream), "sisl_split_diagnose")
+        return eta, w_out
+
+    def _eos(self, core, th_v, pi):
+        ph = self.physics
+        th_p = fortran(torch.as_tensor(th_v).to(core.device, F64) - ph.theta_bg, dtype=core.dtype)
+        pi_p = fortran(torch.as_tensor(pi).to(core.device, F64) - ph.pi_bg, dtype=core.dtype)
+        rho = core.new("m")
+        check(core.lib.sisl_eos(core.handle, th_p.data_ptr(), pi_p.data_ptr(), rho.data_ptr(), core.stream),
+              "sisl_eos")
+        return rho
+
+    def step_device(self, core, st, phys=None):
+        """The three RK3 stages from a diagnosed device state ``st`` (dict of
+        u, v, w, eta_dot, pi_p, th_p, rho in the core's layout) into a new
+        dict of the same fields (rho copied through)."""
+        from .steppers import DeviceState
+        ds_in = DeviceState(core, st)
+        ds_out = DeviceState(core)
+        sin, sout = ds_in.c_struct(), ds_out.c_struct()
+        arr = (ctypes.c_void_p * 4)()  # all null: no physics tendencies
+        if phys is not None:
+            arr = (ctypes.c_void_p * 4)(*[t.data_ptr() if t is not None else None for t in phys])
+        ws, n = core.workspace(_lib.WS_SPLIT)
+        eps_l = float(self.physics.c.get("eps_l", 1e-12))
+        check(core.lib.sisl_split_step(core.handle, ctypes.byref(sin), ctypes.byref(sout), int(self.ns),
+                                       float(self.alpha), eps_l, self._tau_damp(core).data_ptr(), arr,
+                                       ws.data_ptr(), n, core.stream), "sisl_split_step")
+        return {k: ds_out.t[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p", "rho")}
+
+    def step(self, state, t, forcing, bc_fn, ml_params=None):
+        """SplitExplicitStepper3D.step (steppers.py:1117-1270).  As in the
+        reference, the input dict receives the diagnosed eta_dot and w."""
+        from .steppers import _dtype_of
+        ph, op = self.physics, self.physics.op
+        if "rho" not in state:
+            raise ValueError("the split-explicit step needs the density 'rho' in the state")
+        dtype = _dtype_of({k: state[k] for k in ("u", "v", "w")})
+        core = self.core(dtype)
+        f = core.field
+        u, v = f(state["u"], "u"), f(state["v"], "v")
+        eta, w = self._diagnose(core, u, v, f(state["w"], "w"))
+        state["eta_dot"], state["w"] = eta, w
+        pi_p = fortran(torch.as_tensor(state["pi"]).to(core.device, F64) - ph.pi_bg, dtype=dtype)
+        th_p = fortran(torch.as_tensor(state["th_v"]).to(core.device, F64) - ph.theta_bg, dtype=dtype)
+        rho = f(state["rho"], "m")
+        suite = ph.physics_suite
+        bg = ph.precompute_bg(ph.bg_state_ref())
+        phys = None
+        if suite is not None:  # steppers.py:1152-1173
+            sp = {"u": u, "v": v, "w": w, "th_v": f(state["th_v"], "m"), "pi": pi_p, "eta_dot": eta,
+                  "th_v_prime_u": op.avg(th_p, 0, "m", "u"), "th_v_prime_v": op.avg(th_p, 1, "m", "v"),
+                  "th_v_prime_w": op.avg(th_p, 2, "m", "w")}
+            for k in state:
+                if k not in sp:
+                    sp[k] = state[k]
+            pt = suite.get_explicit_tendencies(sp, bg, interior_mask=ph.interior_mask, ml_params=ml_params)
+            phys = [f(pt[k], loc) if k in pt else None for k, loc in LOCS4]
+        st = {"u": u, "v": v, "w": w, "eta_dot": eta, "pi_p": pi_p, "th_p": th_p, "rho": rho}
+        res = self.step_device(core, st, phys)
+        sn = dict(state)
+        sn.pop("_sisl_state", None)
+        sn.update({"u": res["u"], "v": res["v"], "w": res["w"], "eta_dot": res["eta_dot"],
+                   "pi": fortran(res["pi_p"].double() + ph.pi_bg, dtype=dtype),
+                   "th_v": fortran(res["th_p"].double() + ph.theta_bg, dtype=dtype), "rho": rho})
+        eps = ph.c.get("eps", 1e-15)
+        if suite is not None:  # steppers.py:1233-1247
+            state_t = {"u": u, "v": v, "eta_dot": eta}
+            for key in suite.tracer_keys:
+                if key in state:
+                    rq = self.ffsl_advector.advect_3d_split(rho * f(state[key], "m"), state_t, bg)
+                    sn[key] = rq / (sn["rho"] + eps)
+            sn = suite.apply_state_updates(sn)
+        if isinstance(bc_fn, LateralRelaxation):
+            sn = bc_fn.apply_state(sn, ph)
+        elif bc_fn is not None:
+            sn = bc_fn(sn, forcing)
+        sn["eta_dot"], sn["w"] = self._diagnose(core, f(sn["u"], "u"), f(sn["v"], "v"), f(sn["w"], "w"))
+        tmass = {}
+        if suite is not None:
+            tmass = {k: sn["rho"] * sn[k] for k in suite.tracer_keys if k in sn}
+        sn["rho"] = self._eos(core, sn["th_v"], sn["pi"])
+        for k, rq in tmass.items():
+            sn[k] = rq / (sn["rho"] + eps)
+        return sn

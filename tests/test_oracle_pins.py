@@ -370,3 +370,86 @@ def test_gmres_inversion_sweep(r):
     rhs = ph.linear_operator(x, bg, dt, alpha=0.55)
     xn = sol.solve(rhs, bg)
     assert float(sol.relative_residual(xn, rhs, bg)) < 1e-9
+
+
+# ---------------------------------------------------------------------------
+# Split-explicit oracle (oracle/split_explicit.py) pinned to the reference's
+# own split-explicit tests (tests/test_core_formula_regressions.py): the
+# Exner slow forcing carries the theta' flux (:130-166) and a complete step
+# keeps the closed-box density and passive-tracer budgets through the final
+# EOS and tracer reconciliation (:238-292), on their 8x8x5 flat box.
+# ---------------------------------------------------------------------------
+
+def _split_env(dt, suite=None):
+    from oracle.grid import RegionalGrid3D
+    from oracle.ops import CGridOperator3D
+    from oracle.euler import Euler3D
+    g = RegionalGrid3D(8, 8, 5, 2000.0, 2000.0, 500.0, 45.0, 0.0, h_func=lambda x, y: 0.0 * (x + y))
+    op = CGridOperator3D(g)
+    ph = Euler3D(g, op, C, dt=dt, N_bv=0.0, damp_height=1e9, max_damp=0.0, nu_div_factor=0.0, nu_h_factor=0.0,
+                 physics_suite=suite)
+    return g, op, ph
+
+
+def _split_base(ph, g):
+    z = lambda *s: torch.zeros(*s, dtype=torch.float64)
+    rho = C["p0"] / (C["Rd"] * ph.theta_bg) * ph.pi_bg ** (C["cvd"] / C["Rd"])
+    return {"u": z(g.nx + 1, g.ny, g.nz), "v": z(g.nx, g.ny + 1, g.nz), "w": z(g.nx, g.ny, g.nz + 1),
+            "eta_dot": z(g.nx, g.ny, g.nz + 1), "pi": ph.pi_bg.clone(), "th_v": ph.theta_bg.clone(), "rho": rho}
+
+
+def test_split_oracle_continuity_includes_theta_prime_flux():
+    from oracle.split_explicit import SplitExplicitStepper3D
+    g, op, ph = _split_env(0.2)
+    st = SplitExplicitStepper3D(ph, dt=0.2, ns=2, alpha=0.5)
+    s = _split_base(ph, g)
+    x = torch.arange(g.nx + 1, dtype=torch.float64)[:, None, None]
+    zz = torch.arange(g.nz, dtype=torch.float64)[None, None, :]
+    s["u"] = 3.0 + 0.15 * x + torch.zeros_like(s["u"])
+    thp = 4.0 + 0.3 * torch.arange(g.nx, dtype=torch.float64)[:, None, None] + 0.2 * zz + torch.zeros_like(s["th_v"])
+    s["th_v"] = ph.theta_bg + thp
+    s["rho"] = C["p0"] / (C["Rd"] * s["th_v"]) * s["pi"] ** (C["cvd"] / C["Rd"])
+    bg = st._bg()
+    actual = st._compute_slow_tendencies(s, bg, {}, {}, None)["pi"]
+    prime = {"u": s["u"], "v": s["v"], "w": s["w"], "eta_dot": s["eta_dot"], "pi": s["pi"] - ph.pi_bg,
+             "th_v": s["th_v"], "th_v_prime_u": op.avg(thp, 0, "m", "u"), "th_v_prime_v": op.avg(thp, 1, "m", "v"),
+             "th_v_prime_w": op.avg(thp, 2, "m", "w")}
+    linear = ph.get_tendencies(prime, bg, is_explicit=True)["pi"]
+    nonlinear = ph.nonlinear_pi_tendency(prime, thp, bg)
+    err = float((actual - (linear + nonlinear)).abs().max())
+    sig = float(nonlinear.abs().max())
+    assert sig > 1e-12 and err < 1e-11 * sig
+
+
+def test_split_oracle_conserves_density_and_tracer_mass():
+    from oracle.split_explicit import SplitExplicitStepper3D
+
+    class Tracer:
+        tracer_keys = ["q_test"]
+
+        def get_explicit_tendencies(self, state, bg, interior_mask=None, ml_params=None):
+            return {}
+
+        def apply_state_updates(self, state):
+            return state
+
+    dt = 0.02
+    g, op, ph = _split_env(dt, Tracer())
+    s = _split_base(ph, g)
+    iu = torch.arange(g.nx + 1, dtype=torch.float64)[:, None, None]
+    jv = torch.arange(g.ny + 1, dtype=torch.float64)[None, :, None]
+    s["u"] = 2.0 * torch.sin(math.pi * iu / g.nx) + torch.zeros_like(s["u"])
+    s["v"] = -1.5 * torch.sin(math.pi * jv / g.ny) + torch.zeros_like(s["v"])
+    x = torch.arange(g.nx, dtype=torch.float64)[:, None, None]
+    y = torch.arange(g.ny, dtype=torch.float64)[None, :, None]
+    s["q_test"] = 1.0 + 0.2 * torch.sin(2 * math.pi * x / g.nx) * torch.cos(2 * math.pi * y / g.ny) \
+        + torch.zeros_like(s["rho"])
+    vol = g.dx * g.dy * g.dz_m_full / g.m_factors["m"][..., None] ** 2
+    m0 = float((s["rho"] * vol).sum())
+    t0 = float((s["rho"] * s["q_test"] * vol).sum())
+    st = SplitExplicitStepper3D(ph, dt, ns=2, alpha=0.5)
+    moved = st.ffsl_advector.advect_3d_split(s["rho"] * s["q_test"], s, st._bg())
+    r = st.step(dict(s), 0.0, None, lambda a, f: a)
+    assert abs(float((r["rho"] * vol).sum()) - m0) / m0 < 1e-10
+    assert abs(float((r["rho"] * r["q_test"] * vol).sum()) - t0) / t0 < 1e-10
+    assert float(torch.linalg.norm(r["rho"] * r["q_test"] - moved) / torch.linalg.norm(moved)) < 1e-12
