@@ -64,6 +64,10 @@ def parse():
     ap.add_argument("--classes", action="store_true",
                     help="also time every GMRES kernel class separately (diagnostic)")
     ap.add_argument("--no-micro", action="store_true", help="skip the 384x384x96 microbenchmark leg")
+    ap.add_argument("--split-steps", type=int, default=5,
+                    help="timed steps of the split-explicit warm-bubble leg (0 disables the leg)")
+    ap.add_argument("--split-n", type=int, default=256, help="nx = ny of the split-explicit leg")
+    ap.add_argument("--split-nz", type=int, default=64, help="nz of the split-explicit leg")
     ap.add_argument("--c4", action="store_true",
                     help="also run the 192x192x64 60-step checkpointed fwd+VJP leg with its float64 Taylor test")
     ap.add_argument("--micro-solves", type=int, default=10,
@@ -324,6 +328,98 @@ def roofline_leg(args, local, world, cls, peak, peak_kind):
            "timed_in": "2 steps of the same workload with batched GMRES (CUDA events on the launching stream)"}
     del st, ds
     return out
+
+
+def split_leg(args, local, world, peak, peak_kind):
+    """The split-explicit RK3 core (``SplitExplicitStepper3D.step`` through
+    ``sisl_split_step``) on the 3-D warm bubble, float32 and float64, with the
+    device-resident state; the roofline of its acoustic sub-cycle (predictor,
+    column solve, corrector) timed with CUDA events on the launching stream,
+    and the float64 oracle on a window of the same workload on the host."""
+    from suetes_b200 import _lib
+    from suetes_b200.workloads import split_bubble
+    nx = ny = args.split_n
+    nz = args.split_nz
+    cells = nx * ny * nz
+    K, W = args.split_steps, 3
+    ident = lambda a, f: a
+    out = {"metric": "split-explicit cell-steps/s (warm bubble)", "unit": "cell-steps/s",
+           "config": {"workload": f"3-D warm bubble {nx}x{ny}x{nz}, dx = dz = 50 m, dt 0.5 s, ns 12 "
+                                  f"(RK3 stages of 4, 6 and 12 acoustic steps)", "steps": K, "warmup": W}}
+    for dtype, key in ((torch.float32, "f32"), (torch.float64, "f64")):
+        st, s = split_bubble(nx, ny, nz, dtype=dtype, device=f"cuda:{local}")
+        for _ in range(W):
+            s = st.step(s, 0.0, None, ident)
+        core = st.core(dtype)
+        if key == "f32":
+            core.timing_select(_lib.K_OTHER)
+        from suetes_b200.core import kernel_launches
+        torch.cuda.synchronize()
+        barrier(world)
+        l0 = kernel_launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for n in range(K):
+            s = st.step(s, n * 0.5, None, ident)
+        ev1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = dist_max(ev0.elapsed_time(ev1), world)
+        out[key] = {"value": world * cells * K / (ms / 1e3), "ms_per_step": ms / K,
+                    "gpu_launches_per_step": (kernel_launches() - l0) / K,
+                    "w_max": float(s["w"].abs().max())}
+        if key == "f32":
+            k_ms, k_n, k_bytes = core.timing_read()
+            core.timing_select(0)
+            k_ms = dist_max(k_ms, world)
+            achieved = k_bytes / (k_ms / 1e3) / 1e9 if k_ms else None
+            out["roofline"] = {"kernel": "split acoustic sub-cycle (predict + column + correct, stage init/end)",
+                               "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                               "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
+                               "alg_bytes_per_cell_substep": "62 s (predict 16, column 24, correct 22)",
+                               "share_of_step": k_ms / ms, "launches_timed": k_n}
+        del st, s
+    out["value"] = out["f32"]["value"]
+    if rank_of() == 0 and not args.no_cpu:
+        out["cpu_baseline"] = split_cpu_leg(nz)
+    return out
+
+
+def rank_of():
+    return int(os.environ.get("RANK", "0"))
+
+
+def split_cpu_leg(nz, window=32, steps=2):
+    """The float64 oracle of the split-explicit core on a window x window x
+    nz sample of the warm bubble."""
+    from oracle.grid import RegionalGrid3D
+    from oracle.ops import CGridOperator3D
+    from oracle.euler import Euler3D
+    from oracle.split_explicit import SplitExplicitStepper3D
+    import math
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    C = {"g": 9.81, "cp": 1004.0, "Rd": 287.0, "cvd": 717.0, "p0": 100000.0}
+    g = RegionalGrid3D(window, window, nz, 50.0, 50.0, 50.0, 0.0, 0.0)
+    op = CGridOperator3D(g)
+    ph = Euler3D(g, op, C, dt=0.5, N_bv=0.0, damp_height=2500.0, max_damp=0.05, nu_div_factor=0.03,
+                 nu_h_factor=0.03)
+    X, Y, Z = torch.meshgrid(g.x_m, g.y_m, g.z_m, indexing="ij")
+    r = torch.sqrt(X ** 2 + Y ** 2 + (Z - 1500.0) ** 2)
+    th = ph.theta_bg + torch.where(r < 1000.0, 2.0 * torch.cos(0.5 * math.pi * r / 1000.0) ** 2, torch.zeros_like(r))
+    zz = lambda *sh: torch.zeros(*sh, dtype=torch.float64)
+    s = {"u": zz(window + 1, window, nz), "v": zz(window, window + 1, nz), "w": zz(window, window, nz + 1),
+         "eta_dot": zz(window, window, nz + 1), "pi": ph.pi_bg.clone(), "th_v": th,
+         "rho": C["p0"] / (C["Rd"] * th) * ph.pi_bg ** (C["cvd"] / C["Rd"])}
+    st = SplitExplicitStepper3D(ph, 0.5, 12, alpha=0.55)
+    s = st.step(s, 0.0, None, lambda a, f: a)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s = st.step(s, 0.0, None, lambda a, f: a)
+    sec = (time.perf_counter() - t0) / steps
+    return {"value": window * window * nz / sec, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} split-explicit step(s) (after 1 warm-up) of a {window}x{window}x{nz} window of the "
+                      f"warm bubble, float64, oracle restatement of the reference JAX core (JAX not installed)"}
 
 
 def micro_leg(args, local, world, peak):
@@ -789,6 +885,10 @@ def run_ours(args):
     # ---- 384x384x96 kernel microbenchmarks ----
     if args.micro_solves >= 0 and not args.no_micro:
         line["micro"] = micro_leg(args, local, world, peak)
+
+    # ---- split-explicit RK3 core on the warm bubble ----
+    if args.split_steps > 0:
+        line["split_explicit"] = split_leg(args, local, world, peak, peak_kind)
 
     # ---- uneven-size ensemble under one CUDA graph per step ----
     if args.ens_members > 0:

@@ -1181,8 +1181,12 @@ void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int
     a.dtau = (T)dts[stage]; a.alpha = (T)alpha; a.nu_div = (T)c->s.nu_div;
     T* spare_u = w.upp2;
     T* spare_v = w.vpp2;
+    // algorithmic bytes, each distinct 3-D array once per kernel: init 12,
+    // and per sub-step predictor 16, column 24 (its Thomas sweep written and
+    // read back once), corrector 22
+    const double cellb = (double)sizeof(T) * d.nx * d.ny * d.nz;
     {
-      KScope k(c, SISL_K_OTHER, st, 1 + 3 * nst[stage]);
+      KScope k(c, SISL_K_OTHER, st, 1 + 3 * nst[stage], cellb * (12.0 + 62.0 * nst[stage]));
       launch_split_init<T>(d, a, st);
       for (int n = 0; n < nst[stage]; ++n) {
         launch_split_predict<T>(d, cf, a, st);
@@ -1192,8 +1196,8 @@ void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int
         std::swap(a.vpp, spare_v);
       }
     }
-    {
-      KScope k(c, SISL_K_OTHER, st, stage < 2 ? 2 : 1);
+    {  // stage state (17 arrays) and its eta_dot diagnosis (8)
+      KScope k(c, SISL_K_OTHER, st, stage < 2 ? 2 : 1, cellb * (stage < 2 ? 25.0 : 17.0));
       launch_split_end<T>(d, a, nst[stage], dst[0], dst[1], dst[2], dst[3], dst[4], dst[5], st);
       if (stage < 2) launch_split_diag<T>(d, cf, dst[0], dst[1], dst[2], dst[3], dst[2], st);
     }

@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(128) split_column_kernel(Dims d, Coef<T> c, Sp
   const T dx = (T)d.dx, dy = (T)d.dy;
   const T wsfc = kinematic(d, c, W, i, j, 0);
   T fz_lo = T(0), gam_lo = T(0), cprev = T(0), dprev = T(0);
+#pragma unroll 4
   for (int k = 0; k < nz; ++k) {
     T fz_hi = T(0), gam_hi = T(0);
     if (k + 1 < nz) {
@@ -334,6 +335,7 @@ __global__ void __launch_bounds__(128) split_column_kernel(Dims d, Coef<T> c, Sp
     const int p = im(d, i, j, nz - 1);
     a.ppp[p] = a.ppp[p] + xh;
   }
+#pragma unroll 4
   for (int k = nz - 2; k >= 0; --k) {
     const int p = im(d, i, j, k);
     const T x = a.dpr[p] - a.cpr[p] * xh;
@@ -344,6 +346,115 @@ __global__ void __launch_bounds__(128) split_column_kernel(Dims d, Coef<T> c, Sp
   }
   a.wpp[iw(d, i, j, 0)] = wsfc;
   a.wpp[iw(d, i, j, nz)] = T(0);
+}
+
+// The same column solve on tiles of PC columns (one block per tile and
+// row j) so that every thread works outside the recurrence: A1 the w-level
+// terms (explicit w'', the eta_dot flux, the coupling gamma) and A2 the
+// tridiagonal rows at every (level, column) pair, B one warp runs the
+// Thomas sweeps in shared memory, C the pi'' and w'' updates.  Arithmetic
+// is term for term that of split_column_kernel.
+template <typename T, int PT, int PC>
+__global__ void __launch_bounds__(PT) split_column_tile_kernel(Dims d, Coef<T> c, SplitArgs<T> a, T a2cp,
+                                                               T adcp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int nx = d.nx, nz = d.nz;
+  T* s_fz = sm;                      // [nz+1][PC]  eta_dot flux
+  T* s_gam = s_fz + (nz + 1) * PC;   // [nz+1][PC]  gamma
+  T* s_x = s_gam + (nz + 1) * PC;    // [nz][PC]    rhs -> d' -> delta pi
+  T* s_lo = s_x + nz * PC;           // [nz][PC]    lower
+  T* s_up = s_lo + nz * PC;          // [nz][PC]    upper -> c'
+  T* s_mn = s_up + nz * PC;          // [nz][PC]    main
+  const int i0 = blockIdx.x * PC, j = blockIdx.y, tid = threadIdx.x;
+  const T al = a.alpha, dtau = a.dtau, cp = (T)c.s.cp;
+  const T dx = (T)d.dx, dy = (T)d.dy;
+  const Winds<T> W{d, c, a.uh, a.vh};
+  const Grad<T> G{d, c, a.ppp};
+  for (int q = tid; q < (nz + 1) * PC; q += PT) {  // A1
+    const int k = q / PC, i = i0 + q % PC;
+    T fz = T(0), gam = T(0);
+    if (i < nx && k > 0 && k < nz) {
+      const int pw = iw(d, i, j, k);
+      const T thw = ld(c.thw, pw), rw = ld(c.rhow, pw);
+      const T wold = a.wpp[pw];
+      const T wex = wold + dtau * (a.sfw[pw] - cp * thw * G.gzw(i, j, k));
+      const T wav = (T(1) - al) * wold + al * wex;
+      fz = (wav - kinematic(d, c, W, i, j, k)) * rw * thw;
+      gam = a2cp * thw * rw * thw / ld(c.dzw, pw);
+      a.wpp[pw] = wex;
+    }
+    s_fz[q] = fz;
+    s_gam[q] = gam;
+  }
+  __syncthreads();
+  for (int q = tid; q < nz * PC; q += PT) {  // A2
+    const int k = q / PC, i = i0 + q % PC;
+    if (i >= nx) {
+      s_x[q] = T(0);
+      s_lo[q] = T(0);
+      s_up[q] = T(0);
+      s_mn[q] = T(1);
+      continue;
+    }
+    const int p = im(d, i, j, k);
+    const T mm = ld(c.mm, h_m(d, i, j));
+    const T dzm = ld(c.dzm, p), cpidz = ld(c.cpidz, p);
+    const int u0 = iu(d, i, j, k), v0 = iv(d, i, j, k);
+    const T fx0 = a.uh[u0] * ld(c.rdu, u0) * ld(c.thu, u0);
+    const T fx1 = a.uh[u0 + 1] * ld(c.rdu, u0 + 1) * ld(c.thu, u0 + 1);
+    const T fy0 = a.vh[v0] * ld(c.rdv, v0) * ld(c.thv, v0);
+    const T fy1 = a.vh[v0 + nx] * ld(c.rdv, v0 + nx) * ld(c.thv, v0 + nx);
+    const T div_h = mm * ((fx1 - fx0) / dx * mm / dzm + (fy1 - fy0) / dy * mm / dzm);
+    const T div_z = (s_fz[q + PC] - s_fz[q]) / dzm;
+    s_x[q] = dtau * (a.sfp[p] - cpidz * dzm * (div_h + div_z));
+    const T lower = -cpidz * s_gam[q], upper = -cpidz * s_gam[q + PC];
+    s_lo[q] = lower;
+    s_up[q] = upper;
+    s_mn[q] = T(1) - lower - upper;
+  }
+  __syncthreads();
+  if (tid < PC) {  // B
+    T cprev = T(0), dprev = T(0);
+    for (int k = 0; k < nz; ++k) {
+      const int q = k * PC + tid;
+      T cpk, dpk;
+      if (k == 0) {
+        const T inv = T(1) / s_mn[q];
+        cpk = s_up[q] * inv;
+        dpk = s_x[q] * inv;
+      } else {
+        const T lower = s_lo[q];
+        const T inv = T(1) / (s_mn[q] - lower * cprev);
+        cpk = s_up[q] * inv;
+        dpk = (s_x[q] - lower * dprev) * inv;
+      }
+      s_up[q] = cpk;
+      s_x[q] = dpk;
+      cprev = cpk;
+      dprev = dpk;
+    }
+    T xh = dprev;
+    for (int k = nz - 2; k >= 0; --k) {
+      const int q = k * PC + tid;
+      xh = s_x[q] - s_up[q] * xh;
+      s_x[q] = xh;
+    }
+  }
+  __syncthreads();
+  for (int q = tid; q < (nz + 1) * PC; q += PT) {  // C
+    const int k = q / PC, i = i0 + q % PC;
+    if (i >= nx) continue;
+    const int pw = iw(d, i, j, k);
+    if (k == 0) {
+      a.wpp[pw] = kinematic(d, c, W, i, j, 0);
+    } else if (k == nz) {
+      a.wpp[pw] = T(0);
+    } else {
+      a.wpp[pw] = a.wpp[pw] - adcp * ld(c.thw, pw) * ((s_x[q] - s_x[q - PC]) * ld(c.idzw, pw));
+    }
+    if (k < nz) a.ppp[pw] = a.ppp[pw] + s_x[q];
+  }
 }
 
 // PART 3 (steppers.py:1607-1626): the centred corrector of u'', v'' into
@@ -467,6 +578,14 @@ template <typename T>
 void launch_split_column(const Dims& d, const Coef<T>& c, const SplitArgs<T>& a, cudaStream_t st) {
   const double ad = (double)a.alpha * (double)a.dtau;
   const T a2cp = (T)(ad * ad * c.s.cp), adcp = (T)(ad * c.s.cp);
+  constexpr int PT = 256, PC = 32;
+  const size_t smem = (size_t)(6 * d.nz + 2) * PC * sizeof(T);
+  if (smem <= 200 * 1024) {  // tiles of 32 columns; the one-thread-per-column march beyond
+    static std::atomic<size_t> attr_bytes{0};  // per instantiation
+    ensure_smem_limit((const void*)split_column_tile_kernel<T, PT, PC>, attr_bytes, smem);
+    split_column_tile_kernel<T, PT, PC><<<dim3((d.nx + PC - 1) / PC, d.ny), PT, smem, st>>>(d, c, a, a2cp, adcp);
+    return;
+  }
   split_column_kernel<T><<<dim3((d.nx + 127) / 128, d.ny), 128, 0, st>>>(d, c, a, a2cp, adcp);
 }
 

@@ -99,7 +99,7 @@ class SplitExplicitStepper3D:
         th_p = fortran(torch.as_tensor(state["th_v"]).to(core.device, F64) - ph.theta_bg, dtype=dtype)
         rho = f(state["rho"], "m")
         suite = ph.physics_suite
-        bg = ph.precompute_bg(ph.bg_state_ref())
+        bg = ph.precompute_bg(ph.bg_state_ref()) if suite is not None else None  # read by the suite only
         phys = None
         if suite is not None:  # steppers.py:1152-1173
             sp = {"u": u, "v": v, "w": w, "th_v": f(state["th_v"], "m"), "pi": pi_p, "eta_dot": eta,

@@ -86,6 +86,30 @@ def rising_bubble(nx=64, ny=64, nz=48, dx=50.0, amp=2.0, radius=1000.0, center=(
     return stepper, state, None
 
 
+def split_bubble(nx=256, ny=256, nz=64, dx=50.0, amp=2.0, radius=1000.0, center=(0.0, 0.0, 1500.0), dtype=F32,
+                 device="cuda", dt=0.5, ns=12):
+    """The 3-D warm bubble of ``rising_bubble`` (isentropic, flat, dx = dz)
+    for the split-explicit core: ns acoustic steps per large step as in the
+    reference's rising-bubble comparison (rising_bubble_3d/run.py:104-105),
+    the factory's split-explicit stabilisation, damping above 2.5 km."""
+    grid = RegionalGrid3D(nx, ny, nz, dx, dx, dx, 0.0, 0.0, device=device)
+    op = CGridOperator3D(grid)
+    bgp = Euler3D(grid, op, CONSTANTS, dt=dt, N_bv=0.0)
+    c = CONSTANTS
+    X, Y, Zc = torch.meshgrid(grid.x_m, grid.y_m, grid.z_m, indexing="ij")
+    r = torch.sqrt((X - center[0]) ** 2 + (Y - center[1]) ** 2 + (Zc - center[2]) ** 2)
+    th = bgp.theta_bg + torch.where(r < radius, amp * torch.cos(0.5 * math.pi * r / radius) ** 2, torch.zeros_like(r))
+    rho = c["p0"] / (c["Rd"] * th) * bgp.pi_bg ** (c["cvd"] / c["Rd"])
+    z = lambda *s: torch.zeros(*s, dtype=F64, device=grid.device)
+    state = {"u": z(nx + 1, ny, nz), "v": z(nx, ny + 1, nz), "w": z(nx, ny, nz + 1), "eta_dot": z(nx, ny, nz + 1),
+             "pi": bgp.pi_bg.clone(), "th_v": th, "rho": rho}
+    stepper, _ = build_dynamical_core("split-explicit", grid, op, c, state, dt=dt, ns=ns, N_bv=0.0,
+                                      damp_height=2500.0, max_damp=0.05)
+    for k in ("u", "v", "w", "eta_dot", "rho"):
+        state[k] = state[k].to(dtype)
+    return stepper, state
+
+
 def box_energy_objective(stepper, num_steps, last=10, u_ref=10.0, x_box=(5000.0, 25000.0), z_box=(1000.0, 6000.0)):
     """``objective(n, state)`` for ``trajectory_vjp``: J = mean over the last
     ``last`` of ``num_steps`` states of the box-averaged kinetic energy of
