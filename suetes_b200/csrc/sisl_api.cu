@@ -638,7 +638,7 @@ struct SWork {
   T* vel[12];
   T *u_in, *v_in, *w_in, *pi_in, *th_in, *tth, *res;
   T *ru, *rv, *rw, *rp, *tha, *reta;
-  T *hyp[4], *htmp[4];
+  T *hyp[4], *htmp[4], *hgxy[8];
   T *ku, *kv, *kw, *kp;
   T *su, *sv;
   T* div;
@@ -656,6 +656,7 @@ SWork<T> carve_step(Carver& cv, const Dims& d, int R, bool refine) {
   w.tth = F(LOC_M); w.res = F(LOC_W);
   w.ru = F(LOC_U); w.rv = F(LOC_V); w.rw = F(LOC_W); w.rp = F(LOC_M); w.tha = F(LOC_M); w.reta = F(LOC_W);
   for (int q = 0; q < 4; ++q) { w.hyp[q] = F(LOC_M); w.htmp[q] = F(LOC_M); }
+  for (int q = 0; q < 8; ++q) w.hgxy[q] = F(q < 4 ? LOC_U : LOC_V);
   w.ku = F(LOC_U); w.kv = F(LOC_V); w.kw = F(LOC_W); w.kp = F(LOC_M);
   w.su = F(LOC_U); w.sv = F(LOC_V);
   w.div = F(LOC_M);
@@ -695,8 +696,10 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
   if (c->s.nu_h > 0.0) {
     PtrTable<T> t4{}, o4{};
     for (int q = 0; q < 4; ++q) { t4.p[q] = w.htmp[q]; o4.p[q] = w.hyp[q]; }
-    KScope k(c, SISL_K_EXPLICIT, st, 3);
-    launch_hyper<T>(d, cf, u, v, wv, th, t4, o4, st);
+    KScope k(c, SISL_K_EXPLICIT, st, 5);
+    PtrTable<T> g8{};
+    for (int q = 0; q < 8; ++q) g8.p[q] = w.hgxy[q];
+    launch_hyper<T>(d, cf, u, v, wv, th, t4, o4, g8, st);
     for (int q = 0; q < 4; ++q) ein.hyper[q] = w.hyp[q];
   }
   {
@@ -935,8 +938,10 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
   if (hyp) {
     PtrTable<T> t4{}, o4{};
     for (int q = 0; q < 4; ++q) { t4.p[q] = w.htmp[q]; o4.p[q] = w.hyp[q]; }
-    KScope k(c, SISL_K_EXPLICIT, st, 3);
-    launch_hyper<T>(d, cf, u, vv, wv, th, t4, o4, st);
+    KScope k(c, SISL_K_EXPLICIT, st, 5);
+    PtrTable<T> g8{};
+    for (int q = 0; q < 8; ++q) g8.p[q] = w.hgxy[q];
+    launch_hyper<T>(d, cf, u, vv, wv, th, t4, o4, g8, st);
     for (int q = 0; q < 4; ++q) ein.hyper[q] = w.hyp[q];
   }
   {
@@ -1084,7 +1089,7 @@ struct SplitWork {
   T* sf[5];
   T* tend[6];
   T* adv[4];
-  T *hyp_t[4], *hyp_s[4], *htmp[4];
+  T *hyp_t[4], *hyp_s[4], *htmp[4], *hgxy[8];
   T *cpr, *dpr;
   T* st[2][6];  // stage states: u, v, w, eta, pi', th'
 };
@@ -1104,6 +1109,7 @@ void carve_split(Carver& cv, const Dims& d, SplitWork<T>& w) {
     w.hyp_s[q] = f(LOC_M);
     w.htmp[q] = f(LOC_M);
   }
+  for (int q = 0; q < 8; ++q) w.hgxy[q] = f(q < 4 ? LOC_U : LOC_V);
   w.cpr = f(LOC_M);
   w.dpr = f(LOC_M);
   const int s_loc[6] = {LOC_U, LOC_V, LOC_W, LOC_W, LOC_M, LOC_M};
@@ -1137,9 +1143,11 @@ void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int
     for (int q = 0; q < 4; ++q) t.p[q] = a[q];
     return t;
   };
+  PtrTable<T> g8{};
+  for (int q = 0; q < 8; ++q) g8.p[q] = w.hgxy[q];
   if (hyp_t) {
-    KScope k(c, SISL_K_EXPLICIT, st, 3);
-    launch_hyper<T>(d, cf, s0[0], s0[1], s0[2], s0[5], table4(w.htmp), table4(w.hyp_t), st);
+    KScope k(c, SISL_K_EXPLICIT, st, 5);
+    launch_hyper<T>(d, cf, s0[0], s0[1], s0[2], s0[5], table4(w.htmp), table4(w.hyp_t), g8, st);
   }
   const int nst[3] = {std::max(1, (int)std::nearbyint(ns / 3.0)), std::max(1, (int)std::nearbyint(ns / 2.0)), ns};
   const double dts[3] = {(c->s.dt / 3.0) / nst[0], (c->s.dt / 2.0) / nst[1], c->s.dt / nst[2]};
@@ -1150,8 +1158,8 @@ void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int
     // ---- slow tendencies (steppers.py:1362-1465) ----
     const T* hyp[4] = {nullptr, nullptr, nullptr, nullptr};
     if (hyp_s) {
-      KScope k(c, SISL_K_EXPLICIT, st, 3 + (hyp_t ? 4 : 0));
-      launch_hyper<T>(d, cf, cur[0], cur[1], cur[2], cur[5], table4(w.htmp), table4(w.hyp_s), st);
+      KScope k(c, SISL_K_EXPLICIT, st, 5 + (hyp_t ? 4 : 0));
+      launch_hyper<T>(d, cf, cur[0], cur[1], cur[2], cur[5], table4(w.htmp), table4(w.hyp_s), g8, st);
       if (hyp_t)
         for (int q = 0; q < 4; ++q) launch_split_axpy<T>(field_size(d, LOC_M), w.hyp_t[q], w.hyp_s[q], st);
       for (int q = 0; q < 4; ++q) hyp[q] = w.hyp_s[q];
@@ -1336,6 +1344,7 @@ size_t sisl_workspace_bytes(const SislCore* c, int what) {
       break;
     case SISL_WS_EXPLICIT:
       for (int q = 0; q < 8; ++q) cv.take(es * field_size(c->d, LOC_M));
+      for (int q = 0; q < 8; ++q) cv.take(es * field_size(c->d, q < 4 ? LOC_U : LOC_V));
       break;
     case SISL_WS_OPERATOR:
       for (int q = 0; q < 5; ++q) cv.take(es * field_size(c->d, loc_of_field(q)));
@@ -1689,8 +1698,10 @@ int sisl_tendencies(SislCore* c, int is_explicit, const void* const sp[6], void*
       PtrTable<T> t4{}, o4{};
       for (int q = 0; q < 4; ++q) o4.p[q] = (T*)cv.take(sizeof(T) * field_size(c->d, LOC_M));
       for (int q = 0; q < 4; ++q) t4.p[q] = (T*)cv.take(sizeof(T) * field_size(c->d, LOC_M));
-      KScope k(c, SISL_K_EXPLICIT, st, 3);
-      launch_hyper<T>(c->d, cf, ein.u, ein.v, ein.w, ein.th, t4, o4, st);
+      PtrTable<T> g8{};
+      for (int q = 0; q < 8; ++q) g8.p[q] = (T*)cv.take(sizeof(T) * field_size(c->d, q < 4 ? LOC_U : LOC_V));
+      KScope k(c, SISL_K_EXPLICIT, st, 5);
+      launch_hyper<T>(c->d, cf, ein.u, ein.v, ein.w, ein.th, t4, o4, g8, st);
       for (int q = 0; q < 4; ++q) ein.hyper[q] = o4.p[q];
     }
     ExplicitOut<T> eo{};

@@ -52,6 +52,58 @@ __global__ void hyper_lap_kernel(Dims d, Coef<T> c, PtrTable<T> src, PtrTable<T>
   dst.p[f][im(d, i, j, k)] = scale * L.lap(i, j, k);
 }
 
+// The same Laplacian in two passes: the terrain-following gradients at
+// every u face and v face once (hyper_grad_kernel), then the divergence of
+// the stored gradients (hyper_div_kernel), instead of re-forming twelve
+// face gradients per point.  The stored values are the ones HLap::lap forms
+// in registers, so the two paths agree bitwise.
+template <typename T>
+__global__ void hyper_grad_kernel(Dims d, Coef<T> c, PtrTable<T> src, PtrTable<T> gxy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kz = blockIdx.z * blockDim.z + threadIdx.z;
+  const int f = kz / d.nz, k = kz % d.nz;
+  if (i > d.nx || j > d.ny || f >= 4) return;
+  HLap<T> L{d, c, src.p[f]};
+  if (j < d.ny) gxy.p[f][iu(d, i, j, k)] = L.Gx(i, j, k);
+  if (i < d.nx) gxy.p[4 + f][iv(d, i, j, k)] = L.Gy(i, j, k);
+}
+
+template <typename T>
+__global__ void hyper_div_kernel(Dims d, Coef<T> c, PtrTable<T> gxy, PtrTable<T> dst, T scale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int kz = blockIdx.z * blockDim.z + threadIdx.z;
+  const int f = kz / d.nz, k = kz % d.nz;
+  if (i >= d.nx || j >= d.ny || f >= 4) return;
+  const int nz = d.nz;
+  const T* __restrict__ gx = gxy.p[f];
+  const T* __restrict__ gy = gxy.p[4 + f];
+  const int kl = max(k - 1, 0), kh = min(k + 1, nz - 1);
+  const int lv[3] = {kl, k, kh};
+  T gxm[3], gym[3], gx0 = T(0), gx1 = T(0), gy0 = T(0), gy1 = T(0);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const T a0 = ld(gx, iu(d, i, j, lv[q])), a1 = ld(gx, iu(d, i + 1, j, lv[q]));
+    const T b0 = ld(gy, iv(d, i, j, lv[q])), b1 = ld(gy, iv(d, i, j + 1, lv[q]));
+    gxm[q] = T(0.5) * (a0 + a1);
+    gym[q] = T(0.5) * (b0 + b1);
+    if (q == 1) { gx0 = a0; gx1 = a1; gy0 = b0; gy1 = b1; }
+  }
+  auto lvl = [&](int kk) { return kk == kl ? 0 : (kk == k ? 1 : 2); };
+  int al, ar, bl, br;
+  level_pair(k, nz, al, ar);
+  level_pair(k + 1, nz, bl, br);
+  const T iz0 = ld(c.idzw, iw(d, i, j, k)), iz1 = ld(c.idzw, iw(d, i, j, k + 1));
+  const T ex0 = (gxm[lvl(ar)] - gxm[lvl(al)]) * iz0, ex1 = (gxm[lvl(br)] - gxm[lvl(bl)]) * iz1;
+  const T ey0 = (gym[lvl(ar)] - gym[lvl(al)]) * iz0, ey1 = (gym[lvl(br)] - gym[lvl(bl)]) * iz1;
+  const T m = ld(c.mm, h_m(d, i, j));
+  const int p = im(d, i, j, k);
+  const T divx = m * (gx1 - gx0) * (T)(1.0 / d.dx) - ld(c.zxm, p) * T(0.5) * (ex0 + ex1);
+  const T divy = m * (gy1 - gy0) * (T)(1.0 / d.dy) - ld(c.zem, p) * T(0.5) * (ey0 + ey1);
+  dst.p[f][p] = scale * (divx + divy);
+}
+
 // ---------------------------------------------------------------------------
 // explicit tendencies.  mode 0: step inputs (u_in, v_in, w_in, pi_in, th_in,
 // tend_th, residual_n); mode 1: raw tendencies for the operator API.
@@ -303,12 +355,20 @@ __global__ void __launch_bounds__(256) finalize_kernel(Dims d, Coef<T> c, Finali
 
 template <typename T>
 void launch_hyper(const Dims& d, const Coef<T>& c, const T* u, const T* v, const T* w, const T* th,
-                  PtrTable<T> tmp4, PtrTable<T> out4, cudaStream_t st) {
+                  PtrTable<T> tmp4, PtrTable<T> out4, PtrTable<T> gxy8, cudaStream_t st) {
   dim3 blk(32, 4, 2);
   hyper_src_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, u, v, w, th, out4);
-  dim3 g2 = box_grid(d.nx, d.ny, 4 * d.nz, blk);
-  hyper_lap_kernel<T><<<g2, blk, 0, st>>>(d, c, out4, tmp4, T(1));
-  hyper_lap_kernel<T><<<g2, blk, 0, st>>>(d, c, tmp4, out4, (T)(-c.s.nu_h));
+  if (!gxy8.p[0]) {
+    dim3 g2 = box_grid(d.nx, d.ny, 4 * d.nz, blk);
+    hyper_lap_kernel<T><<<g2, blk, 0, st>>>(d, c, out4, tmp4, T(1));
+    hyper_lap_kernel<T><<<g2, blk, 0, st>>>(d, c, tmp4, out4, (T)(-c.s.nu_h));
+    return;
+  }
+  const dim3 gg = box_grid(d.nx + 1, d.ny + 1, 4 * d.nz, blk), gd = box_grid(d.nx, d.ny, 4 * d.nz, blk);
+  hyper_grad_kernel<T><<<gg, blk, 0, st>>>(d, c, out4, gxy8);
+  hyper_div_kernel<T><<<gd, blk, 0, st>>>(d, c, gxy8, tmp4, T(1));
+  hyper_grad_kernel<T><<<gg, blk, 0, st>>>(d, c, tmp4, gxy8);
+  hyper_div_kernel<T><<<gd, blk, 0, st>>>(d, c, gxy8, out4, (T)(-c.s.nu_h));
 }
 
 template <typename T>
@@ -346,7 +406,7 @@ void launch_finalize(const Dims& d, const Coef<T>& c, const FinalizeArgs<T>& fa,
 
 #define SISL_INST_EX(T)                                                                                        \
   template void launch_hyper<T>(const Dims&, const Coef<T>&, const T*, const T*, const T*, const T*,           \
-                                PtrTable<T>, PtrTable<T>, cudaStream_t);                                       \
+                                PtrTable<T>, PtrTable<T>, PtrTable<T>, cudaStream_t);                          \
   template void launch_explicit<T>(const Dims&, const Coef<T>&, const ExplicitIn<T>&, const ExplicitOut<T>&,   \
                                    int, cudaStream_t);                                                         \
   template void launch_corrector_theta<T>(const Dims&, const Coef<T>&, const T*, const T*, const T*, const T*, \

@@ -49,9 +49,11 @@ struct FinalizeArgs {
   Relax<T> relax;
 };
 
+// gxy8: scratch of the face gradients (p[0..3] u faces, p[4..7] v faces) for
+// the two-pass Laplacian, or all null for the one-pass kernel
 template <typename T>
 void launch_hyper(const Dims& d, const Coef<T>& c, const T* u, const T* v, const T* w, const T* th,
-                  PtrTable<T> tmp4, PtrTable<T> out4, cudaStream_t st);
+                  PtrTable<T> tmp4, PtrTable<T> out4, PtrTable<T> gxy8, cudaStream_t st);
 template <typename T>
 void launch_explicit(const Dims& d, const Coef<T>& c, const ExplicitIn<T>& in, const ExplicitOut<T>& out, int mode,
                      cudaStream_t st);
