@@ -41,22 +41,12 @@ __global__ void hyper_src_kernel(Dims d, const T* __restrict__ u, const T* __res
   out.p[3][p] = ld(th, p);
 }
 
-template <typename T>
-__global__ void hyper_lap_kernel(Dims d, Coef<T> c, PtrTable<T> src, PtrTable<T> dst, T scale) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int kz = blockIdx.z * blockDim.z + threadIdx.z;
-  const int f = kz / d.nz, k = kz % d.nz;
-  if (i >= d.nx || j >= d.ny || f >= 4) return;
-  HLap<T> L{d, c, src.p[f]};
-  dst.p[f][im(d, i, j, k)] = scale * L.lap(i, j, k);
-}
-
-// The same Laplacian in two passes: the terrain-following gradients at
-// every u face and v face once (hyper_grad_kernel), then the divergence of
-// the stored gradients (hyper_div_kernel), instead of re-forming twelve
-// face gradients per point.  The stored values are the ones HLap::lap forms
-// in registers, so the two paths agree bitwise.
+// The Cartesian horizontal Laplacian (diffusion.py:93-129) in two passes:
+// the terrain-following gradients at every u face and v face once
+// (hyper_grad_kernel, HLap::Gx/Gy), then the divergence of the stored
+// gradients (hyper_div_kernel), instead of re-forming twelve face
+// gradients per point (the one-pass form this replaced computed the same
+// values in registers; the fields agree bitwise).
 template <typename T>
 __global__ void hyper_grad_kernel(Dims d, Coef<T> c, PtrTable<T> src, PtrTable<T> gxy) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -358,12 +348,6 @@ void launch_hyper(const Dims& d, const Coef<T>& c, const T* u, const T* v, const
                   PtrTable<T> tmp4, PtrTable<T> out4, PtrTable<T> gxy8, cudaStream_t st) {
   dim3 blk(32, 4, 2);
   hyper_src_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, u, v, w, th, out4);
-  if (!gxy8.p[0]) {
-    dim3 g2 = box_grid(d.nx, d.ny, 4 * d.nz, blk);
-    hyper_lap_kernel<T><<<g2, blk, 0, st>>>(d, c, out4, tmp4, T(1));
-    hyper_lap_kernel<T><<<g2, blk, 0, st>>>(d, c, tmp4, out4, (T)(-c.s.nu_h));
-    return;
-  }
   const dim3 gg = box_grid(d.nx + 1, d.ny + 1, 4 * d.nz, blk), gd = box_grid(d.nx, d.ny, 4 * d.nz, blk);
   hyper_grad_kernel<T><<<gg, blk, 0, st>>>(d, c, out4, gxy8);
   hyper_div_kernel<T><<<gd, blk, 0, st>>>(d, c, gxy8, tmp4, T(1));

@@ -49,8 +49,8 @@ struct FinalizeArgs {
   Relax<T> relax;
 };
 
-// gxy8: scratch of the face gradients (p[0..3] u faces, p[4..7] v faces) for
-// the two-pass Laplacian, or all null for the one-pass kernel
+// gxy8: scratch of the face gradients (p[0..3] u faces, p[4..7] v faces) of
+// the two-pass Laplacian
 template <typename T>
 void launch_hyper(const Dims& d, const Coef<T>& c, const T* u, const T* v, const T* w, const T* th,
                   PtrTable<T> tmp4, PtrTable<T> out4, PtrTable<T> gxy8, cudaStream_t st);

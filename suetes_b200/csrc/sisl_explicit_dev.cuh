@@ -107,7 +107,8 @@ __device__ __forceinline__ T divergence(const Dims& d, const Coef<T>& c, const T
   return -ld(c.cpidz, im(d, i, j, k)) * (divh + (fz1 - fz0));
 }
 
-// Cartesian horizontal Laplacian of a mass field (diffusion.py:93-129).
+// Terrain-following face gradients of a mass field, the first pass of the
+// Cartesian horizontal Laplacian (diffusion.py:93-129).
 template <typename T>
 struct HLap {
   const Dims& d;
@@ -131,34 +132,6 @@ struct HLap {
     face_pair(fj, d.ny, d.py, l, r);
     const T deta = (F(i, r, k) - F(i, l, k)) * (T)(1.0 / d.dy) * ld(c.mv, h_v(d, i, fj));
     return deta - ld(c.zev, iv(d, i, fj, k)) * T(0.5) * (dzm(i, l, k) + dzm(i, r, k));
-  }
-  __device__ T lap(int i, int j, int k) const {
-    const int nz = d.nz;
-    // Gx at faces i, i+1 and Gy at faces j, j+1 on the levels k-1, k, k+1 (clamped)
-    const int kl = max(k - 1, 0), kh = min(k + 1, nz - 1);
-    const int lv[3] = {kl, k, kh};
-    T gxm[3], gym[3], gx0 = T(0), gx1 = T(0), gy0 = T(0), gy1 = T(0);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const T a0 = Gx(i, j, lv[q]), a1 = Gx(i + 1, j, lv[q]);
-      const T b0 = Gy(i, j, lv[q]), b1 = Gy(i, j + 1, lv[q]);
-      gxm[q] = T(0.5) * (a0 + a1);
-      gym[q] = T(0.5) * (b0 + b1);
-      if (q == 1) { gx0 = a0; gx1 = a1; gy0 = b0; gy1 = b1; }
-    }
-    // d/dz at w levels k and k+1 of the mass-point Gx_m, Gy_m (edge padded)
-    auto lvl = [&](int kk) { return kk == kl ? 0 : (kk == k ? 1 : 2); };
-    int al, ar, bl, br;
-    level_pair(k, nz, al, ar);
-    level_pair(k + 1, nz, bl, br);
-    const T iz0 = ld(c.idzw, iw(d, i, j, k)), iz1 = ld(c.idzw, iw(d, i, j, k + 1));
-    const T ex0 = (gxm[lvl(ar)] - gxm[lvl(al)]) * iz0, ex1 = (gxm[lvl(br)] - gxm[lvl(bl)]) * iz1;
-    const T ey0 = (gym[lvl(ar)] - gym[lvl(al)]) * iz0, ey1 = (gym[lvl(br)] - gym[lvl(bl)]) * iz1;
-    const T m = ld(c.mm, h_m(d, i, j));
-    const int p = im(d, i, j, k);
-    const T divx = m * (gx1 - gx0) * (T)(1.0 / d.dx) - ld(c.zxm, p) * T(0.5) * (ex0 + ex1);
-    const T divy = m * (gy1 - gy0) * (T)(1.0 / d.dy) - ld(c.zem, p) * T(0.5) * (ey0 + ey1);
-    return divx + divy;
   }
 };
 

@@ -155,3 +155,26 @@ def test_split_conserves_density_and_passive_tracer_mass():
     assert abs(float((res["rho"] * vol).sum()) - mass0) / mass0 < 1e-10
     assert abs(float((res["rho"] * res["q_test"] * vol).sum()) - tracer0) / tracer0 < 1e-10
     assert rel_l2(res["rho"] * res["q_test"], moved) < 1e-12
+
+
+def test_split_with_lateral_relaxation():
+    """bc_fn after the stages (steppers.py:1249-1253): the LateralRelaxation
+    blend against the same blend written out for the oracle."""
+    from suetes_b200 import x_relaxation
+    ost, pst, o = _pair(2.0, 4)
+    ph = o[2]
+    relax = x_relaxation(pst.physics.grid, 1500.0, 3.0)
+    mm, mu, mv = (relax.mask_m.double().cpu(), relax.mask_u.double().cpu(), relax.mask_v.double().cpu())
+
+    def obc(s, f):
+        s = dict(s)
+        for k, m, ext, bg in (("u", mu, 3.0, 0.0), ("v", mv, 0.0, 0.0), ("th_v", mm, 0.0, ph.theta_bg),
+                              ("pi", mm, 0.0, ph.pi_bg)):
+            s[k] = (1.0 - m[..., None]) * (s[k] - bg) + m[..., None] * ext + bg
+        return s
+
+    s0 = _state(o[2], o[0])
+    s0.pop("q")
+    so = ost.step(dict(s0), 0.0, None, obc)
+    sp = pst.step(to_cuda(s0), 0.0, None, relax)
+    _compare(sp, so, ph, 1e-10)
