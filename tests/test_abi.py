@@ -79,3 +79,36 @@ def test_argument_validation_without_gpu():
                                             ctypes.byref(out)) == -1
     assert lib.sisl_step_vjp_graph_create(0, None, None, None, None, None, None, None, None, None,
                                           ctypes.byref(out)) == -1
+
+
+def test_split_and_physics_entries_reject_missing_arguments():
+    """The physics-suite step and the split-explicit entries validate their
+    arguments before any CUDA call."""
+    import ctypes
+    from suetes_b200 import _lib
+    lib = _lib.load()
+    nul4 = (ctypes.c_void_p * 4)()
+    st = _lib.SislState()
+    assert lib.sisl_step_physics(None, None, None, None, nul4, None, None, 0, None, None) == -1
+    assert lib.sisl_step_physics(None, ctypes.byref(st), ctypes.byref(st), None, nul4, None, None, 0, None,
+                                 None) == -1
+    assert lib.sisl_split_step(None, ctypes.byref(st), ctypes.byref(st), 4, 0.55, 1e-12, None, nul4, None, 0,
+                               None) == -1
+    assert lib.sisl_split_diagnose(None, None, None, None, None, None, None) == -1
+    assert lib.sisl_workspace_bytes(None, _lib.WS_SPLIT) == 0
+
+
+def test_split_stepper_stage_counts_follow_python_rounding():
+    """round(ns/3), round(ns/2), ns acoustic steps (steppers.py:1106-1112):
+    Python's round, ties to even, as the C entry's nearbyint."""
+    from suetes_b200.split_explicit import SplitExplicitStepper3D
+
+    class Ph:  # the constructor reads only the grid and periodic axes
+        class op:
+            periodic_axes = ()
+        grid = None
+    for ns, want in ((1, (1, 1, 1)), (2, (1, 1, 2)), (3, (1, 2, 3)), (5, (2, 2, 5)), (7, (2, 4, 7)),
+                     (12, (4, 6, 12))):
+        s = SplitExplicitStepper3D(Ph, 1.0, ns)
+        assert (s.ns_stage1, s.ns_stage2, s.ns_stage3) == want, ns
+        assert abs(s.dtau_stage1 * s.ns_stage1 - 1.0 / 3.0) < 1e-15
