@@ -12,6 +12,7 @@ from .boundaries import LateralRelaxation, x_relaxation
 from .euler import Euler3D
 from .geometry import (GalChenSigma, HybridSigma, RegionalGrid3D, SleveSimple, StretchedSleveSimple)
 from .operators import CGridOperator3D, map_coordinates_linear, tensor_product_interp_3d
+from .output import AsyncSnapshotWriter, NetcdfSnapshots, SimulationOutputWriter, restart_seed
 from .physics import PhysicsSuite
 from .split_explicit import SplitExplicitStepper3D
 from .steppers import (DeviceState, FluxFormAdvector, PingPong, SemiImplicitSolver3D, SemiLagrangianAdvector3D,
@@ -22,5 +23,6 @@ __all__ = [
     "tensor_product_interp_3d", "map_coordinates_linear", "Euler3D", "VerticalPreconditioner",
     "SemiLagrangianAdvector3D", "SemiImplicitSolver3D", "FluxFormAdvector", "SISLStepper3D", "DeviceState",
     "StateRing", "StepGraph", "PingPong", "build_dynamical_core", "LateralRelaxation", "x_relaxation",
-    "PhysicsSuite", "SplitExplicitStepper3D",
+    "PhysicsSuite", "SplitExplicitStepper3D", "SimulationOutputWriter", "AsyncSnapshotWriter", "NetcdfSnapshots",
+    "restart_seed",
 ]
