@@ -249,12 +249,12 @@ class NetcdfSnapshots:
     (x, y[, z]) arrays (the stored (z, y, x) transposed back)."""
 
     def __init__(self, path, keys=None):
-        self._ds = scipy.io.netcdf_file(path, "r", mmap=False)
+        self._ds = scipy.io.netcdf_file(path, "r", mmap=True)  # records are read on access
         avail = [k for k, v in self._ds.variables.items()
                  if v.dimensions and v.dimensions[0] == "time" and k != "time"]
         self.keys = [k for k in (keys or avail) if k in avail]
         self.n = self._ds.variables["time"].shape[0]
-        self.times = np.array(self._ds.variables["time"][:])
+        self.times = np.array(self._ds.variables["time"][:], dtype=np.float64)
 
     def __len__(self):
         return self.n
@@ -263,8 +263,8 @@ class NetcdfSnapshots:
         i = range(self.n)[i]
         out = {}
         for k in self.keys:
-            a = np.array(self._ds.variables[k][i])
-            a = a.astype(a.dtype.newbyteorder("="))  # the file is big-endian
+            a = self._ds.variables[k][i]
+            a = a.astype(a.dtype.newbyteorder("="))  # a native-order copy of the big-endian record
             out[k] = np.transpose(a, tuple(reversed(range(a.ndim))))
         return out
 
