@@ -2156,7 +2156,8 @@ int sisl_split_diagnose(SislCore* c, const void* u, const void* v, const void* w
   cudaStream_t st = (cudaStream_t)stream;
   auto run = [&](auto tag) {
     using T = decltype(tag);
-    KScope k(c, SISL_K_OTHER, st, 1);
+    // u, v, w, z_xi_w, z_eta_w, dz_w in; eta_dot, w out
+    KScope k(c, SISL_K_OTHER, st, 1, 8.0 * sizeof(T) * c->d.nx * c->d.ny * c->d.nz);
     launch_split_diag<T>(c->d, coef_of<T>(c), (const T*)u, (const T*)v, (const T*)w, (T*)eta_out, (T*)w_out, st);
   };
   if (c->grid.dtype == SISL_F64) run(double{});
