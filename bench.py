@@ -373,7 +373,8 @@ def split_leg(args, local, world, peak, peak_kind):
             core.timing_select(0)
             k_ms = dist_max(k_ms, world)
             achieved = k_bytes / (k_ms / 1e3) / 1e9 if k_ms else None
-            out["roofline"] = {"kernel": "split acoustic sub-cycle (predict + column + correct, stage init/end, eta_dot diagnosis)",
+            out["roofline"] = {"kernel": "split acoustic sub-cycle (predict + column + correct, stage init/end, "
+                                         "eta_dot diagnosis)",
                                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
                                "alg_bytes_per_cell_substep": "62 s (predict 16, column 24, correct 22)",
