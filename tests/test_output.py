@@ -104,3 +104,14 @@ def test_async_writer_cpu_tensors_write_in_order(tmp_path):
             np.testing.assert_array_equal(rd[n]["u"], snaps[n]["u"].numpy().astype(np.float32))
     finally:
         rd.close()
+
+
+def test_file_without_snapshots_is_valid(tmp_path):
+    path = str(tmp_path / "empty.nc")
+    SimulationOutputWriter(path, _grid(), ["u"]).close()
+    f = scipy.io.netcdf_file(path, "r", mmap=False)
+    try:
+        assert f.variables["time"].shape == (0,) and "u" not in f.variables
+        assert f.variables["x"].shape == (6,)
+    finally:
+        f.close()
