@@ -93,3 +93,85 @@ def x_relaxation(grid, width_m, exterior_u, fields=("u", "v", "th_v", "pi")):
     mv = mask[:, None].expand(nx, ny + 1)
     return LateralRelaxation(mm, mu, mv, fields=fields,
                              exterior={"u": float(exterior_u), "v": 0.0, "th_v": 0.0, "pi": 0.0})
+
+
+def _avg_face_to_mass(f, axis):
+    n = f.shape[axis]
+    return 0.5 * (f.narrow(axis, 0, n - 1) + f.narrow(axis, 1, n - 1))
+
+
+def _avg_mass_to_face(f, axis, periodic):
+    n = f.shape[axis]
+    if periodic:
+        b = (0.5 * (f.select(axis, 0) + f.select(axis, n - 1))).unsqueeze(axis)
+        return torch.cat([b, _avg_face_to_mass(f, axis), b], dim=axis)
+    a = _avg_face_to_mass(f, axis)
+    return torch.cat([a.narrow(axis, 0, 1), a, a.narrow(axis, n - 2, 1)], dim=axis)
+
+
+class DaviesSponge:
+    """Davies lateral relaxation with directional outflow scaling
+    (boundaries.py:13-120): cos^2 weights over ``sponge_depth`` cells from
+    each lateral edge, reduced to ``outflow_factor`` where the flow leaves
+    the domain, the strongest edge weight blending u, v, th_v, q and pi
+    toward the external state.  Torch on the state's device, for use as (or
+    inside) a ``bc_fn``; ``get_interior_mask`` is the physics suites'
+    ``interior_mask``."""
+
+    BLEND_VARS = ("u", "v", "th_v", "q", "pi")
+
+    def __init__(self, grid, operators, sponge_depth=30, dt=30.0, tau_bndy_factor=10.0, outflow_factor=0.01):
+        self.grid, self.op = grid, operators
+        self.depth = sponge_depth
+        self.outflow_factor = outflow_factor
+        self.max_c = dt / (tau_bndy_factor * dt)  # kept for parity with the reference; the blend does not use it
+        self.masks = {loc: self._masks(grid.nx, grid.ny, sponge_depth, loc) for loc in ("u", "v", "m")}
+
+    @staticmethod
+    def _masks(nx, ny, depth, loc):
+        ix = torch.arange(nx + 1 if loc == "u" else nx, dtype=torch.float32)
+        iy = torch.arange(ny + 1 if loc == "v" else ny, dtype=torch.float32)
+        ox = 0.0 if loc == "u" else 0.5
+        oy = 0.0 if loc == "v" else 0.5
+        w = lambda d: torch.cos(0.5 * math.pi * torch.clamp(d / depth, 0.0, 1.0)) ** 2
+        return {"west": w(ix + ox)[:, None, None], "east": w(nx - (ix + ox))[:, None, None],
+                "south": w(iy + oy)[None, :, None], "north": w(ny - (iy + oy))[None, :, None]}
+
+    def get_interior_mask(self):
+        out = {}
+        for loc in ("u", "v", "m"):
+            m = self.masks[loc]
+            interior = 1.0 - torch.maximum(torch.maximum(m["west"], m["east"]), torch.maximum(m["south"], m["north"]))
+            if loc == "m":
+                out["th_v"] = interior
+                out["w"] = interior
+            else:
+                out[loc] = interior
+        return out
+
+    def blend(self, intermediate_state, external_state):
+        px = 0 in self.op.periodic_axes
+        py = 1 in self.op.periodic_axes
+        u, v = intermediate_state["u"], intermediate_state["v"]
+        out = {}
+        for k, f in intermediate_state.items():
+            if k not in self.BLEND_VARS or k not in external_state:
+                out[k] = f
+                continue
+            masks = self.masks.get(k, self.masks["m"])
+            if k == "u":
+                ue, ve = u, _avg_mass_to_face(_avg_face_to_mass(v, 1), 0, px)
+            elif k == "v":
+                ue, ve = _avg_mass_to_face(_avg_face_to_mass(u, 0), 1, py), v
+            else:
+                ue, ve = _avg_face_to_mass(u, 0), _avg_face_to_mass(v, 1)
+            ud, vd = ue.detach(), ve.detach()  # the directions carry no gradient
+            m = {n: t.to(device=f.device, dtype=f.dtype) for n, t in masks.items()}
+            one = torch.ones((), dtype=f.dtype, device=f.device)
+            of = torch.full((), self.outflow_factor, dtype=f.dtype, device=f.device)
+            c = torch.maximum(torch.maximum(m["west"] * torch.where(ud > 0, one, of),
+                                            m["east"] * torch.where(ud < 0, one, of)),
+                              torch.maximum(m["south"] * torch.where(vd > 0, one, of),
+                                            m["north"] * torch.where(vd < 0, one, of)))
+            out[k] = (1.0 - c) * f + c * external_state[k]
+        return out

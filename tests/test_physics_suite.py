@@ -67,3 +67,32 @@ def test_relaxation_blend_on_state_dict():
     assert torch.allclose(out["th_v"], (1 - m) * st["th_v"] + m * 301.5, rtol=0, atol=1e-12)
     assert torch.allclose(out["pi"].double(), (1 - m) * 0.91 + m * 0.9, rtol=0, atol=1e-7)
     assert out["pi"].dtype == st["pi"].dtype and out["w"] is st["w"]
+
+
+def test_davies_sponge_inflow_outflow():
+    """tests/test_dynamical_core_3d.py:282-333: with a 10 m/s westerly the
+    west edge (inflow) relaxes fully to the exterior, the east edge
+    (outflow) keeps (1 - outflow_factor) of the model state, the interior
+    is untouched; non-blended fields pass through."""
+    from suetes_b200 import DaviesSponge
+
+    class G:
+        nx, ny, nz = 32, 32, 15
+
+    class Op:
+        periodic_axes = ()
+    nx, ny, nz = 32, 32, 15
+    sp = DaviesSponge(G, Op, sponge_depth=5, dt=30.0, outflow_factor=0.01)
+    f64 = torch.float64
+    model = {"u": torch.full((nx + 1, ny, nz), 10.0, dtype=f64), "v": torch.zeros(nx, ny + 1, nz, dtype=f64),
+             "w": torch.zeros(nx, ny, nz + 1, dtype=f64), "th_v": torch.full((nx, ny, nz), 300.0, dtype=f64),
+             "pi": torch.ones(nx, ny, nz, dtype=f64), "q": torch.zeros(nx, ny, nz, dtype=f64)}
+    ext = {k: (torch.zeros_like(v) if k in ("u", "v", "w", "q") else v.clone()) for k, v in model.items()}
+    out = sp.blend(model, ext)
+    assert abs(float(out["u"][nx // 2, ny // 2, nz // 2]) - 10.0) < 1e-12
+    assert abs(float(out["u"][0, ny // 2, nz // 2])) < 1e-12
+    assert abs(float(out["u"][-1, ny // 2, nz // 2]) - 0.99 * 10.0) < 1e-6
+    assert out["w"] is model["w"]
+    mask = sp.get_interior_mask()
+    assert mask["u"].shape == (nx + 1, ny, 1) and mask["th_v"].shape == (nx, ny, 1)
+    assert float(mask["th_v"][nx // 2, ny // 2, 0]) == 1.0 and float(mask["u"][0, ny // 2, 0]) == 0.0
