@@ -175,3 +175,48 @@ class DaviesSponge:
                                             m["north"] * torch.where(vd < 0, one, of)))
             out[k] = (1.0 - c) * f + c * external_state[k]
         return out
+
+
+class BenchmarkSponge:
+    """Symmetric cos^2 relaxation along x and/or y for the benchmark cases
+    (boundaries.py:122-190): weight cos^2(pi d / (2 depth)) at boundary
+    distance d < depth, combined over the axes as 1 - (1 - w_x)(1 - w_y),
+    edge-padded to the u and v faces; ``blend(state, ext)`` relaxes
+    ``blend_vars`` toward ``ext``."""
+
+    def __init__(self, nx, ny=None, sponge_depth=10, axes=("x",), blend_vars=None):
+        self.nx, self.ny, self.sponge_depth, self.axes = nx, ny, sponge_depth, axes
+        if blend_vars is None:
+            blend_vars = (["u", "v", "th_v", "pi", "rho", "q_tr"] if ny is None
+                          else ["u", "v", "w", "th_v", "pi", "rho", "q_tr"])
+        self.blend_vars = list(blend_vars)
+
+        def weight(n, on):
+            if not on:
+                return torch.zeros(n, dtype=torch.float32)
+            i = torch.arange(n, dtype=torch.float32)
+            d = torch.minimum(i, n - 1 - i)
+            return torch.where(d < sponge_depth, torch.cos(0.5 * math.pi * d / sponge_depth) ** 2,
+                               torch.zeros_like(d))
+        wx = weight(nx, "x" in axes)
+        wy = weight(ny if ny is not None else 1, "y" in axes and ny is not None)
+        if ny is not None:
+            self.mask_m = (1.0 - (1.0 - wx[:, None]) * (1.0 - wy[None, :]))[:, :, None]
+            self.mask_u = torch.cat([self.mask_m, self.mask_m[-1:]], dim=0)
+            self.mask_v = torch.cat([self.mask_m, self.mask_m[:, -1:]], dim=1)
+        else:
+            self.mask_m = wx[:, None, None]
+            self.mask_u = torch.cat([self.mask_m, self.mask_m[-1:]], dim=0)
+            self.mask_v = self.mask_m
+        self.mask_w = self.mask_m
+
+    def blend(self, state_in, ext_state):
+        out = {}
+        for k, f in state_in.items():
+            if k in self.blend_vars and k in ext_state:
+                m = {"u": self.mask_u, "v": self.mask_v, "w": self.mask_w}.get(k, self.mask_m)
+                m = m.to(device=f.device, dtype=f.dtype)
+                out[k] = (1.0 - m) * f + m * ext_state[k]
+            else:
+                out[k] = f
+        return out

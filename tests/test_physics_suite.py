@@ -96,3 +96,22 @@ def test_davies_sponge_inflow_outflow():
     mask = sp.get_interior_mask()
     assert mask["u"].shape == (nx + 1, ny, 1) and mask["th_v"].shape == (nx, ny, 1)
     assert float(mask["th_v"][nx // 2, ny // 2, 0]) == 1.0 and float(mask["u"][0, ny // 2, 0]) == 0.0
+
+
+def test_benchmark_sponge_masks_and_blend():
+    """boundaries.py:122-190: cos^2 weights on the outer sponge_depth cells,
+    combined over x and y, edge-padded to the faces."""
+    import math
+    from suetes_b200 import BenchmarkSponge
+    sp = BenchmarkSponge(12, 10, sponge_depth=3, axes=("x", "y"))
+    assert sp.mask_m.shape == (12, 10, 1) and sp.mask_u.shape == (13, 10, 1) and sp.mask_v.shape == (12, 11, 1)
+    assert float(sp.mask_m[0, 5, 0]) == 1.0 and float(sp.mask_m[6, 5, 0]) == 0.0
+    w1 = math.cos(0.5 * math.pi / 3) ** 2
+    assert abs(float(sp.mask_m[1, 5, 0]) - w1) < 1e-6
+    assert abs(float(sp.mask_m[1, 1, 0]) - (1 - (1 - w1) ** 2)) < 1e-6
+    assert torch.equal(sp.mask_u[-1], sp.mask_u[-2])
+    st = {"u": torch.ones(13, 10, 4, dtype=torch.float64), "x_other": torch.ones(3)}
+    out = sp.blend(st, {"u": torch.zeros(13, 10, 4, dtype=torch.float64)})
+    assert float(out["u"][0, 5, 0]) == 0.0 and float(out["u"][6, 5, 0]) == 1.0 and out["x_other"] is st["x_other"]
+    slab = BenchmarkSponge(12, None, sponge_depth=3)
+    assert slab.mask_m.shape == (12, 1, 1) and "w" not in slab.blend_vars
