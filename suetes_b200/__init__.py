@@ -9,6 +9,7 @@ Public API mirrors the reference ``suetes.regional3d`` modules:
 """
 
 from .boundaries import BenchmarkSponge, DaviesSponge, LateralRelaxation, x_relaxation
+from .driver import Simulation
 from .euler import Euler3D
 from .geometry import (GalChenSigma, HybridSigma, RegionalGrid3D, SleveSimple, StretchedSleveSimple)
 from .operators import CGridOperator3D, map_coordinates_linear, tensor_product_interp_3d
@@ -24,5 +25,5 @@ __all__ = [
     "SemiLagrangianAdvector3D", "SemiImplicitSolver3D", "FluxFormAdvector", "SISLStepper3D", "DeviceState",
     "StateRing", "StepGraph", "PingPong", "build_dynamical_core", "LateralRelaxation", "x_relaxation",
     "PhysicsSuite", "SplitExplicitStepper3D", "SimulationOutputWriter", "AsyncSnapshotWriter", "NetcdfSnapshots",
-    "restart_seed", "DaviesSponge", "BenchmarkSponge",
+    "restart_seed", "DaviesSponge", "BenchmarkSponge", "Simulation",
 ]
