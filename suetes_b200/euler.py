@@ -31,6 +31,38 @@ def jnp_interp(x, xp, fp):
     return torch.where(x > xp[-1], fp[-1], f)
 
 
+class HyperFilter:
+    """4th-order terrain-following hyperdiffusion (diffusion.py:80-173) on
+    the CUDA kernels: ``get_tendencies`` returns the u, v, w and th_v
+    tendencies the explicit kernels add (two Cartesian horizontal Laplacians
+    at mass points, staggered back).  It is the filter ``Euler3D`` builds
+    (euler.py:124: the physics' ``nu_h``, ``nu_v = 0``); other coefficients
+    raise."""
+
+    def __init__(self, grid, operators, nu_h=1e6, nu_v=1e6, physics=None):
+        self.grid, self.op, self.nu_h, self.nu_v, self.physics = grid, operators, nu_h, nu_v, physics
+
+    def get_tendencies(self, state_prime, bg_precomputed):
+        ph = self.physics
+        if ph is None or self.nu_v != 0.0 or self.nu_h != ph.nu_h:
+            raise NotImplementedError("the CUDA hyperdiffusion is the filter of an Euler3D (its nu_h, nu_v = 0)")
+        g = self.grid
+        dtype = ph._dtype_of(state_prime)
+        z = lambda loc: torch.zeros(g.shape_of(loc), dtype=dtype, device=g.device)
+        sp = {"u": state_prime.get("u", z("u")), "v": state_prime.get("v", z("v")), "w": state_prime.get("w", z("w")),
+              "pi": state_prime.get("pi", z("m")), "eta_dot": state_prime.get("eta_dot", z("w"))}
+        if "th_v" in state_prime:
+            thp = fortran(state_prime["th_v"], dtype=F64) - fortran(bg_precomputed["th_v"], dtype=F64)
+        elif "th_v_prime_m" in state_prime:
+            thp = state_prime["th_v_prime_m"]
+        else:
+            thp = z("m")
+        _, pd = ph._tendencies(sp, thp.to(dtype), bg_precomputed, True)
+        has = {"u": "u" in state_prime, "v": "v" in state_prime, "w": "w" in state_prime,
+               "th_v": "th_v" in state_prime or "th_v_prime_m" in state_prime}
+        return {k: pd[q] for q, k in enumerate(("u", "v", "w", "th_v")) if has[k]}
+
+
 class Euler3D:
     """Dry non-hydrostatic Euler core: background state plus operators."""
 
@@ -71,6 +103,7 @@ class Euler3D:
             max_damp * 0.5 * (1.0 + torch.tanh(math.pi * (zw - damp_height) / (grid.Lz - damp_height) - math.pi / 2)),
             torch.zeros_like(zw))
         self._cores = {}
+        self.diffusion = HyperFilter(grid, operators, nu_h=self.nu_h, nu_v=0.0, physics=self)  # euler.py:124
 
     # ------------------------------------------------------------------
     def core(self, dtype, dt=None, alpha=0.55, bg=None, solver=None, use_limiter=False):

@@ -132,6 +132,16 @@ def tricubic_vjp(field, coords, cot, use_limiter=False, scale=1.0, out=None):
     return out
 
 
+def cubic_weight(p0, p1, p2, p3, t):
+    """The Catmull-Rom cubic through p1, p2 at fraction t (operators.py:134-144),
+    as the weights of p0..p3 the tricubic kernel applies (tensors or floats)."""
+    w0 = t * (-0.5 + t * (1.0 - 0.5 * t))
+    w1 = 1.0 + t * t * (-2.5 + 1.5 * t)
+    w2 = t * (0.5 + t * (2.0 - 1.5 * t))
+    w3 = t * t * (-0.5 + 0.5 * t)
+    return w0 * p0 + w1 * p1 + w2 * p2 + w3 * p3
+
+
 def tensor_product_interp_3d(field, coords, use_limiter=False):
     """Catmull-Rom tricubic at continuous indices (operators.py:146-209).
 

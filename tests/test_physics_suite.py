@@ -115,3 +115,13 @@ def test_benchmark_sponge_masks_and_blend():
     assert float(out["u"][0, 5, 0]) == 0.0 and float(out["u"][6, 5, 0]) == 1.0 and out["x_other"] is st["x_other"]
     slab = BenchmarkSponge(12, None, sponge_depth=3)
     assert slab.mask_m.shape == (12, 1, 1) and "w" not in slab.blend_vars
+
+
+def test_cubic_weight_matches_the_oracle():
+    from oracle.ops import cubic_weight as ocw
+    from suetes_b200.operators import cubic_weight
+    g = torch.Generator().manual_seed(3)
+    p = [torch.randn(50, generator=g, dtype=torch.float64) for _ in range(4)]
+    t = torch.rand(50, generator=g, dtype=torch.float64)
+    assert torch.allclose(cubic_weight(*p, t), ocw(*p, t), rtol=1e-13, atol=1e-13)
+    assert float(cubic_weight(1.0, 2.0, 3.0, 4.0, 0.0)) == 2.0 and float(cubic_weight(1.0, 2.0, 3.0, 4.0, 1.0)) == 3.0
