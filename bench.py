@@ -21,7 +21,6 @@ Default run (one JSON line on rank 0):
 """
 
 import argparse
-import datetime
 import json
 import math
 import os
@@ -430,7 +429,7 @@ def micro_leg(args, local, world, peak):
     standalone GMRES solves of N(0, 1) right-hand sides on the mountain-wave
     physics over flat terrain.  Achieved GB/s count each distinct array once."""
     import math as _m
-    from suetes_b200 import SemiImplicitSolver3D, SemiLagrangianAdvector3D
+    from suetes_b200 import SemiLagrangianAdvector3D
     from suetes_b200.operators import tensor_product_interp_3d, tricubic_vjp
     from suetes_b200.core import fortran
     from suetes_b200.workloads import mountain_wave
@@ -794,7 +793,6 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"roofline": r, "nx": args.nx, "ny": args.ny, "nz": args.nz}), flush=True)
         return
-    import suetes_b200 as sb
     from suetes_b200 import _lib
     from suetes_b200.workloads import mountain_wave
 

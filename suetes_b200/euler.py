@@ -14,8 +14,7 @@ import torch
 
 from . import _lib
 from ._lib import check, ptrs
-from .core import F64, Core, empty_field, fortran
-from .operators import CGridOperator3D
+from .core import F64, Core, fortran
 
 
 def jnp_interp(x, xp, fp):

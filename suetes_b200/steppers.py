@@ -20,7 +20,7 @@ import torch
 from . import _lib
 from ._lib import check, ptrs
 from .boundaries import LateralRelaxation
-from .core import F32, F64, empty_field, fortran, zeros_field
+from .core import F64, empty_field, fortran, zeros_field
 from .euler import Euler3D
 
 SOLVE_METHODS = {"batched": _lib.SISL_GMRES_BATCHED, "incremental": _lib.SISL_GMRES_INCREMENTAL}

@@ -6,7 +6,7 @@ integration) and the split-explicit core."""
 import pytest
 import torch
 
-from _cases import C, build
+from _cases import build
 
 pytestmark = pytest.mark.gpu
 

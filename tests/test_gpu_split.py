@@ -17,7 +17,7 @@ import math
 import pytest
 import torch
 
-from _cases import C, build, mountain, rel_l2, to_cpu, to_cuda
+from _cases import C, build, mountain, rel_l2, to_cuda
 
 pytestmark = pytest.mark.gpu
 
