@@ -736,7 +736,7 @@ template <typename T, int NT>
 void launch_pt_march(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                      cudaStream_t st) {
   const size_t smem = (size_t)d.nz * NT * sizeof(T);
-  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  static SmemLimit attr_bytes;  // per instantiation
   ensure_smem_limit((const void*)pt_march_kernel<T, NT>, attr_bytes, smem);
   pt_march_kernel<T, NT><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, y, out, active);
 }
@@ -745,7 +745,7 @@ template <typename T, int TPT, int TPC>
 void launch_pt_column(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                       cudaStream_t st) {
   const size_t smem = (size_t)(4 * d.nz) * TPC * sizeof(T);
-  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  static SmemLimit attr_bytes;  // per instantiation
   ensure_smem_limit((const void*)pt_column_kernel<T, TPT, TPC>, attr_bytes, smem);
   pt_column_kernel<T, TPT, TPC><<<dim3((d.nx + TPC - 1) / TPC, d.ny), TPT, smem, st>>>(d, c, y, out, active);
 }
@@ -754,7 +754,7 @@ template <typename T, int TPT, int TPC, int PU>
 void launch_pt_column_batched(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,
                               cudaStream_t st) {
   const size_t smem = (size_t)(4 * d.nz) * TPC * sizeof(T);
-  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  static SmemLimit attr_bytes;  // per instantiation
   ensure_smem_limit((const void*)pt_column_batched_kernel<T, TPT, TPC, PU>, attr_bytes, smem);
   pt_column_batched_kernel<T, TPT, TPC, PU>
       <<<dim3((d.nx + TPC - 1) / TPC, d.ny), TPT, smem, st>>>(d, c, y, out, active);

@@ -16,17 +16,34 @@
 
 namespace sisl {
 
-// Raises a kernel's dynamic shared-memory limit to at least `bytes` (never
-// lowers it).  Host threads that drive different cores call the launchers
-// concurrently, so the check-and-set runs under one lock.
-inline void ensure_smem_limit(const void* fn, std::atomic<size_t>& current, size_t bytes) {
-  if (bytes <= 48 * 1024 || bytes <= current.load()) return;
+// Per-device record of the dynamic shared-memory limit a kernel has been
+// raised to.  cudaFuncSetAttribute acts on the current device only, so each
+// device keeps its own entry (a process may drive cores on several devices).
+constexpr int SMEM_LIMIT_DEVICES = 64;
+struct SmemLimit {
+  std::atomic<size_t> bytes[SMEM_LIMIT_DEVICES];
+};
+
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes` (never lowers it).  Host threads that drive different cores
+// call the launchers concurrently, so the check-and-set runs under one lock.
+// The limit is recorded only when the attribute call succeeds; on failure
+// the launch that follows reports the error.
+inline void ensure_smem_limit(const void* fn, SmemLimit& limit, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  if (dev < 0 || dev >= SMEM_LIMIT_DEVICES) {  // no slot: set it every time
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return;
+  }
+  std::atomic<size_t>& current = limit.bytes[dev];
+  if (bytes <= current.load()) return;
   static std::mutex m;
   std::lock_guard<std::mutex> lock(m);
-  if (bytes > current.load()) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (bytes > current.load() &&
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess)
     current.store(bytes);
-  }
 }
 
 enum Loc { LOC_M = 0, LOC_U = 1, LOC_V = 2, LOC_W = 3 };

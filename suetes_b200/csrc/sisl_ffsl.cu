@@ -426,7 +426,7 @@ extern "C" int sisl_ffsl_lines_noalloc(int dtype, int n, int nlines, const void*
   using namespace sisl;
   if (n < 1 || nlines < 1 || !scalar || !cfl || !out) return SISL_ERR_ARG;
   if (dtype != SISL_F32 && dtype != SISL_F64) return SISL_ERR_ARG;
-  if ((size_t)(n + 1) * (size_t)nlines > (size_t)SISL_FFSL_NOALLOC_MAX_DOUBLES) return SISL_ERR_SCRATCH_LIMIT;
+  if (((size_t)n + 1) * (size_t)nlines > (size_t)SISL_FFSL_NOALLOC_MAX_DOUBLES) return SISL_ERR_SCRATCH_LIMIT;
   double* M = nullptr;
   int rc = line_scratch_address(&M);
   if (rc != SISL_OK) return rc;

@@ -448,13 +448,14 @@ int flat_grid(size_t n, int elems_per_block) {
 // Grid of a grid-stride Krylov kernel: every block resident at once (one
 // wave, no tail of a partial second wave), at most GM_MAXBLOCKS.
 int resident_grid(const void* fn, int threads, size_t smem, size_t n, int elems_per_block) {
-  static std::atomic<int> sms[16];  // SM count per device, found once
+  static std::atomic<int> sms[SMEM_LIMIT_DEVICES];  // SM count per device, found once
   int dev = 0;
   cudaGetDevice(&dev);
-  int ns = sms[dev & 15].load();
+  const bool slot = dev >= 0 && dev < SMEM_LIMIT_DEVICES;
+  int ns = slot ? sms[dev].load() : 0;
   if (ns == 0) {
     if (cudaDeviceGetAttribute(&ns, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || ns < 1) ns = 148;
-    sms[dev & 15].store(ns);
+    if (slot) sms[dev].store(ns);
   }
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1)
@@ -478,7 +479,7 @@ constexpr size_t DOTS_SMEM_MAX = 96 * 1024;
 template <typename T>
 void gm_dots(const T* Vb, size_t stride, int m, const T* w, size_t n, double* partial, GState* gs, int mode,
              int gated, cudaStream_t st) {
-  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  static SmemLimit attr_bytes;  // per instantiation
   ensure_smem_limit((const void*)dots_kernel<T>, attr_bytes, (size_t)DOTS_SMEM_MAX);
   int nt = (int)(DOTS_SMEM_MAX / ((size_t)(m + 1) * sizeof(double)));
   nt = nt >= 256 ? 256 : (nt / 32) * 32;
@@ -513,7 +514,7 @@ void gm_info(const GState* gs, GDevInfo* o, cudaStream_t st) { info_kernel<<<1, 
 void gm_begin_cycle(GState* gs, cudaStream_t st) { begin_cycle_kernel<<<1, 256, 0, st>>>(gs); }
 void gm_small_solve(GState* gs, int restart, cudaStream_t st) {
   const size_t smem = (size_t)restart * restart * sizeof(double);
-  static std::atomic<size_t> attr_bytes{0};
+  static SmemLimit attr_bytes;
   ensure_smem_limit((const void*)small_solve_kernel, attr_bytes, (size_t)GM_MAXR * GM_MAXR * sizeof(double));
   small_solve_kernel<<<1, 256, smem, st>>>(gs);
 }

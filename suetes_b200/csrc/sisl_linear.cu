@@ -618,7 +618,7 @@ template <typename T, int NT>
 void launch_precond_march(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                           cudaStream_t st) {
   const size_t smem = (size_t)d.nz * NT * sizeof(T);
-  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  static SmemLimit attr_bytes;  // per instantiation
   ensure_smem_limit((const void*)precond_march_kernel<T, NT>, attr_bytes, smem);
   // u and v pass straight through (steppers.py:247-249) unless aliased
   if (out.f[0] != r.f[0])
@@ -632,7 +632,7 @@ template <typename T, int PT, int PC>
 void launch_precond_tile(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                          cudaStream_t st) {
   const size_t smem = (size_t)(5 * d.nz + 1) * PC * sizeof(T);
-  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  static SmemLimit attr_bytes;  // per instantiation
   ensure_smem_limit((const void*)precond_tile_kernel<T, PT, PC>, attr_bytes, smem);
   dim3 grd((d.nx + PC - 1) / PC, d.ny);
   precond_tile_kernel<T, PT, PC><<<grd, PT, smem, st>>>(d, c, r, out, active);
@@ -642,7 +642,7 @@ template <typename T, int PT, int PC, int PU>
 void launch_precond_tile_batched(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                                  cudaStream_t st) {
   const size_t smem = (size_t)(5 * d.nz + 1) * PC * sizeof(T);
-  static std::atomic<size_t> attr_bytes{0};  // per instantiation
+  static SmemLimit attr_bytes;  // per instantiation
   ensure_smem_limit((const void*)precond_tile_batched_kernel<T, PT, PC, PU>, attr_bytes, smem);
   dim3 grd((d.nx + PC - 1) / PC, d.ny);
   precond_tile_batched_kernel<T, PT, PC, PU><<<grd, PT, smem, st>>>(d, c, r, out, active);

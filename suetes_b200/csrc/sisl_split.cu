@@ -581,7 +581,7 @@ void launch_split_column(const Dims& d, const Coef<T>& c, const SplitArgs<T>& a,
   constexpr int PT = 256, PC = 32;
   const size_t smem = (size_t)(6 * d.nz + 2) * PC * sizeof(T);
   if (smem <= 200 * 1024) {  // tiles of 32 columns; the one-thread-per-column march beyond
-    static std::atomic<size_t> attr_bytes{0};  // per instantiation
+    static SmemLimit attr_bytes;  // per instantiation
     ensure_smem_limit((const void*)split_column_tile_kernel<T, PT, PC>, attr_bytes, smem);
     split_column_tile_kernel<T, PT, PC><<<dim3((d.nx + PC - 1) / PC, d.ny), PT, smem, st>>>(d, c, a, a2cp, adcp);
     return;
