@@ -160,40 +160,8 @@ def measured_peaks():
 # CPU oracle on a window of the workload (baseline / reference arm)
 # ---------------------------------------------------------------------------
 def oracle_mountain_wave(nx, ny, nz, tol):
-    from oracle.euler import Euler3D
-    from oracle.grid import RegionalGrid3D, StretchedSleveSimple
-    from oracle.ops import CGridOperator3D
-    from oracle.steppers import build_dynamical_core
-
-    C = {"g": 9.81, "cp": 1004.0, "Rd": 287.0, "cvd": 717.0, "p0": 100000.0}
-    ridge = lambda x, y: 250.0 * torch.exp(-(x / 5000.0) ** 2) * torch.cos(math.pi * x / 4000.0) ** 2 + 0.0 * y
-    g = RegionalGrid3D(nx, ny, nz, 500.0, 500.0, 20000.0 / nz, 45.0, 0.0, h_func=ridge,
-                       transform=StretchedSleveSimple(2.5, 4000.0, 1.35))
-    op = CGridOperator3D(g)
-    bgp = Euler3D(g, op, C, dt=8.0, N_bv=0.01)
-    rho = C["p0"] / (C["Rd"] * bgp.theta_bg) * bgp.pi_bg ** (C["cvd"] / C["Rd"])
-    z = lambda *s: torch.zeros(*s, dtype=torch.float64)
-    st = {"u": z(nx + 1, ny, nz) + 10.0, "v": z(nx, ny + 1, nz), "w": z(nx, ny, nz + 1), "eta_dot": z(nx, ny, nz + 1),
-          "pi": bgp.pi_bg.clone(), "rho": rho, "th_v": bgp.theta_bg.clone()}
-    stepper, _ = build_dynamical_core("sisl", g, op, C, st, dt=8.0, alpha=0.5, nu_div_factor=0.0, nu_h_factor=0.0,
-                                      damp_height=12000.0, max_damp=0.5, N_bv=0.01, solver_tol=tol,
-                                      solver_maxiter=30, solver_restart=30)
-    n = round(4000.0 / g.dx)
-    i = torch.arange(nx, dtype=torch.float64)
-    d = torch.minimum(i, nx - 1 - i)
-    mask = torch.where(d < n, torch.cos(0.5 * math.pi * d / n) ** 2, torch.zeros_like(d))[:, None, None]
-    ph = stepper.physics
-
-    def bc(s, forcing):  # schaer_mountain_3d/run.py:111-126
-        out = dict(s)
-        for k in ("u", "v", "th_v", "pi", "rho"):
-            m = torch.cat([mask, mask[-1:]], dim=0) if k == "u" else mask
-            ext = {"u": torch.full_like(s["u"], 10.0), "v": torch.zeros_like(s["v"]), "th_v": ph.theta_bg,
-                   "pi": ph.pi_bg, "rho": ph.bg_state_ref()["rho"]}[k]
-            out[k] = (1.0 - m) * s[k] + m * ext
-        return out
-
-    return stepper, st, bc
+    from oracle.cases import mountain_wave
+    return mountain_wave(nx, ny, nz, solver_tol=tol)
 
 
 def cpu_leg(steps, warmup, window, nz, tol):

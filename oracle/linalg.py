@@ -65,11 +65,18 @@ def _safe_normalize(x, thresh=None):
 
 
 def _arnoldi_step(k, A, M, V, eps):
-    """One Arnoldi step: v = M(A(V_k)), one CGS pass, normalise."""
+    """One Arnoldi step: v = M(A(V_k)), one CGS pass, normalise.
+
+    ``V`` is the (restart + 1, n) basis; JAX projects on every column, and
+    the columns beyond k are still zero, so projecting on ``V[:k + 1]`` gives
+    the same coefficients (zeros for the rest) with a fraction of the work."""
     v = M(A(V[k]))
     v_norm0 = _norm(v)
-    h = torch.stack([torch.dot(V[i], v) for i in range(len(V))])
-    v = v - sum(h[i] * V[i] for i in range(len(V)))
+    Vk = V[:k + 1]
+    hk = Vk @ v
+    v = v - Vk.T @ hk
+    h = torch.zeros(V.shape[0], dtype=v.dtype)
+    h[:k + 1] = hk
     unit, vn1 = _safe_normalize(v, thresh=eps * v_norm0)
     return unit, h, vn1
 
@@ -104,7 +111,8 @@ def gmres(A, b, x0=None, *, tol=1e-5, atol=0.0, restart=20, maxiter=None, M=None
     k = 0
     arnoldi_steps = 0
     while k < maxiter and bool(r_norm > atol):
-        V = [unit_r] + [torch.zeros_like(b) for _ in range(restart)]
+        V = torch.zeros(restart + 1, size, dtype=b.dtype)
+        V[0] = unit_r
         if solve_method == "batched":
             H = torch.eye(restart, restart + 1, dtype=b.dtype)
             j = 0
@@ -160,7 +168,7 @@ def gmres(A, b, x0=None, *, tol=1e-5, atol=0.0, restart=20, maxiter=None, M=None
                 y[:j] = torch.linalg.solve_triangular(T, beta[:j, None], upper=True)[:, 0]
         else:
             raise ValueError(f"invalid solve_method {solve_method}")
-        dx = sum(y[i] * V[i] for i in range(restart))
+        dx = V[:restart].T @ y
         x = x + dx
         unit_r, r_norm = _safe_normalize(M(b - A(x)))
         k += 1
