@@ -34,7 +34,79 @@ __device__ __forceinline__ T gz_mass(const T* __restrict__ p, const T* __restric
           Ph = mul_rn(ld(p, base + kh * plane), sp);
   const T g0 = mul_rn(k == 0 ? Ph - P0 : P0 - Pl, ld(iz, base + k * plane));
   const T g1 = mul_rn(k + 1 == nz ? P0 - Pl : Ph - P0, ld(iz, base + (k + 1) * plane));
-  return T(0.5) * (g0 + g1);
+  return mul_rn(T(0.5), g0 + g1);
+}
+
+// Every value the five rows of one union-box point read.  Values that one
+// thread forms and carries or shares (scaled pressures, vertical gradients,
+// vertical fluxes) are rounded on their own before they get here, so the
+// rows give the same bits whichever kernel shape gathered the inputs.
+template <typename T>
+struct MvIn {
+  T PO, PX, PY, gmO, gmX, gmY;                  // scaled pi' at mass level km, d/dz at km (own, i-1, j-1)
+  T xu_f, thu, zxu, mu_f, fu_f;                 // u face (i, j, km)
+  T xv_f, thv, zev, mv_f, fv_f;                 // v face (i, j, km)
+  T vX0, vX1, vO0, vO1, uY0, uY1, uO0, uO1;     // neighbouring faces at km
+  T xw_k, xW_k, idzw_k, damp, thw, zxw, zew, gzw;  // w level k (interior rows at the clamped level)
+  T uwa, uwb, uwc, uwd, vwa, vwb, vwc, vwd, mw;  // winds at the levels around w level k
+  T rdu0, rdu1, thu0, thu1, rdv0, rdv1, thv0, thv1;  // flux factors of the own cell's faces at km
+  T fz0, fz1, cpidz, xp_k;                      // vertical fluxes (rounded), C_pi/dz_m, own pi' at km
+};
+
+// The five rows of one point (euler.py:374-439 through steppers.py:439-461),
+// L = (Lu, Lv, Lw, Le, Lp): the expressions of matvec_point, term for term.
+template <typename T>
+__device__ __forceinline__ void mv_rows(const Dims& d, const Coef<T>& c, const MvIn<T>& q, T xs, bool u_lock,
+                                        bool v_lock, bool wb, T (&L)[5]) {
+  const T adt = (T)(c.s.alpha * c.s.dt), cp = (T)c.s.cp, a = (T)c.s.alpha, ps = (T)c.s.ps;
+  const T idx = (T)(1.0 / d.dx), idy = (T)(1.0 / d.dy);
+  const T vat = T(0.25) * (q.vX0 + q.vX1 + q.vO0 + q.vO1) * xs;
+  const T tend_u = -cp * q.thu * ((q.PO - q.PX) * idx * q.mu_f - q.zxu * T(0.5) * (q.gmX + q.gmO)) + q.fu_f * vat;
+  L[0] = u_lock ? q.xu_f * xs : q.xu_f * xs - adt * tend_u;
+  const T uat = T(0.25) * (q.uY0 + q.uY1 + q.uO0 + q.uO1) * xs;
+  const T tend_v = -cp * q.thv * ((q.PO - q.PY) * idy * q.mv_f - q.zev * T(0.5) * (q.gmY + q.gmO)) - q.fv_f * uat;
+  L[1] = v_lock ? q.xv_f * xs : q.xv_f * xs - adt * tend_v;
+  L[2] = wb ? q.xw_k * xs : q.damp * q.xw_k * xs + adt * cp * q.thw * q.gzw;
+  const T uw = T(0.25) * (q.uwa + q.uwb + q.uwc + q.uwd) * xs, vw = T(0.25) * (q.vwa + q.vwb + q.vwc + q.vwd) * xs;
+  L[3] = wb ? q.xW_k * xs * q.idzw_k : a * (q.xW_k * xs + q.mw * (uw * q.zxw + vw * q.zew) - q.xw_k * xs);
+  const T fx0 = q.uO0 * q.rdu0 * q.thu0, fx1 = q.uO1 * q.rdu1 * q.thu1;
+  const T fy0 = q.vO0 * q.rdv0 * q.thv0, fy1 = q.vO1 * q.rdv1 * q.thv1;
+  const T divh = q.mw * q.mw * ((fx1 - fx0) * idx + (fy1 - fy0) * idy);
+  L[4] = q.xp_k * xs + adt * ps * q.cpidz * (xs * (divh + (q.fz1 - q.fz0)));
+}
+
+// Stores of one point's rows (residual mode out = b - L when b is given);
+// on a periodic axis the face-0 thread also writes the duplicate face n
+// (euler.py:412, 417).
+template <typename T>
+__device__ __forceinline__ void mv_store(const Dims& d, const CVec5<T>& b, const Vec5<T>& out, int i, int j, int k,
+                                         const T (&L)[5]) {
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const bool do_u = (k < nz) && (j < ny) && !(d.px && i == nx);
+  const bool do_v = (k < nz) && (i < nx) && !(d.py && j == ny);
+  const bool own = (i < nx && j < ny);
+  if (do_u) {
+    const int p = iu(d, i, j, k);
+    out.f[0][p] = b.f[0] ? ld(b.f[0], p) - L[0] : L[0];
+    if (d.px && i == 0) {
+      const int pn = iu(d, nx, j, k);
+      out.f[0][pn] = b.f[0] ? ld(b.f[0], pn) - L[0] : L[0];
+    }
+  }
+  if (do_v) {
+    const int p = iv(d, i, j, k);
+    out.f[1][p] = b.f[1] ? ld(b.f[1], p) - L[1] : L[1];
+    if (d.py && j == 0) {
+      const int pn = iv(d, i, ny, k);
+      out.f[1][pn] = b.f[1] ? ld(b.f[1], pn) - L[1] : L[1];
+    }
+  }
+  if (own) {
+    const int pw = i + nx * (j + ny * k);
+    out.f[2][pw] = b.f[2] ? ld(b.f[2], pw) - L[2] : L[2];
+    out.f[4][pw] = b.f[4] ? ld(b.f[4], pw) - L[3] : L[3];
+    if (k < nz) out.f[3][pw] = b.f[3] ? ld(b.f[3], pw) - L[4] : L[4];
+  }
 }
 
 // Branch-free load phase: every index is clamped into its array, all values
@@ -168,6 +240,206 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LV == 1 ? 6 : 4) : (LV 
 #pragma unroll
   for (int l = 0; l < LV; ++l)
     if (k0 + l <= d.nz) matvec_point(d, c, x, xs, b, out, i, j, k0 + l);
+}
+
+// ---------------------------------------------------------------------------
+// Column march: one thread per (i, j) column of the union box marching up
+// the levels of its z chunk (blockIdx.z of gridDim.z chunks).  Vertical
+// neighbours are carried in registers instead of reloaded: the scaled
+// pressures, the vertical gradients G(k) = (P(k) - P(k-1)) / dz_w(k) of the
+// own, i-1 and j-1 columns (the mass-level gradient is their average), the
+// vertical flux and the winds one level down.  The loads a level needs
+// first (pressures, 1/dz_w, the flux terms) are issued two levels ahead and
+// the rest one level ahead, so each thread keeps ~50 loads in flight.  The
+// rows are mv_rows on the same rounded inputs as matvec_point: bitwise the
+// other shapes.  Needs nz >= 2.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct MvA {  // first-needed loads of level k: pi' (mass level min(k, nz-1)) and
+  T pO, pX, pY, izO, izX, izY, W, rw, tw;  // 1/dz_w of the three columns, eta_dot rho_w th_w (w level k)
+};
+template <typename T>
+struct MvB {  // the rest of level k (faces at mass level min(k, nz-1), w-level terms at k)
+  T uO0, uO1, uY0, uY1, vO0, vO1, vX0, vX1, zxu, zev, rdu0, rdu1, thu0, thu1, rdv0, rdv1, thv0, thv1;
+  T xw, damp, zxw, zew, cpidz;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kernel(Dims d, Coef<T> c, CVec5<T> x,
+                                                                                  const double* xscale, CVec5<T> b,
+                                                                                  Vec5<T> out, const int* active) {
+  if (active && *active == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i > nx || j > ny) return;
+  const int kA = (int)((long)blockIdx.z * (nz + 1) / gridDim.z);
+  const int kB = (int)((long)(blockIdx.z + 1) * (nz + 1) / gridDim.z);
+  if (kA >= kB) return;
+  const T xs = xscale ? (T)(*xscale) : T(1);
+  const T sp = xs / (T)c.s.ps;
+  const int pm = nx * ny, pu = (nx + 1) * ny, pv = nx * (ny + 1);
+  const T* __restrict__ xu = x.f[0];
+  const T* __restrict__ xv = x.f[1];
+  const T* __restrict__ xw = x.f[2];
+  const T* __restrict__ xp = x.f[3];
+  const T* __restrict__ xW = x.f[4];
+  const int ic = min(i, nx - 1), jc = min(j, ny - 1);
+  const int il = (ic == 0) ? nx - 1 : ic - 1;
+  const int jl = (jc == 0) ? ny - 1 : jc - 1;
+  const int hO = ic + nx * jc, hX = il + nx * jc, hY = ic + nx * jl;
+  const int iuc = min(i, nx), jvc = min(j, ny);
+  const int uO = ic + (nx + 1) * jc, uY = ic + (nx + 1) * jl, pU = iuc + (nx + 1) * jc;
+  const int vO = ic + nx * jc, vX = il + nx * jc, pV = ic + nx * jvc;
+  auto lev_a = [&](int k) {
+    MvA<T> a;
+    const int km = min(k, nz - 1);
+    a.pO = ld(xp, hO + km * pm);
+    a.pX = ld(xp, hX + km * pm);
+    a.pY = ld(xp, hY + km * pm);
+    a.izO = ld(c.idzw, hO + k * pm);
+    a.izX = ld(c.idzw, hX + k * pm);
+    a.izY = ld(c.idzw, hY + k * pm);
+    a.W = ld(xW, hO + k * pm);
+    a.rw = ld(c.rhow, hO + k * pm);
+    a.tw = ld(c.thw, hO + k * pm);
+    return a;
+  };
+  auto lev_b = [&](int k) {
+    MvB<T> e;
+    const int km = min(k, nz - 1);
+    const int ou = km * pu, ov = km * pv;
+    e.uO0 = ld(xu, uO + ou);
+    e.uO1 = ld(xu, uO + ou + 1);
+    e.uY0 = ld(xu, uY + ou);
+    e.uY1 = ld(xu, uY + ou + 1);
+    e.vO0 = ld(xv, vO + ov);
+    e.vO1 = ld(xv, vO + ov + nx);
+    e.vX0 = ld(xv, vX + ov);
+    e.vX1 = ld(xv, vX + ov + nx);
+    e.zxu = ld(c.zxu, pU + ou);
+    e.zev = ld(c.zev, pV + ov);
+    e.rdu0 = ld(c.rdu, uO + ou);
+    e.rdu1 = ld(c.rdu, uO + ou + 1);
+    e.thu0 = ld(c.thu, uO + ou);
+    e.thu1 = ld(c.thu, uO + ou + 1);
+    e.rdv0 = ld(c.rdv, vO + ov);
+    e.rdv1 = ld(c.rdv, vO + ov + nx);
+    e.thv0 = ld(c.thv, vO + ov);
+    e.thv1 = ld(c.thv, vO + ov + nx);
+    e.xw = ld(xw, hO + k * pm);
+    e.damp = ld(c.damp, hO + k * pm);
+    e.zxw = ld(c.zxw, hO + k * pm);
+    e.zew = ld(c.zew, hO + k * pm);
+    e.cpidz = ld(c.cpidz, hO + km * pm);
+    return e;
+  };
+  const T mu_f = ld(c.mu, iuc + (nx + 1) * jc), fu_f = ld(c.fu, iuc + (nx + 1) * jc);
+  const T mv_f = ld(c.mv, ic + nx * jvc), fv_f = ld(c.fv, ic + nx * jvc);
+  const T mw = ld(c.mm, hO);
+  const bool u_lock = !d.px && (i == 0 || i == nx), v_lock = !d.py && (j == 0 || j == ny);
+  const bool ui = i < nx, vj = j < ny;
+  // carried state at level kA
+  MvA<T> a0 = lev_a(kA), a1 = lev_a(min(kA + 1, nz));
+  MvB<T> b0 = lev_b(kA);
+  T P0O = mul_rn(a0.pO, sp), P0X = mul_rn(a0.pX, sp), P0Y = mul_rn(a0.pY, sp);
+  T PmO = P0O, PmX = P0X, PmY = P0Y;  // scaled pi' one level down
+  T GO, GX, GY, fz0;
+  T uw_a, uw_b, vw_a, vw_b;  // own-cell faces one level down
+  if (kA == 0) {
+    GO = mul_rn(mul_rn(a1.pO, sp) - P0O, a0.izO);
+    GX = mul_rn(mul_rn(a1.pX, sp) - P0X, a0.izX);
+    GY = mul_rn(mul_rn(a1.pY, sp) - P0Y, a0.izY);
+    fz0 = T(0);
+    uw_a = b0.uO0, uw_b = b0.uO1, vw_a = b0.vO0, vw_b = b0.vO1;
+  } else {
+    const MvA<T> am = lev_a(kA - 1);
+    const MvB<T> bm = lev_b(kA - 1);
+    PmO = mul_rn(am.pO, sp), PmX = mul_rn(am.pX, sp), PmY = mul_rn(am.pY, sp);
+    GO = mul_rn(P0O - PmO, a0.izO);
+    GX = mul_rn(P0X - PmX, a0.izX);
+    GY = mul_rn(P0Y - PmY, a0.izY);
+    fz0 = mul_rn(mul_rn(a0.W, a0.rw), a0.tw);
+    uw_a = bm.uO0, uw_b = bm.uO1, vw_a = bm.vO0, vw_b = bm.vO1;
+  }
+  for (int k = kA; k < kB; ++k) {
+    const MvA<T> a2 = lev_a(min(k + 2, nz));  // prefetch
+    const MvB<T> b1 = lev_b(min(k + 1, nz));
+    // next level's scaled pressures and gradients (the lid gradient repeats
+    // the top pair of mass levels, as the edge padding of gz_mass)
+    const T P1O = mul_rn(a1.pO, sp), P1X = mul_rn(a1.pX, sp), P1Y = mul_rn(a1.pY, sp);
+    const bool top = (k + 1 >= nz);
+    const T G1O = mul_rn(top ? P0O - PmO : P1O - P0O, a1.izO);
+    const T G1X = mul_rn(top ? P0X - PmX : P1X - P0X, a1.izX);
+    const T G1Y = mul_rn(top ? P0Y - PmY : P1Y - P0Y, a1.izY);
+    const T fz1 = top ? T(0) : mul_rn(mul_rn(a1.W, a1.rw), a1.tw);
+    MvIn<T> q;
+    q.PO = P0O;
+    q.PX = P0X;
+    q.PY = P0Y;
+    q.gmO = mul_rn(T(0.5), GO + G1O);
+    q.gmX = mul_rn(T(0.5), GX + G1X);
+    q.gmY = mul_rn(T(0.5), GY + G1Y);
+    q.xu_f = ui ? b0.uO0 : b0.uO1;
+    q.thu = ui ? b0.thu0 : b0.thu1;
+    q.zxu = b0.zxu;
+    q.mu_f = mu_f;
+    q.fu_f = fu_f;
+    q.xv_f = vj ? b0.vO0 : b0.vO1;
+    q.thv = vj ? b0.thv0 : b0.thv1;
+    q.zev = b0.zev;
+    q.mv_f = mv_f;
+    q.fv_f = fv_f;
+    q.vX0 = b0.vX0;
+    q.vX1 = b0.vX1;
+    q.vO0 = b0.vO0;
+    q.vO1 = b0.vO1;
+    q.uY0 = b0.uY0;
+    q.uY1 = b0.uY1;
+    q.uO0 = b0.uO0;
+    q.uO1 = b0.uO1;
+    q.xw_k = b0.xw;
+    q.xW_k = a0.W;
+    q.idzw_k = a0.izO;
+    q.damp = b0.damp;
+    q.thw = a0.tw;
+    q.zxw = b0.zxw;
+    q.zew = b0.zew;
+    q.gzw = GO;
+    q.uwa = uw_a;
+    q.uwb = uw_b;
+    q.uwc = b0.uO0;
+    q.uwd = b0.uO1;
+    q.vwa = vw_a;
+    q.vwb = vw_b;
+    q.vwc = b0.vO0;
+    q.vwd = b0.vO1;
+    q.mw = mw;
+    q.rdu0 = b0.rdu0;
+    q.rdu1 = b0.rdu1;
+    q.thu0 = b0.thu0;
+    q.thu1 = b0.thu1;
+    q.rdv0 = b0.rdv0;
+    q.rdv1 = b0.rdv1;
+    q.thv0 = b0.thv0;
+    q.thv1 = b0.thv1;
+    q.fz0 = fz0;
+    q.fz1 = fz1;
+    q.cpidz = b0.cpidz;
+    q.xp_k = a0.pO;
+    T L[5];
+    mv_rows(d, c, q, xs, u_lock, v_lock, k == 0 || k == nz, L);
+    mv_store(d, b, out, i, j, k, L);
+    // one level up
+    uw_a = b0.uO0, uw_b = b0.uO1, vw_a = b0.vO0, vw_b = b0.vO1;
+    PmO = P0O, PmX = P0X, PmY = P0Y;
+    P0O = P1O, P0X = P1X, P0Y = P1Y;
+    GO = G1O, GX = G1X, GY = G1Y;
+    fz0 = fz1;
+    a0 = a1;
+    a1 = a2;
+    b0 = b1;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -523,6 +795,12 @@ __global__ void __launch_bounds__(PT) precond_tile_batched_kernel(Dims d, Coef<T
 template <typename T>
 void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xscale, CVec5<T> b,
                    Vec5<T> out, const int* active, cudaStream_t st) {
+  if (d.tune_mv >= 6 && d.nz >= 2) {  // column march in 1, 2 or 4 z chunks
+    const dim3 blk(32, 4, 1);
+    dim3 grd((d.nx + 1 + 31) / 32, (d.ny + 1 + 3) / 4, d.tune_mv == 6 ? 1 : (d.tune_mv == 7 ? 2 : 4));
+    matvec_march_kernel<T><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+    return;
+  }
   if (d.tune_mv == 4 || d.tune_mv == 5) {  // two or four levels per thread
     const dim3 blk(32, 8, 1);
     const int lv = d.tune_mv == 4 ? 2 : 4;
@@ -628,6 +906,180 @@ void launch_precond_march(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> o
   precond_march_kernel<T, NT><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, r, out, active);
 }
 
+// ---------------------------------------------------------------------------
+// Pipelined column march: one thread per (i, j) column, NT consecutive
+// columns per block (coalesced rows), the arithmetic of precond_march_kernel
+// term for term (bitwise every other column variant).  Every level's global
+// loads are issued two levels ahead of their use (a three-deep register
+// ring), so a thread keeps about thirty loads in flight while the serial
+// Thomas recurrence runs: with one thread per column the grid holds only
+// nx * ny threads, and that memory-level parallelism per thread is what
+// keeps HBM busy.  d' stays in shared memory (nz * NT values).  HINT = 1
+// marks the values the downward sweep reads again (the eta_dot/alpha - kin
+// term parked in the eta_dot output, the w right-hand side and 1/(1+dt tau))
+// evict-last in L2 and the one-pass streams evict-first, so the re-reads
+// can hit L2 instead of HBM.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ float ld_hint(const float* q, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(q), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_hint(const double* q, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(q), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_hint(float* q, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(q), "f"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_hint(double* q, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(q), "d"(v), "l"(pol) : "memory");
+}
+
+template <typename T, int HINT>
+__device__ __forceinline__ T ldp(const T* __restrict__ q, int i, uint64_t pol) {
+  if (HINT) return ld_hint(q + i, pol);
+  return ld(q, i);
+}
+
+template <typename T>
+struct PcUp {  // inputs of upward step k: faces at mass level k + 1, w level k + 1, mass level k
+  T u0, u1, v0, v1, zx, ze, W, rt, w, id, p, l, lo, inv;
+};
+template <typename T>
+struct PcDown {  // inputs of downward step k: mass level k, w level k + 1
+  T cp, w, id, pb, ep;
+};
+
+template <typename T, int NT, int HINT>
+__global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
+                                                          const int* active) {
+  if (active && *active == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_d = reinterpret_cast<T*>(smem_raw);  // [nz][NT]
+  const int t = threadIdx.x;
+  const int i = blockIdx.x * NT + t, j = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i >= nx) return;
+  const int pm = nx * ny, h = i + nx * j;
+  const int pu = (nx + 1) * ny, pv = nx * (ny + 1);
+  const T inva = T(1) / (T)c.s.alpha, ips = (T)(1.0 / c.s.ps), ps = (T)c.s.ps;
+  const T* __restrict__ ru = r.f[0];
+  const T* __restrict__ rv = r.f[1];
+  const T* __restrict__ rw = r.f[2];
+  const T* __restrict__ rp = r.f[3];
+  const T* __restrict__ rW = r.f[4];
+  T* __restrict__ ow = out.f[2];
+  T* __restrict__ op = out.f[3];
+  T* __restrict__ oW = out.f[4];
+  const uint64_t keep = HINT ? l2_policy_evict_last() : 0, once = HINT ? l2_policy_evict_first() : 0;
+  const T mq = T(0.25) * ld(c.mm, h);
+  const int ub = iu(d, i, j, 0), vb = iv(d, i, j, 0);
+  // loads of upward step k (indices clamped in bounds; values beyond the
+  // column are never used)
+  auto up = [&](int k) {
+    PcUp<T> a;
+    const int kf = min(k + 1, nz - 1), kw = min(k + 1, nz);
+    const int qu = ub + kf * pu, qv = vb + kf * pv, pw = h + kw * pm, p = h + k * pm;
+    a.u0 = ldp<T, HINT>(ru, qu, once);
+    a.u1 = ldp<T, HINT>(ru, qu + 1, once);
+    a.v0 = ldp<T, HINT>(rv, qv, once);
+    a.v1 = ldp<T, HINT>(rv, qv + nx, once);
+    a.zx = ldp<T, HINT>(c.zxw, pw, once);
+    a.ze = ldp<T, HINT>(c.zew, pw, once);
+    a.W = ldp<T, HINT>(rW, pw, once);
+    a.rt = ldp<T, HINT>(c.rtw, pw, once);
+    a.w = ldp<T, HINT>(rw, pw, keep);
+    a.id = ldp<T, HINT>(c.idamp, pw, keep);
+    a.p = ldp<T, HINT>(rp, p, once);
+    a.l = ldp<T, HINT>(c.lpi, p, once);
+    a.lo = ldp<T, HINT>(c.tlo, p, once);
+    a.inv = ldp<T, HINT>(c.tinv, p, once);
+    return a;
+  };
+  T su_lo = ld(ru, ub) + ld(ru, ub + 1), sv_lo = ld(rv, vb) + ld(rv, vb + nx);
+  T wt_lo = T(0), dprev = T(0);
+  PcUp<T> a = up(0), b = up(min(1, nz - 1));
+  for (int k = 0; k < nz; ++k) {
+    const PcUp<T> cnext = up(min(k + 2, nz - 1));
+    T wt_hi = T(0);
+    if (k + 1 < nz) {  // interior w level k + 1 (steppers.py:211-219)
+      const T su_hi = a.u0 + a.u1, sv_hi = a.v0 + a.v1;
+      const T kin = mq * ((su_lo + su_hi) * a.zx + (sv_lo + sv_hi) * a.ze);
+      const T ep = a.W * inva - kin;
+      wt_hi = a.rt * (a.w * a.id + ep);
+      if (HINT) st_hint(oW + h + (k + 1) * pm, ep, keep);
+      else oW[h + (k + 1) * pm] = ep;
+      su_lo = su_hi;
+      sv_lo = sv_hi;
+    }
+    const T rhs = a.p * ips - a.l * (wt_hi - wt_lo);  // steppers.py:223
+    dprev = (rhs - a.lo * dprev) * a.inv;
+    s_d[k * NT + t] = dprev;
+    wt_lo = wt_hi;
+    a = b;
+    b = cnext;
+  }
+  // downward: x(k) = d'(k) - c'(k) x(k+1), then w and eta_dot at w level k+1
+  auto down = [&](int k) {
+    PcDown<T> e;
+    const int p = h + k * pm, pw = p + pm;
+    e.cp = ldp<T, HINT>(c.tcp, p, once);
+    e.w = ldp<T, HINT>(rw, pw, keep);
+    e.id = ldp<T, HINT>(c.idamp, pw, keep);
+    e.pb = ldp<T, HINT>(c.pbw, pw, once);
+    e.ep = oW[pw];
+    return e;
+  };
+  T xh = dprev;
+  op[h + (nz - 1) * pm] = xh * ps;
+  if (nz >= 2) {
+    PcDown<T> e = down(nz - 2), f = down(max(nz - 3, 0));
+    for (int k = nz - 2; k >= 0; --k) {  // steppers.py:227-245
+      const PcDown<T> gnext = down(max(k - 2, 0));
+      const int p = h + k * pm, pw = p + pm;
+      const T x = s_d[k * NT + t] - e.cp * xh;
+      op[p] = x * ps;
+      const T wv = e.w * e.id - e.pb * (xh - x);
+      ow[pw] = wv;
+      oW[pw] = e.ep + wv;
+      xh = x;
+      e = f;
+      f = gnext;
+    }
+  }
+  ow[h] = ld(rw, h);  // ground and lid rows (steppers.py:237-238, 244-245)
+  oW[h] = ld(rW, h) * ld(c.dzw, h);
+  const int ptop = h + nz * pm;
+  ow[ptop] = ld(rw, ptop);
+  oW[ptop] = ld(rW, ptop) * ld(c.dzw, ptop);
+}
+
+template <typename T, int NT, int HINT>
+void launch_precond_pipe(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
+                         cudaStream_t st) {
+  const size_t smem = (size_t)d.nz * NT * sizeof(T);
+  static SmemLimit attr_bytes;  // per instantiation
+  ensure_smem_limit((const void*)precond_pipe_kernel<T, NT, HINT>, attr_bytes, smem);
+  // u and v pass straight through (steppers.py:247-249) unless aliased
+  if (out.f[0] != r.f[0])
+    cudaMemcpyAsync(out.f[0], r.f[0], sizeof(T) * field_size(d, LOC_U), cudaMemcpyDeviceToDevice, st);
+  if (out.f[1] != r.f[1])
+    cudaMemcpyAsync(out.f[1], r.f[1], sizeof(T) * field_size(d, LOC_V), cudaMemcpyDeviceToDevice, st);
+  precond_pipe_kernel<T, NT, HINT><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, r, out, active);
+}
+
 template <typename T, int PT, int PC>
 void launch_precond_tile(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                          cudaStream_t st) {
@@ -658,6 +1110,8 @@ void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, co
     case 2: launch_precond_tile<T, 256, 64>(d, c, r, out, active, st); break;
     case 3: launch_precond_march<T, 128>(d, c, r, out, active, st); break;
     case 4: launch_precond_tile_batched<T, 256, 32, 4>(d, c, r, out, active, st); break;
+    case 5: launch_precond_pipe<T, 64, 0>(d, c, r, out, active, st); break;
+    case 6: launch_precond_pipe<T, 64, 1>(d, c, r, out, active, st); break;
     default: launch_precond_tile<T, 256, 32>(d, c, r, out, active, st); break;
   }
 }
