@@ -221,6 +221,20 @@ int sisl_tricubic(int dtype, const int32_t src_shape[3], const void* field, cons
 int sisl_tricubic_vjp(int dtype, const int32_t src_shape[3], const void* field, const int32_t dst_shape[3],
                       const void* const coords[3], const void* cot, void* grad, int use_limiter, double scale,
                       void* stream);
+/* Deterministic sisl_tricubic_vjp (same arguments and result, operators.py:
+ * 146-209 under jax.vjp): every contribution is summed as a fixed-point
+ * integer (scale 2^e chosen on the device from the largest |scale * cot|
+ * and the densest stencil base, so no sum can overflow), then added to grad
+ * with one rounding per element, so the gradient is the same bits on every
+ * run (float atomics round in arrival order).  ws: 256-byte aligned,
+ * sisl_tricubic_vjp_workspace_bytes(dtype, src_shape) bytes (one 64-bit
+ * word per field element in float32; two in float64, the integer part and
+ * a 32-bit fraction, so double contributions keep their precision). */
+size_t sisl_tricubic_vjp_workspace_bytes(int dtype, const int32_t src_shape[3]);
+int sisl_tricubic_vjp_deterministic(int dtype, const int32_t src_shape[3], const void* field,
+                                    const int32_t dst_shape[3], const void* const coords[3], const void* cot,
+                                    void* grad, int use_limiter, double scale, void* ws, size_t ws_bytes,
+                                    void* stream);
 /* CGridOperator3D.avg / .diff (operators.py:37-132) along one axis of an
  * x-fastest field of shape in_shape: to_face = 1 maps centres to faces
  * (n -> n+1, edge-padded or periodic), 0 faces to centres (n+1 -> n);
@@ -350,8 +364,10 @@ int sisl_split_step(SislCore* core, const SislState* in, const SislState* out, i
  * the history members, where given, are zeroed (no cotangent).  The two
  * transposed solves follow sisl_core_set_adjoint and report in
  * info->solve[0..1].  in_bar must not overlap in, solves or out_bar.
- * ws: sisl_workspace_bytes(core, SISL_WS_STEP_VJP) bytes.  Float32
- * cotangents use atomic adds and are reproducible to rounding. */
+ * ws: sisl_workspace_bytes(core, SISL_WS_STEP_VJP) bytes.  The six
+ * semi-Lagrangian interpolation VJPs sum in fixed point (bitwise
+ * reproducible); the explicit-stencil scatters use float atomic adds and are
+ * reproducible to rounding. */
 int sisl_step_vjp(SislCore* core, const SislState* in, void* const solves[10], const SislRelaxation* relax,
                   const SislState* out_bar, const SislState* in_bar, void* ws, size_t ws_bytes, void* stream,
                   SislStepInfo* info);

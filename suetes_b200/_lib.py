@@ -112,6 +112,10 @@ PROTOTYPES = {
                                      ctypes.c_int, vp]),
     "sisl_tricubic_vjp": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32 * 3, vp, ctypes.c_int32 * 3, vp * 3, vp, vp,
                                          ctypes.c_int, ctypes.c_double, vp]),
+    "sisl_tricubic_vjp_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int32 * 3]),
+    "sisl_tricubic_vjp_deterministic": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32 * 3, vp, ctypes.c_int32 * 3,
+                                                       vp * 3, vp, vp, ctypes.c_int, ctypes.c_double, vp,
+                                                       ctypes.c_size_t, vp]),
     "sisl_stagger": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int32 * 3, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, vp, vp, vp, vp]),
     "sisl_explicit_tendencies": (ctypes.c_int, [vp, vp * 6, vp * 6, vp, vp, ctypes.c_size_t, vp]),

@@ -552,18 +552,99 @@ __device__ __forceinline__ void cr_w(T t, T (&w)[4]) {
 __device__ __forceinline__ void atomic_acc(float* a, float v) { atomicAdd(a, v); }
 __device__ __forceinline__ void atomic_acc(double* a, double v) { atomicAdd(a, v); }
 
+// Scatter targets of the tricubic VJP.  AtomicAcc adds into the gradient
+// with float atomics (the sum's rounding depends on the order the atomics
+// land).  FixedAcc adds each contribution as a fixed-point integer v * 2^e:
+// integer addition is associative, so the sum -- and the gradient formed
+// from it -- is the same bits on every run.  float: one 64-bit word per
+// element.  double: two words, the integer part of v * 2^e and its fraction
+// in 2^fb units, summed separately (the fraction sums carry into the result
+// when it is formed), so double contributions keep their precision.
+template <typename T>
+struct AtomicAcc {
+  T* g;
+  __device__ __forceinline__ void add(int i, T v) const { atomic_acc(g + i, v); }
+};
+template <typename T>
+struct FixedAcc;
+template <>
+struct FixedAcc<float> {
+  unsigned long long* acc;
+  size_t n;
+  double s;  // 2^e (v * s is exact in double)
+  __device__ __forceinline__ void add(int i, float v) const {
+    atomicAdd(acc + i, (unsigned long long)__double2ll_rn((double)v * s));
+  }
+};
+template <>
+struct FixedAcc<double> {
+  unsigned long long* acc;  // [0, n): integer parts, [n, 2n): fractions
+  size_t n;
+  double s;   // 2^e
+  double fs;  // 2^fb
+  __device__ __forceinline__ void add(int i, double v) const {
+    const double y = v * s;
+    double h = floor(y);
+    double r = rint((y - h) * fs);  // y - h is exact; r in [0, 2^fb]
+    if (r == fs) { h += 1.0; r = 0.0; }
+    atomicAdd(acc + i, (unsigned long long)(long long)h);
+    atomicAdd(acc + n + i, (unsigned long long)r);
+  }
+};
+
+// Header of the fixed-point scratch: the largest |scale * cot| (as the bits
+// of a float rounded up, which order like the values) and the largest
+// number of destination points whose stencil base is one source cell.
+struct DetHdr {
+  unsigned int gmax_bits;
+  int max_count;
+};
+
+// The fixed-point exponent.  A target sums contributions of points whose
+// stencil base lies in a 4x4x4 box of cells (64 cells of at most max_count
+// points each), a point giving one target at most 27 weights (clamping
+// folds up to three stencil rows per axis) plus 8 limiter corners, each of
+// magnitude <= gmax: below 2^12 * max_count terms, so the integer sums stay
+// below 2^61.
+__device__ __forceinline__ int det_exponent(const DetHdr* h) {
+  const float gmax = __uint_as_float(h->gmax_bits);
+  int eg, ec;
+  frexpf(gmax, &eg);                         // gmax < 2^eg
+  frexpf((float)max(h->max_count, 1), &ec);  // count < 2^ec
+  return 61 - 12 - ec - eg;
+}
+// fraction bits of the double accumulator: sums of 2^12 * count fractions
+// below 2^fb each stay below 2^63
+__device__ __forceinline__ int det_fraction_bits(const DetHdr* h) {
+  int ec;
+  frexpf((float)max(h->max_count, 1), &ec);
+  return min(32, 63 - 12 - ec);
+}
+
+template <typename T>
+__device__ __forceinline__ FixedAcc<T> make_fixed_acc(unsigned long long* acc, size_t n, const DetHdr* h);
+template <>
+__device__ __forceinline__ FixedAcc<float> make_fixed_acc<float>(unsigned long long* acc, size_t n, const DetHdr* h) {
+  return FixedAcc<float>{acc, n, ldexp(1.0, det_exponent(h))};
+}
+template <>
+__device__ __forceinline__ FixedAcc<double> make_fixed_acc<double>(unsigned long long* acc, size_t n,
+                                                                   const DetHdr* h) {
+  return FixedAcc<double>{acc, n, ldexp(1.0, det_exponent(h)), ldexp(1.0, det_fraction_bits(h))};
+}
+
 // share of the cotangent of op(a, b) that goes to a: 1, 0 or 1/2 on a tie
 template <typename T>
 __device__ __forceinline__ T share_min(T a, T b) { return a < b ? T(1) : (a > b ? T(0) : T(0.5)); }
 template <typename T>
 __device__ __forceinline__ T share_max(T a, T b) { return a > b ? T(1) : (a < b ? T(0) : T(0.5)); }
 
-template <typename T>
-__global__ void __launch_bounds__(256) tricubic_vjp_kernel(int sx, int sy, int sz, int dx, int dy, int dz,
-                                                           const T* __restrict__ f, const T* __restrict__ cx,
-                                                           const T* __restrict__ cy, const T* __restrict__ cz,
-                                                           const T* __restrict__ cot, T* grad, int limiter,
-                                                           T scale) {
+template <typename T, typename Acc>
+__device__ __forceinline__ void tricubic_vjp_point(int sx, int sy, int sz, int dx, int dy, int dz,
+                                                   const T* __restrict__ f, const T* __restrict__ cx,
+                                                   const T* __restrict__ cy, const T* __restrict__ cz,
+                                                   const T* __restrict__ cot, const Acc& grad, int limiter,
+                                                   T scale) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -635,7 +716,7 @@ __global__ void __launch_bounds__(256) tricubic_vjp_kernel(int sx, int sy, int s
     gn[0] += glo + ghi;
 #pragma unroll
     for (int s = 0; s < 8; ++s)
-      if (gn[s] != T(0)) atomic_acc(grad + cidx[s], gn[s]);
+      if (gn[s] != T(0)) grad.add(cidx[s], gn[s]);
     if (gf == T(0)) return;
   }
 #pragma unroll
@@ -646,8 +727,78 @@ __global__ void __launch_bounds__(256) tricubic_vjp_kernel(int sx, int sy, int s
       const int row = ix[a] + sx * iy[b];
       const T gb = ga * wy[b];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) atomic_acc(grad + row + plane * iz[q], gb * wz[q]);
+      for (int q = 0; q < 4; ++q) grad.add(row + plane * iz[q], gb * wz[q]);
     }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) tricubic_vjp_kernel(int sx, int sy, int sz, int dx, int dy, int dz,
+                                                           const T* __restrict__ f, const T* __restrict__ cx,
+                                                           const T* __restrict__ cy, const T* __restrict__ cz,
+                                                           const T* __restrict__ cot, T* grad, int limiter,
+                                                           T scale) {
+  tricubic_vjp_point(sx, sy, sz, dx, dy, dz, f, cx, cy, cz, cot, AtomicAcc<T>{grad}, limiter, scale);
+}
+
+// Deterministic VJP, pass 1: per destination point with a cotangent, count
+// it in the source cell of its stencil base (cnt) and keep the running
+// maxima of the counts and of |scale * cot| in the header.
+template <typename T>
+__global__ void __launch_bounds__(256) tricubic_vjp_count_kernel(int sx, int sy, int sz, int dx, int dy, int dz,
+                                                                 const T* __restrict__ cx, const T* __restrict__ cy,
+                                                                 const T* __restrict__ cz, const T* __restrict__ cot,
+                                                                 T scale, int* cnt, DetHdr* hdr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  float amax = 0.f;
+  int cmax = 0;
+  if (i < dx && j < dy && k < dz) {
+    const int p = i + dx * (j + dy * k);
+    const T g = scale * ld(cot, p);
+    if (g != T(0)) {
+      const T x = fmin(fmax(ld(cx, p), T(0)), (T)(sx - 1));
+      const T y = fmin(fmax(ld(cy, p), T(0)), (T)(sy - 1));
+      const T z = fmin(fmax(ld(cz, p), T(0)), (T)(sz - 1));
+      const int b = (int)floor(x) + sx * ((int)floor(y) + sy * (int)floor(z));
+      cmax = atomicAdd(cnt + b, 1) + 1;
+      amax = __double2float_ru(fabs((double)g));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {  // blockDim.x = 32: a warp is one x row
+    amax = fmaxf(amax, __shfl_down_sync(0xffffffffu, amax, o));
+    cmax = max(cmax, __shfl_down_sync(0xffffffffu, cmax, o));
+  }
+  if (threadIdx.x == 0 && cmax > 0) {
+    atomicMax(&hdr->gmax_bits, __float_as_uint(amax));
+    atomicMax(&hdr->max_count, cmax);
+  }
+}
+
+// pass 2: the scatter in fixed point (acc zeroed beforehand)
+template <typename T>
+__global__ void __launch_bounds__(256) tricubic_vjp_fixed_kernel(int sx, int sy, int sz, int dx, int dy, int dz,
+                                                                 const T* __restrict__ f, const T* __restrict__ cx,
+                                                                 const T* __restrict__ cy, const T* __restrict__ cz,
+                                                                 const T* __restrict__ cot, unsigned long long* acc,
+                                                                 const DetHdr* hdr, int limiter, T scale) {
+  if (hdr->max_count == 0) return;  // no cotangent at all
+  const FixedAcc<T> a = make_fixed_acc<T>(acc, (size_t)sx * sy * sz, hdr);
+  tricubic_vjp_point(sx, sy, sz, dx, dy, dz, f, cx, cy, cz, cot, a, limiter, scale);
+}
+
+// pass 3: grad += acc * 2^-e (one rounding per element, in a fixed order)
+template <typename T>
+__global__ void tricubic_vjp_finish_kernel(size_t n, const unsigned long long* __restrict__ acc,
+                                           const DetHdr* hdr, T* __restrict__ grad) {
+  if (hdr->max_count == 0) return;
+  const double inv = ldexp(1.0, -det_exponent(hdr));
+  const double finv = sizeof(T) == 8 ? ldexp(1.0, -det_fraction_bits(hdr)) : 0.0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    double v = (double)(long long)acc[q];
+    if (sizeof(T) == 8) v += (double)acc[n + q] * finv;
+    if (v != 0.0) grad[q] = grad[q] + (T)(v * inv);
   }
 }
 
@@ -662,6 +813,33 @@ void launch_tricubic_vjp(int sx, int sy, int sz, int dx, int dy, int dz, const T
                                                                     coords3[1], coords3[2], cot, grad,
                                                                     use_limiter, scale);
 }
+size_t tricubic_vjp_det_scratch_bytes(int sx, int sy, int sz, int elem_bytes) {
+  return 256 + (elem_bytes == 8 ? 2 : 1) * sizeof(unsigned long long) * (size_t)sx * sy * sz;
+}
+
+// Deterministic grad += scale * (d tricubic / d field)^T cot with the
+// fixed-point scratch of tricubic_vjp_det_scratch_bytes (256-byte aligned).
+template <typename T>
+void launch_tricubic_vjp_det(int sx, int sy, int sz, int dx, int dy, int dz, const T* field,
+                             const T* const* coords3, const T* cot, T* grad, int use_limiter, T scale, void* scratch,
+                             cudaStream_t st) {
+  DetHdr* hdr = (DetHdr*)scratch;
+  unsigned long long* acc = (unsigned long long*)((char*)scratch + 256);
+  const size_t n = (size_t)sx * sy * sz;
+  dim3 blk(32, 4, 2);
+  cudaMemsetAsync(scratch, 0, 256 + sizeof(int) * n, st);  // header and the counts (in acc's memory)
+  tricubic_vjp_count_kernel<T><<<box_grid(dx, dy, dz, blk), blk, 0, st>>>(
+      sx, sy, sz, dx, dy, dz, coords3[0], coords3[1], coords3[2], cot, scale, (int*)acc, hdr);
+  cudaMemsetAsync(acc, 0, (sizeof(T) == 8 ? 2 : 1) * sizeof(unsigned long long) * n, st);
+  tricubic_vjp_fixed_kernel<T><<<box_grid(dx, dy, dz, blk), blk, 0, st>>>(
+      sx, sy, sz, dx, dy, dz, field, coords3[0], coords3[1], coords3[2], cot, acc, hdr, use_limiter, scale);
+  const size_t nb = (n + 255) / 256;
+  tricubic_vjp_finish_kernel<T><<<(unsigned)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, st>>>(n, acc, hdr, grad);
+}
+template void launch_tricubic_vjp_det<float>(int, int, int, int, int, int, const float*, const float* const*,
+                                             const float*, float*, int, float, void*, cudaStream_t);
+template void launch_tricubic_vjp_det<double>(int, int, int, int, int, int, const double*, const double* const*,
+                                              const double*, double*, int, double, void*, cudaStream_t);
 template void launch_tricubic_vjp<float>(int, int, int, int, int, int, const float*, const float* const*,
                                          const float*, float*, int, float, cudaStream_t);
 template void launch_tricubic_vjp<double>(int, int, int, int, int, int, const double*, const double* const*,

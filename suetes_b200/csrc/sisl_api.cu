@@ -843,6 +843,7 @@ struct VWork {
   T *uinb, *vinb, *winb, *pinb, *thinb, *resb;
   T *hypb[4], *gx4[4], *gy4[4], *tmp4[4];
   T* divb;
+  void* det;         // fixed-point scratch of the deterministic tricubic VJPs
   char* zero_begin;  // the cotangent arrays that start at zero: [zero_begin, zero_end)
   char* zero_end;
 };
@@ -860,6 +861,7 @@ VWork<T> carve_vjp(Carver& cv, const Dims& d) {
   for (int q = 0; q < 4; ++q) { v.gx4[q] = F(LOC_U); v.gy4[q] = F(LOC_V); v.tmp4[q] = F(LOC_M); }
   v.divb = F(LOC_M);
   v.th2b = F(LOC_M);
+  v.det = cv.take(tricubic_vjp_det_scratch_bytes(d.nx + 1, d.ny + 1, d.nz + 1, (int)sizeof(T)));
   v.zero_begin = (char*)cv.take(0);
   for (int q = 0; q < 5; ++q) v.x1b[q] = F(L5[q]);
   v.rub = F(LOC_U); v.rvb = F(LOC_V); v.rwb = F(LOC_W); v.rpb = F(LOC_M); v.reb = F(LOC_W);
@@ -1031,19 +1033,22 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
                                   it ? v.x1b[2] : nullptr, st);
   }
   {  // lateral overrides, then the six departure-point interpolations
-    KScope k(c, SISL_K_SL, st, 7);
+    KScope k(c, SISL_K_SL, st, 19);
     launch_fixup_vjp<T>(d, v.rub, v.rvb, ub, vb, v.reb, st);
     const T* cu[3] = {v.coords[3], v.coords[4], v.coords[5]};
     const T* cvv[3] = {v.coords[6], v.coords[7], v.coords[8]};
     const T* cwv[3] = {v.coords[9], v.coords[10], v.coords[11]};
     const T* cm[3] = {v.coords[0], v.coords[1], v.coords[2]};
     const int ux = d.nx + 1, vy = d.ny + 1, wz = d.nz + 1;
-    launch_tricubic_vjp<T>(ux, d.ny, d.nz, ux, d.ny, d.nz, w.u_in, cu, v.rub, v.uinb, lim, T(1), st);
-    launch_tricubic_vjp<T>(d.nx, vy, d.nz, d.nx, vy, d.nz, w.v_in, cvv, v.rvb, v.vinb, lim, T(1), st);
-    launch_tricubic_vjp<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.w_in, cwv, v.rwb, v.winb, lim, T(1), st);
-    launch_tricubic_vjp<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.res, cwv, v.reb, v.resb, lim, (T)(-(1.0 - a)), st);
-    launch_tricubic_vjp<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.pi_in, cm, v.rpb, v.pinb, lim, T(1), st);
-    launch_tricubic_vjp<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.th_in, cm, v.thab, v.thinb, lim, T(1), st);
+    // deterministic scatters (fixed-point sums): the cotangents are the same bits on every run
+    launch_tricubic_vjp_det<T>(ux, d.ny, d.nz, ux, d.ny, d.nz, w.u_in, cu, v.rub, v.uinb, lim, T(1), v.det, st);
+    launch_tricubic_vjp_det<T>(d.nx, vy, d.nz, d.nx, vy, d.nz, w.v_in, cvv, v.rvb, v.vinb, lim, T(1), v.det, st);
+    launch_tricubic_vjp_det<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.w_in, cwv, v.rwb, v.winb, lim, T(1), v.det, st);
+    launch_tricubic_vjp_det<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.res, cwv, v.reb, v.resb, lim, (T)(-(1.0 - a)),
+                               v.det, st);
+    launch_tricubic_vjp_det<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.pi_in, cm, v.rpb, v.pinb, lim, T(1), v.det, st);
+    launch_tricubic_vjp_det<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.th_in, cm, v.thab, v.thinb, lim, T(1), v.det,
+                               st);
   }
   {  // explicit tendencies with hyperdiffusion (euler.py:208-372, diffusion.py:93-173)
     ExplicitBar<T> bi{};
@@ -1582,6 +1587,35 @@ int sisl_tricubic_vjp(int dtype, const int32_t src[3], const void* field, const 
                                (const float*)cot, (float*)grad, use_limiter, (float)scale, st);
   } else {
     return SISL_ERR_ARG;
+  }
+  return check_cuda();
+}
+
+size_t sisl_tricubic_vjp_workspace_bytes(int dtype, const int32_t src[3]) {
+  if (!src || src[0] < 1 || src[1] < 1 || src[2] < 1 || (dtype != SISL_F32 && dtype != SISL_F64)) return 0;
+  return tricubic_vjp_det_scratch_bytes(src[0], src[1], src[2], dtype == SISL_F64 ? 8 : 4);
+}
+
+int sisl_tricubic_vjp_deterministic(int dtype, const int32_t src[3], const void* field, const int32_t dst[3],
+                                    const void* const coords[3], const void* cot, void* grad, int use_limiter,
+                                    double scale, void* ws, size_t ws_bytes, void* stream) {
+  if (!src || !dst || !coords || !cot || !grad || (use_limiter && !field)) return SISL_ERR_ARG;
+  if (dtype != SISL_F32 && dtype != SISL_F64) return SISL_ERR_ARG;
+  for (int q = 0; q < 3; ++q)
+    if (src[q] < 1 || dst[q] < 0) return SISL_ERR_ARG;
+  if ((int64_t)dst[0] * dst[1] * dst[2] == 0) return SISL_OK;
+  if (!ws || ((uintptr_t)ws & 255) || ws_bytes < sisl_tricubic_vjp_workspace_bytes(dtype, src))
+    return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(nullptr, SISL_K_SL, st, 3);
+  if (dtype == SISL_F64) {
+    const double* co[3] = {(const double*)coords[0], (const double*)coords[1], (const double*)coords[2]};
+    launch_tricubic_vjp_det<double>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const double*)field, co,
+                                    (const double*)cot, (double*)grad, use_limiter, scale, ws, st);
+  } else {
+    const float* co[3] = {(const float*)coords[0], (const float*)coords[1], (const float*)coords[2]};
+    launch_tricubic_vjp_det<float>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const float*)field, co,
+                                   (const float*)cot, (float*)grad, use_limiter, (float)scale, ws, st);
   }
   return check_cuda();
 }

@@ -105,6 +105,15 @@ template <typename T>
 void launch_tricubic_vjp(int sx, int sy, int sz, int dx, int dy, int dz, const T* field, const T* const* coords3,
                          const T* cot, T* grad, int use_limiter, T scale, cudaStream_t st);
 
+// the same, deterministic: contributions summed as fixed-point integers in
+// scratch (tricubic_vjp_det_scratch_bytes of the field shape and element
+// size), so the result is bitwise reproducible
+size_t tricubic_vjp_det_scratch_bytes(int sx, int sy, int sz, int elem_bytes);
+template <typename T>
+void launch_tricubic_vjp_det(int sx, int sy, int sz, int dx, int dy, int dz, const T* field,
+                             const T* const* coords3, const T* cot, T* grad, int use_limiter, T scale, void* scratch,
+                             cudaStream_t st);
+
 // staggered average / difference along one axis and its transpose (sisl_stagger.cu)
 template <typename T>
 void launch_stagger(const int in_shape[3], int axis, int to_face, int periodic, int stop_grad, int transpose, T c0,

@@ -115,9 +115,13 @@ class _Tricubic(torch.autograd.Function):
         return (grad, None, None) + (None,) * len(cs)
 
 
-def tricubic_vjp(field, coords, cot, use_limiter=False, scale=1.0, out=None):
+def tricubic_vjp(field, coords, cot, use_limiter=False, scale=1.0, out=None, deterministic=True):
     """Cotangent of ``field`` for ``scale * tensor_product_interp_3d(field,
-    coords)`` given the output cotangent (accumulated into ``out`` when given)."""
+    coords)`` given the output cotangent (accumulated into ``out`` when given).
+
+    ``deterministic`` (default) sums the scattered contributions as
+    fixed-point integers (``sisl_tricubic_vjp_deterministic``): the result is
+    the same bits on every run.  ``False`` scatters with float atomics."""
     f = fortran(field)
     cs = _coords3(coords, f.dtype, f.device)
     g = fortran(cot, dtype=f.dtype)
@@ -126,9 +130,18 @@ def tricubic_vjp(field, coords, cot, use_limiter=False, scale=1.0, out=None):
     src = (ctypes.c_int32 * 3)(*f.shape)
     dst = (ctypes.c_int32 * 3)(*cs[0].shape)
     co = (ctypes.c_void_p * 3)(*[c.data_ptr() for c in cs])
-    check(_lib.load().sisl_tricubic_vjp(DTYPE_CODE[f.dtype], src, f.data_ptr(), dst, co, g.data_ptr(),
-                                        out.data_ptr(), int(bool(use_limiter)), float(scale),
-                                        stream_ptr(f.device)), "sisl_tricubic_vjp")
+    lib = _lib.load()
+    if deterministic:
+        nbytes = int(lib.sisl_tricubic_vjp_workspace_bytes(DTYPE_CODE[f.dtype], src))
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=f.device)
+        check(lib.sisl_tricubic_vjp_deterministic(DTYPE_CODE[f.dtype], src, f.data_ptr(), dst, co, g.data_ptr(),
+                                                  out.data_ptr(), int(bool(use_limiter)), float(scale),
+                                                  ws.data_ptr(), nbytes, stream_ptr(f.device)),
+              "sisl_tricubic_vjp_deterministic")
+    else:
+        check(lib.sisl_tricubic_vjp(DTYPE_CODE[f.dtype], src, f.data_ptr(), dst, co, g.data_ptr(),
+                                    out.data_ptr(), int(bool(use_limiter)), float(scale),
+                                    stream_ptr(f.device)), "sisl_tricubic_vjp")
     return out
 
 
