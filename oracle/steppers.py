@@ -315,6 +315,11 @@ class SISLStepper3D:
         self.use_checkpointing = use_checkpointing
         self.tracer_keys = physics.physics_suite.tracer_keys if physics.physics_suite is not None else []
         self.solve_stats = []
+        # The reference stop-gradients the departure points (steppers.py:764-767);
+        # True differentiates through them instead (a test switch: with it and
+        # CGridOperator3D.use_stop_grad = False the gradient is the exact
+        # derivative of the discrete step)
+        self.departure_gradient = False
 
     def integrate(self, state, t_start, num_steps, forcing, bc_fn):  # steppers.py:692-714
         for n in range(num_steps):
@@ -333,8 +338,8 @@ class SISLStepper3D:
             traj = {"u": ex("u"), "v": ex("v"), "w": ex("w"), "eta_dot": ex("eta_dot")}
         else:
             traj = state
-        with torch.no_grad():
-            tr = {k: traj[k].detach() for k in ("u", "v", "eta_dot")}
+        with torch.set_grad_enabled(self.departure_gradient and torch.is_grad_enabled()):
+            tr = {k: (traj[k] if self.departure_gradient else traj[k].detach()) for k in ("u", "v", "eta_dot")}
             cu = self.advector.compute_departure_indices(tr, loc="u")
             cv = self.advector.compute_departure_indices(tr, loc="v")
             cw = self.advector.compute_departure_indices(tr, loc="w")

@@ -639,7 +639,28 @@ __device__ __forceinline__ T share_min(T a, T b) { return a < b ? T(1) : (a > b 
 template <typename T>
 __device__ __forceinline__ T share_max(T a, T b) { return a > b ? T(1) : (a < b ? T(0) : T(0.5)); }
 
-template <typename T, typename Acc>
+// Stencil bases and fractions of destination point (i, j, k): from the
+// absolute coordinates (clamped, floored) or, REL, from split-form offsets
+// (cubic_base; source and destination shapes equal).
+template <typename T, int REL>
+__device__ __forceinline__ void vjp_base(int i, int j, int k, int p, int sx, int sy, int sz,
+                                         const T* __restrict__ cx, const T* __restrict__ cy,
+                                         const T* __restrict__ cz, int& x0, int& y0, int& z0, T& tx, T& ty,
+                                         T& tz) {
+  if (REL) {
+    cubic_base(i, ld(cx, p), sx, x0, tx);
+    cubic_base(j, ld(cy, p), sy, y0, ty);
+    cubic_base(k, ld(cz, p), sz, z0, tz);
+  } else {
+    const T x = fmin(fmax(ld(cx, p), T(0)), (T)(sx - 1));
+    const T y = fmin(fmax(ld(cy, p), T(0)), (T)(sy - 1));
+    const T z = fmin(fmax(ld(cz, p), T(0)), (T)(sz - 1));
+    x0 = (int)floor(x), y0 = (int)floor(y), z0 = (int)floor(z);
+    tx = x - (T)x0, ty = y - (T)y0, tz = z - (T)z0;
+  }
+}
+
+template <typename T, typename Acc, int REL = 0>
 __device__ __forceinline__ void tricubic_vjp_point(int sx, int sy, int sz, int dx, int dy, int dz,
                                                    const T* __restrict__ f, const T* __restrict__ cx,
                                                    const T* __restrict__ cy, const T* __restrict__ cz,
@@ -652,14 +673,13 @@ __device__ __forceinline__ void tricubic_vjp_point(int sx, int sy, int sz, int d
   const int p = i + dx * (j + dy * k);
   const T g = scale * ld(cot, p);
   if (g == T(0)) return;
-  const T x = fmin(fmax(ld(cx, p), T(0)), (T)(sx - 1));
-  const T y = fmin(fmax(ld(cy, p), T(0)), (T)(sy - 1));
-  const T z = fmin(fmax(ld(cz, p), T(0)), (T)(sz - 1));
-  const int x0 = (int)floor(x), y0 = (int)floor(y), z0 = (int)floor(z);
+  int x0, y0, z0;
+  T tx, ty, tz;
+  vjp_base<T, REL>(i, j, k, p, sx, sy, sz, cx, cy, cz, x0, y0, z0, tx, ty, tz);
   T wx[4], wy[4], wz[4];
-  cr_w(x - (T)x0, wx);
-  cr_w(y - (T)y0, wy);
-  cr_w(z - (T)z0, wz);
+  cr_w(tx, wx);
+  cr_w(ty, wy);
+  cr_w(tz, wz);
   const int ix[4] = {max(x0 - 1, 0), x0, min(x0 + 1, sx - 1), min(x0 + 2, sx - 1)};
   const int iy[4] = {max(y0 - 1, 0), y0, min(y0 + 1, sy - 1), min(y0 + 2, sy - 1)};
   const int iz[4] = {max(z0 - 1, 0), z0, min(z0 + 1, sz - 1), min(z0 + 2, sz - 1)};
@@ -744,7 +764,7 @@ __global__ void __launch_bounds__(256) tricubic_vjp_kernel(int sx, int sy, int s
 // Deterministic VJP, pass 1: per destination point with a cotangent, count
 // it in the source cell of its stencil base (cnt) and keep the running
 // maxima of the counts and of |scale * cot| in the header.
-template <typename T>
+template <typename T, int REL>
 __global__ void __launch_bounds__(256) tricubic_vjp_count_kernel(int sx, int sy, int sz, int dx, int dy, int dz,
                                                                  const T* __restrict__ cx, const T* __restrict__ cy,
                                                                  const T* __restrict__ cz, const T* __restrict__ cot,
@@ -758,10 +778,10 @@ __global__ void __launch_bounds__(256) tricubic_vjp_count_kernel(int sx, int sy,
     const int p = i + dx * (j + dy * k);
     const T g = scale * ld(cot, p);
     if (g != T(0)) {
-      const T x = fmin(fmax(ld(cx, p), T(0)), (T)(sx - 1));
-      const T y = fmin(fmax(ld(cy, p), T(0)), (T)(sy - 1));
-      const T z = fmin(fmax(ld(cz, p), T(0)), (T)(sz - 1));
-      const int b = (int)floor(x) + sx * ((int)floor(y) + sy * (int)floor(z));
+      int x0, y0, z0;
+      T tx, ty, tz;
+      vjp_base<T, REL>(i, j, k, p, sx, sy, sz, cx, cy, cz, x0, y0, z0, tx, ty, tz);
+      const int b = x0 + sx * (y0 + sy * z0);
       cmax = atomicAdd(cnt + b, 1) + 1;
       amax = __double2float_ru(fabs((double)g));
     }
@@ -777,7 +797,7 @@ __global__ void __launch_bounds__(256) tricubic_vjp_count_kernel(int sx, int sy,
 }
 
 // pass 2: the scatter in fixed point (acc zeroed beforehand)
-template <typename T>
+template <typename T, int REL>
 __global__ void __launch_bounds__(256) tricubic_vjp_fixed_kernel(int sx, int sy, int sz, int dx, int dy, int dz,
                                                                  const T* __restrict__ f, const T* __restrict__ cx,
                                                                  const T* __restrict__ cy, const T* __restrict__ cz,
@@ -785,7 +805,7 @@ __global__ void __launch_bounds__(256) tricubic_vjp_fixed_kernel(int sx, int sy,
                                                                  const DetHdr* hdr, int limiter, T scale) {
   if (hdr->max_count == 0) return;  // no cotangent at all
   const FixedAcc<T> a = make_fixed_acc<T>(acc, (size_t)sx * sy * sz, hdr);
-  tricubic_vjp_point(sx, sy, sz, dx, dy, dz, f, cx, cy, cz, cot, a, limiter, scale);
+  tricubic_vjp_point<T, FixedAcc<T>, REL>(sx, sy, sz, dx, dy, dz, f, cx, cy, cz, cot, a, limiter, scale);
 }
 
 // pass 3: grad += acc * 2^-e (one rounding per element, in a fixed order)
@@ -822,24 +842,33 @@ size_t tricubic_vjp_det_scratch_bytes(int sx, int sy, int sz, int elem_bytes) {
 template <typename T>
 void launch_tricubic_vjp_det(int sx, int sy, int sz, int dx, int dy, int dz, const T* field,
                              const T* const* coords3, const T* cot, T* grad, int use_limiter, T scale, void* scratch,
-                             cudaStream_t st) {
+                             int relative, cudaStream_t st) {
   DetHdr* hdr = (DetHdr*)scratch;
   unsigned long long* acc = (unsigned long long*)((char*)scratch + 256);
   const size_t n = (size_t)sx * sy * sz;
   dim3 blk(32, 4, 2);
   cudaMemsetAsync(scratch, 0, 256 + sizeof(int) * n, st);  // header and the counts (in acc's memory)
-  tricubic_vjp_count_kernel<T><<<box_grid(dx, dy, dz, blk), blk, 0, st>>>(
-      sx, sy, sz, dx, dy, dz, coords3[0], coords3[1], coords3[2], cot, scale, (int*)acc, hdr);
+  const dim3 grd = box_grid(dx, dy, dz, blk);
+  if (relative)
+    tricubic_vjp_count_kernel<T, 1><<<grd, blk, 0, st>>>(sx, sy, sz, dx, dy, dz, coords3[0], coords3[1],
+                                                         coords3[2], cot, scale, (int*)acc, hdr);
+  else
+    tricubic_vjp_count_kernel<T, 0><<<grd, blk, 0, st>>>(sx, sy, sz, dx, dy, dz, coords3[0], coords3[1],
+                                                         coords3[2], cot, scale, (int*)acc, hdr);
   cudaMemsetAsync(acc, 0, (sizeof(T) == 8 ? 2 : 1) * sizeof(unsigned long long) * n, st);
-  tricubic_vjp_fixed_kernel<T><<<box_grid(dx, dy, dz, blk), blk, 0, st>>>(
-      sx, sy, sz, dx, dy, dz, field, coords3[0], coords3[1], coords3[2], cot, acc, hdr, use_limiter, scale);
+  if (relative)
+    tricubic_vjp_fixed_kernel<T, 1><<<grd, blk, 0, st>>>(sx, sy, sz, dx, dy, dz, field, coords3[0], coords3[1],
+                                                         coords3[2], cot, acc, hdr, use_limiter, scale);
+  else
+    tricubic_vjp_fixed_kernel<T, 0><<<grd, blk, 0, st>>>(sx, sy, sz, dx, dy, dz, field, coords3[0], coords3[1],
+                                                         coords3[2], cot, acc, hdr, use_limiter, scale);
   const size_t nb = (n + 255) / 256;
   tricubic_vjp_finish_kernel<T><<<(unsigned)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, st>>>(n, acc, hdr, grad);
 }
 template void launch_tricubic_vjp_det<float>(int, int, int, int, int, int, const float*, const float* const*,
-                                             const float*, float*, int, float, void*, cudaStream_t);
+                                             const float*, float*, int, float, void*, int, cudaStream_t);
 template void launch_tricubic_vjp_det<double>(int, int, int, int, int, int, const double*, const double* const*,
-                                              const double*, double*, int, double, void*, cudaStream_t);
+                                              const double*, double*, int, double, void*, int, cudaStream_t);
 template void launch_tricubic_vjp<float>(int, int, int, int, int, int, const float*, const float* const*,
                                          const float*, float*, int, float, cudaStream_t);
 template void launch_tricubic_vjp<double>(int, int, int, int, int, int, const double*, const double* const*,

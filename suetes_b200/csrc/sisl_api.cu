@@ -933,7 +933,8 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
   const int lim = c->prm.use_limiter;
   {
     KScope k(c, SISL_K_SL, st, 4);
-    for (int l = 0; l < 4; ++l) launch_departure<T>(d, l, dt, w.vel + 3 * l, iters, v.coords + 3 * l, st);
+    // split-form offsets, as the forward's fused semi-Lagrangian kernels form them
+    for (int l = 0; l < 4; ++l) launch_departure<T>(d, l, dt, w.vel + 3 * l, iters, v.coords + 3 * l, 1, st);
   }
   ExplicitIn<T> ein{u, vv, wv, eta, pp, th, {nullptr, nullptr, nullptr, nullptr}};
   const bool hyp = c->s.nu_h > 0.0;
@@ -1041,14 +1042,14 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
     const T* cm[3] = {v.coords[0], v.coords[1], v.coords[2]};
     const int ux = d.nx + 1, vy = d.ny + 1, wz = d.nz + 1;
     // deterministic scatters (fixed-point sums): the cotangents are the same bits on every run
-    launch_tricubic_vjp_det<T>(ux, d.ny, d.nz, ux, d.ny, d.nz, w.u_in, cu, v.rub, v.uinb, lim, T(1), v.det, st);
-    launch_tricubic_vjp_det<T>(d.nx, vy, d.nz, d.nx, vy, d.nz, w.v_in, cvv, v.rvb, v.vinb, lim, T(1), v.det, st);
-    launch_tricubic_vjp_det<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.w_in, cwv, v.rwb, v.winb, lim, T(1), v.det, st);
+    launch_tricubic_vjp_det<T>(ux, d.ny, d.nz, ux, d.ny, d.nz, w.u_in, cu, v.rub, v.uinb, lim, T(1), v.det, 1, st);
+    launch_tricubic_vjp_det<T>(d.nx, vy, d.nz, d.nx, vy, d.nz, w.v_in, cvv, v.rvb, v.vinb, lim, T(1), v.det, 1, st);
+    launch_tricubic_vjp_det<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.w_in, cwv, v.rwb, v.winb, lim, T(1), v.det, 1, st);
     launch_tricubic_vjp_det<T>(d.nx, d.ny, wz, d.nx, d.ny, wz, w.res, cwv, v.reb, v.resb, lim, (T)(-(1.0 - a)),
-                               v.det, st);
-    launch_tricubic_vjp_det<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.pi_in, cm, v.rpb, v.pinb, lim, T(1), v.det, st);
+                               v.det, 1, st);
+    launch_tricubic_vjp_det<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.pi_in, cm, v.rpb, v.pinb, lim, T(1), v.det, 1, st);
     launch_tricubic_vjp_det<T>(d.nx, d.ny, d.nz, d.nx, d.ny, d.nz, w.th_in, cm, v.thab, v.thinb, lim, T(1), v.det,
-                               st);
+                               1, st);
   }
   {  // explicit tendencies with hyperdiffusion (euler.py:208-372, diffusion.py:93-173)
     ExplicitBar<T> bi{};
@@ -1539,7 +1540,7 @@ int sisl_departure(SislCore* c, int loc, const void* u, const void* v, const voi
     }
     T* co[3] = {(T*)coords[0], (T*)coords[1], (T*)coords[2]};
     KScope k(c, SISL_K_SL, st);
-    launch_departure<T>(c->d, loc, c->s.dt, (const T* const*)(vt.p + 3 * loc), iterations, co, st);
+    launch_departure<T>(c->d, loc, c->s.dt, (const T* const*)(vt.p + 3 * loc), iterations, co, 0, st);
   };
   if (c->grid.dtype == SISL_F64) run(double{});
   else run(float{});
@@ -1611,11 +1612,11 @@ int sisl_tricubic_vjp_deterministic(int dtype, const int32_t src[3], const void*
   if (dtype == SISL_F64) {
     const double* co[3] = {(const double*)coords[0], (const double*)coords[1], (const double*)coords[2]};
     launch_tricubic_vjp_det<double>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const double*)field, co,
-                                    (const double*)cot, (double*)grad, use_limiter, scale, ws, st);
+                                    (const double*)cot, (double*)grad, use_limiter, scale, ws, 0, st);
   } else {
     const float* co[3] = {(const float*)coords[0], (const float*)coords[1], (const float*)coords[2]};
     launch_tricubic_vjp_det<float>(src[0], src[1], src[2], dst[0], dst[1], dst[2], (const float*)field, co,
-                                   (const float*)cot, (float*)grad, use_limiter, (float)scale, ws, st);
+                                   (const float*)cot, (float*)grad, use_limiter, (float)scale, ws, 0, st);
   }
   return check_cuda();
 }

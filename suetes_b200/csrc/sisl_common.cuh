@@ -117,6 +117,33 @@ __device__ __forceinline__ void level_pair(int k, int nz, int& l, int& r) {
 template <typename T>
 __device__ __forceinline__ T ld(const T* __restrict__ p, int i) { return __ldg(p + i); }
 
+// Split coordinates of a departure point: integer index i plus offset o (the
+// point i + o, with o = -alpha the displacement in index units).  Forming
+// i - alpha in float32 keeps only ~24 - log2(i) bits of alpha's fraction
+// (about 1e-5 cell at i ~ 200, a systematic error that accumulates step
+// after step); the offset keeps all of alpha's bits, and the stencil base
+// and fraction follow from it exactly.
+//
+// Clamped Catmull-Rom stencil base x0 and fraction t of clip(i + o, 0, n - 1)
+// (operators.py:172-179).
+template <typename T>
+__device__ __forceinline__ void cubic_base(int i, T o, int n, int& x0, T& t) {
+  if (o <= (T)(-i)) { x0 = 0; t = T(0); return; }
+  if (o >= (T)(n - 1 - i)) { x0 = n - 1; t = T(0); return; }
+  const T fo = floor(o);
+  x0 = i + (int)fo;
+  t = o - fo;
+}
+// map_coordinates(order=1) base floor(i + o) and weight (no clamp of the
+// coordinate; the caller clamps the two indices).
+template <typename T>
+__device__ __forceinline__ void linear_base(int i, T o, int& l, T& w) {
+  o = fmin(fmax(o, T(-1e8)), T(1e8));  // keeps i + floor(o) an int for any input (indices are clamped after)
+  const T fo = floor(o);
+  l = i + (int)fo;
+  w = o - fo;
+}
+
 // A product rounded on its own (never contracted into an FMA), for values
 // that several code paths share and must round identically.
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }

@@ -109,10 +109,12 @@ void launch_tricubic_vjp(int sx, int sy, int sz, int dx, int dy, int dz, const T
 // scratch (tricubic_vjp_det_scratch_bytes of the field shape and element
 // size), so the result is bitwise reproducible
 size_t tricubic_vjp_det_scratch_bytes(int sx, int sy, int sz, int elem_bytes);
+// relative = 1: coords3 hold split-form offsets of the destination points
+// (source and destination shapes equal)
 template <typename T>
 void launch_tricubic_vjp_det(int sx, int sy, int sz, int dx, int dy, int dz, const T* field,
                              const T* const* coords3, const T* cot, T* grad, int use_limiter, T scale, void* scratch,
-                             cudaStream_t st);
+                             int relative, cudaStream_t st);
 
 // staggered average / difference along one axis and its transpose (sisl_stagger.cu)
 template <typename T>
@@ -124,9 +126,11 @@ void launch_stagger(const int in_shape[3], int axis, int to_face, int periodic, 
 template <typename T>
 void launch_traj_velocity(const Dims& d, const Coef<T>& c, const T* u, const T* v, const T* eta, const T* up,
                           const T* vp, const T* etap, int extrapolate, PtrTable<T> vel, cudaStream_t st);
+// relative = 1: the coordinates are written as split-form offsets -alpha
+// (the point is index + offset), relative = 0 as index - alpha
 template <typename T>
 void launch_departure(const Dims& d, int loc, double dt, const T* const* vel3, int iterations,
-                      T* const* coords3, cudaStream_t st);
+                      T* const* coords3, int relative, cudaStream_t st);
 // tricubic of a (sx, sy, sz) field at the points of a (dx, dy, dz) coordinate array
 template <typename T>
 void launch_tricubic_ext(int sx, int sy, int sz, int dx, int dy, int dz, const T* field, const T* const* coords3,

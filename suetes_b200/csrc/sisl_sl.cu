@@ -108,6 +108,49 @@ __device__ __forceinline__ T trilinear(const T* __restrict__ f, const Ext& e, T 
   return acc;
 }
 
+// the same gather at the split point (i + ox, j + oy, k + oz)
+template <typename T>
+__device__ __forceinline__ T trilinear_rel(const T* __restrict__ f, const Ext& e, int i, int j, int k, T ox, T oy,
+                                           T oz) {
+  int lx, ly, lz;
+  T wx, wy, wz;
+  linear_base(i, ox, lx, wx);
+  linear_base(j, oy, ly, wy);
+  linear_base(k, oz, lz, wz);
+  const int ix[2] = {min(max(lx, 0), e.ex - 1), min(max(lx + 1, 0), e.ex - 1)};
+  const int iy[2] = {min(max(ly, 0), e.ey - 1), min(max(ly + 1, 0), e.ey - 1)};
+  const int iz[2] = {min(max(lz, 0), e.ez - 1), min(max(lz + 1, 0), e.ez - 1)};
+  const T Wx[2] = {T(1) - wx, wx}, Wy[2] = {T(1) - wy, wy}, Wz[2] = {T(1) - wz, wz};
+  T acc = T(0);
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        acc += Wx[a] * Wy[b] * Wz[q] * ld(f, ix[a] + e.ex * (iy[b] + e.ey * iz[q]));
+  return acc;
+}
+
+// Midpoint departure iteration in split form: the offsets (ox, oy, oz) =
+// -alpha of the point (i, j, k) (steppers.py:318-360).
+template <typename T>
+__device__ __forceinline__ void departure_rel(const Ext& e, int i, int j, int k, T dt, const T* __restrict__ vx,
+                                              const T* __restrict__ vy, const T* __restrict__ vz, int iters, T& ox,
+                                              T& oy, T& oz) {
+  const int p = i + e.ex * (j + e.ey * k);
+  T ax = dt * ld(vx, p), ay = dt * ld(vy, p), az = dt * ld(vz, p);
+  for (int it = 0; it < iters; ++it) {
+    const T mx = T(-0.5) * ax, my = T(-0.5) * ay, mz = T(-0.5) * az;
+    ax = dt * trilinear_rel(vx, e, i, j, k, mx, my, mz);
+    ay = dt * trilinear_rel(vy, e, i, j, k, mx, my, mz);
+    az = dt * trilinear_rel(vz, e, i, j, k, mx, my, mz);
+  }
+  ox = -ax;
+  oy = -ay;
+  oz = -az;
+}
+
 template <typename T>
 __device__ __forceinline__ void departure_at(const Ext& e, int i, int j, int k, T dt, const T* __restrict__ vx,
                                              const T* __restrict__ vy, const T* __restrict__ vz, int iters,
@@ -135,16 +178,15 @@ __device__ __forceinline__ void cr_weights(T t, T (&w)[4]) {
   w[3] = t * t * (T(-0.5) + T(0.5) * t);
 }
 
+// the 64-point Catmull-Rom sum (and the limiter) at stencil bases
+// (x0, y0, z0) with fractions (tx, ty, tz)
 template <typename T>
-__device__ __forceinline__ T tricubic_at(const T* __restrict__ f, const Ext& e, T x, T y, T z, int limiter) {
-  x = fmin(fmax(x, T(0)), (T)(e.ex - 1));
-  y = fmin(fmax(y, T(0)), (T)(e.ey - 1));
-  z = fmin(fmax(z, T(0)), (T)(e.ez - 1));
-  const int x0 = (int)floor(x), y0 = (int)floor(y), z0 = (int)floor(z);
+__device__ __forceinline__ T tricubic_core(const T* __restrict__ f, const Ext& e, int x0, int y0, int z0, T tx,
+                                           T ty, T tz, int limiter) {
   T wx[4], wy[4], wz[4];
-  cr_weights(x - (T)x0, wx);
-  cr_weights(y - (T)y0, wy);
-  cr_weights(z - (T)z0, wz);
+  cr_weights(tx, wx);
+  cr_weights(ty, wy);
+  cr_weights(tz, wz);
   const int ix[4] = {max(x0 - 1, 0), x0, min(x0 + 1, e.ex - 1), min(x0 + 2, e.ex - 1)};
   const int iy[4] = {max(y0 - 1, 0), y0, min(y0 + 1, e.ey - 1), min(y0 + 2, e.ey - 1)};
   const int iz[4] = {max(z0 - 1, 0), z0, min(z0 + 1, e.ez - 1), min(z0 + 2, e.ez - 1)};
@@ -183,15 +225,38 @@ __device__ __forceinline__ T tricubic_at(const T* __restrict__ f, const Ext& e, 
 }
 
 template <typename T>
+__device__ __forceinline__ T tricubic_at(const T* __restrict__ f, const Ext& e, T x, T y, T z, int limiter) {
+  x = fmin(fmax(x, T(0)), (T)(e.ex - 1));
+  y = fmin(fmax(y, T(0)), (T)(e.ey - 1));
+  z = fmin(fmax(z, T(0)), (T)(e.ez - 1));
+  const int x0 = (int)floor(x), y0 = (int)floor(y), z0 = (int)floor(z);
+  return tricubic_core(f, e, x0, y0, z0, x - (T)x0, y - (T)y0, z - (T)z0, limiter);
+}
+
+// the same at the split point (i + ox, j + oy, k + oz)
+template <typename T>
+__device__ __forceinline__ T tricubic_rel(const T* __restrict__ f, const Ext& e, int i, int j, int k, T ox, T oy,
+                                          T oz, int limiter) {
+  int x0, y0, z0;
+  T tx, ty, tz;
+  cubic_base(i, ox, e.ex, x0, tx);
+  cubic_base(j, oy, e.ey, y0, ty);
+  cubic_base(k, oz, e.ez, z0, tz);
+  return tricubic_core(f, e, x0, y0, z0, tx, ty, tz, limiter);
+}
+
+// relative = 1 writes the split-form offsets -alpha instead of the points
+template <typename T>
 __global__ void departure_kernel(Dims d, int loc, T dt, const T* __restrict__ vx, const T* __restrict__ vy,
-                                 const T* __restrict__ vz, int iters, T* cx, T* cy, T* cz) {
+                                 const T* __restrict__ vz, int iters, T* cx, T* cy, T* cz, int relative) {
   const Ext e = loc_ext(d, loc);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i >= e.ex || j >= e.ey || k >= e.ez) return;
   T x, y, z;
-  departure_at(e, i, j, k, dt, vx, vy, vz, iters, x, y, z);
+  if (relative) departure_rel(e, i, j, k, dt, vx, vy, vz, iters, x, y, z);
+  else departure_at(e, i, j, k, dt, vx, vy, vz, iters, x, y, z);
   const int p = i + e.ex * (j + e.ey * k);
   cx[p] = x;
   cy[p] = y;
@@ -221,7 +286,8 @@ __global__ void trilinear_kernel(Ext src, Ext dst, const T* __restrict__ f, cons
   out[p] = trilinear(f, src, ld(cx, p), ld(cy, p), ld(cz, p));
 }
 
-// Departure point + tricubic of up to 2 fields sharing the stagger.
+// Departure point + tricubic of up to 2 fields sharing the stagger, in
+// split coordinates.
 template <typename T>
 __global__ void sl_advect_kernel(Dims d, int loc, T dt, const T* __restrict__ vx, const T* __restrict__ vy,
                                  const T* __restrict__ vz, int iters, int nf, const T* __restrict__ f0,
@@ -231,11 +297,11 @@ __global__ void sl_advect_kernel(Dims d, int loc, T dt, const T* __restrict__ vx
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i >= e.ex || j >= e.ey || k >= e.ez) return;
-  T x, y, z;
-  departure_at(e, i, j, k, dt, vx, vy, vz, iters, x, y, z);
+  T ox, oy, oz;
+  departure_rel(e, i, j, k, dt, vx, vy, vz, iters, ox, oy, oz);
   const int p = i + e.ex * (j + e.ey * k);
-  o0[p] = s0 * tricubic_at(f0, e, x, y, z, limiter);
-  if (nf > 1) o1[p] = s1 * tricubic_at(f1, e, x, y, z, limiter);
+  o0[p] = s0 * tricubic_rel(f0, e, i, j, k, ox, oy, oz, limiter);
+  if (nf > 1) o1[p] = s1 * tricubic_rel(f1, e, i, j, k, ox, oy, oz, limiter);
 }
 
 dim3 box_grid(int ex, int ey, int ez, dim3 blk) {
@@ -254,10 +320,10 @@ void launch_traj_velocity(const Dims& d, const Coef<T>& c, const T* u, const T* 
 
 template <typename T>
 void launch_departure(const Dims& d, int loc, double dt, const T* const* vel3, int iterations, T* const* coords3,
-                      cudaStream_t st) {
+                      int relative, cudaStream_t st) {
   dim3 blk(32, 4, 2);
   departure_kernel<T><<<box_grid(ext_x(d, loc), ext_y(d, loc), ext_z(d, loc), blk), blk, 0, st>>>(
-      d, loc, (T)dt, vel3[0], vel3[1], vel3[2], iterations, coords3[0], coords3[1], coords3[2]);
+      d, loc, (T)dt, vel3[0], vel3[1], vel3[2], iterations, coords3[0], coords3[1], coords3[2], relative);
 }
 
 template <typename T>
@@ -289,7 +355,8 @@ void launch_sl_advect(const Dims& d, int loc, double dt, const T* const* vel3, i
 #define SISL_INST_SL(T)                                                                                     \
   template void launch_traj_velocity<T>(const Dims&, const Coef<T>&, const T*, const T*, const T*, const T*, \
                                         const T*, const T*, int, PtrTable<T>, cudaStream_t);                 \
-  template void launch_departure<T>(const Dims&, int, double, const T* const*, int, T* const*, cudaStream_t); \
+  template void launch_departure<T>(const Dims&, int, double, const T* const*, int, T* const*, int,          \
+                                    cudaStream_t);                                                           \
   template void launch_tricubic_ext<T>(int, int, int, int, int, int, const T*, const T* const*, T*, int, T,  \
                                        cudaStream_t);                                                        \
   template void launch_trilinear_ext<T>(int, int, int, int, int, int, const T*, const T* const*, T*,         \
