@@ -373,6 +373,55 @@ def step_vjp(stepper, state, recorded, cotangents, relax=None):
     return out
 
 
+def generic_bc_map(stepper, bc_fn, pre, forcing=None):
+    """A user ``bc_fn`` applied to a step's output as the reference applies
+    it (steppers.py:1036-1058): the reference state (full ``pi`` and
+    ``th_v``, float64) goes through ``bc_fn``, then the equation of state
+    re-diagnoses ``rho``.  ``pre``: perturbation-form fields of the step
+    output (``DeviceState.t``); returns the post-``bc_fn`` fields in the same
+    form and precision.  Differentiable with torch autograd (the history
+    fields pass through)."""
+    ph = stepper.physics
+    c = ph.c
+    core_dt = pre["u"].dtype
+    res = {"u": pre["u"], "v": pre["v"], "w": pre["w"], "eta_dot": pre["eta_dot"], "rho": pre["rho"],
+           "pi": pre["pi_p"].double() + ph.pi_bg, "th_v": pre["th_p"].double() + ph.theta_bg}
+    res2 = bc_fn(res, forcing)
+    th, pi = res2["th_v"].double(), res2["pi"].double()
+    post = dict(pre)
+    post.update({"u": res2["u"].to(core_dt), "v": res2["v"].to(core_dt), "w": res2["w"].to(core_dt),
+                 "eta_dot": res2["eta_dot"].to(core_dt), "pi_p": (pi - ph.pi_bg).to(core_dt),
+                 "th_p": (th - ph.theta_bg).to(core_dt),
+                 "rho": (c["p0"] / (c["Rd"] * th) * pi ** (c["cvd"] / c["Rd"])).to(core_dt)})
+    return post
+
+
+def _generic_forward(stepper, bc_fn, pre_ds):
+    """The post-``bc_fn`` DeviceState of a fused step's output."""
+    from .steppers import DeviceState
+    core = pre_ds.core
+    locs = dict(DeviceState.FIELDS)
+    post = generic_bc_map(stepper, bc_fn, pre_ds.t)
+    out = DeviceState(core, {k: core.field(v, locs[k]) for k, v in post.items()}, pre_ds.is_first_step)
+    return out
+
+
+def _generic_cotangents(stepper, bc_fn, pre_ds, g_post):
+    """Cotangents of the pre-``bc_fn`` step output from those of the
+    post-``bc_fn`` state (autograd through ``generic_bc_map``)."""
+    pre = {k: v.detach().requires_grad_(True) for k, v in pre_ds.t.items()}
+    with torch.enable_grad():
+        post = generic_bc_map(stepper, bc_fn, pre)
+        outs, grads = [], []
+        for k, g in g_post.items():
+            if k in post and post[k].requires_grad:
+                outs.append(post[k])
+                grads.append(g)
+        keys = list(pre)
+        gs = torch.autograd.grad(outs, [pre[k] for k in keys], grads, allow_unused=True) if outs else []
+    return {k: g for k, g in zip(keys, gs) if g is not None}
+
+
 def _as_dict(ds):
     d = dict(ds.t)
     d["is_first_step"] = ds.is_first_step
@@ -399,10 +448,14 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
     converge to the same cotangent within the solver tolerance).  With
     ``native`` (and no warm start) each step's reverse sweep is one
     ``sisl_step_vjp`` call; otherwise autograd through
-    ``DifferentiableStep``."""
+    ``DifferentiableStep``.  ``bc_fn``: None, a ``LateralRelaxation`` (fused
+    into the step and its sweep) or any torch callable ``bc_fn(state,
+    forcing)`` such as ``DaviesSponge.blend`` (``generic_bc_map``: applied
+    after the fused step, differentiated with autograd, then the step's
+    native sweep)."""
     relax, generic = stepper._relax_of(bc_fn)
-    if generic is not None:
-        raise NotImplementedError("trajectory_vjp supports LateralRelaxation boundary conditions")
+    if generic is not None and not native:
+        raise NotImplementedError("a user bc_fn is differentiated with the native reverse sweep (native=True)")
     from .steppers import DeviceState
     ds0 = state0 if isinstance(state0, DeviceState) else stepper.to_device_state(state0)
     dstep = DifferentiableStep(stepper, ds0.core.dtype)
@@ -412,9 +465,14 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
     kept_states, kept_recs = [ds0], []
     cur = ds0
     J = torch.zeros((), dtype=F64, device=ds0.core.device)
+    pre_states = {}  # step outputs before a generic bc_fn (kept with every state)
     with torch.no_grad():
         for n in range(num_steps):
             cur, rec = _taped_step(stepper, cur, relax, record=keep_all)
+            if generic is not None:
+                if keep_all:
+                    pre_states[n + 1] = cur
+                cur = _generic_forward(stepper, generic, cur)
             if keep_all:
                 kept_states.append(cur)
                 kept_recs.append(rec)
@@ -435,6 +493,9 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
             with torch.no_grad():
                 for n in range(seg0, seg1):
                     nxt, rec = _taped_step(stepper, states[-1], relax)
+                    if generic is not None:
+                        pre_states[n + 1] = nxt
+                        nxt = _generic_forward(stepper, generic, nxt)
                     states.append(nxt)
                     recs.append(rec)
         for n in range(seg1 - 1, seg0 - 1, -1):
@@ -448,6 +509,8 @@ def trajectory_vjp(stepper, state0, num_steps, objective, bc_fn=None, checkpoint
                         if g is not None:
                             g_after[k] = g_after[k] + g if k in g_after else g
             before_ds = states[n - seg0]
+            if generic is not None and g_after:
+                g_after = _generic_cotangents(stepper, generic, pre_states.pop(n + 1), g_after)
             if native and not warm_start:
                 cot = step_vjp(stepper, before_ds, recs[n - seg0], g_after, relax=relax) if g_after else {}
                 continue

@@ -557,8 +557,6 @@ class SISLStepper3D:
         if self.physics.physics_suite is not None:
             raise NotImplementedError("the differentiable step has no physics-suite cotangents")
         relax, generic = self._relax_of(bc_fn)
-        if generic is not None:
-            raise NotImplementedError("the differentiable step supports LateralRelaxation boundary conditions")
         dtype = _dtype_of({k: state[k] for k in ("u", "v", "w")})
         key = ("_dstep", dtype)
         dstep = self.__dict__.get(key)
@@ -579,6 +577,9 @@ class SISLStepper3D:
             first = 1.0
         ps["is_first_step"] = first
         out = dstep(ps, relax=relax)
+        if generic is not None:  # a user bc_fn, then the equation of state (steppers.py:1036-1058)
+            from .adjoint import generic_bc_map
+            out = generic_bc_map(self, generic, out)
         return {"u": out["u"], "v": out["v"], "w": out["w"], "eta_dot": out["eta_dot"], "rho": out["rho"],
                 "pi": out["pi_p"] + dstep.pi_bg, "th_v": out["th_p"] + dstep.theta_bg,
                 "u_prev": state["u"], "v_prev": state["v"], "w_prev": state["w"],

@@ -223,13 +223,69 @@ def test_tricubic_vjp_matches_oracle(dtype, limiter):
     assert rel_l2(gout, gref) < (1e-13 if dtype == torch.float64 else 2e-6), rel_l2(gout, gref)
 
 
+@pytest.mark.parametrize("autograd_step", [False, True])
+def test_trajectory_vjp_through_davies_sponge_matches_oracle(autograd_step):
+    """A user bc_fn -- the ERA5 runs' DaviesSponge (boundaries.py:185-293)
+    with its directional outflow scaling -- differentiated through the
+    trajectory: the native sweep (trajectory_vjp) and autograd through
+    SISLStepper3D.step against the oracle's autograd with the same sponge."""
+    from oracle.steppers import SISLStepper3D as OSt
+    from suetes_b200 import DaviesSponge, SISLStepper3D as PSt
+    from suetes_b200.adjoint import trajectory_vjp
+    kw = dict(dt=10.0, N_bv=0.01, nu_h_factor=0.05, nu_div_factor=0.1, damp_height=4000.0, max_damp=0.5, lat=45.0)
+    o = build("oracle", 12, 10, 9, 500.0, 500.0, 500.0, h=mountain, **kw)
+    p = build("cuda", 12, 10, 9, 500.0, 500.0, 500.0, h=mountain, device="cuda", **kw)
+    skw = dict(alpha=0.55, solver_tol=1e-12, solver_maxiter=60, solver_restart=30)
+    os_, ps_ = OSt(o[2], 10.0, **skw), PSt(p[2], 10.0, **skw)
+    s0 = _bubble(o[2], o[0])
+    ext = {"u": torch.full_like(s0["u"], 2.0), "v": torch.full_like(s0["v"], -1.0), "th_v": o[2].theta_bg + 0.5,
+           "pi": o[2].pi_bg.clone()}
+    sp_o = DaviesSponge(o[0], o[1], sponge_depth=3, dt=10.0, outflow_factor=0.2)
+    sp_p = DaviesSponge(p[0], p[1], sponge_depth=3, dt=10.0, outflow_factor=0.2)
+    ext_p = {k: v.cuda() for k, v in ext.items()}
+    bc_o = lambda s, f: sp_o.blend(s, ext)
+    bc_p = lambda s, f: sp_p.blend(s, ext_p)
+    gen = torch.Generator().manual_seed(9)
+    wts = {k: torch.randn(s0[k].shape, generator=gen, dtype=torch.float64) for k in ("u", "v", "w", "th_v", "rho")}
+    leaves = {k: s0[k].clone().requires_grad_(True) for k in ("u", "v", "w", "eta_dot", "pi", "th_v")}
+    so = dict(s0, **leaves)
+    nsteps = 2
+    for n in range(nsteps):
+        so = os_.step(so, n * 10.0, None, bc_o)
+    J = sum((wts[k] * so[k]).sum() for k in ("u", "v", "w", "rho")) + (wts["th_v"] * (so["th_v"] - o[2].theta_bg)).sum()
+    gref = dict(zip(leaves, torch.autograd.grad(J, list(leaves.values()))))
+    pw = {k: v.cuda() for k, v in wts.items()}
+    pairs = (("u", "u"), ("v", "v"), ("w", "w"), ("eta_dot", "eta_dot"), ("pi", "pi_p"), ("th_v", "th_p"))
+    if autograd_step:
+        sp = {k: (v.cuda().requires_grad_(True) if k in leaves else (v.cuda() if torch.is_tensor(v) else v))
+              for k, v in s0.items()}
+        cur = dict(sp)
+        for n in range(nsteps):
+            cur = ps_.step(cur, n * 10.0, None, bc_p)
+        Jp = sum((pw[k] * cur[k]).sum() for k in ("u", "v", "w", "rho")) + (
+            pw["th_v"] * (cur["th_v"] - p[2].theta_bg)).sum()
+        gp = dict(zip(leaves, torch.autograd.grad(Jp, [sp[k] for k in leaves])))
+        g = {kp: gp[ko] for ko, kp in pairs}
+    else:
+        def objective(n, st):
+            if n != nsteps:
+                return None
+            return sum((pw[k] * st[k]).sum() for k in ("u", "v", "w", "rho")) + (pw["th_v"] * st["th_p"]).sum()
+
+        Jp, g = trajectory_vjp(ps_, to_cuda(s0), nsteps, objective, bc_fn=bc_p, checkpoint_every=1,
+                               wrt=("u", "v", "w", "eta_dot", "pi_p", "th_p"))
+    assert abs(float(Jp) - float(J.detach())) <= 1e-8 * abs(float(J.detach())), (float(Jp), float(J.detach()))
+    for ko, kp in pairs:
+        assert rel_l2(g[kp], gref[ko]) < 1e-7, (kp, rel_l2(g[kp], gref[ko]))
+
+
 @pytest.mark.parametrize("limiter", [False, True])
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 def test_tricubic_vjp_deterministic_is_bitwise_repeatable(dtype, limiter):
     """sisl_tricubic_vjp_deterministic sums in fixed point: three runs on a
     semi-Lagrangian pattern (smooth departure points, Courant numbers up to
     3, several points per source cell) give the same bits, and the result
-    matches the float64 atomic scatter."""
+    matches the float64 atomic scatter of the same inputs."""
     import math
     from suetes_b200.operators import tricubic_vjp
     gen = torch.Generator().manual_seed(5)
@@ -244,7 +300,8 @@ def test_tricubic_vjp_deterministic_is_bitwise_repeatable(dtype, limiter):
     runs = [tricubic_vjp(fd, cd, gd, use_limiter=limiter, scale=0.75) for _ in range(3)]
     for r in runs[1:]:
         assert torch.equal(r, runs[0])
-    ref = tricubic_vjp(f.cuda(), coords.cuda(), cot.cuda(), use_limiter=limiter, scale=0.75, deterministic=False)
+    # the float64 atomic scatter of the same (rounded) inputs
+    ref = tricubic_vjp(fd.double(), cd.double(), gd.double(), use_limiter=limiter, scale=0.75, deterministic=False)
     assert rel_l2(runs[0], ref) < (1e-14 if dtype == torch.float64 else 1e-6), rel_l2(runs[0], ref)
 
 
