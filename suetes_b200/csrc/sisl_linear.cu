@@ -264,10 +264,11 @@ struct MvB {  // the rest of level k (faces at mass level min(k, nz-1), w-level 
   T xw, damp, zxw, zew, cpidz;
 };
 
-template <typename T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kernel(Dims d, Coef<T> c, CVec5<T> x,
-                                                                                  const double* xscale, CVec5<T> b,
-                                                                                  Vec5<T> out, const int* active) {
+// DEEP = 1: the rest of a level (MvB) is loaded two levels ahead too (more
+// registers, three blocks per SM)
+template <typename T, int DEEP>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? (DEEP ? 3 : 4) : 2) matvec_march_kernel(
+    Dims d, Coef<T> c, CVec5<T> x, const double* xscale, CVec5<T> b, Vec5<T> out, const int* active) {
   if (active && *active == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -342,6 +343,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kern
   // carried state at level kA
   MvA<T> a0 = lev_a(kA), a1 = lev_a(min(kA + 1, nz));
   MvB<T> b0 = lev_b(kA);
+  MvB<T> b1 = lev_b(min(kA + 1, nz));  // used only when DEEP
   T P0O = mul_rn(a0.pO, sp), P0X = mul_rn(a0.pX, sp), P0Y = mul_rn(a0.pY, sp);
   T PmO = P0O, PmX = P0X, PmY = P0Y;  // scaled pi' one level down
   T GO, GX, GY, fz0;
@@ -364,7 +366,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kern
   }
   for (int k = kA; k < kB; ++k) {
     const MvA<T> a2 = lev_a(min(k + 2, nz));  // prefetch
-    const MvB<T> b1 = lev_b(min(k + 1, nz));
+    const MvB<T> bn = lev_b(min(k + (DEEP ? 2 : 1), nz));
     // next level's scaled pressures and gradients (the lid gradient repeats
     // the top pair of mass levels, as the edge padding of gz_mass)
     const T P1O = mul_rn(a1.pO, sp), P1X = mul_rn(a1.pX, sp), P1Y = mul_rn(a1.pY, sp);
@@ -438,7 +440,12 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kern
     fz0 = fz1;
     a0 = a1;
     a1 = a2;
-    b0 = b1;
+    if (DEEP) {
+      b0 = b1;
+      b1 = bn;
+    } else {
+      b0 = bn;
+    }
   }
 }
 
@@ -797,8 +804,9 @@ void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xs
                    Vec5<T> out, const int* active, cudaStream_t st) {
   if (d.tune_mv >= 6 && d.nz >= 2) {  // column march in 1, 2 or 4 z chunks
     const dim3 blk(32, 4, 1);
-    dim3 grd((d.nx + 1 + 31) / 32, (d.ny + 1 + 3) / 4, d.tune_mv == 6 ? 1 : (d.tune_mv == 7 ? 2 : 4));
-    matvec_march_kernel<T><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+    dim3 grd((d.nx + 1 + 31) / 32, (d.ny + 1 + 3) / 4, d.tune_mv == 7 ? 2 : (d.tune_mv == 8 ? 4 : 1));
+    if (d.tune_mv == 9) matvec_march_kernel<T, 1><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+    else matvec_march_kernel<T, 0><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
     return;
   }
   if (d.tune_mv == 4 || d.tune_mv == 5) {  // two or four levels per thread
@@ -962,7 +970,7 @@ struct PcDown {  // inputs of downward step k: mass level k, w level k + 1
   T cp, w, id, pb, ep;
 };
 
-template <typename T, int NT, int HINT>
+template <typename T, int NT, int HINT, int R>
 __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
                                                           const int* active) {
   if (active && *active == 0) return;
@@ -990,6 +998,7 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   // column are never used)
   auto up = [&](int k) {
     PcUp<T> a;
+    k = min(k, nz - 1);
     const int kf = min(k + 1, nz - 1), kw = min(k + 1, nz);
     const int qu = ub + kf * pu, qv = vb + kf * pv, pw = h + kw * pm, p = h + k * pm;
     a.u0 = ldp<T, HINT>(ru, qu, once);
@@ -1010,30 +1019,41 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   };
   T su_lo = ld(ru, ub) + ld(ru, ub + 1), sv_lo = ld(rv, vb) + ld(rv, vb + nx);
   T wt_lo = T(0), dprev = T(0);
-  PcUp<T> a = up(0), b = up(min(1, nz - 1));
-  for (int k = 0; k < nz; ++k) {
-    const PcUp<T> cnext = up(min(k + 2, nz - 1));
-    T wt_hi = T(0);
-    if (k + 1 < nz) {  // interior w level k + 1 (steppers.py:211-219)
-      const T su_hi = a.u0 + a.u1, sv_hi = a.v0 + a.v1;
-      const T kin = mq * ((su_lo + su_hi) * a.zx + (sv_lo + sv_hi) * a.ze);
-      const T ep = a.W * inva - kin;
-      wt_hi = a.rt * (a.w * a.id + ep);
-      if (HINT) st_hint(oW + h + (k + 1) * pm, ep, keep);
-      else oW[h + (k + 1) * pm] = ep;
-      su_lo = su_hi;
-      sv_lo = sv_hi;
+  // a ring of R levels in registers: level k is consumed from slot k % R and
+  // the slot is refilled with level k + R (the loop is unrolled by R so the
+  // slot indices are compile-time)
+  PcUp<T> ring[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) ring[q] = up(q);
+  for (int k0 = 0; k0 < nz; k0 += R) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int k = k0 + q;
+      if (k < nz) {
+        const PcUp<T> a = ring[q];
+        ring[q] = up(k + R);
+        T wt_hi = T(0);
+        if (k + 1 < nz) {  // interior w level k + 1 (steppers.py:211-219)
+          const T su_hi = a.u0 + a.u1, sv_hi = a.v0 + a.v1;
+          const T kin = mq * ((su_lo + su_hi) * a.zx + (sv_lo + sv_hi) * a.ze);
+          const T ep = a.W * inva - kin;
+          wt_hi = a.rt * (a.w * a.id + ep);
+          if (HINT) st_hint(oW + h + (k + 1) * pm, ep, keep);
+          else oW[h + (k + 1) * pm] = ep;
+          su_lo = su_hi;
+          sv_lo = sv_hi;
+        }
+        const T rhs = a.p * ips - a.l * (wt_hi - wt_lo);  // steppers.py:223
+        dprev = (rhs - a.lo * dprev) * a.inv;
+        s_d[k * NT + t] = dprev;
+        wt_lo = wt_hi;
+      }
     }
-    const T rhs = a.p * ips - a.l * (wt_hi - wt_lo);  // steppers.py:223
-    dprev = (rhs - a.lo * dprev) * a.inv;
-    s_d[k * NT + t] = dprev;
-    wt_lo = wt_hi;
-    a = b;
-    b = cnext;
   }
   // downward: x(k) = d'(k) - c'(k) x(k+1), then w and eta_dot at w level k+1
   auto down = [&](int k) {
     PcDown<T> e;
+    k = max(k, 0);
     const int p = h + k * pm, pw = p + pm;
     e.cp = ldp<T, HINT>(c.tcp, p, once);
     e.w = ldp<T, HINT>(rw, pw, keep);
@@ -1045,18 +1065,25 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   T xh = dprev;
   op[h + (nz - 1) * pm] = xh * ps;
   if (nz >= 2) {
-    PcDown<T> e = down(nz - 2), f = down(max(nz - 3, 0));
-    for (int k = nz - 2; k >= 0; --k) {  // steppers.py:227-245
-      const PcDown<T> gnext = down(max(k - 2, 0));
-      const int p = h + k * pm, pw = p + pm;
-      const T x = s_d[k * NT + t] - e.cp * xh;
-      op[p] = x * ps;
-      const T wv = e.w * e.id - e.pb * (xh - x);
-      ow[pw] = wv;
-      oW[pw] = e.ep + wv;
-      xh = x;
-      e = f;
-      f = gnext;
+    PcDown<T> dr[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) dr[q] = down(nz - 2 - q);
+    for (int k0 = nz - 2; k0 >= 0; k0 -= R) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int k = k0 - q;
+        if (k >= 0) {  // steppers.py:227-245
+          const PcDown<T> e = dr[q];
+          dr[q] = down(k - R);
+          const int p = h + k * pm, pw = p + pm;
+          const T x = s_d[k * NT + t] - e.cp * xh;
+          op[p] = x * ps;
+          const T wv = e.w * e.id - e.pb * (xh - x);
+          ow[pw] = wv;
+          oW[pw] = e.ep + wv;
+          xh = x;
+        }
+      }
     }
   }
   ow[h] = ld(rw, h);  // ground and lid rows (steppers.py:237-238, 244-245)
@@ -1066,18 +1093,18 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   oW[ptop] = ld(rW, ptop) * ld(c.dzw, ptop);
 }
 
-template <typename T, int NT, int HINT>
+template <typename T, int NT, int HINT, int R>
 void launch_precond_pipe(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                          cudaStream_t st) {
   const size_t smem = (size_t)d.nz * NT * sizeof(T);
   static SmemLimit attr_bytes;  // per instantiation
-  ensure_smem_limit((const void*)precond_pipe_kernel<T, NT, HINT>, attr_bytes, smem);
+  ensure_smem_limit((const void*)precond_pipe_kernel<T, NT, HINT, R>, attr_bytes, smem);
   // u and v pass straight through (steppers.py:247-249) unless aliased
   if (out.f[0] != r.f[0])
     cudaMemcpyAsync(out.f[0], r.f[0], sizeof(T) * field_size(d, LOC_U), cudaMemcpyDeviceToDevice, st);
   if (out.f[1] != r.f[1])
     cudaMemcpyAsync(out.f[1], r.f[1], sizeof(T) * field_size(d, LOC_V), cudaMemcpyDeviceToDevice, st);
-  precond_pipe_kernel<T, NT, HINT><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, r, out, active);
+  precond_pipe_kernel<T, NT, HINT, R><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, r, out, active);
 }
 
 template <typename T, int PT, int PC>
@@ -1110,8 +1137,11 @@ void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, co
     case 2: launch_precond_tile<T, 256, 64>(d, c, r, out, active, st); break;
     case 3: launch_precond_march<T, 128>(d, c, r, out, active, st); break;
     case 4: launch_precond_tile_batched<T, 256, 32, 4>(d, c, r, out, active, st); break;
-    case 5: launch_precond_pipe<T, 64, 0>(d, c, r, out, active, st); break;
-    case 6: launch_precond_pipe<T, 64, 1>(d, c, r, out, active, st); break;
+    case 5: launch_precond_pipe<T, 64, 0, 3>(d, c, r, out, active, st); break;
+    case 6: launch_precond_pipe<T, 64, 1, 3>(d, c, r, out, active, st); break;
+    case 7: launch_precond_pipe<T, 64, 0, 6>(d, c, r, out, active, st); break;
+    case 8: launch_precond_pipe<T, 64, 1, 6>(d, c, r, out, active, st); break;
+    case 9: launch_precond_pipe<T, 32, 1, 8>(d, c, r, out, active, st); break;
     default: launch_precond_tile<T, 256, 32>(d, c, r, out, active, st); break;
   }
 }
