@@ -386,18 +386,17 @@ int sisl_step_vjp(SislCore* core, const SislState* in, void* const solves[10], c
  * 32x4x2, 32x8x1, 32x2x4, 64x4x1 threads; the matvec also 4 and 5: 32x8
  * columns of two or four levels per thread, 6-8: 32x4 columns marching
  * up the levels of 1, 2 or 4 z chunks with the vertical neighbours carried
- * in registers, 9: that march loading every level two levels ahead) of the
- * matvec and of its transpose, and column
+ * in registers) of the matvec and of its transpose, and column
  * variants (0-2: tiles of 256 threads / 32 columns,
  * 128 / 16, 256 / 64; 3: one thread per column marching up and down the
  * precomputed factorisation, 128 columns per block) of the preconditioner
  * and of its transpose; the preconditioner also 4: the 256 / 32 tile with
  * its loads issued in batches of four items and the face sums of u and v
- * staged in shared memory, 5-9: one thread per column marching with every
- * level's loads issued ahead from a ring of registers (64 columns per block
- * and 3 levels: 5, 6; 6 levels: 7, 8; 32 columns and 8 levels: 9), 6, 8 and
- * 9 with L2 evict-last hints on the values the downward sweep reads again;
- * the
+ * staged in shared memory, 5 and 6: one thread per column (64 columns per
+ * block) marching with every level's loads issued two levels ahead, 6 with
+ * L2 evict-last hints on the values the downward sweep reads again, 7: the
+ * march fed by cp.async copies into a six-level shared-memory ring (32
+ * columns per block); the
  * transpose also 4: the 256 / 32 tile with its loads issued in batches of
  * four items. */
 typedef struct SislTuning {

@@ -68,17 +68,18 @@ __host__ inline dim3 stencil_block(int variant) {
   }
 }
 constexpr int N_STENCIL_BLOCKS = 4;
-// the 4 blocks, 32x8 columns of 2 or 4 levels per thread, the column march
-// (32x4 columns) in 1, 2 or 4 z chunks, and the march loading two levels ahead
-constexpr int N_MATVEC_SHAPES = 10;
+// the 4 blocks, 32x8 columns of 2 or 4 levels per thread, and the column
+// march (32x4 columns) in 1, 2 or 4 z chunks
+constexpr int N_MATVEC_SHAPES = 9;
 // column variants: tiles of (threads, columns) = (256, 32), (128, 16), (256, 64),
 // and the one-thread-per-column march (128 columns per block)
 constexpr int N_COLUMN_TILES = 4;
 // forward preconditioner only: also the (256, 32) tile with
-// batched loads and staged face sums, and the pipelined one-thread-per-column
-// march (64 columns per block, loads 3 or 6 levels ahead, without and with
-// L2 eviction hints; 32 columns, 8 levels ahead, hints)
-constexpr int N_PRECOND_SHAPES = 10;
+// batched loads and staged face sums, the pipelined one-thread-per-column
+// march (64 columns per block, loads two levels ahead, without and with L2
+// eviction hints), and the march fed by cp.async copies into a shared ring
+// (32 columns, 6 levels)
+constexpr int N_PRECOND_SHAPES = 8;
 // its transpose: also the (256, 32) tile with batched loads
 constexpr int N_PRECOND_T_SHAPES = 5;
 

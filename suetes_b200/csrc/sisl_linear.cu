@@ -242,6 +242,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? (LV == 1 ? 6 : 4) : (LV 
     if (k0 + l <= d.nz) matvec_point(d, c, x, xs, b, out, i, j, k0 + l);
 }
 
+// cp.async helpers (global -> shared, asynchronous, per thread)
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_t(T* smem, const T* gmem) {
+  if (sizeof(T) == 4) cp_async4(smem, gmem);
+  else cp_async8(smem, gmem);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // ---------------------------------------------------------------------------
 // Column march: one thread per (i, j) column of the union box marching up
 // the levels of its z chunk (blockIdx.z of gridDim.z chunks).  Vertical
@@ -264,11 +282,10 @@ struct MvB {  // the rest of level k (faces at mass level min(k, nz-1), w-level 
   T xw, damp, zxw, zew, cpidz;
 };
 
-// DEEP = 1: the rest of a level (MvB) is loaded two levels ahead too (more
-// registers, three blocks per SM)
-template <typename T, int DEEP>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? (DEEP ? 3 : 4) : 2) matvec_march_kernel(
-    Dims d, Coef<T> c, CVec5<T> x, const double* xscale, CVec5<T> b, Vec5<T> out, const int* active) {
+template <typename T>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kernel(Dims d, Coef<T> c, CVec5<T> x,
+                                                                                  const double* xscale, CVec5<T> b,
+                                                                                  Vec5<T> out, const int* active) {
   if (active && *active == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -343,7 +360,6 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (DEEP ? 3 : 4) : 2) matv
   // carried state at level kA
   MvA<T> a0 = lev_a(kA), a1 = lev_a(min(kA + 1, nz));
   MvB<T> b0 = lev_b(kA);
-  MvB<T> b1 = lev_b(min(kA + 1, nz));  // used only when DEEP
   T P0O = mul_rn(a0.pO, sp), P0X = mul_rn(a0.pX, sp), P0Y = mul_rn(a0.pY, sp);
   T PmO = P0O, PmX = P0X, PmY = P0Y;  // scaled pi' one level down
   T GO, GX, GY, fz0;
@@ -366,7 +382,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (DEEP ? 3 : 4) : 2) matv
   }
   for (int k = kA; k < kB; ++k) {
     const MvA<T> a2 = lev_a(min(k + 2, nz));  // prefetch
-    const MvB<T> bn = lev_b(min(k + (DEEP ? 2 : 1), nz));
+    const MvB<T> b1 = lev_b(min(k + 1, nz));
     // next level's scaled pressures and gradients (the lid gradient repeats
     // the top pair of mass levels, as the edge padding of gz_mass)
     const T P1O = mul_rn(a1.pO, sp), P1X = mul_rn(a1.pX, sp), P1Y = mul_rn(a1.pY, sp);
@@ -440,12 +456,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (DEEP ? 3 : 4) : 2) matv
     fz0 = fz1;
     a0 = a1;
     a1 = a2;
-    if (DEEP) {
-      b0 = b1;
-      b1 = bn;
-    } else {
-      b0 = bn;
-    }
+    b0 = b1;
   }
 }
 
@@ -805,8 +816,7 @@ void launch_matvec(const Dims& d, const Coef<T>& c, CVec5<T> x, const double* xs
   if (d.tune_mv >= 6 && d.nz >= 2) {  // column march in 1, 2 or 4 z chunks
     const dim3 blk(32, 4, 1);
     dim3 grd((d.nx + 1 + 31) / 32, (d.ny + 1 + 3) / 4, d.tune_mv == 7 ? 2 : (d.tune_mv == 8 ? 4 : 1));
-    if (d.tune_mv == 9) matvec_march_kernel<T, 1><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
-    else matvec_march_kernel<T, 0><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
+    matvec_march_kernel<T><<<grd, blk, 0, st>>>(d, c, x, xscale, b, out, active);
     return;
   }
   if (d.tune_mv == 4 || d.tune_mv == 5) {  // two or four levels per thread
@@ -970,7 +980,7 @@ struct PcDown {  // inputs of downward step k: mass level k, w level k + 1
   T cp, w, id, pb, ep;
 };
 
-template <typename T, int NT, int HINT, int R>
+template <typename T, int NT, int HINT>
 __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
                                                           const int* active) {
   if (active && *active == 0) return;
@@ -998,7 +1008,6 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   // column are never used)
   auto up = [&](int k) {
     PcUp<T> a;
-    k = min(k, nz - 1);
     const int kf = min(k + 1, nz - 1), kw = min(k + 1, nz);
     const int qu = ub + kf * pu, qv = vb + kf * pv, pw = h + kw * pm, p = h + k * pm;
     a.u0 = ldp<T, HINT>(ru, qu, once);
@@ -1019,41 +1028,30 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   };
   T su_lo = ld(ru, ub) + ld(ru, ub + 1), sv_lo = ld(rv, vb) + ld(rv, vb + nx);
   T wt_lo = T(0), dprev = T(0);
-  // a ring of R levels in registers: level k is consumed from slot k % R and
-  // the slot is refilled with level k + R (the loop is unrolled by R so the
-  // slot indices are compile-time)
-  PcUp<T> ring[R];
-#pragma unroll
-  for (int q = 0; q < R; ++q) ring[q] = up(q);
-  for (int k0 = 0; k0 < nz; k0 += R) {
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const int k = k0 + q;
-      if (k < nz) {
-        const PcUp<T> a = ring[q];
-        ring[q] = up(k + R);
-        T wt_hi = T(0);
-        if (k + 1 < nz) {  // interior w level k + 1 (steppers.py:211-219)
-          const T su_hi = a.u0 + a.u1, sv_hi = a.v0 + a.v1;
-          const T kin = mq * ((su_lo + su_hi) * a.zx + (sv_lo + sv_hi) * a.ze);
-          const T ep = a.W * inva - kin;
-          wt_hi = a.rt * (a.w * a.id + ep);
-          if (HINT) st_hint(oW + h + (k + 1) * pm, ep, keep);
-          else oW[h + (k + 1) * pm] = ep;
-          su_lo = su_hi;
-          sv_lo = sv_hi;
-        }
-        const T rhs = a.p * ips - a.l * (wt_hi - wt_lo);  // steppers.py:223
-        dprev = (rhs - a.lo * dprev) * a.inv;
-        s_d[k * NT + t] = dprev;
-        wt_lo = wt_hi;
-      }
+  PcUp<T> a = up(0), b = up(min(1, nz - 1));
+  for (int k = 0; k < nz; ++k) {
+    const PcUp<T> cnext = up(min(k + 2, nz - 1));
+    T wt_hi = T(0);
+    if (k + 1 < nz) {  // interior w level k + 1 (steppers.py:211-219)
+      const T su_hi = a.u0 + a.u1, sv_hi = a.v0 + a.v1;
+      const T kin = mq * ((su_lo + su_hi) * a.zx + (sv_lo + sv_hi) * a.ze);
+      const T ep = a.W * inva - kin;
+      wt_hi = a.rt * (a.w * a.id + ep);
+      if (HINT) st_hint(oW + h + (k + 1) * pm, ep, keep);
+      else oW[h + (k + 1) * pm] = ep;
+      su_lo = su_hi;
+      sv_lo = sv_hi;
     }
+    const T rhs = a.p * ips - a.l * (wt_hi - wt_lo);  // steppers.py:223
+    dprev = (rhs - a.lo * dprev) * a.inv;
+    s_d[k * NT + t] = dprev;
+    wt_lo = wt_hi;
+    a = b;
+    b = cnext;
   }
   // downward: x(k) = d'(k) - c'(k) x(k+1), then w and eta_dot at w level k+1
   auto down = [&](int k) {
     PcDown<T> e;
-    k = max(k, 0);
     const int p = h + k * pm, pw = p + pm;
     e.cp = ldp<T, HINT>(c.tcp, p, once);
     e.w = ldp<T, HINT>(rw, pw, keep);
@@ -1065,25 +1063,18 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   T xh = dprev;
   op[h + (nz - 1) * pm] = xh * ps;
   if (nz >= 2) {
-    PcDown<T> dr[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q) dr[q] = down(nz - 2 - q);
-    for (int k0 = nz - 2; k0 >= 0; k0 -= R) {
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-        const int k = k0 - q;
-        if (k >= 0) {  // steppers.py:227-245
-          const PcDown<T> e = dr[q];
-          dr[q] = down(k - R);
-          const int p = h + k * pm, pw = p + pm;
-          const T x = s_d[k * NT + t] - e.cp * xh;
-          op[p] = x * ps;
-          const T wv = e.w * e.id - e.pb * (xh - x);
-          ow[pw] = wv;
-          oW[pw] = e.ep + wv;
-          xh = x;
-        }
-      }
+    PcDown<T> e = down(nz - 2), f = down(max(nz - 3, 0));
+    for (int k = nz - 2; k >= 0; --k) {  // steppers.py:227-245
+      const PcDown<T> gnext = down(max(k - 2, 0));
+      const int p = h + k * pm, pw = p + pm;
+      const T x = s_d[k * NT + t] - e.cp * xh;
+      op[p] = x * ps;
+      const T wv = e.w * e.id - e.pb * (xh - x);
+      ow[pw] = wv;
+      oW[pw] = e.ep + wv;
+      xh = x;
+      e = f;
+      f = gnext;
     }
   }
   ow[h] = ld(rw, h);  // ground and lid rows (steppers.py:237-238, 244-245)
@@ -1093,18 +1084,154 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   oW[ptop] = ld(rW, ptop) * ld(c.dzw, ptop);
 }
 
-template <typename T, int NT, int HINT, int R>
+// ---------------------------------------------------------------------------
+// Asynchronous-copy column march: the one-thread-per-column arithmetic of
+// precond_pipe_kernel, but every level's inputs are copied global -> shared
+// with cp.async (each thread its own values, S - 1 levels ahead, one copy
+// group per level), so the loads in flight hold no registers and each
+// thread reads back only what it copied itself (no block barrier).
+// Shared memory per block: (nz + 16 S) * NT values of T.
+// ---------------------------------------------------------------------------
+template <typename T, int NT, int S>
+__global__ void __launch_bounds__(NT) precond_async_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
+                                                           const int* active) {
+  if (active && *active == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nz = d.nz;
+  T* s_d = reinterpret_cast<T*>(smem_raw);  // [nz][NT]
+  T* ring = s_d + nz * NT;                   // [S][16][NT]
+  const int t = threadIdx.x;
+  const int i = blockIdx.x * NT + t, j = blockIdx.y;
+  const int nx = d.nx, ny = d.ny;
+  if (i >= nx) return;
+  const int pm = nx * ny, h = i + nx * j;
+  const int pu = (nx + 1) * ny, pv = nx * (ny + 1);
+  const T inva = T(1) / (T)c.s.alpha, ips = (T)(1.0 / c.s.ps), ps = (T)c.s.ps;
+  const T* __restrict__ ru = r.f[0];
+  const T* __restrict__ rv = r.f[1];
+  const T* __restrict__ rw = r.f[2];
+  const T* __restrict__ rp = r.f[3];
+  const T* __restrict__ rW = r.f[4];
+  T* __restrict__ ow = out.f[2];
+  T* __restrict__ op = out.f[3];
+  T* __restrict__ oW = out.f[4];
+  const T mq = T(0.25) * ld(c.mm, h);
+  const int ub = iu(d, i, j, 0), vb = iv(d, i, j, 0);
+  // the 14 inputs of upward step k into ring slot `slot` (clamped in bounds)
+  auto issue_up = [&](int k, int slot) {
+    k = min(k, nz - 1);
+    const int kf = min(k + 1, nz - 1), kw = min(k + 1, nz);
+    const int qu = ub + kf * pu, qv = vb + kf * pv, pw = h + kw * pm, p = h + k * pm;
+    T* q = ring + slot * 16 * NT + t;
+    cp_async_t(q + 0 * NT, ru + qu);
+    cp_async_t(q + 1 * NT, ru + qu + 1);
+    cp_async_t(q + 2 * NT, rv + qv);
+    cp_async_t(q + 3 * NT, rv + qv + nx);
+    cp_async_t(q + 4 * NT, c.zxw + pw);
+    cp_async_t(q + 5 * NT, c.zew + pw);
+    cp_async_t(q + 6 * NT, rW + pw);
+    cp_async_t(q + 7 * NT, c.rtw + pw);
+    cp_async_t(q + 8 * NT, rw + pw);
+    cp_async_t(q + 9 * NT, c.idamp + pw);
+    cp_async_t(q + 10 * NT, rp + p);
+    cp_async_t(q + 11 * NT, c.lpi + p);
+    cp_async_t(q + 12 * NT, c.tlo + p);
+    cp_async_t(q + 13 * NT, c.tinv + p);
+  };
+  T su_lo = ld(ru, ub) + ld(ru, ub + 1), sv_lo = ld(rv, vb) + ld(rv, vb + nx);
+  T wt_lo = T(0), dprev = T(0);
+#pragma unroll
+  for (int q = 0; q < S - 1; ++q) {
+    issue_up(q, q);
+    cp_async_commit();
+  }
+  for (int k = 0; k < nz; ++k) {
+    issue_up(k + S - 1, (k + S - 1) % S);
+    cp_async_commit();
+    cp_async_wait<S - 1>();  // level k's group has landed
+    const T* a = ring + (k % S) * 16 * NT + t;
+    T wt_hi = T(0);
+    if (k + 1 < nz) {  // interior w level k + 1 (steppers.py:211-219)
+      const T su_hi = a[0 * NT] + a[1 * NT], sv_hi = a[2 * NT] + a[3 * NT];
+      const T kin = mq * ((su_lo + su_hi) * a[4 * NT] + (sv_lo + sv_hi) * a[5 * NT]);
+      const T ep = a[6 * NT] * inva - kin;
+      wt_hi = a[7 * NT] * (a[8 * NT] * a[9 * NT] + ep);
+      oW[h + (k + 1) * pm] = ep;
+      su_lo = su_hi;
+      sv_lo = sv_hi;
+    }
+    const T rhs = a[10 * NT] * ips - a[11 * NT] * (wt_hi - wt_lo);  // steppers.py:223
+    dprev = (rhs - a[12 * NT] * dprev) * a[13 * NT];
+    s_d[k * NT + t] = dprev;
+    wt_lo = wt_hi;
+  }
+  cp_async_wait<0>();  // the ring is reused below
+  // downward: x(k) = d'(k) - c'(k) x(k+1), then w and eta_dot at w level k+1
+  auto issue_down = [&](int k, int slot) {
+    k = max(k, 0);
+    const int p = h + k * pm, pw = p + pm;
+    T* q = ring + slot * 16 * NT + t;
+    cp_async_t(q + 0 * NT, c.tcp + p);
+    cp_async_t(q + 1 * NT, rw + pw);
+    cp_async_t(q + 2 * NT, c.idamp + pw);
+    cp_async_t(q + 3 * NT, c.pbw + pw);
+    cp_async_t(q + 4 * NT, oW + pw);  // this thread's own eta_dot/alpha - kin of the upward sweep
+  };
+  T xh = dprev;
+  op[h + (nz - 1) * pm] = xh * ps;
+  if (nz >= 2) {
+#pragma unroll
+    for (int q = 0; q < S - 1; ++q) {
+      issue_down(nz - 2 - q, q);
+      cp_async_commit();
+    }
+    for (int k = nz - 2, n = 0; k >= 0; --k, ++n) {  // steppers.py:227-245
+      issue_down(k - (S - 1), (n + S - 1) % S);
+      cp_async_commit();
+      cp_async_wait<S - 1>();
+      const T* e = ring + (n % S) * 16 * NT + t;
+      const int p = h + k * pm, pw = p + pm;
+      const T x = s_d[k * NT + t] - e[0 * NT] * xh;
+      op[p] = x * ps;
+      const T wv = e[1 * NT] * e[2 * NT] - e[3 * NT] * (xh - x);
+      ow[pw] = wv;
+      oW[pw] = e[4 * NT] + wv;
+      xh = x;
+    }
+    cp_async_wait<0>();
+  }
+  ow[h] = ld(rw, h);  // ground and lid rows (steppers.py:237-238, 244-245)
+  oW[h] = ld(rW, h) * ld(c.dzw, h);
+  const int ptop = h + nz * pm;
+  ow[ptop] = ld(rw, ptop);
+  oW[ptop] = ld(rW, ptop) * ld(c.dzw, ptop);
+}
+
+template <typename T, int NT, int S>
+void launch_precond_async(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
+                          cudaStream_t st) {
+  const size_t smem = (size_t)(d.nz + 16 * S) * NT * sizeof(T);
+  static SmemLimit attr_bytes;  // per instantiation
+  ensure_smem_limit((const void*)precond_async_kernel<T, NT, S>, attr_bytes, smem);
+  if (out.f[0] != r.f[0])
+    cudaMemcpyAsync(out.f[0], r.f[0], sizeof(T) * field_size(d, LOC_U), cudaMemcpyDeviceToDevice, st);
+  if (out.f[1] != r.f[1])
+    cudaMemcpyAsync(out.f[1], r.f[1], sizeof(T) * field_size(d, LOC_V), cudaMemcpyDeviceToDevice, st);
+  precond_async_kernel<T, NT, S><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, r, out, active);
+}
+
+template <typename T, int NT, int HINT>
 void launch_precond_pipe(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, const int* active,
                          cudaStream_t st) {
   const size_t smem = (size_t)d.nz * NT * sizeof(T);
   static SmemLimit attr_bytes;  // per instantiation
-  ensure_smem_limit((const void*)precond_pipe_kernel<T, NT, HINT, R>, attr_bytes, smem);
+  ensure_smem_limit((const void*)precond_pipe_kernel<T, NT, HINT>, attr_bytes, smem);
   // u and v pass straight through (steppers.py:247-249) unless aliased
   if (out.f[0] != r.f[0])
     cudaMemcpyAsync(out.f[0], r.f[0], sizeof(T) * field_size(d, LOC_U), cudaMemcpyDeviceToDevice, st);
   if (out.f[1] != r.f[1])
     cudaMemcpyAsync(out.f[1], r.f[1], sizeof(T) * field_size(d, LOC_V), cudaMemcpyDeviceToDevice, st);
-  precond_pipe_kernel<T, NT, HINT, R><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, r, out, active);
+  precond_pipe_kernel<T, NT, HINT><<<dim3((d.nx + NT - 1) / NT, d.ny), NT, smem, st>>>(d, c, r, out, active);
 }
 
 template <typename T, int PT, int PC>
@@ -1137,11 +1264,9 @@ void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, co
     case 2: launch_precond_tile<T, 256, 64>(d, c, r, out, active, st); break;
     case 3: launch_precond_march<T, 128>(d, c, r, out, active, st); break;
     case 4: launch_precond_tile_batched<T, 256, 32, 4>(d, c, r, out, active, st); break;
-    case 5: launch_precond_pipe<T, 64, 0, 3>(d, c, r, out, active, st); break;
-    case 6: launch_precond_pipe<T, 64, 1, 3>(d, c, r, out, active, st); break;
-    case 7: launch_precond_pipe<T, 64, 0, 6>(d, c, r, out, active, st); break;
-    case 8: launch_precond_pipe<T, 64, 1, 6>(d, c, r, out, active, st); break;
-    case 9: launch_precond_pipe<T, 32, 1, 8>(d, c, r, out, active, st); break;
+    case 5: launch_precond_pipe<T, 64, 0>(d, c, r, out, active, st); break;
+    case 6: launch_precond_pipe<T, 64, 1>(d, c, r, out, active, st); break;
+    case 7: launch_precond_async<T, 32, 6>(d, c, r, out, active, st); break;
     default: launch_precond_tile<T, 256, 32>(d, c, r, out, active, st); break;
   }
 }
