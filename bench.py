@@ -77,6 +77,14 @@ def parse():
     ap.add_argument("--micro-solves", type=int, default=10,
                     help="GMRES solves of the 384x384x96 microbenchmark leg (0 disables the leg)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--profile", default=None, choices=["step192", "tricubic384"],
+                    help="run one small profiling case and exit (for ncu): step192 = one float32 step of the "
+                         "192x192x80 mountain wave with --profile-matvec / --profile-precond launch shapes; "
+                         "tricubic384 = three tricubic interpolations of a 384x384x96 field at smooth departure "
+                         "points (Courant numbers up to 3)")
+    ap.add_argument("--profile-matvec", type=int, default=6, help="matvec launch shape of --profile step192")
+    ap.add_argument("--profile-precond", type=int, default=6,
+                    help="preconditioner launch shape of --profile step192")
     ap.add_argument("--roofline-only", action="store_true",
                     help="run only the roofline leg (batched GMRES, one kernel class timed): the profiling command")
     ap.add_argument("--ens-members", type=int, default=32,
@@ -1059,8 +1067,40 @@ def run_ours(args):
     replicas.finalize(world)
 
 
+def profile_case(args):
+    """Small fixed workloads for ncu captures (a few GB on the device at most)."""
+    if args.profile == "step192":
+        from suetes_b200.steppers import DeviceState
+        from suetes_b200.workloads import mountain_wave
+        st, s0, bc = mountain_wave(192, 192, 80, dtype=torch.float32, solver_tol=1e-7, solve_method="batched")
+        ds = st.to_device_state(s0)
+        t = ds.core.tuning()
+        t["matvec_block"], t["precond_tile"] = args.profile_matvec, args.profile_precond
+        ds.core.set_tuning(**t)
+        st.step_device(ds, DeviceState(ds.core), bc)
+        torch.cuda.synchronize()
+        print("step192 ok", st.last_info["solves"][0]["arnoldi_steps"])
+    else:
+        from suetes_b200 import tensor_product_interp_3d
+        nx, ny, nz = 384, 384, 96
+        g = torch.Generator(device="cuda").manual_seed(1)
+        f = torch.randn(nx, ny, nz, device="cuda", generator=g)
+        i, j, k = torch.meshgrid(*(torch.arange(n, device="cuda", dtype=torch.float32) for n in (nx, ny, nz)),
+                                 indexing="ij")
+        co = torch.stack([i - 1.5 - 1.5 * torch.sin(2 * math.pi * j / ny),
+                          j - 1.5 - 1.5 * torch.cos(2 * math.pi * i / nx),
+                          k - 0.5 - 0.5 * torch.sin(2 * math.pi * (i / nx + k / nz))])
+        for _ in range(3):
+            out = tensor_product_interp_3d(f, co)
+        torch.cuda.synchronize()
+        print("tricubic384 ok", float(out.abs().mean()))
+
+
 def main():
     args = parse()
+    if args.profile:
+        profile_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
