@@ -52,10 +52,11 @@ struct Dims {
   int nx, ny, nz;
   int px, py;          // periodic flags for x and y
   double dx, dy, dz;
-  // launch shapes chosen by the autotuner (sisl_autotune): Helmholtz matvec
-  // (block shape; default 4: two levels per thread) and its transpose,
-  // column preconditioner and its transpose (tile)
-  int tune_mv = 4, tune_pc = 0, tune_mvt = 0, tune_pct = 0;
+  // launch shapes chosen by the autotuner (sisl_autotune): the Helmholtz
+  // matvec (default 6: the column march), its transpose (stencil block), the
+  // column preconditioner (default 6: the pipelined column march) and its
+  // transpose (column tile)
+  int tune_mv = 6, tune_pc = 6, tune_mvt = 0, tune_pct = 0;
 };
 
 // block shapes of the 3-D stencil kernels (256 threads each)
