@@ -861,7 +861,11 @@ VWork<T> carve_vjp(Carver& cv, const Dims& d) {
   for (int q = 0; q < 4; ++q) { v.gx4[q] = F(LOC_U); v.gy4[q] = F(LOC_V); v.tmp4[q] = F(LOC_M); }
   v.divb = F(LOC_M);
   v.th2b = F(LOC_M);
-  v.det = cv.take(tricubic_vjp_det_scratch_bytes(d.nx + 1, d.ny + 1, d.nz + 1, (int)sizeof(T)));
+  {  // shared by the deterministic tricubic and stencil VJPs (they run one after another)
+    const size_t a = tricubic_vjp_det_scratch_bytes(d.nx + 1, d.ny + 1, d.nz + 1, (int)sizeof(T));
+    const size_t b = det_scatter_scratch_bytes(d, (int)sizeof(T));
+    v.det = cv.take(a > b ? a : b);
+  }
   v.zero_begin = (char*)cv.take(0);
   for (int q = 0; q < 5; ++q) v.x1b[q] = F(L5[q]);
   v.rub = F(LOC_U); v.rvb = F(LOC_V); v.rwb = F(LOC_W); v.rpb = F(LOC_M); v.reb = F(LOC_W);
@@ -1027,8 +1031,8 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
     cb.geta = it ? v.x1b[4] : eb;
     cb.ug = it ? v.x1b[0] : v.rub;
     cb.vg = it ? v.x1b[1] : v.rvb;
-    KScope k(c, SISL_K_EXPLICIT, st, 2);
-    launch_corrector_vjp<T>(d, cf, ci, cb, st);
+    KScope k(c, SISL_K_EXPLICIT, st, 4);  // corrector^T (max, fixed-point, finish) + predictor^T
+    launch_corrector_vjp<T>(d, cf, ci, cb, v.det, st);
     // theta' predictor; the first predictor's w terms cancel (w_next = w)
     launch_corrector_theta_vjp<T>(d, cf, it ? v.th2b : v.th1b, v.thab, v.tthb, it ? wb : nullptr,
                                   it ? v.x1b[2] : nullptr, st);
@@ -1058,8 +1062,8 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
     StateBar<T> so{ub, vb, wb, eb, pb, hb, {nullptr, nullptr, nullptr, nullptr}};
     if (hyp)
       for (int q = 0; q < 4; ++q) so.hyper[q] = v.hypb[q];
-    KScope k(c, SISL_K_EXPLICIT, st);
-    launch_explicit_vjp<T>(d, cf, ein, bi, so, 0, st);
+    KScope k(c, SISL_K_EXPLICIT, st, 3);  // max pass, fixed-point pass, finish
+    launch_explicit_vjp<T>(d, cf, ein, bi, so, 0, v.det, st);
   }
   if (hyp) {
     PtrTable<T> h4{}, gx{}, gy{}, t4{};
@@ -1387,6 +1391,7 @@ size_t sisl_workspace_bytes(const SislCore* c, int what) {
       for (int q = 0; q < 8; ++q) cv.take(es * field_size(c->d, LOC_M));
       for (int q = 0; q < 4; ++q) cv.take(es * field_size(c->d, LOC_U));
       for (int q = 0; q < 4; ++q) cv.take(es * field_size(c->d, LOC_V));
+      cv.take(det_scatter_scratch_bytes(c->d, (int)es));
       break;
     default: return 0;
   }
@@ -1834,6 +1839,7 @@ int sisl_explicit_tendencies_vjp(SislCore* c, const void* const sp[6], const voi
     for (int q = 0; q < 4; ++q) t4.p[q] = (T*)cv.take(sizeof(T) * field_size(d, LOC_M));
     for (int q = 0; q < 4; ++q) gx.p[q] = (T*)cv.take(sizeof(T) * field_size(d, LOC_U));
     for (int q = 0; q < 4; ++q) gy.p[q] = (T*)cv.take(sizeof(T) * field_size(d, LOC_V));
+    void* det = cv.take(det_scatter_scratch_bytes(d, (int)sizeof(T)));  // deterministic scatter
     const bool hyp = c->s.nu_h > 0.0;
     if (hyp)
       for (int q = 0; q < 4; ++q)
@@ -1848,8 +1854,8 @@ int sisl_explicit_tendencies_vjp(SislCore* c, const void* const sp[6], const voi
     if (hyp)
       for (int q = 0; q < 4; ++q) so.hyper[q] = h4.p[q];
     {
-      KScope k(c, SISL_K_EXPLICIT, st);
-      launch_explicit_vjp<T>(d, cf, ein, bi, so, 1, st);
+      KScope k(c, SISL_K_EXPLICIT, st, 3);
+      launch_explicit_vjp<T>(d, cf, ein, bi, so, 1, det, st);
     }
     if (hyp) {
       KScope k(c, SISL_K_EXPLICIT, st, 5);

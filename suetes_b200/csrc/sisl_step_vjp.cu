@@ -8,11 +8,12 @@
 // cotangent).
 //
 // Stencils whose transposes fan out to a handful of points (explicit and
-// corrector kernels) scatter with atomic adds, one thread per output point,
-// mirroring the forward kernels' point functions; the two horizontal
-// Laplacians of the hyperdiffusion are transposed in gather form (two
-// passes per Laplacian: face gradients, then mass points).  Float atomics
-// make the float32 cotangents reproducible only to rounding.
+// corrector kernels) scatter, one thread per output point, mirroring the
+// forward kernels' point functions -- with a scratch buffer as fixed-point
+// sums (DetSink: the same bits on every run), without one as float atomic
+// adds; the two horizontal Laplacians of the hyperdiffusion are transposed
+// in gather form (two passes per Laplacian: face gradients, then mass
+// points).
 #include "sisl_explicit_dev.cuh"
 #include "sisl_step_vjp.cuh"
 
@@ -25,9 +26,106 @@ dim3 box_grid(int ex, int ey, int ez, dim3 blk) {
   return dim3((ex + blk.x - 1) / blk.x, (ey + blk.y - 1) / blk.y, (ez + blk.z - 1) / blk.z);
 }
 
+// The block's copy of the launch's DetSink and its per-field state.
+__shared__ __align__(16) unsigned char s_det_raw[sizeof(DetSink<double>)];
+__shared__ unsigned s_det_max[DET_FIELDS];
+__shared__ double s_det_scale[DET_FIELDS], s_det_frac[DET_FIELDS];
+
+template <typename T>
+__device__ __forceinline__ const DetSink<T>& det_sink() {
+  return *reinterpret_cast<const DetSink<T>*>(s_det_raw);
+}
+
+// Fixed-point exponent of a field: a target element gathers fewer than 2^12
+// contributions per launch, each at most gmax < 2^eg, so the integer sums
+// stay below 2^61; the double fraction word carries 32 more bits.
+__device__ __forceinline__ int det_field_exponent(unsigned gmax_bits) {
+  int eg;
+  frexpf(__uint_as_float(gmax_bits), &eg);
+  return 61 - 12 - eg;
+}
+
+template <typename T>
+__device__ __forceinline__ void det_begin(const DetSink<T>& sink) {
+  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nw = (int)(sizeof(DetSink<T>) / sizeof(unsigned));
+  for (int q = t; q < nw; q += blockDim.x * blockDim.y * blockDim.z)
+    reinterpret_cast<unsigned*>(s_det_raw)[q] = reinterpret_cast<const unsigned*>(&sink)[q];
+  if (t < DET_FIELDS) {
+    s_det_max[t] = 0u;
+    if (sink.mode == 2 && t < sink.n) {
+      s_det_scale[t] = ldexp(1.0, det_field_exponent(sink.gmax[t]));
+      s_det_frac[t] = 4294967296.0;
+    }
+  }
+  __syncthreads();
+}
+
+// after the point function: the block's field maxima into the launch's (mode 1)
+template <typename T>
+__device__ __forceinline__ void det_end() {
+  const DetSink<T>& s = det_sink<T>();
+  if (s.mode != 1) return;
+  __syncthreads();
+  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  if (t < s.n && s_det_max[t]) atomicMax(s.gmax + t, s_det_max[t]);
+}
+
+// Accumulate v into field p at element i (p is the base pointer of a field;
+// a pointer the sink does not list falls back to a float atomic add).  Every
+// lane of a warp that reaches one call site passes the same field.
 template <typename T>
 __device__ __forceinline__ void radd(T* p, int i, T v) {
-  atomicAdd(p + i, v);
+  const DetSink<T>& s = det_sink<T>();
+  if (s.mode == 0) {
+    atomicAdd(p + i, v);
+    return;
+  }
+  int f = -1;
+  for (int m = 0; m < s.n; ++m)
+    if (p == s.dst[m]) {
+      f = m;
+      break;
+    }
+  if (f < 0) {
+    atomicAdd(p + i, v);
+    return;
+  }
+  if (s.mode == 1) {  // warp maximum, one shared atomic per warp and call
+    const unsigned bits = __float_as_uint(__double2float_ru(fabs((double)v)));
+    const unsigned mask = __activemask();
+    const unsigned mx = __reduce_max_sync(mask, bits);
+    if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(&s_det_max[f], mx);
+    return;
+  }
+  const double y = (double)v * s_det_scale[f];
+  if (sizeof(T) == 4) {
+    atomicAdd(s.acc[f] + i, (unsigned long long)__double2ll_rn(y));
+  } else {
+    double h = floor(y);
+    double r = rint((y - h) * s_det_frac[f]);  // y - h is exact; r in [0, 2^32]
+    if (r == s_det_frac[f]) { h += 1.0; r = 0.0; }
+    atomicAdd(s.acc[f] + i, (unsigned long long)(long long)h);
+    atomicAdd(s.acc[f] + s.len[f] + i, (unsigned long long)r);
+  }
+}
+
+// field[q] += sum * 2^-e for every registered field (one rounding per element)
+template <typename T>
+__global__ void det_finish_kernel(DetSink<T> s) {
+  for (int f = 0; f < s.n; ++f) {
+    const unsigned gb = s.gmax[f];
+    if (gb == 0u) continue;  // no contribution
+    const double inv = ldexp(1.0, -det_field_exponent(gb));
+    const unsigned long long* a = s.acc[f];
+    T* dst = s.dst[f];
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < s.len[f];
+         q += (size_t)gridDim.x * blockDim.x) {
+      double v = (double)(long long)a[q];
+      if (sizeof(T) == 8) v += (double)a[s.len[f] + q] * (1.0 / 4294967296.0);
+      if (v != 0.0) dst[q] = dst[q] + (T)(v * inv);
+    }
+  }
 }
 
 // padded copies of a centre-to-face stagger (no cotangent)
@@ -203,8 +301,8 @@ __device__ __forceinline__ void divergence_adj(const Dims& d, const Coef<T>& c, 
 // explicit tendencies (explicit_kernel modes 0 and 1)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) explicit_vjp_kernel(Dims d, Coef<T> c, ExplicitIn<T> in, ExplicitBar<T> bi,
-                                                           StateBar<T> bo, int mode) {
+__device__ __forceinline__ void explicit_vjp_point(const Dims& d, const Coef<T>& c, const ExplicitIn<T>& in,
+                                                   const ExplicitBar<T>& bi, const StateBar<T>& bo, int mode) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -355,8 +453,16 @@ __global__ void __launch_bounds__(256) explicit_vjp_kernel(Dims d, Coef<T> c, Ex
 // predictor-corrector right-hand side (corrector_rhs_kernel)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) corrector_vjp_kernel(Dims d, Coef<T> c, CorrectorIn<T> in,
-                                                            CorrectorBar<T> cb) {
+__global__ void __launch_bounds__(256) explicit_vjp_kernel(Dims d, Coef<T> c, ExplicitIn<T> in, ExplicitBar<T> bi,
+                                                           StateBar<T> bo, int mode, DetSink<T> sink) {
+  det_begin(sink);
+  explicit_vjp_point(d, c, in, bi, bo, mode);
+  det_end<T>();
+}
+
+template <typename T>
+__device__ __forceinline__ void corrector_vjp_point(const Dims& d, const Coef<T>& c, const CorrectorIn<T>& in,
+                                                    const CorrectorBar<T>& cb) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -442,6 +548,14 @@ __global__ void __launch_bounds__(256) corrector_vjp_kernel(Dims d, Coef<T> c, C
       divergence_adj<T, true>(d, c, in.gu, in.gv, in.geta, th, i, j, k, adt * b, cb.gu, cb.gv, cb.geta, cb.th);
     }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) corrector_vjp_kernel(Dims d, Coef<T> c, CorrectorIn<T> in,
+                                                            CorrectorBar<T> cb, DetSink<T> sink) {
+  det_begin(sink);
+  corrector_vjp_point(d, c, in, cb);
+  det_end<T>();
 }
 
 // th_next = th_adv + adt (tend_th + (w_m(w_now) - w_m(w_next)) dth_bg/dz)
@@ -712,18 +826,78 @@ __global__ void hyper_src_t_kernel(Dims d, PtrTable<T> s, T* ub, T* vb, T* wb, T
 
 }  // namespace
 
+size_t det_scatter_scratch_bytes(const Dims& d, int elem_bytes) {
+  const size_t n = (size_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+  size_t off = 256;
+  for (int f = 0; f < DET_FIELDS; ++f) off += ((elem_bytes == 8 ? 2 : 1) * sizeof(unsigned long long) * n + 255) & ~(size_t)255;
+  return off;
+}
+
+namespace {
+// The sink of a launch: the distinct non-null destinations with their
+// element counts, accumulators carved from scratch.
+template <typename T>
+DetSink<T> det_make(void* scratch, T* const* dst, const unsigned* len, int n) {
+  DetSink<T> s{};
+  s.mode = 0;
+  if (!scratch) return s;
+  s.gmax = (unsigned*)scratch;
+  char* p = (char*)scratch + 256;
+  for (int q = 0; q < n; ++q) {
+    if (!dst[q]) continue;
+    bool seen = false;
+    for (int m = 0; m < s.n; ++m) seen = seen || s.dst[m] == dst[q];
+    if (seen || s.n == DET_FIELDS) continue;
+    s.dst[s.n] = dst[q];
+    s.len[s.n] = len[q];
+    s.acc[s.n] = (unsigned long long*)p;
+    p += ((sizeof(T) == 8 ? 2 : 1) * sizeof(unsigned long long) * (size_t)len[q] + 255) & ~(size_t)255;
+    s.n++;
+  }
+  return s;
+}
+
+// max pass, zeroed accumulators, fixed-point pass, finish (or one atomic pass)
+template <typename T, typename Launch>
+void det_run(DetSink<T> s, Launch&& launch, cudaStream_t st) {
+  if (s.mode == 0 && !s.gmax) {
+    launch(s);
+    return;
+  }
+  cudaMemsetAsync(s.gmax, 0, sizeof(unsigned) * DET_FIELDS, st);
+  s.mode = 1;
+  launch(s);
+  for (int f = 0; f < s.n; ++f)
+    cudaMemsetAsync(s.acc[f], 0, (sizeof(T) == 8 ? 2 : 1) * sizeof(unsigned long long) * (size_t)s.len[f], st);
+  s.mode = 2;
+  launch(s);
+  det_finish_kernel<T><<<148 * 8, 256, 0, st>>>(s);
+}
+}  // namespace
+
 template <typename T>
 void launch_explicit_vjp(const Dims& d, const Coef<T>& c, const ExplicitIn<T>& in, const ExplicitBar<T>& bi,
-                         const StateBar<T>& bo, int mode, cudaStream_t st) {
+                         const StateBar<T>& bo, int mode, void* det_scratch, cudaStream_t st) {
   dim3 blk(32, 4, 2);
-  explicit_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, in, bi, bo, mode);
+  const unsigned m = (unsigned)field_size(d, LOC_M), w = (unsigned)field_size(d, LOC_W);
+  T* dst[10] = {bo.u, bo.v, bo.w, bo.eta, bo.pi, bo.th, bo.hyper[0], bo.hyper[1], bo.hyper[2], bo.hyper[3]};
+  const unsigned len[10] = {(unsigned)field_size(d, LOC_U), (unsigned)field_size(d, LOC_V), w, w, m, m, m, m, m, m};
+  det_run<T>(det_make<T>(det_scratch, dst, len, 10), [&](const DetSink<T>& s) {
+    explicit_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, in, bi, bo, mode, s);
+  }, st);
 }
 
 template <typename T>
 void launch_corrector_vjp(const Dims& d, const Coef<T>& c, const CorrectorIn<T>& in, const CorrectorBar<T>& cb,
-                          cudaStream_t st) {
+                          void* det_scratch, cudaStream_t st) {
   dim3 blk(32, 4, 2);
-  corrector_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, in, cb);
+  const unsigned m = (unsigned)field_size(d, LOC_M), w = (unsigned)field_size(d, LOC_W);
+  const unsigned fu = (unsigned)field_size(d, LOC_U), fv = (unsigned)field_size(d, LOC_V);
+  T* dst[12] = {cb.rhs_u, cb.rhs_v, cb.rhs_w, cb.rhs_pi, cb.reta, cb.th, cb.pg, cb.gu, cb.gv, cb.geta, cb.ug, cb.vg};
+  const unsigned len[12] = {fu, fv, w, m, w, m, m, fu, fv, w, fu, fv};
+  det_run<T>(det_make<T>(det_scratch, dst, len, 12), [&](const DetSink<T>& s) {
+    corrector_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, in, cb, s);
+  }, st);
 }
 
 template <typename T>
@@ -768,9 +942,9 @@ void launch_hyper_vjp(const Dims& d, const Coef<T>& c, PtrTable<T> hyp_bar, PtrT
 
 #define SISL_INST_VJP(T)                                                                                       \
   template void launch_explicit_vjp<T>(const Dims&, const Coef<T>&, const ExplicitIn<T>&, const ExplicitBar<T>&, \
-                                       const StateBar<T>&, int, cudaStream_t);                                 \
+                                       const StateBar<T>&, int, void*, cudaStream_t);                          \
   template void launch_corrector_vjp<T>(const Dims&, const Coef<T>&, const CorrectorIn<T>&,                    \
-                                        const CorrectorBar<T>&, cudaStream_t);                                 \
+                                        const CorrectorBar<T>&, void*, cudaStream_t);                          \
   template void launch_corrector_theta_vjp<T>(const Dims&, const Coef<T>&, const T*, T*, T*, T*, T*,          \
                                               cudaStream_t);                                                   \
   template void launch_fixup_vjp<T>(const Dims&, T*, T*, T*, T*, T*, cudaStream_t);                            \

@@ -41,12 +41,36 @@ struct FinalizeBar {
   Relax<T> relax;
 };
 
+// Deterministic scatter of the explicit and corrector VJP kernels: the
+// fields a launch accumulates into are registered in a DetSink; a first run
+// of the kernel records each field's largest |contribution| (mode 1), a
+// second adds every contribution as a fixed-point integer (mode 2: one
+// 64-bit word per element in float32, an integer and a 32-bit fraction word
+// in float64), and a finish kernel adds the sums to the fields with one
+// rounding per element.  Integer sums do not depend on the order the
+// atomics land, so the cotangents are the same bits on every run.  Mode 0:
+// plain float atomic adds.
+constexpr int DET_FIELDS = 16;
+template <typename T>
+struct DetSink {
+  int mode, n;
+  T* dst[DET_FIELDS];
+  unsigned len[DET_FIELDS];
+  unsigned long long* acc[DET_FIELDS];
+  unsigned* gmax;  // DET_FIELDS words: float bits of the largest |contribution| per field
+};
+// scratch of a deterministic scatter into up to DET_FIELDS fields of at most
+// (nx+1)(ny+1)(nz+1) elements
+size_t det_scatter_scratch_bytes(const Dims& d, int elem_bytes);
+
+// det_scratch: NULL for float atomics, else det_scatter_scratch_bytes(d, sizeof(T))
+// bytes (256-byte aligned) for the deterministic scatter
 template <typename T>
 void launch_explicit_vjp(const Dims& d, const Coef<T>& c, const ExplicitIn<T>& in, const ExplicitBar<T>& bi,
-                         const StateBar<T>& bo, int mode, cudaStream_t st);
+                         const StateBar<T>& bo, int mode, void* det_scratch, cudaStream_t st);
 template <typename T>
 void launch_corrector_vjp(const Dims& d, const Coef<T>& c, const CorrectorIn<T>& in, const CorrectorBar<T>& cb,
-                          cudaStream_t st);
+                          void* det_scratch, cudaStream_t st);
 template <typename T>
 void launch_corrector_theta_vjp(const Dims& d, const Coef<T>& c, const T* thn_bar, T* tha_bar, T* tth_bar,
                                 T* w_now_bar, T* w_next_bar, cudaStream_t st);
