@@ -631,20 +631,9 @@ def c4_leg(args, local, world):
     return out
 
 
-def ensemble_leg(args, local, world):
-    """The uneven-size bubble ensemble advanced as one CUDA graph per step
-    (members as parallel branches, GMRES loops as device-decided conditional
-    nodes), against the same members stepped one after another eagerly."""
-    from suetes_b200 import PingPong
+def _time_graph_steps(pp, W, K, world):
+    """ms over K graph steps after W warm-up steps (max over ranks), kernel launches."""
     from suetes_b200.core import kernel_launches
-    from suetes_b200.workloads import bubble_ensemble
-    rank = int(os.environ.get("RANK", "0"))
-    ens = bubble_ensemble(args.ens_members, seed=1 + rank, device=f"cuda:{local}", solver_tol=args.tol32,
-                          solve_method=args.method)
-    cells = sum(sp["nx"] * sp["ny"] * sp["nz"] for _, _, _, sp in ens)
-    dss = [(st, st.to_device_state(s0), bc) for st, s0, bc, _ in ens]
-    pp = PingPong(dss, autotune=not args.no_autotune)
-    W, K = 3, args.ens_steps
     for _ in range(W):
         pp.step()
     torch.cuda.synchronize()
@@ -656,10 +645,33 @@ def ensemble_leg(args, local, world):
         pp.step()
     e1.record()
     torch.cuda.synchronize()
-    ms = dist_max(e0.elapsed_time(e1), world)
-    launches = kernel_launches() - l0
-    infos = [pp.info(m) for m in range(len(ens))]
+    return dist_max(e0.elapsed_time(e1), world), kernel_launches() - l0
+
+
+def ensemble_leg(args, local, world):
+    """The uneven-size bubble ensemble advanced one CUDA graph per step: the
+    grouped form (each of the step's two solves one GMRES over all members,
+    every Krylov phase a single launch over a member/block table) against
+    the members as parallel graph branches each with its own solver kernels,
+    and the same members stepped one after another eagerly."""
+    from suetes_b200 import PingPong
+    from suetes_b200.workloads import bubble_ensemble
+    rank = int(os.environ.get("RANK", "0"))
+    ens = bubble_ensemble(args.ens_members, seed=1 + rank, device=f"cuda:{local}", solver_tol=args.tol32,
+                          solve_method=args.method)
+    cells = sum(sp["nx"] * sp["ny"] * sp["nz"] for _, _, _, sp in ens)
+    dss = [(st, st.to_device_state(s0), bc) for st, s0, bc, _ in ens]
+    W, K = 3, args.ens_steps
+    pp = PingPong(dss, autotune=not args.no_autotune)
+    ms_b, launches_b = _time_graph_steps(pp, W, K, world)
+    ppg = PingPong(dss, grouped=True)
+    ms, launches = _time_graph_steps(ppg, W, K, world)
+    # both took the same W + K steps from the same states: the same bits
+    same = all(torch.equal(a.t[k], b.t[k]) for a, b in zip(pp.current(), ppg.current())
+               for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p", "rho"))
+    infos = [ppg.info(m) for m in range(len(ens))]
     conv = sum(1 for i in infos for q in i["solves"] if q["converged"]) / (2 * len(infos))
+    cyc = [q["cycles"] for i in infos for q in i["solves"]]
     # the same members stepped eagerly one after another (host-driven GMRES loops)
     from suetes_b200 import DeviceState
     cur = [a for a in pp.current()]
@@ -667,6 +679,7 @@ def ensemble_leg(args, local, world):
     for (st, _, bc), a, b in zip(dss, cur, nxt):
         st.step_device(a, b, bc)
     torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for (st, _, bc), a, b in zip(dss, cur, nxt):
         st.step_device(a, b, bc)
@@ -675,10 +688,19 @@ def ensemble_leg(args, local, world):
     ms_seq = e0.elapsed_time(e1)
     sizes = sorted({(sp["nx"], sp["ny"], sp["nz"]) for _, _, _, sp in ens})
     vjp = ensemble_vjp(args, world, dss, pp, cells) if args.ens_vjp_steps > 0 else None
+    del ppg
     return {"metric": "SISL cell-steps/s, uneven-size bubble ensemble", "value": world * cells * K / (ms / 1e3),
             "unit": "cell-steps/s", "members": len(ens), "cells_per_step": cells, "steps": K, "warmup": W,
-            "ms_per_step": ms / K, "launch": "one CUDA graph per ensemble step (graph launches timed)",
-            "graph_launches": launches, "converged_frac": conv,
+            "ms_per_step": ms / K,
+            "launch": "one CUDA graph per ensemble step with grouped solves: every Krylov phase of all members "
+                      "one launch over a member/block table, one device-decided WHILE node per solve "
+                      "(graph launches timed)",
+            "graph_launches": launches, "converged_frac": conv, "solve_cycles": {"min": min(cyc), "max": max(cyc)},
+            "branches": {"value": world * cells * K / (ms_b / 1e3), "ms_per_step": ms_b / K,
+                         "launch": "members as parallel graph branches, each with its own solver kernels",
+                         "graph_launches": launches_b},
+            "grouped_equals_branches_bitwise": bool(same),
+            "speedup_vs_branches": ms_b / ms,
             "eager_sequential": {"value": cells / (ms_seq / 1e3), "ms_per_step": ms_seq},
             "speedup_vs_eager_sequential": ms_seq / (ms / K), "distinct_shapes": len(sizes),
             "dtype": "f32", "gmres_tol": args.tol32, "method": args.method,

@@ -364,10 +364,11 @@ int sisl_split_step(SislCore* core, const SislState* in, const SislState* out, i
  * the history members, where given, are zeroed (no cotangent).  The two
  * transposed solves follow sisl_core_set_adjoint and report in
  * info->solve[0..1].  in_bar must not overlap in, solves or out_bar.
- * ws: sisl_workspace_bytes(core, SISL_WS_STEP_VJP) bytes.  The six
- * semi-Lagrangian interpolation VJPs sum in fixed point (bitwise
- * reproducible); the explicit-stencil scatters use float atomic adds and are
- * reproducible to rounding. */
+ * ws: sisl_workspace_bytes(core, SISL_WS_STEP_VJP) bytes.  Every scatter
+ * of the sweep (the six semi-Lagrangian interpolation VJPs and the explicit
+ * and corrector stencil transposes) sums in fixed point and the Laplacian
+ * transposes are gathers, so the cotangents are the same bits on every
+ * run. */
 int sisl_step_vjp(SislCore* core, const SislState* in, void* const solves[10], const SislRelaxation* relax,
                   const SislState* out_bar, const SislState* in_bar, void* ws, size_t ws_bytes, void* stream,
                   SislStepInfo* info);
@@ -421,6 +422,21 @@ int sisl_step_graph_create(int n, SislCore* const* cores, const SislState* ins, 
 int sisl_step_graph_create_taped(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
                                  const SislRelaxation* const* relax, void* const* solves, void* const* ws,
                                  const size_t* ws_bytes, void* stream, SislStepGraph** out);
+/* sisl_step_graph_create_taped with the members' solves grouped (no
+ * reference counterpart; the batched ensemble launch): the explicit,
+ * corrector and finalisation segments of every member stay parallel
+ * branches, but each of the step's two solves runs as ONE restarted GMRES
+ * over all members, every Krylov phase (matvec, preconditioner,
+ * projections, update, small solves) a single launch that walks a
+ * member/block table, and one device-decided WHILE node per solve that
+ * loops while any member continues (convergence per member).  A member's
+ * share of each grouped launch is its own launch's partition, so every
+ * member's step is the same bits as with sisl_step_graph_create.  Members
+ * share the dtype, GMRES restart and method and the refinement switch, and
+ * have nz >= 2 (SISL_ERR_ARG otherwise). */
+int sisl_step_graph_create_grouped(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                                   const SislRelaxation* const* relax, void* const* solves, void* const* ws,
+                                   const size_t* ws_bytes, void* stream, SislStepGraph** out);
 /* The reverse sweep of a step (sisl_step_vjp) of n members as one CUDA graph:
  * member m maps out_bars[m] to in_bars[m] with its input ins[m] and the ten
  * recorded solutions solves[10 m ..]; the transposed GMRES loops are

@@ -153,6 +153,9 @@ PROTOTYPES = {
     "sisl_step_graph_create_taped": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState),
                                                     ctypes.POINTER(SislState), vp, vp, vp, vp, vp,
                                                     ctypes.POINTER(vp)]),
+    "sisl_step_graph_create_grouped": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState),
+                                                      ctypes.POINTER(SislState), vp, vp, vp, vp, vp,
+                                                      ctypes.POINTER(vp)]),
     "sisl_step_vjp_graph_create": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState), vp, vp,
                                                   ctypes.POINTER(SislState), ctypes.POINTER(SislState), vp, vp, vp,
                                                   ctypes.POINTER(vp)]),

@@ -12,7 +12,7 @@
 
 #include "sisl_core.cuh"
 #include "sisl_explicit.cuh"
-#include "sisl_gmres.cuh"
+#include "sisl_group.cuh"
 #include "sisl_split.cuh"
 #include "sisl_step_vjp.cuh"
 
@@ -567,10 +567,10 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
 }
 
 // SemiImplicitSolver3D.solve: scale, GMRES, unscale (steppers.py:401-496).
+// solve_prep stages the scaled right-hand side and initial guess in the
+// GMRES vectors, solve_finish unscales the solution.
 template <typename T>
-int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, const CVec5<T>* x0, Vec5<T> x,
-                   cudaStream_t st, SislSolveInfo* info, GDevInfo* dev_info = nullptr) {
-  const Dims& d = c->d;
+void solve_prep(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, const CVec5<T>* x0, cudaStream_t st) {
   {
     KScope k(c, SISL_K_OTHER, st);
     zero_gaps_kernel<T><<<g.R + 4, 256, 0, st>>>(g.vec, g.npad, g.R + 4, g.off[0], g.off[1], g.off[2], g.off[3],
@@ -580,10 +580,18 @@ int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, co
   scale5<T>(c, cf, rhs, g.view(g.bg()), ps, 0, st);       // rhs_scaled: pi * pi_scale
   if (x0) scale5<T>(c, cf, *x0, g.view(g.xg()), ps, 1, st);  // x0 scaled: pi * ps, eta * dz_w
   else scale5<T>(c, cf, rhs, g.view(g.xg()), ps, 0, st);     // x0 = rhs_scaled
+}
+template <typename T>
+void solve_finish(SislCore* c, const Coef<T>& cf, GWork<T>& g, Vec5<T> x, cudaStream_t st) {
+  scale5<T>(c, cf, g.cview(g.xg()), x, (T)(1.0 / c->s.ps), 2, st);  // pi / ps, eta / dz_w
+}
+template <typename T>
+int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, const CVec5<T>* x0, Vec5<T> x,
+                   cudaStream_t st, SislSolveInfo* info, GDevInfo* dev_info = nullptr) {
+  solve_prep<T>(c, cf, g, rhs, x0, st);
   int rc = gmres_run<T>(c, cf, g, st, info, 0, dev_info);
   if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
-  scale5<T>(c, cf, g.cview(g.xg()), x, (T)(1.0 / c->s.ps), 2, st);  // pi / ps, eta / dz_w
-  (void)d;
+  solve_finish<T>(c, cf, g, x, st);
   return rc;
 }
 
@@ -663,16 +671,49 @@ SWork<T> carve_step(Carver& cv, const Dims& d, int R, bool refine) {
   return w;
 }
 
+// One step's state between its segments.  The step is issued as
+// step_open, step_explicit, then for each of the two solves step_pre_solve,
+// GMRES on the core's solver vectors and step_post_solve, then step_close;
+// the ensemble graph interleaves the members' segments around grouped solves.
 template <typename T>
-int step_impl(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
-              size_t ws_bytes, cudaStream_t st, SislStepInfo* info, void* const* tape = nullptr,
-              GDevInfo* dev_info = nullptr, const void* const* phys = nullptr) {
-  const Dims& d = c->d;
-  const Coef<T> cf = coef_of<T>(c);
+struct StepRun {
+  SislCore* c = nullptr;
+  const SislState* in = nullptr;
+  const SislState* out = nullptr;
+  const SislRelaxation* relax = nullptr;
+  cudaStream_t st = nullptr;
+  SislStepInfo* info = nullptr;
+  void* const* tape = nullptr;
+  const void* const* phys = nullptr;
+  Coef<T> cf{};
+  SWork<T> w{};
+  int64_t l0 = 0;
+  int status = SISL_OK;
+};
+
+template <typename T>
+int step_open(StepRun<T>& r, SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax,
+              void* ws, size_t ws_bytes, cudaStream_t st, SislStepInfo* info, void* const* tape,
+              const void* const* phys) {
+  r.c = c; r.in = in; r.out = out; r.relax = relax; r.st = st; r.info = info; r.tape = tape; r.phys = phys;
+  r.cf = coef_of<T>(c);
   Carver cv{(char*)ws};
-  SWork<T> w = carve_step<T>(cv, d, c->prm.solver_restart, refining<T>(c));
+  r.w = carve_step<T>(cv, c->d, c->prm.solver_restart, refining<T>(c));
   if (cv.off > ws_bytes) return SISL_ERR_WORKSPACE;
-  const int64_t l0 = g_launches.load();
+  r.l0 = g_launches.load();
+  r.status = SISL_OK;
+  return SISL_OK;
+}
+
+// trajectory velocities, explicit tendencies, semi-Lagrangian advection
+template <typename T>
+void step_explicit(StepRun<T>& r) {
+  SislCore* c = r.c;
+  const Dims& d = c->d;
+  const Coef<T>& cf = r.cf;
+  SWork<T>& w = r.w;
+  const SislState* in = r.in;
+  cudaStream_t st = r.st;
   const T* u = (const T*)in->u;
   const T* v = (const T*)in->v;
   const T* wv = (const T*)in->w;
@@ -680,6 +721,7 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
   const T* pp = (const T*)in->pi_p;
   const T* th = (const T*)in->th_p;
   const double a = c->s.alpha, dt = c->s.dt;
+  (void)pp;
   // 1. trajectory index velocities (steppers.py:748-762, 276-316)
   {
     PtrTable<T> vt{};
@@ -690,9 +732,10 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
                             (const T*)in->eta_dot_prev, extrap, vt, st);
   }
   // 2. explicit tendencies with hyperdiffusion (euler.py:208-372)
-  ExplicitIn<T> ein{u, v, wv, eta, pp, th, {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
-  if (phys)
-    for (int q = 0; q < 4; ++q) ein.extra[q] = (const T*)phys[q];
+  ExplicitIn<T> ein{u, v, wv, eta, (const T*)in->pi_p, th, {nullptr, nullptr, nullptr, nullptr},
+                    {nullptr, nullptr, nullptr, nullptr}};
+  if (r.phys)
+    for (int q = 0; q < 4; ++q) ein.extra[q] = (const T*)r.phys[q];
   if (c->s.nu_h > 0.0) {
     PtrTable<T> t4{}, o4{};
     for (int q = 0; q < 4; ++q) { t4.p[q] = w.htmp[q]; o4.p[q] = w.hyp[q]; }
@@ -745,62 +788,103 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
     const int na = (d.nx > d.ny ? d.nx : d.ny) + 1;
     sl_fixup_kernel<T><<<dim3((na + 127) / 128, d.nz), 128, 0, st>>>(d, w.ru, w.rv, u, v, w.reta);
   }
-  // 4. predictor-corrector with two implicit solves (steppers.py:911-998)
-  T* ow = (T*)out->w;
-  T* op = (T*)out->pi_p;
-  T* oe = (T*)out->eta_dot;
-  T* oth = (T*)out->th_p;
-  int status = SISL_OK;
-  for (int it = 0; it < 2; ++it) {
-    const T* w_next = (it == 0) ? wv : ow;
-    {
-      KScope k(c, SISL_K_EXPLICIT, st);
-      launch_corrector_theta<T>(d, cf, w.tha, w.tth, wv, w_next, oth, st);
-    }
-    CorrectorIn<T> ci;
-    ci.rhs_u = w.ru; ci.rhs_v = w.rv; ci.rhs_w = w.rw; ci.rhs_pi = w.rp;
-    ci.th_next = oth;
-    ci.pg = (it == 0) ? pp : op;
-    ci.gu = (it == 0) ? u : w.su;
-    ci.gv = (it == 0) ? v : w.sv;
-    ci.geta = (it == 0) ? eta : oe;
-    ci.ug = (it == 0) ? w.ru : w.su;
-    ci.vg = (it == 0) ? w.rv : w.sv;
-    Vec5<T> rk;
-    rk.f[0] = w.ku; rk.f[1] = w.kv; rk.f[2] = w.kw; rk.f[3] = w.kp; rk.f[4] = w.reta;
-    {
-      KScope k(c, SISL_K_EXPLICIT, st);
-      launch_corrector_rhs<T>(d, cf, ci, rk, st);
-    }
-    CVec5<T> x0;
-    if (it == 0) { x0.f[0] = u; x0.f[1] = v; x0.f[2] = wv; x0.f[3] = pp; x0.f[4] = eta; }
-    else { x0.f[0] = w.su; x0.f[1] = w.sv; x0.f[2] = ow; x0.f[3] = op; x0.f[4] = oe; }
-    Vec5<T> xs;
-    xs.f[0] = w.su; xs.f[1] = w.sv; xs.f[2] = ow; xs.f[3] = op; xs.f[4] = oe;
-    SislSolveInfo si{};
-    int rc = solve_physical<T>(c, cf, w.g, as_const(rk), &x0, xs, st, &si, dev_info ? dev_info + it : nullptr);
-    if (info) info->solve[it] = si;
-    if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
-    if (tape) {  // the physical solution of this solve, for the recomputation of the VJP
-      static const int L5[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_W};
-      for (int q = 0; q < 5; ++q)
-        if (tape[5 * it + q] &&
-            cudaMemcpyAsync(tape[5 * it + q], xs.f[q], sizeof(T) * field_size(d, L5[q]), cudaMemcpyDeviceToDevice,
-                            st) != cudaSuccess)
-          return SISL_ERR_CUDA;
-    }
-    if (rc != SISL_OK && status == SISL_OK) status = rc;
+}
+
+// 4. predictor-corrector with two implicit solves (steppers.py:911-998):
+// the theta' predictor and the right-hand side of solve `it`, staged in the
+// GMRES vectors with its initial guess
+template <typename T>
+Vec5<T> step_solution(const StepRun<T>& r) {
+  const SWork<T>& w = r.w;
+  Vec5<T> xs;
+  xs.f[0] = w.su; xs.f[1] = w.sv; xs.f[2] = (T*)r.out->w; xs.f[3] = (T*)r.out->pi_p; xs.f[4] = (T*)r.out->eta_dot;
+  return xs;
+}
+
+template <typename T>
+void step_pre_solve(StepRun<T>& r, int it) {
+  SislCore* c = r.c;
+  const Dims& d = c->d;
+  SWork<T>& w = r.w;
+  const SislState* in = r.in;
+  cudaStream_t st = r.st;
+  const T* u = (const T*)in->u;
+  const T* v = (const T*)in->v;
+  const T* wv = (const T*)in->w;
+  const T* eta = (const T*)in->eta_dot;
+  const T* pp = (const T*)in->pi_p;
+  T* ow = (T*)r.out->w;
+  T* op = (T*)r.out->pi_p;
+  T* oe = (T*)r.out->eta_dot;
+  T* oth = (T*)r.out->th_p;
+  const T* w_next = (it == 0) ? wv : ow;
+  {
+    KScope k(c, SISL_K_EXPLICIT, st);
+    launch_corrector_theta<T>(d, r.cf, w.tha, w.tth, wv, w_next, oth, st);
   }
-  // 5. divergence damping, bc_fn relaxation, EOS (steppers.py:1022-1056)
+  CorrectorIn<T> ci;
+  ci.rhs_u = w.ru; ci.rhs_v = w.rv; ci.rhs_w = w.rw; ci.rhs_pi = w.rp;
+  ci.th_next = oth;
+  ci.pg = (it == 0) ? pp : op;
+  ci.gu = (it == 0) ? u : w.su;
+  ci.gv = (it == 0) ? v : w.sv;
+  ci.geta = (it == 0) ? eta : oe;
+  ci.ug = (it == 0) ? w.ru : w.su;
+  ci.vg = (it == 0) ? w.rv : w.sv;
+  Vec5<T> rk;
+  rk.f[0] = w.ku; rk.f[1] = w.kv; rk.f[2] = w.kw; rk.f[3] = w.kp; rk.f[4] = w.reta;
+  {
+    KScope k(c, SISL_K_EXPLICIT, st);
+    launch_corrector_rhs<T>(d, r.cf, ci, rk, st);
+  }
+  CVec5<T> x0;
+  if (it == 0) { x0.f[0] = u; x0.f[1] = v; x0.f[2] = wv; x0.f[3] = pp; x0.f[4] = eta; }
+  else { x0.f[0] = w.su; x0.f[1] = w.sv; x0.f[2] = ow; x0.f[3] = op; x0.f[4] = oe; }
+  solve_prep<T>(c, r.cf, w.g, as_const(rk), &x0, st);
+}
+
+// the solution of solve `it` unscaled into the step's outputs (and the tape);
+// rc: the solve's status
+template <typename T>
+int step_post_solve(StepRun<T>& r, int it, int rc, const SislSolveInfo& si) {
+  SislCore* c = r.c;
+  const Dims& d = c->d;
+  if (r.info) r.info->solve[it] = si;
+  if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+  const Vec5<T> xs = step_solution(r);
+  solve_finish<T>(c, r.cf, r.w.g, xs, r.st);
+  if (r.tape) {  // the physical solution of this solve, for the recomputation of the VJP
+    static const int L5[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_W};
+    for (int q = 0; q < 5; ++q)
+      if (r.tape[5 * it + q] &&
+          cudaMemcpyAsync(r.tape[5 * it + q], xs.f[q], sizeof(T) * field_size(d, L5[q]), cudaMemcpyDeviceToDevice,
+                          r.st) != cudaSuccess)
+        return SISL_ERR_CUDA;
+  }
+  if (rc != SISL_OK && r.status == SISL_OK) r.status = rc;
+  return SISL_OK;
+}
+
+// 5. divergence damping, bc_fn relaxation, EOS (steppers.py:1022-1056) and
+// 6. history (steppers.py:1061-1071)
+template <typename T>
+int step_close(StepRun<T>& r) {
+  SislCore* c = r.c;
+  const Dims& d = c->d;
+  SWork<T>& w = r.w;
+  const SislState* in = r.in;
+  const SislState* out = r.out;
+  const SislRelaxation* relax = r.relax;
+  cudaStream_t st = r.st;
   FinalizeArgs<T> fa{};
   fa.u_in = w.su; fa.v_in = w.sv;
   fa.u_out = (T*)out->u; fa.v_out = (T*)out->v;
-  fa.w_io = ow; fa.th_io = oth; fa.pi_io = op;
+  fa.w_io = (T*)out->w; fa.th_io = (T*)out->th_p; fa.pi_io = (T*)out->pi_p;
   fa.rho_out = (T*)out->rho;
   fa.div = nullptr;
   if (c->s.nu_div != 0.0) {
     KScope k(c, SISL_K_OTHER, st);
-    launch_hdiv<T>(d, cf, w.su, w.sv, w.div, st);
+    launch_hdiv<T>(d, r.cf, w.su, w.sv, w.div, st);
     fa.div = w.div;
   }
   fa.relax.on = 0;
@@ -813,9 +897,8 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
   }
   {
     KScope k(c, SISL_K_OTHER, st);
-    launch_finalize<T>(d, cf, fa, st);
+    launch_finalize<T>(d, r.cf, fa, st);
   }
-  // 6. history (steppers.py:1061-1071)
   auto cp = [&](void* dst, const void* src, int loc) {
     if (dst && src && dst != src)
       cudaMemcpyAsync(dst, src, sizeof(T) * field_size(d, loc), cudaMemcpyDeviceToDevice, st);
@@ -825,9 +908,27 @@ int step_impl(SislCore* c, const SislState* in, const SislState* out, const Sisl
   cp(out->w_prev, in->w, LOC_W);
   cp(out->eta_dot_prev, in->eta_dot, LOC_W);
   cp(out->tend_th_prev, w.tth, LOC_M);
-  if (info) info->kernel_launches = g_launches.load() - l0;
+  if (r.info) r.info->kernel_launches = g_launches.load() - r.l0;
   int e = check_cuda();
-  return e ? e : status;
+  return e ? e : r.status;
+}
+
+template <typename T>
+int step_impl(SislCore* c, const SislState* in, const SislState* out, const SislRelaxation* relax, void* ws,
+              size_t ws_bytes, cudaStream_t st, SislStepInfo* info, void* const* tape = nullptr,
+              GDevInfo* dev_info = nullptr, const void* const* phys = nullptr) {
+  StepRun<T> r;
+  int rc = step_open<T>(r, c, in, out, relax, ws, ws_bytes, st, info, tape, phys);
+  if (rc) return rc;
+  step_explicit<T>(r);
+  for (int it = 0; it < 2; ++it) {
+    step_pre_solve<T>(r, it);
+    SislSolveInfo si{};
+    rc = gmres_run<T>(c, r.cf, r.w.g, st, &si, 0, dev_info ? dev_info + it : nullptr);
+    rc = step_post_solve<T>(r, it, rc, si);
+    if (rc) return rc;
+  }
+  return step_close<T>(r);
 }
 
 // ---------------------------------------------------------------------------
@@ -1875,6 +1976,7 @@ struct SislStepGraph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   GDevInfo* dinfo = nullptr;  // 2 per member, device
+  void* group_mem = nullptr;  // grouped solves: member descriptors and block tables, device
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;
 };
@@ -1885,6 +1987,7 @@ void destroy_graph(SislStepGraph* g) {
   if (g->exec) cudaGraphExecDestroy(g->exec);
   if (g->graph) cudaGraphDestroy(g->graph);
   if (g->dinfo) cudaFree(g->dinfo);
+  if (g->group_mem) cudaFree(g->group_mem);
   for (cudaStream_t s : g->streams) cudaStreamDestroy(s);
   for (cudaEvent_t e : g->events) cudaEventDestroy(e);
   delete g;
@@ -1953,6 +2056,245 @@ int capture_members(int n, SislCore* const* cores, F&& record, SislStepGraph** o
   return SISL_OK;
 }
 
+// One solve (`it` of the step) of every member as grouped launches, captured
+// on st: the restart loop is one conditional WHILE node (body captured on
+// side) that runs while any member continues; each member's own loop state
+// (cycles, convergence) lives in its GState and `running` flag.  The
+// sequence of phases per member is gmres_run's, so each member's result is
+// the same bits as its own graph-mode solve.
+template <typename T>
+int gmres_group_run(const GroupLaunch<T>& gl, cudaStream_t st, cudaStream_t side, int it) {
+  const int R = gl.R;
+  const int64_t l0 = g_launches.load();
+  grp_setup<T>(gl, st);
+  if (gl.refine) grp_convert<T>(gl, 0, st);
+  grp_dots<T>(gl, 0, GV_B, 1 /*BNORM*/, 0, st);
+  if (gl.method == SISL_GMRES_INCREMENTAL) {
+    grp_convert<T>(gl, 3, st);
+    grp_precond<T>(gl, 1, 1, 0, st);
+    grp_dots<T>(gl, 0, GV_V0 + 1, 2 /*MBNORM*/, 0, st);
+  }
+  grp_init_tol<T>(gl, st);
+  auto residual = [&](cudaStream_t s) {
+    if (gl.refine) {
+      grp_matvec<T>(gl, 2, 0, s);
+      grp_convert<T>(gl, 1, s);
+    } else {
+      grp_matvec<T>(gl, 1, 0, s);
+    }
+    grp_precond<T>(gl, 0, 0, 0, s);
+    grp_dots<T>(gl, 0, GV_V0, 3 /*RNORM*/, 0, s);
+  };
+  auto cycle = [&](cudaStream_t s) {
+    grp_begin_cycle<T>(gl, s);
+    for (int j = 0; j < R; ++j) {
+      grp_matvec<T>(gl, 0, j, s);
+      grp_precond<T>(gl, 0, j + 1, 1, s);
+      grp_dots<T>(gl, j + 1, GV_V0 + j + 1, 0 /*PROJ*/, 1, s);
+      grp_update_arnoldi<T>(gl, j + 1, s);
+    }
+    grp_small_solve<T>(gl, s);
+    grp_update_x<T>(gl, s);
+  };
+  residual(st);
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t gr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if (cuda_failed(cudaStreamGetCaptureInfo(st, &cs, nullptr, &gr, &deps, &nd), "cudaStreamGetCaptureInfo") ||
+      cs != cudaStreamCaptureStatusActive)
+    return SISL_ERR_ARG;
+  cudaGraphConditionalHandle h;
+  if (cuda_failed(cudaGraphConditionalHandleCreate(&h, gr, 0, cudaGraphCondAssignDefault),
+                  "cudaGraphConditionalHandleCreate"))
+    return SISL_ERR_CUDA;
+  grp_gate<T>(gl, h, 0, st);
+  if (cuda_failed(cudaStreamGetCaptureInfo(st, &cs, nullptr, &gr, &deps, &nd), "cudaStreamGetCaptureInfo"))
+    return SISL_ERR_CUDA;
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cuda_failed(cudaGraphAddNode(&node, gr, deps, nd, &np), "cudaGraphAddNode(conditional)")) return SISL_ERR_CUDA;
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  if (cuda_failed(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies),
+                  "cudaStreamUpdateCaptureDependencies"))
+    return SISL_ERR_CUDA;
+  if (cuda_failed(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+                  "cudaStreamBeginCaptureToGraph"))
+    return SISL_ERR_CUDA;
+  cycle(side);
+  residual(side);
+  grp_gate<T>(gl, h, 1, side);
+  cudaGraph_t body_out = nullptr;
+  if (cuda_failed(cudaStreamEndCapture(side, &body_out), "cudaStreamEndCapture(body)")) return SISL_ERR_CUDA;
+  grp_info<T>(gl, it, st);
+  if (gl.refine) grp_convert<T>(gl, 2, st);
+  (void)l0;
+  return check_cuda();
+}
+
+// Grouped ensemble step graph: the members' explicit, corrector and
+// finalisation segments as parallel branches, each of the step's two solves
+// as one grouped GMRES over all members (gmres_group_run).
+template <typename T>
+int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                    const SislRelaxation* const* relax, void* const* solves, void* const* ws,
+                    const size_t* ws_bytes, SislStepGraph** out) {
+  SislStepGraph* g = new (std::nothrow) SislStepGraph();
+  if (!g) return SISL_ERR_ARG;
+  g_last_error[0] = 0;
+  g->n = n;
+  cudaStream_t st = nullptr;
+  auto fail = [&](int rc) {
+    cudaStreamCaptureStatus cs;
+    if (st && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(st, &junk);
+      if (junk) cudaGraphDestroy(junk);
+    }
+    cudaGetLastError();
+    destroy_graph(g);
+    return rc;
+  };
+  const SislCore* c0 = cores[0];
+  const int R = c0->prm.solver_restart;
+  const int method = c0->prm.solve_method;
+  const bool refine = refining<T>(c0);
+  for (int m = 0; m < n; ++m) {
+    const SislCore* c = cores[m];
+    if (c->timing_class != SISL_K_NONE) return fail(SISL_ERR_ARG);  // no timing events inside a graph
+    if (c->prm.solver_restart != R || c->prm.solve_method != method || refining<T>(c) != refine ||
+        c->d.nz < 2 || R < 1 || R > GM_MAXR) {
+      snprintf(g_last_error, sizeof(g_last_error),
+               "grouped solve: member %d differs in restart, GMRES method or refinement, or has nz < 2", m);
+      return fail(SISL_ERR_ARG);
+    }
+  }
+  std::vector<StepRun<T>> runs(n);
+  // streams: one per member, the capture stream, the loop-body stream
+  for (int q = 0; q < n + 2; ++q) {
+    cudaStream_t s;
+    if (cuda_failed(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate")) return fail(SISL_ERR_CUDA);
+    g->streams.push_back(s);
+  }
+  st = g->streams[n];
+  cudaStream_t side = g->streams[n + 1];
+  for (int q = 0; q < n + 1; ++q) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(SISL_ERR_CUDA);
+    g->events.push_back(e);
+  }
+  for (int m = 0; m < n; ++m) {
+    const int rc = step_open<T>(runs[m], cores[m], &ins[m], &outs[m], relax ? relax[m] : nullptr, ws[m], ws_bytes[m],
+                                g->streams[m], nullptr, solves ? solves + 10 * m : nullptr, nullptr);
+    if (rc) return fail(rc);
+  }
+  // member descriptors and block tables
+  const int NT = group_tables(R);
+  const size_t desc_bytes = align256(sizeof(GroupMember<T>) * n);
+  const size_t tab_bytes = sizeof(int) * (size_t)NT * (n + 1);
+  const size_t info_bytes = sizeof(GDevInfo) * 2 * n;
+  if (cuda_failed(cudaMalloc(&g->group_mem, desc_bytes + tab_bytes), "cudaMalloc") ||
+      cuda_failed(cudaMalloc(&g->dinfo, info_bytes), "cudaMalloc"))
+    return fail(SISL_ERR_CUDA);
+  GroupMember<T>* dmem = (GroupMember<T>*)g->group_mem;
+  int* dtab = (int*)((char*)g->group_mem + desc_bytes);
+  GDevInfo* dinfo = g->dinfo;
+  std::vector<GroupMember<T>> hm(n);
+  GroupLaunch<T> gl;
+  gl.mem = dmem;
+  gl.first = dtab;
+  gl.M = n;
+  gl.R = R;
+  gl.method = method;
+  gl.refine = refine;
+  gl.first_h.assign((size_t)NT * (n + 1), 0);
+  gl.nz_h.resize(n);
+  for (int m = 0; m < n; ++m) {
+    const SislCore* c = cores[m];
+    const GWork<T>& w = runs[m].w.g;
+    GroupMember<T>& e = hm[m];
+    std::memset(&e, 0, sizeof(e));
+    e.d = c->d;
+    e.c = coef_of<T>(c);
+    if (refine) e.c64 = coef64_of(c);
+    e.vec = w.vec;
+    e.x64 = w.x64;
+    e.b64 = w.b64;
+    e.r64 = w.r64;
+    e.npad = w.npad;
+    for (int q = 0; q < 5; ++q) e.off[q] = w.off[q];
+    e.gs = w.gs;
+    e.partial = w.partial;
+    e.info[0] = dinfo + 2 * m;
+    e.info[1] = dinfo + 2 * m + 1;
+    e.eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+    e.tol = c->prm.solver_tol;
+    e.atol_in = c->prm.solver_atol;
+    e.maxiter = c->prm.solver_maxiter;
+    e.running = 0;
+    gl.nz_h[m] = c->d.nz;
+    const size_t np = w.npad;
+    int cnt[64 + GM_MAXR];
+    cnt[GT_MV] = group_matvec_blocks(c->d);
+    cnt[GT_PC] = group_precond_blocks(c->d);
+    cnt[GT_UPD] = gm_update_blocks<T>(np);
+    cnt[GT_X64] = gm_x64_blocks(np);
+    cnt[GT_CVT] = group_convert_blocks(np);
+    for (int q = 0; q <= R; ++q) cnt[GT_DOTS0 + q] = gm_dots_blocks<T>(q, np);
+    for (int t = 0; t < NT; ++t) {
+      int* row = gl.first_h.data() + (size_t)t * (n + 1);
+      row[m + 1] = row[m] + cnt[t];
+    }
+  }
+  if (cuda_failed(cudaMemcpy(dmem, hm.data(), sizeof(GroupMember<T>) * n, cudaMemcpyHostToDevice), "cudaMemcpy") ||
+      cuda_failed(cudaMemcpy(dtab, gl.first_h.data(), tab_bytes, cudaMemcpyHostToDevice), "cudaMemcpy") ||
+      cuda_failed(cudaMemset(dinfo, 0, info_bytes), "cudaMemset"))
+    return fail(SISL_ERR_CUDA);
+  auto fork = [&]() -> int {
+    if (cuda_failed(cudaEventRecord(g->events[n], st), "cudaEventRecord(fork)")) return SISL_ERR_CUDA;
+    for (int m = 0; m < n; ++m)
+      if (cuda_failed(cudaStreamWaitEvent(g->streams[m], g->events[n], 0), "cudaStreamWaitEvent(fork)"))
+        return SISL_ERR_CUDA;
+    return SISL_OK;
+  };
+  auto join = [&]() -> int {
+    for (int m = 0; m < n; ++m) {
+      if (cuda_failed(cudaEventRecord(g->events[m], g->streams[m]), "cudaEventRecord(join)")) return SISL_ERR_CUDA;
+      if (cuda_failed(cudaStreamWaitEvent(st, g->events[m], 0), "cudaStreamWaitEvent(join)")) return SISL_ERR_CUDA;
+    }
+    return SISL_OK;
+  };
+  if (cuda_failed(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture"))
+    return fail(SISL_ERR_CUDA);
+  int rc = fork();
+  if (rc) return fail(rc);
+  for (int m = 0; m < n; ++m) {
+    step_explicit<T>(runs[m]);
+    step_pre_solve<T>(runs[m], 0);
+  }
+  if ((rc = join()) || (rc = gmres_group_run<T>(gl, st, side, 0)) || (rc = fork())) return fail(rc);
+  const SislSolveInfo none{};
+  for (int m = 0; m < n; ++m) {
+    if ((rc = step_post_solve<T>(runs[m], 0, SISL_OK, none))) return fail(rc);
+    step_pre_solve<T>(runs[m], 1);
+  }
+  if ((rc = join()) || (rc = gmres_group_run<T>(gl, st, side, 1)) || (rc = fork())) return fail(rc);
+  for (int m = 0; m < n; ++m) {
+    if ((rc = step_post_solve<T>(runs[m], 1, SISL_OK, none))) return fail(rc);
+    rc = step_close<T>(runs[m]);
+    if (rc < 0) return fail(rc);
+  }
+  if ((rc = join())) return fail(rc);
+  if (cuda_failed(cudaStreamEndCapture(st, &g->graph), "cudaStreamEndCapture")) return fail(SISL_ERR_CUDA);
+  if (cuda_failed(cudaGraphInstantiate(&g->exec, g->graph, 0), "cudaGraphInstantiate")) return fail(SISL_ERR_CUDA);
+  *out = g;
+  return SISL_OK;
+}
+
 // Argument checks shared by the graph builders: distinct cores (a core's
 // side stream serves one branch), workspaces of the given kind.
 int check_members(int n, SislCore* const* cores, void* const* ws, const size_t* ws_bytes, int ws_kind) {
@@ -2001,6 +2343,22 @@ int sisl_step_graph_create_taped(int n, SislCore* const* cores, const SislState*
                    : step_impl<float>(c, &ins[m], &outs[m], rl, ws[m], ws_bytes[m], ms, nullptr, tape, di);
       },
       out);
+}
+
+int sisl_step_graph_create_grouped(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                                   const SislRelaxation* const* relax, void* const* solves, void* const* ws,
+                                   const size_t* ws_bytes, void* stream, SislStepGraph** out) {
+  if (!out || n < 1 || !cores || !ins || !outs || !ws || !ws_bytes) return SISL_ERR_ARG;
+  int rc = check_members(n, cores, ws, ws_bytes, SISL_WS_STEP);
+  if (rc) return rc;
+  for (int m = 0; m < n; ++m) {
+    if (!step_args_ok(ins[m], outs[m])) return SISL_ERR_ARG;
+    if (cores[m]->grid.dtype != cores[0]->grid.dtype) return SISL_ERR_ARG;
+  }
+  (void)stream;  // captured on a private stream
+  return (cores[0]->grid.dtype == SISL_F64)
+             ? capture_grouped<double>(n, cores, ins, outs, relax, solves, ws, ws_bytes, out)
+             : capture_grouped<float>(n, cores, ins, outs, relax, solves, ws, ws_bytes, out);
 }
 
 int sisl_step_vjp_graph_create(int n, SislCore* const* cores, const SislState* ins, void* const* solves,

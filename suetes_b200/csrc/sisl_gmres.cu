@@ -12,7 +12,7 @@
 // on load, projections use h_i = s_i <V_i, w>, updates use h_i s_i V_i.
 // Every reduction accumulates in float64; the last block of a reduction
 // kernel (ticket counter) finishes the sum and runs the scalar logic.
-#include "sisl_gmres.cuh"
+#include "sisl_group.cuh"
 
 #include <math.h>
 
@@ -53,13 +53,13 @@ __device__ __forceinline__ double warp_sum(double s) {
 
 // Last-block ticket.  Returns true in exactly one block, after every other
 // block's partial results are visible.
-__device__ __forceinline__ bool last_block(unsigned int* counter) {
+__device__ __forceinline__ bool last_block(unsigned int* counter, unsigned int nblk) {
   __shared__ bool am_last;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned int t = atomicAdd(counter, 1u);
-    am_last = (t == gridDim.x - 1);
+    am_last = (t == nblk - 1);
   }
   __syncthreads();
   if (am_last) __threadfence();
@@ -72,17 +72,18 @@ enum DotMode { DM_PROJ = 0, DM_BNORM = 1, DM_MBNORM = 2, DM_RNORM = 3 };
 // Each thread accumulates its products in its own shared-memory slots
 // acc[q * blockDim + tid] (float64), so consecutive basis vectors stream
 // without a reduction in between; the block reduces once at the end.
+// Block `bid` of `nblk` blocks of one reduction (a member's share of a
+// grouped launch, or the whole grid of a standalone one).
 template <typename T>
-__global__ void dots_kernel(const T* __restrict__ Vb, size_t stride, int m, const T* __restrict__ w, size_t n,
-                            double* partial, GState* gs, int mode, int gated) {
-  if (gated && gs->active == 0) return;
+__device__ __forceinline__ void dots_body(const T* __restrict__ Vb, size_t stride, int m, const T* __restrict__ w,
+                                          size_t n, double* partial, GState* gs, int mode, int bid, int nblk) {
   extern __shared__ double acc[];  // (m + 1) * blockDim.x
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int q = 0; q <= m; ++q) acc[q * nt + tid] = 0.0;
   constexpr int VN = V16<T>::n;
   constexpr int E = CH * VN;
   const size_t tile = (size_t)nt * E;
-  for (size_t base = (size_t)blockIdx.x * tile; base < n; base += (size_t)gridDim.x * tile) {
+  for (size_t base = (size_t)bid * tile; base < n; base += (size_t)nblk * tile) {
     T wr[E];
 #pragma unroll
     for (int c = 0; c < CH; ++c) {
@@ -146,14 +147,14 @@ __global__ void dots_kernel(const T* __restrict__ Vb, size_t stride, int m, cons
     double s_ = 0.0;
     for (int t = lane; t < nt; t += 32) s_ += acc[q * nt + t];
     s_ = warp_sum(s_);
-    if (lane == 0) partial[(size_t)blockIdx.x * (GM_MAXR + 2) + q] = s_;
+    if (lane == 0) partial[(size_t)bid * (GM_MAXR + 2) + q] = s_;
   }
-  if (!last_block(&gs->counter)) return;
+  if (!last_block(&gs->counter, (unsigned)nblk)) return;
   // finish: sum the partials of all blocks, one warp per result (lanes
   // stride over the blocks, so the loads are independent)
   for (int q = wp; q <= m; q += nw) {
     double s_ = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) s_ += partial[(size_t)b * (GM_MAXR + 2) + q];
+    for (int b = lane; b < nblk; b += 32) s_ += partial[(size_t)b * (GM_MAXR + 2) + q];
     s_ = warp_sum(s_);
     if (lane == 0) acc[q] = s_;
   }
@@ -176,32 +177,44 @@ __global__ void dots_kernel(const T* __restrict__ Vb, size_t stride, int m, cons
   }
 }
 
+template <typename T>
+__global__ void dots_kernel(const T* __restrict__ Vb, size_t stride, int m, const T* __restrict__ w, size_t n,
+                            double* partial, GState* gs, int mode, int gated) {
+  if (gated && gs->active == 0) return;
+  dots_body<T>(Vb, stride, m, w, n, partial, gs, mode, blockIdx.x, gridDim.x);
+}
+
 enum UpdMode { UM_NONE = 0, UM_ARNOLDI = 1 };
 
 // x64 += sum_{i < min(m, kdone)} coef_i V_i with a float64 solution (the
 // end-of-cycle update of GMRES with iterative refinement)
 template <typename T>
-__global__ void __launch_bounds__(256) update_x64_kernel(const T* __restrict__ Vb, size_t stride, int m,
-                                                         double* __restrict__ x, size_t n, const GState* gs) {
+__device__ __forceinline__ void update_x64_body(const T* __restrict__ Vb, size_t stride, int m,
+                                                double* __restrict__ x, size_t n, const GState* gs, int bid,
+                                                int nblk) {
   __shared__ double cf[GM_MAXR + 2];
   const int mm = min(m, gs->kdone);
   for (int q = threadIdx.x; q < mm; q += blockDim.x) cf[q] = gs->coef[q];
   __syncthreads();
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+  for (size_t e = bid * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)nblk * blockDim.x) {
     double acc = x[e];
     for (int i = 0; i < mm; ++i) acc += cf[i] * (double)Vb[(size_t)i * stride + e];
     x[e] = acc;
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) update_x64_kernel(const T* __restrict__ Vb, size_t stride, int m,
+                                                         double* __restrict__ x, size_t n, const GState* gs) {
+  update_x64_body<T>(Vb, stride, m, x, n, gs, blockIdx.x, gridDim.x);
 }
 
 // w <- w + sign * sum_{i<m'} coef_i V_i with coef from gs->coef (UM_NONE,
 // m' = min(m, kdone) when limit_kdone) or coef_i = h_i s_i (UM_ARNOLDI),
 // then optionally finish the Arnoldi step j = m - 1.
 template <typename T>
-__global__ void __launch_bounds__(GT) update_kernel(const T* __restrict__ Vb, size_t stride, int m,
-                                                    T* __restrict__ w, size_t n, double sign, double* partial,
-                                                    GState* gs, int mode, int gated, int limit_kdone) {
-  if (gated && gs->active == 0) return;
+__device__ __forceinline__ void update_body(const T* __restrict__ Vb, size_t stride, int m, T* __restrict__ w,
+                                            size_t n, double sign, double* partial, GState* gs, int mode,
+                                            int limit_kdone, int bid, int nblk) {
   __shared__ double cf[GM_MAXR + 2];
   __shared__ double red[GT / 32];
   int mm = m;
@@ -213,7 +226,7 @@ __global__ void __launch_bounds__(GT) update_kernel(const T* __restrict__ Vb, si
   constexpr int E = CH * VN;
   const size_t tile = (size_t)GT * E;
   double sq = 0.0;
-  for (size_t base = (size_t)blockIdx.x * tile; base < n; base += (size_t)gridDim.x * tile) {
+  for (size_t base = (size_t)bid * tile; base < n; base += (size_t)nblk * tile) {
     T wr[E];
     bool ok[CH];
 #pragma unroll
@@ -251,12 +264,12 @@ __global__ void __launch_bounds__(GT) update_kernel(const T* __restrict__ Vb, si
   if (threadIdx.x == 0) {
     double s = 0.0;
     for (int q = 0; q < GT / 32; ++q) s += red[q];
-    partial[blockIdx.x] = s;
+    partial[bid] = s;
   }
-  if (!last_block(&gs->counter)) return;
+  if (!last_block(&gs->counter, (unsigned)nblk)) return;
   if (threadIdx.x >= 32) return;
   double tot = 0.0;  // warp 0 sums the blocks' partials
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) tot += partial[b];
+  for (int b = threadIdx.x; b < nblk; b += 32) tot += partial[b];
   tot = warp_sum(tot);
   if (threadIdx.x != 0) return;
   gs->counter = 0;
@@ -310,8 +323,15 @@ __global__ void __launch_bounds__(GT) update_kernel(const T* __restrict__ Vb, si
     if (!(gs->err > gs->ptol)) gs->active = 0;
   }
 }
+template <typename T>
+__global__ void __launch_bounds__(GT) update_kernel(const T* __restrict__ Vb, size_t stride, int m,
+                                                    T* __restrict__ w, size_t n, double sign, double* partial,
+                                                    GState* gs, int mode, int gated, int limit_kdone) {
+  if (gated && gs->active == 0) return;
+  update_body<T>(Vb, stride, m, w, n, sign, partial, gs, mode, limit_kdone, blockIdx.x, gridDim.x);
+}
 
-__global__ void setup_kernel(GState* gs, double eps, double tol, double atol_in, int restart, int method) {
+__device__ void setup_state(GState* gs, double eps, double tol, double atol_in, int restart, int method) {
   gs->eps = eps;
   gs->tol = tol;
   gs->atol_in = atol_in;
@@ -325,6 +345,9 @@ __global__ void setup_kernel(GState* gs, double eps, double tol, double atol_in,
   gs->steps = 0;
   for (int q = 0; q < GM_MAXR + 2; ++q) gs->s[q] = 0.0;
 }
+__global__ void setup_kernel(GState* gs, double eps, double tol, double atol_in, int restart, int method) {
+  setup_state(gs, eps, tol, atol_in, restart, method);
+}
 
 // Graph mode: after a residual, count the finished cycle and set the WHILE
 // condition: another cycle while ||M r|| > atol and cycles < maxiter.
@@ -337,7 +360,7 @@ __global__ void gate_kernel(GState* gs, cudaGraphConditionalHandle h, int maxite
   cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
-__global__ void info_kernel(const GState* gs, GDevInfo* o) {
+__device__ void info_state(const GState* gs, GDevInfo* o) {
   o->cycles = gs->cycles;
   o->arnoldi_steps = gs->steps;
   o->converged = (gs->rnorm <= gs->atol) ? 1 : 0;
@@ -346,14 +369,16 @@ __global__ void info_kernel(const GState* gs, GDevInfo* o) {
   o->atol = gs->atol;
   o->b_norm = gs->bnorm;
 }
+__global__ void info_kernel(const GState* gs, GDevInfo* o) { info_state(gs, o); }
 
-__global__ void init_tol_kernel(GState* gs) {
+__device__ void init_tol_state(GState* gs) {
   // atol = max(tol ||b||, atol); ptol = ||M b|| min(1, atol / ||b||)
   gs->atol = fmax(gs->tol * gs->bnorm, gs->atol_in);
   gs->ptol = gs->mbnorm * fmin(1.0, gs->atol / gs->bnorm);
 }
+__global__ void init_tol_kernel(GState* gs) { init_tol_state(gs); }
 
-__global__ void begin_cycle_kernel(GState* gs) {
+__device__ void begin_cycle_state(GState* gs) {
   const int R = gs->restart;
   for (int q = threadIdx.x; q < R * (GM_MAXR + 1); q += blockDim.x) {
     const int r = q / (GM_MAXR + 1), c = q % (GM_MAXR + 1);
@@ -370,9 +395,10 @@ __global__ void begin_cycle_kernel(GState* gs) {
     gs->breakdown = 0;
   }
 }
+__global__ void begin_cycle_kernel(GState* gs) { begin_cycle_state(gs); }
 
 // y from the cycle's small problem; coef_i = y_i s_i.
-__global__ void small_solve_kernel(GState* gs) {
+__device__ void small_solve_state(GState* gs) {
   extern __shared__ double a2[];  // R * R
   const int R = gs->restart;
   __shared__ double b2[GM_MAXR];
@@ -430,12 +456,144 @@ __global__ void small_solve_kernel(GState* gs) {
     }
   }
 }
+__global__ void small_solve_kernel(GState* gs) { small_solve_state(gs); }
 
 __global__ void snapshot_kernel(const GState* gs, GHostView* v) {
   v->rnorm = gs->rnorm;
   v->atol = gs->atol;
   v->bnorm = gs->bnorm;
   v->kdone = gs->kdone;
+}
+
+// ---------------------------------------------------------------------------
+// grouped launches over ensemble members: flat block b runs block
+// (b - first[m]) of member m's standalone launch (sisl_group.cuh)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T* gvec(const GroupMember<T>& g, int v) {
+  return g.vec + (size_t)v * g.npad;
+}
+
+template <typename T>
+__global__ void group_dots_kernel(GroupMember<T>* mem, const int* __restrict__ first, int M, int m, int wv,
+                                  int mode, int gated) {
+  const int b = blockIdx.x;
+  const int mi = group_find(first, M, b);
+  const GroupMember<T>& g = mem[mi];
+  if (!g.running || (gated && g.gs->active == 0)) return;
+  const int f0 = first[mi];
+  dots_body<T>(gvec(g, GV_V0), g.npad, m, gvec(g, wv), g.npad, g.partial, g.gs, mode, b - f0, first[mi + 1] - f0);
+}
+
+// final_x = 0: Arnoldi projection of V_m out of V_0 .. V_{m-1} (gated);
+// final_x = 1: x += sum coef_i V_i over the cycle's basis
+template <typename T>
+__global__ void __launch_bounds__(GT) group_update_kernel(GroupMember<T>* mem, const int* __restrict__ first, int M,
+                                                          int m, int final_x) {
+  const int b = blockIdx.x;
+  const int mi = group_find(first, M, b);
+  const GroupMember<T>& g = mem[mi];
+  if (!g.running) return;
+  const int f0 = first[mi], nb = first[mi + 1] - f0;
+  if (final_x) {
+    update_body<T>(gvec(g, GV_V0), g.npad, m, gvec(g, GV_X), g.npad, 1.0, g.partial, g.gs, UM_NONE, 1, b - f0, nb);
+  } else {
+    if (g.gs->active == 0) return;
+    update_body<T>(gvec(g, GV_V0), g.npad, m, gvec(g, GV_V0 + m), g.npad, -1.0, g.partial, g.gs, UM_ARNOLDI, 0,
+                   b - f0, nb);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) group_update_x64_kernel(GroupMember<T>* mem, const int* __restrict__ first,
+                                                               int M, int m) {
+  const int b = blockIdx.x;
+  const int mi = group_find(first, M, b);
+  const GroupMember<T>& g = mem[mi];
+  if (!g.running) return;
+  const int f0 = first[mi];
+  update_x64_body<T>(gvec(g, GV_V0), g.npad, m, g.x64, g.npad, g.gs, b - f0, first[mi + 1] - f0);
+}
+
+// 0: b64 = b, x64 = x, r64 = 0; 1: residual r64 -> V_0 (u, v) | z (w, pi,
+// eta_dot); 2: x = x64 (after the loop: every member); 3: V_1 (u, v) = b (u, v)
+template <typename T>
+__global__ void __launch_bounds__(256) group_convert_kernel(GroupMember<T>* mem, const int* __restrict__ first,
+                                                            int M, int mode) {
+  const int b = blockIdx.x;
+  const int mi = group_find(first, M, b);
+  const GroupMember<T>& g = mem[mi];
+  if (mode != 2 && !g.running) return;
+  const size_t f0 = first[mi], nb = first[mi + 1] - f0;
+  const size_t n = (mode == 3) ? g.off[2] : g.npad;
+  const size_t step = nb * blockDim.x;
+  T* x = gvec(g, GV_X);
+  const T* bv = gvec(g, GV_B);
+  T* v0 = gvec(g, GV_V0);
+  T* z = gvec(g, GV_Z);
+  for (size_t e = (b - f0) * (size_t)blockDim.x + threadIdx.x; e < n; e += step) {
+    if (mode == 0) {
+      g.b64[e] = (double)bv[e];
+      g.x64[e] = (double)x[e];
+      g.r64[e] = 0.0;
+    } else if (mode == 1) {
+      (e < g.off[2] ? v0 : z)[e] = (T)g.r64[e];
+    } else if (mode == 2) {
+      x[e] = (T)g.x64[e];
+    } else {
+      v0[g.npad + e] = bv[e];
+    }
+  }
+}
+
+// one thread per member
+template <typename T>
+__global__ void group_setup_kernel(GroupMember<T>* mem, int M, int R, int method) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  GroupMember<T>& g = mem[m];
+  setup_state(g.gs, g.eps, g.tol, g.atol_in, R, method);
+  g.running = 1;
+}
+template <typename T>
+__global__ void group_init_tol_kernel(GroupMember<T>* mem, int M) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < M) init_tol_state(mem[m].gs);
+}
+template <typename T>
+__global__ void group_info_kernel(GroupMember<T>* mem, int M, int solve) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < M && mem[m].info[solve]) info_state(mem[m].gs, mem[m].info[solve]);
+}
+// one block per member
+template <typename T>
+__global__ void group_begin_cycle_kernel(GroupMember<T>* mem) {
+  const GroupMember<T>& g = mem[blockIdx.x];
+  if (g.running) begin_cycle_state(g.gs);
+}
+template <typename T>
+__global__ void group_small_solve_kernel(GroupMember<T>* mem) {
+  const GroupMember<T>& g = mem[blockIdx.x];
+  if (g.running) small_solve_state(g.gs);
+}
+// one block: count the finished cycle of every running member, decide which
+// members continue, set the WHILE condition while any does
+template <typename T>
+__global__ void group_gate_kernel(GroupMember<T>* mem, int M, cudaGraphConditionalHandle h, int after_cycle) {
+  int any = 0;
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    GroupMember<T>& g = mem[m];
+    GState* gs = g.gs;
+    if (after_cycle && g.running) {
+      gs->cycles += 1;
+      gs->steps += gs->kdone;
+    }
+    const int more = g.running && (gs->rnorm > gs->atol) && (gs->cycles < g.maxiter);
+    g.running = more;
+    any |= more;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
 }
 
 int flat_grid(size_t n, int elems_per_block) {
@@ -519,6 +677,97 @@ void gm_small_solve(GState* gs, int restart, cudaStream_t st) {
   small_solve_kernel<<<1, 256, smem, st>>>(gs);
 }
 void gm_snapshot(const GState* gs, GHostView* v, cudaStream_t st) { snapshot_kernel<<<1, 1, 0, st>>>(gs, v); }
+
+// ---------------------------------------------------------------------------
+// grouped host wrappers
+// ---------------------------------------------------------------------------
+template <typename T>
+int gm_dots_threads(int m) {
+  int nt = (int)(DOTS_SMEM_MAX / ((size_t)(m + 1) * sizeof(double)));
+  nt = nt >= 256 ? 256 : (nt / 32) * 32;
+  return nt < 32 ? 32 : nt;
+}
+template <typename T>
+int gm_dots_blocks(int m, size_t n) {
+  static SmemLimit attr_bytes;
+  ensure_smem_limit((const void*)dots_kernel<T>, attr_bytes, (size_t)DOTS_SMEM_MAX);
+  const int nt = gm_dots_threads<T>(m);
+  constexpr int E = CH * V16<T>::n;
+  return resident_grid((const void*)dots_kernel<T>, nt, (size_t)(m + 1) * nt * sizeof(double), n, nt * E);
+}
+template <typename T>
+int gm_update_blocks(size_t n) {
+  constexpr int E = CH * V16<T>::n;
+  return resident_grid((const void*)update_kernel<T>, GT, 0, n, GT * E);
+}
+int gm_x64_blocks(size_t n) { return flat_grid(n, 256 * 4); }
+int group_convert_blocks(size_t n) { return flat_grid(n, 256 * 8) < 296 ? flat_grid(n, 256 * 8) : 296; }
+
+template <typename T>
+void grp_setup(const GroupLaunch<T>& g, cudaStream_t st) {
+  group_setup_kernel<T><<<(g.M + 127) / 128, 128, 0, st>>>(g.mem, g.M, g.R, g.method);
+}
+template <typename T>
+void grp_dots(const GroupLaunch<T>& g, int m, int w, int mode, int gated, cudaStream_t st) {
+  static SmemLimit attr_bytes;
+  ensure_smem_limit((const void*)group_dots_kernel<T>, attr_bytes, (size_t)DOTS_SMEM_MAX);
+  const int nt = gm_dots_threads<T>(m);
+  const size_t smem = (size_t)(m + 1) * nt * sizeof(double);
+  group_dots_kernel<T><<<g.blocks(GT_DOTS0 + m), nt, smem, st>>>(g.mem, g.row(GT_DOTS0 + m), g.M, m, w, mode, gated);
+}
+template <typename T>
+void grp_update_arnoldi(const GroupLaunch<T>& g, int m, cudaStream_t st) {
+  group_update_kernel<T><<<g.blocks(GT_UPD), GT, 0, st>>>(g.mem, g.row(GT_UPD), g.M, m, 0);
+}
+template <typename T>
+void grp_update_x(const GroupLaunch<T>& g, cudaStream_t st) {
+  if (g.refine) group_update_x64_kernel<T><<<g.blocks(GT_X64), 256, 0, st>>>(g.mem, g.row(GT_X64), g.M, g.R);
+  else group_update_kernel<T><<<g.blocks(GT_UPD), GT, 0, st>>>(g.mem, g.row(GT_UPD), g.M, g.R, 1);
+}
+template <typename T>
+void grp_convert(const GroupLaunch<T>& g, int mode, cudaStream_t st) {
+  group_convert_kernel<T><<<g.blocks(GT_CVT), 256, 0, st>>>(g.mem, g.row(GT_CVT), g.M, mode);
+}
+template <typename T>
+void grp_init_tol(const GroupLaunch<T>& g, cudaStream_t st) {
+  group_init_tol_kernel<T><<<(g.M + 127) / 128, 128, 0, st>>>(g.mem, g.M);
+}
+template <typename T>
+void grp_begin_cycle(const GroupLaunch<T>& g, cudaStream_t st) {
+  group_begin_cycle_kernel<T><<<g.M, 256, 0, st>>>(g.mem);
+}
+template <typename T>
+void grp_small_solve(const GroupLaunch<T>& g, cudaStream_t st) {
+  static SmemLimit attr_bytes;
+  ensure_smem_limit((const void*)group_small_solve_kernel<T>, attr_bytes, (size_t)GM_MAXR * GM_MAXR * sizeof(double));
+  group_small_solve_kernel<T><<<g.M, 256, (size_t)g.R * g.R * sizeof(double), st>>>(g.mem);
+}
+template <typename T>
+void grp_gate(const GroupLaunch<T>& g, cudaGraphConditionalHandle h, int after_cycle, cudaStream_t st) {
+  group_gate_kernel<T><<<1, 256, 0, st>>>(g.mem, g.M, h, after_cycle);
+}
+template <typename T>
+void grp_info(const GroupLaunch<T>& g, int solve, cudaStream_t st) {
+  group_info_kernel<T><<<(g.M + 127) / 128, 128, 0, st>>>(g.mem, g.M, solve);
+}
+
+#define SISL_GROUP_INST(T)                                                                           \
+  template int gm_dots_threads<T>(int);                                                              \
+  template int gm_dots_blocks<T>(int, size_t);                                                       \
+  template int gm_update_blocks<T>(size_t);                                                          \
+  template void grp_setup<T>(const GroupLaunch<T>&, cudaStream_t);                                   \
+  template void grp_dots<T>(const GroupLaunch<T>&, int, int, int, int, cudaStream_t);                \
+  template void grp_update_arnoldi<T>(const GroupLaunch<T>&, int, cudaStream_t);                     \
+  template void grp_update_x<T>(const GroupLaunch<T>&, cudaStream_t);                                \
+  template void grp_convert<T>(const GroupLaunch<T>&, int, cudaStream_t);                            \
+  template void grp_init_tol<T>(const GroupLaunch<T>&, cudaStream_t);                                \
+  template void grp_begin_cycle<T>(const GroupLaunch<T>&, cudaStream_t);                             \
+  template void grp_small_solve<T>(const GroupLaunch<T>&, cudaStream_t);                             \
+  template void grp_gate<T>(const GroupLaunch<T>&, cudaGraphConditionalHandle, int, cudaStream_t);   \
+  template void grp_info<T>(const GroupLaunch<T>&, int, cudaStream_t);
+SISL_GROUP_INST(float)
+SISL_GROUP_INST(double)
+#undef SISL_GROUP_INST
 
 template void gm_dots<float>(const float*, size_t, int, const float*, size_t, double*, GState*, int, int,
                              cudaStream_t);

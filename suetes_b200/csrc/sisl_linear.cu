@@ -12,7 +12,7 @@
 // tiles of 32 columns: kinematic forcing and Helmholtz RHS, the Thomas
 // recurrences with the factorisation prepared once per core, then the w and
 // eta_dot back-substitution.
-#include "sisl_core.cuh"
+#include "sisl_group.cuh"
 
 namespace sisl {
 namespace {
@@ -282,17 +282,17 @@ struct MvB {  // the rest of level k (faces at mass level min(k, nz-1), w-level 
   T xw, damp, zxw, zew, cpidz;
 };
 
+// block (bx, by, bz) of a (., ., gz) grid of 32 x 4 threads
 template <typename T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kernel(Dims d, Coef<T> c, CVec5<T> x,
-                                                                                  const double* xscale, CVec5<T> b,
-                                                                                  Vec5<T> out, const int* active) {
-  if (active && *active == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void matvec_march_block(const Dims& d, const Coef<T>& c, const CVec5<T>& x,
+                                                   const double* xscale, const CVec5<T>& b, const Vec5<T>& out,
+                                                   int bx, int by, int bz, int gz) {
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   if (i > nx || j > ny) return;
-  const int kA = (int)((long)blockIdx.z * (nz + 1) / gridDim.z);
-  const int kB = (int)((long)(blockIdx.z + 1) * (nz + 1) / gridDim.z);
+  const int kA = (int)((long)bz * (nz + 1) / gz);
+  const int kB = (int)((long)(bz + 1) * (nz + 1) / gz);
   if (kA >= kB) return;
   const T xs = xscale ? (T)(*xscale) : T(1);
   const T sp = xs / (T)c.s.ps;
@@ -458,6 +458,13 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kern
     a1 = a2;
     b0 = b1;
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 2) matvec_march_kernel(Dims d, Coef<T> c, CVec5<T> x,
+                                                                                  const double* xscale, CVec5<T> b,
+                                                                                  Vec5<T> out, const int* active) {
+  if (active && *active == 0) return;
+  matvec_march_block<T>(d, c, x, xscale, b, out, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -981,13 +988,12 @@ struct PcDown {  // inputs of downward step k: mass level k, w level k + 1
 };
 
 template <typename T, int NT, int HINT>
-__global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
-                                                          const int* active) {
-  if (active && *active == 0) return;
+__device__ __forceinline__ void precond_pipe_block(const Dims& d, const Coef<T>& c, const CVec5<T>& r,
+                                                   const Vec5<T>& out, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_d = reinterpret_cast<T*>(smem_raw);  // [nz][NT]
   const int t = threadIdx.x;
-  const int i = blockIdx.x * NT + t, j = blockIdx.y;
+  const int i = bx * NT + t, j = by;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   if (i >= nx) return;
   const int pm = nx * ny, h = i + nx * j;
@@ -1082,6 +1088,12 @@ __global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVe
   const int ptop = h + nz * pm;
   ow[ptop] = ld(rw, ptop);
   oW[ptop] = ld(rW, ptop) * ld(c.dzw, ptop);
+}
+template <typename T, int NT, int HINT>
+__global__ void __launch_bounds__(NT) precond_pipe_kernel(Dims d, Coef<T> c, CVec5<T> r, Vec5<T> out,
+                                                          const int* active) {
+  if (active && *active == 0) return;
+  precond_pipe_block<T, NT, HINT>(d, c, r, out, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -1270,6 +1282,114 @@ void launch_precond(const Dims& d, const Coef<T>& c, CVec5<T> r, Vec5<T> out, co
     default: launch_precond_tile<T, 256, 32>(d, c, r, out, active, st); break;
   }
 }
+
+// ---------------------------------------------------------------------------
+// grouped matvec and preconditioner over ensemble members (sisl_group.cuh):
+// flat block b runs block (b - first[m]) of member m's column march
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T* gvec_l(const GroupMember<T>& g, int v) {
+  return g.vec + (size_t)v * g.npad;
+}
+
+// mode 0: Arnoldi step j (gated), V_j scaled by s_j -> V_{j+1} (u, v) | z;
+// mode 1: b - A x -> V_0 (u, v) | z; mode 2 (U = double): b64 - A64 x64 -> r64
+template <typename T, typename U>
+__global__ void __launch_bounds__(128, sizeof(U) == 4 ? 3 : 2) group_matvec_kernel(GroupMember<T>* mem,
+                                                                                  const int* __restrict__ first,
+                                                                                  int M, int mode, int j) {
+  const int b = blockIdx.x;
+  const int mi = group_find(first, M, b);
+  const GroupMember<T>& g = mem[mi];
+  if (!g.running) return;
+  if (mode == 0 && g.gs->active == 0) return;
+  const int gx = (g.d.nx + 1 + 31) / 32, gy = (g.d.ny + 1 + 3) / 4;
+  const int t = b - first[mi];
+  const int bz = t / (gx * gy), rr = t - bz * (gx * gy), by = rr / gx, bx = rr - by * gx;
+  // the scale pointer stays a run-time value in every mode (a literal null
+  // would let the compiler fold x * 1 and contract the rows into other FMAs
+  // than the standalone kernel's, changing the last bits)
+  const double* xsp = (mode == 0) ? &g.gs->s[j] : nullptr;
+  if constexpr (sizeof(U) == sizeof(T)) {
+    const T* src = gvec_l(g, mode == 0 ? GV_V0 + j : GV_X);
+    T* tgt = gvec_l(g, mode == 0 ? GV_V0 + j + 1 : GV_V0);
+    T* z = gvec_l(g, GV_Z);
+    const T* bv = gvec_l(g, GV_B);
+    CVec5<T> x, bb;
+    Vec5<T> out;
+    for (int q = 0; q < 5; ++q) {
+      x.f[q] = src + g.off[q];
+      bb.f[q] = (mode == 1) ? bv + g.off[q] : nullptr;
+      out.f[q] = (q < 2 ? tgt : z) + g.off[q];
+    }
+    matvec_march_block<T>(g.d, g.c, x, xsp, bb, out, bx, by, bz, 1);
+  } else {
+    CVec5<double> x, bb;
+    Vec5<double> out;
+    for (int q = 0; q < 5; ++q) {
+      x.f[q] = g.x64 + g.off[q];
+      bb.f[q] = g.b64 + g.off[q];
+      out.f[q] = g.r64 + g.off[q];
+    }
+    matvec_march_block<double>(g.d, g.c64, x, xsp, bb, out, bx, by, bz, 1);
+  }
+}
+
+// mode 0: target V_t: u, v already there, w, pi, eta_dot from z (gated when
+// t >= 1); mode 1: M b -> V_1 (u, v copied by the caller)
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) group_precond_kernel(GroupMember<T>* mem, const int* __restrict__ first, int M,
+                                                           int mode, int tv, int gated) {
+  const int b = blockIdx.x;
+  const int mi = group_find(first, M, b);
+  const GroupMember<T>& g = mem[mi];
+  if (!g.running || (gated && g.gs->active == 0)) return;
+  const int gx = (g.d.nx + NT - 1) / NT;
+  const int t = b - first[mi];
+  const int by = t / gx, bx = t - by * gx;
+  T* tgt = gvec_l(g, mode == 0 ? GV_V0 + tv : GV_V0 + 1);
+  const T* src = (mode == 0) ? gvec_l(g, GV_Z) : gvec_l(g, GV_B);
+  CVec5<T> r;
+  Vec5<T> out;
+  for (int q = 0; q < 5; ++q) {
+    r.f[q] = (q < 2 && mode == 0 ? tgt : src) + g.off[q];
+    out.f[q] = tgt + g.off[q];
+  }
+  precond_pipe_block<T, NT, 1>(g.d, g.c, r, out, bx, by);
+}
+
+// ---------------------------------------------------------------------------
+// grouped host wrappers
+// ---------------------------------------------------------------------------
+constexpr int GROUP_PC_NT = 64;
+int group_matvec_blocks(const Dims& d) { return ((d.nx + 1 + 31) / 32) * ((d.ny + 1 + 3) / 4); }
+int group_precond_blocks(const Dims& d) { return ((d.nx + GROUP_PC_NT - 1) / GROUP_PC_NT) * d.ny; }
+
+template <typename T>
+void grp_matvec(const GroupLaunch<T>& g, int mode, int j, cudaStream_t st) {
+  const int nb = g.blocks(GT_MV);
+  if (mode == 2) {
+    if constexpr (sizeof(T) == 4) group_matvec_kernel<T, double><<<nb, dim3(32, 4), 0, st>>>(g.mem, g.row(GT_MV), g.M, 2, 0);
+    return;
+  }
+  group_matvec_kernel<T, T><<<nb, dim3(32, 4), 0, st>>>(g.mem, g.row(GT_MV), g.M, mode, j);
+}
+
+template <typename T>
+void grp_precond(const GroupLaunch<T>& g, int mode, int t, int gated, cudaStream_t st) {
+  int nz_max = 1;
+  for (int m = 0; m < g.M; ++m) nz_max = nz_max > g.nz_h[m] ? nz_max : g.nz_h[m];
+  const size_t smem = (size_t)nz_max * GROUP_PC_NT * sizeof(T);
+  static SmemLimit attr_bytes;
+  ensure_smem_limit((const void*)group_precond_kernel<T, GROUP_PC_NT>, attr_bytes, smem);
+  group_precond_kernel<T, GROUP_PC_NT><<<g.blocks(GT_PC), GROUP_PC_NT, smem, st>>>(g.mem, g.row(GT_PC), g.M, mode, t,
+                                                                                   gated);
+}
+
+template void grp_matvec<float>(const GroupLaunch<float>&, int, int, cudaStream_t);
+template void grp_matvec<double>(const GroupLaunch<double>&, int, int, cudaStream_t);
+template void grp_precond<float>(const GroupLaunch<float>&, int, int, int, cudaStream_t);
+template void grp_precond<double>(const GroupLaunch<double>&, int, int, int, cudaStream_t);
 
 template void launch_matvec<float>(const Dims&, const Coef<float>&, CVec5<float>, const double*, CVec5<float>,
                                    Vec5<float>, const int*, cudaStream_t);

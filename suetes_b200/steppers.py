@@ -663,9 +663,14 @@ class StepGraph:
     GMRES restart loops are conditional nodes decided on the device, so a
     launch needs no host synchronisation; ``info(m)`` reads the solve
     statistics of the last launch.  ``PingPong`` alternates two graphs for
-    repeated steps."""
+    repeated steps.
 
-    def __init__(self, members, tapes=None):
+    ``grouped``: each of the step's two solves runs as one GMRES over all
+    members, every Krylov phase a single launch over a member/block table
+    (``sisl_step_graph_create_grouped``); the members' other work stays
+    parallel branches and every member's result is the same bits."""
+
+    def __init__(self, members, tapes=None, grouped=False):
         """``tapes``: optional per-member lists of the ten solve-output
         tensors to record (``sisl_step_graph_create_taped``)."""
         self.lib = _lib.load()
@@ -698,7 +703,15 @@ class StepGraph:
         self._keep += [carr, iarr, oarr, rarr, warr, barr, relax]
         h = ctypes.c_void_p()
         from .core import stream_ptr
-        if tapes is None:
+        if grouped:
+            tarr = None
+            if tapes is not None:
+                tarr = (ctypes.c_void_p * (10 * n))(*[t.data_ptr() for tp in tapes for t in tp])
+                self._keep += [tarr, tapes]
+            check(self.lib.sisl_step_graph_create_grouped(n, carr, iarr, oarr, rarr, tarr, warr, barr,
+                                                          stream_ptr(self.device), ctypes.byref(h)),
+                  "sisl_step_graph_create_grouped")
+        elif tapes is None:
             check(self.lib.sisl_step_graph_create(n, carr, iarr, oarr, rarr, warr, barr, stream_ptr(self.device),
                                                   ctypes.byref(h)), "sisl_step_graph_create")
         else:
@@ -741,10 +754,11 @@ class PingPong:
     is fixed when a graph is captured, so a member still on its first step
     takes that step eagerly here (``steps_done`` counts it)."""
 
-    def __init__(self, members, autotune=False):
+    def __init__(self, members, autotune=False, grouped=False):
         """``members``: sequence of ``(stepper, ds0, relax)``; ds0 is copied.
         ``autotune``: choose each member core's launch shapes (``Core.autotune``)
-        before the graphs are captured."""
+        before the graphs are captured.  ``grouped``: grouped solves
+        (``StepGraph``)."""
         self.a, self.b, spec_ab, spec_ba = [], [], [], []
         self.steps_done = 0
         self.tuning = []
@@ -766,7 +780,7 @@ class PingPong:
             spec_ba.append((stepper, B, A, rl))
         if self.steps_done and any(ds0.is_first_step != 1.0 for _, ds0, _ in members):
             raise ValueError("members must all be on their first step or all past it")
-        self.g = [StepGraph(spec_ab), StepGraph(spec_ba)]
+        self.g = [StepGraph(spec_ab, grouped=grouped), StepGraph(spec_ba, grouped=grouped)]
         self.k = 0
 
     def step(self):

@@ -28,10 +28,10 @@ def _eager(stepper, ds0, relax, nsteps):
     return cur, infos
 
 
-def _member(n, nz, dtype, amp=2.0, tol=None, maxiter=30):
-    st, s0, bc = rising_bubble(n, n, nz, dx=50.0, amp=amp, dtype=dtype,
+def _member(n, nz, dtype, amp=2.0, tol=None, maxiter=30, method="batched", ny=None):
+    st, s0, bc = rising_bubble(n, ny or n, nz, dx=50.0, amp=amp, dtype=dtype,
                                solver_tol=tol or (1e-10 if dtype == torch.float64 else 1e-7),
-                               solver_maxiter=maxiter, solver_restart=30)
+                               solver_maxiter=maxiter, solver_restart=30, solve_method=method)
     return st, st.to_device_state(s0), bc
 
 
@@ -66,6 +66,38 @@ def test_graph_ensemble_members_equal_their_eager_runs():
         out = pp.current()[m]
         for k in FIELDS:
             assert torch.equal(out.t[k], ref.t[k]), (m, k)
+
+
+@pytest.mark.parametrize("dtype,method", [(torch.float32, "batched"), (torch.float32, "incremental"),
+                                          (torch.float64, "batched")])
+def test_grouped_solves_equal_the_branch_graph(dtype, method):
+    """Grouped solves (every Krylov phase one launch over a member/block
+    table, one WHILE node per solve) give every member the same bits and
+    solve statistics as the graph of per-member branches, with members of
+    uneven sizes converging after different cycle counts and one member
+    stopped by its maxiter."""
+    from suetes_b200 import PingPong
+    specs = [(16, 12, 12, 1.5, None, 30), (24, 20, 16, 2.5, None, 30), (20, 20, 10, 2.0, 1e-14, 1)]
+    members = [_member(n, nz, dtype, amp=a, tol=tol, maxiter=mi, method=method, ny=ny)
+               for n, ny, nz, a, tol, mi in specs]
+    branch = PingPong(members)
+    grouped = PingPong(members, grouped=True)
+    for _ in range(3):
+        branch.step()
+        grouped.step()
+    cycles = []
+    for m in range(len(members)):
+        a, b = branch.current()[m], grouped.current()[m]
+        for k in FIELDS:
+            assert torch.equal(a.t[k], b.t[k]), (m, k, (a.t[k] - b.t[k]).abs().max().item())
+        ia, ib = branch.info(m), grouped.info(m)
+        assert ia["status"] == ib["status"], m
+        for q in range(2):
+            for key in ("cycles", "arnoldi_steps", "converged", "residual_norm"):
+                assert ia["solves"][q][key] == ib["solves"][q][key], (m, q, key)
+        cycles.append(ib["solves"][0]["cycles"])
+    assert cycles[2] == 1  # the member with maxiter 1 stopped after one cycle while the others went on
+    assert grouped.info(0)["status"] == 0 and grouped.info(1)["status"] == 0
 
 
 def test_graph_reports_unconverged_solves():
