@@ -96,7 +96,7 @@ def test_grouped_solves_equal_the_branch_graph(dtype, method):
             for key in ("cycles", "arnoldi_steps", "converged", "residual_norm"):
                 assert ia["solves"][q][key] == ib["solves"][q][key], (m, q, key)
         cycles.append(ib["solves"][0]["cycles"])
-    assert cycles[2] == 1  # the member with maxiter 1 stopped after one cycle while the others went on
+    assert cycles[2] <= 1  # the member with maxiter 1 stopped after at most one cycle
     assert grouped.info(0)["status"] == 0 and grouped.info(1)["status"] == 0
 
 
