@@ -45,7 +45,7 @@ enum { SISL_GMRES_BATCHED = 0, SISL_GMRES_INCREMENTAL = 1 };
 enum {
   SISL_WS_STEP = 0, SISL_WS_GMRES = 1, SISL_WS_DEPARTURE = 2, SISL_WS_EXPLICIT = 3, SISL_WS_OPERATOR = 4,
   SISL_WS_FFSL = 5, SISL_WS_STEP_VJP = 6, SISL_WS_EXPLICIT_VJP = 7, SISL_WS_FFSL_VJP = 8,
-  SISL_WS_SPLIT = 9
+  SISL_WS_SPLIT = 9, SISL_WS_SPLIT_VJP = 10
 };
 enum {
   SISL_RELAX_U = 1, SISL_RELAX_V = 2, SISL_RELAX_W = 4, SISL_RELAX_TH = 8, SISL_RELAX_PI = 16
@@ -353,6 +353,21 @@ int sisl_split_diagnose(SislCore* core, const void* u, const void* v, const void
                         void* stream);
 int sisl_split_step(SislCore* core, const SislState* in, const SislState* out, int ns, double alpha, double eps_l,
                     const void* tau_damp, const void* const phys_tend[4], void* ws, size_t ws_bytes, void* stream);
+/* Cotangent of sisl_split_step's input state from the cotangent of its
+ * output (the VJP of SplitExplicitStepper3D's three RK3 stages,
+ * steppers.py:1117-1231 and 1272-1737, as XLA differentiates them: the
+ * padded copies of centre-to-face staggers and the sign of the upwind flux
+ * carry no cotangent).  in, ns, alpha, eps_l, tau_damp: as given to
+ * sisl_split_step (no physics tendencies); out_bar: cotangents of u, v, w,
+ * eta_dot, pi_p, th_p (NULL members zero); in_bar receives the cotangents
+ * of the same input fields and must not alias in or out_bar.  The first two
+ * stage states are recomputed; the acoustic sub-steps are linear, so their
+ * transposes need no recorded intermediates.  Every scatter sums in fixed
+ * point: the same bits on every run.  ws: sisl_workspace_bytes(core,
+ * SISL_WS_SPLIT_VJP) bytes. */
+int sisl_split_step_vjp(SislCore* core, const SislState* in, const SislState* out_bar, const SislState* in_bar,
+                        int ns, double alpha, double eps_l, const void* tau_damp, void* ws, size_t ws_bytes,
+                        void* stream);
 /* Cotangent of one step's input state from the cotangent of its output
  * (the VJP of SISLStepper3D.step under jax.checkpoint, steppers.py:720-1073,
  * 792-850, with the reference's stop_gradient on the departure points and

@@ -15,7 +15,7 @@ SISL_F32, SISL_F64 = 0, 1
 LOC = {"m": 0, "u": 1, "v": 2, "w": 3}
 SISL_GMRES_BATCHED, SISL_GMRES_INCREMENTAL = 0, 1
 WS_STEP, WS_GMRES, WS_DEPARTURE, WS_EXPLICIT, WS_OPERATOR, WS_FFSL = 0, 1, 2, 3, 4, 5
-WS_STEP_VJP, WS_EXPLICIT_VJP, WS_FFSL_VJP, WS_SPLIT = 6, 7, 8, 9
+WS_STEP_VJP, WS_EXPLICIT_VJP, WS_FFSL_VJP, WS_SPLIT, WS_SPLIT_VJP = 6, 7, 8, 9, 10
 RELAX_U, RELAX_V, RELAX_W, RELAX_TH, RELAX_PI = 1, 2, 4, 8, 16
 K_NONE, K_MATVEC, K_PRECOND, K_DOTS, K_UPDATE, K_SL, K_EXPLICIT, K_OTHER = range(8)
 SISL_OK, SISL_NOT_CONVERGED = 0, 1
@@ -144,6 +144,9 @@ PROTOTYPES = {
     "sisl_split_diagnose": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp]),
     "sisl_split_step": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState), ctypes.c_int,
                                        ctypes.c_double, ctypes.c_double, vp, vp * 4, vp, ctypes.c_size_t, vp]),
+    "sisl_split_step_vjp": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
+                                           ctypes.POINTER(SislState), ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                           vp, vp, ctypes.c_size_t, vp]),
     "sisl_step_vjp": (ctypes.c_int, [vp, ctypes.POINTER(SislState), vp * 10, ctypes.POINTER(SislRelaxation),
                                      ctypes.POINTER(SislState), ctypes.POINTER(SislState), vp, ctypes.c_size_t, vp,
                                      ctypes.POINTER(SislStepInfo)]),

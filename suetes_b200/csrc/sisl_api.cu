@@ -1234,9 +1234,11 @@ namespace {
 
 // steppers.py:1117-1231: hyperdiffusion and physics tendencies of the step
 // start, then three stages of slow tendencies and acoustic sub-steps
+// nstages < 3 (the reverse sweep's recomputation): stop after that many
+// stages, whose states stay in the workspace (SplitWork::st)
 template <typename T>
 void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int ns, double alpha, double eps_l,
-                     const T* tau, const void* const* phys, void* ws, cudaStream_t st) {
+                     const T* tau, const void* const* phys, void* ws, cudaStream_t st, int nstages = 3) {
   const Dims& d = c->d;
   const Coef<T> cf = coef_of<T>(c);
   Carver cv{(char*)ws};
@@ -1264,7 +1266,7 @@ void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int
   const double dts[3] = {(c->s.dt / 3.0) / nst[0], (c->s.dt / 2.0) / nst[1], c->s.dt / nst[2]};
   const T* cur[6];
   for (int q = 0; q < 6; ++q) cur[q] = s0[q];
-  for (int stage = 0; stage < 3; ++stage) {
+  for (int stage = 0; stage < nstages; ++stage) {
     T* const* dst = stage == 2 ? dst_out : w.st[stage];
     // ---- slow tendencies (steppers.py:1362-1465) ----
     const T* hyp[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -1322,8 +1324,172 @@ void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int
     }
     for (int q = 0; q < 6; ++q) cur[q] = dst[q];
   }
-  if (out->rho && in->rho && out->rho != in->rho)
+  if (nstages == 3 && out->rho && in->rho && out->rho != in->rho)
     cudaMemcpyAsync(out->rho, in->rho, sizeof(T) * field_size(d, LOC_M), cudaMemcpyDeviceToDevice, st);
+}
+
+// Reverse-sweep buffers of the split-explicit step (after SplitWork).
+template <typename T>
+struct SplitVjpWork {
+  T* sb[2][6];  // stage-state cotangents (u, v, w, eta_dot, pi', th'), two sets
+  T *upp[2], *vpp[2], *wpp, *ppp, *uh, *vh, *gx0, *gy0;
+  T* sf[5];
+  T* tend[6];
+  T* adv[4];
+  T *hyp[4], *hyp_t[4], *gx4[4], *gy4[4], *tmp4[4];
+  T *s1, *s2;
+  void* det;
+};
+
+template <typename T>
+void carve_split_vjp(Carver& cv, const Dims& d, SplitVjpWork<T>& b) {
+  auto f = [&](int loc) { return (T*)cv.take(sizeof(T) * field_size(d, loc)); };
+  const int s_loc[6] = {LOC_U, LOC_V, LOC_W, LOC_W, LOC_M, LOC_M};
+  for (int q = 0; q < 2; ++q)
+    for (int r = 0; r < 6; ++r) b.sb[q][r] = f(s_loc[r]);
+  for (int q = 0; q < 2; ++q) { b.upp[q] = f(LOC_U); b.vpp[q] = f(LOC_V); }
+  b.wpp = f(LOC_W); b.ppp = f(LOC_M); b.uh = f(LOC_U); b.vh = f(LOC_V); b.gx0 = f(LOC_U); b.gy0 = f(LOC_V);
+  const int sf_loc[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_M};
+  for (int q = 0; q < 5; ++q) b.sf[q] = f(sf_loc[q]);
+  const int t_loc[6] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_M, LOC_M};
+  for (int q = 0; q < 6; ++q) b.tend[q] = f(t_loc[q]);
+  for (int q = 0; q < 4; ++q) {
+    b.adv[q] = f(LOC_M);
+    b.hyp[q] = f(LOC_M);
+    b.hyp_t[q] = f(LOC_M);
+    b.tmp4[q] = f(LOC_M);
+    b.gx4[q] = f(LOC_U);
+    b.gy4[q] = f(LOC_V);
+  }
+  b.s1 = f(LOC_M);
+  b.s2 = f(LOC_M);
+  b.det = cv.take(det_scatter_scratch_bytes(d, (int)sizeof(T)));
+}
+
+// The reverse of split_step_impl (steppers.py:1117-1231 under XLA's VJP):
+// recompute the first two stage states, then per stage from the last:
+// eta_dot diagnosis^T, stage assembly^T, the acoustic sub-steps^T (linear:
+// no recorded intermediates), their initialisation^T, the slow forcings^T,
+// upwind advection^T and explicit tendencies^T at the stage start, and the
+// hyperdiffusion^T of the stage and, at the end, of the step start.
+template <typename T>
+int split_vjp_impl(SislCore* c, const SislState* in, const SislState* ob, const SislState* ib, int ns, double alpha,
+                   double eps_l, const T* tau, void* ws, size_t ws_bytes, cudaStream_t st) {
+  const Dims& d = c->d;
+  const Coef<T> cf = coef_of<T>(c);
+  Carver cv{(char*)ws};
+  SplitWork<T> w;
+  carve_split<T>(cv, d, w);
+  SplitVjpWork<T> b;
+  carve_split_vjp<T>(cv, d, b);
+  if (cv.off > ws_bytes) return SISL_ERR_WORKSPACE;
+  static const int LOC6[6] = {LOC_U, LOC_V, LOC_W, LOC_W, LOC_M, LOC_M};
+  auto bytes = [&](int loc) { return sizeof(T) * field_size(d, loc); };
+  auto zero = [&](void* p, int loc) { return cudaMemsetAsync(p, 0, bytes(loc), st) == cudaSuccess; };
+  // recompute the stage states 1 and 2 (into w.st)
+  split_step_impl<T>(c, in, in, ns, alpha, eps_l, tau, nullptr, ws, st, 2);
+  T* s0b[6] = {(T*)ib->u, (T*)ib->v, (T*)ib->w, (T*)ib->eta_dot, (T*)ib->pi_p, (T*)ib->th_p};
+  const void* obv[6] = {ob->u, ob->v, ob->w, ob->eta_dot, ob->pi_p, ob->th_p};
+  const T* s0[6] = {(const T*)in->u, (const T*)in->v, (const T*)in->w, (const T*)in->eta_dot, (const T*)in->pi_p,
+                    (const T*)in->th_p};
+  for (int q = 0; q < 6; ++q) {
+    if (!zero(s0b[q], LOC6[q])) return SISL_ERR_CUDA;
+    T* dst = b.sb[0][q];
+    if (obv[q]) {
+      if (cudaMemcpyAsync(dst, obv[q], bytes(LOC6[q]), cudaMemcpyDeviceToDevice, st) != cudaSuccess) return SISL_ERR_CUDA;
+    } else if (!zero(dst, LOC6[q])) {
+      return SISL_ERR_CUDA;
+    }
+  }
+  const bool hyp_t = c->s.nu_h > 0.0, hyp_s = c->s.nu_h > 0.0 && c->s.nu_div > 0.0;
+  if (hyp_t)
+    for (int q = 0; q < 4; ++q)
+      if (!zero(b.hyp_t[q], LOC_M)) return SISL_ERR_CUDA;
+  const int nst[3] = {std::max(1, (int)std::nearbyint(ns / 3.0)), std::max(1, (int)std::nearbyint(ns / 2.0)), ns};
+  const double dts[3] = {(c->s.dt / 3.0) / nst[0], (c->s.dt / 2.0) / nst[1], c->s.dt / nst[2]};
+  const size_t nm = field_size(d, LOC_M);
+  int D = 0;  // b.sb[D]: cotangents of the current stage's output
+  for (int stage = 2; stage >= 0; --stage) {
+    const T* const* cur = stage == 0 ? s0 : (const T* const*)w.st[stage - 1];
+    T* const* Db = b.sb[D];
+    T* const* Cb = b.sb[1 - D];
+    for (int q = 0; q < 6; ++q)
+      if (!zero(Cb[q], LOC6[q])) return SISL_ERR_CUDA;
+    {
+      KScope k(c, SISL_K_OTHER, st, 4);
+      if (stage < 2) launch_split_diag_vjp<T>(d, cf, Db[2], Db[3], Db[0], Db[1], b.det, st);
+      const T dtau = (T)dts[stage];
+      const T dtns = (T)((double)dtau * nst[stage]);
+      launch_split_end_vjp<T>(d, (const T* const*)Db, Cb, s0b[5], b.upp[0], b.vpp[0], b.wpp, b.ppp, b.sf[4], dtns,
+                              st);
+    }
+    for (int q = 0; q < 4; ++q)
+      if (!zero(b.sf[q], q == 0 ? LOC_U : (q == 1 ? LOC_V : (q == 2 ? LOC_W : LOC_M)))) return SISL_ERR_CUDA;
+    SplitBar<T> a{};
+    a.wpp = b.wpp; a.ppp = b.ppp; a.uh = b.uh; a.vh = b.vh; a.gx0 = b.gx0; a.gy0 = b.gy0;
+    a.sfu = b.sf[0]; a.sfv = b.sf[1]; a.sfw = b.sf[2]; a.sfp = b.sf[3];
+    a.uc = Cb[0]; a.vc = Cb[1]; a.wc = Cb[2]; a.u0 = s0b[0]; a.v0 = s0b[1];
+    a.s1 = b.s1; a.s2 = b.s2; a.tau = tau;
+    a.dtau = (T)dts[stage]; a.alpha = (T)alpha; a.nu_div = (T)c->s.nu_div;
+    int A = 0;  // b.upp[A]: cotangent of u'' after the current sub-step
+    for (int n = nst[stage] - 1; n >= 0; --n) {
+      if (!zero(b.upp[1 - A], LOC_U) || !zero(b.vpp[1 - A], LOC_V) || !zero(b.uh, LOC_U) || !zero(b.vh, LOC_V) ||
+          !zero(b.gx0, LOC_U) || !zero(b.gy0, LOC_V))
+        return SISL_ERR_CUDA;
+      a.upp2 = b.upp[A]; a.vpp2 = b.vpp[A];
+      a.upp = b.upp[1 - A]; a.vpp = b.vpp[1 - A];
+      KScope k(c, SISL_K_OTHER, st, 9);
+      launch_split_substep_vjp<T>(d, cf, a, b.det, st);
+      A = 1 - A;
+    }
+    {
+      KScope k(c, SISL_K_OTHER, st, 6);
+      launch_split_init_vjp<T>(d, b.upp[A], b.vpp[A], b.wpp, b.ppp, s0b, Cb, st);
+      for (int q = 0; q < 4; ++q)
+        if (!zero(b.adv[q], LOC_M)) return SISL_ERR_CUDA;
+      launch_split_slow_vjp<T>(d, (const T* const*)b.sf, b.tend, b.adv, b.det, st);
+      launch_split_adv_vjp<T>(d, cf, cur[0], cur[1], cur[2], cur[3], cur[5], (T)eps_l, (const T* const*)b.adv, Cb[0],
+                              Cb[1], Cb[2], Cb[3], Cb[5], b.det, st);
+    }
+    // explicit tendencies (mode 1) at the stage start; their hyperdiffusion input
+    const bool hyp = hyp_s || hyp_t;
+    if (hyp)
+      for (int q = 0; q < 4; ++q)
+        if (!zero(b.hyp[q], LOC_M)) return SISL_ERR_CUDA;
+    {
+      ExplicitIn<T> ein{cur[0], cur[1], cur[2], cur[3], cur[4], cur[5], {nullptr, nullptr, nullptr, nullptr},
+                        {nullptr, nullptr, nullptr, nullptr}};
+      ExplicitBar<T> bi{};
+      for (int q = 0; q < 6; ++q) bi.f[q] = b.tend[q];
+      StateBar<T> so{Cb[0], Cb[1], Cb[2], Cb[3], Cb[4], Cb[5], {nullptr, nullptr, nullptr, nullptr}};
+      if (hyp)
+        for (int q = 0; q < 4; ++q) so.hyper[q] = b.hyp[q];
+      KScope k(c, SISL_K_EXPLICIT, st, 3);
+      launch_explicit_vjp<T>(d, cf, ein, bi, so, 1, b.det, st);
+    }
+    if (hyp_t && hyp) {  // hyp_s = hyper(stage) + hyp_t, or hyp_t alone
+      KScope k(c, SISL_K_OTHER, st, 4);
+      for (int q = 0; q < 4; ++q) launch_split_axpy<T>(nm, b.hyp[q], b.hyp_t[q], st);
+    }
+    if (hyp_s) {
+      PtrTable<T> h4{}, gx{}, gy{}, t4{};
+      for (int q = 0; q < 4; ++q) { h4.p[q] = b.hyp[q]; gx.p[q] = b.gx4[q]; gy.p[q] = b.gy4[q]; t4.p[q] = b.tmp4[q]; }
+      KScope k(c, SISL_K_EXPLICIT, st, 5);
+      launch_hyper_vjp<T>(d, cf, h4, gx, gy, t4, Cb[0], Cb[1], Cb[2], Cb[5], st);
+    }
+    if (stage == 0) {
+      KScope k(c, SISL_K_OTHER, st, 6);
+      for (int q = 0; q < 6; ++q) launch_split_axpy<T>(field_size(d, LOC6[q]), Cb[q], s0b[q], st);
+    }
+    D = 1 - D;
+  }
+  if (hyp_t) {
+    PtrTable<T> h4{}, gx{}, gy{}, t4{};
+    for (int q = 0; q < 4; ++q) { h4.p[q] = b.hyp_t[q]; gx.p[q] = b.gx4[q]; gy.p[q] = b.gy4[q]; t4.p[q] = b.tmp4[q]; }
+    KScope k(c, SISL_K_EXPLICIT, st, 5);
+    launch_hyper_vjp<T>(d, cf, h4, gx, gy, t4, s0b[0], s0b[1], s0b[2], s0b[5], st);
+  }
+  return check_cuda();
 }
 
 }  // namespace
@@ -1481,6 +1647,19 @@ size_t sisl_workspace_bytes(const SislCore* c, int what) {
       } else {
         SplitWork<float> w;
         carve_split<float>(cv, c->d, w);
+      }
+      break;
+    case SISL_WS_SPLIT_VJP:
+      if (f64) {
+        SplitWork<double> w;
+        carve_split<double>(cv, c->d, w);
+        SplitVjpWork<double> b;
+        carve_split_vjp<double>(cv, c->d, b);
+      } else {
+        SplitWork<float> w;
+        carve_split<float>(cv, c->d, w);
+        SplitVjpWork<float> b;
+        carve_split_vjp<float>(cv, c->d, b);
       }
       break;
     case SISL_WS_FFSL_VJP:
@@ -2584,6 +2763,29 @@ int sisl_split_step(SislCore* c, const SislState* in, const SislState* out, int 
   else
     split_step_impl<float>(c, in, out, ns, alpha, eps_l, (const float*)tau_damp, phys_tend, ws, st);
   return check_cuda();
+}
+
+int sisl_split_step_vjp(SislCore* c, const SislState* in, const SislState* out_bar, const SislState* in_bar, int ns,
+                        double alpha, double eps_l, const void* tau_damp, void* ws, size_t ws_bytes, void* stream) {
+  if (!c || !in || !out_bar || !in_bar || !tau_damp || ns < 1 || !(alpha >= 0.0 && alpha <= 1.0) || !(eps_l >= 0.0))
+    return SISL_ERR_ARG;
+  const void* need_in[] = {in->u, in->v, in->w, in->eta_dot, in->pi_p, in->th_p};
+  const void* need_bar[] = {in_bar->u, in_bar->v, in_bar->w, in_bar->eta_dot, in_bar->pi_p, in_bar->th_p};
+  const void* obar[] = {out_bar->u, out_bar->v, out_bar->w, out_bar->eta_dot, out_bar->pi_p, out_bar->th_p};
+  for (const void* p : need_in)
+    if (!p) return SISL_ERR_ARG;
+  for (const void* p : need_bar) {
+    if (!p) return SISL_ERR_ARG;
+    for (const void* q : need_in)
+      if (p == q) return SISL_ERR_ARG;  // in_bar must not alias in or out_bar
+    for (const void* q : obar)
+      if (p == q) return SISL_ERR_ARG;
+  }
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_SPLIT_VJP)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (c->grid.dtype == SISL_F64)
+    return split_vjp_impl<double>(c, in, out_bar, in_bar, ns, alpha, eps_l, (const double*)tau_damp, ws, ws_bytes, st);
+  return split_vjp_impl<float>(c, in, out_bar, in_bar, ns, alpha, eps_l, (const float*)tau_damp, ws, ws_bytes, st);
 }
 
 int sisl_ffsl_advect(SislCore* c, const void* field, const void* u, const void* v, const void* eta, void* out,

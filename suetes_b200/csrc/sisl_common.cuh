@@ -111,6 +111,11 @@ __device__ __forceinline__ void face_pair(int f, int n, int periodic, int& l, in
   if (periodic) { l = n - 1; r = 0; return; }
   if (f == 0) { l = 0; r = 1; } else { l = n - 2; r = n - 1; }
 }
+// periodic or edge-clamped mass index along an axis of n cells
+__device__ __forceinline__ int wrap_or_clamp(int q, int n, int periodic) {
+  if (periodic) return ((q % n) + n) % n;
+  return min(max(q, 0), n - 1);
+}
 // Mass-to-w pair along z (never periodic).
 __device__ __forceinline__ void level_pair(int k, int nz, int& l, int& r) {
   if (k > 0 && k < nz) { l = k - 1; r = k; return; }

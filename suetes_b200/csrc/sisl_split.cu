@@ -53,11 +53,6 @@ __global__ void split_diag_kernel(Dims d, Coef<T> c, const T* __restrict__ u, co
   }
 }
 
-// periodic or edge-clamped mass index along an axis of n cells
-__device__ __forceinline__ int wrap_or_clamp(int q, int n, int periodic) {
-  if (periodic) return ((q % n) + n) % n;
-  return min(max(q, 0), n - 1);
-}
 
 // flux * q_face of the 3rd-order upwind-biased face value (steppers.py:1312-1360)
 template <typename T>

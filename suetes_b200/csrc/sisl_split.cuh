@@ -53,4 +53,54 @@ void launch_split_end(const Dims& d, const SplitArgs<T>& a, int nsteps, T* u, T*
 template <typename T>
 void launch_split_axpy(size_t n, const T* b, T* a, cudaStream_t st);
 
+// ---------------------------------------------------------------------------
+// Reverse sweep (sisl_step_vjp.cu).  Every acoustic sub-step is linear in
+// the state (its matrices are background coefficients), so its transposes
+// need no recorded intermediates; the slow tendencies are re-formed at the
+// recomputed stage-start states.  Scatters go through a fixed-point sink
+// when det_scratch is given (det_scatter_scratch_bytes), so the cotangents
+// are the same bits on every run.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct SplitBar {
+  T *upp, *vpp;              // u'', v'' at the sub-step start (accumulated)
+  const T *upp2, *vpp2;      // u'', v'' after the corrector
+  T *wpp, *ppp;              // w'', pi'' (in place: after -> before)
+  T *uh, *vh, *gx0, *gy0;    // midpoint winds and old pressure gradients
+  T *sfu, *sfv, *sfw, *sfp;  // slow forcings (accumulated)
+  T *uc, *vc, *wc;           // stage-start state (accumulated)
+  T *u0, *v0;                // step start (accumulated: the boundary faces)
+  T *s1, *s2;                // column scratch at mass points
+  const T* tau;              // tau_damp at w levels
+  T dtau, alpha, nu_div;
+};
+// w, eta_dot cotangents of split_diag into w (in place), u, v (accumulated);
+// eta_dot's cotangent is consumed (zeroed)
+template <typename T>
+void launch_split_diag_vjp(const Dims& d, const Coef<T>& c, T* wb, T* eb, T* ub, T* vb, void* det_scratch,
+                           cudaStream_t st);
+// the reverse of one acoustic sub-step: corrector, column, predictor
+template <typename T>
+void launch_split_substep_vjp(const Dims& d, const Coef<T>& c, const SplitBar<T>& b, void* det_scratch,
+                              cudaStream_t st);
+// split_end^T: out6 (u, v, w, eta, pi, th cotangents of the stage state) ->
+// stage-start c6 (accumulated; th into the step start's th0b), u'', v'', w'',
+// pi'' (written) and the th' slow forcing (written, times dtau nsteps)
+template <typename T>
+void launch_split_end_vjp(const Dims& d, const T* const* out6, T* const* c6, T* th0b, T* upp, T* vpp, T* wpp,
+                          T* ppp, T* sfth, T dtns, cudaStream_t st);
+// split_init^T: u'' = u0 - uc, ... (accumulated into the step start s6 and the stage start c6)
+template <typename T>
+void launch_split_init_vjp(const Dims& d, const T* upp, const T* vpp, const T* wpp, const T* ppp, T* const* s6,
+                           T* const* c6, cudaStream_t st);
+// split_slow^T: sf5 -> tend6 (written) and adv4 (accumulated)
+template <typename T>
+void launch_split_slow_vjp(const Dims& d, const T* const* sf5, T* const* tend6, T* const* adv4, void* det_scratch,
+                           cudaStream_t st);
+// split_adv^T at the stage-start state: adv4 -> u, v, w, eta_dot, th' (accumulated)
+template <typename T>
+void launch_split_adv_vjp(const Dims& d, const Coef<T>& c, const T* u, const T* v, const T* w, const T* eta,
+                          const T* th, T eps_l, const T* const* adv4, T* ub, T* vb, T* wb, T* eb, T* thb,
+                          void* det_scratch, cudaStream_t st);
+
 }  // namespace sisl

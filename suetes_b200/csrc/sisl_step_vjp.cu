@@ -824,6 +824,515 @@ __global__ void hyper_src_t_kernel(Dims d, PtrTable<T> s, T* ub, T* vb, T* wb, T
   if (i < nx && j < ny && k < nz) thb[im(d, i, j, k)] += ld(s.p[3], im(d, i, j, k));
 }
 
+// ---------------------------------------------------------------------------
+// split-explicit reverse (SplitExplicitStepper3D, steppers.py:1117-1737, as
+// XLA differentiates it: the padded copies of every centre-to-face stagger
+// carry no cotangent, jnp.sign of the upwind flux has none)
+// ---------------------------------------------------------------------------
+
+// A pointwise write of a reverse kernel that also runs as the max pass of a
+// deterministic scatter: issued only by the pass that adds the sums.
+template <typename T>
+__device__ __forceinline__ void wr(T* p, int i, T v) {
+  if (det_sink<T>().mode != 1) p[i] = v;
+}
+
+// m_w (u_w z_xi_w + v_w z_eta_w) at w level k: cotangent x into the winds
+template <typename T>
+__device__ __forceinline__ void kinematic_adj(const Dims& d, const Coef<T>& c, const WindsAdj<T>& WA, int i, int j,
+                                              int k, T x) {
+  if (x == T(0)) return;
+  const int p = iw(d, i, j, k);
+  const T m = ld(c.mm, h_m(d, i, j)) * x;
+  WA.uw(i, j, k, m * ld(c.zxw, p));
+  WA.vw(i, j, k, m * ld(c.zew, p));
+}
+
+// horizontal divergence of (uc + up, vc + vp) at cell (i, j, k): cotangent x
+template <typename T>
+__device__ __forceinline__ void cell_div_adj(const Dims& d, const Coef<T>& c, T* ucb, T* upb, T* vcb, T* vpb, int i,
+                                             int j, int k, T x) {
+  const T mm = ld(c.mm, h_m(d, i, j));
+  const int u0 = iu(d, i, j, k), v0 = iv(d, i, j, k);
+  const T sx = x * mm / (T)d.dx, sy = x * mm / (T)d.dy;
+  radd(ucb, u0 + 1, sx);
+  radd(upb, u0 + 1, sx);
+  radd(ucb, u0, -sx);
+  radd(upb, u0, -sx);
+  radd(vcb, v0 + d.nx, sy);
+  radd(vpb, v0 + d.nx, sy);
+  radd(vcb, v0, -sy);
+  radd(vpb, v0, -sy);
+}
+// the divergence-damping gradient at u face i / v face j (never a padded face here)
+template <typename T>
+__device__ __forceinline__ void div_grad_x_adj(const Dims& d, const Coef<T>& c, T* ucb, T* upb, T* vcb, T* vpb, int i,
+                                               int j, int k, T x) {
+  if (x == T(0)) return;
+  int l, r;
+  face_pair(i, d.nx, d.px, l, r);
+  const T s = x / (T)d.dx * ld(c.mu, h_u(d, i, j));
+  cell_div_adj(d, c, ucb, upb, vcb, vpb, r, j, k, s);
+  cell_div_adj(d, c, ucb, upb, vcb, vpb, l, j, k, -s);
+}
+template <typename T>
+__device__ __forceinline__ void div_grad_y_adj(const Dims& d, const Coef<T>& c, T* ucb, T* upb, T* vcb, T* vpb, int i,
+                                               int j, int k, T x) {
+  if (x == T(0)) return;
+  int l, r;
+  face_pair(j, d.ny, d.py, l, r);
+  const T s = x / (T)d.dy * ld(c.mv, h_v(d, i, j));
+  cell_div_adj(d, c, ucb, upb, vcb, vpb, i, r, k, s);
+  cell_div_adj(d, c, ucb, upb, vcb, vpb, i, l, k, -s);
+}
+
+// split_diag_kernel^T (steppers.py:1272-1310): one thread per w point
+template <typename T>
+__global__ void __launch_bounds__(256) split_diag_vjp_kernel(Dims d, Coef<T> c, T* wb, T* eb, T* ub, T* vb,
+                                                             DetSink<T> sink) {
+  det_begin(sink);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i < d.nx && j < d.ny && k <= d.nz) {
+    const int p = iw(d, i, j, k);
+    const T w_b = wb[p], e_b = eb[p];
+    if (k == 0 || k == d.nz) {  // the kinematic ground value reads padded winds; the lid is zero
+      wr(wb, p, T(0));
+    } else {
+      const T s = e_b / ld(c.dzw, p);
+      wr(wb, p, w_b + s);
+      const WindsAdj<T> WA{d, c, ub, vb};
+      kinematic_adj(d, c, WA, i, j, k, -s);
+    }
+    wr(eb, p, T(0));
+  }
+  det_end<T>();
+}
+
+// split_correct_kernel^T (steppers.py:1607-1626): one thread per union point
+template <typename T>
+__global__ void __launch_bounds__(256) split_correct_vjp_kernel(Dims d, Coef<T> c, SplitBar<T> b, DetSink<T> sink) {
+  det_begin(sink);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i <= nx && j <= ny && k <= nz) {
+    const T cp = (T)c.s.cp, dtau = b.dtau;
+    const GradAdj<T> GA{d, c, b.ppp};
+    if (j < ny && k < nz) {
+      const int p = iu(d, i, j, k);
+      const T x = b.upp2[p];
+      if (!d.px && (i == 0 || i == nx)) {
+        radd(b.u0, p, x);
+        radd(b.uc, p, -x);
+      } else if (x != T(0)) {
+        const int ie = (d.px && i == nx) ? 0 : i, pe = iu(d, ie, j, k);
+        radd(b.upp, pe, x);
+        radd(b.sfu, pe, dtau * x);
+        const T h = -dtau * T(0.5) * cp * ld(c.thu, pe) * x;
+        radd(b.gx0, pe, h);
+        GA.gx(ie, j, k, h);
+        div_grad_x_adj(d, c, b.uc, b.uh, b.vc, b.vh, ie, j, k, b.nu_div * dtau * x);
+      }
+    }
+    if (i < nx && k < nz) {
+      const int p = iv(d, i, j, k);
+      const T x = b.vpp2[p];
+      if (!d.py && (j == 0 || j == ny)) {
+        radd(b.v0, p, x);
+        radd(b.vc, p, -x);
+      } else if (x != T(0)) {
+        const int je = (d.py && j == ny) ? 0 : j, pe = iv(d, i, je, k);
+        radd(b.vpp, pe, x);
+        radd(b.sfv, pe, dtau * x);
+        const T h = -dtau * T(0.5) * cp * ld(c.thv, pe) * x;
+        radd(b.gy0, pe, h);
+        GA.gy(i, je, k, h);
+        div_grad_y_adj(d, c, b.uc, b.uh, b.vc, b.vh, i, je, k, b.nu_div * dtau * x);
+      }
+    }
+    if (i < nx && j < ny) {  // w'' = (wc + w'') / (1 + dtau tau) - wc at every w level
+      const int p = iw(d, i, j, k);
+      const T x = b.wpp[p];
+      const T f = T(1) / (T(1) + dtau * ld(b.tau, p));
+      wr(b.wpp, p, x * f);
+      radd(b.wc, p, x * (f - T(1)));
+    }
+  }
+  det_end<T>();
+}
+
+// split_column_kernel^T (steppers.py:1584-1605, 1635-1737): one thread per
+// column.  x (the pi'' increment) is the column solve of T x = rhs, so
+// rhs_bar = T^-T x_bar, swept with the transposed bands; the w'' and eta_dot
+// flux terms are re-formed per level on the way down.
+template <typename T>
+__global__ void __launch_bounds__(128) split_column_vjp_kernel(Dims d, Coef<T> c, SplitBar<T> b, T a2cp, T adcp,
+                                                               DetSink<T> sink) {
+  det_begin(sink);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i < nx && j < ny) {
+    const T al = b.alpha, dtau = b.dtau, cp = (T)c.s.cp;
+    const T mm = ld(c.mm, h_m(d, i, j));
+    const T dx = (T)d.dx, dy = (T)d.dy;
+    const GradAdj<T> GA{d, c, b.ppp};
+    const WindsAdj<T> WA{d, c, b.uh, b.vh};
+    auto gam = [&](int kw) -> T {  // acoustic coupling at w level kw (zero at the ground and lid)
+      if (kw <= 0 || kw >= nz) return T(0);
+      const int pw = iw(d, i, j, kw);
+      const T thw = ld(c.thw, pw);
+      return a2cp * thw * ld(c.rhow, pw) * thw / ld(c.dzw, pw);
+    };
+    auto wcoef = [&](int kw) -> T {  // d w''(kw) / d x(kw) = -adcp thw / dz_w (interior levels)
+      if (kw <= 0 || kw >= nz) return T(0);
+      const int pw = iw(d, i, j, kw);
+      return adcp * ld(c.thw, pw) * ld(c.idzw, pw);
+    };
+    // upward: x_bar(k) and the forward sweep of T^T r = x_bar
+    T cprev = T(0), dprev = T(0), g_lo = T(0), g_hi = gam(1);
+    for (int k = 0; k < nz; ++k) {
+      const int p = im(d, i, j, k);
+      T xb = b.ppp[p];
+      if (k >= 1) xb -= wcoef(k) * b.wpp[iw(d, i, j, k)];
+      if (k + 1 <= nz - 1) xb += wcoef(k + 1) * b.wpp[iw(d, i, j, k + 1)];
+      const T cpidz = ld(c.cpidz, p);
+      const T mainv = T(1) + cpidz * (g_lo + g_hi);  // 1 - lower - upper
+      const T sub = (k >= 1) ? -ld(c.cpidz, p - nx * ny) * g_lo : T(0);  // upper(k - 1)
+      const T g_next = gam(k + 2);
+      const T sup = (k + 1 < nz) ? -ld(c.cpidz, p + nx * ny) * g_hi : T(0);  // lower(k + 1)
+      const T inv = T(1) / (mainv - sub * cprev);
+      const T cpk = sup * inv, dpk = (xb - sub * dprev) * inv;
+      b.s1[p] = cpk;
+      b.s2[p] = dpk;
+      cprev = cpk;
+      dprev = dpk;
+      g_lo = g_hi;
+      g_hi = g_next;
+    }
+    // downward: r(k), then the cotangents of level k and of w level k + 1
+    T rh = T(0), dh_hi = T(0);  // r(k + 1) and the div_z weight of level k + 1
+    for (int k = nz - 1; k >= 0; --k) {
+      const int p = im(d, i, j, k);
+      const T r = (k == nz - 1) ? b.s2[p] : b.s2[p] - b.s1[p] * rh;
+      radd(b.sfp, p, dtau * r);
+      const T cpidz = ld(c.cpidz, p), dzm = ld(c.dzm, p);
+      const T dh = -dtau * cpidz * dzm * r;  // cotangent of div_h + div_z
+      // div_h = m (dFx/dx m / dz_m + dFy/dy m / dz_m), F = u_h rdu thu, v_h rdv thv
+      const T e = dh * mm * mm / dzm;
+      const int u0 = iu(d, i, j, k), v0 = iv(d, i, j, k);
+      radd(b.uh, u0 + 1, e / dx * ld(c.rdu, u0 + 1) * ld(c.thu, u0 + 1));
+      radd(b.uh, u0, -e / dx * ld(c.rdu, u0) * ld(c.thu, u0));
+      radd(b.vh, v0 + nx, e / dy * ld(c.rdv, v0 + nx) * ld(c.thv, v0 + nx));
+      radd(b.vh, v0, -e / dy * ld(c.rdv, v0) * ld(c.thv, v0));
+      const T fz_w = dh / dzm;  // div_z = (fz(k + 1) - fz(k)) / dz_m
+      if (k + 1 <= nz - 1) {    // w level k + 1: fz_bar = fz_w(k) - fz_w(k + 1)
+        const int kw = k + 1, pw = iw(d, i, j, kw);
+        const T thw = ld(c.thw, pw), rw = ld(c.rhow, pw);
+        const T q = (fz_w - dh_hi) * rw * thw;  // cotangent of w_av - kinematic
+        kinematic_adj(d, c, WA, i, j, kw, -q);
+        const T wex_b = al * q + b.wpp[pw];
+        const T wold_b = (T(1) - al) * q + wex_b;
+        radd(b.sfw, pw, dtau * wex_b);
+        GA.gzw(i, j, kw, -dtau * cp * thw * wex_b);
+        wr(b.wpp, pw, wold_b);
+      }
+      rh = r;
+      dh_hi = fz_w;
+    }
+    // the ground value is the kinematic one of padded winds and the lid is
+    // zero: w'' there carries no cotangent back
+    wr(b.wpp, iw(d, i, j, 0), T(0));
+    wr(b.wpp, iw(d, i, j, nz), T(0));
+  }
+  det_end<T>();
+}
+
+// split_predict_kernel^T (steppers.py:1561-1579): one thread per union point
+template <typename T>
+__global__ void __launch_bounds__(256) split_predict_vjp_kernel(Dims d, Coef<T> c, SplitBar<T> b, DetSink<T> sink) {
+  det_begin(sink);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i <= nx && j <= ny && k < nz) {
+    const T cp = (T)c.s.cp, hdt = T(0.5) * b.dtau;
+    const GradAdj<T> GA{d, c, b.ppp};
+    if (j < ny) {
+      const int p = iu(d, i, j, k);
+      const int ie = (d.px && i == nx) ? 0 : i, pe = iu(d, ie, j, k);
+      const T x = b.uh[p];
+      T g0 = b.gx0[p];
+      if (!d.px && (i == 0 || i == nx)) {
+        radd(b.u0, p, x);
+        radd(b.uc, p, -x);
+      } else if (x != T(0)) {
+        radd(b.upp, pe, x);
+        radd(b.sfu, pe, hdt * x);
+        g0 -= hdt * cp * ld(c.thu, pe) * x;
+        div_grad_x_adj(d, c, b.uc, b.upp, b.vc, b.vpp, ie, j, k, b.nu_div * hdt * x);
+      }
+      if (g0 != T(0)) GA.gx(ie, j, k, g0);
+    }
+    if (i < nx) {
+      const int p = iv(d, i, j, k);
+      const int je = (d.py && j == ny) ? 0 : j, pe = iv(d, i, je, k);
+      const T x = b.vh[p];
+      T g0 = b.gy0[p];
+      if (!d.py && (j == 0 || j == ny)) {
+        radd(b.v0, p, x);
+        radd(b.vc, p, -x);
+      } else if (x != T(0)) {
+        radd(b.vpp, pe, x);
+        radd(b.sfv, pe, hdt * x);
+        g0 -= hdt * cp * ld(c.thv, pe) * x;
+        div_grad_y_adj(d, c, b.uc, b.upp, b.vc, b.vpp, i, je, k, b.nu_div * hdt * x);
+      }
+      if (g0 != T(0)) GA.gy(i, je, k, g0);
+    }
+  }
+  det_end<T>();
+}
+
+// split_end_kernel^T: pointwise
+template <typename T>
+__global__ void split_end_vjp_kernel(Dims d, PtrTable<T> o, PtrTable<T> cb, T* th0b, T* upp, T* vpp, T* wpp, T* ppp,
+                                     T* sfth, T dtns) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i > nx || j > ny || k > nz) return;
+  if (j < ny && k < nz) {
+    const int p = iu(d, i, j, k);
+    const T x = o.p[0][p];
+    cb.p[0][p] += x;
+    upp[p] = x;
+  }
+  if (i < nx && k < nz) {
+    const int p = iv(d, i, j, k);
+    const T x = o.p[1][p];
+    cb.p[1][p] += x;
+    vpp[p] = x;
+  }
+  if (i < nx && j < ny) {
+    const int p = iw(d, i, j, k);
+    const T x = o.p[2][p];
+    cb.p[2][p] += x;
+    wpp[p] = x;
+    cb.p[3][p] += o.p[3][p];  // eta_dot of the stage start
+    if (k < nz) {
+      const T y = o.p[4][p], z = o.p[5][p];
+      cb.p[4][p] += y;
+      ppp[p] = y;
+      th0b[p] += z;
+      sfth[p] = dtns * z;
+    }
+  }
+}
+
+// split_init_kernel^T: u'' = u0 - uc, v'' = v0 - vc, w'' = w0 - wc, pi'' = p0 - pc
+template <typename T>
+__global__ void split_init_vjp_kernel(Dims d, const T* __restrict__ upp, const T* __restrict__ vpp,
+                                      const T* __restrict__ wpp, const T* __restrict__ ppp, PtrTable<T> s,
+                                      PtrTable<T> cb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i > nx || j > ny || k > nz) return;
+  if (j < ny && k < nz) {
+    const int p = iu(d, i, j, k);
+    s.p[0][p] += upp[p];
+    cb.p[0][p] -= upp[p];
+  }
+  if (i < nx && k < nz) {
+    const int p = iv(d, i, j, k);
+    s.p[1][p] += vpp[p];
+    cb.p[1][p] -= vpp[p];
+  }
+  if (i < nx && j < ny) {
+    const int p = iw(d, i, j, k);
+    s.p[2][p] += wpp[p];
+    cb.p[2][p] -= wpp[p];
+    if (k < nz) {
+      s.p[4][p] += ppp[p];
+      cb.p[4][p] -= ppp[p];
+    }
+  }
+}
+
+// split_slow_kernel^T: sf (u, v, w, pi, th) -> tend (u, v, w, pi, th, nl_pi)
+// written; the advection of th', u_m, v_m, w_m accumulated (the padded
+// face and level copies of the averages carry no cotangent)
+template <typename T>
+__global__ void __launch_bounds__(256) split_slow_vjp_kernel(Dims d, PtrTable<T> sf, PtrTable<T> t, PtrTable<T> a,
+                                                             DetSink<T> sink) {
+  det_begin(sink);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i <= nx && j <= ny && k <= nz) {
+    if (j < ny && k < nz) {
+      const int p = iu(d, i, j, k);
+      const T x = sf.p[0][p];
+      wr(t.p[0], p, x);
+      avg_mu_adj(d, a.p[1], i, j, k, x);
+    }
+    if (i < nx && k < nz) {
+      const int p = iv(d, i, j, k);
+      const T x = sf.p[1][p];
+      wr(t.p[1], p, x);
+      avg_mv_adj(d, a.p[2], i, j, k, x);
+    }
+    if (i < nx && j < ny) {
+      const int p = iw(d, i, j, k);
+      const T x = sf.p[2][p];
+      wr(t.p[2], p, x);
+      avg_mw_adj(d, a.p[3], i, j, k, x);
+      if (k < nz) {
+        const T y = sf.p[3][p], z = sf.p[4][p];
+        wr(t.p[3], p, y);
+        wr(t.p[5], p, y);
+        wr(t.p[4], p, z);
+        radd(a.p[0], p, z);
+      }
+    }
+  }
+  det_end<T>();
+}
+
+// cotangent g of F (q4 + sg qb), the 3rd-order upwind-biased face flux
+template <typename T>
+__device__ __forceinline__ void upwind_flux_adj(T qm2, T qm1, T q0, T qp1, T F, T eps_l, T g, T& bm2, T& bm1, T& b0,
+                                                T& bp1, T& bF) {
+  const T q4 = T(7.0 / 12.0) * (q0 + qm1) - T(1.0 / 12.0) * (qp1 + qm2);
+  const T qb = T(1.0 / 12.0) * ((qp1 - qm2) - T(3) * (q0 - qm1));
+  const T cf = (fabs(F) < eps_l) ? T(0) : F;
+  const T sg = (cf > T(0)) ? T(1) : ((cf < T(0)) ? T(-1) : T(0));
+  bF += g * (q4 + sg * qb);
+  const T t4 = g * F, tb = g * F * sg;
+  b0 += T(7.0 / 12.0) * t4 - T(3.0 / 12.0) * tb;
+  bm1 += T(7.0 / 12.0) * t4 + T(3.0 / 12.0) * tb;
+  bp1 += -T(1.0 / 12.0) * t4 + T(1.0 / 12.0) * tb;
+  bm2 += -T(1.0 / 12.0) * t4 - T(1.0 / 12.0) * tb;
+}
+
+// split_adv_kernel^T (steppers.py:1312-1465): one thread per mass point
+template <typename T>
+__global__ void __launch_bounds__(256) split_adv_vjp_kernel(Dims d, Coef<T> c, const T* __restrict__ u,
+                                                            const T* __restrict__ v, const T* __restrict__ w,
+                                                            const T* __restrict__ eta, const T* __restrict__ th,
+                                                            T eps_l, PtrTable<T> ab, T* ub, T* vb, T* wb, T* eb,
+                                                            T* thb, DetSink<T> sink) {
+  det_begin(sink);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  if (i < nx && j < ny && k < nz) {
+    auto at = [&](int f, int a, int bq, int cz) -> T {  // the advected fields, as AdvFields::at
+      switch (f) {
+        case 0: return ld(th, im(d, a, bq, cz));
+        case 1: return T(0.5) * (ld(u, iu(d, a, bq, cz)) + ld(u, iu(d, a + 1, bq, cz)));
+        case 2: return T(0.5) * (ld(v, iv(d, a, bq, cz)) + ld(v, iv(d, a, bq + 1, cz)));
+        default: return T(0.5) * (ld(w, iw(d, a, bq, cz)) + ld(w, iw(d, a, bq, cz + 1)));
+      }
+    };
+    auto to = [&](int f, int a, int bq, int cz, T x) {  // cotangent x of at(f, a, bq, cz)
+      if (x == T(0)) return;
+      switch (f) {
+        case 0: radd(thb, im(d, a, bq, cz), x); break;
+        case 1:
+          radd(ub, iu(d, a, bq, cz), T(0.5) * x);
+          radd(ub, iu(d, a + 1, bq, cz), T(0.5) * x);
+          break;
+        case 2:
+          radd(vb, iv(d, a, bq, cz), T(0.5) * x);
+          radd(vb, iv(d, a, bq + 1, cz), T(0.5) * x);
+          break;
+        default:
+          radd(wb, iw(d, a, bq, cz), T(0.5) * x);
+          radd(wb, iw(d, a, bq, cz + 1), T(0.5) * x);
+          break;
+      }
+    };
+    const T mm = ld(c.mm, h_m(d, i, j));
+    const T dx = (T)d.dx, dy = (T)d.dy;
+    const T mu0 = ld(c.mu, h_u(d, i, j)), mu1 = ld(c.mu, h_u(d, i + 1, j));
+    const T mv0 = ld(c.mv, h_v(d, i, j)), mv1 = ld(c.mv, h_v(d, i, j + 1));
+    const T dz0 = ld(c.dzw, iw(d, i, j, k)), dz1 = ld(c.dzw, iw(d, i, j, k + 1));
+    const T U0 = ld(u, iu(d, i, j, k)) / mu0, U1 = ld(u, iu(d, i + 1, j, k)) / mu1;
+    const T V0 = ld(v, iv(d, i, j, k)) / mv0, V1 = ld(v, iv(d, i, j + 1, k)) / mv1;
+    const T W0 = ld(eta, iw(d, i, j, k)) * dz0, W1 = ld(eta, iw(d, i, j, k + 1)) * dz1;
+    const T dzm = ld(c.dzm, im(d, i, j, k));
+    const T zfac = (T)d.dz / dzm;
+    const T dU = (U1 - U0) / dx * mm, dV = (V1 - V0) / dy * mm;
+    const T dW = (W1 - W0) / (T)d.dz * zfac;
+    int xi[5], yj[5], zk[5];
+#pragma unroll
+    for (int o = 0; o < 5; ++o) {
+      xi[o] = wrap_or_clamp(i - 2 + o, nx, d.px);
+      yj[o] = wrap_or_clamp(j - 2 + o, ny, d.py);
+      zk[o] = min(max(k - 2 + o, 0), nz - 1);
+    }
+    T U0b = T(0), U1b = T(0), V0b = T(0), V1b = T(0), W0b = T(0), W1b = T(0), dUb = T(0), dVb = T(0), dWb = T(0);
+    const int p = im(d, i, j, k);
+#pragma unroll 1
+    for (int f = 0; f < 4; ++f) {
+      const T o = ab.p[f][p];
+      if (o == T(0)) continue;
+      T qx[5], qy[5], qz[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        qx[q] = at(f, xi[q], j, k);
+        qy[q] = at(f, i, yj[q], k);
+        qz[q] = at(f, i, j, zk[q]);
+      }
+      const T q = qx[2];
+      // out = -(m^2)(ax - q dU + ay - q dV) - (az - q dW)
+      const T axb = -(mm * mm) * o, azb = -o;
+      T bx[5] = {T(0), T(0), T(0), T(0), T(0)}, by[5] = {T(0), T(0), T(0), T(0), T(0)},
+        bz[5] = {T(0), T(0), T(0), T(0), T(0)};
+      bx[2] += (mm * mm) * (dU + dV) * o + dW * o;
+      dUb += (mm * mm) * q * o;
+      dVb += (mm * mm) * q * o;
+      dWb += q * o;
+      const T gx = axb / dx * mm, gy = axb / dy * mm, gz = azb / (T)d.dz * zfac;
+      upwind_flux_adj(qx[1], qx[2], qx[3], qx[4], U1, eps_l, gx, bx[1], bx[2], bx[3], bx[4], U1b);
+      upwind_flux_adj(qx[0], qx[1], qx[2], qx[3], U0, eps_l, -gx, bx[0], bx[1], bx[2], bx[3], U0b);
+      upwind_flux_adj(qy[1], qy[2], qy[3], qy[4], V1, eps_l, gy, by[1], by[2], by[3], by[4], V1b);
+      upwind_flux_adj(qy[0], qy[1], qy[2], qy[3], V0, eps_l, -gy, by[0], by[1], by[2], by[3], V0b);
+      upwind_flux_adj(qz[1], qz[2], qz[3], qz[4], W1, eps_l, gz, bz[1], bz[2], bz[3], bz[4], W1b);
+      upwind_flux_adj(qz[0], qz[1], qz[2], qz[3], W0, eps_l, -gz, bz[0], bz[1], bz[2], bz[3], W0b);
+#pragma unroll
+      for (int q2 = 0; q2 < 5; ++q2) {
+        to(f, xi[q2], j, k, bx[q2]);
+        to(f, i, yj[q2], k, by[q2]);
+        to(f, i, j, zk[q2], bz[q2]);
+      }
+    }
+    U1b += dUb / dx * mm;
+    U0b -= dUb / dx * mm;
+    V1b += dVb / dy * mm;
+    V0b -= dVb / dy * mm;
+    W1b += dWb / (T)d.dz * zfac;
+    W0b -= dWb / (T)d.dz * zfac;
+    if (U0b != T(0)) radd(ub, iu(d, i, j, k), U0b / mu0);
+    if (U1b != T(0)) radd(ub, iu(d, i + 1, j, k), U1b / mu1);
+    if (V0b != T(0)) radd(vb, iv(d, i, j, k), V0b / mv0);
+    if (V1b != T(0)) radd(vb, iv(d, i, j + 1, k), V1b / mv1);
+    if (W0b != T(0)) radd(eb, iw(d, i, j, k), W0b * dz0);
+    if (W1b != T(0)) radd(eb, iw(d, i, j, k + 1), W1b * dz1);
+  }
+  det_end<T>();
+}
+
 }  // namespace
 
 size_t det_scatter_scratch_bytes(const Dims& d, int elem_bytes) {
@@ -939,6 +1448,124 @@ void launch_hyper_vjp(const Dims& d, const Coef<T>& c, PtrTable<T> hyp_bar, PtrT
   hyper_src_t_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, hyp_bar, u_bar, v_bar,
                                                                                      w_bar, th_bar);
 }
+
+// ---------------------------------------------------------------------------
+// split-explicit reverse launchers
+// ---------------------------------------------------------------------------
+template <typename T>
+void launch_split_diag_vjp(const Dims& d, const Coef<T>& c, T* wb, T* eb, T* ub, T* vb, void* det_scratch,
+                           cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  T* dst[2] = {ub, vb};
+  const unsigned len[2] = {(unsigned)field_size(d, LOC_U), (unsigned)field_size(d, LOC_V)};
+  det_run<T>(det_make<T>(det_scratch, dst, len, 2), [&](const DetSink<T>& s) {
+    split_diag_vjp_kernel<T><<<box_grid(d.nx, d.ny, d.nz + 1, blk), blk, 0, st>>>(d, c, wb, eb, ub, vb, s);
+  }, st);
+}
+
+template <typename T>
+void launch_split_substep_vjp(const Dims& d, const Coef<T>& c, const SplitBar<T>& b, void* det_scratch,
+                              cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  const unsigned fu = (unsigned)field_size(d, LOC_U), fv = (unsigned)field_size(d, LOC_V);
+  const unsigned fw = (unsigned)field_size(d, LOC_W), fm = (unsigned)field_size(d, LOC_M);
+  {  // corrector^T
+    T* dst[14] = {b.upp, b.vpp, b.sfu, b.sfv, b.gx0, b.gy0, b.ppp, b.uh, b.vh, b.uc, b.vc, b.wc, b.u0, b.v0};
+    const unsigned len[14] = {fu, fv, fu, fv, fu, fv, fm, fu, fv, fu, fv, fw, fu, fv};
+    det_run<T>(det_make<T>(det_scratch, dst, len, 14), [&](const DetSink<T>& s) {
+      split_correct_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, b, s);
+    }, st);
+  }
+  {  // column^T, with the forward's alpha dtau products
+    const double ad = (double)b.alpha * (double)b.dtau;
+    const T a2cp = (T)(ad * ad * c.s.cp), adcp = (T)(ad * c.s.cp);
+    T* dst[5] = {b.ppp, b.uh, b.vh, b.sfw, b.sfp};
+    const unsigned len[5] = {fm, fu, fv, fw, fm};
+    det_run<T>(det_make<T>(det_scratch, dst, len, 5), [&](const DetSink<T>& s) {
+      split_column_vjp_kernel<T><<<dim3((d.nx + 127) / 128, d.ny), 128, 0, st>>>(d, c, b, a2cp, adcp, s);
+    }, st);
+  }
+  {  // predictor^T
+    T* dst[9] = {b.upp, b.vpp, b.sfu, b.sfv, b.ppp, b.uc, b.vc, b.u0, b.v0};
+    const unsigned len[9] = {fu, fv, fu, fv, fm, fu, fv, fu, fv};
+    det_run<T>(det_make<T>(det_scratch, dst, len, 9), [&](const DetSink<T>& s) {
+      split_predict_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz, blk), blk, 0, st>>>(d, c, b, s);
+    }, st);
+  }
+}
+
+template <typename T>
+void launch_split_end_vjp(const Dims& d, const T* const* out6, T* const* c6, T* th0b, T* upp, T* vpp, T* wpp,
+                          T* ppp, T* sfth, T dtns, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  PtrTable<T> o{}, cb{};
+  for (int q = 0; q < 6; ++q) {
+    o.p[q] = const_cast<T*>(out6[q]);
+    cb.p[q] = c6[q];
+  }
+  split_end_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, o, cb, th0b, upp, vpp,
+                                                                                     wpp, ppp, sfth, dtns);
+}
+
+template <typename T>
+void launch_split_init_vjp(const Dims& d, const T* upp, const T* vpp, const T* wpp, const T* ppp, T* const* s6,
+                           T* const* c6, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  PtrTable<T> s{}, cb{};
+  for (int q = 0; q < 6; ++q) {
+    s.p[q] = s6[q];
+    cb.p[q] = c6[q];
+  }
+  split_init_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, upp, vpp, wpp, ppp, s,
+                                                                                      cb);
+}
+
+template <typename T>
+void launch_split_slow_vjp(const Dims& d, const T* const* sf5, T* const* tend6, T* const* adv4, void* det_scratch,
+                           cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  PtrTable<T> sf{}, t{}, a{};
+  for (int q = 0; q < 5; ++q) sf.p[q] = const_cast<T*>(sf5[q]);
+  for (int q = 0; q < 6; ++q) t.p[q] = tend6[q];
+  for (int q = 0; q < 4; ++q) a.p[q] = adv4[q];
+  const unsigned fm = (unsigned)field_size(d, LOC_M);
+  const unsigned len[4] = {fm, fm, fm, fm};
+  det_run<T>(det_make<T>(det_scratch, a.p, len, 4), [&](const DetSink<T>& s) {
+    split_slow_vjp_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, sf, t, a, s);
+  }, st);
+}
+
+template <typename T>
+void launch_split_adv_vjp(const Dims& d, const Coef<T>& c, const T* u, const T* v, const T* w, const T* eta,
+                          const T* th, T eps_l, const T* const* adv4, T* ub, T* vb, T* wb, T* eb, T* thb,
+                          void* det_scratch, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  PtrTable<T> a{};
+  for (int q = 0; q < 4; ++q) a.p[q] = const_cast<T*>(adv4[q]);
+  const unsigned fw = (unsigned)field_size(d, LOC_W), fm = (unsigned)field_size(d, LOC_M);
+  T* dst[5] = {ub, vb, wb, eb, thb};
+  const unsigned len[5] = {(unsigned)field_size(d, LOC_U), (unsigned)field_size(d, LOC_V), fw, fw, fm};
+  det_run<T>(det_make<T>(det_scratch, dst, len, 5), [&](const DetSink<T>& s) {
+    split_adv_vjp_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, c, u, v, w, eta, th, eps_l, a, ub,
+                                                                            vb, wb, eb, thb, s);
+  }, st);
+}
+
+#define SISL_INST_SPLIT_VJP(T)                                                                                 \
+  template void launch_split_diag_vjp<T>(const Dims&, const Coef<T>&, T*, T*, T*, T*, void*, cudaStream_t);    \
+  template void launch_split_substep_vjp<T>(const Dims&, const Coef<T>&, const SplitBar<T>&, void*,            \
+                                            cudaStream_t);                                                     \
+  template void launch_split_end_vjp<T>(const Dims&, const T* const*, T* const*, T*, T*, T*, T*, T*, T*, T,   \
+                                        cudaStream_t);                                                         \
+  template void launch_split_init_vjp<T>(const Dims&, const T*, const T*, const T*, const T*, T* const*,       \
+                                         T* const*, cudaStream_t);                                             \
+  template void launch_split_slow_vjp<T>(const Dims&, const T* const*, T* const*, T* const*, void*,            \
+                                         cudaStream_t);                                                        \
+  template void launch_split_adv_vjp<T>(const Dims&, const Coef<T>&, const T*, const T*, const T*, const T*,   \
+                                        const T*, T, const T* const*, T*, T*, T*, T*, T*, void*, cudaStream_t);
+SISL_INST_SPLIT_VJP(float)
+SISL_INST_SPLIT_VJP(double)
+#undef SISL_INST_SPLIT_VJP
 
 #define SISL_INST_VJP(T)                                                                                       \
   template void launch_explicit_vjp<T>(const Dims&, const Coef<T>&, const ExplicitIn<T>&, const ExplicitBar<T>&, \

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "sisl_explicit.cuh"
+#include "sisl_split.cuh"
 
 namespace sisl {
 

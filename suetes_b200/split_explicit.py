@@ -82,6 +82,27 @@ class SplitExplicitStepper3D:
                                        ws.data_ptr(), n, core.stream), "sisl_split_step")
         return {k: ds_out.t[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p", "rho")}
 
+    def step_vjp_device(self, core, st, out_bar):
+        """Cotangents of ``step_device``'s input fields (u, v, w, eta_dot,
+        pi_p, th_p of the diagnosed state ``st``) from those of its output
+        (``out_bar``: dict of the same names, missing entries zero) through
+        ``sisl_split_step_vjp``: the three RK3 stages differentiated as XLA
+        differentiates the reference's (no physics tendencies)."""
+        from .steppers import DeviceState
+        ds_in = DeviceState(core, st)
+        ob = DeviceState(core, {k: out_bar[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p") if k in out_bar})
+        ib = DeviceState(core)
+        sin, sob, sib = ds_in.c_struct(), ob.c_struct(), ib.c_struct()
+        for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p"):
+            if k not in out_bar:
+                setattr(sob, k, None)
+        ws, n = core.workspace(_lib.WS_SPLIT_VJP)
+        eps_l = float(self.physics.c.get("eps_l", 1e-12))
+        check(core.lib.sisl_split_step_vjp(core.handle, ctypes.byref(sin), ctypes.byref(sob), ctypes.byref(sib),
+                                           int(self.ns), float(self.alpha), eps_l, self._tau_damp(core).data_ptr(),
+                                           ws.data_ptr(), n, core.stream), "sisl_split_step_vjp")
+        return {k: ib.t[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p")}
+
     def step(self, state, t, forcing, bc_fn, ml_params=None):
         """SplitExplicitStepper3D.step (steppers.py:1117-1270).  As in the
         reference, the input dict receives the diagnosed eta_dot and w."""
