@@ -409,6 +409,28 @@ def split_leg(args, local, world, peak, peak_kind):
                                "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
                                "alg_bytes_per_cell_substep": "62 s (predict 16, column 24, correct 22)",
                                "share_of_step": k_ms / ms, "launches_timed": k_n}
+        # the native reverse sweep of the three stages (sisl_split_step_vjp)
+        # at the current state, N(0,1) output cotangents
+        ds = st.device_state(core, s)
+        gen = torch.Generator(device=f"cuda:{local}").manual_seed(11)
+        ob = {k: torch.randn(ds[k].shape, generator=gen, device=ds[k].device, dtype=ds[k].dtype)
+              for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p")}
+        ob = {k: core.field(t, loc) for (k, t), loc in zip(ob.items(), ("u", "v", "w", "w", "m", "m"))}
+        st.step_vjp_device(core, ds, ob)  # warm-up (workspace)
+        torch.cuda.synchronize()
+        barrier(world)
+        l0 = kernel_launches()
+        ev0.record()
+        for n in range(K):
+            gb = st.step_vjp_device(core, ds, ob)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms_v = dist_max(ev0.elapsed_time(ev1), world)
+        out[key]["vjp"] = {"ms_per_step": ms_v / K, "value": world * cells * K / (ms_v / 1e3),
+                           "fwd_vjp_value": world * cells * K / ((ms + ms_v) / 1e3),
+                           "gpu_launches_per_step": (kernel_launches() - l0) / K,
+                           "grad_th_norm": float(torch.linalg.vector_norm(gb["th_p"].double())),
+                           "note": "first two stage states recomputed; fixed-point scatters"}
         del st, s
     out["value"] = out["f32"]["value"]
     if rank_of() == 0 and not args.no_cpu:

@@ -103,6 +103,18 @@ class SplitExplicitStepper3D:
                                            ws.data_ptr(), n, core.stream), "sisl_split_step_vjp")
         return {k: ib.t[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p")}
 
+    def device_state(self, core, state):
+        """The diagnosed device state ``step_device`` and ``step_vjp_device``
+        take (u, v, w, eta_dot, pi_p, th_p, rho in the core's layout) from a
+        reference-style state dict (u, v, w, pi, th_v, rho)."""
+        ph = self.physics
+        f = core.field
+        u, v = f(state["u"], "u"), f(state["v"], "v")
+        eta, w = self._diagnose(core, u, v, f(state["w"], "w"))
+        pi_p = fortran(torch.as_tensor(state["pi"]).to(core.device, F64) - ph.pi_bg, dtype=core.dtype)
+        th_p = fortran(torch.as_tensor(state["th_v"]).to(core.device, F64) - ph.theta_bg, dtype=core.dtype)
+        return {"u": u, "v": v, "w": w, "eta_dot": eta, "pi_p": pi_p, "th_p": th_p, "rho": f(state["rho"], "m")}
+
     def step(self, state, t, forcing, bc_fn, ml_params=None):
         """SplitExplicitStepper3D.step (steppers.py:1117-1270).  As in the
         reference, the input dict receives the diagnosed eta_dot and w."""
