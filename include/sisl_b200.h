@@ -353,6 +353,14 @@ int sisl_split_diagnose(SislCore* core, const void* u, const void* v, const void
                         void* stream);
 int sisl_split_step(SislCore* core, const SislState* in, const SislState* out, int ns, double alpha, double eps_l,
                     const void* tau_damp, const void* const phys_tend[4], void* ws, size_t ws_bytes, void* stream);
+/* Cotangents through sisl_split_diagnose (_diagnose_eta_dot,
+ * steppers.py:1272-1310, as XLA differentiates it: the kinematic ground
+ * value reads padded winds and carries none): from the cotangents of w_out
+ * and eta_out, w_in_bar is written (may equal w_out_bar) and u_bar, v_bar
+ * are accumulated.  ws: sisl_workspace_bytes(core, SISL_WS_SPLIT_VJP)
+ * bytes (scratch of the fixed-point scatter). */
+int sisl_split_diagnose_vjp(SislCore* core, const void* w_out_bar, const void* eta_bar, void* u_bar, void* v_bar,
+                            void* w_in_bar, void* ws, size_t ws_bytes, void* stream);
 /* Cotangent of sisl_split_step's input state from the cotangent of its
  * output (the VJP of SplitExplicitStepper3D's three RK3 stages,
  * steppers.py:1117-1231 and 1272-1737, as XLA differentiates them: the

@@ -142,6 +142,7 @@ PROTOTYPES = {
                                          ctypes.POINTER(SislRelaxation), vp * 4, vp, vp, ctypes.c_size_t, vp,
                                          ctypes.POINTER(SislStepInfo)]),
     "sisl_split_diagnose": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp]),
+    "sisl_split_diagnose_vjp": (ctypes.c_int, [vp, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "sisl_split_step": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState), ctypes.c_int,
                                        ctypes.c_double, ctypes.c_double, vp, vp * 4, vp, ctypes.c_size_t, vp]),
     "sisl_split_step_vjp": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),

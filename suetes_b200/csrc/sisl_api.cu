@@ -2743,6 +2743,30 @@ int sisl_split_diagnose(SislCore* c, const void* u, const void* v, const void* w
   return check_cuda();
 }
 
+int sisl_split_diagnose_vjp(SislCore* c, const void* w_out_bar, const void* eta_bar, void* u_bar, void* v_bar,
+                            void* w_in_bar, void* ws, size_t ws_bytes, void* stream) {
+  if (!c || !w_out_bar || !eta_bar || !u_bar || !v_bar || !w_in_bar) return SISL_ERR_ARG;
+  if (w_in_bar == eta_bar || u_bar == v_bar) return SISL_ERR_ARG;
+  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_SPLIT_VJP)) return SISL_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  auto run = [&](auto tag) -> int {
+    using T = decltype(tag);
+    const Dims& d = c->d;
+    const size_t wb = sizeof(T) * field_size(d, LOC_W);
+    Carver cv{(char*)ws};
+    T* eb = (T*)cv.take(wb);  // the kernel consumes (zeroes) its eta_dot cotangent: work on a copy
+    void* det = cv.take(det_scatter_scratch_bytes(d, (int)sizeof(T)));
+    if (w_in_bar != w_out_bar && cudaMemcpyAsync(w_in_bar, w_out_bar, wb, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return SISL_ERR_CUDA;
+    if (cudaMemcpyAsync(eb, eta_bar, wb, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return SISL_ERR_CUDA;
+    KScope k(c, SISL_K_OTHER, st, 3);
+    launch_split_diag_vjp<T>(d, coef_of<T>(c), (T*)w_in_bar, eb, (T*)u_bar, (T*)v_bar, det, st);
+    return SISL_OK;
+  };
+  const int rc = (c->grid.dtype == SISL_F64) ? run(double{}) : run(float{});
+  return rc ? rc : check_cuda();
+}
+
 int sisl_split_step(SislCore* c, const SislState* in, const SislState* out, int ns, double alpha, double eps_l,
                     const void* tau_damp, const void* const phys_tend[4], void* ws, size_t ws_bytes, void* stream) {
   if (!c || !in || !out || !tau_damp || ns < 1 || !(alpha >= 0.0 && alpha <= 1.0) || !(eps_l >= 0.0))

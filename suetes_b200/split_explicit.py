@@ -103,6 +103,92 @@ class SplitExplicitStepper3D:
                                            ws.data_ptr(), n, core.stream), "sisl_split_step_vjp")
         return {k: ib.t[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p")}
 
+    def step_vjp(self, state, cot, bc_fn=None, forcing=None):
+        """``step`` (without a physics suite) and the cotangents of its input
+        state, as ``jax.vjp`` of SplitExplicitStepper3D.step
+        (steppers.py:1117-1270) gives them.  ``cot``: cotangents of the
+        output's u, v, w, eta_dot, pi, th_v, rho (missing keys zero).
+        Returns ``(new_state, grads)`` with grads for u, v, w, eta_dot, pi,
+        th_v, rho of the input (the input's eta_dot and rho are overwritten
+        by the step's diagnosis and equation of state: zero).
+
+        Native reverse pieces: the output diagnosis^T and the input
+        diagnosis^T (``sisl_split_diagnose_vjp``), the three stages^T
+        (``sisl_split_step_vjp``); the equation of state's derivative
+        (rho/th_v and rho cvd/(Rd pi), elementwise) and a torch ``bc_fn``
+        (autograd) are applied in between on the device."""
+        ph = self.physics
+        if ph.physics_suite is not None:
+            raise NotImplementedError("the split-explicit VJP covers the core without a physics suite")
+        dtype = state["u"].dtype if torch.is_tensor(state["u"]) else F64
+        core = self.core(dtype)
+        f = core.field
+        din = self.device_state(core, state)
+        res = self.step_device(core, din)
+        pi = fortran(res["pi_p"].double() + ph.pi_bg, dtype=dtype)
+        th = fortran(res["th_p"].double() + ph.theta_bg, dtype=dtype)
+        pre = {"u": res["u"], "v": res["v"], "w": res["w"], "eta_dot": res["eta_dot"], "pi": pi, "th_v": th,
+               "rho": din["rho"]}
+        # bc_fn on the stage output, recorded for its cotangents
+        if bc_fn is not None:
+            leaves = {k: t.detach().clone().requires_grad_(True) for k, t in pre.items()}
+            with torch.enable_grad():
+                post = bc_fn(dict(leaves), forcing)
+            post_d = {k: (post[k].detach() if torch.is_tensor(post[k]) else post[k]) for k in pre}
+        else:
+            leaves, post, post_d = None, None, dict(pre)
+        u1, v1 = f(post_d["u"], "u"), f(post_d["v"], "v")
+        eta2, w2 = self._diagnose(core, u1, v1, f(post_d["w"], "w"))
+        rho2 = self._eos(core, post_d["th_v"], post_d["pi"])
+        out = dict(state)
+        out.pop("_sisl_state", None)
+        out.update({"u": u1, "v": v1, "w": w2, "eta_dot": eta2, "pi": f(post_d["pi"], "m"),
+                    "th_v": f(post_d["th_v"], "m"), "rho": rho2})
+        locs = {"u": "u", "v": "v", "w": "w", "eta_dot": "w", "pi": "m", "th_v": "m", "rho": "m"}
+
+        def cz(k):
+            t = cot.get(k)
+            return f(t, locs[k]).clone() if t is not None else torch.zeros_like(f(pre[k], locs[k]))
+
+        # equation of state: rho = p0 / (Rd th_v) pi^(cvd/Rd)
+        c = ph.c
+        rb = cz("rho")
+        g = {k: cz(k) for k in ("u", "v", "pi", "th_v")}
+        g["th_v"] = g["th_v"] - rb * rho2 / out["th_v"]
+        g["pi"] = g["pi"] + rb * rho2 * (c["cvd"] / c["Rd"]) / out["pi"]
+        # the final diagnosis: (w, eta_dot) of the bc output -> its w, u, v
+        ws, nb = core.workspace(_lib.WS_SPLIT_VJP)
+        wb = core.new("w")
+        w_bar, e_bar = cz("w"), cz("eta_dot")  # held: a temporary's memory could be handed to the next one
+        check(core.lib.sisl_split_diagnose_vjp(core.handle, w_bar.data_ptr(), e_bar.data_ptr(), g["u"].data_ptr(),
+                                               g["v"].data_ptr(), wb.data_ptr(), ws.data_ptr(), nb, core.stream),
+              "sisl_split_diagnose_vjp")
+        g["w"] = wb
+        g["eta_dot"] = torch.zeros_like(wb)
+        g["rho"] = torch.zeros_like(rb)
+        # bc_fn^T
+        if leaves is not None:
+            outs, gs = [], []
+            for k in pre:
+                if torch.is_tensor(post.get(k)) and post[k].requires_grad:
+                    outs.append(post[k])
+                    gs.append(g[k].to(post[k].dtype).reshape(post[k].shape))
+            grads = torch.autograd.grad(outs, [leaves[k] for k in pre], gs, allow_unused=True) if outs else []
+            g = {k: (f(gk, locs[k]) if gk is not None else torch.zeros_like(f(pre[k], locs[k])))
+                 for k, gk in zip(pre, grads)} if outs else {k: torch.zeros_like(f(pre[k], locs[k])) for k in pre}
+        # the three stages
+        ob = {"u": g["u"], "v": g["v"], "w": g["w"], "eta_dot": g["eta_dot"], "pi_p": g["pi"], "th_p": g["th_v"]}
+        ib = self.step_vjp_device(core, din, ob)
+        # the input diagnosis: (w, eta_dot) of the diagnosed input -> the input's w, u, v
+        gu, gv = ib["u"].clone(), ib["v"].clone()
+        gw = core.new("w")
+        check(core.lib.sisl_split_diagnose_vjp(core.handle, ib["w"].data_ptr(), ib["eta_dot"].data_ptr(),
+                                               gu.data_ptr(), gv.data_ptr(), gw.data_ptr(), ws.data_ptr(), nb,
+                                               core.stream), "sisl_split_diagnose_vjp")
+        grads = {"u": gu, "v": gv, "w": gw, "eta_dot": torch.zeros_like(gw), "pi": ib["pi_p"], "th_v": ib["th_p"],
+                 "rho": g["rho"] if leaves is None else g.get("rho", torch.zeros_like(rb))}
+        return out, grads
+
     def device_state(self, core, state):
         """The diagnosed device state ``step_device`` and ``step_vjp_device``
         take (u, v, w, eta_dot, pi_p, th_p, rho in the core's layout) from a
