@@ -430,7 +430,22 @@ def split_leg(args, local, world, peak, peak_kind):
                            "fwd_vjp_value": world * cells * K / ((ms + ms_v) / 1e3),
                            "gpu_launches_per_step": (kernel_launches() - l0) / K,
                            "grad_th_norm": float(torch.linalg.vector_norm(gb["th_p"].double())),
-                           "note": "first two stage states recomputed; fixed-point scatters"}
+                           "note": "first two stage states recomputed; fixed-point scatters (bitwise repeatable)"}
+        st.step_vjp_device(core, ds, ob, deterministic=False)
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0.record()
+        for n in range(K):
+            ga = st.step_vjp_device(core, ds, ob, deterministic=False)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms_a = dist_max(ev0.elapsed_time(ev1), world)
+        out[key]["vjp_atomic"] = {
+            "ms_per_step": ms_a / K, "value": world * cells * K / (ms_a / 1e3),
+            "fwd_vjp_value": world * cells * K / ((ms + ms_a) / 1e3),
+            "grad_th_rel_vs_deterministic": float(torch.linalg.vector_norm((ga["th_p"] - gb["th_p"]).double())
+                                                  / torch.linalg.vector_norm(gb["th_p"].double())),
+            "note": "float atomic scatters (order-dependent last bits)"}
         del st, s
     out["value"] = out["f32"]["value"]
     if rank_of() == 0 and not args.no_cpu:

@@ -370,12 +370,14 @@ int sisl_split_diagnose_vjp(SislCore* core, const void* w_out_bar, const void* e
  * eta_dot, pi_p, th_p (NULL members zero); in_bar receives the cotangents
  * of the same input fields and must not alias in or out_bar.  The first two
  * stage states are recomputed; the acoustic sub-steps are linear, so their
- * transposes need no recorded intermediates.  Every scatter sums in fixed
- * point: the same bits on every run.  ws: sisl_workspace_bytes(core,
+ * transposes need no recorded intermediates.  deterministic = 1: every
+ * scatter sums in fixed point (the same bits on every run, two passes per
+ * scatter kernel); 0: float atomic adds (one pass; the last bits depend on
+ * the order the adds land).  ws: sisl_workspace_bytes(core,
  * SISL_WS_SPLIT_VJP) bytes. */
 int sisl_split_step_vjp(SislCore* core, const SislState* in, const SislState* out_bar, const SislState* in_bar,
-                        int ns, double alpha, double eps_l, const void* tau_damp, void* ws, size_t ws_bytes,
-                        void* stream);
+                        int ns, double alpha, double eps_l, const void* tau_damp, int deterministic, void* ws,
+                        size_t ws_bytes, void* stream);
 /* Cotangent of one step's input state from the cotangent of its output
  * (the VJP of SISLStepper3D.step under jax.checkpoint, steppers.py:720-1073,
  * 792-850, with the reference's stop_gradient on the departure points and

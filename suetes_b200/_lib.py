@@ -147,7 +147,7 @@ PROTOTYPES = {
                                        ctypes.c_double, ctypes.c_double, vp, vp * 4, vp, ctypes.c_size_t, vp]),
     "sisl_split_step_vjp": (ctypes.c_int, [vp, ctypes.POINTER(SislState), ctypes.POINTER(SislState),
                                            ctypes.POINTER(SislState), ctypes.c_int, ctypes.c_double, ctypes.c_double,
-                                           vp, vp, ctypes.c_size_t, vp]),
+                                           vp, ctypes.c_int, vp, ctypes.c_size_t, vp]),
     "sisl_step_vjp": (ctypes.c_int, [vp, ctypes.POINTER(SislState), vp * 10, ctypes.POINTER(SislRelaxation),
                                      ctypes.POINTER(SislState), ctypes.POINTER(SislState), vp, ctypes.c_size_t, vp,
                                      ctypes.POINTER(SislStepInfo)]),

@@ -1374,7 +1374,7 @@ void carve_split_vjp(Carver& cv, const Dims& d, SplitVjpWork<T>& b) {
 // hyperdiffusion^T of the stage and, at the end, of the step start.
 template <typename T>
 int split_vjp_impl(SislCore* c, const SislState* in, const SislState* ob, const SislState* ib, int ns, double alpha,
-                   double eps_l, const T* tau, void* ws, size_t ws_bytes, cudaStream_t st) {
+                   double eps_l, const T* tau, int deterministic, void* ws, size_t ws_bytes, cudaStream_t st) {
   const Dims& d = c->d;
   const Coef<T> cf = coef_of<T>(c);
   Carver cv{(char*)ws};
@@ -1383,6 +1383,7 @@ int split_vjp_impl(SislCore* c, const SislState* in, const SislState* ob, const 
   SplitVjpWork<T> b;
   carve_split_vjp<T>(cv, d, b);
   if (cv.off > ws_bytes) return SISL_ERR_WORKSPACE;
+  if (!deterministic) b.det = nullptr;  // float atomic adds, one pass per scatter kernel
   static const int LOC6[6] = {LOC_U, LOC_V, LOC_W, LOC_W, LOC_M, LOC_M};
   auto bytes = [&](int loc) { return sizeof(T) * field_size(d, loc); };
   auto zero = [&](void* p, int loc) { return cudaMemsetAsync(p, 0, bytes(loc), st) == cudaSuccess; };
@@ -2790,7 +2791,8 @@ int sisl_split_step(SislCore* c, const SislState* in, const SislState* out, int 
 }
 
 int sisl_split_step_vjp(SislCore* c, const SislState* in, const SislState* out_bar, const SislState* in_bar, int ns,
-                        double alpha, double eps_l, const void* tau_damp, void* ws, size_t ws_bytes, void* stream) {
+                        double alpha, double eps_l, const void* tau_damp, int deterministic, void* ws,
+                        size_t ws_bytes, void* stream) {
   if (!c || !in || !out_bar || !in_bar || !tau_damp || ns < 1 || !(alpha >= 0.0 && alpha <= 1.0) || !(eps_l >= 0.0))
     return SISL_ERR_ARG;
   const void* need_in[] = {in->u, in->v, in->w, in->eta_dot, in->pi_p, in->th_p};
@@ -2808,8 +2810,10 @@ int sisl_split_step_vjp(SislCore* c, const SislState* in, const SislState* out_b
   if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_SPLIT_VJP)) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64)
-    return split_vjp_impl<double>(c, in, out_bar, in_bar, ns, alpha, eps_l, (const double*)tau_damp, ws, ws_bytes, st);
-  return split_vjp_impl<float>(c, in, out_bar, in_bar, ns, alpha, eps_l, (const float*)tau_damp, ws, ws_bytes, st);
+    return split_vjp_impl<double>(c, in, out_bar, in_bar, ns, alpha, eps_l, (const double*)tau_damp, deterministic, ws,
+                                  ws_bytes, st);
+  return split_vjp_impl<float>(c, in, out_bar, in_bar, ns, alpha, eps_l, (const float*)tau_damp, deterministic, ws,
+                               ws_bytes, st);
 }
 
 int sisl_ffsl_advect(SislCore* c, const void* field, const void* u, const void* v, const void* eta, void* out,

@@ -1051,6 +1051,115 @@ __global__ void __launch_bounds__(128) split_column_vjp_kernel(Dims d, Coef<T> c
   det_end<T>();
 }
 
+// split_column_vjp_kernel on tiles of PC columns (one block per tile and row
+// j): A forms x_bar and the transposed bands at every (level, column) pair,
+// B one thread per column sweeps T^T r = x_bar in shared memory, C scatters
+// the cotangents of every (level, column) pair.  Arithmetic term for term
+// that of split_column_vjp_kernel, with the scatters spread over the block.
+template <typename T, int PT, int PC>
+__global__ void __launch_bounds__(PT) split_column_vjp_tile_kernel(Dims d, Coef<T> c, SplitBar<T> b, T a2cp, T adcp,
+                                                                   DetSink<T> sink) {
+  det_begin(sink);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  T* s_x = reinterpret_cast<T*>(smem_raw);  // [nz][PC] x_bar -> r
+  T* s_sub = s_x + nz * PC;                  // [nz][PC] upper(k - 1)
+  T* s_sup = s_sub + nz * PC;                // [nz][PC] lower(k + 1) -> c'
+  T* s_mn = s_sup + nz * PC;                 // [nz][PC] main
+  const int i0 = blockIdx.x * PC, j = blockIdx.y, tid = threadIdx.x;
+  const T al = b.alpha, dtau = b.dtau, cp = (T)c.s.cp;
+  const T dx = (T)d.dx, dy = (T)d.dy;
+  auto gam = [&](int i, int kw) -> T {
+    if (kw <= 0 || kw >= nz) return T(0);
+    const int pw = iw(d, i, j, kw);
+    const T thw = ld(c.thw, pw);
+    return a2cp * thw * ld(c.rhow, pw) * thw / ld(c.dzw, pw);
+  };
+  auto wcoef = [&](int i, int kw) -> T {
+    if (kw <= 0 || kw >= nz) return T(0);
+    const int pw = iw(d, i, j, kw);
+    return adcp * ld(c.thw, pw) * ld(c.idzw, pw);
+  };
+  for (int q = tid; q < nz * PC; q += PT) {  // A
+    const int k = q / PC, i = i0 + q % PC;
+    if (i >= nx) {
+      s_x[q] = T(0);
+      s_sub[q] = T(0);
+      s_sup[q] = T(0);
+      s_mn[q] = T(1);
+      continue;
+    }
+    const int p = im(d, i, j, k);
+    T xb = b.ppp[p];
+    if (k >= 1) xb -= wcoef(i, k) * b.wpp[iw(d, i, j, k)];
+    if (k + 1 <= nz - 1) xb += wcoef(i, k + 1) * b.wpp[iw(d, i, j, k + 1)];
+    s_x[q] = xb;
+    const T g_lo = gam(i, k), g_hi = gam(i, k + 1);
+    s_mn[q] = T(1) + ld(c.cpidz, p) * (g_lo + g_hi);
+    s_sub[q] = (k >= 1) ? -ld(c.cpidz, p - nx * ny) * g_lo : T(0);
+    s_sup[q] = (k + 1 < nz) ? -ld(c.cpidz, p + nx * ny) * g_hi : T(0);
+  }
+  __syncthreads();
+  if (tid < PC) {  // B
+    T cprev = T(0), dprev = T(0);
+    for (int k = 0; k < nz; ++k) {
+      const int q = k * PC + tid;
+      const T sub = s_sub[q];
+      const T inv = T(1) / (s_mn[q] - sub * cprev);
+      const T cpk = s_sup[q] * inv, dpk = (s_x[q] - sub * dprev) * inv;
+      s_sup[q] = cpk;
+      s_x[q] = dpk;
+      cprev = cpk;
+      dprev = dpk;
+    }
+    T rh = dprev;
+    for (int k = nz - 2; k >= 0; --k) {
+      const int q = k * PC + tid;
+      rh = s_x[q] - s_sup[q] * rh;
+      s_x[q] = rh;
+    }
+  }
+  __syncthreads();
+  const GradAdj<T> GA{d, c, b.ppp};
+  const WindsAdj<T> WA{d, c, b.uh, b.vh};
+  for (int q = tid; q < (nz + 1) * PC; q += PT) {  // C: level k (< nz) and w level k + 1
+    const int k = q / PC, i = i0 + q % PC;
+    if (i >= nx) continue;
+    if (k == nz) {  // ground and lid: no cotangent back through w''
+      wr(b.wpp, iw(d, i, j, 0), T(0));
+      wr(b.wpp, iw(d, i, j, nz), T(0));
+      continue;
+    }
+    const int p = im(d, i, j, k);
+    const T r = s_x[q];
+    radd(b.sfp, p, dtau * r);
+    const T cpidz = ld(c.cpidz, p), dzm = ld(c.dzm, p);
+    const T dh = -dtau * cpidz * dzm * r;
+    const T mm = ld(c.mm, h_m(d, i, j));
+    const T e = dh * mm * mm / dzm;
+    const int u0 = iu(d, i, j, k), v0 = iv(d, i, j, k);
+    radd(b.uh, u0 + 1, e / dx * ld(c.rdu, u0 + 1) * ld(c.thu, u0 + 1));
+    radd(b.uh, u0, -e / dx * ld(c.rdu, u0) * ld(c.thu, u0));
+    radd(b.vh, v0 + nx, e / dy * ld(c.rdv, v0 + nx) * ld(c.thv, v0 + nx));
+    radd(b.vh, v0, -e / dy * ld(c.rdv, v0) * ld(c.thv, v0));
+    if (k + 1 <= nz - 1) {
+      const int kw = k + 1, pw = iw(d, i, j, kw);
+      const int p1 = p + nx * ny;
+      const T fz_lo = dh / dzm;
+      const T fz_hi = (-dtau * ld(c.cpidz, p1) * ld(c.dzm, p1) * s_x[q + PC]) / ld(c.dzm, p1);
+      const T thw = ld(c.thw, pw), rw = ld(c.rhow, pw);
+      const T qq = (fz_lo - fz_hi) * rw * thw;
+      kinematic_adj(d, c, WA, i, j, kw, -qq);
+      const T wex_b = al * qq + b.wpp[pw];
+      const T wold_b = (T(1) - al) * qq + wex_b;
+      radd(b.sfw, pw, dtau * wex_b);
+      GA.gzw(i, j, kw, -dtau * cp * thw * wex_b);
+      wr(b.wpp, pw, wold_b);
+    }
+  }
+  det_end<T>();
+}
+
 // split_predict_kernel^T (steppers.py:1561-1579): one thread per union point
 template <typename T>
 __global__ void __launch_bounds__(256) split_predict_vjp_kernel(Dims d, Coef<T> c, SplitBar<T> b, DetSink<T> sink) {
@@ -1481,9 +1590,20 @@ void launch_split_substep_vjp(const Dims& d, const Coef<T>& c, const SplitBar<T>
     const T a2cp = (T)(ad * ad * c.s.cp), adcp = (T)(ad * c.s.cp);
     T* dst[5] = {b.ppp, b.uh, b.vh, b.sfw, b.sfp};
     const unsigned len[5] = {fm, fu, fv, fw, fm};
-    det_run<T>(det_make<T>(det_scratch, dst, len, 5), [&](const DetSink<T>& s) {
-      split_column_vjp_kernel<T><<<dim3((d.nx + 127) / 128, d.ny), 128, 0, st>>>(d, c, b, a2cp, adcp, s);
-    }, st);
+    constexpr int PT = 256, PC = 32;
+    const size_t smem = (size_t)(4 * d.nz) * PC * sizeof(T);
+    if (smem <= 200 * 1024) {  // tiles of 32 columns; the one-thread-per-column march beyond
+      static SmemLimit attr_bytes;  // per instantiation
+      ensure_smem_limit((const void*)split_column_vjp_tile_kernel<T, PT, PC>, attr_bytes, smem);
+      det_run<T>(det_make<T>(det_scratch, dst, len, 5), [&](const DetSink<T>& s) {
+        split_column_vjp_tile_kernel<T, PT, PC>
+            <<<dim3((d.nx + PC - 1) / PC, d.ny), PT, smem, st>>>(d, c, b, a2cp, adcp, s);
+      }, st);
+    } else {
+      det_run<T>(det_make<T>(det_scratch, dst, len, 5), [&](const DetSink<T>& s) {
+        split_column_vjp_kernel<T><<<dim3((d.nx + 127) / 128, d.ny), 128, 0, st>>>(d, c, b, a2cp, adcp, s);
+      }, st);
+    }
   }
   {  // predictor^T
     T* dst[9] = {b.upp, b.vpp, b.sfu, b.sfv, b.ppp, b.uc, b.vc, b.u0, b.v0};

@@ -82,12 +82,14 @@ class SplitExplicitStepper3D:
                                        ws.data_ptr(), n, core.stream), "sisl_split_step")
         return {k: ds_out.t[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p", "rho")}
 
-    def step_vjp_device(self, core, st, out_bar):
+    def step_vjp_device(self, core, st, out_bar, deterministic=True):
         """Cotangents of ``step_device``'s input fields (u, v, w, eta_dot,
         pi_p, th_p of the diagnosed state ``st``) from those of its output
         (``out_bar``: dict of the same names, missing entries zero) through
         ``sisl_split_step_vjp``: the three RK3 stages differentiated as XLA
-        differentiates the reference's (no physics tendencies)."""
+        differentiates the reference's (no physics tendencies).
+        ``deterministic``: fixed-point scatters (the same bits on every run)
+        or float atomic adds (faster, order-dependent last bits)."""
         from .steppers import DeviceState
         ds_in = DeviceState(core, st)
         ob = DeviceState(core, {k: out_bar[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p") if k in out_bar})
@@ -100,7 +102,8 @@ class SplitExplicitStepper3D:
         eps_l = float(self.physics.c.get("eps_l", 1e-12))
         check(core.lib.sisl_split_step_vjp(core.handle, ctypes.byref(sin), ctypes.byref(sob), ctypes.byref(sib),
                                            int(self.ns), float(self.alpha), eps_l, self._tau_damp(core).data_ptr(),
-                                           ws.data_ptr(), n, core.stream), "sisl_split_step_vjp")
+                                           int(bool(deterministic)), ws.data_ptr(), n, core.stream),
+              "sisl_split_step_vjp")
         return {k: ib.t[k] for k in ("u", "v", "w", "eta_dot", "pi_p", "th_p")}
 
     def step_vjp(self, state, cot, bc_fn=None, forcing=None):
