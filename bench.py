@@ -794,7 +794,13 @@ def ensemble_vjp(args, world, dss, pp, cells):
     res_s, ms_seq = timed(sequential)
     graph = EnsembleVJPGraph(members, N)  # capture (2 N graphs over all members), outside the timed region
     graph.run(starts, objective)  # warm-up
+    res_b, ms_branch = timed(lambda: graph.run(starts, objective))
+    del graph
+    graph = EnsembleVJPGraph(members, N, grouped=True)  # the same graphs with grouped solves
+    graph.run(starts, objective)  # warm-up
     res_g, ms_graph = timed(lambda: graph.run(starts, objective))
+    same = all(float(a) == float(b) and torch.equal(ga["th_p"], gb["th_p"])
+               for (a, ga), (b, gb) in zip(res_g, res_b))
     dJg = max(abs(float(a) - float(b)) / max(abs(float(b)), 1e-300) for (a, _), (b, _) in zip(res_g, res_s))
     dgg = max(float(torch.linalg.vector_norm(ga["th_p"].double() - gb["th_p"].double()))
               / max(float(torch.linalg.vector_norm(gb["th_p"].double())), 1e-300)
@@ -811,8 +817,11 @@ def ensemble_vjp(args, world, dss, pp, cells):
     return {"metric": "SISL cell-steps/s fwd+VJP, per member", "value": world * cells * N / (ms_graph / 1e3),
             "unit": "cell-steps/s", "steps": N, "ms_per_ensemble_step": ms_graph / N,
             "launch": "per step one CUDA graph of every member's taped forward and one of every member's "
-                      "reverse sweep (EnsembleVJPGraph)",
+                      "reverse sweep, every solve grouped over the members (EnsembleVJPGraph grouped)",
             "graph_vs_sequential": {"J_max_rel": dJg, "grad_max_rel_l2": dgg},
+            "branches": {"value": world * cells * N / (ms_branch / 1e3), "ms_per_ensemble_step": ms_branch / N,
+                         "launch": "the same graphs with the members as parallel branches"},
+            "grouped_equals_branches_bitwise": bool(same),
             "concurrent_streams": {"value": world * cells * N / (ms / 1e3), "ms_per_ensemble_step": ms / N,
                                    "gpu_launches": launches,
                                    "launch": "members concurrently, one CUDA stream and host thread each",

@@ -474,6 +474,15 @@ int sisl_step_vjp_graph_create(int n, SislCore* const* cores, const SislState* i
                                const SislRelaxation* const* relax, const SislState* out_bars,
                                const SislState* in_bars, void* const* ws, const size_t* ws_bytes, void* stream,
                                SislStepGraph** out);
+/* sisl_step_vjp_graph_create with the members' transposed solves grouped as
+ * in sisl_step_graph_create_grouped (one GMRES on A^T over all members per
+ * solve, every Krylov phase one launch); every member's cotangents are the
+ * same bits.  Members share the dtype, restart, the transposed solves'
+ * GMRES method and the refinement switch. */
+int sisl_step_vjp_graph_create_grouped(int n, SislCore* const* cores, const SislState* ins, void* const* solves,
+                                       const SislRelaxation* const* relax, const SislState* out_bars,
+                                       const SislState* in_bars, void* const* ws, const size_t* ws_bytes,
+                                       void* stream, SislStepGraph** out);
 int sisl_step_graph_launch(SislStepGraph* graph, void* stream);
 /* Solve statistics of the last replay for one member (synchronises stream);
  * returns SISL_NOT_CONVERGED / SISL_ERR_NONFINITE like sisl_step. */

@@ -163,6 +163,9 @@ PROTOTYPES = {
     "sisl_step_vjp_graph_create": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState), vp, vp,
                                                   ctypes.POINTER(SislState), ctypes.POINTER(SislState), vp, vp, vp,
                                                   ctypes.POINTER(vp)]),
+    "sisl_step_vjp_graph_create_grouped": (ctypes.c_int, [ctypes.c_int, vp, ctypes.POINTER(SislState), vp, vp,
+                                                          ctypes.POINTER(SislState), ctypes.POINTER(SislState), vp,
+                                                          vp, vp, ctypes.POINTER(vp)]),
     "sisl_step_graph_launch": (ctypes.c_int, [vp, vp]),
     "sisl_step_graph_info": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(SislStepInfo), vp]),
     "sisl_step_graph_destroy": (ctypes.c_int, [vp]),

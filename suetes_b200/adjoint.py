@@ -584,9 +584,11 @@ class StepVJPGraph:
     fixed tensors by ``STATE_KEYS`` name) with its input ``DeviceState`` and
     the ten solve outputs its taped step recorded; the transposed GMRES loops
     are decided on the device.  ``members``: ``(stepper, ds_in, tape, relax,
-    out_bar, in_bar)``, distinct cores."""
+    out_bar, in_bar)``, distinct cores.  ``grouped``: each transposed solve
+    runs as one GMRES over all members, every Krylov phase a single launch
+    (``sisl_step_vjp_graph_create_grouped``), with the same bits."""
 
-    def __init__(self, members):
+    def __init__(self, members, grouped=False):
         from .core import stream_ptr
         from .steppers import SOLVE_METHODS
         self.lib = _lib.load()
@@ -622,9 +624,9 @@ class StepVJPGraph:
         narr = (ctypes.c_size_t * n)(*nbytes)
         self._keep += [carr, iarr, oarr, barr_, tarr, rarr, warr, narr, relax]
         h = ctypes.c_void_p()
-        check(self.lib.sisl_step_vjp_graph_create(n, carr, iarr, tarr, rarr, oarr, barr_, warr, narr,
-                                                  stream_ptr(self.device), ctypes.byref(h)),
-              "sisl_step_vjp_graph_create")
+        fn = "sisl_step_vjp_graph_create_grouped" if grouped else "sisl_step_vjp_graph_create"
+        check(getattr(self.lib, fn)(n, carr, iarr, tarr, rarr, oarr, barr_, warr, narr, stream_ptr(self.device),
+                                    ctypes.byref(h)), fn)
         self.handle, self.n = h, n
 
     def launch(self):
@@ -659,9 +661,11 @@ class EnsembleVJPGraph:
     between the reverse launches (stream-ordered).
 
     ``members``: ``[(stepper, ds0, relax)]`` with distinct cores; ``ds0``
-    fixes the shapes and the first-step flag of every later start."""
+    fixes the shapes and the first-step flag of every later start.
+    ``grouped``: both graphs run their solves grouped over the members
+    (``StepGraph``, ``StepVJPGraph``)."""
 
-    def __init__(self, members, num_steps):
+    def __init__(self, members, num_steps, grouped=False):
         from .steppers import DeviceState, StepGraph
         N = int(num_steps)
         if N < 1:
@@ -682,9 +686,9 @@ class EnsembleVJPGraph:
             self.B.append(B)
         M = len(members)
         self.fwd = [StepGraph([(members[m][0], self.S[m][n], self.S[m][n + 1], members[m][2]) for m in range(M)],
-                              tapes=[self.T[m][n] for m in range(M)]) for n in range(N)]
+                              tapes=[self.T[m][n] for m in range(M)], grouped=grouped) for n in range(N)]
         self.rev = [StepVJPGraph([(members[m][0], self.S[m][n], self.T[m][n], members[m][2], self.B[m][n + 1],
-                                   self.B[m][n]) for m in range(M)]) for n in range(N)]
+                                   self.B[m][n]) for m in range(M)], grouped=grouped) for n in range(N)]
 
     def run(self, starts, objective, wrt=("th_p",)):
         """``starts``: a ``DeviceState`` per member (same shapes and first-step

@@ -18,7 +18,7 @@
 //  pi row               L_p = p + adt ps cpidz (m^2 (dFx/dx + dFy/dy) + dFz)
 //  with P = p / ps, gzw(k) = (P(kr) - P(kl)) / dz_w(k) on the padded level
 //  pair, gzm(k) = (gzw(k) + gzw(k+1)) / 2, Fx = u rdu thu, Fz = W rhow thw.
-#include "sisl_core.cuh"
+#include "sisl_group.cuh"
 
 namespace sisl {
 namespace {
@@ -50,12 +50,10 @@ __device__ __forceinline__ T ybar_v(const Dims& d, const T* __restrict__ yv, T y
 // Stage 1: gbar_zm(i, j, k) = sum over the live faces whose gradient reads
 // column (i, j) at mass level k of -adt cp th zx / 2 * ybar.
 template <typename T>
-__global__ void at_gzm_kernel(Dims d, Coef<T> c, const T* __restrict__ yu, const T* __restrict__ yv, const double* yscale,
-                              T* __restrict__ gzm, const int* active) {
-  if (active && *active == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+__device__ __forceinline__ void at_gzm_block(const Dims& d, const Coef<T>& c, const T* __restrict__ yu, const T* __restrict__ yv, const double* yscale, T* __restrict__ gzm, int bx, int by, int bz) {
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz * blockDim.z + threadIdx.z;
   const int nx = d.nx, ny = d.ny;
   if (i >= nx || j >= ny || k >= d.nz) return;
   const T ys = yscale ? (T)(*yscale) : T(1);
@@ -87,16 +85,19 @@ __global__ void at_gzm_kernel(Dims d, Coef<T> c, const T* __restrict__ yu, const
   }
   gzm[im(d, i, j, k)] = g;
 }
+template <typename T>
+__global__ void at_gzm_kernel(Dims d, Coef<T> c, const T* __restrict__ yu, const T* __restrict__ yv, const double* yscale,
+                              T* __restrict__ gzm, const int* active) {
+  if (active && *active == 0) return;
+  at_gzm_block<T>(d, c, yu, yv, yscale, gzm, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // Stage 2: every input cotangent at a union-box point.
 template <typename T>
-__global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T> y, const double* yscale,
-                                                      const T* __restrict__ gzm, CVec5<T> b, Vec5<T> out,
-                                                      const int* active) {
-  if (active && *active == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+__device__ __forceinline__ void at_main_block(const Dims& d, const Coef<T>& c, const CVec5<T>& y, const double* yscale, const T* __restrict__ gzm, const CVec5<T>& b, const Vec5<T>& out, int bx, int by, int bz) {
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz * blockDim.z + threadIdx.z;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   if (i > nx || j > ny || k > nz) return;
   const T ys = yscale ? (T)(*yscale) : T(1);
@@ -259,6 +260,13 @@ __global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T
     if (b.f[3]) r = ld(b.f[3], p) - r;
     out.f[3][p] = r;
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) at_main_kernel(Dims d, Coef<T> c, CVec5<T> y, const double* yscale,
+                                                      const T* __restrict__ gzm, CVec5<T> b, Vec5<T> out,
+                                                      const int* active) {
+  if (active && *active == 0) return;
+  at_main_block<T>(d, c, y, yscale, gzm, b, out, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -493,11 +501,10 @@ __global__ void __launch_bounds__(TPT) pt_column_batched_kernel(Dims d, Coef<T> 
 // M^T, horizontal part: out_u = y_u + sum of the kinematic cotangent
 // kinbar = -alpha out_W over the interior w levels of the adjacent cells.
 template <typename T>
-__global__ void __launch_bounds__(256) pt_uv_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out, const int* active) {
-  if (active && *active == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+__device__ __forceinline__ void pt_uv_block(const Dims& d, const Coef<T>& c, const CVec5<T>& y, const Vec5<T>& out, int bx, int by, int bz) {
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz * blockDim.z + threadIdx.z;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   if (i > nx || j > ny || k >= nz) return;
   const T qa = -(T)c.s.alpha * T(0.25);
@@ -530,6 +537,11 @@ __global__ void __launch_bounds__(256) pt_uv_kernel(Dims d, Coef<T> c, CVec5<T> 
     }
     out.f[1][p] = g;
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) pt_uv_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out, const int* active) {
+  if (active && *active == 0) return;
+  pt_uv_block<T>(d, c, y, out, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -882,13 +894,11 @@ template void launch_tricubic_vjp<double>(int, int, int, int, int, int, const do
 // the w and eta_dot cotangents of the w level between z(k) and z(k+1) are
 // formed.  Shared memory per block: nz * NT values of T.
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT) pt_march_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
-                                                      const int* active) {
-  if (active && *active == 0) return;
+__device__ __forceinline__ void pt_march_block(const Dims& d, const Coef<T>& c, const CVec5<T>& y, const Vec5<T>& out, int bx, int by, int bz) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_w = reinterpret_cast<T*>(smem_raw);  // [nz][NT]
   const int t = threadIdx.x;
-  const int i = blockIdx.x * NT + t, j = blockIdx.y;
+  const int i = bx * NT + t, j = by;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   if (i >= nx) return;
   const int pm = nx * ny, h = i + nx * j;
@@ -938,6 +948,140 @@ __global__ void __launch_bounds__(NT) pt_march_kernel(Dims d, Coef<T> c, CVec5<T
   ow[ptop] = ld(yw, ptop);
   oW[ptop] = ld(yW, ptop) * ld(c.dzw, ptop);
 }
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) pt_march_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
+                                                      const int* active) {
+  if (active && *active == 0) return;
+  pt_march_block<T, NT>(d, c, y, out, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ---------------------------------------------------------------------------
+// grouped transposed operators over ensemble members (sisl_group.cuh): flat
+// block b runs block (b - first[m]) of member m's standalone launch
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T* gvec_a(const GroupMember<T>& g, int v) {
+  return g.vec + (size_t)v * g.npad;
+}
+// block (bx, by, bz) of a box of ex x ey x . points covered by blockDim-shaped blocks
+__device__ __forceinline__ void group_box(int t, int ex, int ey, int& bx, int& by, int& bz) {
+  const int gx = (ex + (int)blockDim.x - 1) / (int)blockDim.x, gy = (ey + (int)blockDim.y - 1) / (int)blockDim.y;
+  bz = t / (gx * gy);
+  const int r = t - bz * (gx * gy);
+  by = r / gx;
+  bx = r - by * gx;
+}
+
+// stage 0: at_gzm (mass points), stage 1: at_main (union box).  mode 0
+// Arnoldi step j (gated): V_j scaled by s_j -> z; mode 1 b - A^T x -> z;
+// mode 2 (U = double): b64 - A64^T x64 -> r64
+template <typename T, typename U>
+__global__ void __launch_bounds__(256) group_at_kernel(GroupMember<T>* mem, const int* __restrict__ first, int M,
+                                                       int stage, int mode, int j) {
+  const int b = blockIdx.x;
+  const int mi = group_find(first, M, b);
+  const GroupMember<T>& g = mem[mi];
+  if (!g.running) return;
+  if (mode == 0 && g.gs->active == 0) return;
+  int bx, by, bz;
+  group_box(b - first[mi], stage ? g.d.nx + 1 : g.d.nx, stage ? g.d.ny + 1 : g.d.ny, bx, by, bz);
+  // scale and right-hand side pointers stay run-time values in every mode,
+  // so the rows contract into the same FMAs as the standalone kernels'
+  const double* ysp = (mode == 0) ? &g.gs->s[j] : nullptr;
+  if constexpr (sizeof(U) == sizeof(T)) {
+    const T* src = gvec_a(g, mode == 0 ? GV_V0 + j : GV_X);
+    CVec5<T> y, bb;
+    Vec5<T> out;
+    const T* bv = gvec_a(g, GV_B);
+    T* z = gvec_a(g, GV_Z);
+    for (int q = 0; q < 5; ++q) {
+      y.f[q] = src + g.off[q];
+      bb.f[q] = (mode == 1) ? bv + g.off[q] : nullptr;
+      out.f[q] = z + g.off[q];
+    }
+    if (stage == 0) at_gzm_block<T>(g.d, g.c, y.f[0], y.f[1], ysp, g.tmp, bx, by, bz);
+    else at_main_block<T>(g.d, g.c, y, ysp, g.tmp, bb, out, bx, by, bz);
+  } else {
+    CVec5<double> y, bb;
+    Vec5<double> out;
+    for (int q = 0; q < 5; ++q) {
+      y.f[q] = g.x64 + g.off[q];
+      bb.f[q] = (mode != 0) ? g.b64 + g.off[q] : nullptr;
+      out.f[q] = g.r64 + g.off[q];
+    }
+    if (stage == 0) at_gzm_block<double>(g.d, g.c64, y.f[0], y.f[1], ysp, g.tmp64, bx, by, bz);
+    else at_main_block<double>(g.d, g.c64, y, ysp, g.tmp64, bb, out, bx, by, bz);
+  }
+}
+
+// stage 0: column march (128 columns per block), stage 1: u and v faces.
+// mode 0: z -> V_tv (gated when asked); mode 1: b -> V_1
+template <typename T>
+__global__ void __launch_bounds__(256) group_pt_kernel(GroupMember<T>* mem, const int* __restrict__ first, int M,
+                                                       int stage, int mode, int tv, int gated) {
+  const int b = blockIdx.x;
+  const int mi = group_find(first, M, b);
+  const GroupMember<T>& g = mem[mi];
+  if (!g.running || (gated && g.gs->active == 0)) return;
+  T* tgt = gvec_a(g, mode == 0 ? GV_V0 + tv : GV_V0 + 1);
+  const T* src = gvec_a(g, mode == 0 ? GV_Z : GV_B);
+  CVec5<T> y;
+  Vec5<T> out;
+  for (int q = 0; q < 5; ++q) {
+    y.f[q] = src + g.off[q];
+    out.f[q] = tgt + g.off[q];
+  }
+  const int t = b - first[mi];
+  if (stage == 0) {
+    const int gx = (g.d.nx + 127) / 128;
+    const int by = t / gx;
+    pt_march_block<T, 128>(g.d, g.c, y, out, t - by * gx, by, 0);
+  } else {
+    int bx, by, bz;
+    group_box(t, g.d.nx + 1, g.d.ny + 1, bx, by, bz);
+    pt_uv_block<T>(g.d, g.c, y, out, bx, by, bz);
+  }
+}
+
+int group_at_blocks(const Dims& d, int stage) {
+  const dim3 blk(32, 4, 2);
+  const dim3 g = stage ? box_grid(d.nx + 1, d.ny + 1, d.nz + 1, blk) : box_grid(d.nx, d.ny, d.nz, blk);
+  return (int)(g.x * g.y * g.z);
+}
+int group_pt_blocks(const Dims& d, int stage) {
+  if (stage == 0) return ((d.nx + 127) / 128) * d.ny;
+  const dim3 g = box_grid(d.nx + 1, d.ny + 1, d.nz, dim3(32, 4, 2));
+  return (int)(g.x * g.y * g.z);
+}
+
+template <typename T>
+void grp_matvec_t(const GroupLaunch<T>& g, int mode, int j, cudaStream_t st) {
+  for (int stage = 0; stage < 2; ++stage) {
+    const int tb = stage ? GT_ATM : GT_ATG;
+    if (mode == 2) {
+      if constexpr (sizeof(T) == 4)
+        group_at_kernel<T, double><<<g.blocks(tb), dim3(32, 4, 2), 0, st>>>(g.mem, g.row(tb), g.M, stage, 2, 0);
+    } else {
+      group_at_kernel<T, T><<<g.blocks(tb), dim3(32, 4, 2), 0, st>>>(g.mem, g.row(tb), g.M, stage, mode, j);
+    }
+  }
+}
+
+template <typename T>
+void grp_precond_t(const GroupLaunch<T>& g, int mode, int t, int gated, cudaStream_t st) {
+  int nz_max = 1;
+  for (int m = 0; m < g.M; ++m) nz_max = nz_max > g.nz_h[m] ? nz_max : g.nz_h[m];
+  const size_t smem = (size_t)nz_max * 128 * sizeof(T);
+  static SmemLimit attr_bytes;
+  ensure_smem_limit((const void*)group_pt_kernel<T>, attr_bytes, smem);
+  group_pt_kernel<T><<<g.blocks(GT_PTM), 128, smem, st>>>(g.mem, g.row(GT_PTM), g.M, 0, mode, t, gated);
+  group_pt_kernel<T><<<g.blocks(GT_PTU), dim3(32, 4, 2), 0, st>>>(g.mem, g.row(GT_PTU), g.M, 1, mode, t, gated);
+}
+
+template void grp_matvec_t<float>(const GroupLaunch<float>&, int, int, cudaStream_t);
+template void grp_matvec_t<double>(const GroupLaunch<double>&, int, int, cudaStream_t);
+template void grp_precond_t<float>(const GroupLaunch<float>&, int, int, int, cudaStream_t);
+template void grp_precond_t<double>(const GroupLaunch<double>&, int, int, int, cudaStream_t);
 
 template <typename T, int NT>
 void launch_pt_march(const Dims& d, const Coef<T>& c, CVec5<T> y, Vec5<T> out, const int* active,

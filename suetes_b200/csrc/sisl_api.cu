@@ -598,16 +598,14 @@ int solve_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> rhs, co
 // Cotangent of the physical right-hand side from the cotangent of the
 // physical solution (custom_linear_solve transpose, steppers.py:473-485):
 // unscale (x = S_out x_s), GMRES on A^T from a zero guess, rescale (b_s = S_in b).
+// solve_t_prep stages the GMRES vectors, solve_t_finish rescales the result.
 template <typename T>
-int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> xbar, const CVec5<T>* x0,
-                             Vec5<T> bbar, cudaStream_t st, SislSolveInfo* info, GDevInfo* dev_info = nullptr) {
-  const Dims& d = c->d;
+int solve_t_prep(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> xbar, const CVec5<T>* x0, cudaStream_t st) {
   {
     KScope k(c, SISL_K_OTHER, st);
     zero_gaps_kernel<T><<<g.R + 4, 256, 0, st>>>(g.vec, g.npad, g.R + 4, g.off[0], g.off[1], g.off[2], g.off[3],
                                                 g.off[4], g.sz[0], g.sz[1], g.sz[2], g.sz[3], g.sz[4]);
   }
-  const T ps = (T)c->s.ps;
   scale5<T>(c, cf, xbar, g.view(g.bg()), (T)(1.0 / c->s.ps), 2, st);  // pi / ps, eta / dz_w
   // initial guess: zero as in bwd_solve, or a caller's guess in the units of
   // the result (a warm start: the same solution within the tolerance)
@@ -616,9 +614,8 @@ int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<
   // GMRES treats a preconditioned residual below machine epsilon as zero
   // (_safe_normalize's absolute threshold); cotangents are often far below
   // unit norm, so the right-hand side is solved at unit norm and rescaled
-  const int norm_rhs = c->adj_normalize;
-  const int nb = 2 * 148;
-  if (norm_rhs) {
+  if (c->adj_normalize) {
+    const int nb = 2 * 148;
     KScope k(c, SISL_K_OTHER, st, 4);
     gm_setup(g.gs, 0.0, c->prm.solver_tol, c->prm.solver_atol, g.R, c->prm.solve_method, st);
     gm_dots<T>(g.V(0), g.npad, 0, g.bg(), g.npad, g.partial, g.gs, 1 /*BNORM*/, 0, st);
@@ -626,14 +623,24 @@ int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<
     scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.bg(), g.npad, g.scal, 0);
     if (x0) scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.xg(), g.npad, g.scal, 0);
   }
-  int rc = gmres_run<T>(c, cf, g, st, info, 1, dev_info);
-  if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
-  if (norm_rhs) {
+  return SISL_OK;
+}
+template <typename T>
+void solve_t_finish(SislCore* c, const Coef<T>& cf, GWork<T>& g, Vec5<T> bbar, cudaStream_t st) {
+  if (c->adj_normalize) {
     KScope k(c, SISL_K_OTHER, st);
-    scale_packed_kernel<T><<<nb, 256, 0, st>>>(g.xg(), g.npad, g.scal, 1);
+    scale_packed_kernel<T><<<2 * 148, 256, 0, st>>>(g.xg(), g.npad, g.scal, 1);
   }
-  scale5<T>(c, cf, g.cview(g.xg()), bbar, ps, 0, st);  // pi * ps
-  (void)d;
+  scale5<T>(c, cf, g.cview(g.xg()), bbar, (T)c->s.ps, 0, st);  // pi * ps
+}
+template <typename T>
+int solve_transpose_physical(SislCore* c, const Coef<T>& cf, GWork<T>& g, CVec5<T> xbar, const CVec5<T>* x0,
+                             Vec5<T> bbar, cudaStream_t st, SislSolveInfo* info, GDevInfo* dev_info = nullptr) {
+  int rc = solve_t_prep<T>(c, cf, g, xbar, x0, st);
+  if (rc) return rc;
+  rc = gmres_run<T>(c, cf, g, st, info, 1, dev_info);
+  if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+  solve_t_finish<T>(c, cf, g, bbar, st);
   return rc;
 }
 
@@ -979,17 +986,58 @@ VWork<T> carve_vjp(Carver& cv, const Dims& d) {
   return v;
 }
 
+// One reverse sweep's state between its segments: vjp_open, vjp_forward
+// (recompute and the finalisation's transpose), then for the second solve
+// and the first vjp_pre_solve, the transposed GMRES and vjp_post_solve,
+// then vjp_close (overrides, the six interpolation VJPs, explicit^T).
 template <typename T>
-int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const SislRelaxation* relax,
-                  const SislState* ob, const SislState* ib, void* ws, size_t ws_bytes, cudaStream_t st,
-                  SislStepInfo* info, GDevInfo* dev_info = nullptr) {
-  const Dims& d = c->d;
-  const Coef<T> cf = coef_of<T>(c);
+struct VjpRun {
+  SislCore* c = nullptr;
+  const SislState* in = nullptr;
+  void* const* tape = nullptr;
+  const SislRelaxation* relax = nullptr;
+  const SislState* ob = nullptr;
+  const SislState* ib = nullptr;
+  cudaStream_t st = nullptr;
+  SislStepInfo* info = nullptr;
+  Coef<T> cf{};
+  SWork<T> w{};
+  VWork<T> v{};
+  ExplicitIn<T> ein{};
+  bool hyp = false;
+  int64_t l0 = 0;
+  int status = SISL_OK;
+};
+
+template <typename T>
+int vjp_open(VjpRun<T>& r, SislCore* c, const SislState* in, void* const* tape, const SislRelaxation* relax,
+             const SislState* ob, const SislState* ib, void* ws, size_t ws_bytes, cudaStream_t st,
+             SislStepInfo* info) {
+  r.c = c; r.in = in; r.tape = tape; r.relax = relax; r.ob = ob; r.ib = ib; r.st = st; r.info = info;
+  r.cf = coef_of<T>(c);
   Carver cv{(char*)ws};
-  SWork<T> w = carve_step<T>(cv, d, c->prm.solver_restart, refining<T>(c));
-  VWork<T> v = carve_vjp<T>(cv, d);
+  r.w = carve_step<T>(cv, c->d, c->prm.solver_restart, refining<T>(c));
+  r.v = carve_vjp<T>(cv, c->d);
   if (cv.off > ws_bytes) return SISL_ERR_WORKSPACE;
-  const int64_t l0 = g_launches.load();
+  r.l0 = g_launches.load();
+  r.status = SISL_OK;
+  return SISL_OK;
+}
+
+// cotangent initialisation, the recomputation of the forward step's explicit
+// part, and the transpose of the finalisation
+template <typename T>
+int vjp_forward(VjpRun<T>& r) {
+  SislCore* c = r.c;
+  const Dims& d = c->d;
+  const Coef<T>& cf = r.cf;
+  SWork<T>& w = r.w;
+  VWork<T>& v = r.v;
+  const SislState* in = r.in;
+  const SislState* ob = r.ob;
+  const SislState* ib = r.ib;
+  const SislRelaxation* relax = r.relax;
+  cudaStream_t st = r.st;
   const T* u = (const T*)in->u;
   const T* vv = (const T*)in->v;
   const T* wv = (const T*)in->w;
@@ -998,8 +1046,8 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
   const T* th = (const T*)in->th_p;
   const T* x1[5];
   const T* x2[5];
-  for (int q = 0; q < 5; ++q) { x1[q] = (const T*)tape[q]; x2[q] = (const T*)tape[5 + q]; }
-  const double a = c->s.alpha, dt = c->s.dt;
+  for (int q = 0; q < 5; ++q) { x1[q] = (const T*)r.tape[q]; x2[q] = (const T*)r.tape[5 + q]; }
+  const double dt = c->s.dt;
   auto bytes = [&](int loc) { return sizeof(T) * field_size(d, loc); };
   // cotangents of the input state: the history passes straight through
   // (u_prev' = u, ...), everything else accumulates on top
@@ -1041,8 +1089,9 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
     // split-form offsets, as the forward's fused semi-Lagrangian kernels form them
     for (int l = 0; l < 4; ++l) launch_departure<T>(d, l, dt, w.vel + 3 * l, iters, v.coords + 3 * l, 1, st);
   }
-  ExplicitIn<T> ein{u, vv, wv, eta, pp, th, {nullptr, nullptr, nullptr, nullptr}};
-  const bool hyp = c->s.nu_h > 0.0;
+  ExplicitIn<T>& ein = r.ein;
+  ein = ExplicitIn<T>{u, vv, wv, eta, pp, th, {nullptr, nullptr, nullptr, nullptr}};
+  const bool hyp = r.hyp = c->s.nu_h > 0.0;
   if (hyp) {
     PtrTable<T> t4{}, o4{};
     for (int q = 0; q < 4; ++q) { t4.p[q] = w.htmp[q]; o4.p[q] = w.hyp[q]; }
@@ -1102,42 +1151,94 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
     KScope k(c, SISL_K_OTHER, st, c->s.nu_div != 0.0 ? 3 : 1);
     launch_finalize_vjp<T>(d, cf, fb, v.divb, st);
   }
-  int status = SISL_OK;
-  for (int it = 1; it >= 0; --it) {
-    // b_bar = A^-T x_bar (custom_linear_solve transpose, steppers.py:473-485)
-    CVec5<T> xb;
-    Vec5<T> bo;
-    for (int q = 0; q < 5; ++q) { xb.f[q] = it ? v.x2b[q] : v.x1b[q]; bo.f[q] = v.bb[q]; }
-    SislSolveInfo si{};
-    int rc = solve_transpose_physical<T>(c, cf, w.g, xb, nullptr, bo, st, &si, dev_info ? dev_info + it : nullptr);
-    if (info) info->solve[it] = si;
-    if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
-    if (rc != SISL_OK && status == SISL_OK) status = rc;
-    CorrectorIn<T> ci;
-    ci.rhs_u = w.ru; ci.rhs_v = w.rv; ci.rhs_w = nullptr; ci.rhs_pi = nullptr;
-    ci.th_next = it ? v.th2 : v.th1;
-    ci.pg = it ? x1[3] : pp;
-    ci.gu = it ? x1[0] : u;
-    ci.gv = it ? x1[1] : vv;
-    ci.geta = it ? x1[4] : eta;
-    ci.ug = it ? x1[0] : w.ru;
-    ci.vg = it ? x1[1] : w.rv;
-    CorrectorBar<T> cb;
-    for (int q = 0; q < 5; ++q) cb.b[q] = v.bb[q];
-    cb.rhs_u = v.rub; cb.rhs_v = v.rvb; cb.rhs_w = v.rwb; cb.rhs_pi = v.rpb; cb.reta = v.reb;
-    cb.th = it ? v.th2b : v.th1b;
-    cb.pg = it ? v.x1b[3] : pb;
-    cb.gu = it ? v.x1b[0] : ub;
-    cb.gv = it ? v.x1b[1] : vb;
-    cb.geta = it ? v.x1b[4] : eb;
-    cb.ug = it ? v.x1b[0] : v.rub;
-    cb.vg = it ? v.x1b[1] : v.rvb;
-    KScope k(c, SISL_K_EXPLICIT, st, 4);  // corrector^T (max, fixed-point, finish) + predictor^T
-    launch_corrector_vjp<T>(d, cf, ci, cb, v.det, st);
-    // theta' predictor; the first predictor's w terms cancel (w_next = w)
-    launch_corrector_theta_vjp<T>(d, cf, it ? v.th2b : v.th1b, v.thab, v.tthb, it ? wb : nullptr,
-                                  it ? v.x1b[2] : nullptr, st);
-  }
+  return SISL_OK;
+}
+
+// the transposed solve of the step's solve `it` staged from its solution's cotangent
+template <typename T>
+int vjp_pre_solve(VjpRun<T>& r, int it) {
+  CVec5<T> xb;
+  for (int q = 0; q < 5; ++q) xb.f[q] = it ? r.v.x2b[q] : r.v.x1b[q];
+  return solve_t_prep<T>(r.c, r.cf, r.w.g, xb, nullptr, r.st);
+}
+
+// b_bar = A^-T x_bar into the corrector's cotangents (custom_linear_solve
+// transpose, steppers.py:473-485), then corrector^T and predictor^T of solve it
+template <typename T>
+int vjp_post_solve(VjpRun<T>& r, int it, int rc, const SislSolveInfo& si) {
+  SislCore* c = r.c;
+  const Dims& d = c->d;
+  const Coef<T>& cf = r.cf;
+  SWork<T>& w = r.w;
+  VWork<T>& v = r.v;
+  cudaStream_t st = r.st;
+  const SislState* in = r.in;
+  const SislState* ib = r.ib;
+  if (r.info) r.info->solve[it] = si;
+  if (rc < 0 && rc != SISL_ERR_NONFINITE) return rc;
+  if (rc != SISL_OK && r.status == SISL_OK) r.status = rc;
+  Vec5<T> bo;
+  for (int q = 0; q < 5; ++q) bo.f[q] = v.bb[q];
+  solve_t_finish<T>(c, cf, w.g, bo, st);
+  const T* u = (const T*)in->u;
+  const T* vv = (const T*)in->v;
+  const T* eta = (const T*)in->eta_dot;
+  const T* pp = (const T*)in->pi_p;
+  const T* x1[5];
+  for (int q = 0; q < 5; ++q) x1[q] = (const T*)r.tape[q];
+  T* ub = (T*)ib->u;
+  T* vb = (T*)ib->v;
+  T* wb = (T*)ib->w;
+  T* eb = (T*)ib->eta_dot;
+  T* pb = (T*)ib->pi_p;
+  CorrectorIn<T> ci;
+  ci.rhs_u = w.ru; ci.rhs_v = w.rv; ci.rhs_w = nullptr; ci.rhs_pi = nullptr;
+  ci.th_next = it ? v.th2 : v.th1;
+  ci.pg = it ? x1[3] : pp;
+  ci.gu = it ? x1[0] : u;
+  ci.gv = it ? x1[1] : vv;
+  ci.geta = it ? x1[4] : eta;
+  ci.ug = it ? x1[0] : w.ru;
+  ci.vg = it ? x1[1] : w.rv;
+  CorrectorBar<T> cb;
+  for (int q = 0; q < 5; ++q) cb.b[q] = v.bb[q];
+  cb.rhs_u = v.rub; cb.rhs_v = v.rvb; cb.rhs_w = v.rwb; cb.rhs_pi = v.rpb; cb.reta = v.reb;
+  cb.th = it ? v.th2b : v.th1b;
+  cb.pg = it ? v.x1b[3] : pb;
+  cb.gu = it ? v.x1b[0] : ub;
+  cb.gv = it ? v.x1b[1] : vb;
+  cb.geta = it ? v.x1b[4] : eb;
+  cb.ug = it ? v.x1b[0] : v.rub;
+  cb.vg = it ? v.x1b[1] : v.rvb;
+  KScope k(c, SISL_K_EXPLICIT, st, 4);  // corrector^T (max, fixed-point, finish) + predictor^T
+  launch_corrector_vjp<T>(d, cf, ci, cb, v.det, st);
+  // theta' predictor; the first predictor's w terms cancel (w_next = w)
+  launch_corrector_theta_vjp<T>(d, cf, it ? v.th2b : v.th1b, v.thab, v.tthb, it ? wb : nullptr,
+                                it ? v.x1b[2] : nullptr, st);
+  return SISL_OK;
+}
+
+// lateral overrides, the six departure-point interpolation VJPs, explicit^T
+// and hyperdiffusion^T
+template <typename T>
+int vjp_close(VjpRun<T>& r) {
+  SislCore* c = r.c;
+  const Dims& d = c->d;
+  const Coef<T>& cf = r.cf;
+  SWork<T>& w = r.w;
+  VWork<T>& v = r.v;
+  cudaStream_t st = r.st;
+  const SislState* ib = r.ib;
+  const double a = c->s.alpha;
+  const int lim = c->prm.use_limiter;
+  const bool hyp = r.hyp;
+  const ExplicitIn<T>& ein = r.ein;
+  T* ub = (T*)ib->u;
+  T* vb = (T*)ib->v;
+  T* wb = (T*)ib->w;
+  T* eb = (T*)ib->eta_dot;
+  T* pb = (T*)ib->pi_p;
+  T* hb = (T*)ib->th_p;
   {  // lateral overrides, then the six departure-point interpolations
     KScope k(c, SISL_K_SL, st, 19);
     launch_fixup_vjp<T>(d, v.rub, v.rvb, ub, vb, v.reb, st);
@@ -1172,9 +1273,25 @@ int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const Sis
     KScope k(c, SISL_K_EXPLICIT, st, 5);
     launch_hyper_vjp<T>(d, cf, h4, gx, gy, t4, ub, vb, wb, hb, st);
   }
-  if (info) info->kernel_launches = g_launches.load() - l0;
+  if (r.info) r.info->kernel_launches = g_launches.load() - r.l0;
   int e = check_cuda();
-  return e ? e : status;
+  return e ? e : r.status;
+}
+
+template <typename T>
+int step_vjp_impl(SislCore* c, const SislState* in, void* const* tape, const SislRelaxation* relax,
+                  const SislState* ob, const SislState* ib, void* ws, size_t ws_bytes, cudaStream_t st,
+                  SislStepInfo* info, GDevInfo* dev_info = nullptr) {
+  VjpRun<T> r;
+  int rc = vjp_open<T>(r, c, in, tape, relax, ob, ib, ws, ws_bytes, st, info);
+  if (rc || (rc = vjp_forward<T>(r))) return rc;
+  for (int it = 1; it >= 0; --it) {
+    if ((rc = vjp_pre_solve<T>(r, it))) return rc;
+    SislSolveInfo si{};
+    rc = gmres_run<T>(c, r.cf, r.w.g, st, &si, 1, dev_info ? dev_info + it : nullptr);
+    if ((rc = vjp_post_solve<T>(r, it, rc, si))) return rc;
+  }
+  return vjp_close<T>(r);
 }
 
 bool valid_grid(const SislGrid* g) {
@@ -2236,40 +2353,60 @@ int capture_members(int n, SislCore* const* cores, F&& record, SislStepGraph** o
   return SISL_OK;
 }
 
-// One solve (`it` of the step) of every member as grouped launches, captured
-// on st: the restart loop is one conditional WHILE node (body captured on
-// side) that runs while any member continues; each member's own loop state
-// (cycles, convergence) lives in its GState and `running` flag.  The
-// sequence of phases per member is gmres_run's, so each member's result is
-// the same bits as its own graph-mode solve.
+// One solve of every member as grouped launches, captured on st: the
+// restart loop is one conditional WHILE node (body captured on side) that
+// runs while any member continues; each member's own loop state (cycles,
+// convergence) lives in its GState and `running` flag.  The sequence of
+// phases per member is gmres_run's (transpose: the A^T / M^T iteration of
+// the custom_linear_solve transpose), so each member's result is the same
+// bits as its own graph-mode solve.  slot: the step's solve index for the
+// statistics.
 template <typename T>
-int gmres_group_run(const GroupLaunch<T>& gl, cudaStream_t st, cudaStream_t side, int it) {
+int gmres_group_run(const GroupLaunch<T>& gl, cudaStream_t st, cudaStream_t side, int slot, int transpose) {
   const int R = gl.R;
-  const int64_t l0 = g_launches.load();
-  grp_setup<T>(gl, st);
+  grp_setup<T>(gl, transpose, st);
   if (gl.refine) grp_convert<T>(gl, 0, st);
   grp_dots<T>(gl, 0, GV_B, 1 /*BNORM*/, 0, st);
   if (gl.method == SISL_GMRES_INCREMENTAL) {
-    grp_convert<T>(gl, 3, st);
-    grp_precond<T>(gl, 1, 1, 0, st);
+    if (transpose) {
+      grp_precond_t<T>(gl, 1, 1, 0, st);
+    } else {
+      grp_convert<T>(gl, 3, st);
+      grp_precond<T>(gl, 1, 1, 0, st);
+    }
     grp_dots<T>(gl, 0, GV_V0 + 1, 2 /*MBNORM*/, 0, st);
   }
   grp_init_tol<T>(gl, st);
   auto residual = [&](cudaStream_t s) {
-    if (gl.refine) {
-      grp_matvec<T>(gl, 2, 0, s);
-      grp_convert<T>(gl, 1, s);
+    if (transpose) {
+      if (gl.refine) {
+        grp_matvec_t<T>(gl, 2, 0, s);
+        grp_convert<T>(gl, 4, s);
+      } else {
+        grp_matvec_t<T>(gl, 1, 0, s);
+      }
+      grp_precond_t<T>(gl, 0, 0, 0, s);
     } else {
-      grp_matvec<T>(gl, 1, 0, s);
+      if (gl.refine) {
+        grp_matvec<T>(gl, 2, 0, s);
+        grp_convert<T>(gl, 1, s);
+      } else {
+        grp_matvec<T>(gl, 1, 0, s);
+      }
+      grp_precond<T>(gl, 0, 0, 0, s);
     }
-    grp_precond<T>(gl, 0, 0, 0, s);
     grp_dots<T>(gl, 0, GV_V0, 3 /*RNORM*/, 0, s);
   };
   auto cycle = [&](cudaStream_t s) {
     grp_begin_cycle<T>(gl, s);
     for (int j = 0; j < R; ++j) {
-      grp_matvec<T>(gl, 0, j, s);
-      grp_precond<T>(gl, 0, j + 1, 1, s);
+      if (transpose) {
+        grp_matvec_t<T>(gl, 0, j, s);
+        grp_precond_t<T>(gl, 0, j + 1, 1, s);
+      } else {
+        grp_matvec<T>(gl, 0, j, s);
+        grp_precond<T>(gl, 0, j + 1, 1, s);
+      }
       grp_dots<T>(gl, j + 1, GV_V0 + j + 1, 0 /*PROJ*/, 1, s);
       grp_update_arnoldi<T>(gl, j + 1, s);
     }
@@ -2310,19 +2447,20 @@ int gmres_group_run(const GroupLaunch<T>& gl, cudaStream_t st, cudaStream_t side
   grp_gate<T>(gl, h, 1, side);
   cudaGraph_t body_out = nullptr;
   if (cuda_failed(cudaStreamEndCapture(side, &body_out), "cudaStreamEndCapture(body)")) return SISL_ERR_CUDA;
-  grp_info<T>(gl, it, st);
+  grp_info<T>(gl, slot, st);
   if (gl.refine) grp_convert<T>(gl, 2, st);
-  (void)l0;
+  g_launches += 1;
   return check_cuda();
 }
 
-// Grouped ensemble step graph: the members' explicit, corrector and
-// finalisation segments as parallel branches, each of the step's two solves
-// as one grouped GMRES over all members (gmres_group_run).
-template <typename T>
-int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
-                    const SislRelaxation* const* relax, void* const* solves, void* const* ws,
-                    const size_t* ws_bytes, SislStepGraph** out) {
+// Grouped ensemble graph: every member's segments (open: carve its
+// workspace on its stream; phase p = 0, 1, 2: its work before, between and
+// after the two solves) as parallel branches, each of the two solves as one
+// grouped GMRES over all members (gmres_group_run).  transpose: the solves
+// are the reverse sweep's transposed ones, the step's second solve first.
+template <typename T, typename Open, typename Work, typename Phase>
+int capture_grouped(int n, SislCore* const* cores, int transpose, Open&& open, Work&& gwork, Phase&& phase,
+                    SislStepGraph** out) {
   SislStepGraph* g = new (std::nothrow) SislStepGraph();
   if (!g) return SISL_ERR_ARG;
   g_last_error[0] = 0;
@@ -2339,21 +2477,23 @@ int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const S
     destroy_graph(g);
     return rc;
   };
+  auto method_of = [&](const SislCore* c) {
+    return (transpose && c->adj_method >= 0) ? c->adj_method : c->prm.solve_method;
+  };
   const SislCore* c0 = cores[0];
   const int R = c0->prm.solver_restart;
-  const int method = c0->prm.solve_method;
+  const int method = method_of(c0);
   const bool refine = refining<T>(c0);
   for (int m = 0; m < n; ++m) {
     const SislCore* c = cores[m];
     if (c->timing_class != SISL_K_NONE) return fail(SISL_ERR_ARG);  // no timing events inside a graph
-    if (c->prm.solver_restart != R || c->prm.solve_method != method || refining<T>(c) != refine ||
-        c->d.nz < 2 || R < 1 || R > GM_MAXR) {
+    if (c->prm.solver_restart != R || method_of(c) != method || refining<T>(c) != refine || c->d.nz < 2 || R < 1 ||
+        R > GM_MAXR) {
       snprintf(g_last_error, sizeof(g_last_error),
                "grouped solve: member %d differs in restart, GMRES method or refinement, or has nz < 2", m);
       return fail(SISL_ERR_ARG);
     }
   }
-  std::vector<StepRun<T>> runs(n);
   // streams: one per member, the capture stream, the loop-body stream
   for (int q = 0; q < n + 2; ++q) {
     cudaStream_t s;
@@ -2368,8 +2508,7 @@ int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const S
     g->events.push_back(e);
   }
   for (int m = 0; m < n; ++m) {
-    const int rc = step_open<T>(runs[m], cores[m], &ins[m], &outs[m], relax ? relax[m] : nullptr, ws[m], ws_bytes[m],
-                                g->streams[m], nullptr, solves ? solves + 10 * m : nullptr, nullptr);
+    const int rc = open(m, g->streams[m]);
     if (rc) return fail(rc);
   }
   // member descriptors and block tables
@@ -2395,7 +2534,7 @@ int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const S
   gl.nz_h.resize(n);
   for (int m = 0; m < n; ++m) {
     const SislCore* c = cores[m];
-    const GWork<T>& w = runs[m].w.g;
+    const GWork<T>& w = gwork(m);
     GroupMember<T>& e = hm[m];
     std::memset(&e, 0, sizeof(e));
     e.d = c->d;
@@ -2405,6 +2544,8 @@ int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const S
     e.x64 = w.x64;
     e.b64 = w.b64;
     e.r64 = w.r64;
+    e.tmp = w.tmp;
+    e.tmp64 = w.tmp64;
     e.npad = w.npad;
     for (int q = 0; q < 5; ++q) e.off[q] = w.off[q];
     e.gs = w.gs;
@@ -2413,6 +2554,7 @@ int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const S
     e.info[1] = dinfo + 2 * m + 1;
     e.eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
     e.tol = c->prm.solver_tol;
+    e.tol_t = (c->adj_tol > 0.0) ? c->adj_tol : c->prm.solver_tol;
     e.atol_in = c->prm.solver_atol;
     e.maxiter = c->prm.solver_maxiter;
     e.running = 0;
@@ -2424,6 +2566,10 @@ int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const S
     cnt[GT_UPD] = gm_update_blocks<T>(np);
     cnt[GT_X64] = gm_x64_blocks(np);
     cnt[GT_CVT] = group_convert_blocks(np);
+    cnt[GT_ATG] = group_at_blocks(c->d, 0);
+    cnt[GT_ATM] = group_at_blocks(c->d, 1);
+    cnt[GT_PTM] = group_pt_blocks(c->d, 0);
+    cnt[GT_PTU] = group_pt_blocks(c->d, 1);
     for (int q = 0; q <= R; ++q) cnt[GT_DOTS0 + q] = gm_dots_blocks<T>(q, np);
     for (int t = 0; t < NT; ++t) {
       int* row = gl.first_h.data() + (size_t)t * (n + 1);
@@ -2448,31 +2594,92 @@ int capture_grouped(int n, SislCore* const* cores, const SislState* ins, const S
     }
     return SISL_OK;
   };
+  auto members = [&](int p) -> int {
+    for (int m = 0; m < n; ++m) {
+      const int rc = phase(m, p);
+      if (rc < 0) {
+        if (!g_last_error[0]) snprintf(g_last_error, sizeof(g_last_error), "member %d: status %d", m, rc);
+        return rc;
+      }
+    }
+    return SISL_OK;
+  };
   if (cuda_failed(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture"))
     return fail(SISL_ERR_CUDA);
-  int rc = fork();
-  if (rc) return fail(rc);
-  for (int m = 0; m < n; ++m) {
-    step_explicit<T>(runs[m]);
-    step_pre_solve<T>(runs[m], 0);
-  }
-  if ((rc = join()) || (rc = gmres_group_run<T>(gl, st, side, 0)) || (rc = fork())) return fail(rc);
-  const SislSolveInfo none{};
-  for (int m = 0; m < n; ++m) {
-    if ((rc = step_post_solve<T>(runs[m], 0, SISL_OK, none))) return fail(rc);
-    step_pre_solve<T>(runs[m], 1);
-  }
-  if ((rc = join()) || (rc = gmres_group_run<T>(gl, st, side, 1)) || (rc = fork())) return fail(rc);
-  for (int m = 0; m < n; ++m) {
-    if ((rc = step_post_solve<T>(runs[m], 1, SISL_OK, none))) return fail(rc);
-    rc = step_close<T>(runs[m]);
-    if (rc < 0) return fail(rc);
-  }
-  if ((rc = join())) return fail(rc);
+  int rc;
+  if ((rc = fork()) || (rc = members(0)) || (rc = join()) ||
+      (rc = gmres_group_run<T>(gl, st, side, transpose ? 1 : 0, transpose)) || (rc = fork()) || (rc = members(1)) ||
+      (rc = join()) || (rc = gmres_group_run<T>(gl, st, side, transpose ? 0 : 1, transpose)) || (rc = fork()) ||
+      (rc = members(2)) || (rc = join()))
+    return fail(rc);
   if (cuda_failed(cudaStreamEndCapture(st, &g->graph), "cudaStreamEndCapture")) return fail(SISL_ERR_CUDA);
   if (cuda_failed(cudaGraphInstantiate(&g->exec, g->graph, 0), "cudaGraphInstantiate")) return fail(SISL_ERR_CUDA);
   *out = g;
   return SISL_OK;
+}
+
+// the forward step of every member with grouped solves
+template <typename T>
+int capture_grouped_step(int n, SislCore* const* cores, const SislState* ins, const SislState* outs,
+                         const SislRelaxation* const* relax, void* const* solves, void* const* ws,
+                         const size_t* ws_bytes, SislStepGraph** out) {
+  std::vector<StepRun<T>> runs(n);
+  const SislSolveInfo none{};
+  return capture_grouped<T>(
+      n, cores, 0,
+      [&](int m, cudaStream_t s) {
+        return step_open<T>(runs[m], cores[m], &ins[m], &outs[m], relax ? relax[m] : nullptr, ws[m], ws_bytes[m],
+                            s, nullptr, solves ? solves + 10 * m : nullptr, nullptr);
+      },
+      [&](int m) -> const GWork<T>& { return runs[m].w.g; },
+      [&](int m, int p) -> int {
+        StepRun<T>& r = runs[m];
+        if (p == 0) {
+          step_explicit<T>(r);
+          step_pre_solve<T>(r, 0);
+          return SISL_OK;
+        }
+        const int it = p - 1;
+        int rc = step_post_solve<T>(r, it, SISL_OK, none);
+        if (rc) return rc;
+        if (p == 1) {
+          step_pre_solve<T>(r, 1);
+          return SISL_OK;
+        }
+        rc = step_close<T>(r);
+        return rc < 0 ? rc : SISL_OK;
+      },
+      out);
+}
+
+// the reverse sweep of every member with grouped transposed solves
+template <typename T>
+int capture_grouped_vjp(int n, SislCore* const* cores, const SislState* ins, void* const* solves,
+                        const SislRelaxation* const* relax, const SislState* out_bars, const SislState* in_bars,
+                        void* const* ws, const size_t* ws_bytes, SislStepGraph** out) {
+  std::vector<VjpRun<T>> runs(n);
+  const SislSolveInfo none{};
+  return capture_grouped<T>(
+      n, cores, 1,
+      [&](int m, cudaStream_t s) {
+        return vjp_open<T>(runs[m], cores[m], &ins[m], solves + 10 * m, relax ? relax[m] : nullptr, &out_bars[m],
+                           &in_bars[m], ws[m], ws_bytes[m], s, nullptr);
+      },
+      [&](int m) -> const GWork<T>& { return runs[m].w.g; },
+      [&](int m, int p) -> int {
+        VjpRun<T>& r = runs[m];
+        int rc;
+        if (p == 0) {
+          if ((rc = vjp_forward<T>(r))) return rc;
+          return vjp_pre_solve<T>(r, 1);
+        }
+        const int it = (p == 1) ? 1 : 0;
+        if ((rc = vjp_post_solve<T>(r, it, SISL_OK, none))) return rc;
+        if (p == 1) return vjp_pre_solve<T>(r, 0);
+        rc = vjp_close<T>(r);
+        return rc < 0 ? rc : SISL_OK;
+      },
+      out);
 }
 
 // Argument checks shared by the graph builders: distinct cores (a core's
@@ -2537,15 +2744,14 @@ int sisl_step_graph_create_grouped(int n, SislCore* const* cores, const SislStat
   }
   (void)stream;  // captured on a private stream
   return (cores[0]->grid.dtype == SISL_F64)
-             ? capture_grouped<double>(n, cores, ins, outs, relax, solves, ws, ws_bytes, out)
-             : capture_grouped<float>(n, cores, ins, outs, relax, solves, ws, ws_bytes, out);
+             ? capture_grouped_step<double>(n, cores, ins, outs, relax, solves, ws, ws_bytes, out)
+             : capture_grouped_step<float>(n, cores, ins, outs, relax, solves, ws, ws_bytes, out);
 }
 
-int sisl_step_vjp_graph_create(int n, SislCore* const* cores, const SislState* ins, void* const* solves,
-                               const SislRelaxation* const* relax, const SislState* out_bars,
-                               const SislState* in_bars, void* const* ws, const size_t* ws_bytes, void* stream,
-                               SislStepGraph** out) {
-  if (!out || n < 1 || !cores || !ins || !solves || !out_bars || !in_bars || !ws || !ws_bytes) return SISL_ERR_ARG;
+namespace {
+int check_vjp_members(int n, SislCore* const* cores, const SislState* ins, void* const* solves,
+                      const SislState* out_bars, const SislState* in_bars, void* const* ws, const size_t* ws_bytes) {
+  if (n < 1 || !cores || !ins || !solves || !out_bars || !in_bars || !ws || !ws_bytes) return SISL_ERR_ARG;
   int rc = check_members(n, cores, ws, ws_bytes, SISL_WS_STEP_VJP);
   if (rc) return rc;
   for (int m = 0; m < n; ++m) {
@@ -2558,6 +2764,17 @@ int sisl_step_vjp_graph_create(int n, SislCore* const* cores, const SislState* i
     for (int q = 0; q < 10; ++q)
       if (!solves[10 * m + q]) return SISL_ERR_ARG;
   }
+  return SISL_OK;
+}
+}  // namespace
+
+int sisl_step_vjp_graph_create(int n, SislCore* const* cores, const SislState* ins, void* const* solves,
+                               const SislRelaxation* const* relax, const SislState* out_bars,
+                               const SislState* in_bars, void* const* ws, const size_t* ws_bytes, void* stream,
+                               SislStepGraph** out) {
+  if (!out) return SISL_ERR_ARG;
+  int rc = check_vjp_members(n, cores, ins, solves, out_bars, in_bars, ws, ws_bytes);
+  if (rc) return rc;
   (void)stream;  // captured on a private stream
   return capture_members(
       n, cores,
@@ -2571,6 +2788,21 @@ int sisl_step_vjp_graph_create(int n, SislCore* const* cores, const SislState* i
                                           ws_bytes[m], ms, nullptr, di);
       },
       out);
+}
+
+int sisl_step_vjp_graph_create_grouped(int n, SislCore* const* cores, const SislState* ins, void* const* solves,
+                                       const SislRelaxation* const* relax, const SislState* out_bars,
+                                       const SislState* in_bars, void* const* ws, const size_t* ws_bytes,
+                                       void* stream, SislStepGraph** out) {
+  if (!out) return SISL_ERR_ARG;
+  int rc = check_vjp_members(n, cores, ins, solves, out_bars, in_bars, ws, ws_bytes);
+  if (rc) return rc;
+  for (int m = 0; m < n; ++m)
+    if (cores[m]->grid.dtype != cores[0]->grid.dtype) return SISL_ERR_ARG;
+  (void)stream;  // captured on a private stream
+  return (cores[0]->grid.dtype == SISL_F64)
+             ? capture_grouped_vjp<double>(n, cores, ins, solves, relax, out_bars, in_bars, ws, ws_bytes, out)
+             : capture_grouped_vjp<float>(n, cores, ins, solves, relax, out_bars, in_bars, ws, ws_bytes, out);
 }
 
 int sisl_step_graph_launch(SislStepGraph* g, void* stream) {

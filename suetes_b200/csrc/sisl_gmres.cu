@@ -516,7 +516,8 @@ __global__ void __launch_bounds__(256) group_update_x64_kernel(GroupMember<T>* m
 }
 
 // 0: b64 = b, x64 = x, r64 = 0; 1: residual r64 -> V_0 (u, v) | z (w, pi,
-// eta_dot); 2: x = x64 (after the loop: every member); 3: V_1 (u, v) = b (u, v)
+// eta_dot); 2: x = x64 (after the loop: every member); 3: V_1 (u, v) = b (u, v);
+// 4: transposed residual r64 -> z
 template <typename T>
 __global__ void __launch_bounds__(256) group_convert_kernel(GroupMember<T>* mem, const int* __restrict__ first,
                                                             int M, int mode) {
@@ -540,6 +541,8 @@ __global__ void __launch_bounds__(256) group_convert_kernel(GroupMember<T>* mem,
       (e < g.off[2] ? v0 : z)[e] = (T)g.r64[e];
     } else if (mode == 2) {
       x[e] = (T)g.x64[e];
+    } else if (mode == 4) {
+      z[e] = (T)g.r64[e];
     } else {
       v0[g.npad + e] = bv[e];
     }
@@ -548,11 +551,11 @@ __global__ void __launch_bounds__(256) group_convert_kernel(GroupMember<T>* mem,
 
 // one thread per member
 template <typename T>
-__global__ void group_setup_kernel(GroupMember<T>* mem, int M, int R, int method) {
+__global__ void group_setup_kernel(GroupMember<T>* mem, int M, int R, int method, int transpose) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= M) return;
   GroupMember<T>& g = mem[m];
-  setup_state(g.gs, g.eps, g.tol, g.atol_in, R, method);
+  setup_state(g.gs, g.eps, transpose ? g.tol_t : g.tol, g.atol_in, R, method);
   g.running = 1;
 }
 template <typename T>
@@ -704,8 +707,8 @@ int gm_x64_blocks(size_t n) { return flat_grid(n, 256 * 4); }
 int group_convert_blocks(size_t n) { return flat_grid(n, 256 * 8) < 296 ? flat_grid(n, 256 * 8) : 296; }
 
 template <typename T>
-void grp_setup(const GroupLaunch<T>& g, cudaStream_t st) {
-  group_setup_kernel<T><<<(g.M + 127) / 128, 128, 0, st>>>(g.mem, g.M, g.R, g.method);
+void grp_setup(const GroupLaunch<T>& g, int transpose, cudaStream_t st) {
+  group_setup_kernel<T><<<(g.M + 127) / 128, 128, 0, st>>>(g.mem, g.M, g.R, g.method, transpose);
 }
 template <typename T>
 void grp_dots(const GroupLaunch<T>& g, int m, int w, int mode, int gated, cudaStream_t st) {
@@ -755,7 +758,7 @@ void grp_info(const GroupLaunch<T>& g, int solve, cudaStream_t st) {
   template int gm_dots_threads<T>(int);                                                              \
   template int gm_dots_blocks<T>(int, size_t);                                                       \
   template int gm_update_blocks<T>(size_t);                                                          \
-  template void grp_setup<T>(const GroupLaunch<T>&, cudaStream_t);                                   \
+  template void grp_setup<T>(const GroupLaunch<T>&, int, cudaStream_t);                              \
   template void grp_dots<T>(const GroupLaunch<T>&, int, int, int, int, cudaStream_t);                \
   template void grp_update_arnoldi<T>(const GroupLaunch<T>&, int, cudaStream_t);                     \
   template void grp_update_x<T>(const GroupLaunch<T>&, cudaStream_t);                                \

@@ -24,12 +24,15 @@ struct GroupMember {
   Coef<double> c64;  // float64 operator of the iterative refinement (float32 cores)
   T* vec;            // (R + 4) packed vectors of npad elements: x, b, z, V_0, V_1, ..
   double *x64, *b64, *r64;
+  T* tmp;            // mass-point scratch of the transposed matvec
+  double* tmp64;     // its float64 counterpart (refinement)
   size_t npad;
   size_t off[5];
   GState* gs;
   double* partial;
   GDevInfo* info[2];  // statistics of the step's two solves
   double eps, tol, atol_in;
+  double tol_t;      // tolerance of the transposed solves
   int maxiter;
   int running;  // 1 while this member's restart loop continues (device-written)
 };
@@ -41,6 +44,10 @@ enum GroupTable {
   GT_UPD,     // multi-axpy (+ norm)
   GT_X64,     // float64 solution update
   GT_CVT,     // packed conversions and copies
+  GT_ATG,     // transposed matvec, stage 1 (mass points)
+  GT_ATM,     // transposed matvec, stage 2 (union box)
+  GT_PTM,     // transposed preconditioner, column march
+  GT_PTU,     // transposed preconditioner, u and v faces
   GT_DOTS0    // GT_DOTS0 + m: projections onto m basis vectors
 };
 inline int group_tables(int R) { return GT_DOTS0 + R + 1; }
@@ -79,11 +86,14 @@ int gm_x64_blocks(size_t n);
 int group_matvec_blocks(const Dims& d);
 int group_precond_blocks(const Dims& d);
 int group_convert_blocks(size_t n);
+int group_at_blocks(const Dims& d, int stage);
+int group_pt_blocks(const Dims& d, int stage);
 
 // Krylov phases.  Every launch skips members whose `running` is 0; gated
 // launches also skip members whose current cycle has stopped (gs->active).
+// transpose: the tolerance of the transposed solves (tol_t)
 template <typename T>
-void grp_setup(const GroupLaunch<T>& g, cudaStream_t st);
+void grp_setup(const GroupLaunch<T>& g, int transpose, cudaStream_t st);
 // result over basis vectors V_0 .. V_{m-1} and vector `w` (GroupVec), mode as gm_dots
 template <typename T>
 void grp_dots(const GroupLaunch<T>& g, int m, int w, int mode, int gated, cudaStream_t st);
@@ -94,7 +104,7 @@ void grp_update_arnoldi(const GroupLaunch<T>& g, int m, cudaStream_t st);
 template <typename T>
 void grp_update_x(const GroupLaunch<T>& g, cudaStream_t st);
 // packed conversions: 0 b64 = b, x64 = x, r64 = 0; 1 residual r64 -> V_0
-// (u, v) | z (w, pi, eta); 2 x = x64; 3 V_1 (u, v) = b (u, v)
+// (u, v) | z (w, pi, eta); 2 x = x64; 3 V_1 (u, v) = b (u, v); 4 r64 -> z
 template <typename T>
 void grp_convert(const GroupLaunch<T>& g, int mode, cudaStream_t st);
 template <typename T>
@@ -118,5 +128,12 @@ void grp_matvec(const GroupLaunch<T>& g, int mode, int j, cudaStream_t st);
 // eta from z; gated for the Arnoldi steps (t >= 1); mode 1: M b -> V_1
 template <typename T>
 void grp_precond(const GroupLaunch<T>& g, int mode, int t, int gated, cudaStream_t st);
+// transposed operators.  matvec^T: mode 0 Arnoldi step j (gated), V_j
+// scaled by s_j -> z; mode 1 b - A^T x -> z; mode 2 b64 - A64^T x64 -> r64.
+// preconditioner^T: mode 0 z -> V_t (gated when t >= 1); mode 1 b -> V_1
+template <typename T>
+void grp_matvec_t(const GroupLaunch<T>& g, int mode, int j, cudaStream_t st);
+template <typename T>
+void grp_precond_t(const GroupLaunch<T>& g, int mode, int t, int gated, cudaStream_t st);
 
 }  // namespace sisl

@@ -201,6 +201,35 @@ def test_ensemble_vjp_graph_matches_eager():
                 assert rel_l2(got[m][1][k], ref[m][1][k]) < 1e-10, (trial, m, k)
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_grouped_ensemble_vjp_graph_equals_branches(dtype):
+    """Grouped solves in both graphs of the ensemble VJP (the taped forward
+    and the reverse sweep: one GMRES on A, then on A^T, over all members per
+    solve) give every member's value and gradient the same bits as the
+    graphs of per-member branches."""
+    from suetes_b200.adjoint import EnsembleVJPGraph
+    members = []
+    for nx, ny, nz in ((12, 10, 9), (16, 12, 10), (10, 14, 8)):
+        st, s0, p = _setup((), dtype=dtype, nx=nx, ny=ny, nz=nz)
+        members.append((st, st.to_device_state(s0), None))
+
+    def objective(m, n, s):
+        return (s["w"] ** 2).sum() * (m + 1) if n == 2 else None
+
+    branch = EnsembleVJPGraph(members, 2)
+    grouped = EnsembleVJPGraph(members, 2, grouped=True)
+    starts = [ds for _, ds, _ in members]
+    ra = branch.run(starts, objective, wrt=("th_p", "u", "w"))
+    rb = grouped.run(starts, objective, wrt=("th_p", "u", "w"))
+    for m in range(len(members)):
+        assert float(ra[m][0]) == float(rb[m][0]), m
+        for k in ("th_p", "u", "w"):
+            assert torch.equal(ra[m][1][k], rb[m][1][k]), (m, k)
+        for q in range(2):
+            a, b = branch.rev[0].info(m)["solves"][q], grouped.rev[0].info(m)["solves"][q]
+            assert a["cycles"] == b["cycles"] and a["converged"] == b["converged"], (m, q)
+
+
 @pytest.mark.parametrize("limiter", [False, True])
 def test_float32_step_vjp_is_bitwise_repeatable(limiter):
     """Every scatter of the reverse sweep sums in fixed point (the tricubic
