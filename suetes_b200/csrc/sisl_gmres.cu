@@ -69,17 +69,20 @@ __device__ __forceinline__ bool last_block(unsigned int* counter, unsigned int n
 enum DotMode { DM_PROJ = 0, DM_BNORM = 1, DM_MBNORM = 2, DM_RNORM = 3 };
 
 // result_i = <V_i, w> for i < m and <w, w>; finished according to `mode`.
-// Each thread accumulates its products in its own shared-memory slots
-// acc[q * blockDim + tid] (float64), so consecutive basis vectors stream
-// without a reduction in between; the block reduces once at the end.
+// Per tile, every warp sums its products (float64) with shuffles and lane 0
+// adds them to the warp's shared slot acc[q * warps + warp]: (m + 1) x 8
+// doubles per block, so shared memory never limits the resident blocks
+// (registers do); the block reduces the warps' slots once at the end.
 // Block `bid` of `nblk` blocks of one reduction (a member's share of a
 // grouped launch, or the whole grid of a standalone one).
 template <typename T>
 __device__ __forceinline__ void dots_body(const T* __restrict__ Vb, size_t stride, int m, const T* __restrict__ w,
                                           size_t n, double* partial, GState* gs, int mode, int bid, int nblk) {
-  extern __shared__ double acc[];  // (m + 1) * blockDim.x
+  extern __shared__ double acc[];  // (m + 1) * warps: per-warp sums
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int q = 0; q <= m; ++q) acc[q * nt + tid] = 0.0;
+  const int lane = tid & 31, wp = tid >> 5, nw = nt >> 5;
+  for (int q = tid; q < (m + 1) * nw; q += nt) acc[q] = 0.0;
+  __syncthreads();
   constexpr int VN = V16<T>::n;
   constexpr int E = CH * VN;
   const size_t tile = (size_t)nt * E;
@@ -96,7 +99,8 @@ __device__ __forceinline__ void dots_body(const T* __restrict__ Vb, size_t strid
     double sq = 0.0;
 #pragma unroll
     for (int e = 0; e < E; ++e) sq += (double)wr[e] * (double)wr[e];
-    acc[m * nt + tid] += sq;
+    sq = warp_sum(sq);
+    if (lane == 0) acc[m * nw + wp] += sq;
     // two basis vectors per iteration: both chunks are in flight together
     int i = 0;
     for (; i + 1 < m; i += 2) {
@@ -120,8 +124,12 @@ __device__ __forceinline__ void dots_body(const T* __restrict__ Vb, size_t strid
         pa += (double)va[e] * (double)wr[e];
         pc += (double)vc[e] * (double)wr[e];
       }
-      acc[i * nt + tid] += pa;
-      acc[(i + 1) * nt + tid] += pc;
+      pa = warp_sum(pa);
+      pc = warp_sum(pc);
+      if (lane == 0) {
+        acc[i * nw + wp] += pa;
+        acc[(i + 1) * nw + wp] += pc;
+      }
     }
     if (i < m) {
       const T* __restrict__ Vi = Vb + (size_t)i * stride;
@@ -137,17 +145,16 @@ __device__ __forceinline__ void dots_body(const T* __restrict__ Vb, size_t strid
       double p = 0.0;
 #pragma unroll
       for (int e = 0; e < E; ++e) p += (double)vr[e] * (double)wr[e];
-      acc[i * nt + tid] += p;
+      p = warp_sum(p);
+      if (lane == 0) acc[i * nw + wp] += p;
     }
   }
   __syncthreads();
-  // block reduction: warp wp reduces the slots of q = wp, wp + nwarps, ...
-  const int lane = tid & 31, wp = tid >> 5, nw = nt >> 5;
-  for (int q = wp; q <= m; q += nw) {
+  // block reduction: thread q sums the warps' slots of result q
+  for (int q = tid; q <= m; q += nt) {
     double s_ = 0.0;
-    for (int t = lane; t < nt; t += 32) s_ += acc[q * nt + t];
-    s_ = warp_sum(s_);
-    if (lane == 0) partial[(size_t)bid * (GM_MAXR + 2) + q] = s_;
+    for (int k = 0; k < nw; ++k) s_ += acc[q * nw + k];
+    partial[(size_t)bid * (GM_MAXR + 2) + q] = s_;
   }
   if (!last_block(&gs->counter, (unsigned)nblk)) return;
   // finish: sum the partials of all blocks, one warp per result (lanes
@@ -634,19 +641,18 @@ int resident_grid(const void* fn, int threads, size_t smem, size_t n, int elems_
 // ---------------------------------------------------------------------------
 // host wrappers
 // ---------------------------------------------------------------------------
-// shared memory of the dots kernel: (m + 1) slots per thread, at most 96 KB
-constexpr size_t DOTS_SMEM_MAX = 96 * 1024;
+// shared memory of the dots kernel: (m + 1) per-warp slots of 8 warps
+constexpr size_t DOTS_SMEM_MAX = (size_t)(GM_MAXR + 1) * 8 * sizeof(double);
+constexpr int DOTS_THREADS = 256;
 
 template <typename T>
 void gm_dots(const T* Vb, size_t stride, int m, const T* w, size_t n, double* partial, GState* gs, int mode,
              int gated, cudaStream_t st) {
   static SmemLimit attr_bytes;  // per instantiation
   ensure_smem_limit((const void*)dots_kernel<T>, attr_bytes, (size_t)DOTS_SMEM_MAX);
-  int nt = (int)(DOTS_SMEM_MAX / ((size_t)(m + 1) * sizeof(double)));
-  nt = nt >= 256 ? 256 : (nt / 32) * 32;
-  if (nt < 32) nt = 32;
+  const int nt = DOTS_THREADS;
   constexpr int E = CH * V16<T>::n;
-  const size_t smem = (size_t)(m + 1) * nt * sizeof(double);
+  const size_t smem = (size_t)(m + 1) * (nt / 32) * sizeof(double);
   const int g = resident_grid((const void*)dots_kernel<T>, nt, smem, n, nt * E);
   dots_kernel<T><<<g, nt, smem, st>>>(Vb, stride, m, w, n, partial, gs, mode, gated);
 }
@@ -686,9 +692,8 @@ void gm_snapshot(const GState* gs, GHostView* v, cudaStream_t st) { snapshot_ker
 // ---------------------------------------------------------------------------
 template <typename T>
 int gm_dots_threads(int m) {
-  int nt = (int)(DOTS_SMEM_MAX / ((size_t)(m + 1) * sizeof(double)));
-  nt = nt >= 256 ? 256 : (nt / 32) * 32;
-  return nt < 32 ? 32 : nt;
+  (void)m;
+  return DOTS_THREADS;
 }
 template <typename T>
 int gm_dots_blocks(int m, size_t n) {
@@ -696,7 +701,7 @@ int gm_dots_blocks(int m, size_t n) {
   ensure_smem_limit((const void*)dots_kernel<T>, attr_bytes, (size_t)DOTS_SMEM_MAX);
   const int nt = gm_dots_threads<T>(m);
   constexpr int E = CH * V16<T>::n;
-  return resident_grid((const void*)dots_kernel<T>, nt, (size_t)(m + 1) * nt * sizeof(double), n, nt * E);
+  return resident_grid((const void*)dots_kernel<T>, nt, (size_t)(m + 1) * (nt / 32) * sizeof(double), n, nt * E);
 }
 template <typename T>
 int gm_update_blocks(size_t n) {
@@ -715,7 +720,7 @@ void grp_dots(const GroupLaunch<T>& g, int m, int w, int mode, int gated, cudaSt
   static SmemLimit attr_bytes;
   ensure_smem_limit((const void*)group_dots_kernel<T>, attr_bytes, (size_t)DOTS_SMEM_MAX);
   const int nt = gm_dots_threads<T>(m);
-  const size_t smem = (size_t)(m + 1) * nt * sizeof(double);
+  const size_t smem = (size_t)(m + 1) * (nt / 32) * sizeof(double);
   group_dots_kernel<T><<<g.blocks(GT_DOTS0 + m), nt, smem, st>>>(g.mem, g.row(GT_DOTS0 + m), g.M, m, w, mode, gated);
 }
 template <typename T>
