@@ -170,11 +170,43 @@ __global__ void zero_gaps_kernel(T* base, size_t npad, int nvec, size_t o0, size
 }
 
 // dst = (D) src over a packed vector; elements below `split` go to dst_lo,
-// the rest to dst_hi (the u, v | w, pi, eta_dot split of the solver vectors)
+// the rest to dst_hi (the u, v | w, pi, eta_dot split of the solver
+// vectors).  n and split are multiples of 4 (the packed fields are padded to
+// 64 elements), so every thread moves aligned groups of 4 with vector
+// loads and stores; launch CONVERT_BLOCKS blocks of 256.
+template <typename T>
+__device__ __forceinline__ void load4(const T* p, T (&r)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    r[0] = v.x; r[1] = v.y; r[2] = v.z; r[3] = v.w;
+  } else {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    r[0] = a.x; r[1] = a.y; r[2] = b.x; r[3] = b.y;
+  }
+}
+template <typename T>
+__device__ __forceinline__ void store4(T* p, const T (&r)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(r[0], r[1], r[2], r[3]);
+  } else {
+    reinterpret_cast<double2*>(p)[0] = make_double2(r[0], r[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(r[2], r[3]);
+  }
+}
+constexpr int CONVERT_BLOCKS = 8 * 148;
 template <typename S, typename D>
-__global__ void convert_packed_kernel(const S* __restrict__ src, D* dst_lo, D* dst_hi, size_t split, size_t n) {
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-    (e < split ? dst_lo : dst_hi)[e] = (D)src[e];
+__global__ void __launch_bounds__(256) convert_packed_kernel(const S* __restrict__ src, D* dst_lo, D* dst_hi,
+                                                             size_t split, size_t n) {
+  const size_t n4 = n / 4;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n4; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = 4 * q;
+    S a[4];
+    load4(src + e, a);
+    D b[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) b[k] = (D)a[k];
+    store4((e < split ? dst_lo : dst_hi) + e, b);
+  }
 }
 
 // norm of a packed vector kept for the transposed solve; v *= 1/norm (mode 0)
@@ -358,7 +390,7 @@ int gmres_run(SislCore* c, const Coef<T>& cf, GWork<T>& g, cudaStream_t st, Sisl
   // float64 iterative refinement: x and b held in float64, every restart's
   // residual b - A x formed with the float64 operator, the Krylov cycle in T
   const bool refine = g.refine;
-  const int nconv = 2 * 148;
+  const int nconv = CONVERT_BLOCKS;
   Coef<double> cf64{};
   if (refine) {
     cf64 = coef64_of(c);

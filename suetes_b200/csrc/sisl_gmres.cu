@@ -203,10 +203,43 @@ __device__ __forceinline__ void update_x64_body(const T* __restrict__ Vb, size_t
   const int mm = min(m, gs->kdone);
   for (int q = threadIdx.x; q < mm; q += blockDim.x) cf[q] = gs->coef[q];
   __syncthreads();
-  for (size_t e = bid * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)nblk * blockDim.x) {
-    double acc = x[e];
-    for (int i = 0; i < mm; ++i) acc += cf[i] * (double)Vb[(size_t)i * stride + e];
-    x[e] = acc;
+  // CH 16-byte chunks of T per thread and tile (n is a multiple of 64: the
+  // packed fields are padded), every chunk's loads in flight together; per
+  // element the sum runs in the order acc = x, acc += coef_i V_i (i = 0, 1, ..)
+  constexpr int VN = V16<T>::n;
+  constexpr int E = CH * VN;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const size_t tile = (size_t)nt * E;
+  for (size_t base = (size_t)bid * tile; base < n; base += (size_t)nblk * tile) {
+    double acc[E];
+    bool ok[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      const size_t off = base + ((size_t)c * nt + tid) * VN;
+      ok[c] = off < n;
+#pragma unroll
+      for (int e = 0; e < VN; ++e) acc[c * VN + e] = ok[c] ? x[off + e] : 0.0;
+    }
+    for (int i = 0; i < mm; ++i) {
+      const T* __restrict__ Vi = Vb + (size_t)i * stride;
+      const double ci = cf[i];
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        if (!ok[c]) continue;
+        const size_t off = base + ((size_t)c * nt + tid) * VN;
+        T vr[VN];
+        load16(Vi + off, vr);
+#pragma unroll
+        for (int e = 0; e < VN; ++e) acc[c * VN + e] += ci * (double)vr[e];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      if (!ok[c]) continue;
+      const size_t off = base + ((size_t)c * nt + tid) * VN;
+#pragma unroll
+      for (int e = 0; e < VN; ++e) x[off + e] = acc[c * VN + e];
+    }
   }
 }
 template <typename T>
@@ -638,6 +671,12 @@ int resident_grid(const void* fn, int threads, size_t smem, size_t n, int elems_
 
 }  // namespace
 
+// resident grid of the float64 solution update (tiles of 256 threads x CH 16-byte chunks)
+template <typename T>
+int gm_x64_blocks_t(size_t n) {
+  return resident_grid((const void*)update_x64_kernel<T>, 256, 0, n, 256 * CH * V16<T>::n);
+}
+
 // ---------------------------------------------------------------------------
 // host wrappers
 // ---------------------------------------------------------------------------
@@ -667,7 +706,7 @@ void gm_update(const T* Vb, size_t stride, int m, T* w, size_t n, double sign, d
 
 template <typename T>
 void gm_update_x64(const T* Vb, size_t stride, int m, double* x, size_t n, const GState* gs, cudaStream_t st) {
-  update_x64_kernel<T><<<flat_grid(n, 256 * 4), 256, 0, st>>>(Vb, stride, m, x, n, gs);
+  update_x64_kernel<T><<<gm_x64_blocks_t<T>(n), 256, 0, st>>>(Vb, stride, m, x, n, gs);
 }
 
 void gm_setup(GState* gs, double eps, double tol, double atol_in, int restart, int method, cudaStream_t st) {
@@ -708,7 +747,7 @@ int gm_update_blocks(size_t n) {
   constexpr int E = CH * V16<T>::n;
   return resident_grid((const void*)update_kernel<T>, GT, 0, n, GT * E);
 }
-int gm_x64_blocks(size_t n) { return flat_grid(n, 256 * 4); }
+int gm_x64_blocks(size_t n) { return gm_x64_blocks_t<float>(n); }
 int group_convert_blocks(size_t n) { return flat_grid(n, 256 * 8) < 296 ? flat_grid(n, 256 * 8) : 296; }
 
 template <typename T>
