@@ -76,7 +76,7 @@ def parse():
                     help="skip the 192x192x64 60-step checkpointed fwd+VJP leg with its float64 Taylor test")
     ap.add_argument("--no-config1", action="store_true",
                     help="skip the 64x64x48 warm-bubble leg (GPU float64/float32, CPU oracle on the full grid)")
-    ap.add_argument("--micro-solves", type=int, default=10,
+    ap.add_argument("--micro-solves", type=int, default=50,
                     help="GMRES solves of the 384x384x96 microbenchmark leg (0 disables the leg)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--profile", default=None, choices=["step192", "tricubic384"],
