@@ -373,9 +373,7 @@ __global__ void __launch_bounds__(TPT) pt_column_kernel(Dims d, Coef<T> c, CVec5
 // batching).  Arithmetic is term for term that of pt_column_kernel, so the
 // results are bitwise those of every other column variant.
 template <typename T, int TPT, int TPC, int PU>
-__global__ void __launch_bounds__(TPT) pt_column_batched_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
-                                                                const int* active) {
-  if (active && *active == 0) return;
+__device__ __forceinline__ void pt_column_batched_block(const Dims& d, const Coef<T>& c, const CVec5<T>& y, const Vec5<T>& out, int bx, int by, int bz) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int nx = d.nx, ny = d.ny, nz = d.nz;
@@ -383,8 +381,8 @@ __global__ void __launch_bounds__(TPT) pt_column_batched_kernel(Dims d, Coef<T> 
   T* s_cp = s_x + nz * TPC;   // [nz][TPC]  c'
   T* s_lo = s_cp + nz * TPC;  // [nz][TPC]  lower
   T* s_iv = s_lo + nz * TPC;  // [nz][TPC]  1 / pivot
-  const int i0 = blockIdx.x * TPC;
-  const int j = blockIdx.y;
+  const int i0 = bx * TPC;
+  const int j = by;
   const int tid = threadIdx.x;
   const int pm = nx * ny;
   const int nm = nz * TPC, nw = (nz + 1) * TPC;
@@ -495,6 +493,12 @@ __global__ void __launch_bounds__(TPT) pt_column_batched_kernel(Dims d, Coef<T> 
       }
     }
   }
+}
+template <typename T, int TPT, int TPC, int PU>
+__global__ void __launch_bounds__(TPT) pt_column_batched_kernel(Dims d, Coef<T> c, CVec5<T> y, Vec5<T> out,
+                                                                const int* active) {
+  if (active && *active == 0) return;
+  pt_column_batched_block<T, TPT, TPC, PU>(d, c, y, out, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -1014,8 +1018,9 @@ __global__ void __launch_bounds__(256) group_at_kernel(GroupMember<T>* mem, cons
   }
 }
 
-// stage 0: column march (128 columns per block), stage 1: u and v faces.
-// mode 0: z -> V_tv (gated when asked); mode 1: b -> V_1
+// stage 0: column tile (32 columns per block of 256, batched loads, the
+// autotuner's usual choice), stage 1: u and v faces.  mode 0: z -> V_tv
+// (gated when asked); mode 1: b -> V_1
 template <typename T>
 __global__ void __launch_bounds__(256) group_pt_kernel(GroupMember<T>* mem, const int* __restrict__ first, int M,
                                                        int stage, int mode, int tv, int gated) {
@@ -1033,9 +1038,9 @@ __global__ void __launch_bounds__(256) group_pt_kernel(GroupMember<T>* mem, cons
   }
   const int t = b - first[mi];
   if (stage == 0) {
-    const int gx = (g.d.nx + 127) / 128;
+    const int gx = (g.d.nx + 31) / 32;
     const int by = t / gx;
-    pt_march_block<T, 128>(g.d, g.c, y, out, t - by * gx, by, 0);
+    pt_column_batched_block<T, 256, 32, 4>(g.d, g.c, y, out, t - by * gx, by, 0);
   } else {
     int bx, by, bz;
     group_box(t, g.d.nx + 1, g.d.ny + 1, bx, by, bz);
@@ -1049,7 +1054,7 @@ int group_at_blocks(const Dims& d, int stage) {
   return (int)(g.x * g.y * g.z);
 }
 int group_pt_blocks(const Dims& d, int stage) {
-  if (stage == 0) return ((d.nx + 127) / 128) * d.ny;
+  if (stage == 0) return ((d.nx + 31) / 32) * d.ny;
   const dim3 g = box_grid(d.nx + 1, d.ny + 1, d.nz, dim3(32, 4, 2));
   return (int)(g.x * g.y * g.z);
 }
@@ -1071,10 +1076,10 @@ template <typename T>
 void grp_precond_t(const GroupLaunch<T>& g, int mode, int t, int gated, cudaStream_t st) {
   int nz_max = 1;
   for (int m = 0; m < g.M; ++m) nz_max = nz_max > g.nz_h[m] ? nz_max : g.nz_h[m];
-  const size_t smem = (size_t)nz_max * 128 * sizeof(T);
+  const size_t smem = (size_t)(4 * nz_max) * 32 * sizeof(T);
   static SmemLimit attr_bytes;
   ensure_smem_limit((const void*)group_pt_kernel<T>, attr_bytes, smem);
-  group_pt_kernel<T><<<g.blocks(GT_PTM), 128, smem, st>>>(g.mem, g.row(GT_PTM), g.M, 0, mode, t, gated);
+  group_pt_kernel<T><<<g.blocks(GT_PTM), 256, smem, st>>>(g.mem, g.row(GT_PTM), g.M, 0, mode, t, gated);
   group_pt_kernel<T><<<g.blocks(GT_PTU), dim3(32, 4, 2), 0, st>>>(g.mem, g.row(GT_PTU), g.M, 1, mode, t, gated);
 }
 

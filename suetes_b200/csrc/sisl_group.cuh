@@ -46,7 +46,7 @@ enum GroupTable {
   GT_CVT,     // packed conversions and copies
   GT_ATG,     // transposed matvec, stage 1 (mass points)
   GT_ATM,     // transposed matvec, stage 2 (union box)
-  GT_PTM,     // transposed preconditioner, column march
+  GT_PTM,     // transposed preconditioner, 32-column tiles
   GT_PTU,     // transposed preconditioner, u and v faces
   GT_DOTS0    // GT_DOTS0 + m: projections onto m basis vectors
 };
