@@ -478,3 +478,51 @@ def test_transpose_solve_warm_start_same_solution():
     assert sol.last_transpose_info["cycles"] < cold_cycles
     for k in FIELDS5:
         assert rel_l2(warm[k], cold[k]) < 1e-9, (k, rel_l2(warm[k], cold[k]))
+
+
+def _still_air(ph, g, u0=10.0):
+    """Resting atmosphere with a uniform zonal wind (tests/test_dynamical_core_3d.py:558-574)."""
+    z = lambda *s: torch.zeros(*s, dtype=torch.float64)
+    nx, ny, nz = g.nx, g.ny, g.nz
+    rho = 1e5 / (287.0 * ph.theta_bg) * ph.pi_bg ** (717.0 / 287.0)
+    return {"u": z(nx + 1, ny, nz) + u0, "v": z(nx, ny + 1, nz), "w": z(nx, ny, nz + 1),
+            "eta_dot": z(nx, ny, nz + 1), "pi": ph.pi_bg.clone(), "th_v": ph.theta_bg.clone(), "rho": rho}
+
+
+@pytest.mark.parametrize("tol", [None, 1e-12])
+def test_kinetic_energy_gradient_through_three_steps(tol):
+    """Reverse-mode gradient of the kinetic energy proxy after three steps
+    with respect to the initial u (tests/test_dynamical_core_3d.py:541-616:
+    16x16x8 flat grid, dx = dy = 10 km, dz = 1 km, dt = 30 s, sponge above
+    8 km, N = 0.01, default stepper, u = 10 m/s).  The reference asserts a
+    finite, nonzero gradient; here it also equals the oracle's autograd of
+    the same three steps (the solves differentiated as linear solves), to
+    the solver tolerance at the default 1e-4 and to round-off at 1e-12."""
+    from oracle.steppers import SISLStepper3D as OSt
+    from suetes_b200 import SISLStepper3D as PSt
+    from suetes_b200.adjoint import trajectory_vjp
+    flat = lambda x, y: 0.0 * x
+    kw = dict(dt=30.0, damp_height=8000.0, N_bv=0.01, lat=45.0)
+    o = build("oracle", 16, 16, 8, 10000.0, 10000.0, 1000.0, h=flat, **kw)
+    p = build("cuda", 16, 16, 8, 10000.0, 10000.0, 1000.0, h=flat, device="cuda", **kw)
+    skw = {} if tol is None else dict(solver_tol=tol, solver_maxiter=60, solver_restart=30)
+    os_, ps_ = OSt(o[2], 30.0, **skw), PSt(p[2], 30.0, **skw)
+    s0 = _still_air(o[2], o[0])
+    u = s0["u"].clone().requires_grad_(True)
+    so = dict(s0, u=u, u_prev=u, v_prev=s0["v"], w_prev=s0["w"], eta_dot_prev=s0["eta_dot"],
+              tend_th_v_prev=torch.zeros_like(s0["th_v"]), is_first_step=1.0)
+    for n in range(3):
+        so = os_.step(so, n * 30.0, None, lambda s, f: s)
+    J = 0.5 * ((so["u"] ** 2).sum() + (so["v"] ** 2).sum() + (so["w"] ** 2).sum())
+    (gref,) = torch.autograd.grad(J, u)
+
+    def objective(n, st):
+        return 0.5 * ((st["u"] ** 2).sum() + (st["v"] ** 2).sum() + (st["w"] ** 2).sum()) if n == 3 else None
+
+    Jp, g = trajectory_vjp(ps_, to_cuda(s0), 3, objective, wrt=("u",))
+    gu = g["u"].double().cpu()
+    assert not torch.isnan(gu).any()
+    assert float(gu.abs().max()) > 0.0
+    bound = 1e-9 if tol is not None else 1e-3
+    assert abs(float(Jp) - float(J.detach())) <= bound * abs(float(J.detach())), (float(Jp), float(J))
+    assert rel_l2(gu, gref) < (1e-8 if tol is not None else 1e-3), rel_l2(gu, gref)
