@@ -407,7 +407,8 @@ def split_leg(args, local, world, peak, peak_kind):
                                          "eta_dot diagnosis)",
                                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
-                               "alg_bytes_per_cell_substep": "62 s (predict 16, column 24, correct 22)",
+                               "alg_bytes_per_cell_substep": "60 s (predict 12, column 24, correct 24; a stage's first "
+                                                              "predictor 16)",
                                "share_of_step": k_ms / ms, "launches_timed": k_n}
         # the native reverse sweep of the three stages (sisl_split_step_vjp)
         # at the current state, N(0,1) output cotangents

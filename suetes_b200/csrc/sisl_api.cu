@@ -1345,7 +1345,7 @@ namespace {
 // the Thomas sweep, and two stage states.
 template <typename T>
 struct SplitWork {
-  T *upp, *upp2, *vpp, *vpp2, *wpp, *ppp, *uh, *vh, *gx0, *gy0;
+  T *upp, *upp2, *vpp, *vpp2, *wpp, *ppp, *uh, *vh, *gx0, *gy0, *gx1, *gy1;
   T* sf[5];
   T* tend[6];
   T* adv[4];
@@ -1359,6 +1359,7 @@ void carve_split(Carver& cv, const Dims& d, SplitWork<T>& w) {
   auto f = [&](int loc) { return (T*)cv.take(sizeof(T) * field_size(d, loc)); };
   w.upp = f(LOC_U); w.upp2 = f(LOC_U); w.vpp = f(LOC_V); w.vpp2 = f(LOC_V);
   w.wpp = f(LOC_W); w.ppp = f(LOC_M); w.uh = f(LOC_U); w.vh = f(LOC_V); w.gx0 = f(LOC_U); w.gy0 = f(LOC_V);
+  w.gx1 = f(LOC_U); w.gy1 = f(LOC_V);
   const int sf_loc[5] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_M};
   for (int q = 0; q < 5; ++q) w.sf[q] = f(sf_loc[q]);
   const int t_loc[6] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_M, LOC_M};
@@ -1445,25 +1446,30 @@ void split_step_impl(SislCore* c, const SislState* in, const SislState* out, int
     a.u0 = s0[0]; a.v0 = s0[1]; a.w0 = s0[2]; a.p0 = s0[4]; a.th0 = s0[5];
     a.uc = cur[0]; a.vc = cur[1]; a.wc = cur[2]; a.pc = cur[4]; a.ec = cur[3];
     a.upp = w.upp; a.vpp = w.vpp; a.wpp = w.wpp; a.ppp = w.ppp;
-    a.uh = w.uh; a.vh = w.vh; a.gx0 = w.gx0; a.gy0 = w.gy0;
+    a.uh = w.uh; a.vh = w.vh; a.gx0 = w.gx0; a.gy0 = w.gy0; a.gx1 = w.gx1; a.gy1 = w.gy1;
     a.sfu = w.sf[0]; a.sfv = w.sf[1]; a.sfw = w.sf[2]; a.sfp = w.sf[3]; a.sfth = w.sf[4];
     a.tau = tau; a.cpr = w.cpr; a.dpr = w.dpr;
     a.dtau = (T)dts[stage]; a.alpha = (T)alpha; a.nu_div = (T)c->s.nu_div;
     T* spare_u = w.upp2;
     T* spare_v = w.vpp2;
     // algorithmic bytes, each distinct 3-D array once per kernel: init 12,
-    // and per sub-step predictor 16, column 24 (its Thomas sweep written and
-    // read back once), corrector 22
+    // and per sub-step predictor 12 (16 on a stage's first sub-step, which
+    // forms the pressure gradients from pi'' and the metric), column 24 (its
+    // Thomas sweep written and read back once), corrector 24 (with the two
+    // handed-over gradients)
     const double cellb = (double)sizeof(T) * d.nx * d.ny * d.nz;
     {
-      KScope k(c, SISL_K_OTHER, st, 1 + 3 * nst[stage], cellb * (12.0 + 62.0 * nst[stage]));
+      KScope k(c, SISL_K_OTHER, st, 1 + 3 * nst[stage], cellb * (12.0 + 4.0 + 60.0 * nst[stage]));
       launch_split_init<T>(d, a, st);
       for (int n = 0; n < nst[stage]; ++n) {
+        a.gx0_ready = n > 0;  // the previous corrector's gradients of this pi''
         launch_split_predict<T>(d, cf, a, st);
         launch_split_column<T>(d, cf, a, st);
         launch_split_correct<T>(d, cf, a, spare_u, spare_v, st);
         std::swap(a.upp, spare_u);
         std::swap(a.vpp, spare_v);
+        std::swap(a.gx0, a.gx1);
+        std::swap(a.gy0, a.gy1);
       }
     }
     {  // stage state (17 arrays) and its eta_dot diagnosis (8)
@@ -1701,7 +1707,7 @@ int sisl_core_create(const SislGrid* grid, const SislParams* prm, const SislBack
   }
   for (int q = 0; q < C_COUNT; ++q) c->coef_ptr[q] = (char*)c->coef_mem + offs[q];
   Base64 b{bg->theta_bg, bg->pi_bg, bg->Z_m, bg->dz_m_full, bg->dz_w_full, bg->z_xi_w, bg->z_eta_w, bg->tau_damp,
-           bg->m_m, bg->m_u, bg->m_v, bg->f_u, bg->f_v, bg->dm_dx_m, bg->dm_dy_m};
+           bg->m_m, bg->m_u, bg->m_v, bg->f_u, bg->f_v, bg->dm_dx_m, bg->dm_dy_m, bg->rho_bg};
   cudaStream_t st = (cudaStream_t)stream;
   g_launches += 1;
   if (grid->dtype == SISL_F64) {

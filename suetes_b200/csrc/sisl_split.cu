@@ -202,47 +202,62 @@ __device__ __forceinline__ T cell_div(const Dims& d, const Coef<T>& c, const T* 
   return du + dv;
 }
 
-// the divergence-damping gradient at u face i / v face j (steppers.py:1528-1538)
+// Blocks of the predictor and corrector: SX x SY faces of one level.
+constexpr int SX = 32, SY = 8;
+
+// The horizontal divergence of the total winds (stage + perturbation) of the
+// cells (i0 - 1 + x, j0 - 1 + y), x <= SX, y <= SY, at level k, into Dt.
+// Cell indices beyond the grid wrap on a periodic axis and are clamped on an
+// open one, so every interior face (i, j) of the block finds the two cells
+// of its divergence-damping gradient at tile columns i - i0, i - i0 + 1
+// (rows j - j0, j - j0 + 1), as face_pair gives them, and the periodic
+// duplicate face n its wrapped pair; the open boundary faces take no
+// gradient (the divergence-damping gradient, steppers.py:1528-1538).  One cell divergence per cell of the tile instead of two per
+// face and axis.
 template <typename T>
-__device__ __forceinline__ T div_grad_x(const Dims& d, const Coef<T>& c, const T* uc, const T* up, const T* vc,
-                                        const T* vp, int i, int j, int k) {
-  int l, r;
-  face_pair(i, d.nx, d.px, l, r);
-  return (cell_div(d, c, uc, up, vc, vp, r, j, k) - cell_div(d, c, uc, up, vc, vp, l, j, k)) / (T)d.dx *
-         ld(c.mu, h_u(d, i, j));
-}
-template <typename T>
-__device__ __forceinline__ T div_grad_y(const Dims& d, const Coef<T>& c, const T* uc, const T* up, const T* vc,
-                                        const T* vp, int i, int j, int k) {
-  int l, r;
-  face_pair(j, d.ny, d.py, l, r);
-  return (cell_div(d, c, uc, up, vc, vp, i, r, k) - cell_div(d, c, uc, up, vc, vp, i, l, k)) / (T)d.dy *
-         ld(c.mv, h_v(d, i, j));
+__device__ __forceinline__ void div_tile(const Dims& d, const Coef<T>& c, const T* uc, const T* up, const T* vc,
+                                         const T* vp, int i0, int j0, int k, T (*Dt)[SX + 1]) {
+  const int t = threadIdx.x + SX * threadIdx.y;
+  for (int q = t; q < (SX + 1) * (SY + 1); q += SX * SY) {
+    const int x = q % (SX + 1), y = q / (SX + 1);
+    const int ci = wrap_or_clamp(i0 - 1 + x, d.nx, d.px), cj = wrap_or_clamp(j0 - 1 + y, d.ny, d.py);
+    Dt[y][x] = cell_div(d, c, uc, up, vc, vp, ci, cj, k);
+  }
 }
 
 // PART 1 of the acoustic sub-step (steppers.py:1561-1579): u'' and v'' to
 // the midpoint; the boundary faces take the step-start winds (open) or the
-// first face (periodic duplicate).
+// first face (periodic duplicate).  The pressure gradient of the old pi''
+// is formed here on the first sub-step of a stage and taken from the
+// previous corrector (gx0_ready) on the others.
 template <typename T>
-__global__ void __launch_bounds__(256) split_predict_kernel(Dims d, Coef<T> c, SplitArgs<T> a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
-  const int nx = d.nx, ny = d.ny, nz = d.nz;
-  if (i > nx || j > ny || k >= nz) return;
+__global__ void __launch_bounds__(SX * SY) split_predict_kernel(Dims d, Coef<T> c, SplitArgs<T> a) {
+  __shared__ T Dt[SY + 1][SX + 1];
+  const int i0 = blockIdx.x * SX, j0 = blockIdx.y * SY, k = blockIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = i0 + tx, j = j0 + ty;
+  const int nx = d.nx, ny = d.ny;
+  div_tile<T>(d, c, a.uc, a.upp, a.vc, a.vpp, i0, j0, k, Dt);
+  __syncthreads();
+  if (i > nx || j > ny) return;
   const T cp = (T)c.s.cp, hdt = T(0.5) * a.dtau;
   const Grad<T> G{d, c, a.ppp};
   if (j < ny) {
     const int p = iu(d, i, j, k);
     const int ie = (d.px && i == nx) ? 0 : i, pe = iu(d, ie, j, k);
-    const T g0 = G.gx(ie, j, k);
-    a.gx0[p] = g0;
     T val;
     if (!d.px && (i == 0 || i == nx)) {
       val = a.u0[p] - a.uc[p];
     } else {
-      const T rhs = a.sfu[pe] - cp * ld(c.thu, pe) * g0 +
-                    a.nu_div * div_grad_x(d, c, a.uc, a.upp, a.vc, a.vpp, ie, j, k);
+      T g0;
+      if (a.gx0_ready) {
+        g0 = a.gx0[p];
+      } else {
+        g0 = G.gx(ie, j, k);
+        a.gx0[p] = g0;
+      }
+      const T dgx = (Dt[ty + 1][tx + 1] - Dt[ty + 1][tx]) / (T)d.dx * ld(c.mu, h_u(d, ie, j));
+      const T rhs = a.sfu[pe] - cp * ld(c.thu, pe) * g0 + a.nu_div * dgx;
       val = a.upp[pe] + hdt * rhs;
     }
     a.uh[p] = val;
@@ -250,14 +265,19 @@ __global__ void __launch_bounds__(256) split_predict_kernel(Dims d, Coef<T> c, S
   if (i < nx) {
     const int p = iv(d, i, j, k);
     const int je = (d.py && j == ny) ? 0 : j, pe = iv(d, i, je, k);
-    const T g0 = G.gy(i, je, k);
-    a.gy0[p] = g0;
     T val;
     if (!d.py && (j == 0 || j == ny)) {
       val = a.v0[p] - a.vc[p];
     } else {
-      const T rhs = a.sfv[pe] - cp * ld(c.thv, pe) * g0 +
-                    a.nu_div * div_grad_y(d, c, a.uc, a.upp, a.vc, a.vpp, i, je, k);
+      T g0;
+      if (a.gx0_ready) {
+        g0 = a.gy0[p];
+      } else {
+        g0 = G.gy(i, je, k);
+        a.gy0[p] = g0;
+      }
+      const T dgy = (Dt[ty + 1][tx + 1] - Dt[ty][tx + 1]) / (T)d.dy * ld(c.mv, h_v(d, i, je));
+      const T rhs = a.sfv[pe] - cp * ld(c.thv, pe) * g0 + a.nu_div * dgy;
       val = a.vpp[pe] + hdt * rhs;
     }
     a.vh[p] = val;
@@ -453,15 +473,19 @@ __global__ void __launch_bounds__(PT) split_column_tile_kernel(Dims d, Coef<T> c
 }
 
 // PART 3 (steppers.py:1607-1626): the centred corrector of u'', v'' into
-// upp2/vpp2 (read u'' from upp/vpp), and the backward damping of w''.
+// upp2/vpp2 (read u'' from upp/vpp), and the backward damping of w''.  The
+// gradients of the new pi'' go to gx1/gy1 for the next predictor.
 template <typename T>
-__global__ void __launch_bounds__(256) split_correct_kernel(Dims d, Coef<T> c, SplitArgs<T> a, T* __restrict__ upp2,
-                                                            T* __restrict__ vpp2) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+__global__ void __launch_bounds__(SX * SY) split_correct_kernel(Dims d, Coef<T> c, SplitArgs<T> a,
+                                                                T* __restrict__ upp2, T* __restrict__ vpp2) {
+  __shared__ T Dt[SY + 1][SX + 1];
+  const int i0 = blockIdx.x * SX, j0 = blockIdx.y * SY, k = blockIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = i0 + tx, j = j0 + ty;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  if (i > nx || j > ny || k > nz) return;
+  if (k < nz) div_tile<T>(d, c, a.uc, a.uh, a.vc, a.vh, i0, j0, k, Dt);
+  __syncthreads();
+  if (i > nx || j > ny) return;
   const T cp = (T)c.s.cp, dtau = a.dtau;
   const Grad<T> G{d, c, a.ppp};
   if (j < ny && k < nz) {
@@ -472,8 +496,9 @@ __global__ void __launch_bounds__(256) split_correct_kernel(Dims d, Coef<T> c, S
     } else {
       const int ie = (d.px && i == nx) ? 0 : i, pe = iu(d, ie, j, k);
       const T g1 = G.gx(ie, j, k);
-      val = a.upp[pe] + dtau * (a.sfu[pe] - T(0.5) * cp * ld(c.thu, pe) * (a.gx0[pe] + g1) +
-                                a.nu_div * div_grad_x(d, c, a.uc, a.uh, a.vc, a.vh, ie, j, k));
+      if (a.gx1) a.gx1[p] = g1;
+      const T dgx = (Dt[ty + 1][tx + 1] - Dt[ty + 1][tx]) / (T)d.dx * ld(c.mu, h_u(d, ie, j));
+      val = a.upp[pe] + dtau * (a.sfu[pe] - T(0.5) * cp * ld(c.thu, pe) * (a.gx0[pe] + g1) + a.nu_div * dgx);
     }
     upp2[p] = val;
   }
@@ -485,8 +510,9 @@ __global__ void __launch_bounds__(256) split_correct_kernel(Dims d, Coef<T> c, S
     } else {
       const int je = (d.py && j == ny) ? 0 : j, pe = iv(d, i, je, k);
       const T g1 = G.gy(i, je, k);
-      val = a.vpp[pe] + dtau * (a.sfv[pe] - T(0.5) * cp * ld(c.thv, pe) * (a.gy0[pe] + g1) +
-                                a.nu_div * div_grad_y(d, c, a.uc, a.uh, a.vc, a.vh, i, je, k));
+      if (a.gy1) a.gy1[p] = g1;
+      const T dgy = (Dt[ty + 1][tx + 1] - Dt[ty][tx + 1]) / (T)d.dy * ld(c.mv, h_v(d, i, je));
+      val = a.vpp[pe] + dtau * (a.sfv[pe] - T(0.5) * cp * ld(c.thv, pe) * (a.gy0[pe] + g1) + a.nu_div * dgy);
     }
     vpp2[p] = val;
   }
@@ -565,7 +591,7 @@ void launch_split_init(const Dims& d, const SplitArgs<T>& a, cudaStream_t st) {
 
 template <typename T>
 void launch_split_predict(const Dims& d, const Coef<T>& c, const SplitArgs<T>& a, cudaStream_t st) {
-  const dim3 blk(32, 4, 2);
+  const dim3 blk(SX, SY, 1);
   split_predict_kernel<T><<<box(d.nx + 1, d.ny + 1, d.nz, blk), blk, 0, st>>>(d, c, a);
 }
 
@@ -587,7 +613,7 @@ void launch_split_column(const Dims& d, const Coef<T>& c, const SplitArgs<T>& a,
 template <typename T>
 void launch_split_correct(const Dims& d, const Coef<T>& c, const SplitArgs<T>& a, T* upp2, T* vpp2,
                           cudaStream_t st) {
-  const dim3 blk(32, 4, 2);
+  const dim3 blk(SX, SY, 1);
   split_correct_kernel<T><<<box(d.nx + 1, d.ny + 1, d.nz + 1, blk), blk, 0, st>>>(d, c, a, upp2, vpp2);
 }
 

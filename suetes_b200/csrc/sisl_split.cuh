@@ -16,10 +16,15 @@ struct SplitArgs {
   T *upp, *vpp, *wpp, *ppp;          // acoustic perturbations u'', v'', w'', pi''
   T *uh, *vh;                        // midpoint winds of the acoustic sub-step
   T *gx0, *gy0;                      // horizontal pressure gradients of the old pi''
+  // the corrector's gradients of the new pi'' (NULL: not kept); the next
+  // sub-step's predictor takes them as its gx0, gy0 (same pi'', same bits)
+  // when gx0_ready is set instead of forming them again
+  T *gx1, *gy1;
   const T *sfu, *sfv, *sfw, *sfp, *sfth;  // slow forcings
   const T* tau;                      // tau_damp at w levels
   T *cpr, *dpr;                      // Thomas scratch (mass points)
   T dtau, alpha, nu_div;
+  int gx0_ready;
 };
 
 // eta_dot and the kinematic w boundaries of a state (steppers.py:1272-1310);
