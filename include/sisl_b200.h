@@ -97,11 +97,15 @@ typedef struct SislParams {
 /* float64 background and metrics (device pointers, device layout):
  * Euler3D.theta_bg / pi_bg / tau_damp (euler.py:76-121) and
  * RegionalGrid3D.Z_m, dz_m_full, dz_w_full, z_xi_w, z_eta_w, m_factors,
- * f_u, f_v, dm_dx_m, dm_dy_m (geometry.py:190-261).  Read only during
- * sisl_core_create. */
+ * f_u, f_v, dm_dx_m, dm_dy_m (geometry.py:190-261).  rho_bg: the
+ * background density at mass points, or NULL for the equation of state
+ * p0 / (Rd theta_bg) pi_bg^(cvd/Rd) (the background the step builds,
+ * steppers.py:769-775; Euler3D.precompute_bg, euler.py:127-160, accepts any
+ * density).  Read only during sisl_core_create. */
 typedef struct SislBackground {
   const double *theta_bg, *pi_bg, *Z_m, *dz_m_full, *dz_w_full, *z_xi_w, *z_eta_w, *tau_damp;
   const double *m_m, *m_u, *m_v, *f_u, *f_v, *dm_dx_m, *dm_dy_m;
+  const double* rho_bg;
 } SislBackground;
 
 typedef struct SislCore SislCore;

@@ -45,7 +45,8 @@ class SislParams(ctypes.Structure):
 
 class SislBackground(ctypes.Structure):
     _fields_ = [(n, vp) for n in ("theta_bg", "pi_bg", "Z_m", "dz_m_full", "dz_w_full", "z_xi_w", "z_eta_w",
-                                  "tau_damp", "m_m", "m_u", "m_v", "f_u", "f_v", "dm_dx_m", "dm_dy_m")]
+                                  "tau_damp", "m_m", "m_u", "m_v", "f_u", "f_v", "dm_dx_m", "dm_dy_m",
+                                  "rho_bg")]
 
 
 class SislSolveInfo(ctypes.Structure):

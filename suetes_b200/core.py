@@ -58,7 +58,7 @@ class Core:
     alpha and precision) plus cached device workspaces."""
 
     def __init__(self, grid, constants, theta_bg, pi_bg, tau_damp, dtype, dt, alpha, nu_div, nu_h,
-                 periodic_axes=(), solver=None, use_limiter=False, departure_iterations=2):
+                 periodic_axes=(), solver=None, use_limiter=False, departure_iterations=2, rho_bg=None):
         if grid.device.type != "cuda":
             raise RuntimeError("the SISL core runs on CUDA devices only (no CPU fallback)")
         self.lib = _lib.load()
@@ -87,6 +87,9 @@ class Core:
         keep = [f(theta_bg), f(pi_bg), f(grid.Z_m), f(grid.dz_m_full), f(grid.dz_w_full), f(grid.z_xi_w),
                 f(grid.z_eta_w), f(tau_damp), f(grid.m_factors["m"]), f(grid.m_factors["u"]),
                 f(grid.m_factors["v"]), f(grid.f_u), f(grid.f_v), f(grid.dm_dx_m), f(grid.dm_dy_m)]
+        # rho_bg None: the library takes the equation of state of theta_bg and pi_bg
+        if rho_bg is not None:
+            keep.append(f(rho_bg))
         b = _lib.SislBackground(*[t.data_ptr() for t in keep])
         h = ctypes.c_void_p()
         check(self.lib.sisl_core_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(b),

@@ -13,6 +13,7 @@ namespace sisl {
 struct Base64 {
   const double *theta_bg, *pi_bg, *Z_m, *dz_m, *dz_w, *z_xi_w, *z_eta_w, *tau;
   const double *m_m, *m_u, *m_v, *f_u, *f_v, *dmdx, *dmdy;
+  const double* rho;  // background density, NULL: the equation of state of theta_bg, pi_bg
 };
 
 // Physical and solver scalars.

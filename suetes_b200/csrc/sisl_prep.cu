@@ -57,6 +57,10 @@ namespace {
 __device__ __forceinline__ double rho_of(const Scalars& s, double th, double pi) {
   return s.p0 / (s.Rd * th) * pow(pi, s.cvd / s.Rd);  // steppers.py:770-771
 }
+// background density at mass point p: the caller's, else the equation of state
+__device__ __forceinline__ double rho_at(const Scalars& s, const Base64& b, int p) {
+  return b.rho ? b.rho[p] : rho_of(s, b.theta_bg[p], b.pi_bg[p]);
+}
 
 // One thread per point of the (nx+1, ny+1, nz+1) union box.
 template <typename T>
@@ -71,7 +75,7 @@ __global__ void prep_points(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
   if (i < nx && j < ny && k < nz) {
     const int p = im(d, i, j, k);
     const double th = b.theta_bg[p], pi = b.pi_bg[p];
-    const double rho = rho_of(s, th, pi);
+    const double rho = rho_at(s, b, p);
     const double cpi = (s.Rd / s.cvd) * (pi / (rho * th));
     const double dzm = b.dz_m[p];
     out.p[C_THB][p] = (T)th;
@@ -106,7 +110,7 @@ __global__ void prep_points(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
     face_pair(i, nx, d.px, l, r);
     const int pl = im(d, l, j, k), pr = im(d, r, j, k);
     const double th = 0.5 * (b.theta_bg[pl] + b.theta_bg[pr]);
-    const double rho = 0.5 * (rho_of(s, b.theta_bg[pl], b.pi_bg[pl]) + rho_of(s, b.theta_bg[pr], b.pi_bg[pr]));
+    const double rho = 0.5 * (rho_at(s, b, pl) + rho_at(s, b, pr));
     const double dzu = 0.5 * (b.dz_m[pl] + b.dz_m[pr]);
     const double mu = b.m_u[h_u(d, i, j)];
     const int p = iu(d, i, j, k);
@@ -120,7 +124,7 @@ __global__ void prep_points(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
     face_pair(j, ny, d.py, l, r);
     const int pl = im(d, i, l, k), pr = im(d, i, r, k);
     const double th = 0.5 * (b.theta_bg[pl] + b.theta_bg[pr]);
-    const double rho = 0.5 * (rho_of(s, b.theta_bg[pl], b.pi_bg[pl]) + rho_of(s, b.theta_bg[pr], b.pi_bg[pr]));
+    const double rho = 0.5 * (rho_at(s, b, pl) + rho_at(s, b, pr));
     const double dzv = 0.5 * (b.dz_m[pl] + b.dz_m[pr]);
     const double mv = b.m_v[h_v(d, i, j)];
     const int p = iv(d, i, j, k);
@@ -135,7 +139,7 @@ __global__ void prep_points(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
     const int pl = im(d, i, j, kl), pr = im(d, i, j, kr);
     const int p = iw(d, i, j, k);
     const double th = 0.5 * (b.theta_bg[pl] + b.theta_bg[pr]);
-    const double rho = 0.5 * (rho_of(s, b.theta_bg[pl], b.pi_bg[pl]) + rho_of(s, b.theta_bg[pr], b.pi_bg[pr]));
+    const double rho = 0.5 * (rho_at(s, b, pl) + rho_at(s, b, pr));
     const double dzw = b.dz_w[p];
     out.p[C_THW][p] = (T)th;
     out.p[C_RHOW][p] = (T)rho;
@@ -185,7 +189,7 @@ __global__ void prep_thomas(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
     if (K <= 0 || K >= nz) return 0.0;
     const int pl = im(d, i, j, K - 1), pr = im(d, i, j, K);
     const double th = 0.5 * (b.theta_bg[pl] + b.theta_bg[pr]);
-    const double rho = 0.5 * (rho_of(s, b.theta_bg[pl], b.pi_bg[pl]) + rho_of(s, b.theta_bg[pr], b.pi_bg[pr]));
+    const double rho = 0.5 * (rho_at(s, b, pl) + rho_at(s, b, pr));
     const int pw = iw(d, i, j, K);
     return s.alpha * s.dt * s.cp * th / (b.dz_w[pw] * (1.0 + s.dt * b.tau[pw])) * rho * th;
   };
@@ -193,7 +197,7 @@ __global__ void prep_thomas(Dims d, Scalars s, Base64 b, PtrTable<T> out) {
   for (int k = 0; k < nz; ++k) {
     const int p = im(d, i, j, k);
     const double th = b.theta_bg[p], pi = b.pi_bg[p];
-    const double cpi = (s.Rd / s.cvd) * (pi / (rho_of(s, th, pi) * th));
+    const double cpi = (s.Rd / s.cvd) * (pi / (rho_at(s, b, p) * th));
     const double L = s.alpha * s.dt * cpi / b.dz_m[p];
     const double Pk1 = Pw(k + 1);
     const double lower = -L * Pk, upper = -L * Pk1;

@@ -109,12 +109,13 @@ class Euler3D:
         """The CUDA core for a precision, time step, off-centring and background."""
         dt = self.dt if dt is None else float(dt)
         theta, pi = (self.theta_bg, self.pi_bg) if bg is None else (bg["th_v"], bg["pi_bg"])
-        key = (dtype, dt, float(alpha), id(theta), id(pi), bool(use_limiter))
+        rho = None if bg is None else bg.get("rho")
+        key = (dtype, dt, float(alpha), id(theta), id(pi), id(rho), bool(use_limiter))
         core = self._cores.get(key)
         if core is None:
             core = Core(self.grid, self.c, theta, pi, self.tau_damp, dtype, dt, alpha, self.nu_div, self.nu_h,
-                        periodic_axes=self.op.periodic_axes, solver=solver, use_limiter=use_limiter)
-            self._cores[key] = (core, theta, pi)  # keep the background alive while cached
+                        periodic_axes=self.op.periodic_axes, solver=solver, use_limiter=use_limiter, rho_bg=rho)
+            self._cores[key] = (core, theta, pi, rho)  # keep the background alive while cached
             return core
         return core[0]
 
@@ -125,21 +126,32 @@ class Euler3D:
         return {"rho": rho, "pi": self.pi_bg, "th_v": self.theta_bg}
 
     def precompute_bg(self, bg_state):
-        """``precompute_bg`` (euler.py:127-160): face-mapped background (float64)."""
+        """``precompute_bg`` (euler.py:127-160): face-mapped background
+        (float64), the reference's keys.  A density that is not the equation
+        of state of ``th_v`` and ``pi`` (to round-off) is also kept under
+        ``rho`` for the CUDA core's coefficients; otherwise the core forms
+        that density itself."""
         op, g = self.op, self.grid
         th, rho, pi = (torch.as_tensor(bg_state[k]).to(device=g.device, dtype=F64) for k in ("th_v", "rho", "pi"))
         if bg_state.get("th_v") is self.theta_bg and bg_state.get("pi") is self.pi_bg:
             th, pi = self.theta_bg, self.pi_bg
-        return {
+        c = self.c
+        eos = c["p0"] / (c["Rd"] * th) * pi ** (c["cvd"] / c["Rd"])
+        out = {
             "th_v_u": op.avg(th, 0, "m", "u"), "th_v_v": op.avg(th, 1, "m", "v"), "th_v_w": op.avg(th, 2, "m", "w"),
             "rho_u": op.avg(rho, 0, "m", "u"), "rho_v": op.avg(rho, 1, "m", "v"), "rho_w": op.avg(rho, 2, "m", "w"),
             "dz_m_full": g.dz_m_full, "dz_w_full": g.dz_w_full,
             "dz_u": op.avg(g.dz_m_full, 0, "m", "u"), "dz_v": op.avg(g.dz_m_full, 1, "m", "v"),
             "C_pi": (self.c["Rd"] / self.c["cvd"]) * (pi / (rho * th)), "pi_bg": pi, "th_v": th,
         }
+        if not torch.allclose(rho, eos, rtol=1e-13, atol=0.0):
+            out["rho"] = rho
+        return out
 
     def _bg_arg(self, bg):
-        if bg is None or (bg.get("th_v") is self.theta_bg and bg.get("pi_bg") is self.pi_bg):
+        if bg is None or bg.get("rho") is not None:
+            return bg
+        if bg.get("th_v") is self.theta_bg and bg.get("pi_bg") is self.pi_bg:
             return None
         if torch.equal(bg["th_v"], self.theta_bg) and torch.equal(bg["pi_bg"], self.pi_bg):
             return None
