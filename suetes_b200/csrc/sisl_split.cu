@@ -366,21 +366,22 @@ __global__ void __launch_bounds__(128) split_column_kernel(Dims d, Coef<T> c, Sp
 // The same column solve on tiles of PC columns (one block per tile and
 // row j) so that every thread works outside the recurrence: A1 the w-level
 // terms (explicit w'', the eta_dot flux, the coupling gamma) and A2 the
-// tridiagonal rows at every (level, column) pair, B one warp runs the
-// Thomas sweeps in shared memory, C the pi'' and w'' updates.  Arithmetic
-// is term for term that of split_column_kernel.
+// right-hand sides at every (level, column) pair, B one warp runs the
+// Thomas sweeps in shared memory, forming each row (lower, upper, main)
+// from gamma and C_pi / dz_m, C the pi'' and w'' updates.  Arithmetic is
+// term for term that of split_column_kernel.  Shared memory: (4 nz + 2) PC
+// values (c' overwrites the eta_dot fluxes once the right-hand sides are
+// formed).
 template <typename T, int PT, int PC>
 __global__ void __launch_bounds__(PT) split_column_tile_kernel(Dims d, Coef<T> c, SplitArgs<T> a, T a2cp,
                                                                T adcp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int nx = d.nx, nz = d.nz;
-  T* s_fz = sm;                      // [nz+1][PC]  eta_dot flux
+  T* s_fz = sm;                      // [nz+1][PC]  eta_dot flux -> c'
   T* s_gam = s_fz + (nz + 1) * PC;   // [nz+1][PC]  gamma
   T* s_x = s_gam + (nz + 1) * PC;    // [nz][PC]    rhs -> d' -> delta pi
-  T* s_lo = s_x + nz * PC;           // [nz][PC]    lower
-  T* s_up = s_lo + nz * PC;          // [nz][PC]    upper -> c'
-  T* s_mn = s_up + nz * PC;          // [nz][PC]    main
+  T* s_cz = s_x + nz * PC;           // [nz][PC]    C_pi / dz_m
   const int i0 = blockIdx.x * PC, j = blockIdx.y, tid = threadIdx.x;
   const T al = a.alpha, dtau = a.dtau, cp = (T)c.s.cp;
   const T dx = (T)d.dx, dy = (T)d.dy;
@@ -405,11 +406,9 @@ __global__ void __launch_bounds__(PT) split_column_tile_kernel(Dims d, Coef<T> c
   __syncthreads();
   for (int q = tid; q < nz * PC; q += PT) {  // A2
     const int k = q / PC, i = i0 + q % PC;
-    if (i >= nx) {
+    if (i >= nx) {  // a trivial row: lower = upper = 0, main = 1
       s_x[q] = T(0);
-      s_lo[q] = T(0);
-      s_up[q] = T(0);
-      s_mn[q] = T(1);
+      s_cz[q] = T(0);
       continue;
     }
     const int p = im(d, i, j, k);
@@ -423,28 +422,27 @@ __global__ void __launch_bounds__(PT) split_column_tile_kernel(Dims d, Coef<T> c
     const T div_h = mm * ((fx1 - fx0) / dx * mm / dzm + (fy1 - fy0) / dy * mm / dzm);
     const T div_z = (s_fz[q + PC] - s_fz[q]) / dzm;
     s_x[q] = dtau * (a.sfp[p] - cpidz * dzm * (div_h + div_z));
-    const T lower = -cpidz * s_gam[q], upper = -cpidz * s_gam[q + PC];
-    s_lo[q] = lower;
-    s_up[q] = upper;
-    s_mn[q] = T(1) - lower - upper;
+    s_cz[q] = cpidz;
   }
   __syncthreads();
   if (tid < PC) {  // B
     T cprev = T(0), dprev = T(0);
     for (int k = 0; k < nz; ++k) {
       const int q = k * PC + tid;
+      const T cpidz = s_cz[q];
+      const T lower = -cpidz * s_gam[q], upper = -cpidz * s_gam[q + PC];
+      const T mainv = T(1) - lower - upper;
       T cpk, dpk;
       if (k == 0) {
-        const T inv = T(1) / s_mn[q];
-        cpk = s_up[q] * inv;
+        const T inv = T(1) / mainv;
+        cpk = upper * inv;
         dpk = s_x[q] * inv;
       } else {
-        const T lower = s_lo[q];
-        const T inv = T(1) / (s_mn[q] - lower * cprev);
-        cpk = s_up[q] * inv;
+        const T inv = T(1) / (mainv - lower * cprev);
+        cpk = upper * inv;
         dpk = (s_x[q] - lower * dprev) * inv;
       }
-      s_up[q] = cpk;
+      s_fz[q] = cpk;
       s_x[q] = dpk;
       cprev = cpk;
       dprev = dpk;
@@ -452,7 +450,7 @@ __global__ void __launch_bounds__(PT) split_column_tile_kernel(Dims d, Coef<T> c
     T xh = dprev;
     for (int k = nz - 2; k >= 0; --k) {
       const int q = k * PC + tid;
-      xh = s_x[q] - s_up[q] * xh;
+      xh = s_x[q] - s_fz[q] * xh;
       s_x[q] = xh;
     }
   }
@@ -600,7 +598,7 @@ void launch_split_column(const Dims& d, const Coef<T>& c, const SplitArgs<T>& a,
   const double ad = (double)a.alpha * (double)a.dtau;
   const T a2cp = (T)(ad * ad * c.s.cp), adcp = (T)(ad * c.s.cp);
   constexpr int PT = 256, PC = 32;
-  const size_t smem = (size_t)(6 * d.nz + 2) * PC * sizeof(T);
+  const size_t smem = (size_t)(4 * d.nz + 2) * PC * sizeof(T);
   if (smem <= 200 * 1024) {  // tiles of 32 columns; the one-thread-per-column march beyond
     static SmemLimit attr_bytes;  // per instantiation
     ensure_smem_limit((const void*)split_column_tile_kernel<T, PT, PC>, attr_bytes, smem);
