@@ -82,55 +82,73 @@ struct AdvFields {
   }
 };
 
+// Blocks of AX x AY mass points of one level.  For each of the four fields
+// the block forms the field's values at the (AX + 4) x (AY + 4) cells of its
+// x and y stencils once into shared memory (indices wrapped or clamped as
+// the point form wraps them), instead of five times per point and axis; the
+// z stencil is read per point.
+constexpr int AX = 32, AY = 8;
+
 template <typename T>
-__global__ void __launch_bounds__(256) split_adv_kernel(Dims d, Coef<T> c, const T* __restrict__ u,
-                                                        const T* __restrict__ v, const T* __restrict__ w,
-                                                        const T* __restrict__ eta, const T* __restrict__ th,
-                                                        T eps_l, PtrTable<T> out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+__global__ void __launch_bounds__(AX * AY) split_adv_kernel(Dims d, Coef<T> c, const T* __restrict__ u,
+                                                            const T* __restrict__ v, const T* __restrict__ w,
+                                                            const T* __restrict__ eta, const T* __restrict__ th,
+                                                            T eps_l, PtrTable<T> out) {
+  __shared__ T Qt[AY + 4][AX + 4];
+  const int i0 = blockIdx.x * AX, j0 = blockIdx.y * AY, k = blockIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = i0 + tx, j = j0 + ty;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  if (i >= nx || j >= ny || k >= nz) return;
+  const bool live = i < nx && j < ny;
   const AdvFields<T> F{d, u, v, w, th};
-  const T mm = ld(c.mm, h_m(d, i, j));
   const T dx = (T)d.dx, dy = (T)d.dy;
-  // U = u / m_u, V = v / m_v, W = eta dz_w at the cell's faces (steppers.py:1397-1399)
-  const T U0 = ld(u, iu(d, i, j, k)) / ld(c.mu, h_u(d, i, j));
-  const T U1 = ld(u, iu(d, i + 1, j, k)) / ld(c.mu, h_u(d, i + 1, j));
-  const T V0 = ld(v, iv(d, i, j, k)) / ld(c.mv, h_v(d, i, j));
-  const T V1 = ld(v, iv(d, i, j + 1, k)) / ld(c.mv, h_v(d, i, j + 1));
-  const T W0 = ld(eta, iw(d, i, j, k)) * ld(c.dzw, iw(d, i, j, k));
-  const T W1 = ld(eta, iw(d, i, j, k + 1)) * ld(c.dzw, iw(d, i, j, k + 1));
-  const T dzm = ld(c.dzm, im(d, i, j, k));
-  const T zfac = (T)d.dz / dzm;
-  const T dU = (U1 - U0) / dx * mm, dV = (V1 - V0) / dy * mm;
-  const T dW = (W1 - W0) / (T)d.dz * zfac;
-  int xi[5], yj[5], zk[5];
-#pragma unroll
-  for (int o = 0; o < 5; ++o) {
-    xi[o] = wrap_or_clamp(i - 2 + o, nx, d.px);
-    yj[o] = wrap_or_clamp(j - 2 + o, ny, d.py);
-    zk[o] = min(max(k - 2 + o, 0), nz - 1);
+  T mm = T(0), U0 = T(0), U1 = T(0), V0 = T(0), V1 = T(0), W0 = T(0), W1 = T(0), zfac = T(0);
+  T dU = T(0), dV = T(0), dW = T(0);
+  int zk[5];
+  if (live) {
+    mm = ld(c.mm, h_m(d, i, j));
+    // U = u / m_u, V = v / m_v, W = eta dz_w at the cell's faces (steppers.py:1397-1399)
+    U0 = ld(u, iu(d, i, j, k)) / ld(c.mu, h_u(d, i, j));
+    U1 = ld(u, iu(d, i + 1, j, k)) / ld(c.mu, h_u(d, i + 1, j));
+    V0 = ld(v, iv(d, i, j, k)) / ld(c.mv, h_v(d, i, j));
+    V1 = ld(v, iv(d, i, j + 1, k)) / ld(c.mv, h_v(d, i, j + 1));
+    W0 = ld(eta, iw(d, i, j, k)) * ld(c.dzw, iw(d, i, j, k));
+    W1 = ld(eta, iw(d, i, j, k + 1)) * ld(c.dzw, iw(d, i, j, k + 1));
+    const T dzm = ld(c.dzm, im(d, i, j, k));
+    zfac = (T)d.dz / dzm;
+    dU = (U1 - U0) / dx * mm;
+    dV = (V1 - V0) / dy * mm;
+    dW = (W1 - W0) / (T)d.dz * zfac;
   }
+#pragma unroll
+  for (int o = 0; o < 5; ++o) zk[o] = min(max(k - 2 + o, 0), nz - 1);
+  const int t = tx + AX * ty;
 #pragma unroll 1
   for (int f = 0; f < 4; ++f) {
-    T qx[5], qy[5], qz[5];
-#pragma unroll
-    for (int o = 0; o < 5; ++o) {
-      qx[o] = F.at(f, xi[o], j, k);
-      qy[o] = F.at(f, i, yj[o], k);
-      qz[o] = F.at(f, i, j, zk[o]);
+    for (int q = t; q < (AX + 4) * (AY + 4); q += AX * AY) {
+      const int x = q % (AX + 4), y = q / (AX + 4);
+      Qt[y][x] = F.at(f, wrap_or_clamp(i0 - 2 + x, nx, d.px), wrap_or_clamp(j0 - 2 + y, ny, d.py), k);
     }
-    const T q = qx[2];
-    // faces i (q at i-2..i+1) and i+1 (q at i-1..i+2)
-    const T ax = (upwind_flux(qx[1], qx[2], qx[3], qx[4], U1, eps_l) -
-                  upwind_flux(qx[0], qx[1], qx[2], qx[3], U0, eps_l)) / dx * mm;
-    const T ay = (upwind_flux(qy[1], qy[2], qy[3], qy[4], V1, eps_l) -
-                  upwind_flux(qy[0], qy[1], qy[2], qy[3], V0, eps_l)) / dy * mm;
-    const T az = (upwind_flux(qz[1], qz[2], qz[3], qz[4], W1, eps_l) -
-                  upwind_flux(qz[0], qz[1], qz[2], qz[3], W0, eps_l)) / (T)d.dz * zfac;
-    out.p[f][im(d, i, j, k)] = -(mm * mm) * (ax - q * dU + ay - q * dV) - (az - q * dW);
+    __syncthreads();
+    if (live) {
+      T qx[5], qy[5], qz[5];
+#pragma unroll
+      for (int o = 0; o < 5; ++o) {
+        qx[o] = Qt[ty + 2][tx + o];
+        qy[o] = Qt[ty + o][tx + 2];
+        qz[o] = (o == 2) ? Qt[ty + 2][tx + 2] : F.at(f, i, j, zk[o]);
+      }
+      const T q = qx[2];
+      // faces i (q at i-2..i+1) and i+1 (q at i-1..i+2)
+      const T ax = (upwind_flux(qx[1], qx[2], qx[3], qx[4], U1, eps_l) -
+                    upwind_flux(qx[0], qx[1], qx[2], qx[3], U0, eps_l)) / dx * mm;
+      const T ay = (upwind_flux(qy[1], qy[2], qy[3], qy[4], V1, eps_l) -
+                    upwind_flux(qy[0], qy[1], qy[2], qy[3], V0, eps_l)) / dy * mm;
+      const T az = (upwind_flux(qz[1], qz[2], qz[3], qz[4], W1, eps_l) -
+                    upwind_flux(qz[0], qz[1], qz[2], qz[3], W0, eps_l)) / (T)d.dz * zfac;
+      out.p[f][im(d, i, j, k)] = -(mm * mm) * (ax - q * dU + ay - q * dV) - (az - q * dW);
+    }
+    __syncthreads();  // the next field refills the tile
   }
 }
 
@@ -565,7 +583,7 @@ void launch_split_diag(const Dims& d, const Coef<T>& c, const T* u, const T* v, 
 template <typename T>
 void launch_split_adv(const Dims& d, const Coef<T>& c, const T* u, const T* v, const T* w, const T* eta,
                       const T* th, T eps_l, T* const* adv4, cudaStream_t st) {
-  const dim3 blk(32, 4, 2);
+  const dim3 blk(AX, AY, 1);
   PtrTable<T> o{};
   for (int q = 0; q < 4; ++q) o.p[q] = adv4[q];
   split_adv_kernel<T><<<box(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, c, u, v, w, eta, th, eps_l, o);
