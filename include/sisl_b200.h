@@ -281,6 +281,10 @@ int sisl_ffsl_lines(int dtype, int n, int nlines, const void* scalar, const void
 #define SISL_FFSL_NOALLOC_MAX_DOUBLES (1 << 20)
 int sisl_ffsl_lines_noalloc(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic,
                             void* out, void* stream);
+/* Euler3D.metric_curvature_tendencies(u, v) (euler.py:188-206): the
+ * map-curvature accelerations at the u faces (out_u) and v faces (out_v),
+ * device layout.  No workspace. */
+int sisl_metric_curvature(SislCore* core, const void* u, const void* v, void* out_u, void* out_v, void* stream);
 /* Euler3D.get_tendencies(state_prime, bg, is_explicit) (euler.py:208-372):
  * is_explicit = 0 gives the linear tendencies of the implicit operator.
  * Same arguments as sisl_explicit_tendencies. */

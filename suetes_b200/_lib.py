@@ -121,6 +121,7 @@ PROTOTYPES = {
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, vp, vp, vp, vp]),
     "sisl_explicit_tendencies": (ctypes.c_int, [vp, vp * 6, vp * 6, vp, vp, ctypes.c_size_t, vp]),
     "sisl_tendencies": (ctypes.c_int, [vp, ctypes.c_int, vp * 6, vp * 6, vp, vp, ctypes.c_size_t, vp]),
+    "sisl_metric_curvature": (ctypes.c_int, [vp, vp, vp, vp, vp, vp]),
     "sisl_trilinear": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32 * 3, vp, ctypes.c_int32 * 3, vp * 3, vp, vp]),
     "sisl_ffsl_lines_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
     "sisl_ffsl_lines": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp,

@@ -2159,6 +2159,19 @@ int sisl_explicit_tendencies(SislCore* c, const void* const sp[6], void* const t
   return sisl_tendencies(c, 1, sp, tend, pd, ws, ws_bytes, stream);
 }
 
+int sisl_metric_curvature(SislCore* c, const void* u, const void* v, void* out_u, void* out_v, void* stream) {
+  if (!c || !u || !v || !out_u || !out_v) return SISL_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  KScope k(c, SISL_K_EXPLICIT, st);
+  if (c->grid.dtype == SISL_F64)
+    launch_curvature<double>(c->d, coef_of<double>(c), (const double*)u, (const double*)v, (double*)out_u,
+                             (double*)out_v, st);
+  else
+    launch_curvature<float>(c->d, coef_of<float>(c), (const float*)u, (const float*)v, (float*)out_u,
+                            (float*)out_v, st);
+  return check_cuda();
+}
+
 int sisl_tendencies(SislCore* c, int is_explicit, const void* const sp[6], void* const tend[6],
                     void* const pd[4], void* ws, size_t ws_bytes, void* stream) {
   if (!c || !sp || !tend) return SISL_ERR_ARG;

@@ -382,6 +382,40 @@ void launch_hdiv(const Dims& d, const Coef<T>& c, const T* u, const T* v, T* div
   hdiv_kernel<T><<<box_grid(d.nx, d.ny, d.nz, blk), blk, 0, st>>>(d, c, u, v, div);
 }
 
+// Euler3D.metric_curvature_tendencies (euler.py:188-206): the map-curvature
+// accelerations metric_u v_at_u at the u faces and -metric_v u_at_v at the
+// v faces, metric = v_m dm/dx - u_m dm/dy at mass points averaged to the
+// faces (edge padded) -- the term the explicit kernel adds to its u and v
+// tendencies, on its own.  One thread per (i, j, k) of the union box.
+template <typename T>
+__global__ void curvature_kernel(Dims d, Coef<T> c, const T* __restrict__ u, const T* __restrict__ v,
+                                 T* __restrict__ ou, T* __restrict__ ov) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int nx = d.nx, ny = d.ny;
+  if (i > nx || j > ny || k >= d.nz) return;
+  const Winds<T> W{d, c, u, v};
+  if (j < ny) {
+    int l, r;
+    face_pair(i, nx, d.px, l, r);
+    const T vat = T(0.5) * (W.vm(l, j, k) + W.vm(r, j, k));
+    ou[iu(d, i, j, k)] = T(0.5) * (W.metric_m(l, j, k) + W.metric_m(r, j, k)) * vat;
+  }
+  if (i < nx) {
+    int l, r;
+    face_pair(j, ny, d.py, l, r);
+    const T uat = T(0.5) * (W.um(i, l, k) + W.um(i, r, k));
+    ov[iv(d, i, j, k)] = -(T(0.5) * (W.metric_m(i, l, k) + W.metric_m(i, r, k))) * uat;
+  }
+}
+
+template <typename T>
+void launch_curvature(const Dims& d, const Coef<T>& c, const T* u, const T* v, T* ou, T* ov, cudaStream_t st) {
+  dim3 blk(32, 4, 2);
+  curvature_kernel<T><<<box_grid(d.nx + 1, d.ny + 1, d.nz, blk), blk, 0, st>>>(d, c, u, v, ou, ov);
+}
+
 template <typename T>
 void launch_finalize(const Dims& d, const Coef<T>& c, const FinalizeArgs<T>& fa, cudaStream_t st) {
   dim3 blk(32, 4, 2);
@@ -398,7 +432,8 @@ void launch_finalize(const Dims& d, const Coef<T>& c, const FinalizeArgs<T>& fa,
   template void launch_corrector_rhs<T>(const Dims&, const Coef<T>&, const CorrectorIn<T>&, Vec5<T>,         \
                                         cudaStream_t);                                                         \
   template void launch_hdiv<T>(const Dims&, const Coef<T>&, const T*, const T*, T*, cudaStream_t);             \
-  template void launch_finalize<T>(const Dims&, const Coef<T>&, const FinalizeArgs<T>&, cudaStream_t);
+  template void launch_finalize<T>(const Dims&, const Coef<T>&, const FinalizeArgs<T>&, cudaStream_t);       \
+  template void launch_curvature<T>(const Dims&, const Coef<T>&, const T*, const T*, T*, T*, cudaStream_t);
 SISL_INST_EX(float)
 SISL_INST_EX(double)
 

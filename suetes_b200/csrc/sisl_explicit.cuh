@@ -57,6 +57,9 @@ void launch_hyper(const Dims& d, const Coef<T>& c, const T* u, const T* v, const
 template <typename T>
 void launch_explicit(const Dims& d, const Coef<T>& c, const ExplicitIn<T>& in, const ExplicitOut<T>& out, int mode,
                      cudaStream_t st);
+// map-curvature accelerations at the u and v faces (euler.py:188-206)
+template <typename T>
+void launch_curvature(const Dims& d, const Coef<T>& c, const T* u, const T* v, T* ou, T* ov, cudaStream_t st);
 template <typename T>
 void launch_corrector_theta(const Dims& d, const Coef<T>& c, const T* th_adv, const T* tth, const T* w_now,
                             const T* w_next, T* th_next, cudaStream_t st);

@@ -265,3 +265,14 @@ class Euler3D:
         sp.setdefault("pi", torch.zeros(self.grid.shape, dtype=self._dtype_of(state_prime), device=self.grid.device))
         (_, _, _, _, _, nl), _ = self._tendencies(sp, th_v_prime, bg, True)
         return nl
+
+    def metric_curvature_tendencies(self, u, v):
+        """Map-curvature accelerations (metric_u v_at_u, -metric_v u_at_v) at
+        the u and v faces (euler.py:188-206), ``sisl_metric_curvature``."""
+        dtype = self._dtype_of({"u": u, "v": v})
+        core = self.core(dtype, self.dt, 0.55)
+        ins = [core.field(u, "u"), core.field(v, "v")]
+        outs = [core.new("u"), core.new("v")]
+        check(core.lib.sisl_metric_curvature(core.handle, ins[0].data_ptr(), ins[1].data_ptr(), outs[0].data_ptr(),
+                                             outs[1].data_ptr(), core.stream), "sisl_metric_curvature")
+        return outs[0], outs[1]

@@ -310,3 +310,19 @@ def test_gmres_float32_refinement_reaches_float64_accuracy(mountain_pair):
     plain = SemiImplicitSolver3D(pph, 100.0, refine=False, **kw)
     plain.solve(r32, bg)
     assert not plain.last_info["converged"]
+
+
+@pytest.mark.parametrize("periodic", [(), (0,), (0, 1)])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_metric_curvature_tendencies(periodic, dtype):
+    """Euler3D.metric_curvature_tendencies (euler.py:188-206) on a 1500 km
+    box at 60N, where the map-factor gradients are large."""
+    kw = dict(lat=60.0, lon=30.0, h=mountain, periodic=periodic, dt=60.0)
+    o = build("oracle", 16, 12, 6, 100000.0, 100000.0, 1000.0, **kw)
+    p = build("cuda", 16, 12, 6, 100000.0, 100000.0, 1000.0, device="cuda", **kw)
+    x = random_fields({"u": (17, 12, 6), "v": (16, 13, 6)}, 21, {"u": 20.0, "v": 20.0})
+    ru, rv = o[2].metric_curvature_tendencies(x["u"], x["v"])
+    pu, pv = p[2].metric_curvature_tendencies(x["u"].to("cuda", dtype), x["v"].to("cuda", dtype))
+    assert float(ru.abs().max()) > 0.0 and float(rv.abs().max()) > 0.0
+    assert rel_l2(pu, ru) < TOL[dtype], rel_l2(pu, ru)
+    assert rel_l2(pv, rv) < TOL[dtype], rel_l2(pv, rv)
