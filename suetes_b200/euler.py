@@ -7,6 +7,7 @@ dictionary (for user scripts); the kernels themselves read the coefficient
 set that ``sisl_core_create`` derives once per (precision, dt, alpha).
 """
 
+import collections
 import ctypes
 import math
 
@@ -15,6 +16,9 @@ import torch
 from . import _lib
 from ._lib import check, ptrs
 from .core import F64, Core, fortran
+
+# cores kept per Euler3D for backgrounds other than its own (most recently used)
+BG_CORE_CACHE = 4
 
 
 def jnp_interp(x, xp, fp):
@@ -101,7 +105,8 @@ class Euler3D:
             zw > damp_height,
             max_damp * 0.5 * (1.0 + torch.tanh(math.pi * (zw - damp_height) / (grid.Lz - damp_height) - math.pi / 2)),
             torch.zeros_like(zw))
-        self._cores = {}
+        self._cores = {}  # cores of this physics' own background
+        self._bg_cores = collections.OrderedDict()  # other backgrounds, least recently used first
         self.diffusion = HyperFilter(grid, operators, nu_h=self.nu_h, nu_v=0.0, physics=self)  # euler.py:124
 
     # ------------------------------------------------------------------
@@ -111,13 +116,22 @@ class Euler3D:
         theta, pi = (self.theta_bg, self.pi_bg) if bg is None else (bg["th_v"], bg["pi_bg"])
         rho = None if bg is None else bg.get("rho")
         key = (dtype, dt, float(alpha), id(theta), id(pi), id(rho), bool(use_limiter))
-        core = self._cores.get(key)
-        if core is None:
-            core = Core(self.grid, self.c, theta, pi, self.tau_damp, dtype, dt, alpha, self.nu_div, self.nu_h,
-                        periodic_axes=self.op.periodic_axes, solver=solver, use_limiter=use_limiter, rho_bg=rho)
-            self._cores[key] = (core, theta, pi, rho)  # keep the background alive while cached
-            return core
-        return core[0]
+        own = theta is self.theta_bg and pi is self.pi_bg and rho is None
+        cache = self._cores if own else self._bg_cores
+        hit = cache.get(key)
+        if hit is not None:
+            if not own:
+                cache.move_to_end(key)
+            return hit[0]
+        core = Core(self.grid, self.c, theta, pi, self.tau_damp, dtype, dt, alpha, self.nu_div, self.nu_h,
+                    periodic_axes=self.op.periodic_axes, solver=solver, use_limiter=use_limiter, rho_bg=rho)
+        cache[key] = (core, theta, pi, rho)  # keep the background alive while cached
+        # a fresh precompute_bg dict per call is a new background: keep only
+        # the most recent few of those cores (their coefficients are a
+        # full set of 3-D arrays each)
+        while not own and len(cache) > BG_CORE_CACHE:
+            cache.popitem(last=False)
+        return core
 
     def bg_state_ref(self):
         """Background dict built inside ``step`` (steppers.py:769-774)."""
