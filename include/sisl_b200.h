@@ -22,7 +22,9 @@
  *    th_p = th_v - theta_bg.
  *  - Streams are cudaStream_t passed as void*; NULL is the legacy stream.
  *  - Outputs are caller-allocated; scratch comes from a caller-provided
- *    workspace of sisl_workspace_bytes() bytes (256-byte aligned).
+ *    workspace of sisl_workspace_bytes() bytes (256-byte aligned
+ *    recommended; an absent, short or not 16-byte aligned workspace returns
+ *    SISL_ERR_WORKSPACE before any launch).
  *  - Return value: SISL_OK, a negative error code, or SISL_NOT_CONVERGED
  *    (the GMRES iteration limit was hit; outputs are still written, as in
  *    the reference, which discards GMRES's status at steppers.py:466).

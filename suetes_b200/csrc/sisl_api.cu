@@ -58,6 +58,13 @@ namespace {
 
 size_t esize(int dtype) { return dtype == SISL_F64 ? 8 : 4; }
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+// a workspace the entry points can carve: present, large enough, and
+// 16-byte aligned -- the arrays are carved at multiples of 256 bytes from
+// its start, so each keeps the start's alignment, and the kernels' 16-byte
+// vector loads and stores need that much (a misaligned one would fault)
+inline bool ws_bad(const void* ws, size_t have, size_t need) {
+  return !ws || ((uintptr_t)ws & 15) != 0 || have < need;
+}
 size_t pad64(size_t x) { return (x + 63) & ~(size_t)63; }
 
 // Scoped launch bookkeeping: counts kernels and, for the selected class,
@@ -1837,7 +1844,7 @@ size_t sisl_workspace_bytes(const SislCore* c, int what) {
 int sisl_linear_operator(SislCore* c, const void* const in[5], void* const out[5], void* ws, size_t ws_bytes,
                          void* stream) {
   if (!c || !in || !out) return SISL_ERR_ARG;
-  if (ws_bytes < sisl_workspace_bytes(c, SISL_WS_OPERATOR) || !ws) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_OPERATOR))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv{(char*)ws};
   auto run = [&](auto tag) {
@@ -1888,7 +1895,7 @@ int sisl_precond_apply(SislCore* c, const void* const in[5], void* const out[5],
 int sisl_gmres_solve(SislCore* c, const void* const rhs[5], const void* const x0[5], void* const x[5], void* ws,
                      size_t ws_bytes, void* stream, SislSolveInfo* info) {
   if (!c || !rhs || !x) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_GMRES)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_GMRES))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv{(char*)ws};
   int rc;
@@ -1914,7 +1921,7 @@ int sisl_helmholtz_matvec_t(SislCore* c, const void* const in[5], void* const ou
   if (!c || !in || !out) return SISL_ERR_ARG;
   for (int q = 0; q < 5; ++q)
     if (in[q] == out[q]) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_OPERATOR)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_OPERATOR))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   KScope k(c, SISL_K_MATVEC, st, 2);
   if (c->grid.dtype == SISL_F64)
@@ -1942,7 +1949,7 @@ int sisl_precond_apply_t(SislCore* c, const void* const in[5], void* const out[5
 int sisl_gmres_solve_transpose(SislCore* c, const void* const xbar[5], const void* const x0[5],
                                void* const bbar[5], void* ws, size_t ws_bytes, void* stream, SislSolveInfo* info) {
   if (!c || !xbar || !bbar) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_GMRES)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_GMRES))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv{(char*)ws};
   int rc;
@@ -1966,7 +1973,7 @@ int sisl_gmres_solve_transpose(SislCore* c, const void* const xbar[5], const voi
 int sisl_departure(SislCore* c, int loc, const void* u, const void* v, const void* eta, int iterations,
                    void* const coords[3], void* ws, size_t ws_bytes, void* stream) {
   if (!c || loc < 0 || loc > 3 || !u || !v || !eta || !coords || iterations < 0) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_DEPARTURE)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_DEPARTURE))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv{(char*)ws};
   auto run = [&](auto tag) {
@@ -2115,7 +2122,7 @@ size_t sisl_ffsl_lines_workspace_bytes(int n, int nlines) {
 int sisl_ffsl_lines(int dtype, int n, int nlines, const void* scalar, const void* cfl, int periodic, void* out,
                     void* ws, size_t ws_bytes, void* stream) {
   if (n < 1 || nlines < 1 || !scalar || !cfl || !out) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_ffsl_lines_workspace_bytes(n, nlines)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_ffsl_lines_workspace_bytes(n, nlines))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   KScope k(nullptr, SISL_K_OTHER, st);
   if (dtype == SISL_F64)
@@ -2138,7 +2145,7 @@ int sisl_ffsl_lines_vjp(int dtype, int n, int nlines, const void* scalar, const 
                         const void* out_bar, void* scalar_bar, void* cfl_bar, void* ws, size_t ws_bytes,
                         void* stream) {
   if (n < 1 || nlines < 1 || !scalar || !cfl || !out_bar || !scalar_bar) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_ffsl_lines_vjp_workspace_bytes(n, nlines)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_ffsl_lines_vjp_workspace_bytes(n, nlines))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   double* M = (double*)ws;
   double* Mb = (double*)((char*)ws + align256(sizeof(double) * (size_t)(n + 1) * nlines));
@@ -2175,7 +2182,7 @@ int sisl_metric_curvature(SislCore* c, const void* u, const void* v, void* out_u
 int sisl_tendencies(SislCore* c, int is_explicit, const void* const sp[6], void* const tend[6],
                     void* const pd[4], void* ws, size_t ws_bytes, void* stream) {
   if (!c || !sp || !tend) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_EXPLICIT)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_EXPLICIT))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv{(char*)ws};
   auto run = [&](auto tag) {
@@ -2219,7 +2226,7 @@ int sisl_step_taped(SislCore* c, const SislState* in, const SislState* out, cons
   const void* need_out[] = {out->u, out->v, out->w, out->eta_dot, out->pi_p, out->th_p};
   for (const void* p : need_out)
     if (!p) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_STEP)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_STEP))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64) return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info, solves);
   return step_impl<float>(c, in, out, relax, ws, ws_bytes, st, info, solves);
@@ -2236,7 +2243,7 @@ int sisl_step_physics(SislCore* c, const SislState* in, const SislState* out, co
   const void* need_out[] = {out->u, out->v, out->w, out->eta_dot, out->pi_p, out->th_p};
   for (const void* p : need_out)
     if (!p) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_STEP)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_STEP))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64)
     return step_impl<double>(c, in, out, relax, ws, ws_bytes, st, info, solves, nullptr, phys_tend);
@@ -2260,7 +2267,7 @@ int sisl_step_vjp(SislCore* c, const SislState* in, void* const solves[10], cons
                 ((relax->fields & SISL_RELAX_U) && !relax->mask_u) ||
                 ((relax->fields & SISL_RELAX_V) && !relax->mask_v)))
     return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_STEP_VJP)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_STEP_VJP))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64)
     return step_vjp_impl<double>(c, in, solves, relax, out_bar, in_bar, ws, ws_bytes, st, info);
@@ -2273,7 +2280,7 @@ int sisl_explicit_tendencies_vjp(SislCore* c, const void* const sp[6], const voi
   if (!c || !sp || !tend_bar || !sp_bar) return SISL_ERR_ARG;
   for (int q = 0; q < 6; ++q)
     if (!sp[q] || !sp_bar[q]) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_EXPLICIT_VJP)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_EXPLICIT_VJP))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   static const int LOCS[6] = {LOC_U, LOC_V, LOC_W, LOC_M, LOC_W, LOC_M};
   Carver cv{(char*)ws};
@@ -2738,7 +2745,7 @@ int capture_grouped_vjp(int n, SislCore* const* cores, const SislState* ins, voi
 int check_members(int n, SislCore* const* cores, void* const* ws, const size_t* ws_bytes, int ws_kind) {
   for (int m = 0; m < n; ++m) {
     SislCore* c = cores[m];
-    if (!c || !ws[m] || ws_bytes[m] < sisl_workspace_bytes(c, ws_kind)) return SISL_ERR_WORKSPACE;
+    if (!c || ws_bad(ws[m], ws_bytes[m], sisl_workspace_bytes(c, ws_kind))) return SISL_ERR_WORKSPACE;
     for (int q = 0; q < m; ++q)
       if (cores[q] == c) return SISL_ERR_ARG;
   }
@@ -2979,7 +2986,7 @@ extern "C" {
 
 int sisl_autotune(SislCore* c, void* ws, size_t ws_bytes, void* stream, SislTuning* out) {
   if (!c || !out) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_GMRES)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_GMRES))) return SISL_ERR_WORKSPACE;
   if (c->timing_class != SISL_K_NONE) return SISL_ERR_ARG;
   std::memset(out, 0, sizeof(*out));
   cudaStream_t st = (cudaStream_t)stream;
@@ -3031,7 +3038,7 @@ int sisl_split_diagnose_vjp(SislCore* c, const void* w_out_bar, const void* eta_
                             void* w_in_bar, void* ws, size_t ws_bytes, void* stream) {
   if (!c || !w_out_bar || !eta_bar || !u_bar || !v_bar || !w_in_bar) return SISL_ERR_ARG;
   if (w_in_bar == eta_bar || u_bar == v_bar) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_SPLIT_VJP)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_SPLIT_VJP))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   auto run = [&](auto tag) -> int {
     using T = decltype(tag);
@@ -3064,7 +3071,7 @@ int sisl_split_step(SislCore* c, const SislState* in, const SislState* out, int 
     for (const void* q : need_in)
       if (p == q) return SISL_ERR_ARG;  // out must not alias in
   }
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_SPLIT)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_SPLIT))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64)
     split_step_impl<double>(c, in, out, ns, alpha, eps_l, (const double*)tau_damp, phys_tend, ws, st);
@@ -3090,7 +3097,7 @@ int sisl_split_step_vjp(SislCore* c, const SislState* in, const SislState* out_b
     for (const void* q : obar)
       if (p == q) return SISL_ERR_ARG;
   }
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_SPLIT_VJP)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_SPLIT_VJP))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   if (c->grid.dtype == SISL_F64)
     return split_vjp_impl<double>(c, in, out_bar, in_bar, ns, alpha, eps_l, (const double*)tau_damp, deterministic, ws,
@@ -3102,7 +3109,7 @@ int sisl_split_step_vjp(SislCore* c, const SislState* in, const SislState* out_b
 int sisl_ffsl_advect(SislCore* c, const void* field, const void* u, const void* v, const void* eta, void* out,
                      void* ws, size_t ws_bytes, void* stream) {
   if (!c || !field || !u || !v || !eta || !out) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_FFSL)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_FFSL))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv{(char*)ws};
   auto run = [&](auto tag) {
@@ -3123,7 +3130,7 @@ int sisl_ffsl_advect_vjp(SislCore* c, const void* field, const void* u, const vo
                          const void* out_bar, void* field_bar, void* u_bar, void* v_bar, void* eta_bar, void* ws,
                          size_t ws_bytes, void* stream) {
   if (!c || !field || !u || !v || !eta || !out_bar || !field_bar) return SISL_ERR_ARG;
-  if (!ws || ws_bytes < sisl_workspace_bytes(c, SISL_WS_FFSL_VJP)) return SISL_ERR_WORKSPACE;
+  if (ws_bad(ws, ws_bytes, sisl_workspace_bytes(c, SISL_WS_FFSL_VJP))) return SISL_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv{(char*)ws};
   auto run = [&](auto tag) {

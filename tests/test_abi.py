@@ -73,6 +73,12 @@ def test_argument_validation_without_gpu():
                                     None) == -1
     assert lib.sisl_ffsl_lines_vjp(_lib.SISL_F32, 0, 4, None, None, 0, None, None, None, None, 0, None) == -1
     assert lib.sisl_ffsl_lines_vjp_workspace_bytes(16, 8) >= 2 * 17 * 8 * 8
+    # a workspace that is absent, short or not 16-byte aligned is refused before
+    # any launch (the pointers are never dereferenced on these paths)
+    need = lib.sisl_ffsl_lines_workspace_bytes(16, 8)
+    fake = ctypes.c_void_p(0x100000)
+    for ws, nb in ((None, need), (ctypes.c_void_p(0x200000), need - 8), (ctypes.c_void_p(0x200008), need + 64)):
+        assert lib.sisl_ffsl_lines(_lib.SISL_F32, 16, 8, fake, fake, 0, fake, ws, nb, None) == -3
     assert lib.sisl_ffsl_lines_vjp_workspace_bytes(0, 8) == 0
     out = ctypes.c_void_p()
     assert lib.sisl_step_graph_create_taped(0, None, None, None, None, None, None, None, None,
